@@ -1,0 +1,821 @@
+// CPU oracle for the SPECFEM++ 2D per-time-step spectral-element update.
+//
+// TEST INFRASTRUCTURE ONLY.  This file is a plain C++ restatement of the
+// reference algorithm, used as the checker by tests/, by the smoke test and
+// as the CPU baseline of bench.py.  The product (libsfg) never links it.
+//
+// Everything is templated on the arithmetic type so that the same code runs
+// in FP32 (the reference's type_real = float) and FP64.  Assembly is serial in
+// element order, so an FP32 run is deterministic; with nthreads > 1 the
+// element loop runs under OpenMP with atomic adds, as the reference's
+// Kokkos OpenMP backend does (timing use only).
+//
+// Reference files restated (paths inside the SPECFEM++ tree):
+//   GLL points / weights        src/quadrature/gll/gll_library.cpp:102-190
+//   hprime(i,j) = l'_j(xi_i)    src/quadrature/gll/lagrange_poly.cpp:161-191
+//   Lagrange interpolants       src/quadrature/gll/lagrange_poly.cpp:11-43
+//   shape functions (4/9 node)  core/specfem/shape_function/dim2/*.cpp
+//   Jacobian                    core/specfem/jacobian/dim2/jacobian.cpp
+//   point location              src/algorithms/dim2/locate_point_impl.cpp
+//   properties                  include/medium/dim2/elastic/isotropic/material.hpp:66-69,
+//                               include/medium/dim2/elastic/isotropic/properties.hpp:71-91,
+//                               include/medium/dim2/acoustic/isotropic/properties.hpp:62-72
+//   mass matrix                 include/kokkos_kernels/impl/compute_mass_matrix.tpp:95-121
+//   Stacey (traction + mass)    include/boundary_conditions/stacey/stacey.tpp:50-80,130-146,296-326,817-853
+//   Stacey edge data            core/specfem/assembly/boundaries/dim2/impl/stacey.tpp,
+//                               core/specfem/assembly/boundaries/dim2/impl/utilities.hpp
+//   edge normals                core/specfem/point/jacobian_matrix.hpp:424-449
+//   free surface                include/boundary_conditions/dirichlet/dirichlet.hpp:38-62
+//   stiffness                   include/kokkos_kernels/impl/compute_stiffness_interaction.tpp:140-247
+//   gradient / divergence       include/algorithms/gradient.hpp:40-82, divergence.hpp:41-74
+//   stress                      include/medium/dim2/elastic/isotropic/stress.hpp:38-129,
+//                               include/medium/dim2/acoustic/isotropic/stress.hpp:33-53
+//   F = J sigma dxi/dx          core/specfem/point/stress.hpp:166-183
+//   sources                     include/kokkos_kernels/impl/compute_source_interaction.tpp,
+//                               include/medium/dim2/{elastic,acoustic}/isotropic/source.hpp,
+//                               core/specfem/assembly/compute_source_array/dim2/impl/compute_source_array_from_vector.cpp,
+//                               core/specfem/source/dim2/vector_source/force_source.cpp
+//   Ricker STF                  core/specfem/source_time_functions/ricker.cpp, impl/time_functions.hpp:78
+//   coupling                    include/kokkos_kernels/impl/compute_coupling.tpp:21-115,
+//                               include/medium/dim2/coupling_terms/{acoustic_elastic,elastic_acoustic}.hpp,
+//                               core/specfem/assembly/conforming_interfaces/dim2/impl/interface_container.tpp
+//   Newmark                     core/specfem/timescheme/newmark.tpp:10-128
+//   step order                  core/specfem/solver/time_marching.tpp:33-83
+//   seismograms                 include/kokkos_kernels/impl/compute_seismogram.tpp,
+//                               include/medium/dim2/acoustic/isotropic/wavefield.hpp,
+//                               core/specfem/assembly/receivers/dim2/impl/seismogram_iterator.hpp:37-53
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <limits>
+#include <map>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <vector>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "oracle2d.h"
+
+namespace {
+
+constexpr int NG = 5;
+constexpr int NP = NG * NG;
+
+// ---------------------------------------------------------------- GLL ---
+double legendre(double x, int n) {
+  double p0 = 1.0, p1 = x;
+  if (n == 0) return 1.0;
+  for (int k = 1; k < n; ++k) {
+    double p2 = ((2.0 * k + 1.0) * x * p1 - k * p0) / (k + 1.0);
+    p0 = p1;
+    p1 = p2;
+  }
+  return p1;
+}
+
+// GLL nodes of degree N=4: the roots of (1-x^2) P'_4(x); closed form for NGLL=5.
+void gll_nodes(double z[NG], double w[NG]) {
+  const double a = std::sqrt(3.0 / 7.0);
+  z[0] = -1.0; z[1] = -a; z[2] = 0.0; z[3] = a; z[4] = 1.0;
+  const int N = NG - 1;
+  for (int i = 0; i < NG; ++i) {
+    double p = legendre(z[i], N);
+    w[i] = 2.0 / (N * (N + 1.0) * p * p);
+  }
+}
+
+// hprime[i][j] = l'_j(xi_i): derivative of the j-th Lagrange polynomial at node i.
+void gll_hprime(const double z[NG], double hp[NG][NG]) {
+  const int N = NG - 1;
+  for (int i = 0; i < NG; ++i)
+    for (int j = 0; j < NG; ++j) {
+      if (i == 0 && j == 0) hp[i][j] = -0.25 * N * (N + 1.0);
+      else if (i == N && j == N) hp[i][j] = 0.25 * N * (N + 1.0);
+      else if (i == j) hp[i][j] = 0.0;
+      else hp[i][j] = legendre(z[i], N) / (legendre(z[j], N) * (z[i] - z[j]));
+    }
+}
+
+template <typename T>
+void lagrange_interp(T xi, const T z[NG], T h[NG], T hp[NG]) {
+  for (int d = 0; d < NG; ++d) {
+    T p1 = 1, p2 = 1, sum = 0;
+    for (int i = 0; i < NG; ++i) {
+      if (i == d) continue;
+      p1 *= (xi - z[i]);
+      p2 *= (z[d] - z[i]);
+      T p3 = 1;
+      for (int j = 0; j < NG; ++j)
+        if (j != d && j != i) p3 *= (xi - z[j]);
+      sum += p3;
+    }
+    T inv = T(1) / p2;
+    h[d] = p1 * inv;
+    hp[d] = sum * inv;
+  }
+}
+
+// ------------------------------------------------------ shape functions ---
+template <typename T>
+void shape2d(T xi, T ga, int ngnod, T *s) {
+  if (ngnod == 4) {
+    s[0] = T(0.25) * (xi - 1) * (ga - 1);
+    s[1] = T(-0.25) * (xi + 1) * (ga - 1);
+    s[2] = T(0.25) * (xi + 1) * (ga + 1);
+    s[3] = T(-0.25) * (xi - 1) * (ga + 1);
+  } else {
+    s[0] = T(0.25) * (xi - 1) * xi * (ga - 1) * ga;
+    s[1] = T(0.25) * (xi + 1) * xi * (ga - 1) * ga;
+    s[2] = T(0.25) * (xi + 1) * xi * (ga + 1) * ga;
+    s[3] = T(0.25) * (xi - 1) * xi * (ga + 1) * ga;
+    s[4] = T(0.5) * (1 - xi * xi) * (ga - 1) * ga;
+    s[5] = T(0.5) * (xi + 1) * xi * (1 - ga * ga);
+    s[6] = T(0.5) * (1 - xi * xi) * (ga + 1) * ga;
+    s[7] = T(0.5) * (xi - 1) * xi * (1 - ga * ga);
+    s[8] = (1 - xi * xi) * (1 - ga * ga);
+  }
+}
+
+template <typename T>
+void dshape2d(T xi, T ga, int ngnod, T *dx, T *dg) {
+  if (ngnod == 4) {
+    const T sp = xi + 1, sm = xi - 1, tp = ga + 1, tm = ga - 1;
+    dx[0] = T(0.25) * tm; dx[1] = T(-0.25) * tm; dx[2] = T(0.25) * tp; dx[3] = T(-0.25) * tp;
+    dg[0] = T(0.25) * sm; dg[1] = T(-0.25) * sp; dg[2] = T(0.25) * sp; dg[3] = T(-0.25) * sm;
+  } else {
+    const T sp = xi + 1, sm = xi - 1, tp = ga + 1, tm = ga - 1;
+    const T s2 = xi * 2, t2 = ga * 2, ss = xi * xi, tt = ga * ga, st = xi * ga;
+    dx[0] = T(0.25) * tm * ga * (s2 - 1); dx[1] = T(0.25) * tm * ga * (s2 + 1);
+    dx[2] = T(0.25) * tp * ga * (s2 + 1); dx[3] = T(0.25) * tp * ga * (s2 - 1);
+    dg[0] = T(0.25) * sm * xi * (t2 - 1); dg[1] = T(0.25) * sp * xi * (t2 - 1);
+    dg[2] = T(0.25) * sp * xi * (t2 + 1); dg[3] = T(0.25) * sm * xi * (t2 + 1);
+    dx[4] = -st * tm; dx[5] = T(0.5) * (1 - tt) * (s2 + 1);
+    dx[6] = -st * tp; dx[7] = T(0.5) * (1 - tt) * (s2 - 1);
+    dg[4] = T(0.5) * (1 - ss) * (t2 - 1); dg[5] = -st * sp;
+    dg[6] = T(0.5) * (1 - ss) * (t2 + 1); dg[7] = -st * sm;
+    dx[8] = -s2 * (1 - tt); dg[8] = -t2 * (1 - ss);
+  }
+}
+
+template <typename T>
+struct Jac {
+  T xix, gammax, xiz, gammaz, jac;
+};
+
+template <typename T>
+Jac<T> jacobian_at(const T *cx, const T *cz, int ngnod, T xi, T ga) {
+  T dx[9], dg[9];
+  dshape2d<T>(xi, ga, ngnod, dx, dg);
+  T xxi = 0, zxi = 0, xga = 0, zga = 0;
+  for (int n = 0; n < ngnod; ++n) {
+    xxi += dx[n] * cx[n]; zxi += dx[n] * cz[n];
+    xga += dg[n] * cx[n]; zga += dg[n] * cz[n];
+  }
+  T j = xxi * zga - xga * zxi;
+  return {zga / j, -zxi / j, -xga / j, xxi / j, j};
+}
+
+template <typename T>
+void location_at(const T *cx, const T *cz, int ngnod, T xi, T ga, T &x, T &z) {
+  T s[9];
+  shape2d<T>(xi, ga, ngnod, s);
+  x = 0; z = 0;
+  for (int n = 0; n < ngnod; ++n) { x += s[n] * cx[n]; z += s[n] * cz[n]; }
+}
+
+// -------------------------------------------------------------- model ---
+enum { BOTTOM = 0, RIGHT = 1, TOP = 2, LEFT = 3 };
+enum { MED_ACOUSTIC = 0, MED_ELASTIC = 1 };
+
+bool on_edge(int type, int iz, int ix) {
+  return (type == TOP && iz == NG - 1) || (type == BOTTOM && iz == 0) ||
+         (type == LEFT && ix == 0) || (type == RIGHT && ix == NG - 1);
+}
+
+template <typename T>
+struct Sim {
+  const OracleInput2D &in;
+  int nspec, nglob = 0, ngnod;
+  T z[NG], w[NG], hp[NG][NG];
+  std::vector<int> ibool;           // [nspec][25]
+  std::vector<T> xix, xiz, gax, gaz, jac;  // [nspec][25]
+  std::vector<T> gx, gz;            // coordinates of local points
+  std::vector<int> medium;          // [nspec]
+  // elastic: kappa, mu, rho; acoustic: rho_inverse, kappa
+  std::vector<T> p_kappa, p_mu, p_rho, p_rhoinv;
+  // Stacey point data per element (dense, tag 0/1)
+  std::vector<uint8_t> st_tag, fs_tag;   // [nspec][25]
+  std::vector<T> st_nx, st_nz, st_w;     // [nspec][25]
+  // fields: acoustic (1 comp) and elastic (ncomp_el comps), indexed by global id
+  int ncomp_el;
+  std::vector<T> ua, va, aa, minv_a;
+  std::vector<T> ue, ve, ae, minv_e;    // [nglob][ncomp_el]
+  std::vector<uint8_t> is_ac_glob, is_el_glob;
+  // coupling point lists
+  struct CPoint { int ispec, iz, ix, iglob; T nx, nz, fac; };
+  std::vector<CPoint> cpl_ac, cpl_el;   // self acoustic / self elastic
+  // sources
+  struct Src { int ispec; int medium; T arr[2][NP]; int ncomp; std::vector<T> stf; };
+  std::vector<Src> srcs;
+  struct Rec { int ispec; T h[NP]; };
+  std::vector<Rec> recs;
+  T dt;
+
+  explicit Sim(const OracleInput2D &in_) : in(in_), nspec(in_.nspec), ngnod(in_.ngnod) {}
+
+  void setup() {
+    double zd[NG], wd[NG], hpd[NG][NG];
+    gll_nodes(zd, wd);
+    gll_hprime(zd, hpd);
+    for (int i = 0; i < NG; ++i) {
+      z[i] = T(zd[i]); w[i] = T(wd[i]);
+      for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
+    }
+    dt = T(in.dt);
+    ncomp_el = in.elastic_sh ? 1 : 2;
+    number_points();
+    geometry();
+    properties();
+    boundaries();
+    coupling();
+    mass();
+    sources();
+    receivers();
+  }
+
+  // Global numbering by element topology: corners by control-node id, edge
+  // points by (corner pair, position), element-interior points unique.
+  void number_points() {
+    ibool.assign(size_t(nspec) * NP, -1);
+    std::map<int, int> corner_id;
+    std::map<std::tuple<int, int, int>, int> edge_id;
+    const int cz[4] = {0, 0, NG - 1, NG - 1}, cxx[4] = {0, NG - 1, NG - 1, 0};
+    for (int e = 0; e < nspec; ++e) {
+      const int *kn = in.knods + size_t(e) * ngnod;
+      for (int c = 0; c < 4; ++c) {
+        auto it = corner_id.find(kn[c]);
+        int id;
+        if (it == corner_id.end()) { id = nglob++; corner_id[kn[c]] = id; }
+        else id = it->second;
+        ibool[size_t(e) * NP + cz[c] * NG + cxx[c]] = id;
+      }
+      // edges: (corner A at position 0, corner B at position 4, point(t))
+      for (int ed = 0; ed < 4; ++ed) {
+        int A, B;
+        if (ed == BOTTOM) { A = 0; B = 1; } else if (ed == RIGHT) { A = 1; B = 2; }
+        else if (ed == TOP) { A = 3; B = 2; } else { A = 0; B = 3; }
+        for (int t = 1; t < NG - 1; ++t) {
+          int iz, ix;
+          if (ed == BOTTOM) { iz = 0; ix = t; } else if (ed == RIGHT) { iz = t; ix = NG - 1; }
+          else if (ed == TOP) { iz = NG - 1; ix = t; } else { iz = t; ix = 0; }
+          int na = kn[A], nb = kn[B];
+          int k = na < nb ? t : NG - 1 - t;
+          auto key = std::make_tuple(std::min(na, nb), std::max(na, nb), k);
+          auto it = edge_id.find(key);
+          int id;
+          if (it == edge_id.end()) { id = nglob++; edge_id[key] = id; }
+          else id = it->second;
+          ibool[size_t(e) * NP + iz * NG + ix] = id;
+        }
+      }
+      for (int iz = 1; iz < NG - 1; ++iz)
+        for (int ix = 1; ix < NG - 1; ++ix) ibool[size_t(e) * NP + iz * NG + ix] = nglob++;
+    }
+  }
+
+  void ctrl(int e, T *cx, T *cz) const {
+    for (int n = 0; n < ngnod; ++n) {
+      int id = in.knods[size_t(e) * ngnod + n];
+      cx[n] = T(in.coorg[2 * size_t(id)]);
+      cz[n] = T(in.coorg[2 * size_t(id) + 1]);
+    }
+  }
+
+  void geometry() {
+    size_t n = size_t(nspec) * NP;
+    xix.resize(n); xiz.resize(n); gax.resize(n); gaz.resize(n); jac.resize(n);
+    gx.resize(n); gz.resize(n);
+    for (int e = 0; e < nspec; ++e) {
+      T cx[9], cz[9];
+      ctrl(e, cx, cz);
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) {
+          size_t p = size_t(e) * NP + iz * NG + ix;
+          Jac<T> J = jacobian_at<T>(cx, cz, ngnod, z[ix], z[iz]);
+          xix[p] = J.xix; gax[p] = J.gammax; xiz[p] = J.xiz; gaz[p] = J.gammaz; jac[p] = J.jac;
+          location_at<T>(cx, cz, ngnod, z[ix], z[iz], gx[p], gz[p]);
+        }
+    }
+  }
+
+  void properties() {
+    size_t n = size_t(nspec) * NP;
+    medium.assign(in.medium, in.medium + nspec);
+    p_kappa.resize(n); p_mu.resize(n); p_rho.resize(n); p_rhoinv.resize(n);
+    for (size_t p = 0; p < n; ++p) {
+      const T rho = T(in.rho[p]), vp = T(in.vp[p]), vs = T(in.vs[p]);
+      if (medium[p / NP] == MED_ELASTIC) {
+        p_mu[p] = rho * vs * vs;
+        p_kappa[p] = rho * (vp * vp - T(4.0 / 3.0) * vs * vs);
+        p_rho[p] = rho;
+      } else {
+        p_rhoinv[p] = T(1) / rho;
+        p_kappa[p] = rho * vp * vp;
+        p_rho[p] = rho;
+      }
+    }
+  }
+
+  T lp2m(size_t p) const { return p_kappa[p] + T(4.0 / 3.0) * p_mu[p]; }
+  T rho_vp(size_t p) const { return std::sqrt(lp2m(p) / p_rho[p]) * p_rho[p]; }
+  T rho_vs(size_t p) const { return std::sqrt(p_rho[p] * p_mu[p]); }
+  T rho_vpinv(size_t p) const { return std::sqrt(p_rhoinv[p] * (T(1) / p_kappa[p])); }
+
+  void normal(size_t p, int type, T &nx, T &nz) const {
+    if (type == BOTTOM) { nx = T(-1) * gax[p] * jac[p]; nz = T(-1) * gaz[p] * jac[p]; }
+    else if (type == TOP) { nx = gax[p] * jac[p]; nz = gaz[p] * jac[p]; }
+    else if (type == LEFT) { nx = T(-1) * xix[p] * jac[p]; nz = T(-1) * xiz[p] * jac[p]; }
+    else { nx = xix[p] * jac[p]; nz = xiz[p] * jac[p]; }
+  }
+
+  void boundaries() {
+    size_t n = size_t(nspec) * NP;
+    st_tag.assign(n, 0); fs_tag.assign(n, 0);
+    st_nx.assign(n, 0); st_nz.assign(n, 0); st_w.assign(n, 0);
+    // entries applied in order of appearance; a later edge of the same element
+    // overwrites the normal/weight of a shared corner point (stacey.tpp).
+    for (int i = 0; i < in.nabs; ++i) {
+      int e = in.abs_ispec[i], type = in.abs_type[i];
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) {
+          if (!on_edge(type, iz, ix)) continue;
+          size_t p = size_t(e) * NP + iz * NG + ix;
+          st_tag[p] = 1;
+          normal(p, type, st_nx[p], st_nz[p]);
+          st_w[p] = (type == LEFT || type == RIGHT) ? w[iz] : w[ix];
+        }
+    }
+    for (int i = 0; i < in.nfree; ++i) {
+      int e = in.free_ispec[i], type = in.free_type[i];
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix)
+          if (on_edge(type, iz, ix)) fs_tag[size_t(e) * NP + iz * NG + ix] = 1;
+    }
+  }
+
+  // acoustic/elastic shared edges: for each element pair sharing an edge,
+  // one self point list per side (interface_container.tpp).
+  void coupling() {
+    std::map<std::pair<int, int>, std::vector<std::pair<int, int>>> edges;  // corner pair -> (elem, type)
+    for (int e = 0; e < nspec; ++e) {
+      const int *kn = in.knods + size_t(e) * ngnod;
+      const int ends[4][2] = {{0, 1}, {1, 2}, {3, 2}, {0, 3}};
+      for (int ed = 0; ed < 4; ++ed) {
+        int a = kn[ends[ed][0]], b = kn[ends[ed][1]];
+        edges[{std::min(a, b), std::max(a, b)}].push_back({e, ed});
+      }
+    }
+    for (auto &kv : edges) {
+      if (kv.second.size() != 2) continue;
+      auto [e1, t1] = kv.second[0];
+      auto [e2, t2] = kv.second[1];
+      if (medium[e1] == medium[e2]) continue;
+      for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
+        for (int iz = 0; iz < NG; ++iz)
+          for (int ix = 0; ix < NG; ++ix) {
+            if (!on_edge(t, iz, ix)) continue;
+            size_t p = size_t(e) * NP + iz * NG + ix;
+            CPoint c;
+            c.ispec = e; c.iz = iz; c.ix = ix; c.iglob = ibool[p];
+            normal(p, t, c.nx, c.nz);
+            c.fac = (t == BOTTOM || t == TOP) ? w[ix] : w[iz];
+            (medium[e] == MED_ACOUSTIC ? cpl_ac : cpl_el).push_back(c);
+          }
+      }
+    }
+  }
+
+  // Stacey traction (stacey.tpp:50-80 P-SV, :130-146 SH, :296-326 acoustic)
+  void stacey(size_t p, const T *vel, T *acc) const {
+    const T nx = st_nx[p], nz = st_nz[p];
+    const T j1 = std::sqrt(nx * nx + nz * nz);
+    if (medium[p / NP] == MED_ACOUSTIC) {
+      const T f = st_w[p] * j1;
+      acc[0] += T(-1) * f * rho_vpinv(p) * vel[0];
+    } else if (ncomp_el == 1) {
+      const T f = st_w[p] * j1;
+      acc[0] += T(-1) * f * rho_vs(p) * vel[0];
+    } else {
+      const T vn = vel[0] * nx + vel[1] * nz;
+      const T dn[2] = {nx, nz};
+      T fac[2];
+      for (int c = 0; c < 2; ++c)
+        fac[c] = ((vn * dn[c] / (j1 * j1)) * (rho_vp(p) - rho_vs(p))) + vel[c] * rho_vs(p);
+      acc[0] += T(-1) * fac[0] * j1 * st_w[p];
+      acc[1] += T(-1) * fac[1] * j1 * st_w[p];
+    }
+  }
+
+  void mass() {
+    ua.assign(nglob, 0); va.assign(nglob, 0); aa.assign(nglob, 0); minv_a.assign(nglob, 0);
+    size_t ne = size_t(nglob) * ncomp_el;
+    ue.assign(ne, 0); ve.assign(ne, 0); ae.assign(ne, 0); minv_e.assign(ne, 0);
+    is_ac_glob.assign(nglob, 0); is_el_glob.assign(nglob, 0);
+    for (int e = 0; e < nspec; ++e)
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) {
+          size_t p = size_t(e) * NP + iz * NG + ix;
+          int g = ibool[p];
+          T fac = w[ix] * w[iz] * jac[p];
+          if (medium[e] == MED_ACOUSTIC) {
+            is_ac_glob[g] = 1;
+            T m = (T(1) / p_kappa[p]) * fac;
+            if (st_tag[p]) {
+              T v = T(-1) * dt * T(0.5);
+              T acc = m;
+              stacey(p, &v, &acc);
+              m = acc;
+            }
+            minv_a[g] += m;
+          } else {
+            is_el_glob[g] = 1;
+            T m[2] = {p_rho[p] * fac, p_rho[p] * fac};
+            if (st_tag[p]) {
+              T v[2] = {T(-1) * dt * T(0.5), T(-1) * dt * T(0.5)};
+              stacey(p, v, m);
+            }
+            for (int c = 0; c < ncomp_el; ++c) minv_e[size_t(g) * ncomp_el + c] += m[c];
+          }
+        }
+    for (int g = 0; g < nglob; ++g) {
+      if (is_ac_glob[g]) minv_a[g] = T(1) / minv_a[g];
+      if (is_el_glob[g])
+        for (int c = 0; c < ncomp_el; ++c)
+          minv_e[size_t(g) * ncomp_el + c] = T(1) / minv_e[size_t(g) * ncomp_el + c];
+    }
+  }
+
+  // ------------------------------------------------- point location ---
+  std::tuple<int, T, T> locate(double X, double Z) const {
+    const T x = T(X), zz = T(Z);
+    T best = std::numeric_limits<T>::max();
+    int eg = -1;
+    for (int e = 0; e < nspec; ++e)
+      for (int q = 0; q < NP; ++q) {
+        size_t p = size_t(e) * NP + q;
+        T d = std::sqrt((gx[p] - x) * (gx[p] - x) + (gz[p] - zz) * (gz[p] - zz));
+        if (d < best) { best = d; eg = e; }
+      }
+    // candidates: guess first, then elements sharing a corner node with it
+    std::vector<int> cand{eg};
+    const int *kg = in.knods + size_t(eg) * ngnod;
+    for (int e = 0; e < nspec; ++e) {
+      if (e == eg) continue;
+      const int *ke = in.knods + size_t(e) * ngnod;
+      bool share = false;
+      for (int a = 0; a < 4 && !share; ++a)
+        for (int b = 0; b < 4; ++b)
+          if (kg[a] == ke[b]) { share = true; break; }
+      if (share) cand.push_back(e);
+    }
+    T fd = std::numeric_limits<T>::max();
+    int es = -1; T xs = -9999, gs = -9999;
+    for (int e : cand) {
+      T cx[9], cz[9];
+      ctrl(e, cx, cz);
+      T xi = 0, ga = 0;
+      for (int it = 0; it < 100; ++it) {
+        T lx, lz;
+        location_at<T>(cx, cz, ngnod, xi, ga, lx, lz);
+        Jac<T> J = jacobian_at<T>(cx, cz, ngnod, xi, ga);
+        T dx = -(lx - x), dz = -(lz - zz);
+        T dxi = J.xix * dx + J.xiz * dz, dga = J.gammax * dx + J.gammaz * dz;
+        xi += dxi; ga += dga;
+        xi = std::min(std::max(xi, T(-1.01)), T(1.01));
+        ga = std::min(std::max(ga, T(-1.01)), T(1.01));
+        if (std::abs(dxi) < 1e-12 && std::abs(dga) < 1e-12) break;
+      }
+      T lx, lz;
+      location_at<T>(cx, cz, ngnod, xi, ga, lx, lz);
+      T d = std::sqrt((lx - x) * (lx - x) + (lz - zz) * (lz - zz));
+      if (d < fd) { fd = d; es = e; xs = xi; gs = ga; }
+    }
+    if (es < 0 || std::abs(std::abs(xs) - T(1.01)) < T(1e-6) || std::abs(std::abs(gs) - T(1.01)) < T(1e-6))
+      throw std::runtime_error("Failed to locate point in the mesh");
+    return {es, xs, gs};
+  }
+
+  void sources() {
+    const int nstep = in.nstep;
+    for (int s = 0; s < in.nsrc; ++s) {
+      auto [e, xi, ga] = locate(in.src_x[s], in.src_z[s]);
+      Src S;
+      S.ispec = e;
+      S.medium = medium[e];
+      T hx[NG], hpx[NG], hg[NG], hpg[NG];
+      lagrange_interp<T>(xi, z, hx, hpx);
+      lagrange_interp<T>(ga, z, hg, hpg);
+      T fv[2];
+      if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
+      else {
+        S.ncomp = 2;
+        T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
+        fv[0] = std::sin(ang); fv[1] = std::cos(ang);
+      }
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix)
+          for (int c = 0; c < S.ncomp; ++c) S.arr[c][iz * NG + ix] = hx[ix] * hg[iz] * fv[c];
+      S.stf.resize(size_t(nstep));
+      if (in.stf_table) {
+        for (int i = 0; i < nstep; ++i) S.stf[i] = T(in.stf_table[size_t(i) * in.nsrc + s]);
+      } else {
+        const T f0 = T(in.src_f0[s]), fac = T(in.src_factor[s]), tsh = T(in.src_tshift[s]);
+        const T t0 = T(in.t0);
+        const T pi = T(M_PI);
+        for (int i = 0; i < nstep; ++i) {
+          T t = t0 + T(i) * dt - tsh;
+          T a = pi * pi * f0 * f0;
+          S.stf[i] = fac * ((T(1) - T(2) * a * t * t) * std::exp(-a * t * t));
+        }
+      }
+      srcs.push_back(S);
+    }
+  }
+
+  void receivers() {
+    for (int r = 0; r < in.nrec; ++r) {
+      auto [e, xi, ga] = locate(in.rec_x[r], in.rec_z[r]);
+      Rec R;
+      R.ispec = e;
+      T hx[NG], hpx[NG], hg[NG], hpg[NG];
+      lagrange_interp<T>(xi, z, hx, hpx);
+      lagrange_interp<T>(ga, z, hg, hpg);
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) R.h[iz * NG + ix] = hx[ix] * hg[iz];
+      recs.push_back(R);
+    }
+  }
+
+  // --------------------------------------------------------- kernels ---
+  template <typename AddFn>
+  void stiffness_element(int e, int ncomp, const std::vector<T> &u, const std::vector<T> &v,
+                         AddFn add) const {
+    T fu[NP][2], F[NP][2][2];
+    const int *ib = &ibool[size_t(e) * NP];
+    for (int q = 0; q < NP; ++q)
+      for (int c = 0; c < ncomp; ++c) fu[q][c] = u[size_t(ib[q]) * ncomp + c];
+    const bool acoustic = medium[e] == MED_ACOUSTIC;
+    for (int iz = 0; iz < NG; ++iz)
+      for (int ix = 0; ix < NG; ++ix) {
+        const int q = iz * NG + ix;
+        const size_t p = size_t(e) * NP + q;
+        T dxi[2] = {0, 0}, dga[2] = {0, 0};
+        for (int l = 0; l < NG; ++l)
+          for (int c = 0; c < ncomp; ++c) {
+            dxi[c] += hp[ix][l] * fu[iz * NG + l][c];
+            dga[c] += hp[iz][l] * fu[l * NG + ix][c];
+          }
+        T du[2][2];
+        for (int c = 0; c < ncomp; ++c) {
+          du[c][0] = xix[p] * dxi[c] + gax[p] * dga[c];
+          du[c][1] = xiz[p] * dxi[c] + gaz[p] * dga[c];
+        }
+        T S[2][2];
+        if (acoustic) {
+          S[0][0] = p_rhoinv[p] * du[0][0];
+          S[0][1] = p_rhoinv[p] * du[0][1];
+        } else if (ncomp == 1) {
+          S[0][0] = p_mu[p] * du[0][0];
+          S[0][1] = p_mu[p] * du[0][1];
+        } else {
+          const T l2m = lp2m(p), lam = l2m - T(2) * p_mu[p];
+          const T sxx = l2m * du[0][0] + lam * du[1][1];
+          const T szz = l2m * du[1][1] + lam * du[0][0];
+          const T sxz = p_mu[p] * (du[0][1] + du[1][0]);
+          S[0][0] = sxx; S[0][1] = sxz; S[1][0] = sxz; S[1][1] = szz;
+        }
+        for (int c = 0; c < ncomp; ++c) {
+          F[q][c][0] = jac[p] * (S[c][0] * xix[p] + S[c][1] * xiz[p]);
+          F[q][c][1] = jac[p] * (S[c][0] * gax[p] + S[c][1] * gaz[p]);
+        }
+      }
+    for (int iz = 0; iz < NG; ++iz)
+      for (int ix = 0; ix < NG; ++ix) {
+        const int q = iz * NG + ix;
+        const size_t p = size_t(e) * NP + q;
+        T t1[2] = {0, 0}, t2[2] = {0, 0};
+        for (int l = 0; l < NG; ++l) {
+          for (int c = 0; c < ncomp; ++c) t1[c] += F[iz * NG + l][c][0] * hp[l][ix] * w[l];
+          for (int c = 0; c < ncomp; ++c) t2[c] += F[l * NG + ix][c][1] * hp[l][iz] * w[l];
+        }
+        T acc[2];
+        for (int c = 0; c < ncomp; ++c) acc[c] = T(-1) * (w[iz] * t1[c] + w[ix] * t2[c]);
+        if (st_tag[p]) {
+          T vel[2];
+          for (int c = 0; c < ncomp; ++c) vel[c] = v[size_t(ib[q]) * ncomp + c];
+          stacey(p, vel, acc);
+        }
+        if (acoustic && fs_tag[p]) acc[0] = 0;
+        add(ib[q], acc);
+      }
+  }
+
+  void predictor(std::vector<T> &u, std::vector<T> &v, std::vector<T> &a) {
+    const T dt2 = dt / T(2.0), dtsq2 = dt * dt / T(2.0);
+    for (size_t i = 0; i < u.size(); ++i) {
+      u[i] += dt * v[i] + dtsq2 * a[i];
+      v[i] += dt2 * a[i];
+      a[i] = 0;
+    }
+  }
+  void corrector(std::vector<T> &v, const std::vector<T> &a) {
+    const T dt2 = dt / T(2.0);
+    for (size_t i = 0; i < v.size(); ++i) v[i] += dt2 * a[i];
+  }
+
+  void update_medium(int med, int istep, int nthreads) {
+    const int ncomp = med == MED_ACOUSTIC ? 1 : ncomp_el;
+    std::vector<T> &u = med == MED_ACOUSTIC ? ua : ue;
+    std::vector<T> &v = med == MED_ACOUSTIC ? va : ve;
+    std::vector<T> &a = med == MED_ACOUSTIC ? aa : ae;
+    const std::vector<T> &minv = med == MED_ACOUSTIC ? minv_a : minv_e;
+    // coupling (domain_kernels.hpp:77-94)
+    if (med == MED_ACOUSTIC) {
+      for (const auto &c : cpl_ac) {
+        T val = c.fac * (c.nx * ue[size_t(c.iglob) * ncomp_el + 0] + c.nz * ue[size_t(c.iglob) * ncomp_el + 1]);
+        if (fs_tag[size_t(c.ispec) * NP + c.iz * NG + c.ix]) val = 0;
+        a[c.iglob] += val;
+      }
+    } else if (ncomp_el == 2) {
+      for (const auto &c : cpl_el) {
+        a[size_t(c.iglob) * 2 + 0] += c.fac * c.nx * aa[c.iglob];
+        a[size_t(c.iglob) * 2 + 1] += c.fac * c.nz * aa[c.iglob];
+      }
+    }
+    // sources (:96-110)
+    for (const auto &S : srcs) {
+      if (S.medium != med) continue;
+      const int *ib = &ibool[size_t(S.ispec) * NP];
+      for (int q = 0; q < NP; ++q) {
+        size_t p = size_t(S.ispec) * NP + q;
+        if (med == MED_ACOUSTIC)
+          a[ib[q]] += -S.stf[istep] * S.arr[0][q] / p_kappa[p];
+        else
+          for (int c = 0; c < ncomp; ++c) a[size_t(ib[q]) * ncomp + c] += S.stf[istep] * S.arr[c][q];
+      }
+    }
+    // stiffness (:112-126)
+#ifdef _OPENMP
+    if (nthreads > 1) {
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+      for (int e = 0; e < nspec; ++e) {
+        if (medium[e] != med) continue;
+        stiffness_element(e, ncomp, u, v, [&](int g, const T *acc) {
+          for (int c = 0; c < ncomp; ++c) {
+#pragma omp atomic
+            a[size_t(g) * ncomp + c] += acc[c];
+          }
+        });
+      }
+    } else
+#endif
+    {
+      for (int e = 0; e < nspec; ++e) {
+        if (medium[e] != med) continue;
+        stiffness_element(e, ncomp, u, v, [&](int g, const T *acc) {
+          for (int c = 0; c < ncomp; ++c) a[size_t(g) * ncomp + c] += acc[c];
+        });
+      }
+    }
+    // divide by mass (:128-138), only on this medium's points
+    const std::vector<uint8_t> &own = med == MED_ACOUSTIC ? is_ac_glob : is_el_glob;
+    for (int g = 0; g < nglob; ++g)
+      if (own[g])
+        for (int c = 0; c < ncomp; ++c) a[size_t(g) * ncomp + c] *= minv[size_t(g) * ncomp + c];
+  }
+
+  // seismogram value of one receiver for one type (compute_seismogram.tpp)
+  void seismo(const Rec &R, int type, T out[2]) const {
+    const int e = R.ispec;
+    const int *ib = &ibool[size_t(e) * NP];
+    out[0] = out[1] = 0;
+    if (medium[e] == MED_ACOUSTIC) {
+      const std::vector<T> &f = type == 0 ? ua : type == 1 ? va : aa;
+      if (type == 3) {
+        for (int q = 0; q < NP; ++q) out[0] += R.h[q] * (T(-1.0) * aa[ib[q]]);
+        return;
+      }
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) {
+          const int q = iz * NG + ix;
+          const size_t p = size_t(e) * NP + q;
+          T dxi = 0, dga = 0;
+          for (int l = 0; l < NG; ++l) {
+            dxi += hp[ix][l] * f[ib[iz * NG + l]];
+            dga += hp[iz][l] * f[ib[l * NG + ix]];
+          }
+          T dx = xix[p] * dxi + gax[p] * dga, dz = xiz[p] * dxi + gaz[p] * dga;
+          out[0] += R.h[q] * (p_rhoinv[p] * dx);
+          out[1] += R.h[q] * (p_rhoinv[p] * dz);
+        }
+      return;
+    }
+    const std::vector<T> &f = type == 0 ? ue : type == 1 ? ve : ae;
+    for (int q = 0; q < NP; ++q)
+      for (int c = 0; c < ncomp_el; ++c) out[c] += R.h[q] * f[size_t(ib[q]) * ncomp_el + c];
+  }
+
+  void run(double *seis, int nthreads) {
+    const int nsb = std::max(1, in.nstep_between_samples);
+    int isig = 0;
+    const T ca = std::cos(T(M_PI) / T(180) * T(in.rec_angle));
+    const T sa = std::sin(T(M_PI) / T(180) * T(in.rec_angle));
+    for (int istep = 0; istep < in.nstep; ++istep) {
+      predictor(ua, va, aa);
+      predictor(ue, ve, ae);
+      update_medium(MED_ACOUSTIC, istep, nthreads);
+      corrector(va, aa);
+      update_medium(MED_ELASTIC, istep, nthreads);
+      corrector(ve, ae);
+      if (istep % nsb == 0 && seis) {
+        for (int t = 0; t < in.ntypes; ++t)
+          for (int r = 0; r < in.nrec; ++r) {
+            T o[2];
+            seismo(recs[r], in.seis_types[t], o);
+            size_t k = ((size_t(isig) * in.ntypes + t) * in.nrec + r) * 2;
+            seis[k + 0] = double(ca * o[0] - sa * o[1]);
+            seis[k + 1] = double(sa * o[0] + ca * o[1]);
+          }
+        ++isig;
+      }
+    }
+  }
+};
+
+template <typename T>
+int run_impl(const OracleInput2D *in, OracleOutput2D *out, int nthreads) {
+  try {
+    Sim<T> s(*in);
+    s.setup();
+    s.run(out->seismograms, nthreads);
+    out->nglob = s.nglob;
+    if (out->final_u_elastic) {
+      for (size_t i = 0; i < s.ue.size(); ++i) out->final_u_elastic[i] = double(s.ue[i]);
+    }
+    if (out->final_u_acoustic) {
+      for (size_t i = 0; i < s.ua.size(); ++i) out->final_u_acoustic[i] = double(s.ua[i]);
+    }
+    if (out->ibool) std::copy(s.ibool.begin(), s.ibool.end(), out->ibool);
+    return 0;
+  } catch (const std::exception &ex) {
+    std::snprintf(out->error, sizeof(out->error), "%s", ex.what());
+    return -1;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle2d_run_f32(const OracleInput2D *in, OracleOutput2D *out, int nthreads) {
+  return run_impl<float>(in, out, nthreads);
+}
+
+int oracle2d_run_f64(const OracleInput2D *in, OracleOutput2D *out, int nthreads) {
+  return run_impl<double>(in, out, nthreads);
+}
+
+// Count global points of a mesh (so callers can size final-field buffers).
+int oracle2d_count_nglob(const OracleInput2D *in) {
+  Sim<double> s(*in);
+  s.number_points();
+  return s.nglob;
+}
+
+// Known-answer helpers used by the unit tests.
+void oracle_gll(double *z, double *w, double *hprime) {
+  double zz[NG], ww[NG], hp[NG][NG];
+  gll_nodes(zz, ww);
+  gll_hprime(zz, hp);
+  for (int i = 0; i < NG; ++i) {
+    z[i] = zz[i]; w[i] = ww[i];
+    for (int j = 0; j < NG; ++j) hprime[i * NG + j] = hp[i][j];
+  }
+}
+
+double oracle_legendre(double x, int n) { return legendre(x, n); }
+
+// 2D elastic isotropic P-SV stress (stress.hpp:38-78); du row-major [2][2].
+void oracle_stress_psv(double kappa, double mu, const double *du, double *sigma) {
+  double l2m = kappa + 4.0 / 3.0 * mu, lam = l2m - 2.0 * mu;
+  sigma[0] = l2m * du[0] + lam * du[3];
+  sigma[1] = mu * (du[1] + du[2]);
+  sigma[2] = sigma[1];
+  sigma[3] = l2m * du[3] + lam * du[0];
+}
+
+}  // extern "C"

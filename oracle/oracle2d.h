@@ -1,0 +1,49 @@
+/* CPU oracle for the SPECFEM++ 2D time step (test infrastructure only). */
+#pragma once
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct OracleInput2D {
+  int nspec, npgeo, ngnod;
+  const double *coorg;   /* [npgeo][2] */
+  const int *knods;      /* [nspec][ngnod], 0-based */
+  const int *medium;     /* [nspec]: 0 acoustic, 1 elastic */
+  const double *rho, *vp, *vs; /* [nspec][25] per GLL point */
+  int elastic_sh;        /* 0: P-SV, 1: SH */
+  int nabs;
+  const int *abs_ispec, *abs_type;   /* type: 0 bottom 1 right 2 top 3 left */
+  int nfree;
+  const int *free_ispec, *free_type;
+  int nsrc;
+  const double *src_x, *src_z, *src_angle, *src_f0, *src_factor, *src_tshift;
+  const double *stf_table; /* optional [nstep][nsrc]; overrides Ricker */
+  double t0;
+  int nrec;
+  const double *rec_x, *rec_z;
+  double rec_angle;
+  int ntypes;
+  const int *seis_types;   /* 0 displacement 1 velocity 2 acceleration 3 pressure */
+  double dt;
+  int nstep, nstep_between_samples;
+} OracleInput2D;
+
+typedef struct OracleOutput2D {
+  double *seismograms;       /* [nsig][ntypes][nrec][2] */
+  double *final_u_elastic;   /* optional [nglob][ncomp] */
+  double *final_u_acoustic;  /* optional [nglob] */
+  int *ibool;                /* optional [nspec][25] */
+  int nglob;
+  char error[256];
+} OracleOutput2D;
+
+int oracle2d_run_f32(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
+int oracle2d_run_f64(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
+int oracle2d_count_nglob(const OracleInput2D *in);
+void oracle_gll(double *z, double *w, double *hprime);
+double oracle_legendre(double x, int n);
+void oracle_stress_psv(double kappa, double mu, const double *du, double *sigma);
+
+#ifdef __cplusplus
+}
+#endif

@@ -1,0 +1,311 @@
+"""ctypes front-end of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline leg of bench.py
+may import this module.  It loads ``oracle/_build/liboracle.so`` (built by
+``oracle/Makefile``), turns a mesh plus source/receiver description into the
+plain arrays of ``OracleInput2D`` and returns seismograms as numpy arrays.
+
+The start time follows ``src/io/sources/dim2/read_sources.cpp:142-172``: t0 is
+the minimum of the sources' ``-1.2/f0 + tshift`` and each source's tshift is
+replaced by ``t0_source - t0``.  Seismogram times are
+``isig * dt * nstep_between_samples + t0``
+(``core/specfem/assembly/receivers/dim2/impl/seismogram_iterator.hpp:38``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .database2d import Mesh2D, read_database
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+SEIS_TYPES = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3}
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class OracleInput2D(C.Structure):
+    _fields_ = [
+        ("nspec", C.c_int), ("npgeo", C.c_int), ("ngnod", C.c_int),
+        ("coorg", _dp), ("knods", _ip), ("medium", _ip),
+        ("rho", _dp), ("vp", _dp), ("vs", _dp),
+        ("elastic_sh", C.c_int),
+        ("nabs", C.c_int), ("abs_ispec", _ip), ("abs_type", _ip),
+        ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
+        ("nsrc", C.c_int), ("src_x", _dp), ("src_z", _dp), ("src_angle", _dp),
+        ("src_f0", _dp), ("src_factor", _dp), ("src_tshift", _dp),
+        ("stf_table", _dp), ("t0", C.c_double),
+        ("nrec", C.c_int), ("rec_x", _dp), ("rec_z", _dp), ("rec_angle", C.c_double),
+        ("ntypes", C.c_int), ("seis_types", _ip),
+        ("dt", C.c_double), ("nstep", C.c_int), ("nstep_between_samples", C.c_int),
+    ]
+
+
+class OracleOutput2D(C.Structure):
+    _fields_ = [
+        ("seismograms", _dp), ("final_u_elastic", _dp), ("final_u_acoustic", _dp),
+        ("ibool", _ip), ("nglob", C.c_int), ("error", C.c_char * 256),
+    ]
+
+
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle shared library with its Makefile."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        _lib = C.CDLL(LIB_PATH)
+        for name in ("oracle2d_run_f32", "oracle2d_run_f64"):
+            fn = getattr(_lib, name)
+            fn.argtypes = [C.POINTER(OracleInput2D), C.POINTER(OracleOutput2D), C.c_int]
+            fn.restype = C.c_int
+        _lib.oracle2d_count_nglob.argtypes = [C.POINTER(OracleInput2D)]
+        _lib.oracle2d_count_nglob.restype = C.c_int
+        _lib.oracle_gll.argtypes = [_dp, _dp, _dp]
+        _lib.oracle_legendre.argtypes = [C.c_double, C.c_int]
+        _lib.oracle_legendre.restype = C.c_double
+        _lib.oracle_stress_psv.argtypes = [C.c_double, C.c_double, _dp, _dp]
+    return _lib
+
+
+@dataclass
+class Source:
+    x: float
+    z: float
+    f0: float
+    factor: float
+    tshift: float = 0.0
+    angle: float = 0.0
+    stf: str = "ricker"          # "ricker" or "dirac"
+
+
+@dataclass
+class Case2D:
+    mesh: Mesh2D
+    sources: list
+    rec_x: np.ndarray
+    rec_z: np.ndarray
+    dt: float
+    nstep: int
+    seis_types: list = field(default_factory=lambda: ["displacement"])
+    nstep_between_samples: int = 1
+    rec_angle: float = 0.0
+    elastic_sh: bool = False
+    point_rho: np.ndarray | None = None   # optional per-GLL-point models [nspec, 25]
+    point_vp: np.ndarray | None = None
+    point_vs: np.ndarray | None = None
+    stf_table: np.ndarray | None = None    # optional [nstep, nsrc]
+    stations: list = field(default_factory=list)
+
+
+def start_time(sources) -> tuple[float, list]:
+    """t0 and effective tshifts (read_sources.cpp:142-172), in FP32 like the reference."""
+    f32 = np.float32
+    t0s = [f32(-1.2) * (f32(1.0) / f32(s.f0)) + f32(s.tshift) for s in sources]
+    t0 = min(t0s)
+    return float(t0), [float(t - t0) for t in t0s]
+
+
+def point_models(case: Case2D):
+    m = case.mesh
+    if case.point_rho is not None:
+        return (np.ascontiguousarray(case.point_rho, np.float64),
+                np.ascontiguousarray(case.point_vp, np.float64),
+                np.ascontiguousarray(case.point_vs, np.float64))
+    rho = np.repeat(m.mat_rho[m.kmato][:, None], 25, axis=1)
+    vp = np.repeat(m.mat_vp[m.kmato][:, None], 25, axis=1)
+    vs = np.repeat(m.mat_vs[m.kmato][:, None], 25, axis=1)
+    return rho, vp, vs
+
+
+def _ptr(a, t):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: bool = False):
+    """Run the oracle; returns dict with 'seis' [nsig, ntypes, nrec, 2], 't0', 'times'."""
+    m = case.mesh
+    L = lib()
+    keep = []
+
+    def arr(x, dt):
+        a = np.ascontiguousarray(x, dtype=dt)
+        keep.append(a)
+        return a
+
+    rho, vp, vs = point_models(case)
+    srcs = [effective_f0(s, case.dt) for s in case.sources]
+    t0, tsh = start_time(srcs)
+    stf_table = case.stf_table
+    if stf_table is None and any(s.stf != "ricker" for s in srcs):
+        stf_table = stf_tables(case.sources, case.dt, case.nstep)
+    inp = OracleInput2D()
+    inp.nspec, inp.npgeo, inp.ngnod = m.nspec, m.npgeo, m.ngnod
+    inp.coorg = _ptr(arr(m.coorg, np.float64), _dp)
+    inp.knods = _ptr(arr(m.knods, np.int32), _ip)
+    inp.medium = _ptr(arr(m.mat_medium[m.kmato], np.int32), _ip)
+    inp.rho, inp.vp, inp.vs = (_ptr(arr(a, np.float64), _dp) for a in (rho, vp, vs))
+    inp.elastic_sh = int(case.elastic_sh)
+    inp.nabs = len(m.abs_ispec)
+    inp.abs_ispec = _ptr(arr(m.abs_ispec, np.int32), _ip)
+    inp.abs_type = _ptr(arr(m.abs_type, np.int32), _ip)
+    inp.nfree = len(m.free_ispec)
+    inp.free_ispec = _ptr(arr(m.free_ispec, np.int32), _ip)
+    inp.free_type = _ptr(arr(m.free_type, np.int32), _ip)
+    inp.nsrc = len(srcs)
+    inp.src_x = _ptr(arr([s.x for s in srcs], np.float64), _dp)
+    inp.src_z = _ptr(arr([s.z for s in srcs], np.float64), _dp)
+    inp.src_angle = _ptr(arr([s.angle for s in srcs], np.float64), _dp)
+    inp.src_f0 = _ptr(arr([s.f0 for s in srcs], np.float64), _dp)
+    inp.src_factor = _ptr(arr([s.factor for s in srcs], np.float64), _dp)
+    inp.src_tshift = _ptr(arr(tsh, np.float64), _dp)
+    inp.stf_table = _ptr(arr(stf_table, np.float64), _dp) if stf_table is not None else None
+    inp.t0 = t0
+    inp.nrec = len(case.rec_x)
+    inp.rec_x = _ptr(arr(case.rec_x, np.float64), _dp)
+    inp.rec_z = _ptr(arr(case.rec_z, np.float64), _dp)
+    inp.rec_angle = case.rec_angle
+    types = [SEIS_TYPES[t] for t in case.seis_types]
+    inp.ntypes = len(types)
+    inp.seis_types = _ptr(arr(types, np.int32), _ip)
+    inp.dt, inp.nstep = case.dt, case.nstep
+    nsb = max(1, case.nstep_between_samples)
+    inp.nstep_between_samples = nsb
+    nsig = (case.nstep + nsb - 1) // nsb
+    seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
+    out = OracleOutput2D()
+    out.seismograms = _ptr(seis, _dp)
+    final = None
+    if want_final:
+        nglob = L.oracle2d_count_nglob(C.byref(inp))
+        final = {"elastic": np.zeros((nglob, 1 if case.elastic_sh else 2)),
+                 "acoustic": np.zeros(nglob),
+                 "ibool": np.zeros((m.nspec, 25), np.int32)}
+        out.final_u_elastic = _ptr(final["elastic"], _dp)
+        out.final_u_acoustic = _ptr(final["acoustic"], _dp)
+        out.ibool = _ptr(final["ibool"], _ip)
+    fn = L.oracle2d_run_f32 if precision == "f32" else L.oracle2d_run_f64
+    rc = fn(C.byref(inp), C.byref(out), int(nthreads))
+    if rc != 0:
+        raise RuntimeError(out.error.decode())
+    times = np.arange(nsig) * (case.dt * nsb) + t0
+    return {"seis": seis, "t0": t0, "times": times, "final": final, "nglob": out.nglob}
+
+
+# ------------------------------------------------ reference fixtures ---
+
+def read_stations(path):
+    names, xs, zs = [], [], []
+    with open(path) as f:
+        for line in f:
+            p = line.split()
+            if len(p) < 4:
+                continue
+            names.append((p[1], p[0]))
+            xs.append(float(p[2]))
+            zs.append(float(p[3]))
+    return names, np.asarray(xs), np.asarray(zs)
+
+
+def read_sources_yaml(path):
+    import yaml
+    with open(path) as f:
+        d = yaml.safe_load(f)
+    out = []
+    for s in d["sources"]:
+        if "force" not in s:
+            raise ValueError("only force sources are on this path")
+        fs = s["force"]
+        if "Ricker" in fs:
+            rk, kind = fs["Ricker"], "ricker"
+        elif "Dirac" in fs:
+            rk, kind = fs["Dirac"], "dirac"
+        else:
+            raise ValueError("only Ricker and Dirac time functions are on this path")
+        out.append(Source(x=float(fs["x"]), z=float(fs["z"]), f0=float(rk.get("f0", 0.0)),
+                          factor=float(rk["factor"]), tshift=float(rk.get("tshift", 0.0)),
+                          angle=float(fs.get("angle", 0.0)), stf=kind))
+    return out
+
+
+def stf_tables(sources, dt, nstep):
+    """FP32 source-time-function table [nstep, nsrc] (ricker.cpp, dirac.cpp).
+
+    Ricker: factor * (1 - 2 a t^2) exp(-a t^2); Dirac: factor * (-exp(-a t^2) / (2a))
+    with f0 = 1 / (10 dt); a = pi^2 f0^2, t = t0 + i dt - tshift.
+    """
+    f32 = np.float32
+    srcs = [effective_f0(s, dt) for s in sources]
+    t0, tsh = start_time(srcs)
+    i = np.arange(nstep, dtype=f32)
+    tab = np.zeros((nstep, len(srcs)), np.float32)
+    pi = f32(np.pi)
+    for k, s in enumerate(srcs):
+        t = f32(t0) + i * f32(dt) - f32(tsh[k])
+        a = pi * pi * f32(s.f0) * f32(s.f0)
+        if s.stf == "dirac":
+            tab[:, k] = f32(s.factor) * (f32(-1.0) * np.exp(-a * t * t) / (f32(2.0) * a))
+        else:
+            tab[:, k] = f32(s.factor) * ((f32(1.0) - f32(2.0) * a * t * t) * np.exp(-a * t * t))
+    return tab
+
+
+def effective_f0(s, dt):
+    """Dirac sources use f0 = 1/(10 dt) (dirac.cpp:25)."""
+    if s.stf == "dirac":
+        return Source(x=s.x, z=s.z, f0=float(np.float32(1.0) / (np.float32(10.0) * np.float32(dt))),
+                      factor=s.factor, tshift=s.tshift, angle=s.angle, stf="dirac")
+    return s
+
+
+def load_fixture(fixture_dir, types=("displacement",)):
+    """Load a reference Newmark fixture directory into a Case2D."""
+    import yaml
+    with open(os.path.join(fixture_dir, "specfem_config.yaml")) as f:
+        cfg = yaml.safe_load(f)["parameters"]
+    ts = cfg["simulation-setup"]["solver"]["time-marching"]["time-scheme"]
+    rc = cfg["receivers"]
+    mesh = read_database(os.path.join(fixture_dir, "database.bin"))
+    names, rx, rz = read_stations(os.path.join(fixture_dir, "STATIONS"))
+    src = read_sources_yaml(os.path.join(fixture_dir, "sources.yaml"))
+    return Case2D(mesh=mesh, sources=src, rec_x=rx, rec_z=rz, dt=float(ts["dt"]),
+                  nstep=int(ts["nstep"]), seis_types=list(types),
+                  nstep_between_samples=int(rc.get("nstep_between_samples", 1)),
+                  rec_angle=float(rc.get("angle", 0.0)), stations=names)
+
+
+def read_trace(path):
+    a = np.loadtxt(path)
+    return a[:, 0], a[:, 1]
+
+
+def reference_metric(computed, fixture_dir, stations, kind="semd", comps=("BXX", "BXZ")):
+    """Per-station sum|d| / sum|ref| as in newmark_tests.cpp:331-373.
+
+    ``computed`` is [nsig, nrec, ncomp] for one seismogram type.
+    """
+    errs = []
+    for r, (net, sta) in enumerate(stations):
+        err = norm = 0.0
+        for c, comp in enumerate(comps):
+            t, v = read_trace(os.path.join(fixture_dir, "traces", f"{net}.{sta}.S2.{comp}.{kind}"))
+            n = min(len(v), computed.shape[0])
+            err += np.abs(computed[:n, r, c] - v[:n]).sum()
+            norm += np.abs(v[:n]).sum()
+        errs.append(err / norm if norm > 0 else float("nan"))
+    return np.asarray(errs)
