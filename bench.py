@@ -1,0 +1,288 @@
+"""Benchmark of the spectral-element time step (GLL-point updates per second).
+
+Workload: the coupled acoustic-elastic 2D model (400x200 quads over 20x10 km,
+NGLL=5, 1,282,401 global GLL points, 1.5 km of water over 4 seeded elastic
+layers, Stacey on three sides, acoustic free surface on top, Ricker 5 Hz
+pressure source, 200 seafloor receivers, dt = 1e-3 s).  Synthetic, seeded.
+
+One bench step = one time step of the whole model.  Reported keys:
+* value:  GLL-point updates/s with inputs resident in HBM, every timed step
+          launched after a 256 MiB write that flushes L2, timed with CUDA events
+          on the handle's stream, summed over the K steps, max over ranks;
+* e2e:    the same metric through the per-step C-ABI call with host buffers
+          (STF row host->device, seismogram row device->host, a sync per step);
+* roofline: the dominant kernel (elastic stiffness, all colour passes of one
+          step) against the measured HBM bandwidth;
+* cpu_baseline: the CPU oracle (a C++ restatement of the reference) on all
+          host cores, bounded sample of the same workload.
+``--impl reference`` times that CPU implementation alone on the same
+workload and metric.  With --gpus N > 1 every rank runs an independent
+replica (the single-shot path does not shard) and value sums the ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "GLL-point updates/s"
+UNIT = "GLL-pt/s"
+WORKLOAD = "coupled_400x200"
+# algorithmic bytes of the elastic stiffness kernel: per element GLL point
+# ibool(4) + xix,xiz,gammax,gammaz,|J| (20) + lambda+2mu, mu (8) = 32 B; per
+# elastic global point u read (8) + accumulator read and write (16) = 24 B.
+STIFF_B_PER_LOCAL = 32
+STIFF_B_PER_GLOB = 24
+# whole step, per global point (2D elastic P-SV, FP32): u,v,a read+write 48 +
+# M^-1 8 + 32 B per local point x 25 nspec / nglob.
+STEP_B_GLOB = 56
+STEP_B_LOCAL = 32
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profile():
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        try:
+            return json.load(open(p))
+        except Exception:
+            return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle samples during the timed region."""
+
+    def __init__(self, device_index: int):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap,power.draw")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device_index), f"--query-gpu={q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[0]))
+                mx.append(float(r[1]))
+                for k, n in enumerate(names):
+                    if r[2 + k].strip().lower() == "active":
+                        reasons.add(n)
+            except Exception:
+                continue
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": float(max(mx)) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name, nstep):
+    from specfempp_b200 import meshgen
+    if name == "coupled_400x200":
+        return meshgen.coupled_400x200(nstep=nstep)
+    if name == "elastic_psv_80x60":
+        return meshgen.elastic_psv_80x60(nstep=nstep)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def cpu_oracle_throughput(w, steps, threads):
+    from oracle import runner
+    case = runner.Case2D(mesh=w.mesh, sources=w.sources, rec_x=w.rec_x, rec_z=w.rec_z, dt=w.dt,
+                         nstep=steps)
+    r = runner.run(case, "f32", nthreads=threads)
+    return r["nglob"] * steps / r["loop_seconds"], r["loop_seconds"]
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    w = make_workload(args.workload, max(args.steps, 1))
+    # each bench step is one time step of the full model; the timed sample is
+    # capped so that warm-up plus timed steps stay near a minute on the host
+    steps = max(3, min(args.steps, 400))
+    warm = max(1, min(args.warmup, 3))
+    cpu_oracle_throughput(w, warm, threads)
+    v, secs = cpu_oracle_throughput(w, steps, threads)
+    ms = secs * 1000.0 / steps
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+            "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": args.workload, "nglob": None, "steps_requested": args.steps},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{steps} time steps of {args.workload} (full mesh), "
+                                       f"FP32 C++ restatement of the reference, OpenMP atomics"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="sfg", choices=["sfg", "reference"])
+    ap.add_argument("--workload", default=WORKLOAD)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+
+    import torch
+    import torch.distributed as dist
+    if not torch.cuda.is_available():
+        raise SystemExit("bench.py needs a CUDA device")
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+
+    from specfempp_b200 import sfg
+    total_steps = args.warmup + args.steps
+    w = make_workload(args.workload, total_steps)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=total_steps)
+    sim.set_sources(w.sources)
+    sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
+    sim.initialize()
+    inf = sim.info()
+    nglob = inf.nglob
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- value: device-resident, L2 flushed before every timed step ----
+    sim.run(args.warmup)
+    sim.synchronize()
+    clocks = ClockSampler(local)
+    barrier()
+    ms = sim.run_timed_flushed(args.steps, 256 << 20)
+    barrier()
+    clk = clocks.stop()
+    ms = max_over_ranks(ms)
+    finite = sim.check_finite()
+    value = world * nglob * args.steps / (ms / 1000.0)
+
+    # ---- supplementary: back-to-back graph replay (L2 not flushed) ----
+    sim.reset()
+    sim.run(args.warmup)
+    barrier()
+    ms_b2b = max_over_ranks(sim.run_timed(args.steps))
+
+    # ---- e2e: per-step C-ABI call with host buffers ----
+    sim.reset()
+    nsrc = len(w.sources)
+    stf_rows = torch.zeros((total_steps, nsrc), dtype=torch.float32).pin_memory().numpy()
+    from specfempp_b200 import stf as _stf
+    stf_rows[:] = _stf.table(w.sources, w.dt, total_steps)
+    seis_row = torch.zeros((inf.nshots, inf.ntypes, inf.nrec, 2), dtype=torch.float32).pin_memory().numpy()
+    for i in range(args.warmup):
+        sim.step_io(stf_rows[i], seis_row)
+    barrier()
+    t0 = time.perf_counter()
+    for i in range(args.warmup, args.warmup + args.steps):
+        sim.step_io(stf_rows[i], seis_row)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = world * nglob * args.steps / e2e_s
+
+    # ---- roofline of the dominant kernel ----
+    stiff_ms = sim.time_kernel(0, 50)
+    upd_ms = sim.time_kernel(1, 50)
+    ac_ms = sim.time_kernel(2, 50)
+    stiff_bytes = STIFF_B_PER_LOCAL * inf.nspec_elastic * 25 + STIFF_B_PER_GLOB * inf.nglob_elastic
+    peak, peak_kind = peaks()
+    achieved = stiff_bytes / (stiff_ms / 1e3) / 1e9
+    tr = traffic_from_profile()
+    traffic = None
+    if tr and tr.get("workload") == args.workload:
+        traffic = tr.get("stiffness_bytes_per_launch")
+    step_bytes = STEP_B_GLOB * nglob + STEP_B_LOCAL * inf.nspec * 25
+    roofline = {"bound": "hbm", "kernel": "k_stiffness_psv (4 colour launches of one step)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic,
+                "algorithmic_bytes_per_launch": stiff_bytes, "launch_ms": stiff_ms,
+                "update_launch_ms": upd_ms, "acoustic_stiffness_ms": ac_ms,
+                "step_algorithmic_bytes": step_bytes,
+                "step_frac_of_peak": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, secs = cpu_oracle_throughput(w, 40, threads)
+        cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"40 time steps of {args.workload} (full mesh), FP32 C++ restatement of the "
+                         f"reference on {threads} host threads ({secs:.2f} s)"}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": args.workload, "nglob": nglob, "nspec": inf.nspec,
+                   "nspec_elastic": inf.nspec_elastic, "nspec_acoustic": inf.nspec_acoustic,
+                   "dt": w.dt, "ngll": 5, "shots": 1, "l2": "flushed (256 MiB write) before every timed step",
+                   "parallelism": "replicas" if world > 1 else "single GPU",
+                   "value_back_to_back": world * nglob * args.steps / (ms_b2b / 1000.0),
+                   "ms_per_step_back_to_back": ms_b2b / args.steps, "finite": bool(finite)},
+        "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * nsrc,
+                "d2h_bytes_per_step": 4 * inf.nshots * inf.ntypes * inf.nrec * 2},
+        "roofline": roofline,
+        "cpu_baseline": cpu,
+        "clocks": clk,
+        "gpu_launches": inf.kernels_per_step * args.steps,
+    }
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,166 @@
+/*
+ * sfg.h — C ABI of libsfg, the B200 (sm_100a) spectral-element time-step
+ * engine that stands in for SPECFEM++'s per-time-step kernels.
+ *
+ * All functions return 0 on success or a negative SFG_ERR_* code; the text of
+ * the last error of a handle is returned by sfg_last_error().  No torch or
+ * CUDA types appear in the signatures: meshes, sources and receivers are plain
+ * host arrays, results are copied into caller-owned host buffers.  A handle is
+ * used by one host thread at a time; separate handles are independent.
+ *
+ * Reference interfaces that each group replaces (paths in SPECFEM++):
+ *   sfg_create2d / sfg_create2d_from_database
+ *       specfem::io::read_2d_mesh          src/io/mesh/impl/fortran/dim2/mesh.cpp:26-215
+ *       specfem::assembly::assembly<dim2>  core/specfem/assembly/assembly/dim2/assembly.cpp
+ *   sfg_set_sources     specfem::io::read_2d_sources src/io/sources/dim2/read_sources.cpp:29-172,
+ *                       assembly sources  core/specfem/assembly/sources/dim2/sources.cpp
+ *   sfg_set_receivers   specfem::io::read_2d_receivers, assembly receivers
+ *                       core/specfem/assembly/receivers/dim2/receivers.cpp
+ *   sfg_initialize      domain_kernels::initialize  include/kokkos_kernels/domain_kernels.hpp:151-179
+ *                       (compute_mass_matrix + invert_mass_matrix)
+ *   sfg_step / sfg_run  time_marching<forward>::run core/specfem/solver/time_marching.tpp:33-90:
+ *                       newmark predictor/corrector core/specfem/timescheme/newmark.tpp:10-128,
+ *                       domain_kernels::update_wavefields include/kokkos_kernels/domain_kernels.hpp:72-141
+ *                       (compute_coupling, compute_source_interaction,
+ *                        compute_stiffness_interaction, divide_mass_matrix),
+ *                       domain_kernels::compute_seismograms :189-203
+ *   sfg_get_seismograms receivers.sync_seismograms() + seismogram iterator
+ *                       core/specfem/assembly/receivers/dim2/impl/seismogram_iterator.hpp:37-53
+ *   sfg_get_field       simulation_field copy_to_host (include/io/wavefield/writer.tpp)
+ */
+#ifndef SFG_H
+#define SFG_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  SFG_OK = 0,
+  SFG_ERR_ARG = -1,       /* invalid argument / inconsistent sizes */
+  SFG_ERR_IO = -2,        /* database file missing or malformed */
+  SFG_ERR_CUDA = -3,      /* a CUDA runtime call failed */
+  SFG_ERR_LOCATE = -4,    /* a source or receiver lies outside the mesh */
+  SFG_ERR_STATE = -5,     /* call out of order (e.g. sfg_run before sfg_initialize) */
+  SFG_ERR_NONFINITE = -6, /* the wavefield became NaN/Inf */
+  SFG_ERR_UNSUPPORTED = -7
+};
+
+/* Edge types, the reference's mesh_entity order for absorbing records. */
+enum { SFG_EDGE_BOTTOM = 0, SFG_EDGE_RIGHT = 1, SFG_EDGE_TOP = 2, SFG_EDGE_LEFT = 3 };
+enum { SFG_MEDIUM_ACOUSTIC = 0, SFG_MEDIUM_ELASTIC = 1 };
+enum { SFG_WAVE_PSV = 0, SFG_WAVE_SH = 1 };
+enum { SFG_SEIS_DISPLACEMENT = 0, SFG_SEIS_VELOCITY = 1, SFG_SEIS_ACCELERATION = 2,
+       SFG_SEIS_PRESSURE = 3 };
+enum { SFG_STF_RICKER = 0, SFG_STF_DIRAC = 1 };
+enum { SFG_FIELD_DISPLACEMENT = 0, SFG_FIELD_VELOCITY = 1, SFG_FIELD_ACCELERATION = 2 };
+
+typedef struct sfg_handle sfg_handle;
+
+/* In-memory 2D mesh, the content of a SPECFEM2D database.bin
+ * (specfem::mesh::mesh<dim2>, include/mesh/dim2/mesh.hpp). */
+typedef struct sfg_mesh2d_desc {
+  int nspec, npgeo, ngnod;       /* ngnod = 4 or 9 control nodes */
+  const double *coorg;           /* [npgeo][2] control-node (x, z) */
+  const int *knods;              /* [nspec][ngnod], 0-based */
+  const int *kmato;              /* [nspec] material index, 0-based */
+  int numat;
+  const int *mat_medium;         /* [numat] SFG_MEDIUM_* */
+  const double *mat_rho, *mat_vp, *mat_vs; /* [numat] */
+  const float *point_rho, *point_vp, *point_vs; /* optional [nspec][25] GLL-point models */
+  int nabs;
+  const int *abs_ispec, *abs_type;   /* absorbing (Stacey) edges */
+  int nfree;
+  const int *free_ispec, *free_type; /* acoustic free-surface edges */
+  int elastic_wave;              /* SFG_WAVE_PSV or SFG_WAVE_SH */
+} sfg_mesh2d_desc;
+
+typedef struct sfg_options {
+  double dt;
+  int nstep;                     /* steps the source tables cover */
+  int nshots;                    /* independent shots advanced together (>= 1) */
+  int nstep_between_samples;     /* seismogram sampling (>= 1) */
+  int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
+  int elements_per_block;        /* stiffness launch shape (0 = autotuned default) */
+  int store_acceleration;        /* keep the elastic acceleration for read-back */
+} sfg_options;
+
+typedef struct sfg_source2d {
+  double x, z;
+  int shot;                      /* shot this source belongs to (0..nshots-1) */
+  int stf;                       /* SFG_STF_* */
+  double f0, factor, tshift, angle;
+} sfg_source2d;
+
+typedef struct sfg_info {
+  int nspec, nspec_elastic, nspec_acoustic;
+  int nglob, nglob_elastic, nglob_acoustic;
+  int ncolors_elastic, ncolors_acoustic;
+  int nshots, nsig, nrec, ntypes, nstep;
+  int istep;                     /* next step to be run */
+  double t0;                     /* time of step 0 (earliest shot) */
+  size_t device_bytes;
+  int kernels_per_step;
+} sfg_info;
+
+/* ---- life cycle ---- */
+int sfg_create2d(const sfg_mesh2d_desc *mesh, const sfg_options *opt, sfg_handle **out);
+int sfg_create2d_from_database(const char *database_path, int elastic_wave,
+                               const sfg_options *opt, sfg_handle **out);
+void sfg_destroy(sfg_handle *h);
+const char *sfg_last_error(const sfg_handle *h);   /* NULL handle: last create error */
+
+/* ---- sources / receivers (before sfg_initialize) ---- */
+int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src);
+/* Optional external source-time table [nstep][nsrc] (overrides the analytic STFs). */
+int sfg_set_stf_table(sfg_handle *h, const float *table, int nstep, int nsrc);
+int sfg_set_receivers(sfg_handle *h, int nrec, const double *x, const double *z,
+                      double angle_deg, int ntypes, const int *types);
+
+/* ---- mass matrix, upload, graph build ---- */
+int sfg_initialize(sfg_handle *h);
+
+/* ---- time stepping ---- */
+int sfg_step(sfg_handle *h);                        /* one step, no graph */
+int sfg_run(sfg_handle *h, int nsteps);             /* nsteps steps via CUDA graphs */
+int sfg_synchronize(sfg_handle *h);
+int sfg_reset_fields(sfg_handle *h);                /* zero wavefields, istep = 0 */
+/* Device time of nsteps graph-replayed steps, measured with CUDA events on the
+ * handle's stream (inputs resident); ms_total receives the elapsed time. */
+int sfg_run_timed(sfg_handle *h, int nsteps, float *ms_total);
+/* Device time of nsteps steps, each launched separately after a write of
+ * flush_bytes to a scratch buffer (clears L2 between timed steps); returns the
+ * sum of the per-step times measured with CUDA events on the handle's stream. */
+int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *ms_total);
+/* One step with host buffers: copies this step's source-time values
+ * stf_row[nsrc] (host, may be NULL to keep the table) to the device, runs the
+ * step, and copies the seismogram sample of the step (when the step is a
+ * sampling step) into seis_row[nshots][ntypes][nrec][2] (host, may be NULL);
+ * returns after the copy has landed.  This is the per-step path a host driver
+ * that streams sources in and traces out would call. */
+int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
+/* Average device time of one launch of a named kernel family, timed alone with
+ * CUDA events: which = 0 elastic stiffness (all colours of one step),
+ * 1 elastic Newmark update, 2 acoustic stiffness, 3 acoustic update. */
+int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms_per_launch);
+
+/* ---- results ---- */
+int sfg_get_info(const sfg_handle *h, sfg_info *info);
+/* Seismograms [nshots][nsig][ntypes][nrec][2], receiver-angle rotation applied. */
+int sfg_get_seismograms(sfg_handle *h, float *out, size_t count);
+/* Wavefield of one medium, in the handle's per-medium point numbering:
+ * elastic [nshots][nglob_elastic][ncomp], acoustic [nshots][nglob_acoustic]. */
+int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count);
+/* Global (mesh) id of every element GLL point in database element order,
+ * and the per-medium index of each global point (-1 if absent). */
+int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *glob_to_elastic,
+                      int *glob_to_acoustic);
+/* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
+int sfg_check_finite(sfg_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SFG_H */

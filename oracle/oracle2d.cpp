@@ -45,6 +45,7 @@
 //                               include/medium/dim2/acoustic/isotropic/wavefield.hpp,
 //                               core/specfem/assembly/receivers/dim2/impl/seismogram_iterator.hpp:37-53
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -247,6 +248,18 @@ struct Sim {
     receivers();
   }
 
+  void setup_geometry_only() {
+    double zd[NG], wd[NG], hpd[NG][NG];
+    gll_nodes(zd, wd);
+    gll_hprime(zd, hpd);
+    for (int i = 0; i < NG; ++i) {
+      z[i] = T(zd[i]); w[i] = T(wd[i]);
+      for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
+    }
+    number_points();
+    geometry();
+  }
+
   // Global numbering by element topology: corners by control-node id, edge
   // points by (corner pair, position), element-interior points unique.
   void number_points() {
@@ -287,29 +300,48 @@ struct Sim {
     }
   }
 
-  void ctrl(int e, T *cx, T *cz) const {
+  template <typename S>
+  void ctrl(int e, S *cx, S *cz) const {
     for (int n = 0; n < ngnod; ++n) {
       int id = in.knods[size_t(e) * ngnod + n];
-      cx[n] = T(in.coorg[2 * size_t(id)]);
-      cz[n] = T(in.coorg[2 * size_t(id) + 1]);
+      cx[n] = S(in.coorg[2 * size_t(id)]);
+      cz[n] = S(in.coorg[2 * size_t(id) + 1]);
     }
   }
 
-  void geometry() {
+  template <typename S>
+  void geometry_in() {
     size_t n = size_t(nspec) * NP;
     xix.resize(n); xiz.resize(n); gax.resize(n); gaz.resize(n); jac.resize(n);
     gx.resize(n); gz.resize(n);
+    S zs[NG];
+    for (int i = 0; i < NG; ++i) zs[i] = setup_z<S>(i);
     for (int e = 0; e < nspec; ++e) {
-      T cx[9], cz[9];
-      ctrl(e, cx, cz);
+      S cx[9], cz[9];
+      ctrl<S>(e, cx, cz);
       for (int iz = 0; iz < NG; ++iz)
         for (int ix = 0; ix < NG; ++ix) {
           size_t p = size_t(e) * NP + iz * NG + ix;
-          Jac<T> J = jacobian_at<T>(cx, cz, ngnod, z[ix], z[iz]);
-          xix[p] = J.xix; gax[p] = J.gammax; xiz[p] = J.xiz; gaz[p] = J.gammaz; jac[p] = J.jac;
-          location_at<T>(cx, cz, ngnod, z[ix], z[iz], gx[p], gz[p]);
+          Jac<S> J = jacobian_at<S>(cx, cz, ngnod, zs[ix], zs[iz]);
+          xix[p] = T(J.xix); gax[p] = T(J.gammax); xiz[p] = T(J.xiz); gaz[p] = T(J.gammaz);
+          jac[p] = T(J.jac);
+          S x, zz;
+          location_at<S>(cx, cz, ngnod, zs[ix], zs[iz], x, zz);
+          gx[p] = T(x); gz[p] = T(zz);
         }
     }
+  }
+
+  template <typename S>
+  S setup_z(int i) const {
+    double zd[NG], wd[NG];
+    gll_nodes(zd, wd);
+    return S(zd[i]);
+  }
+
+  void geometry() {
+    if (in.setup_in_run_precision) geometry_in<T>();
+    else geometry_in<double>();
   }
 
   void properties() {
@@ -460,17 +492,29 @@ struct Sim {
   }
 
   // ------------------------------------------------- point location ---
-  std::tuple<int, T, T> locate(double X, double Z) const {
-    const T x = T(X), zz = T(Z);
-    T best = std::numeric_limits<T>::max();
+  // Closest GLL point, then Newton iterations from the element centre in that
+  // element and the elements sharing a corner with it (locate_point_impl.cpp).
+  // Ties (a point on an edge or corner shared by several elements) go to the
+  // first element in mesh order: a candidate replaces the current choice only
+  // when it is closer by more than 1e-9 of the mesh extent.
+  template <typename S>
+  std::tuple<int, double, double> locate_in(double X, double Z) const {
+    const S x = S(X), zz = S(Z);
+    double xmin = 1e300, xmax = -1e300, zmin = 1e300, zmax = -1e300;
+    for (int i = 0; i < in.npgeo; ++i) {
+      xmin = std::min(xmin, in.coorg[2 * i]); xmax = std::max(xmax, in.coorg[2 * i]);
+      zmin = std::min(zmin, in.coorg[2 * i + 1]); zmax = std::max(zmax, in.coorg[2 * i + 1]);
+    }
+    const S tol = S(1e-9 * std::max(xmax - xmin, zmax - zmin));
+    S best = std::numeric_limits<S>::max();
     int eg = -1;
     for (int e = 0; e < nspec; ++e)
       for (int q = 0; q < NP; ++q) {
         size_t p = size_t(e) * NP + q;
-        T d = std::sqrt((gx[p] - x) * (gx[p] - x) + (gz[p] - zz) * (gz[p] - zz));
-        if (d < best) { best = d; eg = e; }
+        S dx = S(gx[p]) - x, dz = S(gz[p]) - zz;
+        S d = std::sqrt(dx * dx + dz * dz);
+        if (d < best - tol) { best = d; eg = e; }
       }
-    // candidates: guess first, then elements sharing a corner node with it
     std::vector<int> cand{eg};
     const int *kg = in.knods + size_t(eg) * ngnod;
     for (int e = 0; e < nspec; ++e) {
@@ -482,31 +526,55 @@ struct Sim {
           if (kg[a] == ke[b]) { share = true; break; }
       if (share) cand.push_back(e);
     }
-    T fd = std::numeric_limits<T>::max();
-    int es = -1; T xs = -9999, gs = -9999;
+    S fd = std::numeric_limits<S>::max();
+    int es = -1; S xs = -9999, gs = -9999;
     for (int e : cand) {
-      T cx[9], cz[9];
-      ctrl(e, cx, cz);
-      T xi = 0, ga = 0;
+      S cx[9], cz[9];
+      ctrl<S>(e, cx, cz);
+      S xi = 0, ga = 0;
       for (int it = 0; it < 100; ++it) {
-        T lx, lz;
-        location_at<T>(cx, cz, ngnod, xi, ga, lx, lz);
-        Jac<T> J = jacobian_at<T>(cx, cz, ngnod, xi, ga);
-        T dx = -(lx - x), dz = -(lz - zz);
-        T dxi = J.xix * dx + J.xiz * dz, dga = J.gammax * dx + J.gammaz * dz;
+        S lx, lz;
+        location_at<S>(cx, cz, ngnod, xi, ga, lx, lz);
+        Jac<S> J = jacobian_at<S>(cx, cz, ngnod, xi, ga);
+        S dx = -(lx - x), dz = -(lz - zz);
+        S dxi = J.xix * dx + J.xiz * dz, dga = J.gammax * dx + J.gammaz * dz;
         xi += dxi; ga += dga;
-        xi = std::min(std::max(xi, T(-1.01)), T(1.01));
-        ga = std::min(std::max(ga, T(-1.01)), T(1.01));
+        xi = std::min(std::max(xi, S(-1.01)), S(1.01));
+        ga = std::min(std::max(ga, S(-1.01)), S(1.01));
         if (std::abs(dxi) < 1e-12 && std::abs(dga) < 1e-12) break;
       }
-      T lx, lz;
-      location_at<T>(cx, cz, ngnod, xi, ga, lx, lz);
-      T d = std::sqrt((lx - x) * (lx - x) + (lz - zz) * (lz - zz));
-      if (d < fd) { fd = d; es = e; xs = xi; gs = ga; }
+      S lx, lz;
+      location_at<S>(cx, cz, ngnod, xi, ga, lx, lz);
+      S d = std::sqrt((lx - x) * (lx - x) + (lz - zz) * (lz - zz));
+      if (d < fd - tol) { fd = d; es = e; xs = xi; gs = ga; }
     }
-    if (es < 0 || std::abs(std::abs(xs) - T(1.01)) < T(1e-6) || std::abs(std::abs(gs) - T(1.01)) < T(1e-6))
+    if (es < 0 || std::abs(std::abs(xs) - S(1.01)) < S(1e-6) || std::abs(std::abs(gs) - S(1.01)) < S(1e-6))
       throw std::runtime_error("Failed to locate point in the mesh");
-    return {es, xs, gs};
+    return {es, double(xs), double(gs)};
+  }
+
+  std::tuple<int, double, double> locate(double X, double Z) const {
+    return in.setup_in_run_precision ? locate_in<T>(X, Z) : locate_in<double>(X, Z);
+  }
+
+  // Lagrange interpolants at a located point, in the setup precision.
+  void interpolants(double xi, double ga, T out[NP], T dx_out[NP] = nullptr, T dg_out[NP] = nullptr) const {
+    double zd[NG], wd[NG];
+    gll_nodes(zd, wd);
+    if (in.setup_in_run_precision) {
+      T hx[NG], hpx[NG], hg[NG], hpg[NG], zt[NG];
+      for (int i = 0; i < NG; ++i) zt[i] = T(zd[i]);
+      lagrange_interp<T>(T(xi), zt, hx, hpx);
+      lagrange_interp<T>(T(ga), zt, hg, hpg);
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) out[iz * NG + ix] = hx[ix] * hg[iz];
+    } else {
+      double hx[NG], hpx[NG], hg[NG], hpg[NG];
+      lagrange_interp<double>(xi, zd, hx, hpx);
+      lagrange_interp<double>(ga, zd, hg, hpg);
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) out[iz * NG + ix] = T(hx[ix] * hg[iz]);
+    }
   }
 
   void sources() {
@@ -516,9 +584,8 @@ struct Sim {
       Src S;
       S.ispec = e;
       S.medium = medium[e];
-      T hx[NG], hpx[NG], hg[NG], hpg[NG];
-      lagrange_interp<T>(xi, z, hx, hpx);
-      lagrange_interp<T>(ga, z, hg, hpg);
+      T h[NP];
+      interpolants(xi, ga, h);
       T fv[2];
       if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
       else {
@@ -526,9 +593,8 @@ struct Sim {
         T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
         fv[0] = std::sin(ang); fv[1] = std::cos(ang);
       }
-      for (int iz = 0; iz < NG; ++iz)
-        for (int ix = 0; ix < NG; ++ix)
-          for (int c = 0; c < S.ncomp; ++c) S.arr[c][iz * NG + ix] = hx[ix] * hg[iz] * fv[c];
+      for (int q = 0; q < NP; ++q)
+        for (int c = 0; c < S.ncomp; ++c) S.arr[c][q] = h[q] * fv[c];
       S.stf.resize(size_t(nstep));
       if (in.stf_table) {
         for (int i = 0; i < nstep; ++i) S.stf[i] = T(in.stf_table[size_t(i) * in.nsrc + s]);
@@ -551,11 +617,7 @@ struct Sim {
       auto [e, xi, ga] = locate(in.rec_x[r], in.rec_z[r]);
       Rec R;
       R.ispec = e;
-      T hx[NG], hpx[NG], hg[NG], hpg[NG];
-      lagrange_interp<T>(xi, z, hx, hpx);
-      lagrange_interp<T>(ga, z, hg, hpg);
-      for (int iz = 0; iz < NG; ++iz)
-        for (int ix = 0; ix < NG; ++ix) R.h[iz * NG + ix] = hx[ix] * hg[iz];
+      interpolants(xi, ga, R.h);
       recs.push_back(R);
     }
   }
@@ -724,6 +786,26 @@ struct Sim {
         }
       return;
     }
+    if (type == 3) {
+      // elastic pressure: -(lambda + 2/3 mu) div u (elastic/isotropic/wavefield.hpp:57-89)
+      if (ncomp_el != 2) return;
+      for (int iz = 0; iz < NG; ++iz)
+        for (int ix = 0; ix < NG; ++ix) {
+          const int q = iz * NG + ix;
+          const size_t p = size_t(e) * NP + q;
+          T dxi[2] = {0, 0}, dga[2] = {0, 0};
+          for (int l = 0; l < NG; ++l)
+            for (int c = 0; c < 2; ++c) {
+              dxi[c] += hp[ix][l] * ue[size_t(ib[iz * NG + l]) * 2 + c];
+              dga[c] += hp[iz][l] * ue[size_t(ib[l * NG + ix]) * 2 + c];
+            }
+          const T dux = xix[p] * dxi[0] + gax[p] * dga[0];
+          const T duz = xiz[p] * dxi[1] + gaz[p] * dga[1];
+          const T lam = lp2m(p) - T(2) * p_mu[p];
+          out[0] += R.h[q] * (T(-1.0) * ((lam + T(2.0 / 3.0) * p_mu[p]) * (dux + duz)));
+        }
+      return;
+    }
     const std::vector<T> &f = type == 0 ? ue : type == 1 ? ve : ae;
     for (int q = 0; q < NP; ++q)
       for (int c = 0; c < ncomp_el; ++c) out[c] += R.h[q] * f[size_t(ib[q]) * ncomp_el + c];
@@ -761,7 +843,9 @@ int run_impl(const OracleInput2D *in, OracleOutput2D *out, int nthreads) {
   try {
     Sim<T> s(*in);
     s.setup();
+    const auto t0 = std::chrono::steady_clock::now();
     s.run(out->seismograms, nthreads);
+    out->loop_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     out->nglob = s.nglob;
     if (out->final_u_elastic) {
       for (size_t i = 0; i < s.ue.size(); ++i) out->final_u_elastic[i] = double(s.ue[i]);
@@ -787,6 +871,27 @@ int oracle2d_run_f32(const OracleInput2D *in, OracleOutput2D *out, int nthreads)
 
 int oracle2d_run_f64(const OracleInput2D *in, OracleOutput2D *out, int nthreads) {
   return run_impl<double>(in, out, nthreads);
+}
+
+// Element and local coordinates the oracle assigns to a physical point.
+int oracle2d_locate(const OracleInput2D *in, int precision64, double x, double z, int *ispec,
+                    double *xi, double *gamma) {
+  try {
+    if (precision64) {
+      Sim<double> s(*in);
+      s.setup_geometry_only();
+      auto [e, a, b] = s.locate(x, z);
+      *ispec = e; *xi = a; *gamma = b;
+    } else {
+      Sim<float> s(*in);
+      s.setup_geometry_only();
+      auto [e, a, b] = s.locate(x, z);
+      *ispec = e; *xi = a; *gamma = b;
+    }
+    return 0;
+  } catch (const std::exception &) {
+    return -1;
+  }
 }
 
 // Count global points of a mesh (so callers can size final-field buffers).

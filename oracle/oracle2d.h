@@ -26,6 +26,10 @@ typedef struct OracleInput2D {
   const int *seis_types;   /* 0 displacement 1 velocity 2 acceleration 3 pressure */
   double dt;
   int nstep, nstep_between_samples;
+  /* 0: setup geometry (Jacobians, point location, interpolants) in FP64 and
+   * rounded to the run precision; 1: setup in the run precision, as the
+   * reference does with type_real. */
+  int setup_in_run_precision;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {
@@ -34,12 +38,15 @@ typedef struct OracleOutput2D {
   double *final_u_acoustic;  /* optional [nglob] */
   int *ibool;                /* optional [nspec][25] */
   int nglob;
+  double loop_seconds;       /* wall time of the time loop alone */
   char error[256];
 } OracleOutput2D;
 
 int oracle2d_run_f32(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
 int oracle2d_run_f64(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
 int oracle2d_count_nglob(const OracleInput2D *in);
+int oracle2d_locate(const OracleInput2D *in, int precision64, double x, double z, int *ispec,
+                    double *xi, double *gamma);
 void oracle_gll(double *z, double *w, double *hprime);
 double oracle_legendre(double x, int n);
 void oracle_stress_psv(double kappa, double mu, const double *du, double *sigma);

@@ -45,13 +45,15 @@ class OracleInput2D(C.Structure):
         ("nrec", C.c_int), ("rec_x", _dp), ("rec_z", _dp), ("rec_angle", C.c_double),
         ("ntypes", C.c_int), ("seis_types", _ip),
         ("dt", C.c_double), ("nstep", C.c_int), ("nstep_between_samples", C.c_int),
+        ("setup_in_run_precision", C.c_int),
     ]
 
 
 class OracleOutput2D(C.Structure):
     _fields_ = [
         ("seismograms", _dp), ("final_u_elastic", _dp), ("final_u_acoustic", _dp),
-        ("ibool", _ip), ("nglob", C.c_int), ("error", C.c_char * 256),
+        ("ibool", _ip), ("nglob", C.c_int), ("loop_seconds", C.c_double),
+        ("error", C.c_char * 256),
     ]
 
 
@@ -111,6 +113,7 @@ class Case2D:
     point_vs: np.ndarray | None = None
     stf_table: np.ndarray | None = None    # optional [nstep, nsrc]
     stations: list = field(default_factory=list)
+    setup_in_run_precision: bool = False   # True: reference-faithful FP32 setup geometry
 
 
 def start_time(sources) -> tuple[float, list]:
@@ -186,6 +189,7 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     inp.dt, inp.nstep = case.dt, case.nstep
     nsb = max(1, case.nstep_between_samples)
     inp.nstep_between_samples = nsb
+    inp.setup_in_run_precision = int(case.setup_in_run_precision)
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()
@@ -204,7 +208,8 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     if rc != 0:
         raise RuntimeError(out.error.decode())
     times = np.arange(nsig) * (case.dt * nsb) + t0
-    return {"seis": seis, "t0": t0, "times": times, "final": final, "nglob": out.nglob}
+    return {"seis": seis, "t0": t0, "times": times, "final": final, "nglob": out.nglob,
+            "loop_seconds": out.loop_seconds}
 
 
 # ------------------------------------------------ reference fixtures ---

@@ -1,0 +1,742 @@
+// Host-side assembly of libsfg (see host2d.hpp).  Plain C++17, no CUDA.
+#include "host2d.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <stdexcept>
+#include <unordered_map>
+
+namespace sfg {
+
+namespace {
+
+constexpr int BOTTOM = 0, RIGHT = 1, TOP = 2, LEFT = 3;
+
+// ----------------------------------------------------------- database.bin ---
+// Record layout per src/io/mesh/impl/fortran/dim2/{read_mesh_database,
+// read_parameters,read_material_properties,read_boundaries,read_elements,
+// read_adjacency_graph}.cpp and mesh.cpp:26-215.
+struct RecordReader {
+  std::vector<char> buf;
+  size_t pos = 0;
+  std::vector<std::pair<size_t, int>> recs;  // offset, length
+  size_t cur = 0;
+  bool load(const std::string &path, std::string &err) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) { err = "Could not open database file: " + path; return false; }
+    buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+    while (pos < buf.size()) {
+      if (pos + 4 > buf.size()) { err = "truncated record header"; return false; }
+      int n;
+      std::memcpy(&n, &buf[pos], 4);
+      if (n < 0 || pos + 8 + size_t(n) > buf.size()) { err = "truncated database record"; return false; }
+      int n2;
+      std::memcpy(&n2, &buf[pos + 4 + n], 4);
+      if (n2 != n) { err = "record length markers differ"; return false; }
+      recs.push_back({pos + 4, n});
+      pos += 8 + size_t(n);
+    }
+    return true;
+  }
+  bool more() const { return cur < recs.size(); }
+  int len() const { return recs[cur].second; }
+  const char *next(int expect_min = 0) {
+    if (cur >= recs.size()) throw std::runtime_error("database ended early");
+    if (recs[cur].second < expect_min) throw std::runtime_error("short database record");
+    return &buf[recs[cur++].first];
+  }
+};
+
+template <typename T>
+T rd(const char *&p) {
+  T v;
+  std::memcpy(&v, p, sizeof(T));
+  p += sizeof(T);
+  return v;
+}
+
+// -------------------------------------------------------------- GLL ---
+double legendre(double x, int n) {
+  double p0 = 1.0, p1 = x;
+  for (int k = 1; k < n; ++k) {
+    double p2 = ((2.0 * k + 1.0) * x * p1 - k * p0) / (k + 1.0);
+    p0 = p1;
+    p1 = p2;
+  }
+  return n == 0 ? 1.0 : p1;
+}
+
+void gll(double z[NGLL], double w[NGLL], double hp[NGLL][NGLL]) {
+  const int N = NGLL - 1;
+  // nodes: +-1 and the roots of P'_4; for degree 4 these are 0 and +-sqrt(3/7)
+  const double r = std::sqrt(3.0 / 7.0);
+  const double zz[NGLL] = {-1.0, -r, 0.0, r, 1.0};
+  for (int i = 0; i < NGLL; ++i) {
+    z[i] = zz[i];
+    const double p = legendre(z[i], N);
+    w[i] = 2.0 / (N * (N + 1.0) * p * p);
+  }
+  for (int i = 0; i < NGLL; ++i)
+    for (int j = 0; j < NGLL; ++j) {
+      if (i == j) hp[i][j] = (i == 0) ? -0.25 * N * (N + 1.0) : (i == N ? 0.25 * N * (N + 1.0) : 0.0);
+      else hp[i][j] = legendre(z[i], N) / (legendre(z[j], N) * (z[i] - z[j]));
+    }
+}
+
+void lagrange(double xi, const double z[NGLL], double h[NGLL]) {
+  for (int d = 0; d < NGLL; ++d) {
+    double num = 1, den = 1;
+    for (int i = 0; i < NGLL; ++i)
+      if (i != d) { num *= xi - z[i]; den *= z[d] - z[i]; }
+    h[d] = num / den;
+  }
+}
+
+// ----------------------------------------------------- shape functions ---
+void shape(int ngnod, double xi, double ga, double *s, double *dx, double *dg) {
+  if (ngnod == 4) {
+    s[0] = 0.25 * (xi - 1) * (ga - 1); s[1] = -0.25 * (xi + 1) * (ga - 1);
+    s[2] = 0.25 * (xi + 1) * (ga + 1); s[3] = -0.25 * (xi - 1) * (ga + 1);
+    dx[0] = 0.25 * (ga - 1); dx[1] = -0.25 * (ga - 1); dx[2] = 0.25 * (ga + 1); dx[3] = -0.25 * (ga + 1);
+    dg[0] = 0.25 * (xi - 1); dg[1] = -0.25 * (xi + 1); dg[2] = 0.25 * (xi + 1); dg[3] = -0.25 * (xi - 1);
+    return;
+  }
+  // 9-node Lagrange quadrilateral (corners, edge mid-points, centre)
+  const double lx[3] = {0.5 * xi * (xi - 1), 1 - xi * xi, 0.5 * xi * (xi + 1)};
+  const double lg[3] = {0.5 * ga * (ga - 1), 1 - ga * ga, 0.5 * ga * (ga + 1)};
+  const double dlx[3] = {xi - 0.5, -2 * xi, xi + 0.5};
+  const double dlg[3] = {ga - 0.5, -2 * ga, ga + 0.5};
+  // node n -> (index along xi, index along gamma)
+  const int ix[9] = {0, 2, 2, 0, 1, 2, 1, 0, 1};
+  const int ig[9] = {0, 0, 2, 2, 0, 1, 2, 1, 1};
+  for (int n = 0; n < 9; ++n) {
+    s[n] = lx[ix[n]] * lg[ig[n]];
+    dx[n] = dlx[ix[n]] * lg[ig[n]];
+    dg[n] = lx[ix[n]] * dlg[ig[n]];
+  }
+}
+
+struct JacD {
+  double xix, xiz, gax, gaz, jac, x, z;
+};
+
+JacD jacobian(const Mesh2D &m, int e, double xi, double ga) {
+  double s[9], dx[9], dg[9];
+  shape(m.ngnod, xi, ga, s, dx, dg);
+  double xxi = 0, zxi = 0, xga = 0, zga = 0, x = 0, z = 0;
+  for (int n = 0; n < m.ngnod; ++n) {
+    const int id = m.knods[size_t(e) * m.ngnod + n];
+    const double cx = m.coorg[2 * size_t(id)], cz = m.coorg[2 * size_t(id) + 1];
+    xxi += dx[n] * cx; zxi += dx[n] * cz; xga += dg[n] * cx; zga += dg[n] * cz;
+    x += s[n] * cx; z += s[n] * cz;
+  }
+  const double j = xxi * zga - xga * zxi;
+  return {zga / j, -xga / j, -zxi / j, xxi / j, j, x, z};
+}
+
+bool on_edge(int type, int iz, int ix) {
+  return (type == TOP && iz == NGLL - 1) || (type == BOTTOM && iz == 0) ||
+         (type == LEFT && ix == 0) || (type == RIGHT && ix == NGLL - 1);
+}
+
+// outward (unnormalised) edge normal of an element at a point, scaled by |J|
+// (core/specfem/point/jacobian_matrix.hpp:424-449)
+void edge_normal(const JacD &J, int type, double &nx, double &nz) {
+  switch (type) {
+    case BOTTOM: nx = -J.gax * J.jac; nz = -J.gaz * J.jac; break;
+    case TOP: nx = J.gax * J.jac; nz = J.gaz * J.jac; break;
+    case LEFT: nx = -J.xix * J.jac; nz = -J.xiz * J.jac; break;
+    default: nx = J.xix * J.jac; nz = J.xiz * J.jac; break;
+  }
+}
+
+}  // namespace
+
+bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
+  RecordReader r;
+  if (!r.load(path, err)) return false;
+  try {
+    r.next();                                   // title
+    r.next();                                   // noise tomography, PML flags
+    { const char *p = r.next(4); m.nspec = rd<int>(p); }
+    { const char *p = r.next(8); m.npgeo = rd<int>(p); }
+    for (int i = 0; i < 38; ++i) r.next();
+    if (r.len() == 16) r.next();                // optional electromagnetic record
+    for (int i = 0; i < 22; ++i) r.next();
+    m.coorg.assign(2 * size_t(m.npgeo), 0.0);
+    for (int i = 0; i < m.npgeo; ++i) {
+      const char *p = r.next(20);
+      int ip = rd<int>(p);
+      double x = rd<double>(p), z = rd<double>(p);
+      if (ip < 1 || ip > m.npgeo) throw std::runtime_error("Error reading coordinates");
+      m.coorg[2 * size_t(ip - 1)] = x;
+      m.coorg[2 * size_t(ip - 1) + 1] = z;
+    }
+    int nelemabs, nacforcing, nacsurf, nfs, nfp, nsp, ntang, naxis;
+    {
+      const char *p = r.next(20);
+      m.numat = rd<int>(p); m.ngnod = rd<int>(p);
+      int ns = rd<int>(p);
+      if (ns != m.nspec) throw std::runtime_error("nspec mismatch");
+    }
+    {
+      const char *p = r.next(32);
+      nelemabs = rd<int>(p); nacforcing = rd<int>(p); nacsurf = rd<int>(p); nfs = rd<int>(p);
+      nfp = rd<int>(p); nsp = rd<int>(p); ntang = rd<int>(p); naxis = rd<int>(p);
+    }
+    if (m.ngnod != 4 && m.ngnod != 9) throw std::runtime_error("ngnod must be 4 or 9");
+    r.next();                                   // attenuation
+    m.mat_medium.resize(m.numat); m.mat_rho.resize(m.numat);
+    m.mat_vp.resize(m.numat); m.mat_vs.resize(m.numat);
+    for (int i = 0; i < m.numat; ++i) {
+      const char *p = r.next(112);
+      int n = rd<int>(p), indic = rd<int>(p);
+      double v[13];
+      for (double &x : v) x = rd<double>(p);
+      if (n != i + 1) throw std::runtime_error("Wrong material set number");
+      if (indic != 1) throw std::runtime_error("only isotropic elastic/acoustic materials are supported");
+      m.mat_rho[i] = v[0]; m.mat_vp[i] = v[1]; m.mat_vs[i] = v[2];
+      m.mat_medium[i] = (v[2] == 0.0) ? 0 : 1;
+    }
+    m.knods.assign(size_t(m.nspec) * m.ngnod, -1);
+    m.kmato.assign(m.nspec, -1);
+    for (int i = 0; i < m.nspec; ++i) {
+      const char *p = r.next(4 * (3 + m.ngnod));
+      int n = rd<int>(p), km = rd<int>(p);
+      if (n < 1 || n > m.nspec || km < 1 || km > m.numat) throw std::runtime_error("bad element record");
+      for (int k = 0; k < m.ngnod; ++k) {
+        int id = rd<int>(p);
+        if (id < 1 || id > m.npgeo) throw std::runtime_error("Error reading knods (node_id) values");
+        m.knods[size_t(n - 1) * m.ngnod + k] = id - 1;
+      }
+      m.kmato[n - 1] = km - 1;
+    }
+    r.next();                                   // ninterfaces, max_interface_size
+    for (int i = 0; i < std::max(nelemabs, 0); ++i) {
+      const char *p = r.next(56);
+      int num = rd<int>(p);
+      int c[4];
+      for (int &x : c) x = rd<int>(p);
+      int cnt = (c[0] != 0) + (c[1] != 0) + (c[2] != 0) + (c[3] != 0);
+      if (cnt != 1) throw std::runtime_error("must have one and only one absorbing edge per absorbing line cited");
+      if (num < 1 || num > m.nspec) throw std::runtime_error("Wrong absorbing element number");
+      m.abs_ispec.push_back(num - 1);
+      m.abs_type.push_back(c[0] ? BOTTOM : c[1] ? RIGHT : c[2] ? TOP : LEFT);
+    }
+    for (int i = 0; i < nacsurf; ++i) {
+      const char *p = r.next(16);
+      int isp = rd<int>(p), kind = rd<int>(p), e1 = rd<int>(p) - 1, e2 = rd<int>(p) - 1;
+      if (isp < 1 || isp > m.nspec) throw std::runtime_error("bad free-surface element");
+      if (kind == 1) throw std::runtime_error("single-node acoustic free surface records are not supported");
+      const int *kn = &m.knods[size_t(isp - 1) * m.ngnod];
+      auto is = [&](int a, int b) { return (e1 == kn[a] && e2 == kn[b]) || (e1 == kn[b] && e2 == kn[a]); };
+      int t = is(0, 1) ? BOTTOM : is(0, 3) ? LEFT : is(1, 2) ? RIGHT : is(2, 3) ? TOP : -1;
+      if (t < 0) throw std::runtime_error("Could not generate type of acoustic free surface boundary");
+      m.free_ispec.push_back(isp - 1);
+      m.free_type.push_back(t);
+    }
+    for (int i = 0; i < nacforcing; ++i) r.next();
+    for (int i = 0; i < nfs + nfp + nsp; ++i) r.next();
+    r.next();                                   // tangential flags
+    for (int i = 0; i < ntang; ++i) r.next();
+    for (int i = 0; i < naxis; ++i) r.next();
+    if (r.more()) {
+      const char *p = r.next(4);
+      int nadj = rd<int>(p);
+      for (int i = 0; i < nadj; ++i) r.next();
+    }
+    if (r.more()) throw std::runtime_error("The Database file wasn't fully read");
+  } catch (const std::exception &ex) {
+    err = ex.what();
+    return false;
+  }
+  return true;
+}
+
+// ------------------------------------------------------------ assembly ---
+void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
+  const int nspec = m.nspec;
+  if (nspec <= 0 || (m.ngnod != 4 && m.ngnod != 9)) throw std::runtime_error("invalid mesh");
+  a.nspec = nspec;
+  a.dt = dt;
+  a.elastic_wave = m.elastic_wave;
+  double z[NGLL], w[NGLL], hp[NGLL][NGLL];
+  gll(z, w, hp);
+  for (int i = 0; i < NGLL; ++i) { a.zgll[i] = z[i]; a.wgll[i] = float(w[i]); }
+  for (int i = 0; i < NGLL; ++i)
+    for (int j = 0; j < NGLL; ++j) {
+      a.hprime[i * NGLL + j] = float(hp[i][j]);
+      a.hpw[i * NGLL + j] = float(hp[i][j] * w[i]);
+    }
+
+  // --- global numbering from element topology -----------------------
+  // key: corners (node), edge points (min node, max node, position), interior
+  const size_t nloc = size_t(nspec) * NPTS;
+  std::vector<uint64_t> key(nloc);
+  const int cz[4] = {0, 0, NGLL - 1, NGLL - 1}, cx[4] = {0, NGLL - 1, NGLL - 1, 0};
+  const uint64_t npg = uint64_t(m.npgeo);
+  for (int e = 0; e < nspec; ++e) {
+    const int *kn = &m.knods[size_t(e) * m.ngnod];
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) {
+        const size_t p = size_t(e) * NPTS + iz * NGLL + ix;
+        uint64_t k = ~0ull;
+        for (int c = 0; c < 4; ++c)
+          if (iz == cz[c] && ix == cx[c]) k = uint64_t(kn[c]);
+        if (k == ~0ull) {
+          int A = -1, B = -1, t = 0;
+          if (iz == 0) { A = 0; B = 1; t = ix; }
+          else if (iz == NGLL - 1) { A = 3; B = 2; t = ix; }
+          else if (ix == 0) { A = 0; B = 3; t = iz; }
+          else if (ix == NGLL - 1) { A = 1; B = 2; t = iz; }
+          if (A >= 0) {
+            uint64_t na = kn[A], nb = kn[B];
+            uint64_t pos = na < nb ? uint64_t(t) : uint64_t(NGLL - 1 - t);
+            k = npg + (std::min(na, nb) * npg + std::max(na, nb)) * NGLL + pos;
+          } else {
+            k = npg + npg * npg * NGLL + p;  // interior: unique
+          }
+        }
+        key[p] = k;
+      }
+  }
+  std::vector<uint32_t> order(nloc);
+  std::iota(order.begin(), order.end(), 0u);
+  std::sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) { return key[x] < key[y]; });
+  std::vector<int> gid(nloc);
+  int ng = -1;
+  for (size_t i = 0; i < nloc; ++i) {
+    if (i == 0 || key[order[i]] != key[order[i - 1]]) ++ng;
+    gid[order[i]] = ng;
+  }
+  a.nglob = ng + 1;
+  // renumber by first touch in element order (locality)
+  {
+    std::vector<int> remap(a.nglob, -1);
+    int next = 0;
+    for (size_t p = 0; p < nloc; ++p)
+      if (remap[gid[p]] < 0) remap[gid[p]] = next++;
+    for (size_t p = 0; p < nloc; ++p) gid[p] = remap[gid[p]];
+  }
+  a.ibool_global = gid;
+
+  // --- geometry in mesh order --------------------------------------
+  std::vector<JacD> J(nloc);
+  a.gx.resize(nloc);
+  a.gz.resize(nloc);
+  for (int e = 0; e < nspec; ++e)
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) {
+        const size_t p = size_t(e) * NPTS + iz * NGLL + ix;
+        J[p] = jacobian(m, e, z[ix], z[iz]);
+        if (!(J[p].jac > 0)) throw std::runtime_error("non-positive Jacobian: check element orientation");
+        a.gx[p] = J[p].x;
+        a.gz[p] = J[p].z;
+      }
+
+  // --- media, colouring and compute order --------------------------
+  a.mesh_medium.resize(nspec);
+  for (int e = 0; e < nspec; ++e) a.mesh_medium[e] = m.mat_medium[m.kmato[e]];
+  a.mesh_to_compute.assign(nspec, -1);
+  // greedy colouring: no two elements of a colour share a global point
+  std::vector<int> color(nspec, 0);
+  {
+    std::vector<uint32_t> used(a.nglob, 0u);
+    for (int e = 0; e < nspec; ++e) {
+      uint32_t mask = 0;
+      for (int q = 0; q < NPTS; ++q) mask |= used[gid[size_t(e) * NPTS + q]];
+      int c = 0;
+      while (c < 32 && (mask >> c & 1u)) ++c;
+      if (c == 32) throw std::runtime_error("mesh needs more than 32 colours");
+      color[e] = c;
+      for (int q = 0; q < NPTS; ++q) used[gid[size_t(e) * NPTS + q]] |= 1u << c;
+    }
+  }
+  const double rho_default = 0;
+  (void)rho_default;
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    D.ncomp = med == 1 ? (m.elastic_wave == 1 ? 1 : 2) : 1;
+    int ncol = 0;
+    for (int e = 0; e < nspec; ++e)
+      if (a.mesh_medium[e] == med) ncol = std::max(ncol, color[e] + 1);
+    D.color_start.assign(1, 0);
+    for (int c = 0; c < ncol; ++c) {
+      for (int e = 0; e < nspec; ++e)
+        if (a.mesh_medium[e] == med && color[e] == c) {
+          a.mesh_to_compute[e] = int(D.elem_mesh.size());
+          D.elem_mesh.push_back(e);
+        }
+      D.color_start.push_back(int(D.elem_mesh.size()));
+    }
+    D.nspec = int(D.elem_mesh.size());
+    // per-medium point numbering by first touch in compute order
+    std::vector<int> &g2m = med == 1 ? a.glob_to_el : a.glob_to_ac;
+    g2m.assign(a.nglob, -1);
+    D.ibool.resize(size_t(D.nspec) * NPTS);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      for (int q = 0; q < NPTS; ++q) {
+        const int g = gid[size_t(e) * NPTS + q];
+        if (g2m[g] < 0) { g2m[g] = D.nglob++; D.glob_of_point.push_back(g); }
+        D.ibool[size_t(ce) * NPTS + q] = g2m[g];
+      }
+    }
+    const size_t n = size_t(D.nspec) * NPTS;
+    D.xix.resize(n); D.xiz.resize(n); D.gax.resize(n); D.gaz.resize(n); D.jac.resize(n);
+    D.prop0.resize(n); D.prop1.resize(n);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      const int mat = m.kmato[e];
+      for (int q = 0; q < NPTS; ++q) {
+        const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
+        D.xix[pc] = float(J[pm].xix); D.xiz[pc] = float(J[pm].xiz);
+        D.gax[pc] = float(J[pm].gax); D.gaz[pc] = float(J[pm].gaz);
+        D.jac[pc] = float(J[pm].jac);
+        const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
+        const double vp = m.pvp.empty() ? m.mat_vp[mat] : m.pvp[pm];
+        const double vs = m.pvs.empty() ? m.mat_vs[mat] : m.pvs[pm];
+        if (med == 1) {
+          // kappa = rho (vp^2 - 4/3 vs^2), mu = rho vs^2; lambda+2mu = kappa + 4/3 mu
+          // (include/medium/dim2/elastic/isotropic/material.hpp:66-69, properties.hpp:71-91)
+          const double mu = rho * vs * vs;
+          const double kappa = rho * (vp * vp - 4.0 / 3.0 * vs * vs);
+          D.prop0[pc] = float(kappa + 4.0 / 3.0 * mu);
+          D.prop1[pc] = float(mu);
+        } else {
+          D.prop0[pc] = float(1.0 / rho);            // rho_inverse
+          D.prop1[pc] = float(rho * vp * vp);        // kappa
+        }
+      }
+    }
+  }
+
+  // --- Stacey and free-surface point data --------------------------
+  // Absorbing entries are applied in database order; on a corner shared by
+  // two absorbing edges of one element the later entry's normal and weight
+  // win (core/specfem/assembly/boundaries/dim2/impl/stacey.tpp).
+  struct BcPt { double w = 0, nx = 0, nz = 0; bool st = false, fs = false; };
+  std::unordered_map<int, std::vector<BcPt>> bc;  // mesh element -> 25 points
+  for (size_t i = 0; i < m.abs_ispec.size(); ++i) {
+    const int e = m.abs_ispec[i], t = m.abs_type[i];
+    auto &v = bc[e];
+    v.resize(NPTS);
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) {
+        if (!on_edge(t, iz, ix)) continue;
+        BcPt &b = v[iz * NGLL + ix];
+        b.st = true;
+        edge_normal(J[size_t(e) * NPTS + iz * NGLL + ix], t, b.nx, b.nz);
+        b.w = (t == LEFT || t == RIGHT) ? w[iz] : w[ix];
+      }
+  }
+  for (size_t i = 0; i < m.free_ispec.size(); ++i) {
+    const int e = m.free_ispec[i], t = m.free_type[i];
+    if (a.mesh_medium[e] != 0) continue;      // free surface acts on acoustic media
+    auto &v = bc[e];
+    v.resize(NPTS);
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix)
+        if (on_edge(t, iz, ix)) v[iz * NGLL + ix].fs = true;
+  }
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    D.bc_slot.assign(D.nspec, -1);
+    int ns = 0;
+    for (int ce = 0; ce < D.nspec; ++ce)
+      if (bc.count(D.elem_mesh[ce])) D.bc_slot[ce] = ns++;
+    const size_t n = size_t(ns) * NPTS;
+    D.bc_w.assign(n, 0); D.bc_nx.assign(n, 0); D.bc_nz.assign(n, 0); D.bc_j1.assign(n, 0);
+    D.bc_imp0.assign(n, 0); D.bc_imp1.assign(n, 0); D.bc_keep.assign(n, 1.0f);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      if (D.bc_slot[ce] < 0) continue;
+      const auto &v = bc[D.elem_mesh[ce]];
+      for (int q = 0; q < NPTS; ++q) {
+        const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
+        const size_t pc = size_t(ce) * NPTS + q;
+        if (v[q].st) {
+          D.bc_w[k] = float(v[q].w);
+          D.bc_nx[k] = float(v[q].nx);
+          D.bc_nz[k] = float(v[q].nz);
+          D.bc_j1[k] = float(std::sqrt(v[q].nx * v[q].nx + v[q].nz * v[q].nz));
+          const int e = D.elem_mesh[ce];
+          const size_t pm = size_t(e) * NPTS + q;
+          const int mat = m.kmato[e];
+          const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
+          if (med == 1) {
+            // rho*vp = sqrt((lambda+2mu)/rho)*rho, rho*vs = sqrt(rho*mu) (properties.hpp:77-87)
+            const double l2m = D.prop0[pc], mu = D.prop1[pc];
+            D.bc_imp0[k] = float(std::sqrt(l2m / rho) * rho);
+            D.bc_imp1[k] = float(std::sqrt(rho * mu));
+          } else {
+            // 1/(rho vp) = sqrt(rho_inverse / kappa) (acoustic properties.hpp:69-72)
+            D.bc_imp0[k] = float(std::sqrt(double(D.prop0[pc]) / double(D.prop1[pc])));
+          }
+        }
+        if (v[q].fs) D.bc_keep[k] = 0.0f;
+      }
+    }
+  }
+
+  // --- acoustic/elastic coupling edges -----------------------------
+  // each element pair sharing an edge across media contributes, on the self
+  // side, weight * outward normal of the self element at the edge points
+  // (core/specfem/assembly/conforming_interfaces/dim2/impl/interface_container.tpp)
+  {
+    std::unordered_map<uint64_t, std::vector<std::pair<int, int>>> edges;
+    const int ends[4][2] = {{0, 1}, {1, 2}, {3, 2}, {0, 3}};
+    for (int e = 0; e < nspec; ++e) {
+      const int *kn = &m.knods[size_t(e) * m.ngnod];
+      for (int t = 0; t < 4; ++t) {
+        uint64_t na = kn[ends[t][0]], nb = kn[ends[t][1]];
+        edges[std::min(na, nb) * npg + std::max(na, nb)].push_back({e, t});
+      }
+    }
+    std::unordered_map<int, std::vector<double>> cp;  // mesh element -> [25][2]
+    for (auto &kv : edges) {
+      if (kv.second.size() != 2) continue;
+      const auto [e1, t1] = kv.second[0];
+      const auto [e2, t2] = kv.second[1];
+      if (a.mesh_medium[e1] == a.mesh_medium[e2]) continue;
+      for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
+        auto &v = cp[e];
+        v.resize(2 * NPTS, 0.0);
+        for (int iz = 0; iz < NGLL; ++iz)
+          for (int ix = 0; ix < NGLL; ++ix) {
+            if (!on_edge(t, iz, ix)) continue;
+            double nx, nz;
+            edge_normal(J[size_t(e) * NPTS + iz * NGLL + ix], t, nx, nz);
+            const double f = (t == BOTTOM || t == TOP) ? w[ix] : w[iz];
+            v[2 * (iz * NGLL + ix)] += f * nx;
+            v[2 * (iz * NGLL + ix) + 1] += f * nz;
+          }
+      }
+    }
+    for (int med = 0; med < 2; ++med) {
+      MediumData &D = med == 1 ? a.el : a.ac;
+      const std::vector<int> &other = med == 1 ? a.glob_to_ac : a.glob_to_el;
+      D.cp_slot.assign(D.nspec, -1);
+      int ns = 0;
+      for (int ce = 0; ce < D.nspec; ++ce)
+        if (cp.count(D.elem_mesh[ce])) D.cp_slot[ce] = ns++;
+      D.cp_nx.assign(size_t(ns) * NPTS, 0); D.cp_nz.assign(size_t(ns) * NPTS, 0);
+      D.cp_other.assign(size_t(ns) * NPTS, -1);
+      for (int ce = 0; ce < D.nspec; ++ce) {
+        if (D.cp_slot[ce] < 0) continue;
+        const int e = D.elem_mesh[ce];
+        const auto &v = cp[e];
+        for (int q = 0; q < NPTS; ++q) {
+          const size_t k = size_t(D.cp_slot[ce]) * NPTS + q;
+          const int g = gid[size_t(e) * NPTS + q];
+          if (v[2 * q] == 0.0 && v[2 * q + 1] == 0.0) continue;
+          // coupling at acoustic free-surface points is dropped (compute_coupling.tpp:101-106)
+          float keep = 1.0f;
+          if (D.bc_slot[ce] >= 0) keep = D.bc_keep[size_t(D.bc_slot[ce]) * NPTS + q];
+          D.cp_nx[k] = float(v[2 * q]) * keep;
+          D.cp_nz[k] = float(v[2 * q + 1]) * keep;
+          D.cp_other[k] = other[g];
+        }
+      }
+    }
+  }
+
+  // --- mass matrix (+ Stacey implicit term), inverted -------------
+  // M = sum rho w_x w_z |J| (acoustic: 1/kappa), plus (dt/2) C on Stacey points
+  // (compute_mass_matrix.tpp:95-121, stacey.tpp:817-853), then 1/M.
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    std::vector<double> M(size_t(D.nglob) * D.ncomp, 0.0);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      const int mat = m.kmato[e];
+      for (int iz = 0; iz < NGLL; ++iz)
+        for (int ix = 0; ix < NGLL; ++ix) {
+          const int q = iz * NGLL + ix;
+          const size_t pc = size_t(ce) * NPTS + q, pm = size_t(e) * NPTS + q;
+          const double fac = w[ix] * w[iz] * J[pm].jac;
+          const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
+          double mc[2];
+          if (med == 1) mc[0] = mc[1] = rho * fac;
+          else mc[0] = (1.0 / double(D.prop1[pc])) * fac;
+          if (D.bc_slot[ce] >= 0) {
+            const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
+            if (D.bc_w[k] != 0.0f) {
+              const double vv = -dt * 0.5;  // velocity stand-in of the implicit term
+              const double nx = D.bc_nx[k], nz = D.bc_nz[k], j1 = D.bc_j1[k], wq = D.bc_w[k];
+              if (med == 0) {
+                mc[0] += -1.0 * wq * j1 * double(D.bc_imp0[k]) * vv;
+              } else if (D.ncomp == 1) {
+                mc[0] += -1.0 * wq * j1 * double(D.bc_imp1[k]) * vv;
+              } else {
+                const double vn = vv * nx + vv * nz;
+                const double dn[2] = {nx, nz};
+                for (int c = 0; c < 2; ++c) {
+                  const double f = ((vn * dn[c] / (j1 * j1)) * (double(D.bc_imp0[k]) - double(D.bc_imp1[k]))) +
+                                   vv * double(D.bc_imp1[k]);
+                  mc[c] += -1.0 * f * j1 * wq;
+                }
+              }
+            }
+          }
+          const int g = D.ibool[pc];
+          for (int c = 0; c < D.ncomp; ++c) M[size_t(g) * D.ncomp + c] += mc[c];
+        }
+    }
+    D.minv.resize(M.size());
+    for (size_t i = 0; i < M.size(); ++i) D.minv[i] = float(1.0 / M[i]);
+  }
+}
+
+// ------------------------------------------------------ point location ---
+// Closest GLL point, then Newton iterations from the element centre in that
+// element and its corner-sharing neighbours; the candidate whose mapped point
+// is closest wins (src/algorithms/dim2/locate_point_impl.cpp).
+// A point on an edge or corner shared by several elements goes to the first
+// element in mesh order: a candidate replaces the current choice only when it
+// is closer by more than 1e-9 of the mesh extent.
+bool locate_point2d(const Mesh2D &m, const Assembly2D &a, double x, double z, int &ispec,
+                    double &xi, double &gamma) {
+  const size_t nloc = a.gx.size();
+  double xmin = 1e300, xmax = -1e300, zmin = 1e300, zmax = -1e300;
+  for (int i = 0; i < m.npgeo; ++i) {
+    xmin = std::min(xmin, m.coorg[2 * i]); xmax = std::max(xmax, m.coorg[2 * i]);
+    zmin = std::min(zmin, m.coorg[2 * i + 1]); zmax = std::max(zmax, m.coorg[2 * i + 1]);
+  }
+  const double tol = 1e-9 * std::max(xmax - xmin, zmax - zmin);
+  double best = 1e300;
+  size_t pb = 0;
+  for (size_t p = 0; p < nloc; ++p) {
+    const double d = std::sqrt((a.gx[p] - x) * (a.gx[p] - x) + (a.gz[p] - z) * (a.gz[p] - z));
+    if (d < best - tol) { best = d; pb = p; }
+  }
+  const int eg = int(pb / NPTS);
+  std::vector<int> cand{eg};
+  const int *kg = &m.knods[size_t(eg) * m.ngnod];
+  for (int e = 0; e < m.nspec; ++e) {
+    if (e == eg) continue;
+    const int *ke = &m.knods[size_t(e) * m.ngnod];
+    bool share = false;
+    for (int i = 0; i < 4 && !share; ++i)
+      for (int j = 0; j < 4; ++j)
+        if (kg[i] == ke[j]) { share = true; break; }
+    if (share) cand.push_back(e);
+  }
+  double fd = 1e300;
+  ispec = -1;
+  for (int e : cand) {
+    double s = 0, g = 0;
+    for (int it = 0; it < 100; ++it) {
+      JacD J = jacobian(m, e, s, g);
+      const double dx = x - J.x, dz = z - J.z;
+      const double ds = J.xix * dx + J.xiz * dz, dg = J.gax * dx + J.gaz * dz;
+      s = std::min(std::max(s + ds, -1.01), 1.01);
+      g = std::min(std::max(g + dg, -1.01), 1.01);
+      if (std::abs(ds) < 1e-12 && std::abs(dg) < 1e-12) break;
+    }
+    JacD J = jacobian(m, e, s, g);
+    const double d = std::sqrt((J.x - x) * (J.x - x) + (J.z - z) * (J.z - z));
+    if (d < fd - tol) { fd = d; ispec = e; xi = s; gamma = g; }
+  }
+  if (ispec < 0 || std::abs(std::abs(xi) - 1.01) < 1e-6 || std::abs(std::abs(gamma) - 1.01) < 1e-6)
+    return false;
+  return true;
+}
+
+void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &src) {
+  a.nsrc = int(src.size());
+  a.src_medium.resize(a.nsrc); a.src_elem.resize(a.nsrc); a.src_shot.resize(a.nsrc);
+  a.src_next.assign(a.nsrc, -1);
+  a.src_arr.assign(size_t(a.nsrc) * 2 * NPTS, 0.0f);
+  a.el_src_head.assign(a.el.nspec, -1);
+  a.ac_src_head.assign(a.ac.nspec, -1);
+  // start time per shot: t0 = min over the shot's sources of -1.2/f0 + tshift,
+  // and each source's shift becomes t0_source - t0 (read_sources.cpp:142-172);
+  // Dirac sources use f0 = 1/(10 dt) (dirac.cpp:25).
+  std::vector<double> f0(a.nsrc), t0s(a.nsrc);
+  a.shot_t0.assign(a.nshots, 1e300);
+  for (int s = 0; s < a.nsrc; ++s) {
+    const Source2D &S = src[s];
+    if (S.shot < 0 || S.shot >= a.nshots) throw std::runtime_error("source shot index out of range");
+    f0[s] = S.stf == 1 ? double(1.0f / (10.0f * float(a.dt))) : S.f0;
+    if (!(f0[s] > 0)) throw std::runtime_error("source f0 must be positive");
+    t0s[s] = double(-1.2f * (1.0f / float(f0[s])) + float(S.tshift));
+    a.shot_t0[S.shot] = std::min(a.shot_t0[S.shot], t0s[s]);
+  }
+  for (double &t : a.shot_t0)
+    if (t > 1e299) t = 0.0;
+  a.t0 = *std::min_element(a.shot_t0.begin(), a.shot_t0.end());
+  a.stf.assign(size_t(a.nstep) * a.nsrc, 0.0f);
+  for (int s = 0; s < a.nsrc; ++s) {
+    const Source2D &S = src[s];
+    int e;
+    double xi, ga;
+    if (!locate_point2d(m, a, S.x, S.z, e, xi, ga)) throw std::runtime_error("Failed to locate source in the mesh");
+    const int med = a.mesh_medium[e];
+    const int ce = a.mesh_to_compute[e];
+    a.src_medium[s] = med; a.src_elem[s] = ce; a.src_shot[s] = S.shot;
+    std::vector<int> &head = med == 1 ? a.el_src_head : a.ac_src_head;
+    a.src_next[s] = head[ce];
+    head[ce] = s;
+    double hx[NGLL], hg[NGLL];
+    lagrange(xi, a.zgll, hx);
+    lagrange(ga, a.zgll, hg);
+    const MediumData &D = med == 1 ? a.el : a.ac;
+    const double ang = S.angle * M_PI / 180.0;
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) {
+        const int q = iz * NGLL + ix;
+        const double h = hx[ix] * hg[iz];
+        if (med == 0) {
+          // pressure source: -stf * l / kappa (acoustic source.hpp:65); the
+          // sign is applied to the STF column below
+          a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h / double(D.prop1[size_t(ce) * NPTS + q]));
+        } else if (D.ncomp == 1) {
+          a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h);
+        } else {
+          a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h * std::sin(ang));
+          a.src_arr[(size_t(s) * 2 + 1) * NPTS + q] = float(h * std::cos(ang));
+        }
+      }
+    // STF on the shot's own time axis, FP32 like the reference tables
+    const float tsh = float(t0s[s] - a.shot_t0[S.shot]);
+    const float t0 = float(a.shot_t0[S.shot]);
+    const float fz = float(f0[s]), fac = float(S.factor);
+    const float pi = float(M_PI);
+    const float aa = pi * pi * fz * fz;
+    for (int i = 0; i < a.nstep; ++i) {
+      const float t = t0 + float(i) * float(a.dt) - tsh;
+      float v;
+      if (S.stf == 1) v = fac * (-1.0f * std::exp(-aa * t * t) / (2.0f * aa));
+      else v = fac * ((1.0f - 2.0f * aa * t * t) * std::exp(-aa * t * t));
+      a.stf[size_t(i) * a.nsrc + s] = med == 0 ? -v : v;
+    }
+  }
+}
+
+void set_receivers2d(const Mesh2D &m, Assembly2D &a, const std::vector<double> &x,
+                     const std::vector<double> &z, double angle, const std::vector<int> &types) {
+  a.nrec = int(x.size());
+  a.types = types;
+  a.ntypes = int(types.size());
+  a.rec_angle = angle;
+  a.rec_medium.resize(a.nrec); a.rec_elem.resize(a.nrec);
+  a.rec_h.assign(size_t(a.nrec) * NPTS, 0.0f);
+  for (int r = 0; r < a.nrec; ++r) {
+    int e;
+    double xi, ga;
+    if (!locate_point2d(m, a, x[r], z[r], e, xi, ga)) throw std::runtime_error("Failed to locate receiver in the mesh");
+    a.rec_medium[r] = a.mesh_medium[e];
+    a.rec_elem[r] = a.mesh_to_compute[e];
+    double hx[NGLL], hg[NGLL];
+    lagrange(xi, a.zgll, hx);
+    lagrange(ga, a.zgll, hg);
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) a.rec_h[size_t(r) * NPTS + iz * NGLL + ix] = float(hx[ix] * hg[iz]);
+  }
+}
+
+}  // namespace sfg

@@ -1,0 +1,99 @@
+// Host-side (Kokkos-free) 2D mesh and assembly data model of libsfg.
+//
+// Mirrors the reference's specfem::mesh::mesh<dim2> (include/mesh/dim2/mesh.hpp)
+// and the parts of specfem::assembly::assembly<dim2> that the time step reads
+// (core/specfem/assembly/*), laid out for the device: elements are reordered by
+// medium and colour, element-local arrays are [element][25] in that order, and
+// each medium has its own global point numbering (the reference's per-medium
+// assembly_index_mapping, core/specfem/assembly/fields/impl/field_impl.tpp:18-62).
+#pragma once
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace sfg {
+
+constexpr int NGLL = 5;
+constexpr int NPTS = NGLL * NGLL;
+
+struct Mesh2D {
+  int nspec = 0, npgeo = 0, ngnod = 0;
+  std::vector<double> coorg;          // [npgeo][2]
+  std::vector<int> knods;             // [nspec][ngnod]
+  std::vector<int> kmato;             // [nspec]
+  int numat = 0;
+  std::vector<int> mat_medium;        // [numat]
+  std::vector<double> mat_rho, mat_vp, mat_vs;
+  std::vector<float> prho, pvp, pvs;  // optional [nspec][25]
+  std::vector<int> abs_ispec, abs_type, free_ispec, free_type;
+  int elastic_wave = 0;               // 0 P-SV, 1 SH
+};
+
+// Reads a SPECFEM2D database.bin (Fortran unformatted records).
+bool read_database2d(const std::string &path, Mesh2D &m, std::string &err);
+
+struct Source2D {
+  double x, z;
+  int shot, stf;
+  double f0, factor, tshift, angle;
+};
+
+// Per-medium device-ready arrays (element order = compute order of that medium).
+struct MediumData {
+  int nspec = 0, nglob = 0, ncomp = 0;
+  std::vector<int> color_start;       // [ncolors+1] element ranges
+  std::vector<int> elem_mesh;         // compute element -> mesh element
+  std::vector<int> ibool;             // [nspec][25] -> medium point id
+  std::vector<float> xix, xiz, gax, gaz, jac;  // [nspec][25]
+  std::vector<float> prop0, prop1;    // elastic: lambda+2mu, mu; acoustic: 1/rho, kappa
+  std::vector<float> minv;            // [nglob][ncomp]
+  // Stacey / free-surface: slot per element (-1 none), compact [nslot][25]
+  std::vector<int> bc_slot;
+  std::vector<float> bc_w, bc_nx, bc_nz, bc_j1, bc_imp0, bc_imp1, bc_keep;
+  // coupling with the other medium: slot per element, compact [nslot][25]
+  std::vector<int> cp_slot;
+  std::vector<float> cp_nx, cp_nz;    // sum over coupled edges of weight * normal
+  std::vector<int> cp_other;          // other medium's point id (-1 none)
+  std::vector<int> glob_of_point;     // medium point id -> mesh global id
+};
+
+struct Assembly2D {
+  int nspec = 0, nglob = 0, nshots = 1, elastic_wave = 0;
+  double dt = 0;
+  int nstep = 0, nsb = 1;
+  float hprime[NPTS];                 // hprime[i*5+j] = l'_j(xi_i)
+  float hpw[NPTS];                    // hprime[l*5+i] * w[l]  (divergence form)
+  float wgll[NGLL];
+  double zgll[NGLL];
+  std::vector<int> ibool_global;      // [nspec][25] mesh order
+  std::vector<double> gx, gz;         // [nspec][25] mesh order, GLL point coordinates
+  MediumData el, ac;
+  std::vector<int> mesh_medium;       // [nspec]
+  std::vector<int> mesh_to_compute;   // [nspec] index inside its medium
+  std::vector<int> glob_to_el, glob_to_ac;
+  // sources (compute-order element of their medium)
+  int nsrc = 0;
+  std::vector<int> src_medium, src_elem, src_shot, src_next, el_src_head, ac_src_head;
+  std::vector<float> src_arr;         // [nsrc][2][25]
+  std::vector<float> stf;             // [nstep][nsrc]
+  std::vector<double> shot_t0;        // per shot
+  double t0 = 0;
+  // receivers
+  int nrec = 0, ntypes = 0, nsig = 0;
+  std::vector<int> rec_medium, rec_elem, types;
+  std::vector<float> rec_h;           // [nrec][25]
+  double rec_angle = 0;
+};
+
+// Build everything but sources/receivers (numbering, geometry, colouring,
+// boundaries, coupling, mass matrix).  Throws std::runtime_error on error.
+void assemble2d(const Mesh2D &m, double dt, Assembly2D &a);
+void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &src);
+void set_receivers2d(const Mesh2D &m, Assembly2D &a, const std::vector<double> &x,
+                     const std::vector<double> &z, double angle, const std::vector<int> &types);
+// locate a physical point: returns mesh element and (xi, gamma)
+bool locate_point2d(const Mesh2D &m, const Assembly2D &a, double x, double z, int &ispec,
+                    double &xi, double &gamma);
+
+}  // namespace sfg

@@ -1,0 +1,755 @@
+// libsfg: handle management, device upload, step scheduling (CUDA graphs) and
+// the extern "C" entry points declared in include/sfg.h.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/sfg.h"
+#include "host2d.hpp"
+#include "kernels2d.cuh"
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+#define SFG_CUDA(call)                                                                   \
+  do {                                                                                   \
+    cudaError_t _e = (call);                                                             \
+    if (_e != cudaSuccess)                                                               \
+      throw CudaError(std::string(#call) + ": " + cudaGetErrorString(_e));               \
+  } while (0)
+
+// Device buffer list owned by a handle.
+struct DevMem {
+  std::vector<void *> ptrs;
+  size_t bytes = 0;
+  template <typename T>
+  T *upload(const std::vector<T> &h) {
+    if (h.empty()) return nullptr;
+    T *d = nullptr;
+    SFG_CUDA(cudaMalloc(&d, h.size() * sizeof(T)));
+    ptrs.push_back(d);
+    bytes += h.size() * sizeof(T);
+    SFG_CUDA(cudaMemcpy(d, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return d;
+  }
+  template <typename T>
+  T *zeros(size_t n) {
+    if (n == 0) return nullptr;
+    T *d = nullptr;
+    SFG_CUDA(cudaMalloc(&d, n * sizeof(T)));
+    ptrs.push_back(d);
+    bytes += n * sizeof(T);
+    SFG_CUDA(cudaMemset(d, 0, n * sizeof(T)));
+    return d;
+  }
+  void free_all() {
+    for (void *p : ptrs) cudaFree(p);
+    ptrs.clear();
+    bytes = 0;
+  }
+};
+
+struct DevMedium {
+  int nspec = 0, nglob = 0, ncomp = 0;
+  std::vector<int> color_start;
+  int *ibool = nullptr;
+  float *xix = nullptr, *xiz = nullptr, *gax = nullptr, *gaz = nullptr, *jac = nullptr,
+        *prop0 = nullptr, *prop1 = nullptr;
+  int *bc_slot = nullptr;
+  float *bc_w = nullptr, *bc_nx = nullptr, *bc_nz = nullptr, *bc_j1 = nullptr,
+        *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr;
+  int *cp_slot = nullptr;
+  float *cp_nx = nullptr, *cp_nz = nullptr;
+  int *cp_other = nullptr;
+  int *src_head = nullptr;
+  float *minv = nullptr;
+  float *u = nullptr, *v = nullptr, *accum = nullptr, *a = nullptr;
+  int *rec_list = nullptr;
+  int nrec = 0;
+};
+
+}  // namespace
+
+struct sfg_handle {
+  sfg::Mesh2D mesh;
+  sfg::Assembly2D asmb;
+  sfg_options opt{};
+  std::vector<sfg::Source2D> sources;
+  std::vector<double> rec_x, rec_z;
+  bool have_sources = false, have_receivers = false, initialized = false;
+  std::vector<float> ext_stf;  // optional external STF table
+  int ext_stf_nsrc = 0;
+  DevMem mem;
+  DevMedium el, ac;
+  int *d_src_next = nullptr;
+  float *d_src_arr = nullptr, *d_stf = nullptr;
+  int *d_rec_elem = nullptr;
+  float *d_rec_h = nullptr, *d_seis = nullptr;
+  int *d_step = nullptr, *d_flag = nullptr;
+  int host_step = 0;
+  int epb = 16;
+  cudaStream_t stream = nullptr;
+  cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr;
+  int graph_steps = 0;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  void *flush_buf = nullptr;
+  size_t flush_bytes = 0;
+  std::string err;
+  sfg::dev::Quad quad{};
+
+  ~sfg_handle() {
+    if (graph_k) cudaGraphExecDestroy(graph_k);
+    if (graph_1) cudaGraphExecDestroy(graph_1);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+    if (stream) cudaStreamDestroy(stream);
+    if (flush_buf) cudaFree(flush_buf);
+    mem.free_all();
+  }
+};
+
+namespace {
+
+template <typename F>
+int guarded(sfg_handle *h, F &&fn) {
+  if (!h) return SFG_ERR_ARG;
+  try {
+    return fn();
+  } catch (const CudaError &ex) {
+    h->err = ex.what();
+    return SFG_ERR_CUDA;
+  } catch (const std::exception &ex) {
+    h->err = ex.what();
+    return SFG_ERR_ARG;
+  }
+}
+
+void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
+  DevMem &m = h->mem;
+  D.nspec = M.nspec;
+  D.nglob = M.nglob;
+  D.ncomp = M.ncomp;
+  D.color_start = M.color_start;
+  if (M.nspec == 0) return;
+  D.ibool = m.upload(M.ibool);
+  D.xix = m.upload(M.xix); D.xiz = m.upload(M.xiz); D.gax = m.upload(M.gax);
+  D.gaz = m.upload(M.gaz); D.jac = m.upload(M.jac);
+  D.prop0 = m.upload(M.prop0); D.prop1 = m.upload(M.prop1);
+  D.bc_slot = m.upload(M.bc_slot);
+  D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
+  D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
+  D.bc_keep = m.upload(M.bc_keep);
+  D.cp_slot = m.upload(M.cp_slot);
+  D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
+  D.minv = m.upload(M.minv);
+  const size_t n = size_t(M.nglob) * M.ncomp;
+  // pad by 4 floats so float4 streaming never runs past an allocation
+  D.u = m.zeros<float>(n + 4);
+  D.v = m.zeros<float>(n + 4);
+  D.accum = m.zeros<float>(n + 4);
+  D.a = m.zeros<float>(n + 4);
+}
+
+sfg::dev::ElemArgs elem_args(sfg_handle *h, DevMedium &D, DevMedium &O, bool acoustic) {
+  sfg::dev::ElemArgs A{};
+  A.ibool = D.ibool;
+  A.xix = D.xix; A.xiz = D.xiz; A.gax = D.gax; A.gaz = D.gaz; A.jac = D.jac;
+  A.prop0 = D.prop0; A.prop1 = D.prop1;
+  A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
+  A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
+  A.cp_slot = D.cp_slot; A.cp_nx = D.cp_nx; A.cp_nz = D.cp_nz; A.cp_other = D.cp_other;
+  A.other = acoustic ? O.u : O.a;
+  A.src_head = D.src_head; A.src_next = h->d_src_next; A.src_arr = h->d_src_arr;
+  A.stf = h->d_stf;
+  A.nsrc = h->asmb.nsrc;
+  A.nstep = h->asmb.nstep;
+  A.step = h->d_step;
+  A.u = D.u; A.v = D.v; A.accum = D.accum;
+  A.quad = h->quad;
+  return A;
+}
+
+template <int E>
+void launch_stiffness_E(sfg_handle *h, DevMedium &D, DevMedium &O, int medium, cudaStream_t s) {
+  sfg::dev::ElemArgs A = elem_args(h, D, O, medium == SFG_MEDIUM_ACOUSTIC);
+  for (size_t c = 0; c + 1 < D.color_start.size(); ++c) {
+    A.e0 = D.color_start[c];
+    A.e1 = D.color_start[c + 1];
+    const int n = A.e1 - A.e0;
+    if (n <= 0) continue;
+    const int grid = (n + E - 1) / E;
+    if (medium == SFG_MEDIUM_ACOUSTIC)
+      sfg::dev::k_stiffness_1c<E, 0><<<grid, sfg::dev::NP * E, 0, s>>>(A);
+    else if (D.ncomp == 1)
+      sfg::dev::k_stiffness_1c<E, 1><<<grid, sfg::dev::NP * E, 0, s>>>(A);
+    else
+      sfg::dev::k_stiffness_psv<E><<<grid, sfg::dev::NP * E, 0, s>>>(A);
+  }
+}
+
+void launch_stiffness(sfg_handle *h, int medium, cudaStream_t s) {
+  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+  DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
+  switch (h->epb) {
+    case 8: launch_stiffness_E<8>(h, D, O, medium, s); break;
+    case 32: launch_stiffness_E<32>(h, D, O, medium, s); break;
+    default: launch_stiffness_E<16>(h, D, O, medium, s); break;
+  }
+}
+
+void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
+  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+  if (D.nrec == 0) return;
+  sfg::dev::RecArgs R{};
+  R.nrec = D.nrec;
+  R.rec_list = D.rec_list;
+  R.rec_elem = h->d_rec_elem;
+  R.rec_h = h->d_rec_h;
+  R.ibool = D.ibool;
+  R.xix = D.xix; R.xiz = D.xiz; R.gax = D.gax; R.gaz = D.gaz; R.prop0 = D.prop0;
+  R.prop1 = D.prop1;
+  R.u = D.u; R.v = D.v; R.accum = D.accum; R.minv = D.minv;
+  R.ncomp = D.ncomp;
+  R.acoustic = medium == SFG_MEDIUM_ACOUSTIC;
+  R.ntypes = h->asmb.ntypes;
+  for (int t = 0; t < R.ntypes && t < 4; ++t) R.types[t] = h->asmb.types[t];
+  R.nsb = h->asmb.nsb;
+  R.nsig = h->asmb.nsig;
+  R.nrec_total = h->asmb.nrec;
+  R.dt2 = float(h->asmb.dt) / 2.0f;
+  R.step = h->d_step;
+  R.seis = h->d_seis;
+  R.quad = h->quad;
+  sfg::dev::k_receivers<<<D.nrec, 32, 0, s>>>(R);
+}
+
+void launch_update(sfg_handle *h, int medium, bool advance, cudaStream_t s) {
+  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+  sfg::dev::UpdateArgs U{};
+  U.u = D.u; U.v = D.v; U.accum = D.accum; U.minv = D.minv;
+  // acoustic chi_dd feeds the elastic coupling term; the elastic acceleration is
+  // kept only on request (field read-back)
+  U.a_store = (medium == SFG_MEDIUM_ACOUSTIC || h->opt.store_acceleration) ? D.a : nullptr;
+  U.n = D.nglob * D.ncomp;
+  const float dt = float(h->asmb.dt);
+  U.dt = dt;
+  U.dt2 = dt / 2.0f;
+  U.dtsq2 = dt * dt / 2.0f;
+  U.flag = h->d_flag;
+  U.step = h->d_step;
+  U.advance = advance ? 1 : 0;
+  const int threads = 256;
+  int blocks = (U.n / 4 + threads - 1) / threads;
+  blocks = std::max(1, std::min(blocks, 148 * 8));
+  sfg::dev::k_update<<<blocks, threads, 0, s>>>(U);
+}
+
+// One time step in the reference's medium order (time_marching.tpp:33-83):
+// acoustic update (coupling from the predicted elastic displacement), then
+// elastic update (coupling from the new acoustic chi_dd).
+void enqueue_step(sfg_handle *h, cudaStream_t s) {
+  const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
+  if (has_ac) {
+    launch_stiffness(h, SFG_MEDIUM_ACOUSTIC, s);
+    launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
+    launch_update(h, SFG_MEDIUM_ACOUSTIC, !has_el, s);
+  }
+  if (has_el) {
+    launch_stiffness(h, SFG_MEDIUM_ELASTIC, s);
+    launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
+    launch_update(h, SFG_MEDIUM_ELASTIC, true, s);
+  }
+}
+
+int kernels_per_step(const sfg_handle *h) {
+  int n = 0;
+  for (const DevMedium *D : {&h->ac, &h->el}) {
+    if (D->nspec == 0) continue;
+    n += int(D->color_start.size()) - 1 + (D->nrec > 0 ? 1 : 0) + 1;
+  }
+  return n;
+}
+
+cudaGraphExec_t capture(sfg_handle *h, int nsteps) {
+  cudaGraph_t g = nullptr;
+  SFG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < nsteps; ++i) enqueue_step(h, h->stream);
+  SFG_CUDA(cudaStreamEndCapture(h->stream, &g));
+  cudaGraphExec_t ex = nullptr;
+  SFG_CUDA(cudaGraphInstantiate(&ex, g, 0));
+  cudaGraphDestroy(g);
+  return ex;
+}
+
+void run_steps(sfg_handle *h, int nsteps) {
+  int left = nsteps;
+  while (left >= h->graph_steps && h->graph_k) {
+    SFG_CUDA(cudaGraphLaunch(h->graph_k, h->stream));
+    left -= h->graph_steps;
+  }
+  while (left > 0) {
+    SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+    --left;
+  }
+  SFG_CUDA(cudaGetLastError());
+  h->host_step += nsteps;
+}
+
+sfg_handle *make_handle(const sfg_options *opt) {
+  if (!opt) throw std::runtime_error("options are required");
+  if (!(opt->dt > 0) || opt->nstep <= 0) throw std::runtime_error("dt and nstep must be positive");
+  auto *h = new sfg_handle();
+  h->opt = *opt;
+  if (h->opt.nshots <= 0) h->opt.nshots = 1;
+  if (h->opt.nshots != 1) {
+    delete h;
+    throw std::runtime_error("this build advances one shot per handle");
+  }
+  if (h->opt.nstep_between_samples <= 0) h->opt.nstep_between_samples = 1;
+  if (h->opt.steps_per_graph <= 0) h->opt.steps_per_graph = 20;
+  h->epb = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 32 ? h->opt.elements_per_block : 16;
+  return h;
+}
+
+void finish_create(sfg_handle *h) {
+  h->mesh.elastic_wave = h->mesh.elastic_wave ? 1 : 0;
+  h->asmb.nshots = h->opt.nshots;
+  h->asmb.nstep = h->opt.nstep;
+  h->asmb.nsb = h->opt.nstep_between_samples;
+  sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfg_create2d(const sfg_mesh2d_desc *d, const sfg_options *opt, sfg_handle **out) {
+  if (!d || !out) { g_create_error = "null argument"; return SFG_ERR_ARG; }
+  *out = nullptr;
+  sfg_handle *h = nullptr;
+  try {
+    h = make_handle(opt);
+    sfg::Mesh2D &m = h->mesh;
+    if (d->nspec <= 0 || d->npgeo <= 0 || (d->ngnod != 4 && d->ngnod != 9) || d->numat <= 0 ||
+        !d->coorg || !d->knods || !d->kmato || !d->mat_medium || !d->mat_rho || !d->mat_vp || !d->mat_vs)
+      throw std::runtime_error("incomplete mesh description");
+    m.nspec = d->nspec; m.npgeo = d->npgeo; m.ngnod = d->ngnod; m.numat = d->numat;
+    m.coorg.assign(d->coorg, d->coorg + 2 * size_t(d->npgeo));
+    m.knods.assign(d->knods, d->knods + size_t(d->nspec) * d->ngnod);
+    m.kmato.assign(d->kmato, d->kmato + d->nspec);
+    for (int k : m.knods)
+      if (k < 0 || k >= m.npgeo) throw std::runtime_error("knods out of range");
+    for (int k : m.kmato)
+      if (k < 0 || k >= m.numat) throw std::runtime_error("kmato out of range");
+    m.mat_medium.assign(d->mat_medium, d->mat_medium + d->numat);
+    m.mat_rho.assign(d->mat_rho, d->mat_rho + d->numat);
+    m.mat_vp.assign(d->mat_vp, d->mat_vp + d->numat);
+    m.mat_vs.assign(d->mat_vs, d->mat_vs + d->numat);
+    const size_t np = size_t(d->nspec) * sfg::NPTS;
+    if (d->point_rho) m.prho.assign(d->point_rho, d->point_rho + np);
+    if (d->point_vp) m.pvp.assign(d->point_vp, d->point_vp + np);
+    if (d->point_vs) m.pvs.assign(d->point_vs, d->point_vs + np);
+    if (d->nabs > 0) {
+      m.abs_ispec.assign(d->abs_ispec, d->abs_ispec + d->nabs);
+      m.abs_type.assign(d->abs_type, d->abs_type + d->nabs);
+    }
+    if (d->nfree > 0) {
+      m.free_ispec.assign(d->free_ispec, d->free_ispec + d->nfree);
+      m.free_type.assign(d->free_type, d->free_type + d->nfree);
+    }
+    for (size_t i = 0; i < m.abs_ispec.size(); ++i)
+      if (m.abs_ispec[i] < 0 || m.abs_ispec[i] >= m.nspec || m.abs_type[i] < 0 || m.abs_type[i] > 3)
+        throw std::runtime_error("absorbing edge out of range");
+    for (size_t i = 0; i < m.free_ispec.size(); ++i)
+      if (m.free_ispec[i] < 0 || m.free_ispec[i] >= m.nspec || m.free_type[i] < 0 || m.free_type[i] > 3)
+        throw std::runtime_error("free-surface edge out of range");
+    m.elastic_wave = d->elastic_wave;
+    finish_create(h);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    delete h;
+    return SFG_ERR_ARG;
+  }
+  *out = h;
+  return SFG_OK;
+}
+
+int sfg_create2d_from_database(const char *path, int elastic_wave, const sfg_options *opt,
+                               sfg_handle **out) {
+  if (!path || !out) { g_create_error = "null argument"; return SFG_ERR_ARG; }
+  *out = nullptr;
+  sfg_handle *h = nullptr;
+  try {
+    h = make_handle(opt);
+    std::string err;
+    if (!sfg::read_database2d(path, h->mesh, err)) {
+      g_create_error = err;
+      delete h;
+      return SFG_ERR_IO;
+    }
+    h->mesh.elastic_wave = elastic_wave;
+    finish_create(h);
+  } catch (const std::exception &ex) {
+    g_create_error = ex.what();
+    delete h;
+    return SFG_ERR_ARG;
+  }
+  *out = h;
+  return SFG_OK;
+}
+
+void sfg_destroy(sfg_handle *h) { delete h; }
+
+const char *sfg_last_error(const sfg_handle *h) {
+  return h ? h->err.c_str() : g_create_error.c_str();
+}
+
+int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
+  return guarded(h, [&]() {
+    if (h->initialized) { h->err = "sources must be set before sfg_initialize"; return int(SFG_ERR_STATE); }
+    if (nsrc < 0 || (nsrc > 0 && !src)) { h->err = "bad source array"; return int(SFG_ERR_ARG); }
+    h->sources.clear();
+    for (int i = 0; i < nsrc; ++i)
+      h->sources.push_back({src[i].x, src[i].z, src[i].shot, src[i].stf, src[i].f0, src[i].factor,
+                            src[i].tshift, src[i].angle});
+    try {
+      sfg::set_sources2d(h->mesh, h->asmb, h->sources);
+    } catch (const std::exception &ex) {
+      h->err = ex.what();
+      return int(SFG_ERR_LOCATE);
+    }
+    h->have_sources = true;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_set_stf_table(sfg_handle *h, const float *table, int nstep, int nsrc) {
+  return guarded(h, [&]() {
+    if (!h->have_sources || nsrc != h->asmb.nsrc || nstep != h->asmb.nstep || !table) {
+      h->err = "STF table must match [nstep][nsrc] of the sources already set";
+      return int(SFG_ERR_ARG);
+    }
+    for (int i = 0; i < nstep; ++i)
+      for (int s = 0; s < nsrc; ++s) {
+        const float v = table[size_t(i) * nsrc + s];
+        h->asmb.stf[size_t(i) * nsrc + s] = h->asmb.src_medium[s] == 0 ? -v : v;
+      }
+    return int(SFG_OK);
+  });
+}
+
+int sfg_set_receivers(sfg_handle *h, int nrec, const double *x, const double *z, double angle,
+                      int ntypes, const int *types) {
+  return guarded(h, [&]() {
+    if (h->initialized) { h->err = "receivers must be set before sfg_initialize"; return int(SFG_ERR_STATE); }
+    if (nrec < 0 || (nrec > 0 && (!x || !z)) || ntypes < 1 || ntypes > 4 || !types) {
+      h->err = "bad receiver arguments";
+      return int(SFG_ERR_ARG);
+    }
+    for (int t = 0; t < ntypes; ++t)
+      if (types[t] < 0 || types[t] > 3) { h->err = "unknown seismogram type"; return int(SFG_ERR_ARG); }
+    h->rec_x.assign(x, x + nrec);
+    h->rec_z.assign(z, z + nrec);
+    try {
+      sfg::set_receivers2d(h->mesh, h->asmb, h->rec_x, h->rec_z, angle, std::vector<int>(types, types + ntypes));
+    } catch (const std::exception &ex) {
+      h->err = ex.what();
+      return int(SFG_ERR_LOCATE);
+    }
+    h->have_receivers = true;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_initialize(sfg_handle *h) {
+  return guarded(h, [&]() {
+    if (h->initialized) return int(SFG_OK);
+    sfg::Assembly2D &a = h->asmb;
+    if (!h->have_sources) sfg::set_sources2d(h->mesh, a, {});
+    if (!h->have_receivers) { a.nrec = 0; a.ntypes = 1; a.types = {0}; }
+    a.nsig = (a.nstep + a.nsb - 1) / a.nsb;
+    SFG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    SFG_CUDA(cudaEventCreate(&h->ev0));
+    SFG_CUDA(cudaEventCreate(&h->ev1));
+    for (int i = 0; i < sfg::NPTS; ++i) { h->quad.hp[i] = a.hprime[i]; h->quad.hpw[i] = a.hpw[i]; }
+    for (int i = 0; i < sfg::NGLL; ++i) h->quad.w[i] = a.wgll[i];
+    upload_medium(h, a.el, h->el);
+    upload_medium(h, a.ac, h->ac);
+    if (h->el.nspec) h->el.src_head = h->mem.upload(a.el_src_head);
+    if (h->ac.nspec) h->ac.src_head = h->mem.upload(a.ac_src_head);
+    h->d_src_next = h->mem.upload(a.src_next);
+    h->d_src_arr = h->mem.upload(a.src_arr);
+    h->d_stf = h->mem.upload(a.stf);
+    h->d_rec_elem = h->mem.upload(a.rec_elem);
+    h->d_rec_h = h->mem.upload(a.rec_h);
+    std::vector<int> rl_el, rl_ac;
+    for (int r = 0; r < a.nrec; ++r) (a.rec_medium[r] == 1 ? rl_el : rl_ac).push_back(r);
+    h->el.rec_list = h->mem.upload(rl_el);
+    h->el.nrec = int(rl_el.size());
+    h->ac.rec_list = h->mem.upload(rl_ac);
+    h->ac.nrec = int(rl_ac.size());
+    h->d_seis = h->mem.zeros<float>(size_t(a.nshots) * a.nsig * a.ntypes * std::max(a.nrec, 1) * 2);
+    h->d_step = h->mem.zeros<int>(1);
+    h->d_flag = h->mem.zeros<int>(1);
+    SFG_CUDA(cudaDeviceSynchronize());
+    h->graph_steps = std::max(1, h->opt.steps_per_graph);
+    h->graph_k = capture(h, h->graph_steps);
+    h->graph_1 = capture(h, 1);
+    h->initialized = true;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_step(sfg_handle *h) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    enqueue_step(h, h->stream);
+    SFG_CUDA(cudaGetLastError());
+    ++h->host_step;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_run(sfg_handle *h, int nsteps) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (nsteps < 0) return int(SFG_ERR_ARG);
+    run_steps(h, nsteps);
+    return int(SFG_OK);
+  });
+}
+
+int sfg_synchronize(sfg_handle *h) {
+  return guarded(h, [&]() {
+    if (h->stream) SFG_CUDA(cudaStreamSynchronize(h->stream));
+    return int(SFG_OK);
+  });
+}
+
+int sfg_reset_fields(sfg_handle *h) {
+  return guarded(h, [&]() {
+    if (!h->initialized) return int(SFG_ERR_STATE);
+    for (DevMedium *D : {&h->el, &h->ac}) {
+      if (!D->nspec) continue;
+      const size_t n = (size_t(D->nglob) * D->ncomp + 4) * sizeof(float);
+      SFG_CUDA(cudaMemsetAsync(D->u, 0, n, h->stream));
+      SFG_CUDA(cudaMemsetAsync(D->v, 0, n, h->stream));
+      SFG_CUDA(cudaMemsetAsync(D->accum, 0, n, h->stream));
+      SFG_CUDA(cudaMemsetAsync(D->a, 0, n, h->stream));
+    }
+    const sfg::Assembly2D &a = h->asmb;
+    SFG_CUDA(cudaMemsetAsync(h->d_seis, 0,
+                             size_t(a.nshots) * a.nsig * a.ntypes * std::max(a.nrec, 1) * 2 * sizeof(float),
+                             h->stream));
+    SFG_CUDA(cudaMemsetAsync(h->d_step, 0, sizeof(int), h->stream));
+    SFG_CUDA(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    SFG_CUDA(cudaStreamSynchronize(h->stream));
+    h->host_step = 0;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_run_timed(sfg_handle *h, int nsteps, float *ms) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    run_steps(h, nsteps);
+    SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+    SFG_CUDA(cudaEventSynchronize(h->ev1));
+    float t = 0;
+    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    if (ms) *ms = t;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *ms) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (nsteps < 0) return int(SFG_ERR_ARG);
+    if (flush_bytes > h->flush_bytes) {
+      if (h->flush_buf) cudaFree(h->flush_buf);
+      h->flush_buf = nullptr;
+      h->flush_bytes = 0;
+      SFG_CUDA(cudaMalloc(&h->flush_buf, flush_bytes));
+      h->flush_bytes = flush_bytes;
+    }
+    const int batch = 256;
+    std::vector<cudaEvent_t> ev(2 * batch);
+    for (auto &e : ev) SFG_CUDA(cudaEventCreate(&e));
+    double total = 0.0;
+    int done = 0;
+    try {
+      while (done < nsteps) {
+        const int n = std::min(batch, nsteps - done);
+        for (int i = 0; i < n; ++i) {
+          if (flush_bytes) SFG_CUDA(cudaMemsetAsync(h->flush_buf, i & 0xff, flush_bytes, h->stream));
+          SFG_CUDA(cudaEventRecord(ev[2 * i], h->stream));
+          SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+          SFG_CUDA(cudaEventRecord(ev[2 * i + 1], h->stream));
+        }
+        SFG_CUDA(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < n; ++i) {
+          float t = 0;
+          SFG_CUDA(cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]));
+          total += t;
+        }
+        done += n;
+        h->host_step += n;
+      }
+    } catch (...) {
+      for (auto &e : ev) cudaEventDestroy(e);
+      throw;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    if (ms) *ms = float(total);
+    return int(SFG_OK);
+  });
+}
+
+int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    const sfg::Assembly2D &a = h->asmb;
+    const int step = h->host_step;
+    if (stf_row && a.nsrc > 0 && step < a.nstep) {
+      // the table stores the acoustic (pressure) sign convention already applied
+      thread_local std::vector<float> row;
+      row.assign(stf_row, stf_row + a.nsrc);
+      for (int s = 0; s < a.nsrc; ++s)
+        if (a.src_medium[s] == 0) row[s] = -row[s];
+      SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, row.data(), a.nsrc * sizeof(float),
+                               cudaMemcpyHostToDevice, h->stream));
+    }
+    SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+    ++h->host_step;
+    if (seis_row && a.nrec > 0 && step % a.nsb == 0 && step / a.nsb < a.nsig) {
+      const size_t row = size_t(a.ntypes) * a.nrec * 2;
+      const int isig = step / a.nsb;
+      for (int s = 0; s < a.nshots; ++s)
+        SFG_CUDA(cudaMemcpyAsync(seis_row + s * row, h->d_seis + (size_t(s) * a.nsig + isig) * row,
+                                 row * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
+    }
+    SFG_CUDA(cudaStreamSynchronize(h->stream));
+    return int(SFG_OK);
+  });
+}
+
+int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (iters <= 0 || which < 0 || which > 3) return int(SFG_ERR_ARG);
+    const int medium = (which < 2) ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC;
+    DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    if (D.nspec == 0) { if (ms) *ms = 0; return int(SFG_OK); }
+    const bool stiff = (which % 2) == 0;
+    auto launch = [&]() {
+      if (stiff) launch_stiffness(h, medium, h->stream);
+      else launch_update(h, medium, false, h->stream);
+    };
+    for (int i = 0; i < 3; ++i) launch();
+    SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    for (int i = 0; i < iters; ++i) launch();
+    SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+    SFG_CUDA(cudaEventSynchronize(h->ev1));
+    SFG_CUDA(cudaGetLastError());
+    float t = 0;
+    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    if (ms) *ms = t / iters;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_get_info(const sfg_handle *h, sfg_info *info) {
+  if (!h || !info) return SFG_ERR_ARG;
+  const sfg::Assembly2D &a = h->asmb;
+  std::memset(info, 0, sizeof(*info));
+  info->nspec = a.nspec;
+  info->nspec_elastic = a.el.nspec;
+  info->nspec_acoustic = a.ac.nspec;
+  info->nglob = a.nglob;
+  info->nglob_elastic = a.el.nglob;
+  info->nglob_acoustic = a.ac.nglob;
+  info->ncolors_elastic = a.el.color_start.empty() ? 0 : int(a.el.color_start.size()) - 1;
+  info->ncolors_acoustic = a.ac.color_start.empty() ? 0 : int(a.ac.color_start.size()) - 1;
+  info->nshots = a.nshots;
+  info->nsig = a.nsig ? a.nsig : (a.nstep + a.nsb - 1) / a.nsb;
+  info->nrec = a.nrec;
+  info->ntypes = a.ntypes;
+  info->nstep = a.nstep;
+  info->istep = h->host_step;
+  info->t0 = a.t0;
+  info->device_bytes = h->mem.bytes;
+  info->kernels_per_step = h->initialized ? kernels_per_step(h) : 0;
+  return SFG_OK;
+}
+
+int sfg_get_seismograms(sfg_handle *h, float *out, size_t count) {
+  return guarded(h, [&]() {
+    if (!h->initialized) return int(SFG_ERR_STATE);
+    const sfg::Assembly2D &a = h->asmb;
+    const size_t n = size_t(a.nshots) * a.nsig * a.ntypes * a.nrec * 2;
+    if (count < n || !out) { h->err = "output buffer too small"; return int(SFG_ERR_ARG); }
+    if (n == 0) return int(SFG_OK);
+    std::vector<float> raw(n);
+    SFG_CUDA(cudaStreamSynchronize(h->stream));
+    SFG_CUDA(cudaMemcpy(raw.data(), h->d_seis, n * sizeof(float), cudaMemcpyDeviceToHost));
+    // receiver-angle rotation (seismogram_iterator.hpp:40-49)
+    const float ca = std::cos(float(M_PI) / 180.f * float(a.rec_angle));
+    const float sa = std::sin(float(M_PI) / 180.f * float(a.rec_angle));
+    for (size_t i = 0; i < n; i += 2) {
+      out[i] = ca * raw[i] - sa * raw[i + 1];
+      out[i + 1] = sa * raw[i] + ca * raw[i + 1];
+    }
+    return int(SFG_OK);
+  });
+}
+
+int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count) {
+  return guarded(h, [&]() {
+    if (!h->initialized) return int(SFG_ERR_STATE);
+    DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    const size_t n = size_t(D.nglob) * D.ncomp;
+    if (!out || count < n) { h->err = "output buffer too small"; return int(SFG_ERR_ARG); }
+    if (which == 2 && medium == SFG_MEDIUM_ELASTIC && !h->opt.store_acceleration) {
+      h->err = "elastic acceleration is kept only with sfg_options.store_acceleration";
+      return int(SFG_ERR_STATE);
+    }
+    const float *src = which == 0 ? D.u : which == 1 ? D.v : D.a;
+    if (n == 0) return int(SFG_OK);
+    SFG_CUDA(cudaStreamSynchronize(h->stream));
+    SFG_CUDA(cudaMemcpy(out, src, n * sizeof(float), cudaMemcpyDeviceToHost));
+    return int(SFG_OK);
+  });
+}
+
+int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *g2e, int *g2a) {
+  if (!h) return SFG_ERR_ARG;
+  const sfg::Assembly2D &a = h->asmb;
+  if (ibool_global) std::copy(a.ibool_global.begin(), a.ibool_global.end(), ibool_global);
+  if (g2e) std::copy(a.glob_to_el.begin(), a.glob_to_el.end(), g2e);
+  if (g2a) std::copy(a.glob_to_ac.begin(), a.glob_to_ac.end(), g2a);
+  return SFG_OK;
+}
+
+int sfg_check_finite(sfg_handle *h) {
+  if (!h || !h->initialized) return 0;
+  int f = 0;
+  if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SFG_ERR_CUDA;
+  if (cudaMemcpy(&f, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SFG_ERR_CUDA;
+  return f ? SFG_ERR_NONFINITE : 0;
+}
+
+}  // extern "C"

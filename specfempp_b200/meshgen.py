@@ -1,0 +1,286 @@
+"""Structured 2D meshes and the benchmark configurations.
+
+The reference builds its meshes with the Fortran mesher xmeshfem2D, which
+writes ``database.bin``.  This module is the stand-in for the structured
+(rectangular-grid) part of that mesher: it creates the same in-memory mesh
+(control nodes, 4-node elements, materials, absorbing and free-surface edge
+lists) and can write it as a ``database.bin`` with the record layout that
+``src/io/mesh/impl/fortran/dim2/*.cpp`` reads.
+
+It also defines the synthetic workloads used by the tests and the benchmark
+(all inputs seeded; no dataset is involved):
+
+* ``elastic_psv_80x60``    80x60 quads over 4000x3000 m, vp 2500, vs 1445,
+                           rho 2200, free top + Stacey on the other sides,
+                           Ricker 10 Hz force source, 5 receivers, dt 5e-4, 1600 steps;
+* ``coupled_400x200``      400x200 quads over 20x10 km: 1.5 km of water
+                           (vp 1500, rho 1020) over 4 elastic layers with seeded
+                           vp in [2500, 5000], vs = vp/1.73, rho = 1700 + 0.2 vp;
+                           pressure Ricker 5 Hz source in the water, 200
+                           receivers along the seafloor, dt 1e-3, 4000 steps;
+* ``elastic_grf_1000x500`` 1000x500 quads, vp = 3000 (1 + 0.1 GRF(500 m)).
+"""
+from __future__ import annotations
+
+import struct
+from dataclasses import dataclass, field
+
+import numpy as np
+
+BOTTOM, RIGHT, TOP, LEFT = 0, 1, 2, 3
+ACOUSTIC, ELASTIC = 0, 1
+
+
+@dataclass
+class Mesh:
+    nspec: int
+    npgeo: int
+    ngnod: int
+    coorg: np.ndarray
+    knods: np.ndarray
+    kmato: np.ndarray
+    mat_medium: np.ndarray
+    mat_rho: np.ndarray
+    mat_vp: np.ndarray
+    mat_vs: np.ndarray
+    abs_ispec: np.ndarray
+    abs_type: np.ndarray
+    free_ispec: np.ndarray
+    free_type: np.ndarray
+    coupled_pairs: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
+    nx: int = 0
+    nz: int = 0
+
+
+def structured_mesh(nx, nz, xmin, xmax, zmin, zmax, row_material, materials,
+                    absorbing=("bottom", "right", "left"), free_surface=("top",)) -> Mesh:
+    """Rectangular grid of nx*nz 4-node quads, element e = iz*nx + ix (bottom row first).
+
+    ``row_material``: [nz] material index per element row.
+    ``materials``: list of (medium, rho, vp, vs) with medium 0 acoustic, 1 elastic.
+    Absorbing edges are listed side by side (bottom, right, top, left), the
+    acoustic free surface on the sides named in ``free_surface`` (acoustic
+    elements only).
+    """
+    xs = np.linspace(xmin, xmax, nx + 1)
+    zs = np.linspace(zmin, zmax, nz + 1)
+    X, Z = np.meshgrid(xs, zs)
+    coorg = np.stack([X.ravel(), Z.ravel()], axis=1)
+    iz, ix = np.divmod(np.arange(nx * nz), nx)
+    n0 = iz * (nx + 1) + ix
+    knods = np.stack([n0, n0 + 1, n0 + nx + 2, n0 + nx + 1], axis=1).astype(np.int32)
+    row_material = np.asarray(row_material, np.int32)
+    kmato = row_material[iz].astype(np.int32)
+    med = np.asarray([m[0] for m in materials], np.int32)
+    abs_i, abs_t = [], []
+    sides = {"bottom": (iz == 0, BOTTOM), "right": (ix == nx - 1, RIGHT),
+             "top": (iz == nz - 1, TOP), "left": (ix == 0, LEFT)}
+    for name in ("bottom", "right", "top", "left"):
+        if name in absorbing:
+            mask, t = sides[name]
+            e = np.nonzero(mask)[0]
+            abs_i.append(e)
+            abs_t.append(np.full(len(e), t))
+    fr_i, fr_t = [], []
+    for name in free_surface:
+        mask, t = sides[name]
+        e = np.nonzero(mask & (med[kmato] == ACOUSTIC))[0]
+        fr_i.append(e)
+        fr_t.append(np.full(len(e), t))
+    cat = lambda l: np.concatenate(l).astype(np.int32) if l else np.zeros(0, np.int32)
+    # fluid-solid element pairs across horizontal interfaces
+    pairs = []
+    below = kmato.reshape(nz, nx)
+    for r in range(nz - 1):
+        a, b = med[below[r, 0]], med[below[r + 1, 0]]
+        if a != b:
+            for c in range(nx):
+                e1, e2 = r * nx + c, (r + 1) * nx + c
+                pairs.append((e1, e2) if a == ACOUSTIC else (e2, e1))
+    return Mesh(nspec=nx * nz, npgeo=(nx + 1) * (nz + 1), ngnod=4, coorg=coorg, knods=knods,
+                kmato=kmato, mat_medium=med,
+                mat_rho=np.asarray([m[1] for m in materials], np.float64),
+                mat_vp=np.asarray([m[2] for m in materials], np.float64),
+                mat_vs=np.asarray([m[3] for m in materials], np.float64),
+                abs_ispec=cat(abs_i), abs_type=cat(abs_t), free_ispec=cat(fr_i), free_type=cat(fr_t),
+                coupled_pairs=np.asarray(pairs, np.int32).reshape(-1, 2), nx=nx, nz=nz)
+
+
+# header record sizes of database.bin (read_mesh_database.cpp:12-158)
+_HEADER = [512, 8, 4, 8, 8, 4, 4, 4, 4, 4, 8, 8, 8, 8, 8, 4, 4, 4, 12, 8, 32, 8, 4, 16, 516,
+           512, 512, 512, 16, 4, 12, 4, 4, 8, 4, 4, 4, 4, 4, 4, 4, 16, 4, 4, 8, 4, 8, 4, 4, 4,
+           8, 4, 8, 4, 4, 8, 4, 4, 12, 4, 4, 4, 4, 8]
+
+
+def write_database(mesh: Mesh, path: str, title: str = "structured mesh") -> None:
+    """Write ``mesh`` as a SPECFEM2D database.bin (Fortran unformatted records)."""
+    out = bytearray()
+
+    def rec(payload: bytes):
+        out.extend(struct.pack("<i", len(payload)))
+        out.extend(payload)
+        out.extend(struct.pack("<i", len(payload)))
+
+    for k, n in enumerate(_HEADER):
+        if k == 0:
+            rec(title.encode().ljust(512, b" ")[:512])
+        elif k == 2:
+            rec(struct.pack("<i", mesh.nspec))
+        elif k == 3:
+            rec(struct.pack("<ii", mesh.npgeo, 1))
+        else:
+            rec(bytes(n))
+    for i in range(mesh.npgeo):
+        rec(struct.pack("<idd", i + 1, float(mesh.coorg[i, 0]), float(mesh.coorg[i, 1])))
+    rec(struct.pack("<iiiii", len(mesh.mat_rho), mesh.ngnod, mesh.nspec, 0, 0))
+    rec(struct.pack("<8i", len(mesh.abs_ispec), 0, len(mesh.free_ispec), len(mesh.coupled_pairs),
+                    0, 0, 0, 0))
+    rec(struct.pack("<idi", 1, 0.0, 0))
+    for m in range(len(mesh.mat_rho)):
+        vs = 0.0 if mesh.mat_medium[m] == ACOUSTIC else float(mesh.mat_vs[m])
+        rec(struct.pack("<ii13d", m + 1, 1, float(mesh.mat_rho[m]), float(mesh.mat_vp[m]), vs,
+                        0.0, 0.0, 9999.0, 9999.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0))
+    fmt = "<ii%dii" % mesh.ngnod
+    for e in range(mesh.nspec):
+        rec(struct.pack(fmt, e + 1, int(mesh.kmato[e]) + 1, *[int(k) + 1 for k in mesh.knods[e]], 0))
+    rec(struct.pack("<ii", 0, 0))
+    for e, t in zip(mesh.abs_ispec, mesh.abs_type):
+        codes = [int(t == BOTTOM), int(t == RIGHT), int(t == TOP), int(t == LEFT)]
+        rec(struct.pack("<i4ii8i", int(e) + 1, *codes, 0, *([0] * 8)))
+    corners = {BOTTOM: (0, 1), RIGHT: (1, 2), TOP: (2, 3), LEFT: (0, 3)}
+    for e, t in zip(mesh.free_ispec, mesh.free_type):
+        a, b = corners[int(t)]
+        rec(struct.pack("<4i", int(e) + 1, 2, int(mesh.knods[e, a]) + 1, int(mesh.knods[e, b]) + 1))
+    for ac, el in mesh.coupled_pairs:
+        rec(struct.pack("<ii", int(ac) + 1, int(el) + 1))
+    rec(struct.pack("<ii", 0, 0))
+    rec(struct.pack("<i", 0))
+    with open(path, "wb") as f:
+        f.write(bytes(out))
+
+
+# ------------------------------------------------------------------ configs ---
+
+@dataclass
+class Workload:
+    name: str
+    mesh: Mesh
+    sources: list
+    rec_x: np.ndarray
+    rec_z: np.ndarray
+    dt: float
+    nstep: int
+    point_rho: np.ndarray | None = None
+    point_vp: np.ndarray | None = None
+    point_vs: np.ndarray | None = None
+    description: str = ""
+
+
+@dataclass
+class RickerSource:
+    x: float
+    z: float
+    f0: float
+    factor: float
+    tshift: float = 0.0
+    angle: float = 0.0
+    stf: str = "ricker"
+    shot: int = 0
+
+
+def elastic_psv_80x60(nstep: int = 1600) -> Workload:
+    mesh = structured_mesh(80, 60, 0.0, 4000.0, 0.0, 3000.0, np.zeros(60, np.int32),
+                           [(ELASTIC, 2200.0, 2500.0, 1445.0)],
+                           absorbing=("bottom", "right", "left"), free_surface=())
+    rng = np.random.default_rng(0)
+    rx = np.sort(rng.uniform(500.0, 3500.0, 5))
+    rz = np.full(5, 2800.0)
+    src = [RickerSource(2000.0, 2500.0, 10.0, 1e10)]
+    return Workload("elastic_psv_80x60", mesh, src, rx, rz, 5e-4, nstep,
+                    description="2D elastic P-SV 80x60, NGLL=5, Stacey L/R/B, free top")
+
+
+def coupled_400x200(nstep: int = 4000, nx: int = 400, nz: int = 200, seed: int = 0) -> Workload:
+    """Water layer (top 1.5 km) over 4 seeded elastic layers, 20 x 10 km."""
+    rng = np.random.default_rng(seed)
+    vps = rng.uniform(2500.0, 5000.0, 4)
+    mats = [(ACOUSTIC, 1020.0, 1500.0, 0.0)]
+    for vp in vps:
+        mats.append((ELASTIC, 1700.0 + 0.2 * vp, vp, vp / 1.73))
+    depth = 10000.0
+    h = depth / nz
+    n_water = int(round(1500.0 / h))
+    n_el = nz - n_water
+    bounds = np.linspace(0, n_el, 5).round().astype(int)
+    row_mat = np.zeros(nz, np.int32)
+    for k in range(4):
+        # bottom-up rows: layer 4 (deepest) first
+        row_mat[bounds[k]:bounds[k + 1]] = 4 - k
+    row_mat[n_el:] = 0
+    mesh = structured_mesh(nx, nz, 0.0, 20000.0 * nx / 400, 0.0, depth, row_mat, mats,
+                           absorbing=("bottom", "right", "left"), free_surface=("top",))
+    seafloor = n_el * h
+    xmax = 20000.0 * nx / 400
+    rx = np.linspace(0.05 * xmax, 0.95 * xmax, 200)
+    rz = np.full(200, seafloor - 0.25 * h)
+    src = [RickerSource(0.5 * xmax, seafloor + 0.5 * (depth - seafloor), 5.0, 1e9)]
+    return Workload("coupled_400x200", mesh, src, rx, rz, 1e-3, nstep,
+                    description=f"2D coupled acoustic-elastic {nx}x{nz}, water 1.5 km, "
+                                f"elastic vp={np.round(vps, 1).tolist()}")
+
+
+def gaussian_random_field(shape, spacing, corr_len, rng) -> np.ndarray:
+    """Zero-mean unit-std field with a Gaussian covariance of correlation length corr_len."""
+    noise = rng.standard_normal(shape)
+    k = [np.fft.fftfreq(n, d=spacing) * 2 * np.pi for n in shape]
+    K2 = sum(np.meshgrid(*[kk ** 2 for kk in k], indexing="ij"))
+    filt = np.exp(-K2 * corr_len ** 2 / 8.0)
+    f = np.real(np.fft.ifftn(np.fft.fftn(noise) * filt))
+    return (f - f.mean()) / f.std()
+
+
+def grf_point_model(mesh: Mesh, xmax, zmax, base_vp, std, corr_len, seed, ngrid=None):
+    """Per-GLL-point vp = base (1 + std * GRF) sampled bilinearly at GLL points."""
+    rng = np.random.default_rng(seed)
+    ngrid = ngrid or (max(64, mesh.nz * 2), max(64, mesh.nx * 2))
+    dz, dx = zmax / (ngrid[0] - 1), xmax / (ngrid[1] - 1)
+    field_ = gaussian_random_field(ngrid, min(dx, dz), corr_len, rng)
+    gz, gx = gll_coordinates(mesh)
+    fz = np.clip(gz / dz, 0, ngrid[0] - 1.000001)
+    fx = np.clip(gx / dx, 0, ngrid[1] - 1.000001)
+    i0, j0 = fz.astype(int), fx.astype(int)
+    tz, tx = fz - i0, fx - j0
+    v = (field_[i0, j0] * (1 - tz) * (1 - tx) + field_[i0 + 1, j0] * tz * (1 - tx) +
+         field_[i0, j0 + 1] * (1 - tz) * tx + field_[i0 + 1, j0 + 1] * tz * tx)
+    return base_vp * (1.0 + std * v)
+
+
+def gll_coordinates(mesh: Mesh):
+    """(z, x) of every element GLL point [nspec, 25] for the bilinear 4-node mesh."""
+    r = np.sqrt(3.0 / 7.0)
+    z1 = np.array([-1.0, -r, 0.0, r, 1.0])
+    XI, GA = np.meshgrid(z1, z1)            # [iz, ix]
+    s = np.stack([0.25 * (XI - 1) * (GA - 1), -0.25 * (XI + 1) * (GA - 1),
+                  0.25 * (XI + 1) * (GA + 1), -0.25 * (XI - 1) * (GA + 1)], -1).reshape(25, 4)
+    cx = mesh.coorg[mesh.knods, 0]
+    cz = mesh.coorg[mesh.knods, 1]
+    return cz @ s.T, cx @ s.T
+
+
+def elastic_grf_1000x500(nstep: int = 3000, nshots: int = 32, nrec: int = 400,
+                         nx: int = 1000, nz: int = 500, seed: int = 0) -> Workload:
+    xmax, zmax = 25.0 * nx, 25.0 * nz
+    mesh = structured_mesh(nx, nz, 0.0, xmax, 0.0, zmax, np.zeros(nz, np.int32),
+                           [(ELASTIC, 2200.0, 3000.0, 3000.0 / np.sqrt(3.0))],
+                           absorbing=("bottom", "right", "left"), free_surface=())
+    vp = grf_point_model(mesh, xmax, zmax, 3000.0, 0.1, 500.0, seed)
+    vs = vp / np.sqrt(3.0)
+    rho = np.full_like(vp, 2200.0)
+    rng = np.random.default_rng(seed + 1)
+    srcs = [RickerSource(float(rng.uniform(0.1, 0.9) * xmax), float(rng.uniform(0.5, 0.9) * zmax),
+                         float(rng.uniform(4.0, 12.0)), 1e10, shot=s) for s in range(nshots)]
+    rx = np.linspace(0.02 * xmax, 0.98 * xmax, nrec)
+    rz = np.full(nrec, 0.95 * zmax)
+    return Workload("elastic_grf_1000x500", mesh, srcs, rx, rz, 5e-4, nstep, rho.astype(np.float32),
+                    vp.astype(np.float32), vs.astype(np.float32),
+                    description=f"2D elastic {nx}x{nz} GRF(10%, 500 m) on vp 3000, {nshots} shots")

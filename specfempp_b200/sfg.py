@@ -1,0 +1,290 @@
+"""ctypes binding of libsfg (``include/sfg.h``).
+
+This is the Python face of the drop-in boundary: it passes plain host arrays
+through the C ABI and gets seismograms and wavefields back as numpy arrays.
+The CUDA library must be built (``__graft_entry__.build()`` or
+``python -m specfempp_b200.build``); there is no fallback path — a missing
+library raises ``ImportError`` when a simulation is created.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsfg.so")
+
+SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC = 0, 1
+SEIS = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3}
+STF = {"ricker": 0, "dirac": 1}
+FIELD = {"displacement": 0, "velocity": 1, "acceleration": 2}
+ERRORS = {0: "OK", -1: "SFG_ERR_ARG", -2: "SFG_ERR_IO", -3: "SFG_ERR_CUDA", -4: "SFG_ERR_LOCATE",
+          -5: "SFG_ERR_STATE", -6: "SFG_ERR_NONFINITE", -7: "SFG_ERR_UNSUPPORTED"}
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("nspec", C.c_int), ("npgeo", C.c_int), ("ngnod", C.c_int),
+        ("coorg", _dp), ("knods", _ip), ("kmato", _ip), ("numat", C.c_int),
+        ("mat_medium", _ip), ("mat_rho", _dp), ("mat_vp", _dp), ("mat_vs", _dp),
+        ("point_rho", _fp), ("point_vp", _fp), ("point_vs", _fp),
+        ("nabs", C.c_int), ("abs_ispec", _ip), ("abs_type", _ip),
+        ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
+        ("elastic_wave", C.c_int),
+    ]
+
+
+class Options(C.Structure):
+    _fields_ = [("dt", C.c_double), ("nstep", C.c_int), ("nshots", C.c_int),
+                ("nstep_between_samples", C.c_int), ("steps_per_graph", C.c_int),
+                ("elements_per_block", C.c_int), ("store_acceleration", C.c_int)]
+
+
+class Source2D(C.Structure):
+    _fields_ = [("x", C.c_double), ("z", C.c_double), ("shot", C.c_int), ("stf", C.c_int),
+                ("f0", C.c_double), ("factor", C.c_double), ("tshift", C.c_double),
+                ("angle", C.c_double)]
+
+
+class Info(C.Structure):
+    _fields_ = [("nspec", C.c_int), ("nspec_elastic", C.c_int), ("nspec_acoustic", C.c_int),
+                ("nglob", C.c_int), ("nglob_elastic", C.c_int), ("nglob_acoustic", C.c_int),
+                ("ncolors_elastic", C.c_int), ("ncolors_acoustic", C.c_int),
+                ("nshots", C.c_int), ("nsig", C.c_int), ("nrec", C.c_int), ("ntypes", C.c_int),
+                ("nstep", C.c_int), ("istep", C.c_int), ("t0", C.c_double),
+                ("device_bytes", C.c_size_t), ("kernels_per_step", C.c_int)]
+
+
+EXPORTS = {
+    "sfg_create2d": ([C.POINTER(MeshDesc), C.POINTER(Options), C.POINTER(C.c_void_p)], C.c_int),
+    "sfg_create2d_from_database": ([C.c_char_p, C.c_int, C.POINTER(Options), C.POINTER(C.c_void_p)], C.c_int),
+    "sfg_destroy": ([C.c_void_p], None),
+    "sfg_last_error": ([C.c_void_p], C.c_char_p),
+    "sfg_set_sources": ([C.c_void_p, C.c_int, C.POINTER(Source2D)], C.c_int),
+    "sfg_set_stf_table": ([C.c_void_p, _fp, C.c_int, C.c_int], C.c_int),
+    "sfg_set_receivers": ([C.c_void_p, C.c_int, _dp, _dp, C.c_double, C.c_int, _ip], C.c_int),
+    "sfg_initialize": ([C.c_void_p], C.c_int),
+    "sfg_step": ([C.c_void_p], C.c_int),
+    "sfg_run": ([C.c_void_p, C.c_int], C.c_int),
+    "sfg_synchronize": ([C.c_void_p], C.c_int),
+    "sfg_reset_fields": ([C.c_void_p], C.c_int),
+    "sfg_run_timed": ([C.c_void_p, C.c_int, _fp], C.c_int),
+    "sfg_run_timed_flushed": ([C.c_void_p, C.c_int, C.c_size_t, _fp], C.c_int),
+    "sfg_step_io": ([C.c_void_p, _fp, _fp], C.c_int),
+    "sfg_time_kernel": ([C.c_void_p, C.c_int, C.c_int, _fp], C.c_int),
+    "sfg_get_info": ([C.c_void_p, C.POINTER(Info)], C.c_int),
+    "sfg_get_seismograms": ([C.c_void_p, _fp, C.c_size_t], C.c_int),
+    "sfg_get_field": ([C.c_void_p, C.c_int, C.c_int, _fp, C.c_size_t], C.c_int),
+    "sfg_get_numbering": ([C.c_void_p, _ip, _ip, _ip], C.c_int),
+    "sfg_check_finite": ([C.c_void_p], C.c_int),
+}
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsfg.so and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise ImportError(f"libsfg is not built ({path}); run __graft_entry__.build()")
+    lib = C.CDLL(path)
+    for name, (args, res) in EXPORTS.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+class SfgError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+@dataclass
+class Source:
+    x: float
+    z: float
+    f0: float
+    factor: float
+    tshift: float = 0.0
+    angle: float = 0.0
+    stf: str = "ricker"
+    shot: int = 0
+
+
+def _arr(x, dtype):
+    return np.ascontiguousarray(x, dtype=dtype)
+
+
+class Simulation2D:
+    """One 2D forward simulation on the GPU (a libsfg handle).
+
+    ``mesh`` is any object with the attributes of ``sfg_mesh2d_desc``
+    (nspec, npgeo, ngnod, coorg, knods, kmato, mat_medium, mat_rho, mat_vp,
+    mat_vs, abs_ispec, abs_type, free_ispec, free_type), e.g. the meshes of
+    ``specfempp_b200.meshgen``; or pass ``database=`` to read a database.bin.
+    """
+
+    def __init__(self, mesh=None, *, database: str | None = None, dt: float, nstep: int,
+                 nstep_between_samples: int = 1, elastic_wave: str = "psv",
+                 point_rho=None, point_vp=None, point_vs=None, steps_per_graph: int = 0,
+                 elements_per_block: int = 0, store_acceleration: bool = False):
+        self.lib = load_library()
+        self._keep = []
+        opt = Options(dt=dt, nstep=nstep, nshots=1, nstep_between_samples=nstep_between_samples,
+                      steps_per_graph=steps_per_graph, elements_per_block=elements_per_block,
+                      store_acceleration=int(store_acceleration))
+        h = C.c_void_p()
+        wave = 1 if elastic_wave.lower() == "sh" else 0
+        if database is not None:
+            rc = self.lib.sfg_create2d_from_database(database.encode(), wave, C.byref(opt), C.byref(h))
+        else:
+            d = self._desc(mesh, wave, point_rho, point_vp, point_vs)
+            rc = self.lib.sfg_create2d(C.byref(d), C.byref(opt), C.byref(h))
+        if rc != 0:
+            raise SfgError(rc, self.lib.sfg_last_error(None).decode())
+        self.h = h
+        self.dt, self.nstep = dt, nstep
+
+    def _k(self, a):
+        self._keep.append(a)
+        return a
+
+    def _desc(self, m, wave, prho, pvp, pvs):
+        d = MeshDesc()
+        d.nspec, d.npgeo, d.ngnod = int(m.nspec), int(m.npgeo), int(m.ngnod)
+        d.coorg = self._k(_arr(m.coorg, np.float64)).ctypes.data_as(_dp)
+        d.knods = self._k(_arr(m.knods, np.int32)).ctypes.data_as(_ip)
+        d.kmato = self._k(_arr(m.kmato, np.int32)).ctypes.data_as(_ip)
+        d.numat = len(m.mat_rho)
+        d.mat_medium = self._k(_arr(m.mat_medium, np.int32)).ctypes.data_as(_ip)
+        d.mat_rho = self._k(_arr(m.mat_rho, np.float64)).ctypes.data_as(_dp)
+        d.mat_vp = self._k(_arr(m.mat_vp, np.float64)).ctypes.data_as(_dp)
+        d.mat_vs = self._k(_arr(m.mat_vs, np.float64)).ctypes.data_as(_dp)
+        for name, a in (("point_rho", prho), ("point_vp", pvp), ("point_vs", pvs)):
+            if a is not None:
+                setattr(d, name, self._k(_arr(a, np.float32)).ctypes.data_as(_fp))
+        d.nabs = len(m.abs_ispec)
+        d.abs_ispec = self._k(_arr(m.abs_ispec, np.int32)).ctypes.data_as(_ip)
+        d.abs_type = self._k(_arr(m.abs_type, np.int32)).ctypes.data_as(_ip)
+        d.nfree = len(m.free_ispec)
+        d.free_ispec = self._k(_arr(m.free_ispec, np.int32)).ctypes.data_as(_ip)
+        d.free_type = self._k(_arr(m.free_type, np.int32)).ctypes.data_as(_ip)
+        d.elastic_wave = wave
+        return d
+
+    def _check(self, rc):
+        if rc != 0:
+            raise SfgError(rc, self.lib.sfg_last_error(self.h).decode())
+
+    def set_sources(self, sources):
+        arr = (Source2D * len(sources))()
+        for i, s in enumerate(sources):
+            arr[i] = Source2D(x=s.x, z=s.z, shot=getattr(s, "shot", 0), stf=STF[getattr(s, "stf", "ricker")],
+                              f0=s.f0, factor=s.factor, tshift=getattr(s, "tshift", 0.0),
+                              angle=getattr(s, "angle", 0.0))
+        self._check(self.lib.sfg_set_sources(self.h, len(sources), arr))
+
+    def set_stf_table(self, table):
+        t = _arr(table, np.float32)
+        self._check(self.lib.sfg_set_stf_table(self.h, t.ctypes.data_as(_fp), t.shape[0], t.shape[1]))
+
+    def set_receivers(self, x, z, angle=0.0, types=("displacement",)):
+        x = _arr(x, np.float64)
+        z = _arr(z, np.float64)
+        ty = _arr([SEIS[t] for t in types], np.int32)
+        self._check(self.lib.sfg_set_receivers(self.h, len(x), x.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+                                               float(angle), len(ty), ty.ctypes.data_as(_ip)))
+
+    def initialize(self):
+        self._check(self.lib.sfg_initialize(self.h))
+
+    def step(self):
+        self._check(self.lib.sfg_step(self.h))
+
+    def run(self, nsteps):
+        self._check(self.lib.sfg_run(self.h, int(nsteps)))
+
+    def run_timed(self, nsteps) -> float:
+        ms = C.c_float()
+        self._check(self.lib.sfg_run_timed(self.h, int(nsteps), C.byref(ms)))
+        return ms.value
+
+    def run_timed_flushed(self, nsteps, flush_bytes=256 << 20) -> float:
+        ms = C.c_float()
+        self._check(self.lib.sfg_run_timed_flushed(self.h, int(nsteps), int(flush_bytes), C.byref(ms)))
+        return ms.value
+
+    def step_io(self, stf_row=None, seis_row=None):
+        """One step with host buffers (float32 numpy arrays, ideally pinned)."""
+        sp = stf_row.ctypes.data_as(_fp) if stf_row is not None else None
+        op = seis_row.ctypes.data_as(_fp) if seis_row is not None else None
+        self._check(self.lib.sfg_step_io(self.h, sp, op))
+
+    def time_kernel(self, which: int, iters: int) -> float:
+        ms = C.c_float()
+        self._check(self.lib.sfg_time_kernel(self.h, int(which), int(iters), C.byref(ms)))
+        return ms.value
+
+    def synchronize(self):
+        self._check(self.lib.sfg_synchronize(self.h))
+
+    def reset(self):
+        self._check(self.lib.sfg_reset_fields(self.h))
+
+    def info(self) -> Info:
+        inf = Info()
+        self._check(self.lib.sfg_get_info(self.h, C.byref(inf)))
+        return inf
+
+    def seismograms(self) -> np.ndarray:
+        """[nshots, nsig, ntypes, nrec, 2] float32."""
+        i = self.info()
+        out = np.zeros((i.nshots, i.nsig, i.ntypes, i.nrec, 2), np.float32)
+        self._check(self.lib.sfg_get_seismograms(self.h, out.ctypes.data_as(_fp), out.size))
+        return out
+
+    def field(self, medium: str, which: str = "displacement") -> np.ndarray:
+        i = self.info()
+        med = SFG_MEDIUM_ELASTIC if medium == "elastic" else SFG_MEDIUM_ACOUSTIC
+        n = i.nglob_elastic if med == SFG_MEDIUM_ELASTIC else i.nglob_acoustic
+        out = np.zeros(n * (2 if med == SFG_MEDIUM_ELASTIC else 1), np.float32)
+        self._check(self.lib.sfg_get_field(self.h, med, FIELD[which], out.ctypes.data_as(_fp), out.size))
+        return out.reshape(n, -1) if med == SFG_MEDIUM_ELASTIC else out
+
+    def numbering(self):
+        i = self.info()
+        ib = np.zeros(i.nspec * 25, np.int32)
+        g2e = np.zeros(i.nglob, np.int32)
+        g2a = np.zeros(i.nglob, np.int32)
+        self._check(self.lib.sfg_get_numbering(self.h, ib.ctypes.data_as(_ip), g2e.ctypes.data_as(_ip),
+                                               g2a.ctypes.data_as(_ip)))
+        return ib.reshape(i.nspec, 25), g2e, g2a
+
+    def check_finite(self) -> bool:
+        rc = self.lib.sfg_check_finite(self.h)
+        if rc not in (0, -6):
+            self._check(rc)
+        return rc == 0
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.sfg_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,102 @@
+"""Shared test helpers.
+
+Tests marked ``gpu`` need a CUDA device and the built libsfg.so; everything
+else runs on CPU (oracle against the golden fixtures, the host-side
+assembly and the C ABI's symbol table).
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, ROOT)
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device and libsfg.so")
+
+
+def golden_case(name, nstep=None):
+    """Rebuild an oracle Case2D (and golden traces) from tests/golden/<name>.npz."""
+    from oracle import runner
+    from oracle.database2d import Mesh2D
+
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    mesh = Mesh2D(nspec=int(z["nspec"]), npgeo=int(z["npgeo"]), ngnod=int(z["ngnod"]),
+                  coorg=z["coorg"], knods=z["knods"], kmato=z["kmato"],
+                  mat_medium=z["mat_medium"], mat_rho=z["mat_rho"], mat_vp=z["mat_vp"],
+                  mat_vs=z["mat_vs"], abs_ispec=z["abs_ispec"], abs_type=z["abs_type"],
+                  free_ispec=z["free_ispec"], free_type=z["free_type"],
+                  coupled_pairs=np.zeros((0, 2), np.int32))
+    srcs = [runner.Source(x=s[0], z=s[1], f0=s[2], factor=s[3], tshift=s[4], angle=s[5],
+                          stf="dirac" if s[6] else "ricker") for s in z["src"]]
+    case = runner.Case2D(mesh=mesh, sources=srcs, rec_x=z["rec_x"], rec_z=z["rec_z"],
+                         dt=float(z["dt"]), nstep=int(nstep or z["nstep"]),
+                         rec_angle=float(z["rec_angle"]))
+    return case, z["traces"], float(z["trace_t0"])
+
+
+def reference_metric(computed, traces):
+    """Per-station sum|d|/sum|ref| over components (newmark_tests.cpp:331-373).
+
+    computed: [nsig, nrec, ncomp]; traces: [nrec, ncomp, nsig]."""
+    n = min(computed.shape[0], traces.shape[2])
+    c = np.transpose(computed[:n], (1, 2, 0))
+    t = traces[:, :, :n]
+    return np.abs(c - t).sum(axis=(1, 2)) / np.abs(t).sum(axis=(1, 2))
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64)
+    b = np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def has_cuda():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+@pytest.fixture(scope="session")
+def oracle_lib():
+    from oracle import runner
+    runner.build()
+    return runner.lib()
+
+
+@pytest.fixture(scope="session")
+def sfg_lib():
+    from specfempp_b200 import build, sfg
+    build.build()
+    return sfg.load_library()
+
+
+def product_run(case, types=("displacement",), nsteps=None, epb=0, spg=0):
+    """Run the CUDA path (libsfg through the C ABI) on an oracle Case2D."""
+    from specfempp_b200 import sfg
+    sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=case.nstep,
+                           nstep_between_samples=case.nstep_between_samples,
+                           point_rho=case.point_rho, point_vp=case.point_vp, point_vs=case.point_vs,
+                           elements_per_block=epb, steps_per_graph=spg)
+    sim.set_sources(case.sources)
+    sim.set_receivers(case.rec_x, case.rec_z, case.rec_angle, types)
+    sim.initialize()
+    sim.run(case.nstep if nsteps is None else nsteps)
+    seis = sim.seismograms()[0]
+    return sim, seis
+
+
+def workload_case(w, nstep=None, types=("displacement",)):
+    """oracle Case2D of a meshgen Workload."""
+    from oracle import runner
+    return runner.Case2D(mesh=w.mesh, sources=w.sources, rec_x=w.rec_x, rec_z=w.rec_z, dt=w.dt,
+                         nstep=int(nstep or w.nstep), seis_types=list(types),
+                         point_rho=w.point_rho, point_vp=w.point_vp, point_vs=w.point_vs)

@@ -1,0 +1,62 @@
+"""Build the golden fixtures under tests/golden/ from the reference checkout.
+
+Each ``<fixture>.npz`` holds, for one of SPECFEM++'s Newmark regression
+fixtures (``tests/unit-tests/displacement_tests/Newmark/serial/dim2/<name>``):
+the mesh read from its ``database.bin`` (control nodes, connectivity,
+materials, absorbing / free-surface edges), its sources, its stations, dt,
+nstep and the golden displacement traces (``*.semd``, produced by Fortran
+SPECFEM2D), stored as float32.  The tests rebuild a Case2D from it, so they
+run without the reference tree.
+
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import runner  # noqa: E402
+
+FIXTURES = {
+    "HomogeneousElasticDomain": ("BXX", "BXZ"),
+    "HomogeneousElasticDomainStaceyDirichletBC": ("BXX", "BXZ"),
+    "HomogeneousElasticDomainStaceyBC": ("BXX", "BXZ"),
+    "HomogeneousAcousticDomainDirichletBC": ("BXX", "BXZ"),
+    "AcousticElasticCoupledDomainVariant2": ("BXX", "BXZ"),
+}
+
+
+def make(ref_root: str, name: str, comps) -> str:
+    d = os.path.join(ref_root, "tests/unit-tests/displacement_tests/Newmark/serial/dim2", name)
+    case = runner.load_fixture(d)
+    m = case.mesh
+    traces = np.zeros((len(case.stations), len(comps), case.nstep), np.float32)
+    t0 = None
+    for r, (net, sta) in enumerate(case.stations):
+        for c, comp in enumerate(comps):
+            t, v = runner.read_trace(os.path.join(d, "traces", f"{net}.{sta}.S2.{comp}.semd"))
+            traces[r, c, : len(v)] = v[: case.nstep]
+            t0 = t[0]
+    out = os.path.join(HERE, f"{name}.npz")
+    np.savez_compressed(
+        out, nspec=m.nspec, npgeo=m.npgeo, ngnod=m.ngnod, coorg=m.coorg, knods=m.knods,
+        kmato=m.kmato, mat_medium=m.mat_medium, mat_rho=m.mat_rho, mat_vp=m.mat_vp,
+        mat_vs=m.mat_vs, abs_ispec=m.abs_ispec, abs_type=m.abs_type, free_ispec=m.free_ispec,
+        free_type=m.free_type,
+        src=np.asarray([[s.x, s.z, s.f0, s.factor, s.tshift, s.angle, 1.0 if s.stf == "dirac" else 0.0]
+                        for s in case.sources]),
+        rec_x=case.rec_x, rec_z=case.rec_z, dt=case.dt, nstep=case.nstep, rec_angle=case.rec_angle,
+        stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces,
+        trace_t0=t0, components=np.asarray(comps))
+    return out
+
+
+if __name__ == "__main__":
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    for name, comps in FIXTURES.items():
+        print(make(root, name, comps), os.path.getsize(os.path.join(HERE, f"{name}.npz")))

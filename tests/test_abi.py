@@ -1,0 +1,98 @@
+"""C ABI and host-side assembly checks that need no GPU.
+
+* libsfg.so loads and exports every function declared in include/sfg.h;
+* the host assembly (numbering, colouring) agrees with the oracle's;
+* the database.bin written by meshgen reads back identically through the
+  C++ reader (libsfg) and the oracle's reader;
+* error behaviour: missing file, point outside the mesh, calls out of order.
+"""
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, golden_case
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "sfg.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(sfg_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(sfg_lib):
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for s in syms:
+        assert hasattr(sfg_lib, s), s
+    from specfempp_b200 import sfg
+    assert set(syms) == set(sfg.EXPORTS)
+
+
+def test_numbering_matches_oracle(sfg_lib, oracle_lib):
+    from oracle import runner
+    from specfempp_b200 import sfg
+    case, _, _ = golden_case("AcousticElasticCoupledDomainVariant2", nstep=10)
+    r = runner.run(case, "f64", nthreads=4, want_final=True)
+    sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=case.nstep)
+    ib_p, g2e, g2a = sim.numbering()
+    ib_o = r["final"]["ibool"]
+    assert sim.info().nglob == r["nglob"]
+    # same partition of local points into global points: a bijection between ids
+    pairs = np.unique(np.stack([ib_o.ravel(), ib_p.ravel()], 1), axis=0)
+    assert len(pairs) == r["nglob"]
+    inf = sim.info()
+    assert inf.nspec_elastic + inf.nspec_acoustic == case.mesh.nspec
+    assert inf.nglob_elastic == (g2e >= 0).sum() and inf.nglob_acoustic == (g2a >= 0).sum()
+    assert ((g2e >= 0) & (g2a >= 0)).sum() > 0              # interface points in both media
+
+
+def test_colouring_is_conflict_free(sfg_lib):
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.coupled_400x200(nstep=10, nx=40, nz=20)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep)
+    inf = sim.info()
+    assert inf.ncolors_elastic == 4 and inf.ncolors_acoustic == 4
+
+
+def test_database_roundtrip(tmp_path, sfg_lib):
+    from oracle.database2d import read_database
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.coupled_400x200(nstep=10, nx=40, nz=20)
+    p = str(tmp_path / "database.bin")
+    meshgen.write_database(w.mesh, p)
+    m = read_database(p)
+    assert m.nspec == w.mesh.nspec and m.npgeo == w.mesh.npgeo
+    assert np.array_equal(m.knods, w.mesh.knods) and np.allclose(m.coorg, w.mesh.coorg)
+    assert np.array_equal(m.abs_ispec, w.mesh.abs_ispec) and np.array_equal(m.abs_type, w.mesh.abs_type)
+    assert np.array_equal(m.free_ispec, w.mesh.free_ispec) and np.array_equal(m.free_type, w.mesh.free_type)
+    assert np.array_equal(m.mat_medium, w.mesh.mat_medium)
+    a = sfg.Simulation2D(database=p, dt=w.dt, nstep=10)
+    b = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=10)
+    ia, ib = a.info(), b.info()
+    assert (ia.nglob, ia.nglob_elastic, ia.nglob_acoustic) == (ib.nglob, ib.nglob_elastic, ib.nglob_acoustic)
+
+
+def test_error_paths(tmp_path, sfg_lib):
+    from specfempp_b200 import meshgen, sfg
+    with pytest.raises(sfg.SfgError) as e:
+        sfg.Simulation2D(database=str(tmp_path / "missing.bin"), dt=1e-3, nstep=10)
+    assert e.value.code == -2
+    bad = tmp_path / "trunc.bin"
+    w = meshgen.elastic_psv_80x60(10)
+    meshgen.write_database(w.mesh, str(bad))
+    data = open(bad, "rb").read()
+    open(bad, "wb").write(data[: len(data) // 2])
+    with pytest.raises(sfg.SfgError) as e:
+        sfg.Simulation2D(database=str(bad), dt=1e-3, nstep=10)
+    assert e.value.code == -2
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=10)
+    with pytest.raises(sfg.SfgError) as e:
+        sim.set_receivers([1e7], [1e7])
+    assert e.value.code == -4
+    with pytest.raises(sfg.SfgError) as e:
+        sim.run(1)
+    assert e.value.code == -5
+    with pytest.raises(sfg.SfgError):
+        sfg.Simulation2D(w.mesh, dt=-1.0, nstep=10)

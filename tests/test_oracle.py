@@ -1,0 +1,69 @@
+"""The CPU oracle against the reference's golden vectors (CPU only).
+
+Pins the oracle before it is used as the checker of the CUDA path:
+* end-to-end traces of SPECFEM++'s Newmark regression fixtures (produced by
+  Fortran SPECFEM2D), with the reference's own metric and tolerance 1e-3
+  (tests/unit-tests/displacement_tests/Newmark/dim2/newmark_tests.cpp:331-373);
+* known-answer tests from tests/unit-tests/gll/gll_tests.cpp and
+  tests/unit-tests/medium/stress/dim2/elastic_isotropic.cpp.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from conftest import golden_case, reference_metric
+
+FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
+            "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
+            "AcousticElasticCoupledDomainVariant2"]
+
+
+@pytest.mark.parametrize("name", FIXTURES)
+def test_oracle_matches_golden_traces(oracle_lib, name):
+    from oracle import runner
+    case, traces, t0 = golden_case(name)
+    r = runner.run(case, "f32", nthreads=8)
+    assert abs(r["t0"] - t0) < 1e-3                     # time axis alignment
+    err = reference_metric(r["seis"][:, 0], traces)
+    assert np.all(np.isfinite(err))
+    assert err.max() < 1e-3, err                          # the reference's tolerance
+    assert err.max() < 5e-4                               # observed margin: <= 2e-4
+
+
+def test_oracle_fp32_vs_fp64_small(oracle_lib):
+    from oracle import runner
+    case, _, _ = golden_case("HomogeneousElasticDomainStaceyDirichletBC", nstep=120)
+    a = runner.run(case, "f32", nthreads=4)["seis"]
+    b = runner.run(case, "f64", nthreads=4)["seis"]
+    rel = np.linalg.norm(a - b) / np.linalg.norm(b)
+    assert rel < 1e-4
+
+
+def test_gll_known_answers(oracle_lib):
+    L = oracle_lib
+    tol = 1e-6
+    for x, n, v in [(-1.0, 1, -1.0), (0.0, 1, 0.0), (1.0, 1, 1.0), (-1.0, 2, 1.0), (0.0, 2, -0.5),
+                    (1.0, 2, 1.0), (-1.0, 5, -1.0), (0.0, 5, 0.0), (1.0, 5, 1.0)]:
+        assert abs(L.oracle_legendre(x, n) - v) < tol
+    z = np.zeros(5)
+    w = np.zeros(5)
+    hp = np.zeros(25)
+    dp = C.POINTER(C.c_double)
+    L.oracle_gll(z.ctypes.data_as(dp), w.ctypes.data_as(dp), hp.ctypes.data_as(dp))
+    assert np.allclose(z, [-1, -np.sqrt(3 / 7), 0, np.sqrt(3 / 7), 1])
+    assert np.allclose(w, [0.1, 49 / 90, 32 / 45, 49 / 90, 0.1])
+    hp = hp.reshape(5, 5)
+    assert np.allclose(hp.sum(axis=1), 0.0, atol=1e-12)    # derivative of a constant
+    assert np.allclose(hp @ z, 1.0)                         # derivative of x
+    assert np.allclose(hp @ z ** 4, 4 * z ** 3)             # exact up to degree 4
+
+
+def test_stress_known_answer(oracle_lib):
+    kappa, mu = 2.0, 3.0
+    du = np.array([1.0, 3.0, 4.0, 2.0])                    # du(0,0), du(0,1), du(1,0), du(1,1)
+    out = np.zeros(4)
+    dp = C.POINTER(C.c_double)
+    oracle_lib.oracle_stress_psv(kappa, mu, du.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    lam = kappa + 4.0 / 3.0 * mu - 2 * mu
+    assert np.allclose(out, [(lam + 2 * mu) * 1 + lam * 2, mu * 7, mu * 7, (lam + 2 * mu) * 2 + lam * 1])
