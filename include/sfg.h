@@ -84,7 +84,7 @@ typedef struct sfg_options {
   int nstep_between_samples;     /* seismogram sampling (>= 1) */
   int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
   int elements_per_block;        /* stiffness launch shape (0 = autotuned default) */
-  int store_acceleration;        /* keep the elastic acceleration for read-back */
+  int store_acceleration;        /* also keep the elastic acceleration inside runs */
 } sfg_options;
 
 typedef struct sfg_source2d {
@@ -123,7 +123,9 @@ int sfg_set_receivers(sfg_handle *h, int nrec, const double *x, const double *z,
 int sfg_initialize(sfg_handle *h);
 
 /* ---- time stepping ---- */
-int sfg_step(sfg_handle *h);                        /* one step, no graph */
+/* After sfg_step and sfg_run the fields hold the reference's end-of-step
+ * state (displacement after the predictor, velocity after the corrector). */
+int sfg_step(sfg_handle *h);                        /* one step */
 int sfg_run(sfg_handle *h, int nsteps);             /* nsteps steps via CUDA graphs */
 int sfg_synchronize(sfg_handle *h);
 int sfg_reset_fields(sfg_handle *h);                /* zero wavefields, istep = 0 */
@@ -142,8 +144,9 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
  * that streams sources in and traces out would call. */
 int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
 /* Average device time of one launch of a named kernel family, timed alone with
- * CUDA events: which = 0 elastic stiffness (all colours of one step),
- * 1 elastic Newmark update, 2 acoustic stiffness, 3 acoustic update. */
+ * CUDA events: which = 0 element (stiffness) launches of one step, all colours
+ * and both media; 1 elastic point update; 2 acoustic point update;
+ * 3 receiver kernels.  Leaves the fields mid-step (sfg_reset_fields after). */
 int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms_per_launch);
 
 /* ---- results ---- */

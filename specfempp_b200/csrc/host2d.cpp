@@ -338,7 +338,7 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
         a.gz[p] = J[p].z;
       }
 
-  // --- media, colouring and compute order --------------------------
+  // --- media and colouring ------------------------------------------
   a.mesh_medium.resize(nspec);
   for (int e = 0; e < nspec; ++e) a.mesh_medium[e] = m.mat_medium[m.kmato[e]];
   a.mesh_to_compute.assign(nspec, -1);
@@ -356,8 +356,86 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       for (int q = 0; q < NPTS; ++q) used[gid[size_t(e) * NPTS + q]] |= 1u << c;
     }
   }
-  const double rho_default = 0;
-  (void)rho_default;
+
+  // --- Stacey and free-surface point data (mesh order) ----------------
+  // Absorbing entries are applied in database order; on a corner shared by
+  // two absorbing edges of one element the later entry's normal and weight
+  // win (core/specfem/assembly/boundaries/dim2/impl/stacey.tpp).
+  struct BcPt { double w = 0, nx = 0, nz = 0; bool st = false, fs = false; };
+  std::unordered_map<int, std::vector<BcPt>> bc;  // mesh element -> 25 points
+  for (size_t i = 0; i < m.abs_ispec.size(); ++i) {
+    const int e = m.abs_ispec[i], t = m.abs_type[i];
+    auto &v = bc[e];
+    v.resize(NPTS);
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix) {
+        if (!on_edge(t, iz, ix)) continue;
+        BcPt &b = v[iz * NGLL + ix];
+        b.st = true;
+        edge_normal(J[size_t(e) * NPTS + iz * NGLL + ix], t, b.nx, b.nz);
+        b.w = (t == LEFT || t == RIGHT) ? w[iz] : w[ix];
+      }
+  }
+  for (size_t i = 0; i < m.free_ispec.size(); ++i) {
+    const int e = m.free_ispec[i], t = m.free_type[i];
+    if (a.mesh_medium[e] != 0) continue;      // free surface acts on acoustic media
+    auto &v = bc[e];
+    v.resize(NPTS);
+    for (int iz = 0; iz < NGLL; ++iz)
+      for (int ix = 0; ix < NGLL; ++ix)
+        if (on_edge(t, iz, ix)) v[iz * NGLL + ix].fs = true;
+  }
+
+  // --- acoustic/elastic coupling -------------------------------------
+  // Each element pair sharing an edge across media contributes, on the self
+  // side, GLL weight * outward normal of the self element at the edge points
+  // (core/specfem/assembly/conforming_interfaces/dim2/impl/interface_container.tpp);
+  // the contribution of an acoustic point on the free surface is dropped
+  // (compute_coupling.tpp:101-106).  The term is linear in the other medium's
+  // field at the same global point, so the edge contributions of a point are
+  // summed once here and applied per point in the update kernels.
+  std::vector<double> cpl[2];                 // [medium][glob][2]
+  std::vector<uint8_t> is_iface[2];
+  cpl[0].assign(2 * size_t(a.nglob), 0.0); cpl[1].assign(2 * size_t(a.nglob), 0.0);
+  is_iface[0].assign(a.nglob, 0); is_iface[1].assign(a.nglob, 0);
+  {
+    std::unordered_map<uint64_t, std::vector<std::pair<int, int>>> edges;
+    const int ends[4][2] = {{0, 1}, {1, 2}, {3, 2}, {0, 3}};
+    for (int e = 0; e < nspec; ++e) {
+      const int *kn = &m.knods[size_t(e) * m.ngnod];
+      for (int t = 0; t < 4; ++t) {
+        uint64_t na = kn[ends[t][0]], nb = kn[ends[t][1]];
+        edges[std::min(na, nb) * npg + std::max(na, nb)].push_back({e, t});
+      }
+    }
+    std::vector<std::pair<uint64_t, std::vector<std::pair<int, int>>>> sorted(edges.begin(), edges.end());
+    std::sort(sorted.begin(), sorted.end(), [](const auto &x, const auto &y) { return x.first < y.first; });
+    for (auto &kv : sorted) {
+      if (kv.second.size() != 2) continue;
+      const auto [e1, t1] = kv.second[0];
+      const auto [e2, t2] = kv.second[1];
+      if (a.mesh_medium[e1] == a.mesh_medium[e2]) continue;
+      for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
+        const int med = a.mesh_medium[e];
+        const auto it = bc.find(e);
+        for (int iz = 0; iz < NGLL; ++iz)
+          for (int ix = 0; ix < NGLL; ++ix) {
+            if (!on_edge(t, iz, ix)) continue;
+            const int q = iz * NGLL + ix;
+            const int g = gid[size_t(e) * NPTS + q];
+            is_iface[med][g] = 1;
+            if (it != bc.end() && it->second[q].fs) continue;
+            double nx, nz;
+            edge_normal(J[size_t(e) * NPTS + q], t, nx, nz);
+            const double f = (t == BOTTOM || t == TOP) ? w[ix] : w[iz];
+            cpl[med][2 * size_t(g)] += f * nx;
+            cpl[med][2 * size_t(g) + 1] += f * nz;
+          }
+      }
+    }
+  }
+
+  // --- compute order, per-medium numbering, element arrays -----------
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
     D.ncomp = med == 1 ? (m.elastic_wave == 1 ? 1 : 2) : 1;
@@ -374,17 +452,26 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       D.color_start.push_back(int(D.elem_mesh.size()));
     }
     D.nspec = int(D.elem_mesh.size());
-    // per-medium point numbering by first touch in compute order
+    // per-medium point numbering: coupled-interface points first, then the
+    // others, each by first touch in compute order (locality of the gathers)
     std::vector<int> &g2m = med == 1 ? a.glob_to_el : a.glob_to_ac;
     g2m.assign(a.nglob, -1);
     D.ibool.resize(size_t(D.nspec) * NPTS);
+    for (int pass = 0; pass < 2; ++pass)
+      for (int ce = 0; ce < D.nspec; ++ce) {
+        const int e = D.elem_mesh[ce];
+        for (int q = 0; q < NPTS; ++q) {
+          const int g = gid[size_t(e) * NPTS + q];
+          if (g2m[g] >= 0 || (pass == 0) != bool(is_iface[med][g])) continue;
+          g2m[g] = D.nglob++;
+          D.glob_of_point.push_back(g);
+        }
+        if (pass == 0 && ce == D.nspec - 1) D.niface = D.nglob;
+      }
+    if (D.nspec == 0) D.niface = 0;
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
-      for (int q = 0; q < NPTS; ++q) {
-        const int g = gid[size_t(e) * NPTS + q];
-        if (g2m[g] < 0) { g2m[g] = D.nglob++; D.glob_of_point.push_back(g); }
-        D.ibool[size_t(ce) * NPTS + q] = g2m[g];
-      }
+      for (int q = 0; q < NPTS; ++q) D.ibool[size_t(ce) * NPTS + q] = g2m[gid[size_t(e) * NPTS + q]];
     }
     const size_t n = size_t(D.nspec) * NPTS;
     D.xix.resize(n); D.xiz.resize(n); D.gax.resize(n); D.gaz.resize(n); D.jac.resize(n);
@@ -414,35 +501,21 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       }
     }
   }
+  // per-point coupling coefficients of the interface points of each medium
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    const std::vector<int> &other = med == 1 ? a.glob_to_ac : a.glob_to_el;
+    D.cp_nx.assign(D.niface, 0.f); D.cp_nz.assign(D.niface, 0.f); D.cp_other.assign(D.niface, -1);
+    for (int i = 0; i < D.niface; ++i) {
+      const int g = D.glob_of_point[i];
+      D.cp_nx[i] = float(cpl[med][2 * size_t(g)]);
+      D.cp_nz[i] = float(cpl[med][2 * size_t(g) + 1]);
+      D.cp_other[i] = other[g];
+      if (D.cp_other[i] < 0) throw std::runtime_error("coupled point missing in the other medium");
+    }
+  }
 
-  // --- Stacey and free-surface point data --------------------------
-  // Absorbing entries are applied in database order; on a corner shared by
-  // two absorbing edges of one element the later entry's normal and weight
-  // win (core/specfem/assembly/boundaries/dim2/impl/stacey.tpp).
-  struct BcPt { double w = 0, nx = 0, nz = 0; bool st = false, fs = false; };
-  std::unordered_map<int, std::vector<BcPt>> bc;  // mesh element -> 25 points
-  for (size_t i = 0; i < m.abs_ispec.size(); ++i) {
-    const int e = m.abs_ispec[i], t = m.abs_type[i];
-    auto &v = bc[e];
-    v.resize(NPTS);
-    for (int iz = 0; iz < NGLL; ++iz)
-      for (int ix = 0; ix < NGLL; ++ix) {
-        if (!on_edge(t, iz, ix)) continue;
-        BcPt &b = v[iz * NGLL + ix];
-        b.st = true;
-        edge_normal(J[size_t(e) * NPTS + iz * NGLL + ix], t, b.nx, b.nz);
-        b.w = (t == LEFT || t == RIGHT) ? w[iz] : w[ix];
-      }
-  }
-  for (size_t i = 0; i < m.free_ispec.size(); ++i) {
-    const int e = m.free_ispec[i], t = m.free_type[i];
-    if (a.mesh_medium[e] != 0) continue;      // free surface acts on acoustic media
-    auto &v = bc[e];
-    v.resize(NPTS);
-    for (int iz = 0; iz < NGLL; ++iz)
-      for (int ix = 0; ix < NGLL; ++ix)
-        if (on_edge(t, iz, ix)) v[iz * NGLL + ix].fs = true;
-  }
+  // --- Stacey / free-surface arrays in compute order -----------------
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
     D.bc_slot.assign(D.nspec, -1);
@@ -478,68 +551,6 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
           }
         }
         if (v[q].fs) D.bc_keep[k] = 0.0f;
-      }
-    }
-  }
-
-  // --- acoustic/elastic coupling edges -----------------------------
-  // each element pair sharing an edge across media contributes, on the self
-  // side, weight * outward normal of the self element at the edge points
-  // (core/specfem/assembly/conforming_interfaces/dim2/impl/interface_container.tpp)
-  {
-    std::unordered_map<uint64_t, std::vector<std::pair<int, int>>> edges;
-    const int ends[4][2] = {{0, 1}, {1, 2}, {3, 2}, {0, 3}};
-    for (int e = 0; e < nspec; ++e) {
-      const int *kn = &m.knods[size_t(e) * m.ngnod];
-      for (int t = 0; t < 4; ++t) {
-        uint64_t na = kn[ends[t][0]], nb = kn[ends[t][1]];
-        edges[std::min(na, nb) * npg + std::max(na, nb)].push_back({e, t});
-      }
-    }
-    std::unordered_map<int, std::vector<double>> cp;  // mesh element -> [25][2]
-    for (auto &kv : edges) {
-      if (kv.second.size() != 2) continue;
-      const auto [e1, t1] = kv.second[0];
-      const auto [e2, t2] = kv.second[1];
-      if (a.mesh_medium[e1] == a.mesh_medium[e2]) continue;
-      for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
-        auto &v = cp[e];
-        v.resize(2 * NPTS, 0.0);
-        for (int iz = 0; iz < NGLL; ++iz)
-          for (int ix = 0; ix < NGLL; ++ix) {
-            if (!on_edge(t, iz, ix)) continue;
-            double nx, nz;
-            edge_normal(J[size_t(e) * NPTS + iz * NGLL + ix], t, nx, nz);
-            const double f = (t == BOTTOM || t == TOP) ? w[ix] : w[iz];
-            v[2 * (iz * NGLL + ix)] += f * nx;
-            v[2 * (iz * NGLL + ix) + 1] += f * nz;
-          }
-      }
-    }
-    for (int med = 0; med < 2; ++med) {
-      MediumData &D = med == 1 ? a.el : a.ac;
-      const std::vector<int> &other = med == 1 ? a.glob_to_ac : a.glob_to_el;
-      D.cp_slot.assign(D.nspec, -1);
-      int ns = 0;
-      for (int ce = 0; ce < D.nspec; ++ce)
-        if (cp.count(D.elem_mesh[ce])) D.cp_slot[ce] = ns++;
-      D.cp_nx.assign(size_t(ns) * NPTS, 0); D.cp_nz.assign(size_t(ns) * NPTS, 0);
-      D.cp_other.assign(size_t(ns) * NPTS, -1);
-      for (int ce = 0; ce < D.nspec; ++ce) {
-        if (D.cp_slot[ce] < 0) continue;
-        const int e = D.elem_mesh[ce];
-        const auto &v = cp[e];
-        for (int q = 0; q < NPTS; ++q) {
-          const size_t k = size_t(D.cp_slot[ce]) * NPTS + q;
-          const int g = gid[size_t(e) * NPTS + q];
-          if (v[2 * q] == 0.0 && v[2 * q + 1] == 0.0) continue;
-          // coupling at acoustic free-surface points is dropped (compute_coupling.tpp:101-106)
-          float keep = 1.0f;
-          if (D.bc_slot[ce] >= 0) keep = D.bc_keep[size_t(D.bc_slot[ce]) * NPTS + q];
-          D.cp_nx[k] = float(v[2 * q]) * keep;
-          D.cp_nz[k] = float(v[2 * q + 1]) * keep;
-          D.cp_other[k] = other[g];
-        }
       }
     }
   }

@@ -51,10 +51,12 @@ struct MediumData {
   // Stacey / free-surface: slot per element (-1 none), compact [nslot][25]
   std::vector<int> bc_slot;
   std::vector<float> bc_w, bc_nx, bc_nz, bc_j1, bc_imp0, bc_imp1, bc_keep;
-  // coupling with the other medium: slot per element, compact [nslot][25]
-  std::vector<int> cp_slot;
-  std::vector<float> cp_nx, cp_nz;    // sum over coupled edges of weight * normal
-  std::vector<int> cp_other;          // other medium's point id (-1 none)
+  // coupling with the other medium: the first niface points of the medium's
+  // numbering lie on coupled edges; per point the sum over the coupled edges
+  // of GLL weight * outward normal, and the other medium's id of the point
+  int niface = 0;
+  std::vector<float> cp_nx, cp_nz;    // [niface]
+  std::vector<int> cp_other;          // [niface]
   std::vector<int> glob_of_point;     // medium point id -> mesh global id
 };
 

@@ -1,28 +1,36 @@
 // sm_100a kernels of the 2D spectral-element time step (FP32).
 //
-// One time step of one medium is: [colour passes of the element kernel]
-// -> [receiver kernel] -> [point update kernel].
+// One time step is: [one element-kernel launch per mesh colour, covering the
+// elements of that colour in both media] -> [acoustic receivers] ->
+// [acoustic point update] -> [elastic receivers] -> [elastic point update].
 //
 // * Element kernel (stiffness): one thread per element GLL point, E elements
-//   per block (25*E threads, element-local arrays [element][25] so a block
-//   reads one contiguous run of each geometry array).  The displacement is
-//   gathered through ibool into shared memory, the 5-term Lagrange-derivative
-//   contractions and the stress run in registers, the stress integrand F goes
-//   back to shared memory for the divergence, and the epilogue adds Stacey
-//   traction, the acoustic/elastic coupling term and point sources before a
-//   plain (non-atomic) += into the accumulator.  Elements of one launch share
-//   no global point (mesh colouring), so the assembly is race-free and its
-//   summation order is fixed: results are deterministic.
+//   per block (25*E threads; element-local arrays are [element][25] so a block
+//   reads one contiguous run of each geometry array).  Every load that does not
+//   depend on shared memory (index, Jacobian, material, the gathered
+//   displacement and the accumulator value) is issued before the first
+//   barrier.  The 5-term Lagrange-derivative contractions and the stress run
+//   in registers, the stress integrand F goes through shared memory for the
+//   divergence, and the epilogue adds Stacey traction, the acoustic free
+//   surface and point sources before a plain (non-atomic) += into the
+//   accumulator.  Elements of one launch share no global point (mesh
+//   colouring), so assembly is race-free with a fixed summation order: results
+//   are deterministic and independent of the launch shape.
 //   Reference: include/kokkos_kernels/impl/compute_stiffness_interaction.tpp:140-247,
 //   include/algorithms/gradient.hpp:40-82, divergence.hpp:41-74,
 //   include/medium/dim2/*/isotropic/stress.hpp, core/specfem/point/stress.hpp:166-183,
 //   include/boundary_conditions/stacey/stacey.tpp:50-80,130-146,296-326,
 //   include/boundary_conditions/dirichlet/dirichlet.hpp:38-62,
-//   include/kokkos_kernels/impl/compute_coupling.tpp:21-115,
 //   include/kokkos_kernels/impl/compute_source_interaction.tpp:17-104.
-// * Point update: a = accum * M^-1, the Newmark corrector of this step and
-//   the predictor of the next step in one streaming pass; the accumulator is
-//   cleared for the next step (divide_mass_matrix.tpp:10-65, newmark.tpp:10-128).
+// * Point update: a = (accum + coupling) * M^-1 and the Newmark corrector of
+//   this step; inside a run the predictor of the next step is fused into the
+//   same float4 streaming pass, the last step of a run stops after the
+//   corrector (so the fields read back are the reference's end-of-step state)
+//   and k_predict applies the pending predictor when the next run starts
+//   (divide_mass_matrix.tpp:10-65, newmark.tpp:10-128).  The acoustic/elastic
+//   coupling term (compute_coupling.tpp:21-115) is linear in the other
+//   medium's field at the same point; the interface points are numbered first
+//   in each medium, so the update adds it for indices below niface only.
 // * Receiver kernel: one warp per receiver, Lagrange interpolation of the
 //   corrected fields (compute_seismogram.tpp:19-171).
 #pragma once
@@ -42,259 +50,307 @@ struct Quad {
   float w[NG];
 };
 
-struct ElemArgs {
+// Element arrays of one medium.
+struct MedArgs {
   const int *__restrict__ ibool;
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
   const int *__restrict__ bc_slot;
   const float *__restrict__ bc_w, *__restrict__ bc_nx, *__restrict__ bc_nz, *__restrict__ bc_j1,
       *__restrict__ bc_imp0, *__restrict__ bc_imp1, *__restrict__ bc_keep;
-  const int *__restrict__ cp_slot;
-  const float *__restrict__ cp_nx, *__restrict__ cp_nz;
-  const int *__restrict__ cp_other;
-  const float *__restrict__ other;     // elastic: acoustic chi_dd; acoustic: elastic u (float2)
-  const int *__restrict__ src_head, *__restrict__ src_next;
+  const int *__restrict__ src_head;
+  const float *__restrict__ u, *__restrict__ v;
+  float *__restrict__ accum;
+  int e0, e1;      // element range of the colour
+  int nblocks;     // blocks of this medium in the launch
+};
+
+struct StiffArgs {
+  MedArgs el, ac;
+  const int *__restrict__ src_next;
   const float *__restrict__ src_arr;   // [nsrc][2][25]
   const float *__restrict__ stf;       // [nstep][nsrc]
   int nsrc, nstep;
   const int *__restrict__ step;        // device step counter
-  const float *__restrict__ u, *__restrict__ v;
-  float *__restrict__ accum;
-  int e0, e1;
   Quad quad;
 };
 
-// 2D elastic P-SV, two components.
-template <int E>
-__global__ void __launch_bounds__(NP * E) k_stiffness_psv(ElemArgs A) {
-  __shared__ float2 su[NP * E];
-  __shared__ float4 sF[NP * E];
-  __shared__ float shp[NP], shpw[NP], sw[NG];
+__device__ __forceinline__ void load_quad(const Quad &Q, float *shp, float *shpw, float *sw,
+                                          int tid) {
+  if (tid < NP) { shp[tid] = Q.hp[tid]; shpw[tid] = Q.hpw[tid]; }
+  if (tid < NG) sw[tid] = Q.w[tid];
+}
+
+// Elastic element block; EK 0 = P-SV (two components), 1 = SH (one component).
+template <int E, int EK>
+__device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs &A, int ebase,
+                                              unsigned char *smem, float *shp, float *shpw,
+                                              float *sw) {
+  constexpr int NC = EK == 0 ? 2 : 1;
+  float *su = reinterpret_cast<float *>(smem);                               // [E][NC][25]
+  float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * 2);  // [E][NC][2][25]
   const int tid = threadIdx.x;
-  if (tid < NP) { shp[tid] = A.quad.hp[tid]; shpw[tid] = A.quad.hpw[tid]; }
-  if (tid < NG) sw[tid] = A.quad.w[tid];
   const int le = tid / NP, q = tid - le * NP;
-  const int e = A.e0 + blockIdx.x * E + le;
+  const int e = ebase + le;
   const bool act = e < A.e1;
-  const size_t p = size_t(e) * NP + q;
-  const float2 *u2 = reinterpret_cast<const float2 *>(A.u);
-  int g = 0;
-  float2 uu = make_float2(0.f, 0.f);
-  if (act) {
-    g = __ldg(A.ibool + p);
-    uu = u2[g];
+  const size_t p = size_t(act ? e : A.e0) * NP + q;
+  // early loads: everything that does not need shared memory
+  const int g = act ? __ldg(A.ibool + p) : 0;
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+  float uu[NC], acc[NC];
+  if (NC == 2) {
+    const float2 t = act ? reinterpret_cast<const float2 *>(A.u)[g] : make_float2(0.f, 0.f);
+    const float2 r = act ? reinterpret_cast<const float2 *>(A.accum)[g] : make_float2(0.f, 0.f);
+    uu[0] = t.x; uu[NC - 1] = t.y; acc[0] = r.x; acc[NC - 1] = r.y;
+  } else {
+    uu[0] = act ? A.u[g] : 0.f;
+    acc[0] = act ? A.accum[g] : 0.f;
   }
-  su[tid] = uu;
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  const int src = act ? __ldg(A.src_head + e) : -1;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) su[(le * NC + c) * NP + q] = uu[c];
   __syncthreads();
   const int iz = q / NG, ix = q - iz * NG;
-  const int rb = le * NP + iz * NG, cb = le * NP + ix;
-  float dxi0 = 0.f, dxi1 = 0.f, dga0 = 0.f, dga1 = 0.f;
+  float dxi[NC], dga[NC];
 #pragma unroll
-  for (int l = 0; l < NG; ++l) {
-    const float hx = shp[ix * NG + l], hz = shp[iz * NG + l];
-    const float2 ur = su[rb + l], uc = su[cb + l * NG];
-    dxi0 = fmaf(hx, ur.x, dxi0);
-    dxi1 = fmaf(hx, ur.y, dxi1);
-    dga0 = fmaf(hz, uc.x, dga0);
-    dga1 = fmaf(hz, uc.y, dga1);
+  for (int c = 0; c < NC; ++c) {
+    dxi[c] = 0.f;
+    dga[c] = 0.f;
+    const float *fu = su + (le * NC + c) * NP;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      dxi[c] = fmaf(shp[ix * NG + l], fu[iz * NG + l], dxi[c]);
+      dga[c] = fmaf(shp[iz * NG + l], fu[l * NG + ix], dga[c]);
+    }
   }
-  float4 F = make_float4(0.f, 0.f, 0.f, 0.f);
-  if (act) {
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    const float l2m = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
-    const float du00 = xix * dxi0 + gax * dga0, du01 = xiz * dxi0 + gaz * dga0;
-    const float du10 = xix * dxi1 + gax * dga1, du11 = xiz * dxi1 + gaz * dga1;
-    const float lam = l2m - 2.f * mu;
-    const float sxx = l2m * du00 + lam * du11;
-    const float szz = l2m * du11 + lam * du00;
+  // stress (P-SV: isotropic Hooke with lambda+2mu = c0; SH: sigma = mu grad u_y)
+  float Sx[NC], Sz[NC];
+  if (EK == 0) {
+    const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+    const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
+    const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+    const float lam = c0 - 2.f * mu;
+    const float sxx = c0 * du00 + lam * du11;
+    const float szz = c0 * du11 + lam * du00;
     const float sxz = mu * (du01 + du10);
-    F.x = jac * (sxx * xix + sxz * xiz);
-    F.y = jac * (sxx * gax + sxz * gaz);
-    F.z = jac * (sxz * xix + szz * xiz);
-    F.w = jac * (sxz * gax + szz * gaz);
+    Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
+  } else {
+    Sx[0] = mu * (xix * dxi[0] + gax * dga[0]);
+    Sz[0] = mu * (xiz * dxi[0] + gaz * dga[0]);
   }
-  sF[tid] = F;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    sF[((le * NC + c) * 2 + 0) * NP + q] = jac * (Sx[c] * xix + Sz[c] * xiz);
+    sF[((le * NC + c) * 2 + 1) * NP + q] = jac * (Sx[c] * gax + Sz[c] * gaz);
+  }
   __syncthreads();
   if (!act) return;
-  float t1x = 0.f, t1z = 0.f, t2x = 0.f, t2z = 0.f;
+  float a[NC];
 #pragma unroll
-  for (int l = 0; l < NG; ++l) {
-    const float4 fr = sF[rb + l], fc = sF[cb + l * NG];
-    const float h1 = shpw[l * NG + ix], h2 = shpw[l * NG + iz];
-    t1x = fmaf(fr.x, h1, t1x);
-    t1z = fmaf(fr.z, h1, t1z);
-    t2x = fmaf(fc.y, h2, t2x);
-    t2z = fmaf(fc.w, h2, t2z);
+  for (int c = 0; c < NC; ++c) {
+    const float *f0 = sF + ((le * NC + c) * 2 + 0) * NP;
+    const float *f1 = sF + ((le * NC + c) * 2 + 1) * NP;
+    float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      t1 = fmaf(f0[iz * NG + l], shpw[l * NG + ix], t1);
+      t2 = fmaf(f1[l * NG + ix], shpw[l * NG + iz], t2);
+    }
+    a[c] = -(sw[iz] * t1 + sw[ix] * t2);
   }
-  float ax = -(sw[iz] * t1x + sw[ix] * t2x);
-  float az = -(sw[iz] * t1z + sw[ix] * t2z);
-  const int bs = __ldg(A.bc_slot + e);
   if (bs >= 0) {
     const size_t k = size_t(bs) * NP + q;
     const float wq = A.bc_w[k];
     if (wq != 0.f) {
-      const float2 vv = reinterpret_cast<const float2 *>(A.v)[g];
       const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
-      const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
-      const float vn = vv.x * nx + vv.y * nz;
-      const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vv.x * rvs;
-      const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vv.y * rvs;
-      ax += -1.f * fx * j1 * wq;
-      az += -1.f * fz * j1 * wq;
+      if (EK == 0) {
+        const float2 vv = reinterpret_cast<const float2 *>(A.v)[g];
+        const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+        const float vn = vv.x * nx + vv.y * nz;
+        const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vv.x * rvs;
+        const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vv.y * rvs;
+        a[0] += -1.f * fx * j1 * wq;
+        a[NC - 1] += -1.f * fz * j1 * wq;
+      } else {
+        a[0] += -1.f * (wq * j1) * A.bc_imp1[k] * A.v[g];
+      }
     }
   }
-  const int cs = __ldg(A.cp_slot + e);
-  if (cs >= 0) {
-    const size_t k = size_t(cs) * NP + q;
-    const int o = A.cp_other[k];
-    if (o >= 0) {
-      const float chi_dd = A.other[o];
-      ax += A.cp_nx[k] * chi_dd;
-      az += A.cp_nz[k] * chi_dd;
+  if (src >= 0) {
+    const int step = *S.step;
+    for (int s = src; s >= 0; s = S.src_next[s]) {
+      const float f = step < S.nstep ? S.stf[size_t(step) * S.nsrc + s] : 0.f;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
     }
   }
-  int s = __ldg(A.src_head + e);
-  if (s >= 0) {
-    const int step = *A.step;
-    while (s >= 0) {
-      const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
-      ax += f * A.src_arr[(size_t(s) * 2) * NP + q];
-      az += f * A.src_arr[(size_t(s) * 2 + 1) * NP + q];
-      s = A.src_next[s];
-    }
+  if (NC == 2) {
+    reinterpret_cast<float2 *>(A.accum)[g] = make_float2(acc[0] + a[0], acc[NC - 1] + a[NC - 1]);
+  } else {
+    A.accum[g] = acc[0] + a[0];
   }
-  float2 *acc2 = reinterpret_cast<float2 *>(A.accum);
-  float2 acc = acc2[g];
-  acc.x += ax;
-  acc.y += az;
-  acc2[g] = acc;
 }
 
-// One-component media: KIND 0 acoustic (potential chi), KIND 1 elastic SH.
-template <int E, int KIND>
-__global__ void __launch_bounds__(NP * E) k_stiffness_1c(ElemArgs A) {
-  __shared__ float su[NP * E];
-  __shared__ float2 sF[NP * E];
-  __shared__ float shp[NP], shpw[NP], sw[NG];
+// Acoustic element block (potential chi; sigma = rho^-1 grad chi).
+template <int E>
+__device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs &A, int ebase,
+                                               unsigned char *smem, float *shp, float *shpw,
+                                               float *sw) {
+  float *su = reinterpret_cast<float *>(smem);
+  float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * 2);
   const int tid = threadIdx.x;
-  if (tid < NP) { shp[tid] = A.quad.hp[tid]; shpw[tid] = A.quad.hpw[tid]; }
-  if (tid < NG) sw[tid] = A.quad.w[tid];
   const int le = tid / NP, q = tid - le * NP;
-  const int e = A.e0 + blockIdx.x * E + le;
+  const int e = ebase + le;
   const bool act = e < A.e1;
-  const size_t p = size_t(e) * NP + q;
-  int g = 0;
-  float uu = 0.f;
-  if (act) {
-    g = __ldg(A.ibool + p);
-    uu = A.u[g];
-  }
-  su[tid] = uu;
+  const size_t p = size_t(act ? e : A.e0) * NP + q;
+  const int g = act ? __ldg(A.ibool + p) : 0;
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float rhoinv = __ldg(A.prop0 + p);
+  const float chi = act ? A.u[g] : 0.f;
+  const float acc = act ? A.accum[g] : 0.f;
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  const int src = act ? __ldg(A.src_head + e) : -1;
+  su[le * NP + q] = chi;
   __syncthreads();
   const int iz = q / NG, ix = q - iz * NG;
-  const int rb = le * NP + iz * NG, cb = le * NP + ix;
   float dxi = 0.f, dga = 0.f;
 #pragma unroll
   for (int l = 0; l < NG; ++l) {
-    dxi = fmaf(shp[ix * NG + l], su[rb + l], dxi);
-    dga = fmaf(shp[iz * NG + l], su[cb + l * NG], dga);
+    dxi = fmaf(shp[ix * NG + l], su[le * NP + iz * NG + l], dxi);
+    dga = fmaf(shp[iz * NG + l], su[le * NP + l * NG + ix], dga);
   }
-  float2 F = make_float2(0.f, 0.f);
-  if (act) {
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    // acoustic: sigma = rho^-1 grad chi; SH: sigma = mu grad u_y
-    const float c = KIND == 0 ? __ldg(A.prop0 + p) : __ldg(A.prop1 + p);
-    const float s0 = c * (xix * dxi + gax * dga);
-    const float s1 = c * (xiz * dxi + gaz * dga);
-    F.x = jac * (s0 * xix + s1 * xiz);
-    F.y = jac * (s0 * gax + s1 * gaz);
-  }
-  sF[tid] = F;
+  const float s0 = rhoinv * (xix * dxi + gax * dga);
+  const float s1 = rhoinv * (xiz * dxi + gaz * dga);
+  sF[(le * 2 + 0) * NP + q] = jac * (s0 * xix + s1 * xiz);
+  sF[(le * 2 + 1) * NP + q] = jac * (s0 * gax + s1 * gaz);
   __syncthreads();
   if (!act) return;
   float t1 = 0.f, t2 = 0.f;
 #pragma unroll
   for (int l = 0; l < NG; ++l) {
-    t1 = fmaf(sF[rb + l].x, shpw[l * NG + ix], t1);
-    t2 = fmaf(sF[cb + l * NG].y, shpw[l * NG + iz], t2);
+    t1 = fmaf(sF[(le * 2 + 0) * NP + iz * NG + l], shpw[l * NG + ix], t1);
+    t2 = fmaf(sF[(le * 2 + 1) * NP + l * NG + ix], shpw[l * NG + iz], t2);
   }
   float a = -(sw[iz] * t1 + sw[ix] * t2);
-  const int bs = __ldg(A.bc_slot + e);
   if (bs >= 0) {
     const size_t k = size_t(bs) * NP + q;
     const float wq = A.bc_w[k];
-    if (wq != 0.f) {
-      const float imp = KIND == 0 ? A.bc_imp0[k] : A.bc_imp1[k];
-      a += -1.f * (wq * A.bc_j1[k]) * imp * A.v[g];
-    }
+    if (wq != 0.f) a += -1.f * (wq * A.bc_j1[k]) * A.bc_imp0[k] * A.v[g];
     a *= A.bc_keep[k];   // acoustic free surface (Dirichlet) zeroes the element term
   }
-  if (KIND == 0) {
-    const int cs = __ldg(A.cp_slot + e);
-    if (cs >= 0) {
-      const size_t k = size_t(cs) * NP + q;
-      const int o = A.cp_other[k];
-      if (o >= 0) {
-        const float2 ue = reinterpret_cast<const float2 *>(A.other)[o];
-        a += A.cp_nx[k] * ue.x + A.cp_nz[k] * ue.y;
-      }
+  if (src >= 0) {
+    const int step = *S.step;
+    for (int s = src; s >= 0; s = S.src_next[s]) {
+      const float f = step < S.nstep ? S.stf[size_t(step) * S.nsrc + s] : 0.f;
+      a += f * S.src_arr[(size_t(s) * 2) * NP + q];
     }
   }
-  int s = __ldg(A.src_head + e);
-  if (s >= 0) {
-    const int step = *A.step;
-    while (s >= 0) {
-      const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
-      a += f * A.src_arr[(size_t(s) * 2) * NP + q];
-      s = A.src_next[s];
-    }
-  }
-  A.accum[g] += a;
+  A.accum[g] = acc + a;
+}
+
+// One launch per colour: blocks [0, el.nblocks) run elastic elements of the
+// colour, the following ac.nblocks blocks acoustic ones.
+template <int E, int EK>
+__global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
+  __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * 6];
+  __shared__ float shp[NP], shpw[NP], sw[NG];
+  load_quad(S.quad, shp, shpw, sw, threadIdx.x);
+  if (int(blockIdx.x) < S.el.nblocks)
+    elastic_block<E, EK>(S, S.el, S.el.e0 + blockIdx.x * E, smem, shp, shpw, sw);
+  else
+    acoustic_block<E>(S, S.ac, S.ac.e0 + (blockIdx.x - S.el.nblocks) * E, smem, shp, shpw, sw);
 }
 
 struct UpdateArgs {
   float *__restrict__ u, *__restrict__ v, *__restrict__ accum;
   const float *__restrict__ minv;
-  float *__restrict__ a_store;   // optional copy of the new acceleration
+  float *__restrict__ a_store;   // copy of the new acceleration (optional when predicting)
   int n;                         // nglob * ncomp
+  int ncomp;
+  // coupling: the first niface points take cp_n . other[cp_other] (acoustic
+  // self: other = elastic displacement, float2) or cp_n * other (elastic self:
+  // other = acoustic chi_dd)
+  int niface;
+  const float *__restrict__ cp_nx, *__restrict__ cp_nz;
+  const int *__restrict__ cp_other;
+  const float *__restrict__ other;
   float dt, dt2, dtsq2;
+  int predict;                   // fuse the next step's predictor
   int *flag;                     // set to 1 on a non-finite displacement
   int *step;
   int advance;                   // increment the step counter (last update of a step)
 };
 
-// a = accum * M^-1; v += dt/2 a (corrector); u += dt v + dt^2/2 a; v += dt/2 a
-// (predictor of the next step); accum = 0.  Streams float4.
+__device__ __forceinline__ float coupling_term(const UpdateArgs &A, int pt, int comp) {
+  const int o = A.cp_other[pt];
+  if (A.ncomp == 1) {  // acoustic self: n . u_elastic
+    const float2 ue = reinterpret_cast<const float2 *>(A.other)[o];
+    return A.cp_nx[pt] * ue.x + A.cp_nz[pt] * ue.y;
+  }
+  const float chi_dd = A.other[o];  // elastic self: n * chi_dd
+  return (comp == 0 ? A.cp_nx[pt] : A.cp_nz[pt]) * chi_dd;
+}
+
+// Newmark predictor u += dt v + dt^2/2 a; v += dt/2 a (newmark.tpp:64-128),
+// with every product and sum rounded separately (no contraction into FMA), so
+// the fused update and k_predict give equal bits, as does a CPU build with
+// contraction off.
+__device__ __forceinline__ void newmark_predict(float &u, float &v, float a, float dt, float dt2,
+                                                float dtsq2) {
+  u = __fadd_rn(u, __fadd_rn(__fmul_rn(dt, v), __fmul_rn(dtsq2, a)));
+  v = __fadd_rn(v, __fmul_rn(dt2, a));
+}
+
+// Newmark corrector v += dt/2 a (newmark.tpp:10-62).
+__device__ __forceinline__ float newmark_correct(float v, float a, float dt2) {
+  return __fadd_rn(v, __fmul_rn(dt2, a));
+}
+
+// a = (accum [+ coupling]) * M^-1; v += dt/2 a (corrector); optionally the
+// predictor of the next step; accum = 0.
 __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
   const int n4 = A.n >> 2;
   const int stride = gridDim.x * blockDim.x;
   bool bad = false;
+  const int nc_iface = A.niface * A.ncomp;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
     float4 ac = reinterpret_cast<float4 *>(A.accum)[i];
     const float4 mi = reinterpret_cast<const float4 *>(A.minv)[i];
     float4 uu = reinterpret_cast<float4 *>(A.u)[i];
     float4 vv = reinterpret_cast<float4 *>(A.v)[i];
-    float a[4] = {ac.x * mi.x, ac.y * mi.y, ac.z * mi.z, ac.w * mi.w};
-    float *pu = &uu.x, *pv = &vv.x;
+    float *pa = &ac.x, *pu = &uu.x, *pv = &vv.x;
+    const float *pm = &mi.x;
+    if (4 * i < nc_iface) {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const int k = 4 * i + c;
+        if (k < nc_iface) pa[c] += coupling_term(A, k / A.ncomp, k % A.ncomp);
+      }
+    }
+    float a[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-      pv[c] = pv[c] + A.dt2 * a[c];
-      pu[c] = pu[c] + (A.dt * pv[c] + A.dtsq2 * a[c]);
-      pv[c] = pv[c] + A.dt2 * a[c];
+      a[c] = __fmul_rn(pa[c], pm[c]);
+      pv[c] = newmark_correct(pv[c], a[c], A.dt2);
+      if (A.predict) newmark_predict(pu[c], pv[c], a[c], A.dt, A.dt2, A.dtsq2);
       bad |= !isfinite(pu[c]);
     }
-    reinterpret_cast<float4 *>(A.u)[i] = uu;
+    if (A.predict) reinterpret_cast<float4 *>(A.u)[i] = uu;
     reinterpret_cast<float4 *>(A.v)[i] = vv;
     reinterpret_cast<float4 *>(A.accum)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     if (A.a_store) reinterpret_cast<float4 *>(A.a_store)[i] = make_float4(a[0], a[1], a[2], a[3]);
   }
   for (int i = (n4 << 2) + blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
-    const float a = A.accum[i] * A.minv[i];
-    float vv = A.v[i] + A.dt2 * a;
-    const float uu = A.u[i] + (A.dt * vv + A.dtsq2 * a);
-    vv = vv + A.dt2 * a;
+    float acc = A.accum[i];
+    if (i < nc_iface) acc += coupling_term(A, i / A.ncomp, i % A.ncomp);
+    const float a = __fmul_rn(acc, A.minv[i]);
+    float vv = newmark_correct(A.v[i], a, A.dt2);
+    float uu = A.u[i];
+    if (A.predict) newmark_predict(uu, vv, a, A.dt, A.dt2, A.dtsq2);
     A.u[i] = uu;
     A.v[i] = vv;
     A.accum[i] = 0.f;
@@ -303,6 +359,18 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
   }
   if (bad) *A.flag = 1;
   if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
+// Pending predictor of a run that ended on a corrector-only update.
+__global__ void __launch_bounds__(256) k_predict(float *__restrict__ u, float *__restrict__ v,
+                                                 const float *__restrict__ a, int n, float dt,
+                                                 float dt2, float dtsq2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    float uu = u[i], vv = v[i];
+    newmark_predict(uu, vv, a[i], dt, dt2, dtsq2);
+    u[i] = uu;
+    v[i] = vv;
+  }
 }
 
 struct RecArgs {
@@ -314,6 +382,7 @@ struct RecArgs {
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ prop0, *__restrict__ prop1;
   const float *__restrict__ u, *__restrict__ v, *__restrict__ accum, *__restrict__ minv;
+  UpdateArgs cpl;                      // coupling data of the medium (niface, cp_*, other)
   int ncomp, acoustic;
   int ntypes;
   int types[4];
@@ -330,9 +399,16 @@ __device__ __forceinline__ float warp_sum(float x) {
   return x;
 }
 
+__device__ __forceinline__ float rec_accel(const RecArgs &A, int g, int c) {
+  const size_t k = size_t(g) * A.ncomp + c;
+  float acc = A.accum[k];
+  if (g < A.cpl.niface) acc += coupling_term(A.cpl, g, c);
+  return __fmul_rn(acc, A.minv[k]);
+}
+
 // One warp per receiver of one medium; runs before that medium's update, so
 // it reconstructs the corrected velocity and the new acceleration from the
-// accumulator.
+// accumulator (plus the coupling term on interface points).
 __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
   __shared__ float sf[3][NP];
   const int step = *A.step;
@@ -374,24 +450,17 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
           }
         }
         o[0] = warp_sum(h * pr);
-        if (lane == 0) {
-          float *dst = A.seis + ((size_t(isig) * A.ntypes + t) * A.nrec_total + r) * 2;
-          dst[0] = o[0];
-          dst[1] = 0.f;
+      } else {
+        for (int c = 0; c < A.ncomp; ++c) {
+          const size_t k = size_t(g) * A.ncomp + c;
+          float val = 0.f;
+          switch (A.types[t]) {
+            case 0: val = A.u[k]; break;
+            case 1: val = newmark_correct(A.v[k], rec_accel(A, g, c), A.dt2); break;
+            default: val = rec_accel(A, g, c); break;
+          }
+          o[c] = warp_sum(h * val);
         }
-        continue;
-      }
-      for (int c = 0; c < A.ncomp; ++c) {
-        const size_t k = size_t(g) * A.ncomp + c;
-        const float a = A.accum[k] * A.minv[k];
-        float val = 0.f;
-        switch (A.types[t]) {
-          case 0: val = A.u[k]; break;
-          case 1: val = A.v[k] + A.dt2 * a; break;
-          case 2: val = a; break;
-          default: val = 0.f; break;
-        }
-        o[c] = warp_sum(h * val);
       }
       if (lane == 0) {
         float *dst = A.seis + ((size_t(isig) * A.ntypes + t) * A.nrec_total + r) * 2;
@@ -402,10 +471,10 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
     return;
   }
   // acoustic: displacement-like outputs are rho^-1 grad(field); pressure = -chi_dd
-  const float a = A.accum[g] * A.minv[g];
+  const float a = rec_accel(A, g, 0);
   if (on) {
     sf[0][q] = A.u[g];
-    sf[1][q] = A.v[g] + A.dt2 * a;
+    sf[1][q] = newmark_correct(A.v[g], a, A.dt2);
     sf[2][q] = a;
   }
   __syncwarp();

@@ -70,7 +70,7 @@ struct DevMedium {
   int *bc_slot = nullptr;
   float *bc_w = nullptr, *bc_nx = nullptr, *bc_nz = nullptr, *bc_j1 = nullptr,
         *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr;
-  int *cp_slot = nullptr;
+  int niface = 0;
   float *cp_nx = nullptr, *cp_nz = nullptr;
   int *cp_other = nullptr;
   int *src_head = nullptr;
@@ -101,8 +101,11 @@ struct sfg_handle {
   int host_step = 0;
   int epb = 16;
   cudaStream_t stream = nullptr;
-  cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr;
+  cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr, graph_e = nullptr;
   int graph_steps = 0;
+  // true when u, v hold the end-of-step state of the reference (after the
+  // corrector); false inside a run, where the next predictor is already applied
+  bool state_final = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
@@ -112,6 +115,7 @@ struct sfg_handle {
   ~sfg_handle() {
     if (graph_k) cudaGraphExecDestroy(graph_k);
     if (graph_1) cudaGraphExecDestroy(graph_1);
+    if (graph_e) cudaGraphExecDestroy(graph_e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (stream) cudaStreamDestroy(stream);
@@ -151,7 +155,7 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
   D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
   D.bc_keep = m.upload(M.bc_keep);
-  D.cp_slot = m.upload(M.cp_slot);
+  D.niface = M.niface;
   D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
   D.minv = m.upload(M.minv);
   const size_t n = size_t(M.nglob) * M.ncomp;
@@ -162,51 +166,93 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.a = m.zeros<float>(n + 4);
 }
 
-sfg::dev::ElemArgs elem_args(sfg_handle *h, DevMedium &D, DevMedium &O, bool acoustic) {
-  sfg::dev::ElemArgs A{};
+sfg::dev::MedArgs med_args(const DevMedium &D) {
+  sfg::dev::MedArgs A{};
   A.ibool = D.ibool;
   A.xix = D.xix; A.xiz = D.xiz; A.gax = D.gax; A.gaz = D.gaz; A.jac = D.jac;
   A.prop0 = D.prop0; A.prop1 = D.prop1;
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
-  A.cp_slot = D.cp_slot; A.cp_nx = D.cp_nx; A.cp_nz = D.cp_nz; A.cp_other = D.cp_other;
-  A.other = acoustic ? O.u : O.a;
-  A.src_head = D.src_head; A.src_next = h->d_src_next; A.src_arr = h->d_src_arr;
-  A.stf = h->d_stf;
-  A.nsrc = h->asmb.nsrc;
-  A.nstep = h->asmb.nstep;
-  A.step = h->d_step;
+  A.src_head = D.src_head;
   A.u = D.u; A.v = D.v; A.accum = D.accum;
-  A.quad = h->quad;
   return A;
 }
 
-template <int E>
-void launch_stiffness_E(sfg_handle *h, DevMedium &D, DevMedium &O, int medium, cudaStream_t s) {
-  sfg::dev::ElemArgs A = elem_args(h, D, O, medium == SFG_MEDIUM_ACOUSTIC);
-  for (size_t c = 0; c + 1 < D.color_start.size(); ++c) {
-    A.e0 = D.color_start[c];
-    A.e1 = D.color_start[c + 1];
-    const int n = A.e1 - A.e0;
-    if (n <= 0) continue;
-    const int grid = (n + E - 1) / E;
-    if (medium == SFG_MEDIUM_ACOUSTIC)
-      sfg::dev::k_stiffness_1c<E, 0><<<grid, sfg::dev::NP * E, 0, s>>>(A);
-    else if (D.ncomp == 1)
-      sfg::dev::k_stiffness_1c<E, 1><<<grid, sfg::dev::NP * E, 0, s>>>(A);
-    else
-      sfg::dev::k_stiffness_psv<E><<<grid, sfg::dev::NP * E, 0, s>>>(A);
+int ncolors(const DevMedium &D) { return D.nspec ? int(D.color_start.size()) - 1 : 0; }
+
+template <int E, int EK>
+void launch_stiffness_E(sfg_handle *h, cudaStream_t s) {
+  sfg::dev::StiffArgs S{};
+  S.el = med_args(h->el);
+  S.ac = med_args(h->ac);
+  S.src_next = h->d_src_next;
+  S.src_arr = h->d_src_arr;
+  S.stf = h->d_stf;
+  S.nsrc = h->asmb.nsrc;
+  S.nstep = h->asmb.nstep;
+  S.step = h->d_step;
+  S.quad = h->quad;
+  const int nc = std::max(ncolors(h->el), ncolors(h->ac));
+  for (int c = 0; c < nc; ++c) {
+    auto range = [&](const DevMedium &D, sfg::dev::MedArgs &A) {
+      A.e0 = A.e1 = 0;
+      A.nblocks = 0;
+      if (c < ncolors(D)) {
+        A.e0 = D.color_start[c];
+        A.e1 = D.color_start[c + 1];
+        A.nblocks = (A.e1 - A.e0 + E - 1) / E;
+      }
+    };
+    range(h->el, S.el);
+    range(h->ac, S.ac);
+    const int grid = S.el.nblocks + S.ac.nblocks;
+    if (grid == 0) continue;
+    sfg::dev::k_stiffness<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
   }
 }
 
-void launch_stiffness(sfg_handle *h, int medium, cudaStream_t s) {
+template <int E>
+void launch_stiffness_W(sfg_handle *h, cudaStream_t s) {
+  if (h->el.ncomp == 1) launch_stiffness_E<E, 1>(h, s);
+  else launch_stiffness_E<E, 0>(h, s);
+}
+
+void launch_stiffness(sfg_handle *h, cudaStream_t s) {
+  switch (h->epb) {
+    case 8: launch_stiffness_W<8>(h, s); break;
+    case 32: launch_stiffness_W<32>(h, s); break;
+    default: launch_stiffness_W<16>(h, s); break;
+  }
+}
+
+sfg::dev::UpdateArgs update_args(sfg_handle *h, int medium, bool predict, bool advance) {
   DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
-  switch (h->epb) {
-    case 8: launch_stiffness_E<8>(h, D, O, medium, s); break;
-    case 32: launch_stiffness_E<32>(h, D, O, medium, s); break;
-    default: launch_stiffness_E<16>(h, D, O, medium, s); break;
-  }
+  sfg::dev::UpdateArgs U{};
+  U.u = D.u; U.v = D.v; U.accum = D.accum; U.minv = D.minv;
+  // acoustic chi_dd feeds the elastic coupling term; the last step of a run
+  // keeps the acceleration for the predictor that resumes the next run
+  U.a_store = (medium == SFG_MEDIUM_ACOUSTIC || !predict || h->opt.store_acceleration) ? D.a : nullptr;
+  U.n = D.nglob * D.ncomp;
+  U.ncomp = D.ncomp;
+  U.niface = D.niface;
+  U.cp_nx = D.cp_nx; U.cp_nz = D.cp_nz; U.cp_other = D.cp_other;
+  U.other = medium == SFG_MEDIUM_ELASTIC ? O.a : O.u;
+  const float dt = float(h->asmb.dt);
+  U.dt = dt;
+  U.dt2 = dt / 2.0f;
+  U.dtsq2 = dt * dt / 2.0f;
+  U.predict = predict ? 1 : 0;
+  U.flag = h->d_flag;
+  U.step = h->d_step;
+  U.advance = advance ? 1 : 0;
+  return U;
+}
+
+int grid_for(int n) {
+  const int threads = 256;
+  int blocks = (n + threads - 1) / threads;
+  return std::max(1, std::min(blocks, 148 * 8));
 }
 
 void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
@@ -221,6 +267,7 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.xix = D.xix; R.xiz = D.xiz; R.gax = D.gax; R.gaz = D.gaz; R.prop0 = D.prop0;
   R.prop1 = D.prop1;
   R.u = D.u; R.v = D.v; R.accum = D.accum; R.minv = D.minv;
+  R.cpl = update_args(h, medium, true, false);
   R.ncomp = D.ncomp;
   R.acoustic = medium == SFG_MEDIUM_ACOUSTIC;
   R.ntypes = h->asmb.ntypes;
@@ -235,57 +282,51 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   sfg::dev::k_receivers<<<D.nrec, 32, 0, s>>>(R);
 }
 
-void launch_update(sfg_handle *h, int medium, bool advance, cudaStream_t s) {
-  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
-  sfg::dev::UpdateArgs U{};
-  U.u = D.u; U.v = D.v; U.accum = D.accum; U.minv = D.minv;
-  // acoustic chi_dd feeds the elastic coupling term; the elastic acceleration is
-  // kept only on request (field read-back)
-  U.a_store = (medium == SFG_MEDIUM_ACOUSTIC || h->opt.store_acceleration) ? D.a : nullptr;
-  U.n = D.nglob * D.ncomp;
+void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaStream_t s) {
+  sfg::dev::UpdateArgs U = update_args(h, medium, predict, advance);
+  sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
+}
+
+void launch_predict(sfg_handle *h, cudaStream_t s) {
   const float dt = float(h->asmb.dt);
-  U.dt = dt;
-  U.dt2 = dt / 2.0f;
-  U.dtsq2 = dt * dt / 2.0f;
-  U.flag = h->d_flag;
-  U.step = h->d_step;
-  U.advance = advance ? 1 : 0;
-  const int threads = 256;
-  int blocks = (U.n / 4 + threads - 1) / threads;
-  blocks = std::max(1, std::min(blocks, 148 * 8));
-  sfg::dev::k_update<<<blocks, threads, 0, s>>>(U);
+  for (DevMedium *D : {&h->ac, &h->el}) {
+    if (!D->nspec) continue;
+    const int n = D->nglob * D->ncomp;
+    sfg::dev::k_predict<<<grid_for(n), 256, 0, s>>>(D->u, D->v, D->a, n, dt, dt / 2.0f, dt * dt / 2.0f);
+  }
 }
 
 // One time step in the reference's medium order (time_marching.tpp:33-83):
-// acoustic update (coupling from the predicted elastic displacement), then
-// elastic update (coupling from the new acoustic chi_dd).
-void enqueue_step(sfg_handle *h, cudaStream_t s) {
+// the element launches of both media, then the acoustic update (its coupling
+// reads the predicted elastic displacement), then the elastic update (its
+// coupling reads the new acoustic chi_dd).  predict = fuse the next step's
+// predictor into the updates.
+void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
+  launch_stiffness(h, s);
   if (has_ac) {
-    launch_stiffness(h, SFG_MEDIUM_ACOUSTIC, s);
     launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
-    launch_update(h, SFG_MEDIUM_ACOUSTIC, !has_el, s);
+    launch_update(h, SFG_MEDIUM_ACOUSTIC, predict, !has_el, s);
   }
   if (has_el) {
-    launch_stiffness(h, SFG_MEDIUM_ELASTIC, s);
     launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
-    launch_update(h, SFG_MEDIUM_ELASTIC, true, s);
+    launch_update(h, SFG_MEDIUM_ELASTIC, predict, true, s);
   }
 }
 
 int kernels_per_step(const sfg_handle *h) {
-  int n = 0;
+  int n = std::max(ncolors(h->el), ncolors(h->ac));
   for (const DevMedium *D : {&h->ac, &h->el}) {
     if (D->nspec == 0) continue;
-    n += int(D->color_start.size()) - 1 + (D->nrec > 0 ? 1 : 0) + 1;
+    n += (D->nrec > 0 ? 1 : 0) + 1;
   }
   return n;
 }
 
-cudaGraphExec_t capture(sfg_handle *h, int nsteps) {
+cudaGraphExec_t capture(sfg_handle *h, int nsteps, bool last_predicts) {
   cudaGraph_t g = nullptr;
   SFG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-  for (int i = 0; i < nsteps; ++i) enqueue_step(h, h->stream);
+  for (int i = 0; i < nsteps; ++i) enqueue_step(h, h->stream, i + 1 < nsteps || last_predicts);
   SFG_CUDA(cudaStreamEndCapture(h->stream, &g));
   cudaGraphExec_t ex = nullptr;
   SFG_CUDA(cudaGraphInstantiate(&ex, g, 0));
@@ -293,16 +334,29 @@ cudaGraphExec_t capture(sfg_handle *h, int nsteps) {
   return ex;
 }
 
+void resume(sfg_handle *h) {
+  if (h->state_final) {
+    launch_predict(h, h->stream);
+    h->state_final = false;
+  }
+}
+
+// nsteps steps; the run ends on a corrector-only update so that the fields
+// are the reference's end-of-step state.
 void run_steps(sfg_handle *h, int nsteps) {
-  int left = nsteps;
-  while (left >= h->graph_steps && h->graph_k) {
+  if (nsteps <= 0) return;
+  resume(h);
+  int fused = nsteps - 1;
+  while (fused >= h->graph_steps && h->graph_k) {
     SFG_CUDA(cudaGraphLaunch(h->graph_k, h->stream));
-    left -= h->graph_steps;
+    fused -= h->graph_steps;
   }
-  while (left > 0) {
+  while (fused > 0) {
     SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
-    --left;
+    --fused;
   }
+  SFG_CUDA(cudaGraphLaunch(h->graph_e, h->stream));
+  h->state_final = true;
   SFG_CUDA(cudaGetLastError());
   h->host_step += nsteps;
 }
@@ -505,8 +559,9 @@ int sfg_initialize(sfg_handle *h) {
     h->d_flag = h->mem.zeros<int>(1);
     SFG_CUDA(cudaDeviceSynchronize());
     h->graph_steps = std::max(1, h->opt.steps_per_graph);
-    h->graph_k = capture(h, h->graph_steps);
-    h->graph_1 = capture(h, 1);
+    h->graph_k = capture(h, h->graph_steps, true);
+    h->graph_1 = capture(h, 1, true);
+    h->graph_e = capture(h, 1, false);
     h->initialized = true;
     return int(SFG_OK);
   });
@@ -515,7 +570,9 @@ int sfg_initialize(sfg_handle *h) {
 int sfg_step(sfg_handle *h) {
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
-    enqueue_step(h, h->stream);
+    resume(h);
+    enqueue_step(h, h->stream, false);
+    h->state_final = true;
     SFG_CUDA(cudaGetLastError());
     ++h->host_step;
     return int(SFG_OK);
@@ -557,6 +614,7 @@ int sfg_reset_fields(sfg_handle *h) {
     SFG_CUDA(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
     SFG_CUDA(cudaStreamSynchronize(h->stream));
     h->host_step = 0;
+    h->state_final = true;
     return int(SFG_OK);
   });
 }
@@ -591,6 +649,7 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
     for (auto &e : ev) SFG_CUDA(cudaEventCreate(&e));
     double total = 0.0;
     int done = 0;
+    resume(h);
     try {
       while (done < nsteps) {
         const int n = std::min(batch, nsteps - done);
@@ -614,6 +673,8 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
       throw;
     }
     for (auto &e : ev) cudaEventDestroy(e);
+    // every timed step fused the next predictor: the fields are mid-step
+    h->state_final = false;
     if (ms) *ms = float(total);
     return int(SFG_OK);
   });
@@ -633,7 +694,9 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
       SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, row.data(), a.nsrc * sizeof(float),
                                cudaMemcpyHostToDevice, h->stream));
     }
-    SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+    resume(h);
+    SFG_CUDA(cudaGraphLaunch(h->graph_e, h->stream));
+    h->state_final = true;
     ++h->host_step;
     if (seis_row && a.nrec > 0 && step % a.nsb == 0 && step / a.nsb < a.nsig) {
       const size_t row = size_t(a.ntypes) * a.nrec * 2;
@@ -651,14 +714,16 @@ int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms) {
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
     if (iters <= 0 || which < 0 || which > 3) return int(SFG_ERR_ARG);
-    const int medium = (which < 2) ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC;
+    const int medium = which == 2 ? SFG_MEDIUM_ACOUSTIC : SFG_MEDIUM_ELASTIC;
     DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
-    if (D.nspec == 0) { if (ms) *ms = 0; return int(SFG_OK); }
-    const bool stiff = (which % 2) == 0;
+    if (which != 0 && D.nspec == 0) { if (ms) *ms = 0; return int(SFG_OK); }
     auto launch = [&]() {
-      if (stiff) launch_stiffness(h, medium, h->stream);
-      else launch_update(h, medium, false, h->stream);
+      if (which == 0) launch_stiffness(h, h->stream);
+      else if (which == 3) { launch_receivers(h, SFG_MEDIUM_ACOUSTIC, h->stream);
+                             launch_receivers(h, SFG_MEDIUM_ELASTIC, h->stream); }
+      else launch_update(h, medium, true, false, h->stream);
     };
+    h->state_final = false;
     for (int i = 0; i < 3; ++i) launch();
     SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
     for (int i = 0; i < iters; ++i) launch();
@@ -723,8 +788,8 @@ int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count
     DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
     const size_t n = size_t(D.nglob) * D.ncomp;
     if (!out || count < n) { h->err = "output buffer too small"; return int(SFG_ERR_ARG); }
-    if (which == 2 && medium == SFG_MEDIUM_ELASTIC && !h->opt.store_acceleration) {
-      h->err = "elastic acceleration is kept only with sfg_options.store_acceleration";
+    if (!h->state_final) {
+      h->err = "fields are mid-step after a timing call; run a step first";
       return int(SFG_ERR_STATE);
     }
     const float *src = which == 0 ? D.u : which == 1 ? D.v : D.a;
