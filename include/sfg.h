@@ -83,7 +83,10 @@ typedef struct sfg_options {
   int nshots;                    /* independent shots advanced together (>= 1) */
   int nstep_between_samples;     /* seismogram sampling (>= 1) */
   int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
-  int elements_per_block;        /* stiffness launch shape (0 = autotuned default) */
+  int elements_per_block;        /* elements per block of the element kernel: 8, 16, 32
+                                    (0 = chosen by the autotuner at sfg_initialize) */
+  int kernel_variant;            /* element kernel: 1 one block per chunk, 2 persistent
+                                    with prefetch (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
 } sfg_options;
 
@@ -103,6 +106,7 @@ typedef struct sfg_info {
   double t0;                     /* time of step 0 (earliest shot) */
   size_t device_bytes;
   int kernels_per_step;
+  int elements_per_block, kernel_variant; /* launch shape in use */
 } sfg_info;
 
 /* ---- life cycle ---- */

@@ -9,8 +9,11 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = ["csrc/sfg.cu", "csrc/host2d.cpp"]
 HEADERS = ["csrc/kernels2d.cuh", "csrc/host2d.hpp", "../include/sfg.h"]
+# -fmad=false: products and sums are rounded separately unless a kernel asks
+# for an FMA explicitly, so every launch shape of a kernel (and the CPU oracle,
+# built with contraction off) performs the same rounding steps.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-Xcompiler", "-fPIC,-O3", "-shared"]
+              "-fmad=false", "-Xcompiler", "-fPIC,-O3", "-shared"]
 
 
 def nvcc() -> str:

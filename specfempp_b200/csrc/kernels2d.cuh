@@ -265,6 +265,197 @@ __global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
     acoustic_block<E>(S, S.ac, S.ac.e0 + (blockIdx.x - S.el.nblocks) * E, smem, shp, shpw, sw);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent variant of the element kernel.  A colour launch holds exactly as
+// many blocks as fit on the GPU at once; blocks [0, el.nblocks) loop over the
+// elastic element chunks of the colour, the others over the acoustic ones
+// (chunk = E consecutive elements).  While a chunk is computed, the next
+// chunk's index and geometry are already in flight, and its displacement and
+// accumulator values are requested once its indices have arrived, so the
+// memory latency of one chunk hides behind the arithmetic of the previous.
+// Shared memory keeps every field both as rows and as transposed rows
+// (padded to 8), so each 5-term contraction reads two vectors; the Lagrange
+// coefficients a thread needs stay in registers for the whole loop.
+// Elements of one colour share no global point, so the order in which the
+// chunks run does not change any sum: results equal the one-pass kernel's.
+
+template <int NC>
+struct ChunkRegs {
+  int g;
+  float xix, xiz, gax, gaz, jac, c0, c1;
+  float u[NC], acc[NC];
+  int bs, src;
+  bool act;
+};
+
+template <int NC>
+__device__ __forceinline__ void chunk_fetch_static(const MedArgs &A, int e, int q, ChunkRegs<NC> &R) {
+  R.act = e < A.e1;
+  const size_t p = size_t(R.act ? e : A.e0) * NP + q;
+  R.g = R.act ? __ldg(A.ibool + p) : 0;
+  R.xix = __ldg(A.xix + p); R.xiz = __ldg(A.xiz + p);
+  R.gax = __ldg(A.gax + p); R.gaz = __ldg(A.gaz + p); R.jac = __ldg(A.jac + p);
+  R.c0 = __ldg(A.prop0 + p); R.c1 = __ldg(A.prop1 + p);
+  R.bs = R.act ? __ldg(A.bc_slot + e) : -1;
+  R.src = R.act ? __ldg(A.src_head + e) : -1;
+}
+
+template <int NC>
+__device__ __forceinline__ void chunk_fetch_fields(const MedArgs &A, ChunkRegs<NC> &R) {
+  if (NC == 2) {
+    const float2 t = R.act ? reinterpret_cast<const float2 *>(A.u)[R.g] : make_float2(0.f, 0.f);
+    const float2 r = R.act ? reinterpret_cast<const float2 *>(A.accum)[R.g] : make_float2(0.f, 0.f);
+    R.u[0] = t.x; R.u[NC - 1] = t.y; R.acc[0] = r.x; R.acc[NC - 1] = r.y;
+  } else {
+    R.u[0] = R.act ? A.u[R.g] : 0.f;
+    R.acc[0] = R.act ? A.accum[R.g] : 0.f;
+  }
+}
+
+__device__ __forceinline__ float dot5(const float *row, const float (&c)[NG]) {
+  const float4 a = *reinterpret_cast<const float4 *>(row);
+  float s = c[0] * a.x;
+  s = fmaf(c[1], a.y, s);
+  s = fmaf(c[2], a.z, s);
+  s = fmaf(c[3], a.w, s);
+  return fmaf(c[4], row[4], s);
+}
+
+// KIND 0 acoustic, 1 elastic SH, 2 elastic P-SV.
+template <int E, int KIND>
+__device__ __forceinline__ void stiffness_loop(const StiffArgs &S, const MedArgs &A, int chunk0,
+                                               int stride, float *sm, const float *shp,
+                                               const float *shpw, const float *sw) {
+  constexpr int NC = KIND == 2 ? 2 : 1;
+  constexpr int RS = 8;                     // padded row stride
+  constexpr int ARR = NG * RS;              // one 5x5 array, rows padded
+  const int nchunks = (A.e1 - A.e0 + E - 1) / E;
+  if (chunk0 >= nchunks) return;
+  const int tid = threadIdx.x;
+  const int le = tid / NP, q = tid - le * NP;
+  const int iz = q / NG, ix = q - iz * NG;
+  // per element: NC x {U, UT, F0, F1T}
+  float *base = sm + le * (NC * 4 * ARR);
+  float hx[NG], hz[NG], wx[NG], wz[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    hx[l] = shp[ix * NG + l];
+    hz[l] = shp[iz * NG + l];
+    wx[l] = shpw[l * NG + ix];
+    wz[l] = shpw[l * NG + iz];
+  }
+  const float wiz = sw[iz], wix = sw[ix];
+  ChunkRegs<NC> cur, nxt;
+  nxt.act = false;
+  chunk_fetch_static<NC>(A, A.e0 + chunk0 * E + le, q, cur);
+  chunk_fetch_fields<NC>(A, cur);
+  for (int chunk = chunk0; chunk < nchunks; chunk += stride) {
+    const int e = A.e0 + chunk * E + le;
+    const bool more = chunk + stride < nchunks;
+    if (more) chunk_fetch_static<NC>(A, A.e0 + (chunk + stride) * E + le, q, nxt);
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      base[(c * 4 + 0) * ARR + iz * RS + ix] = cur.u[c];
+      base[(c * 4 + 1) * ARR + ix * RS + iz] = cur.u[c];
+    }
+    __syncthreads();
+    float Sx[NC], Sz[NC];
+    {
+      float dxi[NC], dga[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        dxi[c] = dot5(base + (c * 4 + 0) * ARR + iz * RS, hx);
+        dga[c] = dot5(base + (c * 4 + 1) * ARR + ix * RS, hz);
+      }
+      if (KIND == 2) {
+        const float du00 = cur.xix * dxi[0] + cur.gax * dga[0];
+        const float du01 = cur.xiz * dxi[0] + cur.gaz * dga[0];
+        const float du10 = cur.xix * dxi[NC - 1] + cur.gax * dga[NC - 1];
+        const float du11 = cur.xiz * dxi[NC - 1] + cur.gaz * dga[NC - 1];
+        const float lam = cur.c0 - 2.f * cur.c1;
+        const float sxx = cur.c0 * du00 + lam * du11;
+        const float szz = cur.c0 * du11 + lam * du00;
+        const float sxz = cur.c1 * (du01 + du10);
+        Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
+      } else {
+        // acoustic: rho^-1 grad chi (c0 = 1/rho); SH: mu grad u_y (c1 = mu)
+        const float k = KIND == 0 ? cur.c0 : cur.c1;
+        Sx[0] = k * (cur.xix * dxi[0] + cur.gax * dga[0]);
+        Sz[0] = k * (cur.xiz * dxi[0] + cur.gaz * dga[0]);
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      base[(c * 4 + 2) * ARR + iz * RS + ix] = cur.jac * (Sx[c] * cur.xix + Sz[c] * cur.xiz);
+      base[(c * 4 + 3) * ARR + ix * RS + iz] = cur.jac * (Sx[c] * cur.gax + Sz[c] * cur.gaz);
+    }
+    if (more) chunk_fetch_fields<NC>(A, nxt);
+    __syncthreads();
+    if (cur.act) {
+      float a[NC];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float t1 = dot5(base + (c * 4 + 2) * ARR + iz * RS, wx);
+        const float t2 = dot5(base + (c * 4 + 3) * ARR + ix * RS, wz);
+        a[c] = -(wiz * t1 + wix * t2);
+      }
+      if (cur.bs >= 0) {
+        const size_t k = size_t(cur.bs) * NP + q;
+        const float wq = A.bc_w[k];
+        if (KIND == 2) {
+          if (wq != 0.f) {
+            const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
+            const float2 vv = reinterpret_cast<const float2 *>(A.v)[cur.g];
+            const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+            const float vn = vv.x * nx + vv.y * nz;
+            const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vv.x * rvs;
+            const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vv.y * rvs;
+            a[0] += -1.f * fx * j1 * wq;
+            a[NC - 1] += -1.f * fz * j1 * wq;
+          }
+        } else {
+          if (wq != 0.f) {
+            const float imp = KIND == 0 ? A.bc_imp0[k] : A.bc_imp1[k];
+            a[0] += -1.f * (wq * A.bc_j1[k]) * imp * A.v[cur.g];
+          }
+          if (KIND == 0) a[0] *= A.bc_keep[k];
+        }
+      }
+      if (cur.src >= 0) {
+        const int step = *S.step;
+        for (int s = cur.src; s >= 0; s = S.src_next[s]) {
+          const float f = step < S.nstep ? S.stf[size_t(step) * S.nsrc + s] : 0.f;
+#pragma unroll
+          for (int c = 0; c < NC; ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
+        }
+      }
+      if (NC == 2) {
+        reinterpret_cast<float2 *>(A.accum)[cur.g] =
+            make_float2(cur.acc[0] + a[0], cur.acc[NC - 1] + a[NC - 1]);
+      } else {
+        A.accum[cur.g] = cur.acc[0] + a[0];
+      }
+    }
+    (void)e;
+    cur = nxt;
+  }
+}
+
+template <int E, int EK>
+__global__ void __launch_bounds__(NP * E) k_stiffness_persistent(StiffArgs S) {
+  // largest need: P-SV, 2 components x 4 padded arrays of 40 floats per element
+  __shared__ __align__(16) float sm[E * 2 * 4 * NG * 8];
+  __shared__ float shp[NP], shpw[NP], sw[NG];
+  load_quad(S.quad, shp, shpw, sw, threadIdx.x);
+  __syncthreads();
+  if (int(blockIdx.x) < S.el.nblocks) {
+    if (EK == 0) stiffness_loop<E, 2>(S, S.el, blockIdx.x, S.el.nblocks, sm, shp, shpw, sw);
+    else stiffness_loop<E, 1>(S, S.el, blockIdx.x, S.el.nblocks, sm, shp, shpw, sw);
+  } else {
+    stiffness_loop<E, 0>(S, S.ac, blockIdx.x - S.el.nblocks, S.ac.nblocks, sm, shp, shpw, sw);
+  }
+}
+
 struct UpdateArgs {
   float *__restrict__ u, *__restrict__ v, *__restrict__ accum;
   const float *__restrict__ minv;

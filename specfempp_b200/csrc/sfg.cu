@@ -100,6 +100,9 @@ struct sfg_handle {
   int *d_step = nullptr, *d_flag = nullptr;
   int host_step = 0;
   int epb = 16;
+  int variant = 1;           // 1 one-pass element kernel, 2 persistent
+  int sm_count = 148;
+  int resident[2][3] = {{0}};  // persistent: resident blocks per SM [EK][E index]
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr, graph_e = nullptr;
   int graph_steps = 0;
@@ -192,22 +195,46 @@ void launch_stiffness_E(sfg_handle *h, cudaStream_t s) {
   S.nstep = h->asmb.nstep;
   S.step = h->d_step;
   S.quad = h->quad;
+  const bool persistent = h->variant == 2;
+  int capacity = 0;
+  if (persistent) {
+    const int ei = E == 8 ? 0 : (E == 16 ? 1 : 2);
+    int &nb = h->resident[EK][ei];
+    if (nb == 0) {
+      SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &nb, sfg::dev::k_stiffness_persistent<E, EK>, sfg::dev::NP * E, 0));
+      nb = std::max(nb, 1);
+    }
+    capacity = nb * h->sm_count;
+  }
   const int nc = std::max(ncolors(h->el), ncolors(h->ac));
   for (int c = 0; c < nc; ++c) {
-    auto range = [&](const DevMedium &D, sfg::dev::MedArgs &A) {
-      A.e0 = A.e1 = 0;
-      A.nblocks = 0;
-      if (c < ncolors(D)) {
-        A.e0 = D.color_start[c];
-        A.e1 = D.color_start[c + 1];
-        A.nblocks = (A.e1 - A.e0 + E - 1) / E;
+    int chunks[2] = {0, 0};
+    sfg::dev::MedArgs *M[2] = {&S.el, &S.ac};
+    const DevMedium *D[2] = {&h->el, &h->ac};
+    for (int k = 0; k < 2; ++k) {
+      M[k]->e0 = M[k]->e1 = 0;
+      if (c < ncolors(*D[k])) {
+        M[k]->e0 = D[k]->color_start[c];
+        M[k]->e1 = D[k]->color_start[c + 1];
+        chunks[k] = (M[k]->e1 - M[k]->e0 + E - 1) / E;
       }
-    };
-    range(h->el, S.el);
-    range(h->ac, S.ac);
+      M[k]->nblocks = chunks[k];
+    }
+    if (chunks[0] + chunks[1] == 0) continue;
+    if (persistent && chunks[0] + chunks[1] > capacity) {
+      // split the resident blocks between the media in proportion to their work
+      int bel = chunks[0] == 0 ? 0
+                : std::max(1, int(double(capacity) * chunks[0] / (chunks[0] + chunks[1]) + 0.5));
+      if (chunks[1] > 0) bel = std::min(bel, capacity - 1);
+      S.el.nblocks = std::min(bel, chunks[0]);
+      S.ac.nblocks = std::min(capacity - S.el.nblocks, chunks[1]);
+    }
     const int grid = S.el.nblocks + S.ac.nblocks;
-    if (grid == 0) continue;
-    sfg::dev::k_stiffness<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
+    if (persistent)
+      sfg::dev::k_stiffness_persistent<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
+    else
+      sfg::dev::k_stiffness<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
   }
 }
 
@@ -223,6 +250,45 @@ void launch_stiffness(sfg_handle *h, cudaStream_t s) {
     case 32: launch_stiffness_W<32>(h, s); break;
     default: launch_stiffness_W<16>(h, s); break;
   }
+}
+
+// Element-kernel autotuner: every (variant, elements per block) candidate
+// gives bit-identical results (a colour's elements share no point), so the
+// fastest one measured on this mesh is kept.  Runs on scratch accumulators at
+// sfg_initialize, before the step graphs are captured.
+void autotune(sfg_handle *h) {
+  const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
+                     h->opt.elements_per_block == 32;
+  const bool fix_v = h->opt.kernel_variant == 1 || h->opt.kernel_variant == 2;
+  if (fix_e) h->epb = h->opt.elements_per_block;
+  if (fix_v) h->variant = h->opt.kernel_variant;
+  if (fix_e && fix_v) return;
+  std::vector<std::pair<int, int>> cand;
+  for (int v : {1, 2})
+    for (int e : {8, 16, 32})
+      if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
+  float best = 1e30f;
+  std::pair<int, int> pick = cand.front();
+  for (auto [v, e] : cand) {
+    h->variant = v;
+    h->epb = e;
+    for (int i = 0; i < 2; ++i) launch_stiffness(h, h->stream);
+    SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+    const int reps = 5;
+    for (int i = 0; i < reps; ++i) launch_stiffness(h, h->stream);
+    SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+    SFG_CUDA(cudaEventSynchronize(h->ev1));
+    SFG_CUDA(cudaGetLastError());
+    float t = 0;
+    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    if (t < best) { best = t; pick = {v, e}; }
+  }
+  h->variant = pick.first;
+  h->epb = pick.second;
+  // the tuning launches added into the accumulators: clear them
+  for (DevMedium *D : {&h->el, &h->ac})
+    if (D->nspec) SFG_CUDA(cudaMemsetAsync(D->accum, 0, (size_t(D->nglob) * D->ncomp + 4) * sizeof(float), h->stream));
+  SFG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 sfg::dev::UpdateArgs update_args(sfg_handle *h, int medium, bool predict, bool advance) {
@@ -373,7 +439,7 @@ sfg_handle *make_handle(const sfg_options *opt) {
   }
   if (h->opt.nstep_between_samples <= 0) h->opt.nstep_between_samples = 1;
   if (h->opt.steps_per_graph <= 0) h->opt.steps_per_graph = 20;
-  h->epb = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 32 ? h->opt.elements_per_block : 16;
+  h->epb = 16;
   return h;
 }
 
@@ -558,6 +624,12 @@ int sfg_initialize(sfg_handle *h) {
     h->d_step = h->mem.zeros<int>(1);
     h->d_flag = h->mem.zeros<int>(1);
     SFG_CUDA(cudaDeviceSynchronize());
+    {
+      int dev = 0;
+      SFG_CUDA(cudaGetDevice(&dev));
+      SFG_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    }
+    autotune(h);
     h->graph_steps = std::max(1, h->opt.steps_per_graph);
     h->graph_k = capture(h, h->graph_steps, true);
     h->graph_1 = capture(h, 1, true);
@@ -758,6 +830,8 @@ int sfg_get_info(const sfg_handle *h, sfg_info *info) {
   info->t0 = a.t0;
   info->device_bytes = h->mem.bytes;
   info->kernels_per_step = h->initialized ? kernels_per_step(h) : 0;
+  info->elements_per_block = h->epb;
+  info->kernel_variant = h->variant;
   return SFG_OK;
 }
 

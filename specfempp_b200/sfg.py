@@ -44,7 +44,8 @@ class MeshDesc(C.Structure):
 class Options(C.Structure):
     _fields_ = [("dt", C.c_double), ("nstep", C.c_int), ("nshots", C.c_int),
                 ("nstep_between_samples", C.c_int), ("steps_per_graph", C.c_int),
-                ("elements_per_block", C.c_int), ("store_acceleration", C.c_int)]
+                ("elements_per_block", C.c_int), ("kernel_variant", C.c_int),
+                ("store_acceleration", C.c_int)]
 
 
 class Source2D(C.Structure):
@@ -59,7 +60,8 @@ class Info(C.Structure):
                 ("ncolors_elastic", C.c_int), ("ncolors_acoustic", C.c_int),
                 ("nshots", C.c_int), ("nsig", C.c_int), ("nrec", C.c_int), ("ntypes", C.c_int),
                 ("nstep", C.c_int), ("istep", C.c_int), ("t0", C.c_double),
-                ("device_bytes", C.c_size_t), ("kernels_per_step", C.c_int)]
+                ("device_bytes", C.c_size_t), ("kernels_per_step", C.c_int),
+                ("elements_per_block", C.c_int), ("kernel_variant", C.c_int)]
 
 
 EXPORTS = {
@@ -139,12 +141,13 @@ class Simulation2D:
     def __init__(self, mesh=None, *, database: str | None = None, dt: float, nstep: int,
                  nstep_between_samples: int = 1, elastic_wave: str = "psv",
                  point_rho=None, point_vp=None, point_vs=None, steps_per_graph: int = 0,
-                 elements_per_block: int = 0, store_acceleration: bool = False):
+                 elements_per_block: int = 0, kernel_variant: int = 0,
+                 store_acceleration: bool = False):
         self.lib = load_library()
         self._keep = []
         opt = Options(dt=dt, nstep=nstep, nshots=1, nstep_between_samples=nstep_between_samples,
                       steps_per_graph=steps_per_graph, elements_per_block=elements_per_block,
-                      store_acceleration=int(store_acceleration))
+                      kernel_variant=kernel_variant, store_acceleration=int(store_acceleration))
         h = C.c_void_p()
         wave = 1 if elastic_wave.lower() == "sh" else 0
         if database is not None:

@@ -79,13 +79,13 @@ def sfg_lib():
     return sfg.load_library()
 
 
-def product_run(case, types=("displacement",), nsteps=None, epb=0, spg=0):
+def product_run(case, types=("displacement",), nsteps=None, epb=0, spg=0, variant=0):
     """Run the CUDA path (libsfg through the C ABI) on an oracle Case2D."""
     from specfempp_b200 import sfg
     sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=case.nstep,
                            nstep_between_samples=case.nstep_between_samples,
                            point_rho=case.point_rho, point_vp=case.point_vp, point_vs=case.point_vs,
-                           elements_per_block=epb, steps_per_graph=spg)
+                           elements_per_block=epb, steps_per_graph=spg, kernel_variant=variant)
     sim.set_sources(case.sources)
     sim.set_receivers(case.rec_x, case.rec_z, case.rec_angle, types)
     sim.initialize()

@@ -101,15 +101,16 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
 
 
-@pytest.mark.parametrize("epb,spg", [(8, 7), (32, 1)])
-def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg):
+@pytest.mark.parametrize("epb,spg,variant", [(8, 7, 1), (32, 1, 1), (8, 3, 2), (16, 20, 2), (32, 5, 2)])
+def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg, variant):
     from specfempp_b200 import meshgen
     w = meshgen.coupled_400x200(nstep=120, nx=40, nz=20)
     case = workload_case(w)
-    _, a = product_run(case)
-    _, b = product_run(case, epb=epb, spg=spg)
-    # a different block shape changes no summation order: bitwise equal
-    assert np.array_equal(a, b)
+    _, a = product_run(case, epb=16, variant=1)
+    _, b = product_run(case, epb=epb, spg=spg, variant=variant)
+    # a different block shape or element order inside a colour changes no
+    # summation order: bitwise equal
+    assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
 
 
 def test_deterministic(sfg_lib):
