@@ -184,16 +184,17 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
 int ncolors(const DevMedium &D) { return D.nspec ? int(D.color_start.size()) - 1 : 0; }
 
 template <int E, int EK>
-void launch_stiffness_E(sfg_handle *h, cudaStream_t s) {
+void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
+                        cudaStream_t s) {
   sfg::dev::StiffArgs S{};
-  S.el = med_args(h->el);
-  S.ac = med_args(h->ac);
+  S.el = med_args(el);
+  S.ac = med_args(ac);
   S.src_next = h->d_src_next;
   S.src_arr = h->d_src_arr;
   S.stf = h->d_stf;
   S.nsrc = h->asmb.nsrc;
   S.nstep = h->asmb.nstep;
-  S.step = h->d_step;
+  S.step = step;
   S.quad = h->quad;
   const bool persistent = h->variant == 2;
   int capacity = 0;
@@ -207,11 +208,11 @@ void launch_stiffness_E(sfg_handle *h, cudaStream_t s) {
     }
     capacity = nb * h->sm_count;
   }
-  const int nc = std::max(ncolors(h->el), ncolors(h->ac));
+  const int nc = std::max(ncolors(el), ncolors(ac));
   for (int c = 0; c < nc; ++c) {
     int chunks[2] = {0, 0};
     sfg::dev::MedArgs *M[2] = {&S.el, &S.ac};
-    const DevMedium *D[2] = {&h->el, &h->ac};
+    const DevMedium *D[2] = {&el, &ac};
     for (int k = 0; k < 2; ++k) {
       M[k]->e0 = M[k]->e1 = 0;
       if (c < ncolors(*D[k])) {
@@ -239,18 +240,22 @@ void launch_stiffness_E(sfg_handle *h, cudaStream_t s) {
 }
 
 template <int E>
-void launch_stiffness_W(sfg_handle *h, cudaStream_t s) {
-  if (h->el.ncomp == 1) launch_stiffness_E<E, 1>(h, s);
-  else launch_stiffness_E<E, 0>(h, s);
+void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
+                        cudaStream_t s) {
+  if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s);
+  else launch_stiffness_E<E, 0>(h, el, ac, step, s);
 }
 
-void launch_stiffness(sfg_handle *h, cudaStream_t s) {
+void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
+                      cudaStream_t s) {
   switch (h->epb) {
-    case 8: launch_stiffness_W<8>(h, s); break;
-    case 32: launch_stiffness_W<32>(h, s); break;
-    default: launch_stiffness_W<16>(h, s); break;
+    case 8: launch_stiffness_W<8>(h, el, ac, step, s); break;
+    case 32: launch_stiffness_W<32>(h, el, ac, step, s); break;
+    default: launch_stiffness_W<16>(h, el, ac, step, s); break;
   }
 }
+
+void launch_stiffness(sfg_handle *h, cudaStream_t s) { launch_stiffness(h, h->el, h->ac, h->d_step, s); }
 
 // Element-kernel autotuner: every (variant, elements per block) candidate
 // gives bit-identical results (a colour's elements share no point), so the
@@ -291,9 +296,8 @@ void autotune(sfg_handle *h) {
   SFG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
-sfg::dev::UpdateArgs update_args(sfg_handle *h, int medium, bool predict, bool advance) {
-  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
-  DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
+sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMedium &O, int medium,
+                                 bool predict, bool advance) {
   sfg::dev::UpdateArgs U{};
   U.u = D.u; U.v = D.v; U.accum = D.accum; U.minv = D.minv;
   // acoustic chi_dd feeds the elastic coupling term; the last step of a run
@@ -333,7 +337,7 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.xix = D.xix; R.xiz = D.xiz; R.gax = D.gax; R.gaz = D.gaz; R.prop0 = D.prop0;
   R.prop1 = D.prop1;
   R.u = D.u; R.v = D.v; R.accum = D.accum; R.minv = D.minv;
-  R.cpl = update_args(h, medium, true, false);
+  R.cpl = update_args(h, D, medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el, medium, true, false);
   R.ncomp = D.ncomp;
   R.acoustic = medium == SFG_MEDIUM_ACOUSTIC;
   R.ntypes = h->asmb.ntypes;
@@ -349,17 +353,22 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
 }
 
 void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaStream_t s) {
-  sfg::dev::UpdateArgs U = update_args(h, medium, predict, advance);
+  const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+  const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
+  sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
   sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
 }
 
-void launch_predict(sfg_handle *h, cudaStream_t s) {
+void launch_predict_medium(sfg_handle *h, const DevMedium &D, cudaStream_t s) {
+  if (!D.nspec) return;
   const float dt = float(h->asmb.dt);
-  for (DevMedium *D : {&h->ac, &h->el}) {
-    if (!D->nspec) continue;
-    const int n = D->nglob * D->ncomp;
-    sfg::dev::k_predict<<<grid_for(n), 256, 0, s>>>(D->u, D->v, D->a, n, dt, dt / 2.0f, dt * dt / 2.0f);
-  }
+  const int n = D.nglob * D.ncomp;
+  sfg::dev::k_predict<<<grid_for(n), 256, 0, s>>>(D.u, D.v, D.a, n, dt, dt / 2.0f, dt * dt / 2.0f);
+}
+
+void launch_predict(sfg_handle *h, cudaStream_t s) {
+  launch_predict_medium(h, h->ac, s);
+  launch_predict_medium(h, h->el, s);
 }
 
 // One time step in the reference's medium order (time_marching.tpp:33-83):
