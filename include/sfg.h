@@ -167,6 +167,28 @@ int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *glob_to_elastic,
 /* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
 int sfg_check_finite(sfg_handle *h);
 
+/* One time step of the handle's elastic model on device buffers the caller
+ * owns, with no device memory allocated by the call.  This entry point has no
+ * counterpart in the reference.  It is for callers that cannot call
+ * cudaMalloc while they step: a host framework that owns and budgets all
+ * device memory itself (as the reference's Kokkos runtime does), or a time
+ * loop that runs after the device memory has been sized and frozen.  The
+ * handle must be initialised (that is where its read-only mesh arrays were
+ * uploaded) and hold a single elastic medium.  u, v, a are the displacement,
+ * velocity and acceleration in the handle's elastic point numbering
+ * ([nglob_elastic][ncomp] floats on the handle's device), in the end-of-step
+ * state that sfg_step leaves; the call applies the predictor, the element
+ * kernel and the corrector exactly as sfg_step does and writes the new state
+ * back into u, v, a, using source-time values of step istep.  The element
+ * kernel's accumulator lives in a fixed array inside the library, limited to
+ * 4,194,304 point values (2,097,152 two-component points); larger models are
+ * rejected with SFG_ERR_ARG.  All calls share that array (it is cleared at
+ * the start of every call), so calls that overlap on the GPU race.  The first
+ * call on a device looks up the array's device address; make that first call
+ * before any stream capture.  The handle's own fields and step count are not
+ * touched; the call returns after the step has finished on the GPU. */
+int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a);
+
 #ifdef __cplusplus
 }
 #endif

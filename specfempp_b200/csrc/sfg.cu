@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -460,6 +461,49 @@ void finish_create(sfg_handle *h) {
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
 }
 
+// ---------------------------------------------------------------------------
+// Scratch of sfg_step_noalloc.  The element kernel adds every element's
+// contribution into an accumulator that is neither an input nor an output of
+// a time step; the handle-based path allocates it with cudaMalloc at
+// sfg_initialize.  sfg_step_noalloc uses this fixed array instead, so that it
+// allocates nothing.  It is sized for NOALLOC_MAX_VALUES floats (one per point
+// component: 2,097,152 two-component points) plus the 4-float tail the float4
+// update reads, and every GPU that loads the library holds it (16 MiB) until
+// the process exits.  Every call shares it: the accumulator is cleared at the
+// start of each call, and calls that overlap on the GPU race on it.
+constexpr size_t NOALLOC_MAX_VALUES = size_t(1) << 22;
+static __device__ __align__(256) float g_noalloc_accum[NOALLOC_MAX_VALUES + 4];
+static __device__ __align__(256) int g_noalloc_words[4];  // [0] step index, [1] non-finite flag
+
+struct NoallocDevice {
+  float *accum = nullptr;
+  int *words = nullptr;
+};
+
+// Device addresses of the scratch, looked up once per device with that device
+// current (a __device__ symbol's host-side name is not a device address).
+int noalloc_device(NoallocDevice &out, std::string &err) {
+  static std::mutex mu;
+  static std::vector<NoallocDevice> table;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) { err = cudaGetErrorString(e); return SFG_ERR_CUDA; }
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev >= int(table.size())) table.resize(dev + 1);
+  NoallocDevice &d = table[dev];
+  if (!d.accum) {
+    void *pa = nullptr, *pw = nullptr;
+    e = cudaGetSymbolAddress(&pa, g_noalloc_accum);
+    if (e != cudaSuccess) { err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return SFG_ERR_CUDA; }
+    e = cudaGetSymbolAddress(&pw, g_noalloc_words);
+    if (e != cudaSuccess) { err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e); return SFG_ERR_CUDA; }
+    d.accum = static_cast<float *>(pa);
+    d.words = static_cast<int *>(pw);
+  }
+  out = d;
+  return SFG_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -898,6 +942,47 @@ int sfg_check_finite(sfg_handle *h) {
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SFG_ERR_CUDA;
   if (cudaMemcpy(&f, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SFG_ERR_CUDA;
   return f ? SFG_ERR_NONFINITE : 0;
+}
+
+int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (h->ac.nspec != 0 || h->el.nspec == 0) {
+      h->err = "sfg_step_noalloc advances single-medium elastic models only";
+      return int(SFG_ERR_UNSUPPORTED);
+    }
+    if (!u || !v || !a || istep < 0) { h->err = "null field pointer or negative step"; return int(SFG_ERR_ARG); }
+    const size_t n = size_t(h->el.nglob) * h->el.ncomp;
+    if (n > NOALLOC_MAX_VALUES) {
+      h->err = "sfg_step_noalloc: the model has " + std::to_string(n) +
+               " point values, above the fixed scratch of " + std::to_string(NOALLOC_MAX_VALUES);
+      return int(SFG_ERR_ARG);
+    }
+    NoallocDevice nd;
+    const int rc = noalloc_device(nd, h->err);
+    if (rc != SFG_OK) return rc;
+    cudaStream_t s = h->stream;
+    // the caller's fields replace the handle's, the fixed array its accumulator
+    DevMedium el = h->el;
+    el.u = u;
+    el.v = v;
+    el.a = a;
+    el.accum = nd.accum;
+    SFG_CUDA(cudaMemsetAsync(nd.accum, 0, (n + 4) * sizeof(float), s));
+    const int words[2] = {istep, 0};
+    SFG_CUDA(cudaMemcpyAsync(nd.words, words, sizeof(words), cudaMemcpyHostToDevice, s));
+    // predictor, element launches, corrector: the kernels of sfg_step
+    launch_predict_medium(h, el, s);
+    launch_stiffness(h, el, h->ac, nd.words, s);
+    sfg::dev::UpdateArgs U = update_args(h, el, h->ac, SFG_MEDIUM_ELASTIC, false, false);
+    U.a_store = a;
+    U.flag = nd.words + 1;
+    U.step = nd.words;
+    sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
+    SFG_CUDA(cudaGetLastError());
+    SFG_CUDA(cudaStreamSynchronize(s));
+    return int(SFG_OK);
+  });
 }
 
 }  // extern "C"

@@ -86,6 +86,7 @@ EXPORTS = {
     "sfg_get_field": ([C.c_void_p, C.c_int, C.c_int, _fp, C.c_size_t], C.c_int),
     "sfg_get_numbering": ([C.c_void_p, _ip, _ip, _ip], C.c_int),
     "sfg_check_finite": ([C.c_void_p], C.c_int),
+    "sfg_step_noalloc": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }
 
 _lib = None
