@@ -606,36 +606,99 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
 // Closest GLL point, then Newton iterations from the element centre in that
 // element and its corner-sharing neighbours; the candidate whose mapped point
 // is closest wins (src/algorithms/dim2/locate_point_impl.cpp).
-// A point on an edge or corner shared by several elements goes to the first
-// element in mesh order: a candidate replaces the current choice only when it
-// is closer by more than 1e-9 of the mesh extent.
-bool locate_point2d(const Mesh2D &m, const Assembly2D &a, double x, double z, int &ispec,
-                    double &xi, double &gamma) {
-  const size_t nloc = a.gx.size();
+namespace {
+
+void build_locate_index(const Mesh2D &m, Assembly2D &a) {
+  Assembly2D::LocateIndex &L = a.loc;
   double xmin = 1e300, xmax = -1e300, zmin = 1e300, zmax = -1e300;
   for (int i = 0; i < m.npgeo; ++i) {
     xmin = std::min(xmin, m.coorg[2 * i]); xmax = std::max(xmax, m.coorg[2 * i]);
     zmin = std::min(zmin, m.coorg[2 * i + 1]); zmax = std::max(zmax, m.coorg[2 * i + 1]);
   }
-  const double tol = 1e-9 * std::max(xmax - xmin, zmax - zmin);
+  L.tol = 1e-9 * std::max(xmax - xmin, zmax - zmin);
+  // cell size: the largest element bounding-box extent, so the GLL point
+  // nearest to any point inside the mesh lies in the 3x3 cells around it
+  double h = 0;
+  for (int e = 0; e < m.nspec; ++e) {
+    double ex0 = 1e300, ex1 = -1e300, ez0 = 1e300, ez1 = -1e300;
+    for (int k = 0; k < m.ngnod; ++k) {
+      const int id = m.knods[size_t(e) * m.ngnod + k];
+      ex0 = std::min(ex0, m.coorg[2 * id]); ex1 = std::max(ex1, m.coorg[2 * id]);
+      ez0 = std::min(ez0, m.coorg[2 * id + 1]); ez1 = std::max(ez1, m.coorg[2 * id + 1]);
+    }
+    h = std::max(h, std::max(ex1 - ex0, ez1 - ez0));
+  }
+  L.h = h > 0 ? h : 1.0;
+  L.x0 = xmin;
+  L.z0 = zmin;
+  L.nx = int((xmax - xmin) / L.h) + 1;
+  L.nz = int((zmax - zmin) / L.h) + 1;
+  const size_t ncell = size_t(L.nx) * L.nz;
+  auto cell_of = [&](double x, double z) {
+    int cx = std::min(std::max(int((x - L.x0) / L.h), 0), L.nx - 1);
+    int cz = std::min(std::max(int((z - L.z0) / L.h), 0), L.nz - 1);
+    return size_t(cz) * L.nx + cx;
+  };
+  L.cell_start.assign(ncell + 1, 0);
+  for (size_t p = 0; p < a.gx.size(); ++p) ++L.cell_start[cell_of(a.gx[p], a.gz[p]) + 1];
+  for (size_t c = 0; c < ncell; ++c) L.cell_start[c + 1] += L.cell_start[c];
+  L.cell_pts.resize(a.gx.size());
+  std::vector<int> fill(L.cell_start.begin(), L.cell_start.end() - 1);
+  for (size_t p = 0; p < a.gx.size(); ++p) L.cell_pts[fill[cell_of(a.gx[p], a.gz[p])]++] = int(p);
+  L.node_start.assign(m.npgeo + 1, 0);
+  for (int e = 0; e < m.nspec; ++e)
+    for (int k = 0; k < 4; ++k) ++L.node_start[m.knods[size_t(e) * m.ngnod + k] + 1];
+  for (int i = 0; i < m.npgeo; ++i) L.node_start[i + 1] += L.node_start[i];
+  L.node_elems.resize(L.node_start[m.npgeo]);
+  std::vector<int> nf(L.node_start.begin(), L.node_start.end() - 1);
+  for (int e = 0; e < m.nspec; ++e)
+    for (int k = 0; k < 4; ++k) L.node_elems[nf[m.knods[size_t(e) * m.ngnod + k]]++] = e;
+  L.built = true;
+}
+
+}  // namespace
+
+// Closest GLL point, then Newton iterations from the element centre in that
+// element and its corner-sharing neighbours; the candidate whose mapped point
+// is closest wins (src/algorithms/dim2/locate_point_impl.cpp).  A point on an
+// edge or corner shared by several elements goes to the first element in mesh
+// order: a candidate replaces the current choice only when it is closer by
+// more than 1e-9 of the mesh extent.  Candidates are scanned in mesh order;
+// the grid index only narrows the scan.
+bool locate_point2d(const Mesh2D &m, Assembly2D &a, double x, double z, int &ispec, double &xi,
+                    double &gamma) {
+  if (!a.loc.built) build_locate_index(m, a);
+  const Assembly2D::LocateIndex &L = a.loc;
+  const double tol = L.tol;
+  std::vector<int> pts;
+  const int cx = int(std::floor((x - L.x0) / L.h)), cz = int(std::floor((z - L.z0) / L.h));
+  for (int jz = cz - 1; jz <= cz + 1; ++jz)
+    for (int jx = cx - 1; jx <= cx + 1; ++jx) {
+      if (jx < 0 || jz < 0 || jx >= L.nx || jz >= L.nz) continue;
+      const size_t c = size_t(jz) * L.nx + jx;
+      pts.insert(pts.end(), L.cell_pts.begin() + L.cell_start[c], L.cell_pts.begin() + L.cell_start[c + 1]);
+    }
+  if (pts.empty()) {  // outside the gridded area: scan everything
+    pts.resize(a.gx.size());
+    std::iota(pts.begin(), pts.end(), 0);
+  }
+  std::sort(pts.begin(), pts.end());
   double best = 1e300;
   size_t pb = 0;
-  for (size_t p = 0; p < nloc; ++p) {
+  for (int p : pts) {
     const double d = std::sqrt((a.gx[p] - x) * (a.gx[p] - x) + (a.gz[p] - z) * (a.gz[p] - z));
-    if (d < best - tol) { best = d; pb = p; }
+    if (d < best - tol) { best = d; pb = size_t(p); }
   }
   const int eg = int(pb / NPTS);
-  std::vector<int> cand{eg};
-  const int *kg = &m.knods[size_t(eg) * m.ngnod];
-  for (int e = 0; e < m.nspec; ++e) {
-    if (e == eg) continue;
-    const int *ke = &m.knods[size_t(e) * m.ngnod];
-    bool share = false;
-    for (int i = 0; i < 4 && !share; ++i)
-      for (int j = 0; j < 4; ++j)
-        if (kg[i] == ke[j]) { share = true; break; }
-    if (share) cand.push_back(e);
+  std::vector<int> cand;
+  for (int k = 0; k < 4; ++k) {
+    const int node = m.knods[size_t(eg) * m.ngnod + k];
+    for (int i = L.node_start[node]; i < L.node_start[node + 1]; ++i)
+      if (L.node_elems[i] != eg) cand.push_back(L.node_elems[i]);
   }
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  cand.insert(cand.begin(), eg);
   double fd = 1e300;
   ispec = -1;
   for (int e : cand) {

@@ -86,6 +86,15 @@ struct Assembly2D {
   std::vector<int> rec_medium, rec_elem, types;
   std::vector<float> rec_h;           // [nrec][25]
   double rec_angle = 0;
+  // point-location index (built on first use): GLL points bucketed on a
+  // uniform grid, and the elements around every control node
+  struct LocateIndex {
+    bool built = false;
+    double x0 = 0, z0 = 0, h = 1, tol = 0;
+    int nx = 0, nz = 0;
+    std::vector<int> cell_start, cell_pts;    // CSR over cells -> local point
+    std::vector<int> node_start, node_elems;  // CSR over control nodes -> elements
+  } loc;
 };
 
 // Build everything but sources/receivers (numbering, geometry, colouring,
@@ -95,7 +104,7 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
 void set_receivers2d(const Mesh2D &m, Assembly2D &a, const std::vector<double> &x,
                      const std::vector<double> &z, double angle, const std::vector<int> &types);
 // locate a physical point: returns mesh element and (xi, gamma)
-bool locate_point2d(const Mesh2D &m, const Assembly2D &a, double x, double z, int &ispec,
+bool locate_point2d(const Mesh2D &m, Assembly2D &a, double x, double z, int &ispec,
                     double &xi, double &gamma);
 
 }  // namespace sfg

@@ -1,0 +1,216 @@
+// Batched-shot kernels of the 2D elastic time step (FP32).
+//
+// S independent shots (different sources, same mesh and model) advance in one
+// launch per colour.  Fields are [point][component][shot], so the 32 lanes of
+// a warp are 32 shots of one GLL point: the index, Jacobian and material
+// loads of a point are warp-uniform (one transaction serves all shots) and
+// the field loads are 128-byte coalesced.  A block is one element: 25 warps,
+// one per GLL point, over a tile of up to 32 shots.  The Lagrange
+// coefficients a warp needs are warp-uniform too and come from constant
+// memory.
+//
+// Per shot the arithmetic is the single-shot element kernel's, operation for
+// operation (same explicit FMAs in the contractions, everything else rounded
+// separately), so a batched run gives the same bits as S separate runs.
+// Reference: as kernels2d.cuh (compute_stiffness_interaction.tpp:140-247,
+// stacey.tpp:50-80, compute_source_interaction.tpp:17-104, newmark.tpp:10-128,
+// compute_seismogram.tpp:19-171).
+#pragma once
+
+#include "kernels2d.cuh"
+
+namespace sfg {
+namespace dev {
+
+__constant__ float c_hp[NP];    // hp[i*5+j] = l'_j(xi_i)
+__constant__ float c_hpw[NP];   // hp[l*5+i] * w[l]
+__constant__ float c_w[NG];
+
+struct BatchArgs {
+  const int *__restrict__ ibool;
+  const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
+      *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
+  const int *__restrict__ bc_slot;
+  const float *__restrict__ bc_w, *__restrict__ bc_nx, *__restrict__ bc_nz, *__restrict__ bc_j1,
+      *__restrict__ bc_imp0, *__restrict__ bc_imp1;
+  const int *__restrict__ src_head, *__restrict__ src_next, *__restrict__ src_shot;
+  const float *__restrict__ src_arr;   // [nsrc][2][25]
+  const float *__restrict__ stf;       // [nstep][nsrc]
+  int nsrc, nstep;
+  const int *__restrict__ step;
+  const float *__restrict__ u, *__restrict__ v;   // [nglob][NC][S]
+  float *__restrict__ accum;
+  int e0;                              // first element of the colour
+  int S;                               // shots
+};
+
+// grid: (elements of the colour, shot tiles of 32); block: 25 warps x 32 lanes.
+template <int NC>
+__global__ void __launch_bounds__(NP * 32) k_stiffness_batched(BatchArgs A) {
+  __shared__ float su[NC][NP][32];
+  __shared__ float sF[NC][2][NP][32];
+  const int q = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int shot = blockIdx.y * 32 + lane;
+  const bool act = shot < A.S;
+  const int e = A.e0 + blockIdx.x;
+  const size_t p = size_t(e) * NP + q;
+  const int iz = q / NG, ix = q - iz * NG;
+  const int g = __ldg(A.ibool + p);
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+  float uu[NC], acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const size_t k = (size_t(g) * NC + c) * A.S + shot;
+    uu[c] = act ? A.u[k] : 0.f;
+    acc[c] = act ? A.accum[k] : 0.f;
+    su[c][q][lane] = uu[c];
+  }
+  const int bs = __ldg(A.bc_slot + e);
+  const int src = __ldg(A.src_head + e);
+  __syncthreads();
+  float dxi[NC], dga[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    dxi[c] = 0.f;
+    dga[c] = 0.f;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      dxi[c] = fmaf(c_hp[ix * NG + l], su[c][iz * NG + l][lane], dxi[c]);
+      dga[c] = fmaf(c_hp[iz * NG + l], su[c][l * NG + ix][lane], dga[c]);
+    }
+  }
+  float Sx[NC], Sz[NC];
+  if (NC == 2) {
+    const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+    const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
+    const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+    const float lam = c0 - 2.f * mu;
+    const float sxx = c0 * du00 + lam * du11;
+    const float szz = c0 * du11 + lam * du00;
+    const float sxz = mu * (du01 + du10);
+    Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
+  } else {
+    Sx[0] = mu * (xix * dxi[0] + gax * dga[0]);
+    Sz[0] = mu * (xiz * dxi[0] + gaz * dga[0]);
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    sF[c][0][q][lane] = jac * (Sx[c] * xix + Sz[c] * xiz);
+    sF[c][1][q][lane] = jac * (Sx[c] * gax + Sz[c] * gaz);
+  }
+  __syncthreads();
+  if (!act) return;
+  float a[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      t1 = fmaf(sF[c][0][iz * NG + l][lane], c_hpw[l * NG + ix], t1);
+      t2 = fmaf(sF[c][1][l * NG + ix][lane], c_hpw[l * NG + iz], t2);
+    }
+    a[c] = -(c_w[iz] * t1 + c_w[ix] * t2);
+  }
+  if (bs >= 0) {
+    const size_t k = size_t(bs) * NP + q;
+    const float wq = A.bc_w[k];
+    if (wq != 0.f) {
+      const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
+      if (NC == 2) {
+        const float vx = A.v[(size_t(g) * NC) * A.S + shot];
+        const float vz = A.v[(size_t(g) * NC + NC - 1) * A.S + shot];
+        const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+        const float vn = vx * nx + vz * nz;
+        const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vx * rvs;
+        const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vz * rvs;
+        a[0] += -1.f * fx * j1 * wq;
+        a[NC - 1] += -1.f * fz * j1 * wq;
+      } else {
+        a[0] += -1.f * (wq * j1) * A.bc_imp1[k] * A.v[size_t(g) * A.S + shot];
+      }
+    }
+  }
+  if (src >= 0) {
+    const int step = *A.step;
+    for (int s = src; s >= 0; s = A.src_next[s]) {
+      if (A.src_shot[s] != shot) continue;
+      const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) a[c] += f * A.src_arr[(size_t(s) * 2 + c) * NP + q];
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) A.accum[(size_t(g) * NC + c) * A.S + shot] = acc[c] + a[c];
+}
+
+// a = accum * M^-1 (M^-1 shared by the shots); corrector; optional fused
+// predictor; accumulator clear.  Flat index i over [nglob][NC][S].
+__global__ void __launch_bounds__(256) k_update_batched(UpdateArgs A, int S) {
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+    const float a = __fmul_rn(A.accum[i], A.minv[i / S]);
+    float vv = newmark_correct(A.v[i], a, A.dt2);
+    float uu = A.u[i];
+    if (A.predict) newmark_predict(uu, vv, a, A.dt, A.dt2, A.dtsq2);
+    A.u[i] = uu;
+    A.v[i] = vv;
+    A.accum[i] = 0.f;
+    if (A.a_store) A.a_store[i] = a;
+    bad |= !isfinite(uu);
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
+// One block per receiver, lanes over shots (tiles of 32): displacement,
+// velocity (corrected) or acceleration interpolated with the receiver's
+// Lagrange weights.  seis is [S][nsig][ntypes][nrec][2].
+__global__ void __launch_bounds__(32) k_receivers_batched(RecArgs A, int S) {
+  const int step = *A.step;
+  if (step % A.nsb != 0) return;
+  const int isig = step / A.nsb;
+  if (isig >= A.nsig) return;
+  const int r = A.rec_list[blockIdx.x];
+  const int ce = A.rec_elem[r];
+  const int NC = A.ncomp;
+  for (int s0 = 0; s0 < S; s0 += 32) {
+    const int shot = s0 + threadIdx.x;
+    if (shot >= S) continue;
+    for (int t = 0; t < A.ntypes; ++t) {
+      float o[2] = {0.f, 0.f};
+      for (int c = 0; c < NC; ++c) {
+        // the 25 weighted values, summed in the order of the single-shot
+        // kernel's xor butterfly (lane i + lane i^o), so traces match it bitwise
+        float x[32];
+#pragma unroll
+        for (int q = 0; q < 32; ++q) x[q] = 0.f;
+        for (int q = 0; q < NP; ++q) {
+          const int g = A.ibool[size_t(ce) * NP + q];
+          const size_t k = (size_t(g) * NC + c) * S + shot;
+          const float acc = __fmul_rn(A.accum[k], A.minv[size_t(g) * NC + c]);
+          float val;
+          switch (A.types[t]) {
+            case 0: val = A.u[k]; break;
+            case 1: val = newmark_correct(A.v[k], acc, A.dt2); break;
+            default: val = acc; break;
+          }
+          x[q] = A.rec_h[size_t(r) * NP + q] * val;
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+          for (int i = 0; i < o; ++i) x[i] = x[i] + x[i + o];
+        o[c] = x[0];
+      }
+      float *dst = A.seis + (((size_t(shot) * A.nsig + isig) * A.ntypes + t) * A.nrec_total + r) * 2;
+      dst[0] = o[0];
+      dst[1] = NC > 1 ? o[1] : 0.f;
+    }
+  }
+}
+
+}  // namespace dev
+}  // namespace sfg

@@ -15,6 +15,7 @@
 #include "../../include/sfg.h"
 #include "host2d.hpp"
 #include "kernels2d.cuh"
+#include "kernels2d_batched.cuh"
 
 namespace {
 
@@ -64,6 +65,8 @@ struct DevMem {
 
 struct DevMedium {
   int nspec = 0, nglob = 0, ncomp = 0;
+  int S = 1;                       // shots sharing the mesh: fields are [point][comp][shot]
+  size_t values() const { return size_t(nglob) * ncomp * S; }
   std::vector<int> color_start;
   int *ibool = nullptr;
   float *xix = nullptr, *xiz = nullptr, *gax = nullptr, *gaz = nullptr, *jac = nullptr,
@@ -94,7 +97,7 @@ struct sfg_handle {
   int ext_stf_nsrc = 0;
   DevMem mem;
   DevMedium el, ac;
-  int *d_src_next = nullptr;
+  int *d_src_next = nullptr, *d_src_shot = nullptr;
   float *d_src_arr = nullptr, *d_stf = nullptr;
   int *d_rec_elem = nullptr;
   float *d_rec_h = nullptr, *d_seis = nullptr;
@@ -162,7 +165,8 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.niface = M.niface;
   D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
   D.minv = m.upload(M.minv);
-  const size_t n = size_t(M.nglob) * M.ncomp;
+  D.S = h->asmb.nshots;
+  const size_t n = D.values();
   // pad by 4 floats so float4 streaming never runs past an allocation
   D.u = m.zeros<float>(n + 4);
   D.v = m.zeros<float>(n + 4);
@@ -247,8 +251,35 @@ void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
   else launch_stiffness_E<E, 0>(h, el, ac, step, s);
 }
 
+void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *step, cudaStream_t s) {
+  sfg::dev::BatchArgs B{};
+  B.ibool = el.ibool;
+  B.xix = el.xix; B.xiz = el.xiz; B.gax = el.gax; B.gaz = el.gaz; B.jac = el.jac;
+  B.prop0 = el.prop0; B.prop1 = el.prop1;
+  B.bc_slot = el.bc_slot; B.bc_w = el.bc_w; B.bc_nx = el.bc_nx; B.bc_nz = el.bc_nz;
+  B.bc_j1 = el.bc_j1; B.bc_imp0 = el.bc_imp0; B.bc_imp1 = el.bc_imp1;
+  B.src_head = el.src_head; B.src_next = h->d_src_next; B.src_shot = h->d_src_shot;
+  B.src_arr = h->d_src_arr; B.stf = h->d_stf;
+  B.nsrc = h->asmb.nsrc; B.nstep = h->asmb.nstep;
+  B.step = step;
+  B.u = el.u; B.v = el.v; B.accum = el.accum;
+  B.S = el.S;
+  for (int c = 0; c < ncolors(el); ++c) {
+    B.e0 = el.color_start[c];
+    const int n = el.color_start[c + 1] - B.e0;
+    if (n <= 0) continue;
+    const dim3 grid(n, (el.S + 31) / 32);
+    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    else sfg::dev::k_stiffness_batched<1><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+  }
+}
+
 void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
                       cudaStream_t s) {
+  if (el.S > 1) {
+    launch_stiffness_batched(h, el, step, s);
+    return;
+  }
   switch (h->epb) {
     case 8: launch_stiffness_W<8>(h, el, ac, step, s); break;
     case 32: launch_stiffness_W<32>(h, el, ac, step, s); break;
@@ -268,7 +299,7 @@ void autotune(sfg_handle *h) {
   const bool fix_v = h->opt.kernel_variant == 1 || h->opt.kernel_variant == 2;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
-  if (fix_e && fix_v) return;
+  if ((fix_e && fix_v) || h->asmb.nshots > 1) return;  // batched shots: one launch shape
   std::vector<std::pair<int, int>> cand;
   for (int v : {1, 2})
     for (int e : {8, 16, 32})
@@ -293,7 +324,7 @@ void autotune(sfg_handle *h) {
   h->epb = pick.second;
   // the tuning launches added into the accumulators: clear them
   for (DevMedium *D : {&h->el, &h->ac})
-    if (D->nspec) SFG_CUDA(cudaMemsetAsync(D->accum, 0, (size_t(D->nglob) * D->ncomp + 4) * sizeof(float), h->stream));
+    if (D->nspec) SFG_CUDA(cudaMemsetAsync(D->accum, 0, (D->values() + 4) * sizeof(float), h->stream));
   SFG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
@@ -304,7 +335,7 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   // acoustic chi_dd feeds the elastic coupling term; the last step of a run
   // keeps the acceleration for the predictor that resumes the next run
   U.a_store = (medium == SFG_MEDIUM_ACOUSTIC || !predict || h->opt.store_acceleration) ? D.a : nullptr;
-  U.n = D.nglob * D.ncomp;
+  U.n = int(D.values());
   U.ncomp = D.ncomp;
   U.niface = D.niface;
   U.cp_nx = D.cp_nx; U.cp_nz = D.cp_nz; U.cp_other = D.cp_other;
@@ -350,20 +381,22 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.step = h->d_step;
   R.seis = h->d_seis;
   R.quad = h->quad;
-  sfg::dev::k_receivers<<<D.nrec, 32, 0, s>>>(R);
+  if (D.S > 1) sfg::dev::k_receivers_batched<<<D.nrec, 32, 0, s>>>(R, D.S);
+  else sfg::dev::k_receivers<<<D.nrec, 32, 0, s>>>(R);
 }
 
 void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaStream_t s) {
   const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
   sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
-  sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
+  if (D.S > 1) sfg::dev::k_update_batched<<<grid_for(U.n), 256, 0, s>>>(U, D.S);
+  else sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
 }
 
 void launch_predict_medium(sfg_handle *h, const DevMedium &D, cudaStream_t s) {
   if (!D.nspec) return;
   const float dt = float(h->asmb.dt);
-  const int n = D.nglob * D.ncomp;
+  const int n = int(D.values());
   sfg::dev::k_predict<<<grid_for(n), 256, 0, s>>>(D.u, D.v, D.a, n, dt, dt / 2.0f, dt * dt / 2.0f);
 }
 
@@ -443,10 +476,6 @@ sfg_handle *make_handle(const sfg_options *opt) {
   auto *h = new sfg_handle();
   h->opt = *opt;
   if (h->opt.nshots <= 0) h->opt.nshots = 1;
-  if (h->opt.nshots != 1) {
-    delete h;
-    throw std::runtime_error("this build advances one shot per handle");
-  }
   if (h->opt.nstep_between_samples <= 0) h->opt.nstep_between_samples = 1;
   if (h->opt.steps_per_graph <= 0) h->opt.steps_per_graph = 20;
   h->epb = 16;
@@ -459,6 +488,8 @@ void finish_create(sfg_handle *h) {
   h->asmb.nstep = h->opt.nstep;
   h->asmb.nsb = h->opt.nstep_between_samples;
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
+  if (h->asmb.nshots > 1 && (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0))
+    throw std::runtime_error("batched shots (nshots > 1) need a single elastic medium");
 }
 
 // ---------------------------------------------------------------------------
@@ -663,6 +694,10 @@ int sfg_initialize(sfg_handle *h) {
     if (h->el.nspec) h->el.src_head = h->mem.upload(a.el_src_head);
     if (h->ac.nspec) h->ac.src_head = h->mem.upload(a.ac_src_head);
     h->d_src_next = h->mem.upload(a.src_next);
+    h->d_src_shot = h->mem.upload(a.src_shot);
+    SFG_CUDA(cudaMemcpyToSymbol(sfg::dev::c_hp, a.hprime, sizeof(a.hprime)));
+    SFG_CUDA(cudaMemcpyToSymbol(sfg::dev::c_hpw, a.hpw, sizeof(a.hpw)));
+    SFG_CUDA(cudaMemcpyToSymbol(sfg::dev::c_w, a.wgll, sizeof(a.wgll)));
     h->d_src_arr = h->mem.upload(a.src_arr);
     h->d_stf = h->mem.upload(a.stf);
     h->d_rec_elem = h->mem.upload(a.rec_elem);
@@ -725,7 +760,7 @@ int sfg_reset_fields(sfg_handle *h) {
     if (!h->initialized) return int(SFG_ERR_STATE);
     for (DevMedium *D : {&h->el, &h->ac}) {
       if (!D->nspec) continue;
-      const size_t n = (size_t(D->nglob) * D->ncomp + 4) * sizeof(float);
+      const size_t n = (D->values() + 4) * sizeof(float);
       SFG_CUDA(cudaMemsetAsync(D->u, 0, n, h->stream));
       SFG_CUDA(cudaMemsetAsync(D->v, 0, n, h->stream));
       SFG_CUDA(cudaMemsetAsync(D->accum, 0, n, h->stream));
@@ -913,7 +948,7 @@ int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count
   return guarded(h, [&]() {
     if (!h->initialized) return int(SFG_ERR_STATE);
     DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
-    const size_t n = size_t(D.nglob) * D.ncomp;
+    const size_t n = D.values();
     if (!out || count < n) { h->err = "output buffer too small"; return int(SFG_ERR_ARG); }
     if (!h->state_final) {
       h->err = "fields are mid-step after a timing call; run a step first";
@@ -922,7 +957,16 @@ int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count
     const float *src = which == 0 ? D.u : which == 1 ? D.v : D.a;
     if (n == 0) return int(SFG_OK);
     SFG_CUDA(cudaStreamSynchronize(h->stream));
-    SFG_CUDA(cudaMemcpy(out, src, n * sizeof(float), cudaMemcpyDeviceToHost));
+    if (D.S == 1) {
+      SFG_CUDA(cudaMemcpy(out, src, n * sizeof(float), cudaMemcpyDeviceToHost));
+      return int(SFG_OK);
+    }
+    // device layout [point][comp][shot] -> [shot][point][comp]
+    std::vector<float> tmp(n);
+    SFG_CUDA(cudaMemcpy(tmp.data(), src, n * sizeof(float), cudaMemcpyDeviceToHost));
+    const size_t pc = size_t(D.nglob) * D.ncomp;
+    for (size_t k = 0; k < pc; ++k)
+      for (int sh = 0; sh < D.S; ++sh) out[size_t(sh) * pc + k] = tmp[k * D.S + sh];
     return int(SFG_OK);
   });
 }
@@ -947,8 +991,8 @@ int sfg_check_finite(sfg_handle *h) {
 int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
-    if (h->ac.nspec != 0 || h->el.nspec == 0) {
-      h->err = "sfg_step_noalloc advances single-medium elastic models only";
+    if (h->ac.nspec != 0 || h->el.nspec == 0 || h->el.S != 1) {
+      h->err = "sfg_step_noalloc advances single-shot, single-medium elastic models only";
       return int(SFG_ERR_UNSUPPORTED);
     }
     if (!u || !v || !a || istep < 0) { h->err = "null field pointer or negative step"; return int(SFG_ERR_ARG); }

@@ -140,13 +140,13 @@ class Simulation2D:
     """
 
     def __init__(self, mesh=None, *, database: str | None = None, dt: float, nstep: int,
-                 nstep_between_samples: int = 1, elastic_wave: str = "psv",
+                 nshots: int = 1, nstep_between_samples: int = 1, elastic_wave: str = "psv",
                  point_rho=None, point_vp=None, point_vs=None, steps_per_graph: int = 0,
                  elements_per_block: int = 0, kernel_variant: int = 0,
                  store_acceleration: bool = False):
         self.lib = load_library()
         self._keep = []
-        opt = Options(dt=dt, nstep=nstep, nshots=1, nstep_between_samples=nstep_between_samples,
+        opt = Options(dt=dt, nstep=nstep, nshots=nshots, nstep_between_samples=nstep_between_samples,
                       steps_per_graph=steps_per_graph, elements_per_block=elements_per_block,
                       kernel_variant=kernel_variant, store_acceleration=int(store_acceleration))
         h = C.c_void_p()
@@ -160,6 +160,7 @@ class Simulation2D:
             raise SfgError(rc, self.lib.sfg_last_error(None).decode())
         self.h = h
         self.dt, self.nstep = dt, nstep
+        self.ncomp = 1 if wave == 1 else 2
 
     def _k(self, a):
         self._keep.append(a)
@@ -260,12 +261,17 @@ class Simulation2D:
         return out
 
     def field(self, medium: str, which: str = "displacement") -> np.ndarray:
+        """Field of one medium in the handle's point numbering: elastic [nglob, ncomp]
+        (with nshots > 1: [nshots, nglob, ncomp]), acoustic [nglob]."""
         i = self.info()
         med = SFG_MEDIUM_ELASTIC if medium == "elastic" else SFG_MEDIUM_ACOUSTIC
         n = i.nglob_elastic if med == SFG_MEDIUM_ELASTIC else i.nglob_acoustic
-        out = np.zeros(n * (2 if med == SFG_MEDIUM_ELASTIC else 1), np.float32)
+        nc = self.ncomp if med == SFG_MEDIUM_ELASTIC else 1
+        out = np.zeros(i.nshots * n * nc, np.float32)
         self._check(self.lib.sfg_get_field(self.h, med, FIELD[which], out.ctypes.data_as(_fp), out.size))
-        return out.reshape(n, -1) if med == SFG_MEDIUM_ELASTIC else out
+        if med == SFG_MEDIUM_ACOUSTIC:
+            return out if i.nshots == 1 else out.reshape(i.nshots, n)
+        return out.reshape(n, nc) if i.nshots == 1 else out.reshape(i.nshots, n, nc)
 
     def numbering(self):
         i = self.info()
