@@ -42,6 +42,10 @@ WORKLOAD = "coupled_400x200"
 # elastic global point u read (8) + accumulator read and write (16) = 24 B.
 STIFF_B_PER_LOCAL = 32
 STIFF_B_PER_GLOB = 24
+# acoustic element point: ibool + Jacobian (20) + 1/rho = 28 B; point: chi read,
+# accumulator read and write = 12 B
+STIFF_B_PER_LOCAL_AC = 28
+STIFF_B_PER_GLOB_AC = 12
 # whole step, per global point (2D elastic P-SV, FP32): u,v,a read+write 48 +
 # M^-1 8 + 32 B per local point x 25 nspec / nglob.
 STEP_B_GLOB = 56
@@ -125,6 +129,53 @@ def cpu_oracle_throughput(w, steps, threads):
     return r["nglob"] * steps / r["loop_seconds"], r["loop_seconds"]
 
 
+def bench_batched(args, world, barrier, max_over_ranks):
+    """Config 3: S shots on a 2D elastic GRF model, batched in one launch per
+    step against the same shots run one at a time (shot.steps/s).  The model
+    holds S x 8M points of state (inputs far larger than L2); timed with CUDA
+    events over graph-replayed steps.  With N ranks the shots are split, S per
+    rank (weak scaling, no collective)."""
+    from specfempp_b200 import meshgen, sfg
+    nx, nz = (int(v) for v in args.batched_mesh.split("x"))
+    S = args.batched_shots
+    steps = args.batched_steps
+    warm = 3
+    w = meshgen.elastic_grf_1000x500(nstep=steps + warm + 2, nshots=S, nx=nx, nz=nz)
+
+    def make(nshots, srcs):
+        sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, nshots=nshots, point_rho=w.point_rho,
+                               point_vp=w.point_vp, point_vs=w.point_vs)
+        sim.set_sources(srcs)
+        sim.set_receivers(w.rec_x, w.rec_z)
+        sim.initialize()
+        return sim
+
+    sim = make(S, w.sources)
+    inf = sim.info()
+    sim.run(warm)
+    barrier()
+    ms_b = max_over_ranks(sim.run_timed(steps))
+    stiff_b = sim.time_kernel(0, 5)
+    del sim
+    from dataclasses import replace
+    one = make(1, [replace(w.sources[0], shot=0)])
+    one.run(warm)
+    barrier()
+    ms_1 = max_over_ranks(one.run_timed(steps))
+    del one
+    rate_b = world * S * steps / (ms_b / 1e3)
+    rate_1 = world * steps / (ms_1 / 1e3)
+    per_shot_b = STEP_B_GLOB + STEP_B_LOCAL * inf.nspec * 25 / (inf.nglob * S)
+    return {"workload": f"elastic_grf_{nx}x{nz}", "shots_per_gpu": S, "nglob": inf.nglob,
+            "steps": steps, "ms_per_step_batched": ms_b / steps, "ms_per_step_one_shot": ms_1 / steps,
+            "shot_steps_per_s_batched": rate_b, "shot_steps_per_s_one_at_a_time": rate_1,
+            "speedup": rate_b / rate_1,
+            "gll_pt_updates_per_s_batched": rate_b * inf.nglob,
+            "batched_stiffness_ms": stiff_b,
+            "batched_frac_of_hbm": per_shot_b * inf.nglob * S / (ms_b / steps / 1e3) / 1e9 / peaks()[0],
+            "timing": "CUDA events, graph-replayed steps, inputs larger than L2"}
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -156,6 +207,11 @@ def main():
     ap.add_argument("--impl", default="sfg", choices=["sfg", "reference"])
     ap.add_argument("--workload", default=WORKLOAD)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--batched-mesh", default="1000x500",
+                    help="elements of the batched-shot model, NXxNZ (config 3: 1000x500)")
+    ap.add_argument("--batched-shots", type=int, default=32)
+    ap.add_argument("--batched-steps", type=int, default=30)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -236,7 +292,8 @@ def main():
     stiff_ms = sim.time_kernel(0, 50)
     upd_ms = sim.time_kernel(1, 50)
     ac_ms = sim.time_kernel(2, 50)
-    stiff_bytes = STIFF_B_PER_LOCAL * inf.nspec_elastic * 25 + STIFF_B_PER_GLOB * inf.nglob_elastic
+    stiff_bytes = (STIFF_B_PER_LOCAL * inf.nspec_elastic * 25 + STIFF_B_PER_GLOB * inf.nglob_elastic +
+                   STIFF_B_PER_LOCAL_AC * inf.nspec_acoustic * 25 + STIFF_B_PER_GLOB_AC * inf.nglob_acoustic)
     peak, peak_kind = peaks()
     achieved = stiff_bytes / (stiff_ms / 1e3) / 1e9
     tr = traffic_from_profile()
@@ -244,13 +301,19 @@ def main():
     if tr and tr.get("workload") == args.workload:
         traffic = tr.get("stiffness_bytes_per_launch")
     step_bytes = STEP_B_GLOB * nglob + STEP_B_LOCAL * inf.nspec * 25
-    roofline = {"bound": "hbm", "kernel": "k_stiffness_psv (4 colour launches of one step)",
+    roofline = {"bound": "hbm", "kernel": f"element kernel, all {inf.ncolors_elastic} colour launches of one "
+                                          f"step (variant {inf.kernel_variant}, {inf.elements_per_block} "
+                                          f"elements/block, both media)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": stiff_bytes, "launch_ms": stiff_ms,
                 "update_launch_ms": upd_ms, "acoustic_stiffness_ms": ac_ms,
                 "step_algorithmic_bytes": step_bytes,
                 "step_frac_of_peak": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak}
+
+    batched = None
+    if not args.no_batched:
+        batched = bench_batched(args, world, barrier, max_over_ranks)
 
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
@@ -280,6 +343,7 @@ def main():
         "cpu_baseline": cpu,
         "clocks": clk,
         "gpu_launches": inf.kernels_per_step * args.steps,
+        "batched": batched,
     }
     print(json.dumps(line), flush=True)
 
