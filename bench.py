@@ -292,8 +292,14 @@ def main():
     stiff_ms = sim.time_kernel(0, 50)
     upd_ms = sim.time_kernel(1, 50)
     ac_ms = sim.time_kernel(2, 50)
-    stiff_bytes = (STIFF_B_PER_LOCAL * inf.nspec_elastic * 25 + STIFF_B_PER_GLOB * inf.nglob_elastic +
-                   STIFF_B_PER_LOCAL_AC * inf.nspec_acoustic * 25 + STIFF_B_PER_GLOB_AC * inf.nglob_acoustic)
+    if inf.kernel_variant == 3:
+        # owner-computes: the element kernel reads geometry and the gathered field
+        # and writes each element point's contribution once (8 B elastic, 4 B acoustic)
+        stiff_bytes = ((STIFF_B_PER_LOCAL + 8) * inf.nspec_elastic * 25 + 8 * inf.nglob_elastic +
+                       (STIFF_B_PER_LOCAL_AC + 4) * inf.nspec_acoustic * 25 + 4 * inf.nglob_acoustic)
+    else:
+        stiff_bytes = (STIFF_B_PER_LOCAL * inf.nspec_elastic * 25 + STIFF_B_PER_GLOB * inf.nglob_elastic +
+                       STIFF_B_PER_LOCAL_AC * inf.nspec_acoustic * 25 + STIFF_B_PER_GLOB_AC * inf.nglob_acoustic)
     peak, peak_kind = peaks()
     achieved = stiff_bytes / (stiff_ms / 1e3) / 1e9
     tr = traffic_from_profile()
@@ -301,9 +307,10 @@ def main():
     if tr and tr.get("workload") == args.workload:
         traffic = tr.get("stiffness_bytes_per_launch")
     step_bytes = STEP_B_GLOB * nglob + STEP_B_LOCAL * inf.nspec * 25
-    roofline = {"bound": "hbm", "kernel": f"element kernel, all {inf.ncolors_elastic} colour launches of one "
-                                          f"step (variant {inf.kernel_variant}, {inf.elements_per_block} "
-                                          f"elements/block, both media)",
+    kname = ("element kernel, one owner-computes launch of one step" if inf.kernel_variant == 3 else
+             f"element kernel, all {inf.ncolors_elastic} colour launches of one step")
+    roofline = {"bound": "hbm", "kernel": f"{kname} (variant {inf.kernel_variant}, "
+                                          f"{inf.elements_per_block} elements/block, both media)",
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": stiff_bytes, "launch_ms": stiff_ms,

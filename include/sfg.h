@@ -85,8 +85,11 @@ typedef struct sfg_options {
   int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
   int elements_per_block;        /* elements per block of the element kernel: 8, 16, 32
                                     (0 = chosen by the autotuner at sfg_initialize) */
-  int kernel_variant;            /* element kernel: 1 one block per chunk, 2 persistent
-                                    with prefetch (0 = chosen by the autotuner) */
+  int kernel_variant;            /* assembly / element kernel: 1 colour passes (one block
+                                    per chunk), 2 colour passes with a persistent
+                                    prefetching kernel, 3 owner-computes (one element
+                                    launch, per-point gather in colour order); all give
+                                    the same bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
 } sfg_options;
 

@@ -473,6 +473,14 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       const int e = D.elem_mesh[ce];
       for (int q = 0; q < NPTS; ++q) D.ibool[size_t(ce) * NPTS + q] = g2m[gid[size_t(e) * NPTS + q]];
     }
+    D.inv_start.assign(D.nglob + 1, 0);
+    for (int v : D.ibool) ++D.inv_start[v + 1];
+    for (int i = 0; i < D.nglob; ++i) D.inv_start[i + 1] += D.inv_start[i];
+    D.inv_idx.resize(D.ibool.size());
+    {
+      std::vector<int> fill(D.inv_start.begin(), D.inv_start.end() - 1);
+      for (size_t pl = 0; pl < D.ibool.size(); ++pl) D.inv_idx[fill[D.ibool[pl]]++] = int(pl);
+    }
     const size_t n = size_t(D.nspec) * NPTS;
     D.xix.resize(n); D.xiz.resize(n); D.gax.resize(n); D.gaz.resize(n); D.jac.resize(n);
     D.prop0.resize(n); D.prop1.resize(n);

@@ -58,6 +58,10 @@ struct MediumData {
   std::vector<float> cp_nx, cp_nz;    // [niface]
   std::vector<int> cp_other;          // [niface]
   std::vector<int> glob_of_point;     // medium point id -> mesh global id
+  // owner-computes assembly: for every medium point, the element-local
+  // indices (compute element * 25 + GLL point) that contribute to it, in
+  // increasing compute order (= colour order)
+  std::vector<int> inv_start, inv_idx;
 };
 
 struct Assembly2D {

@@ -61,6 +61,7 @@ struct MedArgs {
   const int *__restrict__ src_head;
   const float *__restrict__ u, *__restrict__ v;
   float *__restrict__ accum;
+  float *__restrict__ r;   // element-local results [element*25 + point][comp] (owner-computes)
   int e0, e1;      // element range of the colour
   int nblocks;     // blocks of this medium in the launch
 };
@@ -82,7 +83,9 @@ __device__ __forceinline__ void load_quad(const Quad &Q, float *shp, float *shpw
 }
 
 // Elastic element block; EK 0 = P-SV (two components), 1 = SH (one component).
-template <int E, int EK>
+// LOCAL: write the element's contribution to its own slot of A.r (summed per
+// point later by the update) instead of adding it into the accumulator.
+template <int E, int EK, bool LOCAL>
 __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs &A, int ebase,
                                               unsigned char *smem, float *shp, float *shpw,
                                               float *sw) {
@@ -102,11 +105,14 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   float uu[NC], acc[NC];
   if (NC == 2) {
     const float2 t = act ? reinterpret_cast<const float2 *>(A.u)[g] : make_float2(0.f, 0.f);
-    const float2 r = act ? reinterpret_cast<const float2 *>(A.accum)[g] : make_float2(0.f, 0.f);
-    uu[0] = t.x; uu[NC - 1] = t.y; acc[0] = r.x; acc[NC - 1] = r.y;
+    uu[0] = t.x; uu[NC - 1] = t.y;
+    if (!LOCAL) {
+      const float2 r = act ? reinterpret_cast<const float2 *>(A.accum)[g] : make_float2(0.f, 0.f);
+      acc[0] = r.x; acc[NC - 1] = r.y;
+    }
   } else {
     uu[0] = act ? A.u[g] : 0.f;
-    acc[0] = act ? A.accum[g] : 0.f;
+    if (!LOCAL) acc[0] = act ? A.accum[g] : 0.f;
   }
   const int bs = act ? __ldg(A.bc_slot + e) : -1;
   const int src = act ? __ldg(A.src_head + e) : -1;
@@ -187,7 +193,10 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
       for (int c = 0; c < NC; ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
     }
   }
-  if (NC == 2) {
+  if (LOCAL) {
+    if (NC == 2) reinterpret_cast<float2 *>(A.r)[p] = make_float2(a[0], a[NC - 1]);
+    else A.r[p] = a[0];
+  } else if (NC == 2) {
     reinterpret_cast<float2 *>(A.accum)[g] = make_float2(acc[0] + a[0], acc[NC - 1] + a[NC - 1]);
   } else {
     A.accum[g] = acc[0] + a[0];
@@ -195,7 +204,7 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
 }
 
 // Acoustic element block (potential chi; sigma = rho^-1 grad chi).
-template <int E>
+template <int E, bool LOCAL>
 __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs &A, int ebase,
                                                unsigned char *smem, float *shp, float *shpw,
                                                float *sw) {
@@ -211,7 +220,7 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
               gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
   const float rhoinv = __ldg(A.prop0 + p);
   const float chi = act ? A.u[g] : 0.f;
-  const float acc = act ? A.accum[g] : 0.f;
+  const float acc = (act && !LOCAL) ? A.accum[g] : 0.f;
   const int bs = act ? __ldg(A.bc_slot + e) : -1;
   const int src = act ? __ldg(A.src_head + e) : -1;
   su[le * NP + q] = chi;
@@ -249,20 +258,21 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
       a += f * S.src_arr[(size_t(s) * 2) * NP + q];
     }
   }
-  A.accum[g] = acc + a;
+  if (LOCAL) A.r[p] = a;
+  else A.accum[g] = acc + a;
 }
 
 // One launch per colour: blocks [0, el.nblocks) run elastic elements of the
 // colour, the following ac.nblocks blocks acoustic ones.
-template <int E, int EK>
+template <int E, int EK, bool LOCAL>
 __global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
   __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * 6];
   __shared__ float shp[NP], shpw[NP], sw[NG];
   load_quad(S.quad, shp, shpw, sw, threadIdx.x);
   if (int(blockIdx.x) < S.el.nblocks)
-    elastic_block<E, EK>(S, S.el, S.el.e0 + blockIdx.x * E, smem, shp, shpw, sw);
+    elastic_block<E, EK, LOCAL>(S, S.el, S.el.e0 + blockIdx.x * E, smem, shp, shpw, sw);
   else
-    acoustic_block<E>(S, S.ac, S.ac.e0 + (blockIdx.x - S.el.nblocks) * E, smem, shp, shpw, sw);
+    acoustic_block<E, LOCAL>(S, S.ac, S.ac.e0 + (blockIdx.x - S.el.nblocks) * E, smem, shp, shpw, sw);
 }
 
 // ---------------------------------------------------------------------------
@@ -469,6 +479,9 @@ struct UpdateArgs {
   const float *__restrict__ cp_nx, *__restrict__ cp_nz;
   const int *__restrict__ cp_other;
   const float *__restrict__ other;
+  // owner-computes assembly: accum of point g = sum of r over inv_idx[inv_start[g] ..)
+  const int *__restrict__ inv_start, *__restrict__ inv_idx;
+  const float *__restrict__ r;
   float dt, dt2, dtsq2;
   int predict;                   // fuse the next step's predictor
   int *flag;                     // set to 1 on a non-finite displacement
@@ -552,6 +565,65 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
   if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
 }
 
+// Owner-computes form of k_update: one thread per point gathers the
+// element-local contributions in increasing compute order (colour order), so
+// the sum is the colour passes' sum bit for bit; then coupling, M^-1,
+// corrector and optional predictor as k_update.  No accumulator to clear.
+template <int NC>
+__global__ void __launch_bounds__(256) k_update_gather(UpdateArgs A) {
+  const int npts = A.n / NC;
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
+    float acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+    const int k1 = A.inv_start[g + 1];
+    for (int k = A.inv_start[g]; k < k1; ++k) {
+      const int pl = A.inv_idx[k];
+      if (NC == 2) {
+        const float2 t = reinterpret_cast<const float2 *>(A.r)[pl];
+        acc[0] = acc[0] + t.x;
+        acc[NC - 1] = acc[NC - 1] + t.y;
+      } else {
+        acc[0] = acc[0] + A.r[pl];
+      }
+    }
+    if (g < A.niface) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] += coupling_term(A, g, c);
+    }
+    float uu[NC], vv[NC], mi[NC];
+    if (NC == 2) {
+      const float2 u2 = reinterpret_cast<const float2 *>(A.u)[g];
+      const float2 v2 = reinterpret_cast<const float2 *>(A.v)[g];
+      const float2 m2 = reinterpret_cast<const float2 *>(A.minv)[g];
+      uu[0] = u2.x; uu[NC - 1] = u2.y; vv[0] = v2.x; vv[NC - 1] = v2.y; mi[0] = m2.x; mi[NC - 1] = m2.y;
+    } else {
+      uu[0] = A.u[g]; vv[0] = A.v[g]; mi[0] = A.minv[g];
+    }
+    float a[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      a[c] = __fmul_rn(acc[c], mi[c]);
+      vv[c] = newmark_correct(vv[c], a[c], A.dt2);
+      if (A.predict) newmark_predict(uu[c], vv[c], a[c], A.dt, A.dt2, A.dtsq2);
+      bad |= !isfinite(uu[c]);
+    }
+    if (NC == 2) {
+      if (A.predict) reinterpret_cast<float2 *>(A.u)[g] = make_float2(uu[0], uu[NC - 1]);
+      reinterpret_cast<float2 *>(A.v)[g] = make_float2(vv[0], vv[NC - 1]);
+      if (A.a_store) reinterpret_cast<float2 *>(A.a_store)[g] = make_float2(a[0], a[NC - 1]);
+    } else {
+      if (A.predict) A.u[g] = uu[0];
+      A.v[g] = vv[0];
+      if (A.a_store) A.a_store[g] = a[0];
+    }
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
 // Pending predictor of a run that ended on a corrector-only update.
 __global__ void __launch_bounds__(256) k_predict(float *__restrict__ u, float *__restrict__ v,
                                                  const float *__restrict__ a, int n, float dt,
@@ -592,7 +664,14 @@ __device__ __forceinline__ float warp_sum(float x) {
 
 __device__ __forceinline__ float rec_accel(const RecArgs &A, int g, int c) {
   const size_t k = size_t(g) * A.ncomp + c;
-  float acc = A.accum[k];
+  float acc;
+  if (A.cpl.inv_start) {   // owner-computes: gather in colour order
+    acc = 0.f;
+    for (int j = A.cpl.inv_start[g]; j < A.cpl.inv_start[g + 1]; ++j)
+      acc = acc + A.cpl.r[size_t(A.cpl.inv_idx[j]) * A.ncomp + c];
+  } else {
+    acc = A.accum[k];
+  }
   if (g < A.cpl.niface) acc += coupling_term(A.cpl, g, c);
   return __fmul_rn(acc, A.minv[k]);
 }

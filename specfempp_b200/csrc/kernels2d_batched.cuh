@@ -40,12 +40,15 @@ struct BatchArgs {
   const int *__restrict__ step;
   const float *__restrict__ u, *__restrict__ v;   // [nglob][NC][S]
   float *__restrict__ accum;
+  float *__restrict__ r;               // owner-computes: [element*25 + point][NC][S]
   int e0;                              // first element of the colour
   int S;                               // shots
 };
 
 // grid: (elements of the colour, shot tiles of 32); block: 25 warps x 32 lanes.
-template <int NC>
+// LOCAL: write the element's contribution to its own slot of A.r instead of
+// adding it into the accumulator (then e0 = 0 and the grid covers all elements).
+template <int NC, bool LOCAL>
 __global__ void __launch_bounds__(NP * 32) k_stiffness_batched(BatchArgs A) {
   __shared__ float su[NC][NP][32];
   __shared__ float sF[NC][2][NP][32];
@@ -64,7 +67,7 @@ __global__ void __launch_bounds__(NP * 32) k_stiffness_batched(BatchArgs A) {
   for (int c = 0; c < NC; ++c) {
     const size_t k = (size_t(g) * NC + c) * A.S + shot;
     uu[c] = act ? A.u[k] : 0.f;
-    acc[c] = act ? A.accum[k] : 0.f;
+    acc[c] = (act && !LOCAL) ? A.accum[k] : 0.f;
     su[c][q][lane] = uu[c];
   }
   const int bs = __ldg(A.bc_slot + e);
@@ -142,7 +145,37 @@ __global__ void __launch_bounds__(NP * 32) k_stiffness_batched(BatchArgs A) {
     }
   }
 #pragma unroll
-  for (int c = 0; c < NC; ++c) A.accum[(size_t(g) * NC + c) * A.S + shot] = acc[c] + a[c];
+  for (int c = 0; c < NC; ++c) {
+    if (LOCAL) A.r[(p * NC + c) * A.S + shot] = a[c];
+    else A.accum[(size_t(g) * NC + c) * A.S + shot] = acc[c] + a[c];
+  }
+}
+
+// Owner-computes update for [point][NC][S] fields: each (point, comp, shot)
+// gathers its element contributions in colour order (bitwise the colour
+// passes' sum), then M^-1, corrector and optional predictor.
+__global__ void __launch_bounds__(256) k_update_batched_gather(UpdateArgs A, int S, int NC) {
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+    const int s = i % S;
+    const int gc = i / S;
+    const int g = gc / NC, c = gc - g * NC;
+    float acc = 0.f;
+    const int k1 = A.inv_start[g + 1];
+    for (int k = A.inv_start[g]; k < k1; ++k)
+      acc = acc + A.r[(size_t(A.inv_idx[k]) * NC + c) * S + s];
+    const float a = __fmul_rn(acc, A.minv[gc]);
+    float vv = newmark_correct(A.v[i], a, A.dt2);
+    float uu = A.u[i];
+    if (A.predict) newmark_predict(uu, vv, a, A.dt, A.dt2, A.dtsq2);
+    A.u[i] = uu;
+    A.v[i] = vv;
+    if (A.a_store) A.a_store[i] = a;
+    bad |= !isfinite(uu);
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
 }
 
 // a = accum * M^-1 (M^-1 shared by the shots); corrector; optional fused
@@ -190,7 +223,14 @@ __global__ void __launch_bounds__(32) k_receivers_batched(RecArgs A, int S) {
         for (int q = 0; q < NP; ++q) {
           const int g = A.ibool[size_t(ce) * NP + q];
           const size_t k = (size_t(g) * NC + c) * S + shot;
-          const float acc = __fmul_rn(A.accum[k], A.minv[size_t(g) * NC + c]);
+          float sum = 0.f;
+          if (A.cpl.inv_start) {
+            for (int j = A.cpl.inv_start[g]; j < A.cpl.inv_start[g + 1]; ++j)
+              sum = sum + A.cpl.r[(size_t(A.cpl.inv_idx[j]) * NC + c) * S + shot];
+          } else {
+            sum = A.accum[k];
+          }
+          const float acc = __fmul_rn(sum, A.minv[size_t(g) * NC + c]);
           float val;
           switch (A.types[t]) {
             case 0: val = A.u[k]; break;

@@ -80,6 +80,8 @@ struct DevMedium {
   int *src_head = nullptr;
   float *minv = nullptr;
   float *u = nullptr, *v = nullptr, *accum = nullptr, *a = nullptr;
+  float *r = nullptr;              // element-local contributions (owner-computes assembly)
+  int *inv_start = nullptr, *inv_idx = nullptr;
   int *rec_list = nullptr;
   int nrec = 0;
 };
@@ -104,7 +106,7 @@ struct sfg_handle {
   int *d_step = nullptr, *d_flag = nullptr;
   int host_step = 0;
   int epb = 16;
-  int variant = 1;           // 1 one-pass element kernel, 2 persistent
+  int variant = 1;           // 1 colour passes, 2 persistent colour passes, 3 owner-computes
   int sm_count = 148;
   int resident[2][3] = {{0}};  // persistent: resident blocks per SM [EK][E index]
   cudaStream_t stream = nullptr;
@@ -172,6 +174,9 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.v = m.zeros<float>(n + 4);
   D.accum = m.zeros<float>(n + 4);
   D.a = m.zeros<float>(n + 4);
+  D.inv_start = m.upload(M.inv_start);
+  D.inv_idx = m.upload(M.inv_idx);
+  D.r = m.zeros<float>(size_t(M.nspec) * sfg::NPTS * M.ncomp * D.S + 4);
 }
 
 sfg::dev::MedArgs med_args(const DevMedium &D) {
@@ -182,7 +187,7 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
   A.src_head = D.src_head;
-  A.u = D.u; A.v = D.v; A.accum = D.accum;
+  A.u = D.u; A.v = D.v; A.accum = D.accum; A.r = D.r;
   return A;
 }
 
@@ -190,7 +195,7 @@ int ncolors(const DevMedium &D) { return D.nspec ? int(D.color_start.size()) - 1
 
 template <int E, int EK>
 void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
-                        cudaStream_t s) {
+                        cudaStream_t s, int variant) {
   sfg::dev::StiffArgs S{};
   S.el = med_args(el);
   S.ac = med_args(ac);
@@ -201,7 +206,15 @@ void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
   S.nstep = h->asmb.nstep;
   S.step = step;
   S.quad = h->quad;
-  const bool persistent = h->variant == 2;
+  if (variant == 3) {
+    // owner-computes: one launch over every element of both media
+    S.el.e0 = 0; S.el.e1 = el.nspec; S.el.nblocks = (el.nspec + E - 1) / E;
+    S.ac.e0 = 0; S.ac.e1 = ac.nspec; S.ac.nblocks = (ac.nspec + E - 1) / E;
+    const int grid = S.el.nblocks + S.ac.nblocks;
+    if (grid > 0) sfg::dev::k_stiffness<E, EK, true><<<grid, sfg::dev::NP * E, 0, s>>>(S);
+    return;
+  }
+  const bool persistent = variant == 2;
   int capacity = 0;
   if (persistent) {
     const int ei = E == 8 ? 0 : (E == 16 ? 1 : 2);
@@ -240,18 +253,19 @@ void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
     if (persistent)
       sfg::dev::k_stiffness_persistent<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
     else
-      sfg::dev::k_stiffness<E, EK><<<grid, sfg::dev::NP * E, 0, s>>>(S);
+      sfg::dev::k_stiffness<E, EK, false><<<grid, sfg::dev::NP * E, 0, s>>>(S);
   }
 }
 
 template <int E>
 void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
-                        cudaStream_t s) {
-  if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s);
-  else launch_stiffness_E<E, 0>(h, el, ac, step, s);
+                        cudaStream_t s, int variant) {
+  if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s, variant);
+  else launch_stiffness_E<E, 0>(h, el, ac, step, s, variant);
 }
 
-void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *step, cudaStream_t s) {
+void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *step, cudaStream_t s,
+                              int variant) {
   sfg::dev::BatchArgs B{};
   B.ibool = el.ibool;
   B.xix = el.xix; B.xiz = el.xiz; B.gax = el.gax; B.gaz = el.gaz; B.jac = el.jac;
@@ -262,70 +276,40 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
   B.src_arr = h->d_src_arr; B.stf = h->d_stf;
   B.nsrc = h->asmb.nsrc; B.nstep = h->asmb.nstep;
   B.step = step;
-  B.u = el.u; B.v = el.v; B.accum = el.accum;
+  B.u = el.u; B.v = el.v; B.accum = el.accum; B.r = el.r;
   B.S = el.S;
+  if (variant == 3) {
+    B.e0 = 0;
+    const dim3 grid(el.nspec, (el.S + 31) / 32);
+    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2, true><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    else sfg::dev::k_stiffness_batched<1, true><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    return;
+  }
   for (int c = 0; c < ncolors(el); ++c) {
     B.e0 = el.color_start[c];
     const int n = el.color_start[c + 1] - B.e0;
     if (n <= 0) continue;
     const dim3 grid(n, (el.S + 31) / 32);
-    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
-    else sfg::dev::k_stiffness_batched<1><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2, false><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    else sfg::dev::k_stiffness_batched<1, false><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
   }
 }
 
 void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
-                      cudaStream_t s) {
+                      cudaStream_t s, int variant) {
   if (el.S > 1) {
-    launch_stiffness_batched(h, el, step, s);
+    launch_stiffness_batched(h, el, step, s, variant);
     return;
   }
   switch (h->epb) {
-    case 8: launch_stiffness_W<8>(h, el, ac, step, s); break;
-    case 32: launch_stiffness_W<32>(h, el, ac, step, s); break;
-    default: launch_stiffness_W<16>(h, el, ac, step, s); break;
+    case 8: launch_stiffness_W<8>(h, el, ac, step, s, variant); break;
+    case 32: launch_stiffness_W<32>(h, el, ac, step, s, variant); break;
+    default: launch_stiffness_W<16>(h, el, ac, step, s, variant); break;
   }
 }
 
-void launch_stiffness(sfg_handle *h, cudaStream_t s) { launch_stiffness(h, h->el, h->ac, h->d_step, s); }
-
-// Element-kernel autotuner: every (variant, elements per block) candidate
-// gives bit-identical results (a colour's elements share no point), so the
-// fastest one measured on this mesh is kept.  Runs on scratch accumulators at
-// sfg_initialize, before the step graphs are captured.
-void autotune(sfg_handle *h) {
-  const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
-                     h->opt.elements_per_block == 32;
-  const bool fix_v = h->opt.kernel_variant == 1 || h->opt.kernel_variant == 2;
-  if (fix_e) h->epb = h->opt.elements_per_block;
-  if (fix_v) h->variant = h->opt.kernel_variant;
-  if ((fix_e && fix_v) || h->asmb.nshots > 1) return;  // batched shots: one launch shape
-  std::vector<std::pair<int, int>> cand;
-  for (int v : {1, 2})
-    for (int e : {8, 16, 32})
-      if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
-  float best = 1e30f;
-  std::pair<int, int> pick = cand.front();
-  for (auto [v, e] : cand) {
-    h->variant = v;
-    h->epb = e;
-    for (int i = 0; i < 2; ++i) launch_stiffness(h, h->stream);
-    SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
-    const int reps = 5;
-    for (int i = 0; i < reps; ++i) launch_stiffness(h, h->stream);
-    SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
-    SFG_CUDA(cudaEventSynchronize(h->ev1));
-    SFG_CUDA(cudaGetLastError());
-    float t = 0;
-    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
-    if (t < best) { best = t; pick = {v, e}; }
-  }
-  h->variant = pick.first;
-  h->epb = pick.second;
-  // the tuning launches added into the accumulators: clear them
-  for (DevMedium *D : {&h->el, &h->ac})
-    if (D->nspec) SFG_CUDA(cudaMemsetAsync(D->accum, 0, (D->values() + 4) * sizeof(float), h->stream));
-  SFG_CUDA(cudaStreamSynchronize(h->stream));
+void launch_stiffness(sfg_handle *h, cudaStream_t s) {
+  launch_stiffness(h, h->el, h->ac, h->d_step, s, h->variant);
 }
 
 sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMedium &O, int medium,
@@ -345,6 +329,11 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   U.dt2 = dt / 2.0f;
   U.dtsq2 = dt * dt / 2.0f;
   U.predict = predict ? 1 : 0;
+  if (h->variant == 3) {
+    U.inv_start = D.inv_start;
+    U.inv_idx = D.inv_idx;
+    U.r = D.r;
+  }
   U.flag = h->d_flag;
   U.step = h->d_step;
   U.advance = advance ? 1 : 0;
@@ -389,6 +378,12 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
   const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
   sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
+  if (h->variant == 3) {
+    if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
+    else if (D.ncomp == 2) sfg::dev::k_update_gather<2><<<grid_for(U.n / 2), 256, 0, s>>>(U);
+    else sfg::dev::k_update_gather<1><<<grid_for(U.n), 256, 0, s>>>(U);
+    return;
+  }
   if (D.S > 1) sfg::dev::k_update_batched<<<grid_for(U.n), 256, 0, s>>>(U, D.S);
   else sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
 }
@@ -468,6 +463,69 @@ void run_steps(sfg_handle *h, int nsteps) {
   h->state_final = true;
   SFG_CUDA(cudaGetLastError());
   h->host_step += nsteps;
+}
+
+// Launch-shape autotuner: every candidate (colour passes, persistent colour
+// passes or owner-computes assembly; 8, 16 or 32 elements per block) gives
+// bit-identical results, so the one with the fastest whole step measured on
+// this mesh is kept.  Runs at sfg_initialize, before the step graphs are
+// captured; the fields and counters it touches are cleared afterwards.
+void autotune(sfg_handle *h) {
+  const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
+                     h->opt.elements_per_block == 32;
+  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 3;
+  if (fix_e) h->epb = h->opt.elements_per_block;
+  if (fix_v) h->variant = h->opt.kernel_variant;
+  if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
+  std::vector<std::pair<int, int>> cand;
+  if (h->asmb.nshots > 1) {
+    for (int v : {1, 3})
+      if (!fix_v || v == h->variant) cand.push_back({v, 16});
+  } else {
+    for (int v : {1, 2, 3})
+      for (int e : {8, 16, 32})
+        if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
+  }
+  if (cand.empty()) cand.push_back({h->variant, h->epb});
+  if (cand.size() > 1) {
+    float best = 1e30f;
+    std::pair<int, int> pick = cand.front();
+    const int reps = h->asmb.nshots > 1 ? 2 : 5;
+    for (auto [v, e] : cand) {
+      h->variant = v;
+      h->epb = e;
+      for (int i = 0; i < 2; ++i) enqueue_step(h, h->stream, true);
+      SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+      for (int i = 0; i < reps; ++i) enqueue_step(h, h->stream, true);
+      SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+      SFG_CUDA(cudaEventSynchronize(h->ev1));
+      SFG_CUDA(cudaGetLastError());
+      float t = 0;
+      SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+      if (t < best) { best = t; pick = {v, e}; }
+    }
+    h->variant = pick.first;
+    h->epb = pick.second;
+  } else {
+    h->variant = cand[0].first;
+    h->epb = cand[0].second;
+  }
+  // the tuning steps ran on the (zero) fields: clear every state word again
+  for (DevMedium *D : {&h->el, &h->ac}) {
+    if (!D->nspec) continue;
+    const size_t n = (D->values() + 4) * sizeof(float);
+    SFG_CUDA(cudaMemsetAsync(D->u, 0, n, h->stream));
+    SFG_CUDA(cudaMemsetAsync(D->v, 0, n, h->stream));
+    SFG_CUDA(cudaMemsetAsync(D->accum, 0, n, h->stream));
+    SFG_CUDA(cudaMemsetAsync(D->a, 0, n, h->stream));
+  }
+  const sfg::Assembly2D &a = h->asmb;
+  SFG_CUDA(cudaMemsetAsync(h->d_seis, 0,
+                           size_t(a.nshots) * a.nsig * a.ntypes * std::max(a.nrec, 1) * 2 * sizeof(float),
+                           h->stream));
+  SFG_CUDA(cudaMemsetAsync(h->d_step, 0, sizeof(int), h->stream));
+  SFG_CUDA(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+  SFG_CUDA(cudaStreamSynchronize(h->stream));
 }
 
 sfg_handle *make_handle(const sfg_options *opt) {
@@ -1017,8 +1075,12 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
     SFG_CUDA(cudaMemcpyAsync(nd.words, words, sizeof(words), cudaMemcpyHostToDevice, s));
     // predictor, element launches, corrector: the kernels of sfg_step
     launch_predict_medium(h, el, s);
-    launch_stiffness(h, el, h->ac, nd.words, s);
+    // colour passes into the fixed accumulator (every launch shape gives the same bits)
+    launch_stiffness(h, el, h->ac, nd.words, s, h->variant == 2 ? 2 : 1);
     sfg::dev::UpdateArgs U = update_args(h, el, h->ac, SFG_MEDIUM_ELASTIC, false, false);
+    U.inv_start = nullptr;
+    U.inv_idx = nullptr;
+    U.r = nullptr;
     U.a_store = a;
     U.flag = nd.words + 1;
     U.step = nd.words;

@@ -20,9 +20,9 @@ def shots(nshots, seed=3):
                                  float(rng.uniform(6.0, 14.0)), 1e10, shot=s) for s in range(nshots)]
 
 
-def run(w, srcs, nshots, types=("displacement", "velocity")):
+def run(w, srcs, nshots, types=("displacement", "velocity"), variant=0):
     from specfempp_b200 import sfg
-    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, nshots=nshots)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, nshots=nshots, kernel_variant=variant)
     sim.set_sources(srcs)
     sim.set_receivers(w.rec_x, w.rec_z, types=types)
     sim.initialize()
@@ -30,13 +30,13 @@ def run(w, srcs, nshots, types=("displacement", "velocity")):
     return sim
 
 
-@pytest.mark.parametrize("nshots", [5, 37])
-def test_batched_equals_single_shots(sfg_lib, nshots):
+@pytest.mark.parametrize("nshots,variant", [(5, 1), (5, 3), (37, 1), (37, 3)])
+def test_batched_equals_single_shots(sfg_lib, nshots, variant):
     from dataclasses import replace
     from specfempp_b200 import meshgen
     w = meshgen.elastic_psv_80x60(nstep=400)
     srcs = shots(nshots)
-    batched = run(w, srcs, nshots)
+    batched = run(w, srcs, nshots, variant=variant)
     seis_b = batched.seismograms()
     u_b = batched.field("elastic", "displacement")
     assert seis_b.shape[0] == nshots and u_b.shape[0] == nshots

@@ -101,7 +101,8 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
 
 
-@pytest.mark.parametrize("epb,spg,variant", [(8, 7, 1), (32, 1, 1), (8, 3, 2), (16, 20, 2), (32, 5, 2)])
+@pytest.mark.parametrize("epb,spg,variant", [(8, 7, 1), (32, 1, 1), (8, 3, 2), (16, 20, 2), (32, 5, 2),
+                                             (8, 4, 3), (16, 20, 3), (32, 1, 3)])
 def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg, variant):
     from specfempp_b200 import meshgen
     w = meshgen.coupled_400x200(nstep=120, nx=40, nz=20)
