@@ -178,6 +178,204 @@ __global__ void __launch_bounds__(256) k_update_batched_gather(UpdateArgs A, int
   if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
 }
 
+// ---------------------------------------------------------------------------
+// Quad-shot form (S a multiple of 4): each thread carries 4 consecutive shots
+// of one GLL point as a float4, so it has four times the field bytes in
+// flight of the one-shot-per-lane kernel.  Block: one element, 25 points x T
+// threads (T = shots in the tile / 4, at most 8); grid: (elements, shot tiles).
+// Per shot the operations are those of k_stiffness_batched.
+template <int NC, bool LOCAL>
+__global__ void __launch_bounds__(NP * 8) k_stiffness_batched4(BatchArgs A, int T) {
+  __shared__ float4 su[NC][NP][8];
+  __shared__ float4 sF[NC][2][NP][8];
+  const int q = threadIdx.x / T, j = threadIdx.x - q * T;
+  const int shot0 = (blockIdx.y * T + j) * 4;
+  const bool act = shot0 < A.S;
+  const int e = A.e0 + blockIdx.x;
+  const size_t p = size_t(e) * NP + q;
+  const int iz = q / NG, ix = q - iz * NG;
+  const int g = __ldg(A.ibool + p);
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+  float4 acc4[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    const size_t k = (size_t(g) * NC + c) * A.S + shot0;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    su[c][q][j] = act ? *reinterpret_cast<const float4 *>(A.u + k) : z;
+    acc4[c] = (act && !LOCAL) ? *reinterpret_cast<const float4 *>(A.accum + k) : z;
+  }
+  const int bs = __ldg(A.bc_slot + e);
+  const int src = __ldg(A.src_head + e);
+  __syncthreads();
+  float a[NC][4];
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+    float dxi[NC], dga[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      dxi[c] = 0.f;
+      dga[c] = 0.f;
+#pragma unroll
+      for (int l = 0; l < NG; ++l) {
+        dxi[c] = fmaf(c_hp[ix * NG + l], (&su[c][iz * NG + l][j].x)[w], dxi[c]);
+        dga[c] = fmaf(c_hp[iz * NG + l], (&su[c][l * NG + ix][j].x)[w], dga[c]);
+      }
+    }
+    float Sx[NC], Sz[NC];
+    if (NC == 2) {
+      const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+      const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
+      const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+      const float lam = c0 - 2.f * mu;
+      const float sxx = c0 * du00 + lam * du11;
+      const float szz = c0 * du11 + lam * du00;
+      const float sxz = mu * (du01 + du10);
+      Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
+    } else {
+      Sx[0] = mu * (xix * dxi[0] + gax * dga[0]);
+      Sz[0] = mu * (xiz * dxi[0] + gaz * dga[0]);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      a[c][w] = jac * (Sx[c] * xix + Sz[c] * xiz);       // F0 for now
+      (&sF[c][1][q][j].x)[w] = jac * (Sx[c] * gax + Sz[c] * gaz);
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) sF[c][0][q][j] = make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
+  __syncthreads();
+  if (!act) return;
+#pragma unroll
+  for (int w = 0; w < 4; ++w) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+      for (int l = 0; l < NG; ++l) {
+        t1 = fmaf((&sF[c][0][iz * NG + l][j].x)[w], c_hpw[l * NG + ix], t1);
+        t2 = fmaf((&sF[c][1][l * NG + ix][j].x)[w], c_hpw[l * NG + iz], t2);
+      }
+      a[c][w] = -(c_w[iz] * t1 + c_w[ix] * t2);
+    }
+  }
+  if (bs >= 0) {
+    const size_t k = size_t(bs) * NP + q;
+    const float wq = A.bc_w[k];
+    if (wq != 0.f) {
+      const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
+      if (NC == 2) {
+        const float4 vx4 = *reinterpret_cast<const float4 *>(A.v + (size_t(g) * NC) * A.S + shot0);
+        const float4 vz4 = *reinterpret_cast<const float4 *>(A.v + (size_t(g) * NC + NC - 1) * A.S + shot0);
+        const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+#pragma unroll
+        for (int w = 0; w < 4; ++w) {
+          const float vx = (&vx4.x)[w], vz = (&vz4.x)[w];
+          const float vn = vx * nx + vz * nz;
+          const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vx * rvs;
+          const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vz * rvs;
+          a[0][w] += -1.f * fx * j1 * wq;
+          a[NC - 1][w] += -1.f * fz * j1 * wq;
+        }
+      } else {
+        const float4 v4 = *reinterpret_cast<const float4 *>(A.v + size_t(g) * A.S + shot0);
+#pragma unroll
+        for (int w = 0; w < 4; ++w) a[0][w] += -1.f * (wq * j1) * A.bc_imp1[k] * (&v4.x)[w];
+      }
+    }
+  }
+  if (src >= 0) {
+    const int step = *A.step;
+    for (int s = src; s >= 0; s = A.src_next[s]) {
+      const int w = A.src_shot[s] - shot0;
+      if (w < 0 || w > 3) continue;
+      const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        const float add = f * A.src_arr[(size_t(s) * 2 + c) * NP + q];
+        // the one-shot kernel adds sources in chain order; so does this loop
+        if (w == 0) a[c][0] += add;
+        else if (w == 1) a[c][1] += add;
+        else if (w == 2) a[c][2] += add;
+        else a[c][3] += add;
+      }
+    }
+  }
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    if (LOCAL) {
+      *reinterpret_cast<float4 *>(A.r + (p * NC + c) * A.S + shot0) =
+          make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
+    } else {
+      *reinterpret_cast<float4 *>(A.accum + (size_t(g) * NC + c) * A.S + shot0) =
+          make_float4(acc4[c].x + a[c][0], acc4[c].y + a[c][1], acc4[c].z + a[c][2], acc4[c].w + a[c][3]);
+    }
+  }
+}
+
+// Quad-shot updates (S a multiple of 4): flat float4 index over [nglob][NC][S].
+__global__ void __launch_bounds__(256) k_update_batched4(UpdateArgs A, int S) {
+  const int n4 = A.n >> 2;
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const float mi = A.minv[(4 * i) / S];
+    float4 ac = reinterpret_cast<const float4 *>(A.accum)[i];
+    float4 uu = reinterpret_cast<float4 *>(A.u)[i];
+    float4 vv = reinterpret_cast<float4 *>(A.v)[i];
+    float *pa = &ac.x, *pu = &uu.x, *pv = &vv.x;
+    float a[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      a[w] = __fmul_rn(pa[w], mi);
+      pv[w] = newmark_correct(pv[w], a[w], A.dt2);
+      if (A.predict) newmark_predict(pu[w], pv[w], a[w], A.dt, A.dt2, A.dtsq2);
+      bad |= !isfinite(pu[w]);
+    }
+    if (A.predict) reinterpret_cast<float4 *>(A.u)[i] = uu;
+    reinterpret_cast<float4 *>(A.v)[i] = vv;
+    reinterpret_cast<float4 *>(A.accum)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (A.a_store) reinterpret_cast<float4 *>(A.a_store)[i] = make_float4(a[0], a[1], a[2], a[3]);
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
+__global__ void __launch_bounds__(256) k_update_batched4_gather(UpdateArgs A, int S, int NC) {
+  const int n4 = A.n >> 2;
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n4; i += stride) {
+    const int s = (4 * i) % S;
+    const int gc = (4 * i) / S;
+    const int g = gc / NC, c = gc - g * NC;
+    float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
+    const int k1 = A.inv_start[g + 1];
+    for (int k = A.inv_start[g]; k < k1; ++k) {
+      const float4 t = *reinterpret_cast<const float4 *>(A.r + (size_t(A.inv_idx[k]) * NC + c) * S + s);
+      acc.x = acc.x + t.x; acc.y = acc.y + t.y; acc.z = acc.z + t.z; acc.w = acc.w + t.w;
+    }
+    const float mi = A.minv[gc];
+    float4 uu = reinterpret_cast<float4 *>(A.u)[i];
+    float4 vv = reinterpret_cast<float4 *>(A.v)[i];
+    float *pc = &acc.x, *pu = &uu.x, *pv = &vv.x;
+    float a[4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+      a[w] = __fmul_rn(pc[w], mi);
+      pv[w] = newmark_correct(pv[w], a[w], A.dt2);
+      if (A.predict) newmark_predict(pu[w], pv[w], a[w], A.dt, A.dt2, A.dtsq2);
+      bad |= !isfinite(pu[w]);
+    }
+    if (A.predict) reinterpret_cast<float4 *>(A.u)[i] = uu;
+    reinterpret_cast<float4 *>(A.v)[i] = vv;
+    if (A.a_store) reinterpret_cast<float4 *>(A.a_store)[i] = make_float4(a[0], a[1], a[2], a[3]);
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
 // a = accum * M^-1 (M^-1 shared by the shots); corrector; optional fused
 // predictor; accumulator clear.  Flat index i over [nglob][NC][S].
 __global__ void __launch_bounds__(256) k_update_batched(UpdateArgs A, int S) {

@@ -278,20 +278,37 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
   B.step = step;
   B.u = el.u; B.v = el.v; B.accum = el.accum; B.r = el.r;
   B.S = el.S;
+  // quad-shot kernels when the shots come in fours
+  const bool quad = el.S % 4 == 0;
+  const int T = std::min(8, el.S / 4);
+  const int tiles = quad ? (el.S + 4 * T - 1) / (4 * T) : (el.S + 31) / 32;
+  const int threads = quad ? sfg::dev::NP * T : sfg::dev::NP * 32;
+  auto launch = [&](int e0, int n, bool local) {
+    B.e0 = e0;
+    const dim3 grid(n, tiles);
+    if (quad) {
+      if (el.ncomp == 2) {
+        if (local) sfg::dev::k_stiffness_batched4<2, true><<<grid, threads, 0, s>>>(B, T);
+        else sfg::dev::k_stiffness_batched4<2, false><<<grid, threads, 0, s>>>(B, T);
+      } else {
+        if (local) sfg::dev::k_stiffness_batched4<1, true><<<grid, threads, 0, s>>>(B, T);
+        else sfg::dev::k_stiffness_batched4<1, false><<<grid, threads, 0, s>>>(B, T);
+      }
+    } else if (el.ncomp == 2) {
+      if (local) sfg::dev::k_stiffness_batched<2, true><<<grid, threads, 0, s>>>(B);
+      else sfg::dev::k_stiffness_batched<2, false><<<grid, threads, 0, s>>>(B);
+    } else {
+      if (local) sfg::dev::k_stiffness_batched<1, true><<<grid, threads, 0, s>>>(B);
+      else sfg::dev::k_stiffness_batched<1, false><<<grid, threads, 0, s>>>(B);
+    }
+  };
   if (variant == 3) {
-    B.e0 = 0;
-    const dim3 grid(el.nspec, (el.S + 31) / 32);
-    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2, true><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
-    else sfg::dev::k_stiffness_batched<1, true><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    launch(0, el.nspec, true);
     return;
   }
   for (int c = 0; c < ncolors(el); ++c) {
-    B.e0 = el.color_start[c];
-    const int n = el.color_start[c + 1] - B.e0;
-    if (n <= 0) continue;
-    const dim3 grid(n, (el.S + 31) / 32);
-    if (el.ncomp == 2) sfg::dev::k_stiffness_batched<2, false><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
-    else sfg::dev::k_stiffness_batched<1, false><<<grid, sfg::dev::NP * 32, 0, s>>>(B);
+    const int n = el.color_start[c + 1] - el.color_start[c];
+    if (n > 0) launch(el.color_start[c], n, false);
   }
 }
 
@@ -379,12 +396,15 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
   const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
   sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
   if (h->variant == 3) {
-    if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
+    if (D.S > 1 && D.S % 4 == 0)
+      sfg::dev::k_update_batched4_gather<<<grid_for(U.n / 4), 256, 0, s>>>(U, D.S, D.ncomp);
+    else if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.ncomp == 2) sfg::dev::k_update_gather<2><<<grid_for(U.n / 2), 256, 0, s>>>(U);
     else sfg::dev::k_update_gather<1><<<grid_for(U.n), 256, 0, s>>>(U);
     return;
   }
-  if (D.S > 1) sfg::dev::k_update_batched<<<grid_for(U.n), 256, 0, s>>>(U, D.S);
+  if (D.S > 1 && D.S % 4 == 0) sfg::dev::k_update_batched4<<<grid_for(U.n / 4), 256, 0, s>>>(U, D.S);
+  else if (D.S > 1) sfg::dev::k_update_batched<<<grid_for(U.n), 256, 0, s>>>(U, D.S);
   else sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
 }
 
