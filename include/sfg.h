@@ -170,6 +170,25 @@ int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *glob_to_elastic,
 /* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
 int sfg_check_finite(sfg_handle *h);
 
+/* ---- adjoint (2D elastic P-SV, one shot, displacement seismograms every step) ----
+ * Replace the model by per-GLL-point rho, kappa, mu ([nspec][25], database
+ * element order; kappa = lambda + 2/3 mu as the reference stores it).
+ * Reference: the property container, core/specfem/assembly/properties. */
+int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const float *mu);
+/* Forward run of nsteps steps from rest that keeps the state every `interval`
+ * steps on the device (seismograms as sfg_run).  Replaces the reference's
+ * forward-wavefield dump for adjoint runs (include/io/wavefield/writer.tpp). */
+int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval);
+/* Gradient of a misfit L with respect to rho, kappa, mu at every GLL point
+ * ([nspec][25], database element order) given seis_grad = dL/d(seismogram)
+ * [nsteps][nrec][2]: the reverse sweep recomputes each checkpoint segment and
+ * runs the discrete adjoint of the time step.  Replaces the reference's
+ * combined adjoint/backward run and compute_material_derivatives
+ * (core/specfem/solver/time_marching.tpp:133-264,
+ *  include/kokkos_kernels/impl/compute_material_derivatives.tpp:14-153). */
+int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho, float *grad_kappa,
+                         float *grad_mu);
+
 /* One time step of the handle's elastic model on device buffers the caller
  * owns, with no device memory allocated by the call.  This entry point has no
  * counterpart in the reference.  It is for callers that cannot call

@@ -257,6 +257,162 @@ bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
   return true;
 }
 
+// --------------------------------------------------- model-dependent part ---
+// Material words, Stacey impedances, the assembled Stacey matrices and the
+// inverse mass matrix: everything that changes when the model changes.
+void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
+  const double dt = a.dt;
+  double w[NGLL];
+  for (int i = 0; i < NGLL; ++i) w[i] = double(a.wgll_d[i]);
+  auto model = [&](int e, size_t pm, double &rho, double &vp, double &vs) {
+    const int mat = m.kmato[e];
+    rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
+    vp = m.pvp.empty() ? m.mat_vp[mat] : m.pvp[pm];
+    vs = m.pvs.empty() ? m.mat_vs[mat] : m.pvs[pm];
+  };
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    const size_t n = size_t(D.nspec) * NPTS;
+    D.prop0.resize(n);
+    D.prop1.resize(n);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      for (int q = 0; q < NPTS; ++q) {
+        const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
+        double rho, vp, vs;
+        model(e, pm, rho, vp, vs);
+        if (med == 1) {
+          // kappa = rho (vp^2 - 4/3 vs^2), mu = rho vs^2; lambda+2mu = kappa + 4/3 mu
+          // (include/medium/dim2/elastic/isotropic/material.hpp:66-69, properties.hpp:71-91)
+          const double mu = rho * vs * vs;
+          const double kappa = rho * (vp * vp - 4.0 / 3.0 * vs * vs);
+          D.prop0[pc] = float(kappa + 4.0 / 3.0 * mu);
+          D.prop1[pc] = float(mu);
+        } else {
+          D.prop0[pc] = float(1.0 / rho);            // rho_inverse
+          D.prop1[pc] = float(rho * vp * vp);        // kappa
+        }
+      }
+    }
+    // Stacey impedances
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      if (D.bc_slot[ce] < 0) continue;
+      const int e = D.elem_mesh[ce];
+      for (int q = 0; q < NPTS; ++q) {
+        const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
+        if (D.bc_w[k] == 0.0f) continue;
+        const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
+        double rho, vp, vs;
+        model(e, pm, rho, vp, vs);
+        if (med == 1) {
+          // rho*vp = sqrt((lambda+2mu)/rho)*rho, rho*vs = sqrt(rho*mu) (properties.hpp:77-87)
+          const double l2m = D.prop0[pc], mu = D.prop1[pc];
+          D.bc_imp0[k] = float(std::sqrt(l2m / rho) * rho);
+          D.bc_imp1[k] = float(std::sqrt(rho * mu));
+        } else {
+          // 1/(rho vp) = sqrt(rho_inverse / kappa) (acoustic properties.hpp:69-72)
+          D.bc_imp0[k] = float(std::sqrt(double(D.prop0[pc]) / double(D.prop1[pc])));
+        }
+      }
+    }
+  }
+  // assembled per-point Stacey matrices of the elastic P-SV medium: the
+  // traction of an element point is -C_e v with C_e = w |n| [(rho vp - rho vs)
+  // n n^T / |n|^2 + rho vs I] (stacey.tpp:50-80); the adjoint applies C^T = C
+  {
+    MediumData &D = a.el;
+    D.stacey_pt.clear();
+    D.stacey_c.clear();
+    if (D.ncomp == 2) {
+      std::unordered_map<int, size_t> slot;
+      for (int ce = 0; ce < D.nspec; ++ce) {
+        if (D.bc_slot[ce] < 0) continue;
+        for (int q = 0; q < NPTS; ++q) {
+          const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
+          if (D.bc_w[k] == 0.0f) continue;
+          const int g = D.ibool[size_t(ce) * NPTS + q];
+          auto it = slot.find(g);
+          size_t j;
+          if (it == slot.end()) {
+            j = D.stacey_pt.size();
+            slot[g] = j;
+            D.stacey_pt.push_back(g);
+            D.stacey_c.resize(3 * (j + 1), 0.0f);
+          } else {
+            j = it->second;
+          }
+          const double nx = D.bc_nx[k], nz = D.bc_nz[k], j1 = D.bc_j1[k], wq = D.bc_w[k];
+          const double rvp = D.bc_imp0[k], rvs = D.bc_imp1[k];
+          const double f = wq * j1, d = (rvp - rvs) / (j1 * j1);
+          D.stacey_c[3 * j + 0] += float(f * (d * nx * nx + rvs));
+          D.stacey_c[3 * j + 1] += float(f * (d * nx * nz));
+          D.stacey_c[3 * j + 2] += float(f * (d * nz * nz + rvs));
+        }
+      }
+    }
+  }
+  // --- mass matrix (+ Stacey implicit term), inverted -------------
+  // M = sum rho w_x w_z |J| (acoustic: 1/kappa), plus (dt/2) C on Stacey points
+  // (compute_mass_matrix.tpp:95-121, stacey.tpp:817-853), then 1/M.
+  for (int med = 0; med < 2; ++med) {
+    MediumData &D = med == 1 ? a.el : a.ac;
+    std::vector<double> M(size_t(D.nglob) * D.ncomp, 0.0);
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      for (int iz = 0; iz < NGLL; ++iz)
+        for (int ix = 0; ix < NGLL; ++ix) {
+          const int q = iz * NGLL + ix;
+          const size_t pc = size_t(ce) * NPTS + q, pm = size_t(e) * NPTS + q;
+          const double fac = w[ix] * w[iz] * a.jac_d[pm];
+          double rho, vp, vs;
+          model(e, pm, rho, vp, vs);
+          double mc[2];
+          if (med == 1) mc[0] = mc[1] = rho * fac;
+          else mc[0] = (1.0 / double(D.prop1[pc])) * fac;
+          if (D.bc_slot[ce] >= 0) {
+            const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
+            if (D.bc_w[k] != 0.0f) {
+              const double vv = -dt * 0.5;  // velocity stand-in of the implicit term
+              const double nx = D.bc_nx[k], nz = D.bc_nz[k], j1 = D.bc_j1[k], wq = D.bc_w[k];
+              if (med == 0) {
+                mc[0] += -1.0 * wq * j1 * double(D.bc_imp0[k]) * vv;
+              } else if (D.ncomp == 1) {
+                mc[0] += -1.0 * wq * j1 * double(D.bc_imp1[k]) * vv;
+              } else {
+                const double vn = vv * nx + vv * nz;
+                const double dn[2] = {nx, nz};
+                for (int c = 0; c < 2; ++c) {
+                  const double f = ((vn * dn[c] / (j1 * j1)) * (double(D.bc_imp0[k]) - double(D.bc_imp1[k]))) +
+                                   vv * double(D.bc_imp1[k]);
+                  mc[c] += -1.0 * f * j1 * wq;
+                }
+              }
+            }
+          }
+          const int g = D.ibool[pc];
+          for (int c = 0; c < D.ncomp; ++c) M[size_t(g) * D.ncomp + c] += mc[c];
+        }
+    }
+    D.minv.resize(M.size());
+    for (size_t i = 0; i < M.size(); ++i) D.minv[i] = float(1.0 / M[i]);
+  }
+}
+
+void set_model2d(Mesh2D &m, Assembly2D &a, const float *rho, const float *kappa, const float *mu) {
+  const size_t n = size_t(m.nspec) * NPTS;
+  m.prho.resize(n);
+  m.pvp.resize(n);
+  m.pvs.resize(n);
+  for (size_t p = 0; p < n; ++p) {
+    if (!(rho[p] > 0) || !(mu[p] >= 0) || !(kappa[p] + 4.0 / 3.0 * mu[p] > 0))
+      throw std::runtime_error("model values must give rho > 0, mu >= 0, lambda + 2 mu > 0");
+    m.prho[p] = rho[p];
+    m.pvs[p] = float(std::sqrt(double(mu[p]) / rho[p]));
+    m.pvp[p] = float(std::sqrt((double(kappa[p]) + 4.0 / 3.0 * double(mu[p])) / rho[p]));
+  }
+  assemble_model2d(m, a);
+}
+
 // ------------------------------------------------------------ assembly ---
 void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
   const int nspec = m.nspec;
@@ -266,7 +422,7 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
   a.elastic_wave = m.elastic_wave;
   double z[NGLL], w[NGLL], hp[NGLL][NGLL];
   gll(z, w, hp);
-  for (int i = 0; i < NGLL; ++i) { a.zgll[i] = z[i]; a.wgll[i] = float(w[i]); }
+  for (int i = 0; i < NGLL; ++i) { a.zgll[i] = z[i]; a.wgll[i] = float(w[i]); a.wgll_d[i] = w[i]; }
   for (int i = 0; i < NGLL; ++i)
     for (int j = 0; j < NGLL; ++j) {
       a.hprime[i * NGLL + j] = float(hp[i][j]);
@@ -483,29 +639,13 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
     }
     const size_t n = size_t(D.nspec) * NPTS;
     D.xix.resize(n); D.xiz.resize(n); D.gax.resize(n); D.gaz.resize(n); D.jac.resize(n);
-    D.prop0.resize(n); D.prop1.resize(n);
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
-      const int mat = m.kmato[e];
       for (int q = 0; q < NPTS; ++q) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         D.xix[pc] = float(J[pm].xix); D.xiz[pc] = float(J[pm].xiz);
         D.gax[pc] = float(J[pm].gax); D.gaz[pc] = float(J[pm].gaz);
         D.jac[pc] = float(J[pm].jac);
-        const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
-        const double vp = m.pvp.empty() ? m.mat_vp[mat] : m.pvp[pm];
-        const double vs = m.pvs.empty() ? m.mat_vs[mat] : m.pvs[pm];
-        if (med == 1) {
-          // kappa = rho (vp^2 - 4/3 vs^2), mu = rho vs^2; lambda+2mu = kappa + 4/3 mu
-          // (include/medium/dim2/elastic/isotropic/material.hpp:66-69, properties.hpp:71-91)
-          const double mu = rho * vs * vs;
-          const double kappa = rho * (vp * vp - 4.0 / 3.0 * vs * vs);
-          D.prop0[pc] = float(kappa + 4.0 / 3.0 * mu);
-          D.prop1[pc] = float(mu);
-        } else {
-          D.prop0[pc] = float(1.0 / rho);            // rho_inverse
-          D.prop1[pc] = float(rho * vp * vp);        // kappa
-        }
       }
     }
   }
@@ -538,76 +678,20 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       const auto &v = bc[D.elem_mesh[ce]];
       for (int q = 0; q < NPTS; ++q) {
         const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
-        const size_t pc = size_t(ce) * NPTS + q;
         if (v[q].st) {
           D.bc_w[k] = float(v[q].w);
           D.bc_nx[k] = float(v[q].nx);
           D.bc_nz[k] = float(v[q].nz);
           D.bc_j1[k] = float(std::sqrt(v[q].nx * v[q].nx + v[q].nz * v[q].nz));
-          const int e = D.elem_mesh[ce];
-          const size_t pm = size_t(e) * NPTS + q;
-          const int mat = m.kmato[e];
-          const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
-          if (med == 1) {
-            // rho*vp = sqrt((lambda+2mu)/rho)*rho, rho*vs = sqrt(rho*mu) (properties.hpp:77-87)
-            const double l2m = D.prop0[pc], mu = D.prop1[pc];
-            D.bc_imp0[k] = float(std::sqrt(l2m / rho) * rho);
-            D.bc_imp1[k] = float(std::sqrt(rho * mu));
-          } else {
-            // 1/(rho vp) = sqrt(rho_inverse / kappa) (acoustic properties.hpp:69-72)
-            D.bc_imp0[k] = float(std::sqrt(double(D.prop0[pc]) / double(D.prop1[pc])));
-          }
         }
         if (v[q].fs) D.bc_keep[k] = 0.0f;
       }
     }
   }
 
-  // --- mass matrix (+ Stacey implicit term), inverted -------------
-  // M = sum rho w_x w_z |J| (acoustic: 1/kappa), plus (dt/2) C on Stacey points
-  // (compute_mass_matrix.tpp:95-121, stacey.tpp:817-853), then 1/M.
-  for (int med = 0; med < 2; ++med) {
-    MediumData &D = med == 1 ? a.el : a.ac;
-    std::vector<double> M(size_t(D.nglob) * D.ncomp, 0.0);
-    for (int ce = 0; ce < D.nspec; ++ce) {
-      const int e = D.elem_mesh[ce];
-      const int mat = m.kmato[e];
-      for (int iz = 0; iz < NGLL; ++iz)
-        for (int ix = 0; ix < NGLL; ++ix) {
-          const int q = iz * NGLL + ix;
-          const size_t pc = size_t(ce) * NPTS + q, pm = size_t(e) * NPTS + q;
-          const double fac = w[ix] * w[iz] * J[pm].jac;
-          const double rho = m.prho.empty() ? m.mat_rho[mat] : m.prho[pm];
-          double mc[2];
-          if (med == 1) mc[0] = mc[1] = rho * fac;
-          else mc[0] = (1.0 / double(D.prop1[pc])) * fac;
-          if (D.bc_slot[ce] >= 0) {
-            const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
-            if (D.bc_w[k] != 0.0f) {
-              const double vv = -dt * 0.5;  // velocity stand-in of the implicit term
-              const double nx = D.bc_nx[k], nz = D.bc_nz[k], j1 = D.bc_j1[k], wq = D.bc_w[k];
-              if (med == 0) {
-                mc[0] += -1.0 * wq * j1 * double(D.bc_imp0[k]) * vv;
-              } else if (D.ncomp == 1) {
-                mc[0] += -1.0 * wq * j1 * double(D.bc_imp1[k]) * vv;
-              } else {
-                const double vn = vv * nx + vv * nz;
-                const double dn[2] = {nx, nz};
-                for (int c = 0; c < 2; ++c) {
-                  const double f = ((vn * dn[c] / (j1 * j1)) * (double(D.bc_imp0[k]) - double(D.bc_imp1[k]))) +
-                                   vv * double(D.bc_imp1[k]);
-                  mc[c] += -1.0 * f * j1 * wq;
-                }
-              }
-            }
-          }
-          const int g = D.ibool[pc];
-          for (int c = 0; c < D.ncomp; ++c) M[size_t(g) * D.ncomp + c] += mc[c];
-        }
-    }
-    D.minv.resize(M.size());
-    for (size_t i = 0; i < M.size(); ++i) D.minv[i] = float(1.0 / M[i]);
-  }
+  a.jac_d.resize(nloc);
+  for (size_t p = 0; p < nloc; ++p) a.jac_d[p] = J[p].jac;
+  assemble_model2d(m, a);
 }
 
 // ------------------------------------------------------ point location ---

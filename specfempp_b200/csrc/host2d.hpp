@@ -62,6 +62,9 @@ struct MediumData {
   // indices (compute element * 25 + GLL point) that contribute to it, in
   // increasing compute order (= colour order)
   std::vector<int> inv_start, inv_idx;
+  // assembled Stacey matrices (elastic P-SV): point ids and (Cxx, Cxz, Czz)
+  std::vector<int> stacey_pt;
+  std::vector<float> stacey_c;
 };
 
 struct Assembly2D {
@@ -71,7 +74,9 @@ struct Assembly2D {
   float hprime[NPTS];                 // hprime[i*5+j] = l'_j(xi_i)
   float hpw[NPTS];                    // hprime[l*5+i] * w[l]  (divergence form)
   float wgll[NGLL];
+  double wgll_d[NGLL];
   double zgll[NGLL];
+  std::vector<double> jac_d;          // [nspec][25] mesh order, |J| in FP64
   std::vector<int> ibool_global;      // [nspec][25] mesh order
   std::vector<double> gx, gz;         // [nspec][25] mesh order, GLL point coordinates
   MediumData el, ac;
@@ -104,6 +109,10 @@ struct Assembly2D {
 // Build everything but sources/receivers (numbering, geometry, colouring,
 // boundaries, coupling, mass matrix).  Throws std::runtime_error on error.
 void assemble2d(const Mesh2D &m, double dt, Assembly2D &a);
+// Model-dependent arrays (material words, Stacey impedances and matrices, M^-1).
+void assemble_model2d(const Mesh2D &m, Assembly2D &a);
+// Replace the model by per-GLL-point rho, kappa, mu ([nspec][25], mesh order).
+void set_model2d(Mesh2D &m, Assembly2D &a, const float *rho, const float *kappa, const float *mu);
 void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &src);
 void set_receivers2d(const Mesh2D &m, Assembly2D &a, const std::vector<double> &x,
                      const std::vector<double> &z, double angle, const std::vector<int> &types);

@@ -411,7 +411,7 @@ __global__ void __launch_bounds__(32) k_receivers_batched(RecArgs A, int S) {
     const int shot = s0 + threadIdx.x;
     if (shot >= S) continue;
     for (int t = 0; t < A.ntypes; ++t) {
-      float o[2] = {0.f, 0.f};
+      float tr[2] = {0.f, 0.f};
       for (int c = 0; c < NC; ++c) {
         // the 25 weighted values, summed in the order of the single-shot
         // kernel's xor butterfly (lane i + lane i^o), so traces match it bitwise
@@ -441,11 +441,11 @@ __global__ void __launch_bounds__(32) k_receivers_batched(RecArgs A, int S) {
         for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
           for (int i = 0; i < o; ++i) x[i] = x[i] + x[i + o];
-        o[c] = x[0];
+        tr[c] = x[0];
       }
       float *dst = A.seis + (((size_t(shot) * A.nsig + isig) * A.ntypes + t) * A.nrec_total + r) * 2;
-      dst[0] = o[0];
-      dst[1] = NC > 1 ? o[1] : 0.f;
+      dst[0] = tr[0];
+      dst[1] = NC > 1 ? tr[1] : 0.f;
     }
   }
 }

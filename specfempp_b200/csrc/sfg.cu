@@ -16,6 +16,7 @@
 #include "host2d.hpp"
 #include "kernels2d.cuh"
 #include "kernels2d_batched.cuh"
+#include "kernels2d_adjoint.cuh"
 
 namespace {
 
@@ -88,7 +89,25 @@ struct DevMedium {
 
 }  // namespace
 
+// Device state of the adjoint (allocated on first use).
+struct AdjointState {
+  int nstep = 0, interval = 0, ncheck = 0;
+  size_t nvals = 0, nloc = 0;
+  float *ckpt = nullptr;                        // [ncheck][u, v, a][nvals]
+  float *seg_u = nullptr, *seg_a = nullptr;     // [interval][nvals]
+  float *lu = nullptr, *lv = nullptr, *la = nullptr, *mu = nullptr;
+  float *r = nullptr;                           // [nloc][2]
+  float *sum = nullptr, *comp = nullptr, *seg = nullptr;  // [3][nloc]: kappa, mu, rho
+  float *gtab = nullptr;                        // [nstep][nrec][2]
+  int *ad_head = nullptr, *ad_next = nullptr;
+  int *st_pt = nullptr;
+  float *st_c = nullptr;
+  int nst = 0;
+  bool forward_done = false;
+};
+
 struct sfg_handle {
+  AdjointState adj;
   sfg::Mesh2D mesh;
   sfg::Assembly2D asmb;
   sfg_options opt{};
@@ -122,6 +141,11 @@ struct sfg_handle {
   sfg::dev::Quad quad{};
 
   ~sfg_handle() {
+    for (void *p : {(void *)adj.ckpt, (void *)adj.seg_u, (void *)adj.seg_a, (void *)adj.lu, (void *)adj.lv,
+                    (void *)adj.la, (void *)adj.mu, (void *)adj.r, (void *)adj.sum, (void *)adj.comp,
+                    (void *)adj.seg, (void *)adj.gtab, (void *)adj.ad_head, (void *)adj.ad_next,
+                    (void *)adj.st_pt, (void *)adj.st_c})
+      if (p) cudaFree(p);
     if (graph_k) cudaGraphExecDestroy(graph_k);
     if (graph_1) cudaGraphExecDestroy(graph_1);
     if (graph_e) cudaGraphExecDestroy(graph_e);
@@ -1107,6 +1131,238 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
     sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
     SFG_CUDA(cudaGetLastError());
     SFG_CUDA(cudaStreamSynchronize(s));
+    return int(SFG_OK);
+  });
+}
+
+// ---------------------------------------------------------------- adjoint ---
+
+int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const float *mu) {
+  return guarded(h, [&]() {
+    if (!rho || !kappa || !mu) return int(SFG_ERR_ARG);
+    sfg::set_model2d(h->mesh, h->asmb, rho, kappa, mu);
+    if (h->initialized) {
+      for (int med = 0; med < 2; ++med) {
+        const sfg::MediumData &M = med == 1 ? h->asmb.el : h->asmb.ac;
+        DevMedium &D = med == 1 ? h->el : h->ac;
+        if (!D.nspec) continue;
+        auto put = [&](float *d, const std::vector<float> &v) {
+          if (d && !v.empty()) SFG_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(float), cudaMemcpyHostToDevice));
+        };
+        put(D.prop0, M.prop0); put(D.prop1, M.prop1);
+        put(D.bc_imp0, M.bc_imp0); put(D.bc_imp1, M.bc_imp1);
+        put(D.minv, M.minv);
+      }
+      if (h->adj.st_c && !h->asmb.el.stacey_c.empty())
+        SFG_CUDA(cudaMemcpy(h->adj.st_c, h->asmb.el.stacey_c.data(), h->asmb.el.stacey_c.size() * sizeof(float),
+                            cudaMemcpyHostToDevice));
+      h->adj.forward_done = false;
+    }
+    return int(SFG_OK);
+  });
+}
+
+}  // extern "C"
+
+namespace {
+
+int adjoint_checks(sfg_handle *h) {
+  if (!h->initialized) { h->err = "sfg_initialize first"; return SFG_ERR_STATE; }
+  const sfg::Assembly2D &a = h->asmb;
+  if (h->ac.nspec || !h->el.nspec || h->el.ncomp != 2 || h->el.S != 1 || a.nsb != 1 ||
+      a.ntypes != 1 || a.types[0] != SFG_SEIS_DISPLACEMENT) {
+    h->err = "the adjoint needs one elastic P-SV medium, one shot, and displacement seismograms "
+             "sampled every step";
+    return SFG_ERR_UNSUPPORTED;
+  }
+  return SFG_OK;
+}
+
+template <typename T>
+T *dalloc(size_t n) {
+  T *p = nullptr;
+  SFG_CUDA(cudaMalloc(&p, std::max<size_t>(n, 1) * sizeof(T)));
+  SFG_CUDA(cudaMemset(p, 0, std::max<size_t>(n, 1) * sizeof(T)));
+  return p;
+}
+
+void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
+  AdjointState &A = h->adj;
+  const size_t nvals = h->el.values();
+  const size_t nloc = size_t(h->el.nspec) * sfg::NPTS;
+  const int ncheck = (nstep + interval - 1) / interval;
+  const bool resize = A.nvals != nvals || A.interval != interval || A.ncheck < ncheck;
+  if (resize) {
+    for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a})
+      if (*p) { cudaFree(*p); *p = nullptr; }
+    A.ckpt = dalloc<float>(size_t(ncheck) * 3 * (nvals + 4));
+    A.seg_u = dalloc<float>(size_t(interval) * (nvals + 4));
+    A.seg_a = dalloc<float>(size_t(interval) * (nvals + 4));
+  }
+  if (!A.lu) {
+    A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4);
+    A.la = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
+    A.r = dalloc<float>(2 * nloc);
+    A.sum = dalloc<float>(3 * nloc); A.comp = dalloc<float>(3 * nloc); A.seg = dalloc<float>(3 * nloc);
+    // receivers as adjoint sources: chain per elastic compute element
+    const sfg::Assembly2D &as = h->asmb;
+    std::vector<int> head(h->el.nspec, -1), next(std::max(as.nrec, 1), -1);
+    for (int r = 0; r < as.nrec; ++r) {
+      next[r] = head[as.rec_elem[r]];
+      head[as.rec_elem[r]] = r;
+    }
+    A.ad_head = dalloc<int>(head.size());
+    SFG_CUDA(cudaMemcpy(A.ad_head, head.data(), head.size() * sizeof(int), cudaMemcpyHostToDevice));
+    A.ad_next = dalloc<int>(next.size());
+    SFG_CUDA(cudaMemcpy(A.ad_next, next.data(), next.size() * sizeof(int), cudaMemcpyHostToDevice));
+    const auto &sp = as.el.stacey_pt;
+    const auto &sc = as.el.stacey_c;
+    A.nst = int(sp.size());
+    A.st_pt = dalloc<int>(sp.size());
+    A.st_c = dalloc<float>(sc.size());
+    if (!sp.empty()) {
+      SFG_CUDA(cudaMemcpy(A.st_pt, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice));
+      SFG_CUDA(cudaMemcpy(A.st_c, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+  }
+  A.nvals = nvals;
+  A.nloc = nloc;
+  A.interval = interval;
+  A.ncheck = ncheck;
+  A.nstep = nstep;
+}
+
+void save_state(sfg_handle *h, float *dst) {
+  const size_t n = h->el.values() + 4;
+  SFG_CUDA(cudaMemcpyAsync(dst, h->el.u, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(dst + n, h->el.v, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, h->el.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+}
+
+void restore_state(sfg_handle *h, const float *src, int step) {
+  const size_t n = h->el.values() + 4;
+  SFG_CUDA(cudaMemcpyAsync(h->el.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(h->el.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(h->el.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(h->d_step, &step, sizeof(int), cudaMemcpyHostToDevice, h->stream));
+  SFG_CUDA(cudaStreamSynchronize(h->stream));
+  h->state_final = true;
+  h->host_step = step;
+}
+
+}  // namespace
+
+extern "C" {
+
+int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval) {
+  return guarded(h, [&]() {
+    const int rc = adjoint_checks(h);
+    if (rc != SFG_OK) return rc;
+    if (nsteps <= 0 || nsteps > h->asmb.nstep || interval <= 0) {
+      h->err = "need 0 < nsteps <= nstep and interval > 0";
+      return int(SFG_ERR_ARG);
+    }
+    adjoint_alloc(h, nsteps, std::min(interval, nsteps));
+    AdjointState &A = h->adj;
+    const int ret = sfg_reset_fields(h);
+    if (ret != SFG_OK) return ret;
+    const size_t stride = 3 * (A.nvals + 4);
+    for (int c = 0; c < A.ncheck; ++c) {
+      save_state(h, A.ckpt + size_t(c) * stride);
+      run_steps(h, std::min(A.interval, nsteps - c * A.interval));
+    }
+    SFG_CUDA(cudaStreamSynchronize(h->stream));
+    A.forward_done = true;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho, float *grad_kappa,
+                         float *grad_mu) {
+  return guarded(h, [&]() {
+    const int rc = adjoint_checks(h);
+    if (rc != SFG_OK) return rc;
+    AdjointState &A = h->adj;
+    if (!A.forward_done) { h->err = "run sfg_forward_checkpointed first"; return int(SFG_ERR_STATE); }
+    if (!seis_grad) return int(SFG_ERR_ARG);
+    const sfg::Assembly2D &as = h->asmb;
+    const int nrec = as.nrec;
+    cudaStream_t s = h->stream;
+    // dL/d(seismogram) of every step on the device: [nstep][nrec][2]
+    if (A.gtab) cudaFree(A.gtab);
+    A.gtab = dalloc<float>(size_t(A.nstep) * nrec * 2);
+    if (nrec) {
+      // the seismograms leave the library rotated by the receiver angle
+      // (sfg_get_seismograms); the adjoint sources are rotated back
+      std::vector<float> g(size_t(A.nstep) * nrec * 2);
+      const float ca = std::cos(float(M_PI) / 180.f * float(as.rec_angle));
+      const float sa = std::sin(float(M_PI) / 180.f * float(as.rec_angle));
+      for (size_t i = 0; i < g.size(); i += 2) {
+        g[i] = ca * seis_grad[i] + sa * seis_grad[i + 1];
+        g[i + 1] = -sa * seis_grad[i] + ca * seis_grad[i + 1];
+      }
+      SFG_CUDA(cudaMemcpy(A.gtab, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    const size_t nv = A.nvals;
+    for (float *p : {A.lu, A.lv, A.la, A.mu})
+      SFG_CUDA(cudaMemsetAsync(p, 0, (nv + 4) * sizeof(float), s));
+    for (float *p : {A.sum, A.comp, A.seg})
+      SFG_CUDA(cudaMemsetAsync(p, 0, 3 * A.nloc * sizeof(float), s));
+    const float dt = float(as.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
+    sfg::dev::AdjArgs J{};
+    const DevMedium &D = h->el;
+    J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
+    J.prop0 = D.prop0; J.prop1 = D.prop1;
+    J.mu = A.mu; J.r = A.r;
+    J.seg_k = A.seg; J.seg_m = A.seg + A.nloc; J.seg_r = A.seg + 2 * A.nloc;
+    J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
+    J.nspec = D.nspec;
+    J.quad = h->quad;
+    constexpr int E = 8;
+    const int eblocks = (D.nspec + E - 1) / E;
+    const int npts = D.nglob;
+    const size_t stride = 3 * (nv + 4);
+    for (int c = A.ncheck - 1; c >= 0; --c) {
+      const int k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
+      // recompute the segment's forward states from its checkpoint
+      restore_state(h, A.ckpt + size_t(c) * stride, k0);
+      for (int k = k0; k < k1; ++k) {
+        resume(h);
+        SFG_CUDA(cudaGraphLaunch(h->graph_e, s));
+        h->state_final = true;
+        SFG_CUDA(cudaMemcpyAsync(A.seg_u + size_t(k - k0) * (nv + 4), D.u, nv * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, s));
+        SFG_CUDA(cudaMemcpyAsync(A.seg_a + size_t(k - k0) * (nv + 4), D.a, nv * sizeof(float),
+                                 cudaMemcpyDeviceToDevice, s));
+      }
+      // reverse sweep over the segment
+      for (int k = k1 - 1; k >= k0; --k) {
+        sfg::dev::k_adj_pre<<<grid_for(int(nv)), 256, 0, s>>>(A.la, A.lv, D.minv, A.mu, int(nv), dt2);
+        J.uf = A.seg_u + size_t(k - k0) * (nv + 4);
+        J.af = A.seg_a + size_t(k - k0) * (nv + 4);
+        J.ad_g = A.gtab + size_t(k) * nrec * 2;
+        sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, s>>>(J);
+        sfg::dev::k_adj_post<<<grid_for(npts), 256, 0, s>>>(A.lu, A.lv, A.la, A.r, D.inv_start, D.inv_idx,
+                                                            npts, dt, dt2, dtsq2);
+        if (A.nst)
+          sfg::dev::k_adj_stacey<<<grid_for(A.nst), 256, 0, s>>>(A.lv, A.la, A.mu, A.st_pt, A.st_c, A.nst, dt2);
+      }
+      sfg::dev::k_kahan_fold<<<grid_for(int(3 * A.nloc)), 256, 0, s>>>(A.sum, A.comp, A.seg, int(3 * A.nloc));
+      SFG_CUDA(cudaGetLastError());
+    }
+    SFG_CUDA(cudaStreamSynchronize(s));
+    // compute order -> mesh order
+    std::vector<float> tot(3 * A.nloc);
+    SFG_CUDA(cudaMemcpy(tot.data(), A.sum, tot.size() * sizeof(float), cudaMemcpyDeviceToHost));
+    float *outs[3] = {grad_kappa, grad_mu, grad_rho};
+    for (int t = 0; t < 3; ++t) {
+      if (!outs[t]) continue;
+      for (int ce = 0; ce < D.nspec; ++ce) {
+        const int e = as.el.elem_mesh[ce];
+        for (int q = 0; q < sfg::NPTS; ++q)
+          outs[t][size_t(e) * sfg::NPTS + q] = tot[size_t(t) * A.nloc + size_t(ce) * sfg::NPTS + q];
+      }
+    }
     return int(SFG_OK);
   });
 }

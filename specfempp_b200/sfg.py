@@ -86,6 +86,9 @@ EXPORTS = {
     "sfg_get_field": ([C.c_void_p, C.c_int, C.c_int, _fp, C.c_size_t], C.c_int),
     "sfg_get_numbering": ([C.c_void_p, _ip, _ip, _ip], C.c_int),
     "sfg_check_finite": ([C.c_void_p], C.c_int),
+    "sfg_set_model2d": ([C.c_void_p, _fp, _fp, _fp], C.c_int),
+    "sfg_forward_checkpointed": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "sfg_adjoint_gradient": ([C.c_void_p, _fp, _fp, _fp, _fp], C.c_int),
     "sfg_step_noalloc": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
 }
 
@@ -287,6 +290,26 @@ class Simulation2D:
         if rc not in (0, -6):
             self._check(rc)
         return rc == 0
+
+    # ---- adjoint -------------------------------------------------------
+    def set_model(self, rho, kappa, mu):
+        """Per-GLL-point model [nspec, 25] (database element order)."""
+        r, k, m = (_arr(x, np.float32) for x in (rho, kappa, mu))
+        self._check(self.lib.sfg_set_model2d(self.h, r.ctypes.data_as(_fp), k.ctypes.data_as(_fp),
+                                             m.ctypes.data_as(_fp)))
+
+    def forward_checkpointed(self, nsteps, interval):
+        self._check(self.lib.sfg_forward_checkpointed(self.h, int(nsteps), int(interval)))
+        return self.seismograms()[0, :nsteps, 0]
+
+    def adjoint_gradient(self, seis_grad):
+        """dL/d(rho, kappa, mu) per GLL point [nspec, 25] given dL/dseis [nsteps, nrec, 2]."""
+        i = self.info()
+        g = _arr(seis_grad, np.float32)
+        out = [np.zeros((i.nspec, 25), np.float32) for _ in range(3)]
+        self._check(self.lib.sfg_adjoint_gradient(self.h, g.ctypes.data_as(_fp),
+                                                  *[o.ctypes.data_as(_fp) for o in out]))
+        return tuple(out)
 
     def close(self):
         if getattr(self, "h", None):
