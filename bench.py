@@ -176,6 +176,83 @@ def bench_batched(args, world, barrier, max_over_ranks):
             "timing": "CUDA events, graph-replayed steps, inputs larger than L2"}
 
 
+def bench_adjoint(args, world, barrier, max_over_ranks):
+    """Config 4: cost of an L2-misfit gradient (checkpointed forward + reverse
+    sweep) against a plain forward run of the same source, on the 500x250
+    elastic model (wall clock around synchronous calls, after one untimed
+    gradient that allocates the checkpoints and captures the recording
+    graphs).  With --adjoint-fd K, also the fourth-order central-difference
+    check of the all-source gradient along K seeded smooth perturbations."""
+    from specfempp_b200 import adjoint, meshgen, sfg
+    nx, nz = (int(v) for v in args.adjoint_mesh.split("x"))
+    nstep = args.adjoint_steps
+    aw = meshgen.elastic_adjoint_500x250(nstep=nstep, nx=nx, nz=nz)
+    w = aw.workload
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=nstep, point_rho=w.point_rho, point_vp=w.point_vp,
+                           point_vs=w.point_vs)
+    sim.set_sources([w.sources[0]])
+    sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
+    sim.initialize()
+    inf = sim.info()
+    f64 = lambda a: a.astype(np.float64)  # noqa: E731
+    kt, mt = adjoint.moduli(f64(aw.true_rho), f64(aw.true_vp), f64(aw.true_vs))
+    rho0 = f64(w.point_rho)
+    k0, m0 = adjoint.moduli(rho0, f64(w.point_vp), f64(w.point_vs))
+    nsrc = len(w.sources) if args.adjoint_fd > 0 else 1
+    obs = adjoint.observed_data(sim, w.sources[:nsrc], aw.true_rho, kt, mt, nstep)
+
+    def forward_s():
+        sim.reset()
+        barrier()
+        t0 = time.perf_counter()
+        sim.run(nstep)
+        sim.synchronize()
+        return time.perf_counter() - t0
+
+    def gradient_s():
+        barrier()
+        t0 = time.perf_counter()
+        res = sim.forward_checkpointed(nstep, aw.interval) - obs[0]
+        sim.adjoint_gradient(res)
+        return time.perf_counter() - t0
+
+    sim.set_model(rho0, k0, m0)
+    sim.set_sources([w.sources[0]])
+    forward_s()
+    gradient_s()
+    t_fwd = max_over_ranks(min(forward_s() for _ in range(3)))
+    t_grad = max_over_ranks(min(gradient_s() for _ in range(2)))
+    out = {"workload": f"elastic_adjoint_{nx}x{nz}", "nglob": inf.nglob, "steps": nstep,
+           "checkpoint_interval": aw.interval, "forward_s": t_fwd, "gradient_s": t_grad,
+           "cost_ratio": t_grad / t_fwd,
+           "gradient_gll_pt_steps_per_s": inf.nglob * nstep / t_grad,
+           "timing": "wall clock around synchronous calls, one source; gradient = checkpointed "
+                     "forward + segment recompute + reverse sweep"}
+    if args.adjoint_fd > 0:
+        L, grads = adjoint.l2_misfit_gradient(sim, w.sources, rho0, k0, m0, obs, nstep, aw.interval)
+        xmax, zmax = 25.0 * nx, 25.0 * nz
+        pert = meshgen.smooth_perturbations(w.mesh, xmax, zmax, args.adjoint_fd, 1000.0, seed=7)
+        model = [rho0, k0, m0]
+        rows = []
+        h = 0.02
+        for i in range(args.adjoint_fd):
+            which = i % 3
+            d = pert[i] * model[which]
+
+            def f(hh):
+                m = [x.copy() for x in model]
+                m[which] = m[which] + hh * d
+                return adjoint.l2_misfit(sim, w.sources, *m, obs, nstep)
+            fd = (8.0 * (f(h) - f(-h)) - (f(2 * h) - f(-2 * h))) / (12.0 * h)
+            ad = float((grads[which] * d).sum())
+            rows.append({"parameter": ["rho", "kappa", "mu"][which], "adjoint": ad, "fd4": fd,
+                         "rel_err": abs(ad - fd) / abs(fd)})
+        out["fd"] = {"misfit": L, "sources": len(w.sources), "step": h, "stencil": "4th-order central",
+                     "perturbations": rows, "max_rel_err": max(r["rel_err"] for r in rows)}
+    del sim
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -212,6 +289,11 @@ def main():
                     help="elements of the batched-shot model, NXxNZ (config 3: 1000x500)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-steps", type=int, default=30)
+    ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--adjoint-mesh", default="500x250")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-fd", type=int, default=0,
+                    help="finite-difference check along this many perturbations (all 8 sources)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -322,6 +404,10 @@ def main():
     if not args.no_batched:
         batched = bench_batched(args, world, barrier, max_over_ranks)
 
+    adj = None
+    if not args.no_adjoint:
+        adj = bench_adjoint(args, world, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -351,6 +437,7 @@ def main():
         "clocks": clk,
         "gpu_launches": inf.kernels_per_step * args.steps,
         "batched": batched,
+        "adjoint": adj,
     }
     print(json.dumps(line), flush=True)
 

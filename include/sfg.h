@@ -120,6 +120,8 @@ void sfg_destroy(sfg_handle *h);
 const char *sfg_last_error(const sfg_handle *h);   /* NULL handle: last create error */
 
 /* ---- sources / receivers (before sfg_initialize) ---- */
+/* After sfg_initialize, sources may be replaced by as many new ones (next
+ * shot of a sequential survey, e.g. one source per adjoint gradient). */
 int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src);
 /* Optional external source-time table [nstep][nsrc] (overrides the analytic STFs). */
 int sfg_set_stf_table(sfg_handle *h, const float *table, int nstep, int nsrc);

@@ -53,3 +53,63 @@ def seismograms(sim: Simulation2D, rho, kappa, mu, nsteps: int, interval: int = 
     plus 2 states per step of one interval.
     """
     return SeismogramFunction.apply(rho, kappa, mu, sim, int(nsteps), int(interval))
+
+
+def moduli(rho, vp, vs):
+    """(kappa, mu) of the reference's elastic isotropic material:
+    mu = rho vs^2, kappa = rho (vp^2 - 4/3 vs^2)
+    (include/medium/dim2/elastic/isotropic/material.hpp:66-69)."""
+    mu = rho * vs * vs
+    return rho * vp * vp - 4.0 / 3.0 * mu, mu
+
+
+def l2_misfit_gradient(sim: Simulation2D, sources, rho, kappa, mu, observed, nsteps: int,
+                       interval: int):
+    """Waveform misfit L = sum over sources of 1/2 ||d_s - d_obs,s||^2 and its
+    gradient (dL/drho, dL/dkappa, dL/dmu) per GLL point [nspec, 25].
+
+    ``observed``: [nsrc, nsteps, nrec, 2].  Each source runs as the handle's
+    single source in turn (forward with checkpoints, then the adjoint with the
+    residual as adjoint source), and the gradients are summed, as the
+    reference's adjoint workflow sums event kernels.
+    """
+    sim.set_model(rho, kappa, mu)
+    total = 0.0
+    grads = [np.zeros(np.shape(rho), np.float64) for _ in range(3)]
+    for s, src in enumerate(sources):
+        sim.set_sources([src])
+        syn = sim.forward_checkpointed(nsteps, interval).astype(np.float64)
+        res = syn - np.asarray(observed[s], np.float64)
+        total += 0.5 * float((res * res).sum())
+        g = sim.adjoint_gradient(res.astype(np.float32))
+        for a, b in zip(grads, g):
+            a += b
+    return total, tuple(grads)
+
+
+def l2_misfit(sim: Simulation2D, sources, rho, kappa, mu, observed, nsteps: int) -> float:
+    """The misfit of ``l2_misfit_gradient`` without the gradient (forward runs only)."""
+    sim.set_model(rho, kappa, mu)
+    total = 0.0
+    for s, src in enumerate(sources):
+        sim.set_sources([src])
+        syn = _forward(sim, nsteps).astype(np.float64)
+        res = syn - np.asarray(observed[s], np.float64)
+        total += 0.5 * float((res * res).sum())
+    return total
+
+
+def observed_data(sim: Simulation2D, sources, rho, kappa, mu, nsteps: int) -> np.ndarray:
+    """Displacement seismograms [nsrc, nsteps, nrec, 2] of a model (the 'true' data)."""
+    sim.set_model(rho, kappa, mu)
+    out = []
+    for src in sources:
+        sim.set_sources([src])
+        out.append(_forward(sim, nsteps))
+    return np.stack(out)
+
+
+def _forward(sim: Simulation2D, nsteps: int) -> np.ndarray:
+    sim.reset()
+    sim.run(nsteps)
+    return sim.seismograms()[0, :nsteps, 0].copy()

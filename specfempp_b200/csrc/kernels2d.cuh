@@ -466,6 +466,20 @@ __global__ void __launch_bounds__(NP * E) k_stiffness_persistent(StiffArgs S) {
   }
 }
 
+// Recording of a recomputed forward segment (adjoint runs): the update of
+// step k writes the step's displacement u~ and new acceleration a' to slot
+// k - k0 of the segment buffers.
+struct SegRecord {
+  float *u, *a;
+  size_t stride;  // floats per slot (a multiple of 4)
+  int k0;
+  // predicted velocity v~ of the step at the nst Stacey points st_pt
+  float *vst;
+  size_t vstride;
+  const int *st_pt;
+  int nst;
+};
+
 struct UpdateArgs {
   float *__restrict__ u, *__restrict__ v, *__restrict__ accum;
   const float *__restrict__ minv;
@@ -487,6 +501,7 @@ struct UpdateArgs {
   int *flag;                     // set to 1 on a non-finite displacement
   int *step;
   int advance;                   // increment the step counter (last update of a step)
+  const SegRecord *rec;          // optional segment recording (then advance = 0)
 };
 
 __device__ __forceinline__ float coupling_term(const UpdateArgs &A, int pt, int comp) {
@@ -537,8 +552,14 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
     }
     float a[4];
 #pragma unroll
+    for (int c = 0; c < 4; ++c) a[c] = __fmul_rn(pa[c], pm[c]);
+    if (A.rec) {
+      const size_t off = size_t(*A.step - A.rec->k0) * A.rec->stride;
+      reinterpret_cast<float4 *>(A.rec->u + off)[i] = uu;
+      reinterpret_cast<float4 *>(A.rec->a + off)[i] = make_float4(a[0], a[1], a[2], a[3]);
+    }
+#pragma unroll
     for (int c = 0; c < 4; ++c) {
-      a[c] = __fmul_rn(pa[c], pm[c]);
       pv[c] = newmark_correct(pv[c], a[c], A.dt2);
       if (A.predict) newmark_predict(pu[c], pv[c], a[c], A.dt, A.dt2, A.dtsq2);
       bad |= !isfinite(pu[c]);
@@ -554,6 +575,11 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
     const float a = __fmul_rn(acc, A.minv[i]);
     float vv = newmark_correct(A.v[i], a, A.dt2);
     float uu = A.u[i];
+    if (A.rec) {
+      const size_t off = size_t(*A.step - A.rec->k0) * A.rec->stride;
+      A.rec->u[off + i] = uu;
+      A.rec->a[off + i] = a;
+    }
     if (A.predict) newmark_predict(uu, vv, a, A.dt, A.dt2, A.dtsq2);
     A.u[i] = uu;
     A.v[i] = vv;
@@ -604,8 +630,17 @@ __global__ void __launch_bounds__(256) k_update_gather(UpdateArgs A) {
     }
     float a[NC];
 #pragma unroll
+    for (int c = 0; c < NC; ++c) a[c] = __fmul_rn(acc[c], mi[c]);
+    if (A.rec) {
+      const size_t off = size_t(*A.step - A.rec->k0) * A.rec->stride;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        A.rec->u[off + size_t(g) * NC + c] = uu[c];
+        A.rec->a[off + size_t(g) * NC + c] = a[c];
+      }
+    }
+#pragma unroll
     for (int c = 0; c < NC; ++c) {
-      a[c] = __fmul_rn(acc[c], mi[c]);
       vv[c] = newmark_correct(vv[c], a[c], A.dt2);
       if (A.predict) newmark_predict(uu[c], vv[c], a[c], A.dt, A.dt2, A.dtsq2);
       bad |= !isfinite(uu[c]);

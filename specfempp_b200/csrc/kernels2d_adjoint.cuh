@@ -5,19 +5,22 @@
 //   predictor   u~ = u + dt v + dt^2/2 a,   v~ = v + dt/2 a
 //   forces      a' = B (f_k - K u~ - C v~)            (B = M_eff^-1, diagonal)
 //   corrector   v' = v~ + dt/2 a',  u' = u~;  seismogram d_k = R u'
-// Reverse sweep of step k, for adjoint state (lu, lv, la) of (u', v', a')
-// and g_k = dL/dd_k:
-//   mu  = B (la + dt/2 lv)                              k_adj_pre
-//   lu~ = lu + R^T g_k - K mu                           k_adj_elem (-K mu, R^T g_k per element point)
+// Reverse sweep of step k, for adjoint state (lu, lv) of (u', v') with
+// mu_k = B (la + dt/2 lv) already formed and g_k = dL/dd_k:
+//   lv~ = lv - C mu_k                                   k_adj_stacey (start of the step)
+//   lu~ = lu + R^T g_k - K mu_k                         k_adj_elem (-K mu, R^T g_k per element point)
 //                                                       + k_adj_post (per-point sum)
-//   lv~ = lv - C mu                                     k_adj_stacey
-//   (lu, lv, la) <- (lu~, dt lu~ + lv~, dt^2/2 lu~ + dt/2 lv~)
+//   lu <- lu~,  lv <- dt lu~ + lv~,  la = dt^2/2 lu~ + dt/2 lv~,
+//   mu_(k-1) = B (la + dt/2 lv)                         k_adj_post
 // and the model gradient of the step, per element GLL point p with
 // W_p = w_x w_z |J|:
 //   dL/dkappa_p += -W_p (div mu)(div u~)
 //   dL/dmu_p    += -W_p [4/3 (mxx uxx + mzz uzz) - 2/3 (mxx uzz + mzz uxx)
 //                        + (mxz + mzx)(uxz + uzx)]
-//   dL/drho_p   += -W_p mu . a'        (mass part of B)
+//   dL/drho_p   += -W_p G(g_p),  G(g) += mu_k(g) . a'_k(g)   (mass part of B,
+//                                                              summed per global point)
+// plus, on the absorbing edges, the dependence of the Stacey impedances
+// rho vp and rho vs on (rho, kappa, mu) (k_adj_stacey_grad).
 // kappa is the bulk modulus the reference stores (lambda + 2mu = kappa +
 // 4/3 mu, include/medium/dim2/elastic/isotropic/properties.hpp:71-91).  The
 // per-step terms are summed in FP32 over a checkpoint segment and folded into
@@ -37,11 +40,10 @@ struct AdjArgs {
   const int *__restrict__ ibool;
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
-  const float *__restrict__ mu;      // adjoint field B (la + dt/2 lv) [nglob][2]
+  const float *__restrict__ mu;      // adjoint field mu_k [nglob][2]
   const float *__restrict__ uf;      // forward u~ of the step [nglob][2]
-  const float *__restrict__ af;      // forward a' of the step [nglob][2]
   float *__restrict__ r;             // element-point results [nspec*25][2]
-  float *__restrict__ seg_k, *__restrict__ seg_m, *__restrict__ seg_r;  // segment sums [nspec*25]
+  float *__restrict__ seg;           // segment sums [nspec*25][kappa, mu]
   const int *__restrict__ ad_head, *__restrict__ ad_next;  // receivers per element
   const float *__restrict__ ad_h;    // receiver Lagrange weights [nrec][25]
   const float *__restrict__ ad_g;    // dL/d seismogram of this step [nrec][2]
@@ -66,7 +68,6 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
   const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
   const float2 m2 = act ? reinterpret_cast<const float2 *>(A.mu)[g] : make_float2(0.f, 0.f);
   const float2 u2 = act ? reinterpret_cast<const float2 *>(A.uf)[g] : make_float2(0.f, 0.f);
-  const float2 a2 = act ? reinterpret_cast<const float2 *>(A.af)[g] : make_float2(0.f, 0.f);
   const int rh = act ? __ldg(A.ad_head + e) : -1;
   sm_[0][le][q] = m2.x; sm_[1][le][q] = m2.y;
   su_[0][le][q] = u2.x; su_[1][le][q] = u2.y;
@@ -124,24 +125,20 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
   const float tk = -W * (divm * divu);
   const float tm = -W * ((4.f / 3.f) * (mxx * uxx + mzz * uzz) - (2.f / 3.f) * (mxx * uzz + mzz * uxx) +
                          (mxz + mzx) * (uxz + uzx));
-  const float tr = -W * (m2.x * a2.x + m2.y * a2.y);
-  A.seg_k[p] += tk;
-  A.seg_m[p] += tm;
-  A.seg_r[p] += tr;
+  float2 sg = reinterpret_cast<float2 *>(A.seg)[p];
+  sg.x += tk;
+  sg.y += tm;
+  reinterpret_cast<float2 *>(A.seg)[p] = sg;
 }
 
-// mu = B (la + dt/2 lv)
-__global__ void __launch_bounds__(256) k_adj_pre(const float *__restrict__ la, const float *__restrict__ lv,
-                                                 const float *__restrict__ minv, float *__restrict__ mu,
-                                                 int n, float dt2) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    mu[i] = __fmul_rn(minv[i], __fadd_rn(la[i], __fmul_rn(dt2, lv[i])));
-}
-
-// lu~ = lu + sum of the element-point results (colour order); then the
-// transposed predictor.  One thread per point.
+// Per point: lu~ = lu + sum of the element-point results (colour order);
+// G += mu_k . a'_k; then the transposed predictor and mu_(k-1).  lv holds
+// lv~ (Stacey already applied).  One thread per point.
 __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float *__restrict__ lv,
-                                                  float *__restrict__ la, const float *__restrict__ r,
+                                                  float *__restrict__ mu, float *__restrict__ grho,
+                                                  const float *__restrict__ af,
+                                                  const float *__restrict__ minv,
+                                                  const float *__restrict__ r,
                                                   const int *__restrict__ inv_start,
                                                   const int *__restrict__ inv_idx, int npts, float dt,
                                                   float dt2, float dtsq2) {
@@ -154,30 +151,89 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
     }
     const float2 u = reinterpret_cast<const float2 *>(lu)[g];
     const float2 v = reinterpret_cast<const float2 *>(lv)[g];
+    const float2 m = reinterpret_cast<const float2 *>(mu)[g];
+    const float2 a = reinterpret_cast<const float2 *>(af)[g];
+    const float2 mi = reinterpret_cast<const float2 *>(minv)[g];
+    grho[g] += m.x * a.x + m.y * a.y;
     const float lux = u.x + s0, luz = u.y + s1;
+    const float lvx = dt * lux + v.x, lvz = dt * luz + v.y;
+    const float lax = dtsq2 * lux + dt2 * v.x, laz = dtsq2 * luz + dt2 * v.y;
     reinterpret_cast<float2 *>(lu)[g] = make_float2(lux, luz);
-    reinterpret_cast<float2 *>(lv)[g] = make_float2(dt * lux + v.x, dt * luz + v.y);
-    reinterpret_cast<float2 *>(la)[g] = make_float2(dtsq2 * lux + dt2 * v.x, dtsq2 * luz + dt2 * v.y);
+    reinterpret_cast<float2 *>(lv)[g] = make_float2(lvx, lvz);
+    reinterpret_cast<float2 *>(mu)[g] =
+        make_float2(__fmul_rn(mi.x, __fadd_rn(lax, __fmul_rn(dt2, lvx))),
+                    __fmul_rn(mi.y, __fadd_rn(laz, __fmul_rn(dt2, lvz))));
   }
 }
 
-// Stacey part of the transposed step on the absorbing points:
-// lv -= C mu, la -= dt/2 C mu (C symmetric 2x2 per point: xx, xz, zz).
-__global__ void __launch_bounds__(256) k_adj_stacey(float *__restrict__ lv, float *__restrict__ la,
-                                                    const float *__restrict__ mu,
+// Stacey part of the transposed step on the absorbing points, at the start
+// of a reverse step: lv -= C mu (C symmetric 2x2 per point: xx, xz, zz).
+__global__ void __launch_bounds__(256) k_adj_stacey(float *__restrict__ lv, const float *__restrict__ mu,
                                                     const int *__restrict__ pt,
-                                                    const float *__restrict__ cm, int n, float dt2) {
+                                                    const float *__restrict__ cm, int n) {
   for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
     const int g = pt[j];
     const float mx = mu[2 * g], mz = mu[2 * g + 1];
-    const float cx = cm[3 * j] * mx + cm[3 * j + 1] * mz;
-    const float cz = cm[3 * j + 1] * mx + cm[3 * j + 2] * mz;
-    lv[2 * g] -= cx;
-    lv[2 * g + 1] -= cz;
-    la[2 * g] -= dt2 * cx;
-    la[2 * g + 1] -= dt2 * cz;
+    lv[2 * g] -= cm[3 * j] * mx + cm[3 * j + 1] * mz;
+    lv[2 * g + 1] -= cm[3 * j + 1] * mx + cm[3 * j + 2] * mz;
   }
 }
+
+// Recording: the predicted velocity v~ of the step at the Stacey points
+// (launched before the step's element kernels, which read v~).
+__global__ void __launch_bounds__(256) k_record_stacey_v(const SegRecord *__restrict__ rec,
+                                                         const float *__restrict__ v,
+                                                         const int *__restrict__ step) {
+  const int n = rec->nst;
+  float *dst = rec->vst + size_t(*step - rec->k0) * rec->vstride;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+    reinterpret_cast<float2 *>(dst)[j] = reinterpret_cast<const float2 *>(v)[rec->st_pt[j]];
+}
+
+// Model dependence of the Stacey terms, per element-local boundary point i
+// (global point g, Stacey slot j, unnormalised normal n, |n| = j1, edge
+// weight wq).  The traction is -C v~ with C = wq j1 [(rvp - rvs) n n^T / j1^2
+// + rvs I] and the implicit mass term adds dt/2 wq j1 [(nx + nz) n_c (rvp -
+// rvs) / j1^2 + rvs] to M_c, so per step
+//   dL/drvp = -wq j1 (A1 + dt/2 A3),  dL/drvs = -wq j1 (A2 - A1 + dt/2 (A4 - A3))
+// with A1 = (mu.n)(n.v~)/j1^2, A2 = mu.v~, A3 = (nx + nz)/j1^2 sum_c mu_c n_c a'_c,
+// A4 = mu.a'.  The four sums are accumulated per point (acc[4 i + 0..3]).
+__global__ void __launch_bounds__(256) k_adj_stacey_grad(const int *__restrict__ lb_g,
+                                                         const int *__restrict__ lb_j,
+                                                         const float4 *__restrict__ geo,
+                                                         const float *__restrict__ mu,
+                                                         const float *__restrict__ vst,
+                                                         const float *__restrict__ af,
+                                                         float *__restrict__ acc, int n) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int g = lb_g[i];
+    const float4 q = geo[i];
+    const float2 m = reinterpret_cast<const float2 *>(mu)[g];
+    const float2 v = reinterpret_cast<const float2 *>(vst)[lb_j[i]];
+    const float2 a = reinterpret_cast<const float2 *>(af)[g];
+    const float inv = 1.0f / (q.z * q.z);
+    const float mn = m.x * q.x + m.y * q.y, vn = v.x * q.x + v.y * q.y;
+    float4 t = reinterpret_cast<float4 *>(acc)[i];
+    t.x += mn * vn * inv;
+    t.y += m.x * v.x + m.y * v.y;
+    t.z += (q.x + q.y) * inv * (m.x * q.x * a.x + m.y * q.y * a.y);
+    t.w += m.x * a.x + m.y * a.y;
+    reinterpret_cast<float4 *>(acc)[i] = t;
+  }
+}
+
+// Point the recording at one segment buffer and set the step counter to the
+// segment's first step.
+__global__ void k_set_segment(SegRecord *rec, int *step, float *u, float *a, float *vst, int k0) {
+  rec->u = u;
+  rec->a = a;
+  rec->vst = vst;
+  rec->k0 = k0;
+  *step = k0;
+}
+
+// Step counter of a recording segment (the recording update leaves it alone).
+__global__ void k_advance(int *step) { *step += 1; }
 
 // total += segment sum with Kahan compensation; segment sum cleared.
 __global__ void __launch_bounds__(256) k_kahan_fold(float *__restrict__ total, float *__restrict__ comp,

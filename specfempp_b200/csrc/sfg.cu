@@ -10,6 +10,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../../include/sfg.h"
@@ -92,22 +93,41 @@ struct DevMedium {
 // Device state of the adjoint (allocated on first use).
 struct AdjointState {
   int nstep = 0, interval = 0, ncheck = 0;
-  size_t nvals = 0, nloc = 0;
-  float *ckpt = nullptr;                        // [ncheck][u, v, a][nvals]
-  float *seg_u = nullptr, *seg_a = nullptr;     // [interval][nvals]
-  float *lu = nullptr, *lv = nullptr, *la = nullptr, *mu = nullptr;
+  size_t nvals = 0, nloc = 0, stride = 0, nglob = 0;
+  float *ckpt = nullptr;                        // [ncheck][u, v, a][nvals + 4]
+  // two segment buffers, so that the recompute of one segment overlaps the
+  // reverse sweep of the next (streams: the handle's and rstream)
+  float *seg_u = nullptr, *seg_a = nullptr;     // [2][interval][stride]
+  float *seg_v = nullptr;                       // [2][interval][vstride]: v~ at the Stacey points
+  cudaStream_t rstream = nullptr;
+  cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
+  int recorded = -1;                            // segment recorded by the forward run
+  size_t vstride = 0;
+  float *lu = nullptr, *lv = nullptr, *mu = nullptr;
   float *r = nullptr;                           // [nloc][2]
-  float *sum = nullptr, *comp = nullptr, *seg = nullptr;  // [3][nloc]: kappa, mu, rho
+  // gradient sums: [nloc][kappa, mu], [nglob] rho-term per global point,
+  // then (from a 16-byte boundary) [nlb][4] Stacey impedance terms
+  float *sum = nullptr, *comp = nullptr, *seg = nullptr;
+  size_t off_lb = 0;
+  int nlb = 0;                                  // element-local Stacey points
+  int *lb_g = nullptr, *lb_j = nullptr;
+  float *lb_geo = nullptr;                      // [nlb][nx, nz, j1, wq]
+  std::vector<size_t> lb_k;                     // index into the boundary arrays
+  std::vector<size_t> lb_pm;                    // mesh-order element point
   float *gtab = nullptr;                        // [nstep][nrec][2]
   int *ad_head = nullptr, *ad_next = nullptr;
   int *st_pt = nullptr;
   float *st_c = nullptr;
   int nst = 0;
+  sfg::dev::SegRecord *d_rec = nullptr;
+  cudaGraphExec_t graph_r1 = nullptr, graph_re = nullptr;  // recording steps
   bool forward_done = false;
+  size_t nsum() const { return off_lb + 4 * size_t(nlb); }
 };
 
 struct sfg_handle {
   AdjointState adj;
+  bool recording = false;  // update_args: record u~ and a' of each step (adjoint recompute)
   sfg::Mesh2D mesh;
   sfg::Assembly2D asmb;
   sfg_options opt{};
@@ -142,10 +162,18 @@ struct sfg_handle {
 
   ~sfg_handle() {
     for (void *p : {(void *)adj.ckpt, (void *)adj.seg_u, (void *)adj.seg_a, (void *)adj.lu, (void *)adj.lv,
-                    (void *)adj.la, (void *)adj.mu, (void *)adj.r, (void *)adj.sum, (void *)adj.comp,
-                    (void *)adj.seg, (void *)adj.gtab, (void *)adj.ad_head, (void *)adj.ad_next,
-                    (void *)adj.st_pt, (void *)adj.st_c})
+                    (void *)adj.mu, (void *)adj.r, (void *)adj.sum, (void *)adj.comp, (void *)adj.seg,
+                    (void *)adj.gtab, (void *)adj.ad_head, (void *)adj.ad_next, (void *)adj.st_pt,
+                    (void *)adj.st_c, (void *)adj.d_rec, (void *)adj.seg_v, (void *)adj.lb_g,
+                    (void *)adj.lb_j, (void *)adj.lb_geo})
       if (p) cudaFree(p);
+    if (adj.graph_r1) cudaGraphExecDestroy(adj.graph_r1);
+    for (int b = 0; b < 2; ++b) {
+      if (adj.ev_rec[b]) cudaEventDestroy(adj.ev_rec[b]);
+      if (adj.ev_rev[b]) cudaEventDestroy(adj.ev_rev[b]);
+    }
+    if (adj.rstream) cudaStreamDestroy(adj.rstream);
+    if (adj.graph_re) cudaGraphExecDestroy(adj.graph_re);
     if (graph_k) cudaGraphExecDestroy(graph_k);
     if (graph_1) cudaGraphExecDestroy(graph_1);
     if (graph_e) cudaGraphExecDestroy(graph_e);
@@ -377,7 +405,8 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   }
   U.flag = h->d_flag;
   U.step = h->d_step;
-  U.advance = advance ? 1 : 0;
+  U.advance = advance && !h->recording ? 1 : 0;
+  if (h->recording) U.rec = h->adj.d_rec;
   return U;
 }
 
@@ -451,6 +480,8 @@ void launch_predict(sfg_handle *h, cudaStream_t s) {
 // predictor into the updates.
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
+  if (h->recording && h->adj.nst)
+    sfg::dev::k_record_stacey_v<<<grid_for(h->adj.nst), 256, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
   launch_stiffness(h, s);
   if (has_ac) {
     launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
@@ -459,6 +490,7 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   if (has_el) {
     launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
     launch_update(h, SFG_MEDIUM_ELASTIC, predict, true, s);
+    if (h->recording) sfg::dev::k_advance<<<1, 1, 0, s>>>(h->d_step);
   }
 }
 
@@ -724,8 +756,11 @@ const char *sfg_last_error(const sfg_handle *h) {
 
 int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
   return guarded(h, [&]() {
-    if (h->initialized) { h->err = "sources must be set before sfg_initialize"; return int(SFG_ERR_STATE); }
     if (nsrc < 0 || (nsrc > 0 && !src)) { h->err = "bad source array"; return int(SFG_ERR_ARG); }
+    if (h->initialized && nsrc != h->asmb.nsrc) {
+      h->err = "after sfg_initialize the number of sources is fixed";
+      return int(SFG_ERR_STATE);
+    }
     h->sources.clear();
     for (int i = 0; i < nsrc; ++i)
       h->sources.push_back({src[i].x, src[i].z, src[i].shot, src[i].stf, src[i].f0, src[i].factor,
@@ -737,6 +772,22 @@ int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
       return int(SFG_ERR_LOCATE);
     }
     h->have_sources = true;
+    if (h->initialized) {
+      // same source count: the device tables keep their sizes (and the step
+      // graphs their pointers); refill them in place
+      const sfg::Assembly2D &a = h->asmb;
+      auto put = [&](auto *d, const auto &v) {
+        if (d && !v.empty()) SFG_CUDA(cudaMemcpy(d, v.data(), v.size() * sizeof(v[0]), cudaMemcpyHostToDevice));
+      };
+      SFG_CUDA(cudaStreamSynchronize(h->stream));
+      if (h->el.nspec) put(h->el.src_head, a.el_src_head);
+      if (h->ac.nspec) put(h->ac.src_head, a.ac_src_head);
+      put(h->d_src_next, a.src_next);
+      put(h->d_src_shot, a.src_shot);
+      put(h->d_src_arr, a.src_arr);
+      put(h->d_stf, a.stf);
+      h->adj.forward_done = false;
+    }
     return int(SFG_OK);
   });
 }
@@ -1190,20 +1241,60 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   AdjointState &A = h->adj;
   const size_t nvals = h->el.values();
   const size_t nloc = size_t(h->el.nspec) * sfg::NPTS;
+  const size_t stride = ((nvals + 3) / 4) * 4 + 4;
   const int ncheck = (nstep + interval - 1) / interval;
-  const bool resize = A.nvals != nvals || A.interval != interval || A.ncheck < ncheck;
-  if (resize) {
-    for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a})
+  const int nst = int(h->asmb.el.stacey_pt.size());
+  const size_t vstride = ((2 * size_t(nst) + 3) / 4) * 4 + 4;
+  if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck) {
+    for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a, &A.seg_v})
       if (*p) { cudaFree(*p); *p = nullptr; }
     A.ckpt = dalloc<float>(size_t(ncheck) * 3 * (nvals + 4));
-    A.seg_u = dalloc<float>(size_t(interval) * (nvals + 4));
-    A.seg_a = dalloc<float>(size_t(interval) * (nvals + 4));
+    A.seg_u = dalloc<float>(2 * size_t(interval) * stride);
+    A.seg_a = dalloc<float>(2 * size_t(interval) * stride);
+    A.seg_v = dalloc<float>(2 * size_t(interval) * vstride);
+    A.recorded = -1;
   }
+  A.vstride = vstride;
+  A.nvals = nvals;
+  A.nloc = nloc;
+  A.nglob = size_t(h->el.nglob);
+  A.stride = stride;
+  A.interval = interval;
+  A.ncheck = ncheck;
+  A.nstep = nstep;
   if (!A.lu) {
-    A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4);
-    A.la = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
+    A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
     A.r = dalloc<float>(2 * nloc);
-    A.sum = dalloc<float>(3 * nloc); A.comp = dalloc<float>(3 * nloc); A.seg = dalloc<float>(3 * nloc);
+    // element-local Stacey points: global point, Stacey slot, geometry
+    const sfg::MediumData &M = h->asmb.el;
+    std::unordered_map<int, int> slot;
+    for (size_t j = 0; j < M.stacey_pt.size(); ++j) slot[M.stacey_pt[j]] = int(j);
+    std::vector<int> lg, lj;
+    std::vector<float> geo;
+    A.lb_k.clear();
+    A.lb_pm.clear();
+    for (int ce = 0; ce < M.nspec; ++ce) {
+      if (M.bc_slot[ce] < 0) continue;
+      for (int q = 0; q < sfg::NPTS; ++q) {
+        const size_t k = size_t(M.bc_slot[ce]) * sfg::NPTS + q;
+        if (M.bc_w[k] == 0.0f) continue;
+        const int g = M.ibool[size_t(ce) * sfg::NPTS + q];
+        lg.push_back(g);
+        lj.push_back(slot.at(g));
+        geo.insert(geo.end(), {M.bc_nx[k], M.bc_nz[k], M.bc_j1[k], M.bc_w[k]});
+        A.lb_k.push_back(k);
+        A.lb_pm.push_back(size_t(M.elem_mesh[ce]) * sfg::NPTS + q);
+      }
+    }
+    A.nlb = int(lg.size());
+    A.off_lb = ((2 * nloc + A.nglob + 3) / 4) * 4;
+    A.lb_g = dalloc<int>(lg.size()); A.lb_j = dalloc<int>(lj.size()); A.lb_geo = dalloc<float>(geo.size());
+    if (A.nlb) {
+      SFG_CUDA(cudaMemcpy(A.lb_g, lg.data(), lg.size() * sizeof(int), cudaMemcpyHostToDevice));
+      SFG_CUDA(cudaMemcpy(A.lb_j, lj.data(), lj.size() * sizeof(int), cudaMemcpyHostToDevice));
+      SFG_CUDA(cudaMemcpy(A.lb_geo, geo.data(), geo.size() * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    A.sum = dalloc<float>(A.nsum()); A.comp = dalloc<float>(A.nsum()); A.seg = dalloc<float>(A.nsum());
     // receivers as adjoint sources: chain per elastic compute element
     const sfg::Assembly2D &as = h->asmb;
     std::vector<int> head(h->el.nspec, -1), next(std::max(as.nrec, 1), -1);
@@ -1224,12 +1315,23 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
       SFG_CUDA(cudaMemcpy(A.st_pt, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice));
       SFG_CUDA(cudaMemcpy(A.st_c, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
+    A.d_rec = dalloc<sfg::dev::SegRecord>(1);
+    SFG_CUDA(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
+    for (int b = 0; b < 2; ++b) {
+      SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rec[b], cudaEventDisableTiming));
+      SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rev[b], cudaEventDisableTiming));
+    }
   }
-  A.nvals = nvals;
-  A.nloc = nloc;
-  A.interval = interval;
-  A.ncheck = ncheck;
-  A.nstep = nstep;
+  sfg::dev::SegRecord rec{A.seg_u, A.seg_a, stride, 0, A.seg_v, vstride, A.st_pt, A.nst};
+  SFG_CUDA(cudaMemcpy(A.d_rec, &rec, sizeof(rec), cudaMemcpyHostToDevice));
+  if (!A.graph_r1) {
+    // one recording step with the next predictor fused, and one ending on
+    // the corrector (the segment's last step)
+    h->recording = true;
+    A.graph_r1 = capture(h, 1, true);
+    A.graph_re = capture(h, 1, false);
+    h->recording = false;
+  }
 }
 
 void save_state(sfg_handle *h, float *dst) {
@@ -1239,15 +1341,28 @@ void save_state(sfg_handle *h, float *dst) {
   SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, h->el.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
 }
 
-void restore_state(sfg_handle *h, const float *src, int step) {
+// Recompute (or, in the forward run, compute) segment c from the state in
+// the fields, recording u~, a' and the Stacey v~ of each step into segment
+// buffer c % 2.  Stream-ordered on the handle's stream.
+void record_segment(sfg_handle *h, int c) {
+  AdjointState &A = h->adj;
+  const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
+  const size_t ob = size_t(b) * A.interval;
+  sfg::dev::k_set_segment<<<1, 1, 0, h->stream>>>(A.d_rec, h->d_step, A.seg_u + ob * A.stride,
+                                                  A.seg_a + ob * A.stride, A.seg_v + ob * A.vstride, k0);
+  resume(h);
+  for (int k = k0; k + 1 < k1; ++k) SFG_CUDA(cudaGraphLaunch(A.graph_r1, h->stream));
+  SFG_CUDA(cudaGraphLaunch(A.graph_re, h->stream));
+  h->state_final = true;
+  h->host_step = k1;
+}
+
+void restore_state(sfg_handle *h, const float *src) {
   const size_t n = h->el.values() + 4;
   SFG_CUDA(cudaMemcpyAsync(h->el.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
   SFG_CUDA(cudaMemcpyAsync(h->el.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
   SFG_CUDA(cudaMemcpyAsync(h->el.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(h->d_step, &step, sizeof(int), cudaMemcpyHostToDevice, h->stream));
-  SFG_CUDA(cudaStreamSynchronize(h->stream));
   h->state_final = true;
-  h->host_step = step;
 }
 
 }  // namespace
@@ -1269,9 +1384,13 @@ int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval) {
     const size_t stride = 3 * (A.nvals + 4);
     for (int c = 0; c < A.ncheck; ++c) {
       save_state(h, A.ckpt + size_t(c) * stride);
-      run_steps(h, std::min(A.interval, nsteps - c * A.interval));
+      // the last segment is recorded on the way, so the reverse sweep starts
+      // without recomputing it
+      if (c + 1 == A.ncheck) record_segment(h, c);
+      else run_steps(h, std::min(A.interval, nsteps - c * A.interval));
     }
     SFG_CUDA(cudaStreamSynchronize(h->stream));
+    A.recorded = A.ncheck - 1;
     A.forward_done = true;
     return int(SFG_OK);
   });
@@ -1304,64 +1423,98 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       SFG_CUDA(cudaMemcpy(A.gtab, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     const size_t nv = A.nvals;
-    for (float *p : {A.lu, A.lv, A.la, A.mu})
+    for (float *p : {A.lu, A.lv, A.mu})
       SFG_CUDA(cudaMemsetAsync(p, 0, (nv + 4) * sizeof(float), s));
     for (float *p : {A.sum, A.comp, A.seg})
-      SFG_CUDA(cudaMemsetAsync(p, 0, 3 * A.nloc * sizeof(float), s));
+      SFG_CUDA(cudaMemsetAsync(p, 0, A.nsum() * sizeof(float), s));
     const float dt = float(as.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
     sfg::dev::AdjArgs J{};
     const DevMedium &D = h->el;
     J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
     J.prop0 = D.prop0; J.prop1 = D.prop1;
-    J.mu = A.mu; J.r = A.r;
-    J.seg_k = A.seg; J.seg_m = A.seg + A.nloc; J.seg_r = A.seg + 2 * A.nloc;
+    J.mu = A.mu; J.r = A.r; J.seg = A.seg;
     J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
     J.nspec = D.nspec;
     J.quad = h->quad;
     constexpr int E = 8;
     const int eblocks = (D.nspec + E - 1) / E;
     const int npts = D.nglob;
-    const size_t stride = 3 * (nv + 4);
+    const size_t cstride = 3 * (nv + 4);
+    cudaStream_t rs = A.rstream;
+    // the reverse stream starts after the set-up above
+    SFG_CUDA(cudaEventRecord(A.ev_rec[0], s));
+    SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[0], 0));
     for (int c = A.ncheck - 1; c >= 0; --c) {
-      const int k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
-      // recompute the segment's forward states from its checkpoint
-      restore_state(h, A.ckpt + size_t(c) * stride, k0);
-      for (int k = k0; k < k1; ++k) {
-        resume(h);
-        SFG_CUDA(cudaGraphLaunch(h->graph_e, s));
-        h->state_final = true;
-        SFG_CUDA(cudaMemcpyAsync(A.seg_u + size_t(k - k0) * (nv + 4), D.u, nv * sizeof(float),
-                                 cudaMemcpyDeviceToDevice, s));
-        SFG_CUDA(cudaMemcpyAsync(A.seg_a + size_t(k - k0) * (nv + 4), D.a, nv * sizeof(float),
-                                 cudaMemcpyDeviceToDevice, s));
+      const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
+      const size_t ob = size_t(b) * A.interval;
+      if (!(c == A.ncheck - 1 && A.recorded == c)) {
+        // buffer b is free once the reverse sweep of segment c + 2 is done
+        SFG_CUDA(cudaStreamWaitEvent(s, A.ev_rev[b], 0));
+        restore_state(h, A.ckpt + size_t(c) * cstride);
+        record_segment(h, c);
       }
+      SFG_CUDA(cudaEventRecord(A.ev_rec[b], s));
+      SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[b], 0));
       // reverse sweep over the segment
       for (int k = k1 - 1; k >= k0; --k) {
-        sfg::dev::k_adj_pre<<<grid_for(int(nv)), 256, 0, s>>>(A.la, A.lv, D.minv, A.mu, int(nv), dt2);
-        J.uf = A.seg_u + size_t(k - k0) * (nv + 4);
-        J.af = A.seg_a + size_t(k - k0) * (nv + 4);
+        const size_t sl = ob + size_t(k - k0);
+        if (A.nst && k + 1 < A.nstep) {
+          sfg::dev::k_adj_stacey_grad<<<grid_for(A.nlb), 256, 0, rs>>>(
+              A.lb_g, A.lb_j, reinterpret_cast<const float4 *>(A.lb_geo), A.mu, A.seg_v + sl * A.vstride,
+              A.seg_a + sl * A.stride, A.seg + A.off_lb, A.nlb);
+          sfg::dev::k_adj_stacey<<<grid_for(A.nst), 256, 0, rs>>>(A.lv, A.mu, A.st_pt, A.st_c, A.nst);
+        }
+        J.uf = A.seg_u + sl * A.stride;
         J.ad_g = A.gtab + size_t(k) * nrec * 2;
-        sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, s>>>(J);
-        sfg::dev::k_adj_post<<<grid_for(npts), 256, 0, s>>>(A.lu, A.lv, A.la, A.r, D.inv_start, D.inv_idx,
-                                                            npts, dt, dt2, dtsq2);
-        if (A.nst)
-          sfg::dev::k_adj_stacey<<<grid_for(A.nst), 256, 0, s>>>(A.lv, A.la, A.mu, A.st_pt, A.st_c, A.nst, dt2);
+        sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+        sfg::dev::k_adj_post<<<grid_for(npts), 256, 0, rs>>>(
+            A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+            D.inv_idx, npts, dt, dt2, dtsq2);
       }
-      sfg::dev::k_kahan_fold<<<grid_for(int(3 * A.nloc)), 256, 0, s>>>(A.sum, A.comp, A.seg, int(3 * A.nloc));
+      sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
+      SFG_CUDA(cudaEventRecord(A.ev_rev[b], rs));
       SFG_CUDA(cudaGetLastError());
     }
+    A.recorded = -1;
+    SFG_CUDA(cudaStreamSynchronize(rs));
     SFG_CUDA(cudaStreamSynchronize(s));
-    // compute order -> mesh order
-    std::vector<float> tot(3 * A.nloc);
+    h->host_step = A.nstep;
+    // compute order -> mesh order; rho: -W_p G(g_p)
+    std::vector<float> tot(A.nsum());
     SFG_CUDA(cudaMemcpy(tot.data(), A.sum, tot.size() * sizeof(float), cudaMemcpyDeviceToHost));
-    float *outs[3] = {grad_kappa, grad_mu, grad_rho};
-    for (int t = 0; t < 3; ++t) {
-      if (!outs[t]) continue;
-      for (int ce = 0; ce < D.nspec; ++ce) {
-        const int e = as.el.elem_mesh[ce];
-        for (int q = 0; q < sfg::NPTS; ++q)
-          outs[t][size_t(e) * sfg::NPTS + q] = tot[size_t(t) * A.nloc + size_t(ce) * sfg::NPTS + q];
+    const float *grho = tot.data() + 2 * A.nloc;
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = as.el.elem_mesh[ce];
+      for (int q = 0; q < sfg::NPTS; ++q) {
+        const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(e) * sfg::NPTS + q;
+        if (grad_kappa) grad_kappa[pm] = tot[2 * pc];
+        if (grad_mu) grad_mu[pm] = tot[2 * pc + 1];
+        if (grad_rho) {
+          const double W = as.wgll_d[q % sfg::NGLL] * as.wgll_d[q / sfg::NGLL] * as.jac_d[pm];
+          grad_rho[pm] = float(-W * double(grho[as.el.ibool[pc]]));
+        }
       }
+    }
+    // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu)
+    const float *lbs = tot.data() + A.off_lb;
+    for (int i = 0; i < A.nlb; ++i) {
+      const size_t k = A.lb_k[i];
+      const sfg::MediumData &M = as.el;
+      const double A1 = lbs[4 * i], A2 = lbs[4 * i + 1], A3 = lbs[4 * i + 2], A4 = lbs[4 * i + 3];
+      const double wj = double(M.bc_w[k]) * double(M.bc_j1[k]);
+      const double g_vp = -wj * (A1 + double(dt2) * A3);
+      const double g_vs = -wj * (A2 - A1 + double(dt2) * (A4 - A3));
+      const size_t pm = A.lb_pm[i];
+      const double rho = h->mesh.prho.empty() ? h->mesh.mat_rho[h->mesh.kmato[pm / sfg::NPTS]] : h->mesh.prho[pm];
+      const double rvp = M.bc_imp0[k], rvs = M.bc_imp1[k];
+      double dr = g_vp * rvp / (2 * rho), dk = g_vp * rho / (2 * rvp), dm = g_vp * (2.0 / 3.0) * rho / rvp;
+      if (rvs > 0) {
+        dr += g_vs * rvs / (2 * rho);
+        dm += g_vs * rho / (2 * rvs);
+      }
+      if (grad_rho) grad_rho[pm] += float(dr);
+      if (grad_kappa) grad_kappa[pm] += float(dk);
+      if (grad_mu) grad_mu[pm] += float(dm);
     }
     return int(SFG_OK);
   });

@@ -284,3 +284,61 @@ def elastic_grf_1000x500(nstep: int = 3000, nshots: int = 32, nrec: int = 400,
     return Workload("elastic_grf_1000x500", mesh, srcs, rx, rz, 5e-4, nstep, rho.astype(np.float32),
                     vp.astype(np.float32), vs.astype(np.float32),
                     description=f"2D elastic {nx}x{nz} GRF(10%, 500 m) on vp 3000, {nshots} shots")
+
+
+@dataclass
+class AdjointWorkload:
+    """Waveform-inversion test case: an initial model (the workload's point
+    model) and the true model that made the observed data."""
+    workload: Workload
+    true_rho: np.ndarray
+    true_vp: np.ndarray
+    true_vs: np.ndarray
+    anomaly: tuple  # (x0, z0, radius) of the Gaussian anomaly
+    interval: int   # steps between forward checkpoints
+
+
+def elastic_adjoint_500x250(nstep: int = 4000, nx: int = 500, nz: int = 250, nsrc: int = 8,
+                            nrec: int = 200, seed: int = 0) -> AdjointWorkload:
+    """2D elastic 500x250 quads over 12.5 x 6.25 km (h = 25 m); true model
+    vp 3000, vs 1730, rho 2300 times (1 + 0.05 exp(-r^2/400^2)) around a seeded
+    point, initial model without the anomaly; seeded sources at depth, a
+    receiver line under the free surface; Stacey left/right/bottom."""
+    xmax, zmax = 25.0 * nx, 25.0 * nz
+    mesh = structured_mesh(nx, nz, 0.0, xmax, 0.0, zmax, np.zeros(nz, np.int32),
+                           [(ELASTIC, 2300.0, 3000.0, 1730.0)],
+                           absorbing=("bottom", "right", "left"), free_surface=())
+    rng = np.random.default_rng(seed)
+    x0 = float(rng.uniform(0.35, 0.65) * xmax)
+    z0 = float(rng.uniform(0.40, 0.70) * zmax)
+    radius = 400.0
+    gz, gx = gll_coordinates(mesh)
+    bump = np.exp(-((gx - x0) ** 2 + (gz - z0) ** 2) / radius ** 2)
+    ones = np.ones((mesh.nspec, 25))
+    srcs = [RickerSource(float(rng.uniform(0.05, 0.95) * xmax), float(rng.uniform(0.10, 0.35) * zmax),
+                         8.0, 1e10) for _ in range(nsrc)]
+    rx = np.linspace(0.02 * xmax, 0.98 * xmax, nrec)
+    rz = np.full(nrec, zmax - 50.0)
+    w = Workload(f"elastic_adjoint_{nx}x{nz}", mesh, srcs, rx, rz, 5e-4, nstep,
+                 (2300.0 * ones).astype(np.float32), (3000.0 * ones).astype(np.float32),
+                 (1730.0 * ones).astype(np.float32),
+                 description=f"2D elastic {nx}x{nz} adjoint: +5% Gaussian (r=400 m) at "
+                             f"({x0:.0f}, {z0:.0f}) m, {nsrc} sources, {nrec} receivers")
+    f = 1.0 + 0.05 * bump
+    return AdjointWorkload(w, (2300.0 * f).astype(np.float32), (3000.0 * f).astype(np.float32),
+                           (1730.0 * f).astype(np.float32), (x0, z0, radius), 200)
+
+
+def smooth_perturbations(mesh: Mesh, xmax: float, zmax: float, n: int, margin: float, seed: int):
+    """n seeded smooth perturbations [n, nspec, 25] (sums of 3 Gaussians of
+    radius 300-800 m, centres at least ``margin`` from the sides and bottom)."""
+    rng = np.random.default_rng(seed)
+    gz, gx = gll_coordinates(mesh)
+    out = np.zeros((n, mesh.nspec, 25))
+    for i in range(n):
+        for _ in range(3):
+            x0 = rng.uniform(margin, xmax - margin)
+            z0 = rng.uniform(margin, zmax - 0.1 * zmax)
+            r = rng.uniform(300.0, 800.0)
+            out[i] += rng.choice([-1.0, 1.0]) * np.exp(-((gx - x0) ** 2 + (gz - z0) ** 2) / r ** 2)
+    return out
