@@ -478,6 +478,7 @@ struct SegRecord {
   size_t vstride;
   const int *st_pt;
   int nst;
+  int i;          // next step of the segment (k0 + i)
 };
 
 struct UpdateArgs {

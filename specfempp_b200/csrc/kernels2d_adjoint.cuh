@@ -20,7 +20,7 @@
 //   dL/drho_p   += -W_p G(g_p),  G(g) += mu_k(g) . a'_k(g)   (mass part of B,
 //                                                              summed per global point)
 // plus, on the absorbing edges, the dependence of the Stacey impedances
-// rho vp and rho vs on (rho, kappa, mu) (k_adj_stacey_grad).
+// rho vp and rho vs on (rho, kappa, mu) (adj_stacey_grad).
 // kappa is the bulk modulus the reference stores (lambda + 2mu = kappa +
 // 4/3 mu, include/medium/dim2/elastic/isotropic/properties.hpp:71-91).  The
 // per-step terms are summed in FP32 over a checkpoint segment and folded into
@@ -46,7 +46,10 @@ struct AdjArgs {
   float *__restrict__ seg;           // segment sums [nspec*25][kappa, mu]
   const int *__restrict__ ad_head, *__restrict__ ad_next;  // receivers per element
   const float *__restrict__ ad_h;    // receiver Lagrange weights [nrec][25]
-  const float *__restrict__ ad_g;    // dL/d seismogram of this step [nrec][2]
+  const float *__restrict__ gtab;    // dL/d seismogram [nstep][nrec][2]
+  const int *__restrict__ seg_k0;    // first step of the segment (device)
+  int slot;                          // step of the segment: k = *seg_k0 + slot
+  int nrec;
   int nspec;
   Quad quad;
 };
@@ -113,10 +116,13 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
     r[c] = -(sw[iz] * t1 + sw[ix] * t2);
   }
   // receivers of this element inject R^T g (the adjoint sources)
-  for (int k = rh; k >= 0; k = A.ad_next[k]) {
-    const float h = A.ad_h[size_t(k) * NP + q];
-    r[0] += A.ad_g[2 * k] * h;
-    r[1] += A.ad_g[2 * k + 1] * h;
+  if (rh >= 0) {
+    const float *g_k = A.gtab + size_t(*A.seg_k0 + A.slot) * A.nrec * 2;
+    for (int k = rh; k >= 0; k = A.ad_next[k]) {
+      const float h = A.ad_h[size_t(k) * NP + q];
+      r[0] += g_k[2 * k] * h;
+      r[1] += g_k[2 * k + 1] * h;
+    }
   }
   reinterpret_cast<float2 *>(A.r)[p] = make_float2(r[0], r[1]);
   // gradient terms of this step, summed over the segment
@@ -166,28 +172,20 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
   }
 }
 
-// Stacey part of the transposed step on the absorbing points, at the start
-// of a reverse step: lv -= C mu (C symmetric 2x2 per point: xx, xz, zz).
-__global__ void __launch_bounds__(256) k_adj_stacey(float *__restrict__ lv, const float *__restrict__ mu,
-                                                    const int *__restrict__ pt,
-                                                    const float *__restrict__ cm, int n) {
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
-    const int g = pt[j];
-    const float mx = mu[2 * g], mz = mu[2 * g + 1];
-    lv[2 * g] -= cm[3 * j] * mx + cm[3 * j + 1] * mz;
-    lv[2 * g + 1] -= cm[3 * j + 1] * mx + cm[3 * j + 2] * mz;
-  }
-}
-
-// Recording: the predicted velocity v~ of the step at the Stacey points
-// (launched before the step's element kernels, which read v~).
-__global__ void __launch_bounds__(256) k_record_stacey_v(const SegRecord *__restrict__ rec,
-                                                         const float *__restrict__ v,
-                                                         const int *__restrict__ step) {
-  const int n = rec->nst;
-  float *dst = rec->vst + size_t(*step - rec->k0) * rec->vstride;
-  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x)
+// Start of a recording step (one block): store the predicted velocity v~ of
+// the step at the Stacey points (the step's element kernels read v~ next),
+// then set the step counter to the segment's next step.
+__global__ void __launch_bounds__(512) k_record_begin(SegRecord *__restrict__ rec,
+                                                      const float *__restrict__ v, int *step) {
+  const int i = rec->i, n = rec->nst;
+  float *dst = rec->vst + size_t(i) * rec->vstride;
+  for (int j = threadIdx.x; j < n; j += blockDim.x)
     reinterpret_cast<float2 *>(dst)[j] = reinterpret_cast<const float2 *>(v)[rec->st_pt[j]];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    *step = rec->k0 + i;
+    rec->i = i + 1;
+  }
 }
 
 // Model dependence of the Stacey terms, per element-local boundary point i
@@ -198,14 +196,11 @@ __global__ void __launch_bounds__(256) k_record_stacey_v(const SegRecord *__rest
 //   dL/drvp = -wq j1 (A1 + dt/2 A3),  dL/drvs = -wq j1 (A2 - A1 + dt/2 (A4 - A3))
 // with A1 = (mu.n)(n.v~)/j1^2, A2 = mu.v~, A3 = (nx + nz)/j1^2 sum_c mu_c n_c a'_c,
 // A4 = mu.a'.  The four sums are accumulated per point (acc[4 i + 0..3]).
-__global__ void __launch_bounds__(256) k_adj_stacey_grad(const int *__restrict__ lb_g,
-                                                         const int *__restrict__ lb_j,
-                                                         const float4 *__restrict__ geo,
-                                                         const float *__restrict__ mu,
-                                                         const float *__restrict__ vst,
-                                                         const float *__restrict__ af,
-                                                         float *__restrict__ acc, int n) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+__device__ __forceinline__ void adj_stacey_grad(const int *__restrict__ lb_g, const int *__restrict__ lb_j,
+                                                const float4 *__restrict__ geo, const float *__restrict__ mu,
+                                                const float *__restrict__ vst, const float *__restrict__ af,
+                                                float *__restrict__ acc, int n, int first, int stride) {
+  for (int i = first; i < n; i += stride) {
     const int g = lb_g[i];
     const float4 q = geo[i];
     const float2 m = reinterpret_cast<const float2 *>(mu)[g];
@@ -222,6 +217,38 @@ __global__ void __launch_bounds__(256) k_adj_stacey_grad(const int *__restrict__
   }
 }
 
+// Stacey part of the transposed step at the start of a reverse step, one
+// launch: blocks [0, nb_grad) accumulate the impedance terms per
+// element-local boundary point, the others apply lv -= C mu per Stacey point
+// (C symmetric 2x2 per point: xx, xz, zz).
+struct AdjStaceyArgs {
+  const int *lb_g, *lb_j;
+  const float4 *geo;
+  const float *mu, *vst, *af;
+  float *acc;
+  int nlb;
+  float *lv;
+  const int *pt;
+  const float *cm;
+  int nst;
+  int nb_grad;
+};
+
+__global__ void __launch_bounds__(256) k_adj_stacey(AdjStaceyArgs S) {
+  if (int(blockIdx.x) < S.nb_grad) {
+    adj_stacey_grad(S.lb_g, S.lb_j, S.geo, S.mu, S.vst, S.af, S.acc, S.nlb,
+                    blockIdx.x * blockDim.x + threadIdx.x, S.nb_grad * blockDim.x);
+    return;
+  }
+  const int stride = (gridDim.x - S.nb_grad) * blockDim.x;
+  for (int j = (blockIdx.x - S.nb_grad) * blockDim.x + threadIdx.x; j < S.nst; j += stride) {
+    const int g = S.pt[j];
+    const float mx = S.mu[2 * g], mz = S.mu[2 * g + 1];
+    S.lv[2 * g] -= S.cm[3 * j] * mx + S.cm[3 * j + 1] * mz;
+    S.lv[2 * g + 1] -= S.cm[3 * j + 1] * mx + S.cm[3 * j + 2] * mz;
+  }
+}
+
 // Point the recording at one segment buffer and set the step counter to the
 // segment's first step.
 __global__ void k_set_segment(SegRecord *rec, int *step, float *u, float *a, float *vst, int k0) {
@@ -229,11 +256,12 @@ __global__ void k_set_segment(SegRecord *rec, int *step, float *u, float *a, flo
   rec->a = a;
   rec->vst = vst;
   rec->k0 = k0;
+  rec->i = 0;
   *step = k0;
 }
 
-// Step counter of a recording segment (the recording update leaves it alone).
-__global__ void k_advance(int *step) { *step += 1; }
+// Step counter after a recorded segment.
+__global__ void k_set_step(int *step, int k) { *step = k; }
 
 // total += segment sum with Kahan compensation; segment sum cleared.
 __global__ void __launch_bounds__(256) k_kahan_fold(float *__restrict__ total, float *__restrict__ comp,

@@ -121,13 +121,18 @@ struct AdjointState {
   int nst = 0;
   sfg::dev::SegRecord *d_rec = nullptr;
   cudaGraphExec_t graph_r1 = nullptr, graph_re = nullptr;  // recording steps
+  cudaGraphExec_t graph_rseg = nullptr;         // interval - 1 recording steps
+  cudaGraphExec_t graph_rev[2] = {nullptr, nullptr};  // reverse sweep of a full segment, per buffer
+  int *d_k0 = nullptr;                          // first step of the segment in reverse
   bool forward_done = false;
   size_t nsum() const { return off_lb + 4 * size_t(nlb); }
 };
 
 struct sfg_handle {
   AdjointState adj;
-  bool recording = false;  // update_args: record u~ and a' of each step (adjoint recompute)
+  // update_args: record u~ and a' of each step (adjoint); 2 = recompute
+  // (seismograms are those of the forward run and are not computed again)
+  int recording = 0;
   sfg::Mesh2D mesh;
   sfg::Assembly2D asmb;
   sfg_options opt{};
@@ -168,6 +173,10 @@ struct sfg_handle {
                     (void *)adj.lb_j, (void *)adj.lb_geo})
       if (p) cudaFree(p);
     if (adj.graph_r1) cudaGraphExecDestroy(adj.graph_r1);
+    if (adj.graph_rseg) cudaGraphExecDestroy(adj.graph_rseg);
+    for (auto &g : adj.graph_rev)
+      if (g) cudaGraphExecDestroy(g);
+    if (adj.d_k0) cudaFree(adj.d_k0);
     for (int b = 0; b < 2; ++b) {
       if (adj.ev_rec[b]) cudaEventDestroy(adj.ev_rec[b]);
       if (adj.ev_rev[b]) cudaEventDestroy(adj.ev_rev[b]);
@@ -480,17 +489,16 @@ void launch_predict(sfg_handle *h, cudaStream_t s) {
 // predictor into the updates.
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
-  if (h->recording && h->adj.nst)
-    sfg::dev::k_record_stacey_v<<<grid_for(h->adj.nst), 256, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+  if (h->recording) sfg::dev::k_record_begin<<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
   launch_stiffness(h, s);
   if (has_ac) {
-    launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
+    if (h->recording != 2) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
     launch_update(h, SFG_MEDIUM_ACOUSTIC, predict, !has_el, s);
   }
   if (has_el) {
-    launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
+    // a recorded (recomputed) step's seismograms are those of the forward run
+    if (h->recording != 2) launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
     launch_update(h, SFG_MEDIUM_ELASTIC, predict, true, s);
-    if (h->recording) sfg::dev::k_advance<<<1, 1, 0, s>>>(h->d_step);
   }
 }
 
@@ -1253,6 +1261,8 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     A.seg_a = dalloc<float>(2 * size_t(interval) * stride);
     A.seg_v = dalloc<float>(2 * size_t(interval) * vstride);
     A.recorded = -1;
+    for (cudaGraphExec_t *g : {&A.graph_rseg, &A.graph_rev[0], &A.graph_rev[1]})
+      if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
   }
   A.vstride = vstride;
   A.nvals = nvals;
@@ -1316,21 +1326,27 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
       SFG_CUDA(cudaMemcpy(A.st_c, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice));
     }
     A.d_rec = dalloc<sfg::dev::SegRecord>(1);
+    A.d_k0 = dalloc<int>(1);
     SFG_CUDA(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
     for (int b = 0; b < 2; ++b) {
       SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rec[b], cudaEventDisableTiming));
       SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rev[b], cudaEventDisableTiming));
     }
   }
-  sfg::dev::SegRecord rec{A.seg_u, A.seg_a, stride, 0, A.seg_v, vstride, A.st_pt, A.nst};
+  sfg::dev::SegRecord rec{A.seg_u, A.seg_a, stride, 0, A.seg_v, vstride, A.st_pt, A.nst, 0};
   SFG_CUDA(cudaMemcpy(A.d_rec, &rec, sizeof(rec), cudaMemcpyHostToDevice));
   if (!A.graph_r1) {
     // one recording step with the next predictor fused, and one ending on
     // the corrector (the segment's last step)
-    h->recording = true;
+    h->recording = 1;
     A.graph_r1 = capture(h, 1, true);
     A.graph_re = capture(h, 1, false);
-    h->recording = false;
+    h->recording = 0;
+  }
+  if (!A.graph_rseg && interval > 1) {
+    h->recording = 2;
+    A.graph_rseg = capture(h, interval - 1, true);
+    h->recording = 0;
   }
 }
 
@@ -1341,20 +1357,73 @@ void save_state(sfg_handle *h, float *dst) {
   SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, h->el.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
 }
 
-// Recompute (or, in the forward run, compute) segment c from the state in
-// the fields, recording u~, a' and the Stacey v~ of each step into segment
-// buffer c % 2.  Stream-ordered on the handle's stream.
-void record_segment(sfg_handle *h, int c) {
+// Recompute (or, in the forward run, compute: `seismograms`) segment c from
+// the state in the fields, recording u~, a' and the Stacey v~ of each step
+// into segment buffer c % 2.  Stream-ordered on the handle's stream.
+void record_segment(sfg_handle *h, int c, bool seismograms) {
   AdjointState &A = h->adj;
   const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
   const size_t ob = size_t(b) * A.interval;
   sfg::dev::k_set_segment<<<1, 1, 0, h->stream>>>(A.d_rec, h->d_step, A.seg_u + ob * A.stride,
                                                   A.seg_a + ob * A.stride, A.seg_v + ob * A.vstride, k0);
   resume(h);
-  for (int k = k0; k + 1 < k1; ++k) SFG_CUDA(cudaGraphLaunch(A.graph_r1, h->stream));
+  if (!seismograms && k1 - k0 == A.interval && A.graph_rseg) {
+    SFG_CUDA(cudaGraphLaunch(A.graph_rseg, h->stream));
+  } else {
+    for (int k = k0; k + 1 < k1; ++k) SFG_CUDA(cudaGraphLaunch(A.graph_r1, h->stream));
+  }
   SFG_CUDA(cudaGraphLaunch(A.graph_re, h->stream));
+  sfg::dev::k_set_step<<<1, 1, 0, h->stream>>>(h->d_step, k1);
   h->state_final = true;
   h->host_step = k1;
+}
+
+// Reverse sweep over one segment of n steps held in buffer b (slots n-1 ..
+// 0), then the Kahan fold of its sums.  `last`: the run's final segment,
+// whose final step has no Stacey term (mu is zero there).
+template <int E>
+void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
+  AdjointState &A = h->adj;
+  const DevMedium &D = h->el;
+  const float dt = float(h->asmb.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
+  sfg::dev::AdjArgs J{};
+  J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
+  J.prop0 = D.prop0; J.prop1 = D.prop1;
+  J.mu = A.mu; J.r = A.r; J.seg = A.seg;
+  J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
+  J.gtab = A.gtab; J.seg_k0 = A.d_k0; J.nrec = h->asmb.nrec;
+  J.nspec = D.nspec;
+  J.quad = h->quad;
+  sfg::dev::AdjStaceyArgs St{};
+  St.lb_g = A.lb_g; St.lb_j = A.lb_j; St.geo = reinterpret_cast<const float4 *>(A.lb_geo);
+  St.mu = A.mu; St.acc = A.seg + A.off_lb; St.nlb = A.nlb;
+  St.lv = A.lv; St.pt = A.st_pt; St.cm = A.st_c; St.nst = A.nst;
+  St.nb_grad = grid_for(A.nlb);
+  const int eblocks = (D.nspec + E - 1) / E;
+  const size_t ob = size_t(b) * A.interval;
+  for (int i = n - 1; i >= 0; --i) {
+    const size_t sl = ob + size_t(i);
+    if (A.nst && !(last && i == n - 1)) {
+      St.vst = A.seg_v + sl * A.vstride;
+      St.af = A.seg_a + sl * A.stride;
+      sfg::dev::k_adj_stacey<<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
+    }
+    J.uf = A.seg_u + sl * A.stride;
+    J.slot = i;
+    sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+    sfg::dev::k_adj_post<<<grid_for(D.nglob), 256, 0, rs>>>(
+        A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+        D.inv_idx, D.nglob, dt, dt2, dtsq2);
+  }
+  sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
+}
+
+void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
+  switch (h->epb) {
+    case 16: reverse_segment_E<16>(h, b, n, last, rs); break;
+    case 32: reverse_segment_E<32>(h, b, n, last, rs); break;
+    default: reverse_segment_E<8>(h, b, n, last, rs); break;
+  }
 }
 
 void restore_state(sfg_handle *h, const float *src) {
@@ -1386,7 +1455,7 @@ int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval) {
       save_state(h, A.ckpt + size_t(c) * stride);
       // the last segment is recorded on the way, so the reverse sweep starts
       // without recomputing it
-      if (c + 1 == A.ncheck) record_segment(h, c);
+      if (c + 1 == A.ncheck) record_segment(h, c, true);
       else run_steps(h, std::min(A.interval, nsteps - c * A.interval));
     }
     SFG_CUDA(cudaStreamSynchronize(h->stream));
@@ -1427,18 +1496,6 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       SFG_CUDA(cudaMemsetAsync(p, 0, (nv + 4) * sizeof(float), s));
     for (float *p : {A.sum, A.comp, A.seg})
       SFG_CUDA(cudaMemsetAsync(p, 0, A.nsum() * sizeof(float), s));
-    const float dt = float(as.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
-    sfg::dev::AdjArgs J{};
-    const DevMedium &D = h->el;
-    J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
-    J.prop0 = D.prop0; J.prop1 = D.prop1;
-    J.mu = A.mu; J.r = A.r; J.seg = A.seg;
-    J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
-    J.nspec = D.nspec;
-    J.quad = h->quad;
-    constexpr int E = 8;
-    const int eblocks = (D.nspec + E - 1) / E;
-    const int npts = D.nglob;
     const size_t cstride = 3 * (nv + 4);
     cudaStream_t rs = A.rstream;
     // the reverse stream starts after the set-up above
@@ -1446,32 +1503,29 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[0], 0));
     for (int c = A.ncheck - 1; c >= 0; --c) {
       const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
-      const size_t ob = size_t(b) * A.interval;
       if (!(c == A.ncheck - 1 && A.recorded == c)) {
         // buffer b is free once the reverse sweep of segment c + 2 is done
         SFG_CUDA(cudaStreamWaitEvent(s, A.ev_rev[b], 0));
         restore_state(h, A.ckpt + size_t(c) * cstride);
-        record_segment(h, c);
+        record_segment(h, c, false);
       }
       SFG_CUDA(cudaEventRecord(A.ev_rec[b], s));
       SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[b], 0));
-      // reverse sweep over the segment
-      for (int k = k1 - 1; k >= k0; --k) {
-        const size_t sl = ob + size_t(k - k0);
-        if (A.nst && k + 1 < A.nstep) {
-          sfg::dev::k_adj_stacey_grad<<<grid_for(A.nlb), 256, 0, rs>>>(
-              A.lb_g, A.lb_j, reinterpret_cast<const float4 *>(A.lb_geo), A.mu, A.seg_v + sl * A.vstride,
-              A.seg_a + sl * A.stride, A.seg + A.off_lb, A.nlb);
-          sfg::dev::k_adj_stacey<<<grid_for(A.nst), 256, 0, rs>>>(A.lv, A.mu, A.st_pt, A.st_c, A.nst);
+      sfg::dev::k_set_step<<<1, 1, 0, rs>>>(A.d_k0, k0);
+      if (c + 1 < A.ncheck && k1 - k0 == A.interval) {
+        // full segment, not the run's last: one graph per buffer
+        if (!A.graph_rev[b]) {
+          cudaGraph_t g = nullptr;
+          SFG_CUDA(cudaStreamBeginCapture(rs, cudaStreamCaptureModeThreadLocal));
+          reverse_segment(h, b, k1 - k0, false, rs);
+          SFG_CUDA(cudaStreamEndCapture(rs, &g));
+          SFG_CUDA(cudaGraphInstantiate(&A.graph_rev[b], g, 0));
+          cudaGraphDestroy(g);
         }
-        J.uf = A.seg_u + sl * A.stride;
-        J.ad_g = A.gtab + size_t(k) * nrec * 2;
-        sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
-        sfg::dev::k_adj_post<<<grid_for(npts), 256, 0, rs>>>(
-            A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
-            D.inv_idx, npts, dt, dt2, dtsq2);
+        SFG_CUDA(cudaGraphLaunch(A.graph_rev[b], rs));
+      } else {
+        reverse_segment(h, b, k1 - k0, c + 1 == A.ncheck, rs);
       }
-      sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
       SFG_CUDA(cudaEventRecord(A.ev_rev[b], rs));
       SFG_CUDA(cudaGetLastError());
     }
@@ -1479,6 +1533,8 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     SFG_CUDA(cudaStreamSynchronize(rs));
     SFG_CUDA(cudaStreamSynchronize(s));
     h->host_step = A.nstep;
+    const DevMedium &D = h->el;
+    const float dt2 = float(as.dt) / 2.0f;
     // compute order -> mesh order; rho: -W_p G(g_p)
     std::vector<float> tot(A.nsum());
     SFG_CUDA(cudaMemcpy(tot.data(), A.sum, tot.size() * sizeof(float), cudaMemcpyDeviceToHost));

@@ -187,3 +187,16 @@ def test_sources_replaced_after_initialize(sfg_lib):
     assert np.array_equal(a.seismograms(), b.seismograms())
     with pytest.raises(sfg.SfgError):
         a.set_sources([other, other])
+
+
+@pytest.mark.parametrize("interval", [50, 37, NSTEP])
+def test_checkpointed_forward_equals_plain_run(problem, interval):
+    """The checkpointed forward (its last segment recorded on the way) gives
+    the plain run's seismograms bit for bit."""
+    w, sim, model, weights = problem
+    sim.set_model(*[m.astype(np.float32) for m in model])
+    sim.reset()
+    sim.run(NSTEP)
+    plain = sim.seismograms()[0, :, 0].copy()
+    ck = sim.forward_checkpointed(NSTEP, interval)
+    assert np.array_equal(plain, ck)
