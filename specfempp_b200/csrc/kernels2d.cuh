@@ -61,7 +61,11 @@ struct MedArgs {
   const int *__restrict__ src_head;
   const float *__restrict__ u, *__restrict__ v;
   float *__restrict__ accum;
-  float *__restrict__ r;   // element-local results [element*25 + point][comp] (owner-computes)
+  // owner-computes: element results in point-major order, the contribution
+  // of element point p at r[slot[p]] (each point's contributions adjacent,
+  // in increasing element order)
+  float *__restrict__ r;
+  const int *__restrict__ slot;
   int e0, e1;      // element range of the colour
   int nblocks;     // blocks of this medium in the launch
 };
@@ -194,8 +198,9 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     }
   }
   if (LOCAL) {
-    if (NC == 2) reinterpret_cast<float2 *>(A.r)[p] = make_float2(a[0], a[NC - 1]);
-    else A.r[p] = a[0];
+    const int sl = __ldg(A.slot + p);
+    if (NC == 2) reinterpret_cast<float2 *>(A.r)[sl] = make_float2(a[0], a[NC - 1]);
+    else A.r[sl] = a[0];
   } else if (NC == 2) {
     reinterpret_cast<float2 *>(A.accum)[g] = make_float2(acc[0] + a[0], acc[NC - 1] + a[NC - 1]);
   } else {
@@ -258,7 +263,7 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
       a += f * S.src_arr[(size_t(s) * 2) * NP + q];
     }
   }
-  if (LOCAL) A.r[p] = a;
+  if (LOCAL) A.r[__ldg(A.slot + p)] = a;
   else A.accum[g] = acc + a;
 }
 
@@ -494,8 +499,8 @@ struct UpdateArgs {
   const float *__restrict__ cp_nx, *__restrict__ cp_nz;
   const int *__restrict__ cp_other;
   const float *__restrict__ other;
-  // owner-computes assembly: accum of point g = sum of r over inv_idx[inv_start[g] ..)
-  const int *__restrict__ inv_start, *__restrict__ inv_idx;
+  // owner-computes assembly: accum of point g = sum of r[inv_start[g] .. inv_start[g+1])
+  const int *__restrict__ inv_start;
   const float *__restrict__ r;
   float dt, dt2, dtsq2;
   int predict;                   // fuse the next step's predictor
@@ -607,7 +612,7 @@ __global__ void __launch_bounds__(256) k_update_gather(UpdateArgs A) {
     for (int c = 0; c < NC; ++c) acc[c] = 0.f;
     const int k1 = A.inv_start[g + 1];
     for (int k = A.inv_start[g]; k < k1; ++k) {
-      const int pl = A.inv_idx[k];
+      const int pl = k;
       if (NC == 2) {
         const float2 t = reinterpret_cast<const float2 *>(A.r)[pl];
         acc[0] = acc[0] + t.x;
@@ -704,7 +709,7 @@ __device__ __forceinline__ float rec_accel(const RecArgs &A, int g, int c) {
   if (A.cpl.inv_start) {   // owner-computes: gather in colour order
     acc = 0.f;
     for (int j = A.cpl.inv_start[g]; j < A.cpl.inv_start[g + 1]; ++j)
-      acc = acc + A.cpl.r[size_t(A.cpl.inv_idx[j]) * A.ncomp + c];
+      acc = acc + A.cpl.r[size_t(j) * A.ncomp + c];
   } else {
     acc = A.accum[k];
   }

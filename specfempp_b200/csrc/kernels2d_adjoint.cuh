@@ -42,7 +42,8 @@ struct AdjArgs {
       *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
   const float *__restrict__ mu;      // adjoint field mu_k [nglob][2]
   const float *__restrict__ uf;      // forward u~ of the step [nglob][2]
-  float *__restrict__ r;             // element-point results [nspec*25][2]
+  float *__restrict__ r;             // element-point results [pslot[p]][2] (point-major)
+  const int *__restrict__ pslot;
   float *__restrict__ seg;           // segment sums [nspec*25][kappa, mu]
   const int *__restrict__ ad_head, *__restrict__ ad_next;  // receivers per element
   const float *__restrict__ ad_h;    // receiver Lagrange weights [nrec][25]
@@ -124,7 +125,7 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
       r[1] += g_k[2 * k + 1] * h;
     }
   }
-  reinterpret_cast<float2 *>(A.r)[p] = make_float2(r[0], r[1]);
+  reinterpret_cast<float2 *>(A.r)[__ldg(A.pslot + p)] = make_float2(r[0], r[1]);
   // gradient terms of this step, summed over the segment
   const float W = sw[ix] * sw[iz] * jac;
   const float divm = mxx + mzz, divu = uxx + uzz;
@@ -145,13 +146,12 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
                                                   const float *__restrict__ af,
                                                   const float *__restrict__ minv,
                                                   const float *__restrict__ r,
-                                                  const int *__restrict__ inv_start,
-                                                  const int *__restrict__ inv_idx, int npts, float dt,
+                                                  const int *__restrict__ inv_start, int npts, float dt,
                                                   float dt2, float dtsq2) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += gridDim.x * blockDim.x) {
     float s0 = 0.f, s1 = 0.f;
     for (int k = inv_start[g]; k < inv_start[g + 1]; ++k) {
-      const float2 t = reinterpret_cast<const float2 *>(r)[inv_idx[k]];
+      const float2 t = reinterpret_cast<const float2 *>(r)[k];
       s0 = s0 + t.x;
       s1 = s1 + t.y;
     }

@@ -40,7 +40,8 @@ struct BatchArgs {
   const int *__restrict__ step;
   const float *__restrict__ u, *__restrict__ v;   // [nglob][NC][S]
   float *__restrict__ accum;
-  float *__restrict__ r;               // owner-computes: [element*25 + point][NC][S]
+  float *__restrict__ r;               // owner-computes: [slot[element*25 + point]][NC][S]
+  const int *__restrict__ slot;
   int e0;                              // first element of the colour
   int S;                               // shots
 };
@@ -146,7 +147,7 @@ __global__ void __launch_bounds__(NP * 32) k_stiffness_batched(BatchArgs A) {
   }
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
-    if (LOCAL) A.r[(p * NC + c) * A.S + shot] = a[c];
+    if (LOCAL) A.r[(size_t(__ldg(A.slot + p)) * NC + c) * A.S + shot] = a[c];
     else A.accum[(size_t(g) * NC + c) * A.S + shot] = acc[c] + a[c];
   }
 }
@@ -164,7 +165,7 @@ __global__ void __launch_bounds__(256) k_update_batched_gather(UpdateArgs A, int
     float acc = 0.f;
     const int k1 = A.inv_start[g + 1];
     for (int k = A.inv_start[g]; k < k1; ++k)
-      acc = acc + A.r[(size_t(A.inv_idx[k]) * NC + c) * S + s];
+      acc = acc + A.r[(size_t(k) * NC + c) * S + s];
     const float a = __fmul_rn(acc, A.minv[gc]);
     float vv = newmark_correct(A.v[i], a, A.dt2);
     float uu = A.u[i];
@@ -305,7 +306,7 @@ __global__ void __launch_bounds__(NP * 8) k_stiffness_batched4(BatchArgs A, int 
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     if (LOCAL) {
-      *reinterpret_cast<float4 *>(A.r + (p * NC + c) * A.S + shot0) =
+      *reinterpret_cast<float4 *>(A.r + (size_t(__ldg(A.slot + p)) * NC + c) * A.S + shot0) =
           make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
     } else {
       *reinterpret_cast<float4 *>(A.accum + (size_t(g) * NC + c) * A.S + shot0) =
@@ -353,7 +354,7 @@ __global__ void __launch_bounds__(256) k_update_batched4_gather(UpdateArgs A, in
     float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
     const int k1 = A.inv_start[g + 1];
     for (int k = A.inv_start[g]; k < k1; ++k) {
-      const float4 t = *reinterpret_cast<const float4 *>(A.r + (size_t(A.inv_idx[k]) * NC + c) * S + s);
+      const float4 t = *reinterpret_cast<const float4 *>(A.r + (size_t(k) * NC + c) * S + s);
       acc.x = acc.x + t.x; acc.y = acc.y + t.y; acc.z = acc.z + t.z; acc.w = acc.w + t.w;
     }
     const float mi = A.minv[gc];
@@ -424,7 +425,7 @@ __global__ void __launch_bounds__(32) k_receivers_batched(RecArgs A, int S) {
           float sum = 0.f;
           if (A.cpl.inv_start) {
             for (int j = A.cpl.inv_start[g]; j < A.cpl.inv_start[g + 1]; ++j)
-              sum = sum + A.cpl.r[(size_t(A.cpl.inv_idx[j]) * NC + c) * S + shot];
+              sum = sum + A.cpl.r[(size_t(j) * NC + c) * S + shot];
           } else {
             sum = A.accum[k];
           }

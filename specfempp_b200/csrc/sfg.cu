@@ -18,6 +18,7 @@
 #include "kernels2d.cuh"
 #include "kernels2d_batched.cuh"
 #include "kernels2d_adjoint.cuh"
+#include "kernels2d_tma.cuh"
 
 namespace {
 
@@ -83,7 +84,8 @@ struct DevMedium {
   float *minv = nullptr;
   float *u = nullptr, *v = nullptr, *accum = nullptr, *a = nullptr;
   float *r = nullptr;              // element-local contributions (owner-computes assembly)
-  int *inv_start = nullptr, *inv_idx = nullptr;
+  int *inv_start = nullptr;
+  int *slot = nullptr;  // CSR position of each element point's contribution
   int *rec_list = nullptr;
   int nrec = 0;
 };
@@ -150,9 +152,12 @@ struct sfg_handle {
   int *d_step = nullptr, *d_flag = nullptr;
   int host_step = 0;
   int epb = 16;
-  int variant = 1;           // 1 colour passes, 2 persistent colour passes, 3 owner-computes
+  // 1 colour passes, 2 persistent colour passes, 3 owner-computes,
+  // 4 owner-computes with bulk-copy staged element arrays
+  int variant = 1;
   int sm_count = 148;
   int resident[2][3] = {{0}};  // persistent: resident blocks per SM [EK][E index]
+  int resident_tma[2][3] = {{0}};  // bulk-copy element kernel: resident blocks per SM
   cudaStream_t stream = nullptr;
   cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr, graph_e = nullptr;
   int graph_steps = 0;
@@ -217,10 +222,18 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.ncomp = M.ncomp;
   D.color_start = M.color_start;
   if (M.nspec == 0) return;
-  D.ibool = m.upload(M.ibool);
-  D.xix = m.upload(M.xix); D.xiz = m.upload(M.xiz); D.gax = m.upload(M.gax);
-  D.gaz = m.upload(M.gaz); D.jac = m.upload(M.jac);
-  D.prop0 = m.upload(M.prop0); D.prop1 = m.upload(M.prop1);
+  // element arrays padded with zeros to whole tiles of 32 elements (the
+  // bulk-copy element kernel always moves whole tiles)
+  const size_t npad = size_t((M.nspec + 31) / 32 * 32) * sfg::NPTS;
+  auto padded = [&](const auto &v) {
+    auto w = v;
+    w.resize(std::max(npad, v.size()), 0);
+    return m.upload(w);
+  };
+  D.ibool = padded(M.ibool);
+  D.xix = padded(M.xix); D.xiz = padded(M.xiz); D.gax = padded(M.gax);
+  D.gaz = padded(M.gaz); D.jac = padded(M.jac);
+  D.prop0 = padded(M.prop0); D.prop1 = padded(M.prop1);
   D.bc_slot = m.upload(M.bc_slot);
   D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
   D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
@@ -236,7 +249,11 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.accum = m.zeros<float>(n + 4);
   D.a = m.zeros<float>(n + 4);
   D.inv_start = m.upload(M.inv_start);
-  D.inv_idx = m.upload(M.inv_idx);
+  {
+    std::vector<int> slot(M.inv_idx.size());
+    for (size_t k = 0; k < M.inv_idx.size(); ++k) slot[size_t(M.inv_idx[k])] = int(k);
+    D.slot = m.upload(slot);
+  }
   D.r = m.zeros<float>(size_t(M.nspec) * sfg::NPTS * M.ncomp * D.S + 4);
 }
 
@@ -248,7 +265,7 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
   A.src_head = D.src_head;
-  A.u = D.u; A.v = D.v; A.accum = D.accum; A.r = D.r;
+  A.u = D.u; A.v = D.v; A.accum = D.accum; A.r = D.r; A.slot = D.slot;
   return A;
 }
 
@@ -273,6 +290,25 @@ void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
     S.ac.e0 = 0; S.ac.e1 = ac.nspec; S.ac.nblocks = (ac.nspec + E - 1) / E;
     const int grid = S.el.nblocks + S.ac.nblocks;
     if (grid > 0) sfg::dev::k_stiffness<E, EK, true><<<grid, sfg::dev::NP * E, 0, s>>>(S);
+    return;
+  }
+  if (variant == 4) {
+    // owner-computes, persistent, element arrays staged by bulk copies
+    constexpr int ST = 3;
+    const int smem = sfg::dev::TmaLayout<E>::bytes(ST);
+    auto kern = sfg::dev::k_stiffness_tma<E, EK, ST>;
+    const int ei = E == 8 ? 0 : (E == 16 ? 1 : 2);
+    int &nb = h->resident_tma[EK][ei];
+    if (nb == 0) {
+      SFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, sfg::dev::NP * E, smem));
+      nb = std::max(nb, 1);
+    }
+    S.el.e0 = 0; S.el.e1 = el.nspec;
+    S.ac.e0 = 0; S.ac.e1 = ac.nspec;
+    const int nt_el = (el.nspec + E - 1) / E, nt_ac = (ac.nspec + E - 1) / E;
+    const int grid = std::min(nt_el + nt_ac, nb * h->sm_count);
+    if (grid > 0) kern<<<grid, sfg::dev::NP * E, smem, s>>>(S, nt_el, nt_ac, h->d_flag);
     return;
   }
   const bool persistent = variant == 2;
@@ -337,7 +373,7 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
   B.src_arr = h->d_src_arr; B.stf = h->d_stf;
   B.nsrc = h->asmb.nsrc; B.nstep = h->asmb.nstep;
   B.step = step;
-  B.u = el.u; B.v = el.v; B.accum = el.accum; B.r = el.r;
+  B.u = el.u; B.v = el.v; B.accum = el.accum; B.r = el.r; B.slot = el.slot;
   B.S = el.S;
   // quad-shot kernels when the shots come in fours
   const bool quad = el.S % 4 == 0;
@@ -363,7 +399,7 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
       else sfg::dev::k_stiffness_batched<1, false><<<grid, threads, 0, s>>>(B);
     }
   };
-  if (variant == 3) {
+  if (variant == 3 || variant == 4) {
     launch(0, el.nspec, true);
     return;
   }
@@ -407,9 +443,8 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   U.dt2 = dt / 2.0f;
   U.dtsq2 = dt * dt / 2.0f;
   U.predict = predict ? 1 : 0;
-  if (h->variant == 3) {
+  if (h->variant == 3 || h->variant == 4) {
     U.inv_start = D.inv_start;
-    U.inv_idx = D.inv_idx;
     U.r = D.r;
   }
   U.flag = h->d_flag;
@@ -457,7 +492,7 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
   const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
   sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
-  if (h->variant == 3) {
+  if (h->variant == 3 || h->variant == 4) {
     if (D.S > 1 && D.S % 4 == 0)
       sfg::dev::k_update_batched4_gather<<<grid_for(U.n / 4), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
@@ -557,16 +592,17 @@ void run_steps(sfg_handle *h, int nsteps) {
 void autotune(sfg_handle *h) {
   const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
                      h->opt.elements_per_block == 32;
-  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 3;
+  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 4;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
+  if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
   std::vector<std::pair<int, int>> cand;
   if (h->asmb.nshots > 1) {
     for (int v : {1, 3})
       if (!fix_v || v == h->variant) cand.push_back({v, 16});
   } else {
-    for (int v : {1, 2, 3})
+    for (int v : {1, 2, 3, 4})
       for (int e : {8, 16, 32})
         if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
   }
@@ -1146,6 +1182,10 @@ int sfg_check_finite(sfg_handle *h) {
   int f = 0;
   if (cudaStreamSynchronize(h->stream) != cudaSuccess) return SFG_ERR_CUDA;
   if (cudaMemcpy(&f, h->d_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return SFG_ERR_CUDA;
+  if (f == 2) {
+    h->err = "an element kernel gave up waiting for its staged element data";
+    return SFG_ERR_CUDA;
+  }
   return f ? SFG_ERR_NONFINITE : 0;
 }
 
@@ -1182,7 +1222,6 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
     launch_stiffness(h, el, h->ac, nd.words, s, h->variant == 2 ? 2 : 1);
     sfg::dev::UpdateArgs U = update_args(h, el, h->ac, SFG_MEDIUM_ELASTIC, false, false);
     U.inv_start = nullptr;
-    U.inv_idx = nullptr;
     U.r = nullptr;
     U.a_store = a;
     U.flag = nd.words + 1;
@@ -1389,7 +1428,7 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   sfg::dev::AdjArgs J{};
   J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
   J.prop0 = D.prop0; J.prop1 = D.prop1;
-  J.mu = A.mu; J.r = A.r; J.seg = A.seg;
+  J.mu = A.mu; J.r = A.r; J.pslot = D.slot; J.seg = A.seg;
   J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
   J.gtab = A.gtab; J.seg_k0 = A.d_k0; J.nrec = h->asmb.nrec;
   J.nspec = D.nspec;
@@ -1413,7 +1452,7 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
     sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
     sfg::dev::k_adj_post<<<grid_for(D.nglob), 256, 0, rs>>>(
         A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
-        D.inv_idx, D.nglob, dt, dt2, dtsq2);
+        D.nglob, dt, dt2, dtsq2);
   }
   sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
 }

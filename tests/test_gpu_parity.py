@@ -102,7 +102,8 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
 
 
 @pytest.mark.parametrize("epb,spg,variant", [(8, 7, 1), (32, 1, 1), (8, 3, 2), (16, 20, 2), (32, 5, 2),
-                                             (8, 4, 3), (16, 20, 3), (32, 1, 3)])
+                                             (8, 4, 3), (16, 20, 3), (32, 1, 3),
+                                             (8, 4, 4), (16, 20, 4), (32, 1, 4)])
 def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg, variant):
     from specfempp_b200 import meshgen
     w = meshgen.coupled_400x200(nstep=120, nx=40, nz=20)
@@ -148,3 +149,14 @@ def test_step_and_run_agree(sfg_lib):
     for _ in range(case.nstep):
         sim.step()
     assert np.array_equal(a, sim.seismograms()[0])
+
+
+@pytest.mark.parametrize("name", ["HomogeneousAcousticDomainDirichletBC", "HomogeneousElasticDomainStaceyBC"])
+@pytest.mark.parametrize("variant", [3, 4])
+def test_owner_computes_variants_equal_colour_passes(sfg_lib, name, variant):
+    """Single-medium fixtures: the owner-computes kernels (plain and with
+    bulk-copy staging) give the colour passes' bits."""
+    case, _, _ = golden_case(name)
+    _, a = product_run(case, epb=16, variant=1)
+    _, b = product_run(case, epb=8, variant=variant)
+    assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
