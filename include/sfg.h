@@ -88,7 +88,8 @@ typedef struct sfg_options {
   int kernel_variant;            /* assembly / element kernel: 1 colour passes (one block
                                     per chunk), 2 colour passes with a persistent
                                     prefetching kernel, 3 owner-computes (one element
-                                    launch, per-point gather in colour order); all give
+                                    launch, per-point sum in colour order), 4 owner-computes
+                                    with the element arrays staged by bulk copies; all give
                                     the same bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
 } sfg_options;

@@ -71,12 +71,15 @@ __device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t by
 }
 
 constexpr int TMA_ARRAYS = 8;  // ibool, xix, xiz, gax, gaz, jac, c0, c1
+// Shared words per element: NC x {U, UT, F0, F1T} as 5 rows of 8, plus 4 so
+// that consecutive elements start 4 banks apart (fewer bank conflicts).
+constexpr int ELEM_WORK = 2 * 4 * NG * 8 + 4;
 
 template <int E>
 struct TmaLayout {
   static constexpr int TW = E * NP;                                   // words per array per tile
   static constexpr int STAGE_BYTES = TMA_ARRAYS * TW * 4;
-  static constexpr int WORK_FLOATS = E * 2 * 4 * NG * 8;              // NC x {U, UT, F0, F1T}, rows of 8
+  static constexpr int WORK_FLOATS = E * ELEM_WORK;
   static constexpr int bytes(int S) { return 64 + S * STAGE_BYTES + WORK_FLOATS * 4; }
 };
 
@@ -93,25 +96,26 @@ __device__ __forceinline__ void tma_issue(const StiffArgs &A, int nt_el, int til
   for (int k = 0; k < TMA_ARRAYS; ++k) bulk_g2s(stage + k * TW * 4, src[k], TW * 4, bar);
 }
 
-// One tile of one medium (KIND 0 acoustic, 1 elastic SH, 2 elastic P-SV).
-// Returns after the tile's second barrier; `refill` runs right after it (the
-// stage is free then).
+// Per-element-point geometry and material words.
+struct PointGeom {
+  int g;
+  float xix, xiz, gax, gaz, jac, c0, c1;
+};
+
+// One tile of one medium (KIND 0 acoustic, 1 elastic SH, 2 elastic P-SV),
+// given this thread's point geometry and field value.  Returns after the
+// tile's second barrier; `refill` runs right after it.
 template <int E, int KIND, typename Refill>
-__device__ __forceinline__ void tma_tile(const StiffArgs &S, const MedArgs &A, int e, int le, int q,
-                                         int iz, int ix, const unsigned char *stage, float *base,
-                                         const float (&hx)[NG], const float (&hz)[NG], const float (&wx)[NG],
-                                         const float (&wz)[NG], float wix, float wiz, float2 u_in,
-                                         Refill refill) {
+__device__ __forceinline__ void tile_compute(const StiffArgs &S, const MedArgs &A, int e, int q, int iz, int ix,
+                                             const PointGeom &P, float *base, const float (&hx)[NG],
+                                             const float (&hz)[NG], const float (&wx)[NG], const float (&wz)[NG],
+                                             float wix, float wiz, float2 u_in, Refill refill) {
   constexpr int NC = KIND == 2 ? 2 : 1;
   constexpr int RS = 8;
   constexpr int ARR = NG * RS;
-  constexpr int TW = TmaLayout<E>::TW;
-  const int t = le * NP + q;
   const bool act = e < A.e1;
-  const float *sg = reinterpret_cast<const float *>(stage);
-  const int g = act ? reinterpret_cast<const int *>(stage)[t] : 0;
-  const float xix = sg[1 * TW + t], xiz = sg[2 * TW + t], gax = sg[3 * TW + t], gaz = sg[4 * TW + t],
-              jac = sg[5 * TW + t], c0 = sg[6 * TW + t], c1 = sg[7 * TW + t];
+  const int g = P.g;
+  const float xix = P.xix, xiz = P.xiz, gax = P.gax, gaz = P.gaz, jac = P.jac, c0 = P.c0, c1 = P.c1;
   const int bs = act ? __ldg(A.bc_slot + e) : -1;
   const int src = act ? __ldg(A.src_head + e) : -1;
   float uu[NC];
@@ -198,6 +202,21 @@ __device__ __forceinline__ void tma_tile(const StiffArgs &S, const MedArgs &A, i
   else A.r[sl] = a[0];
 }
 
+template <int E, int KIND, typename Refill>
+__device__ __forceinline__ void tma_tile(const StiffArgs &S, const MedArgs &A, int e, int le, int q, int iz,
+                                         int ix, const unsigned char *stage, float *base, const float (&hx)[NG],
+                                         const float (&hz)[NG], const float (&wx)[NG], const float (&wz)[NG],
+                                         float wix, float wiz, float2 u_in, Refill refill) {
+  constexpr int TW = TmaLayout<E>::TW;
+  const int t = le * NP + q;
+  const float *sg = reinterpret_cast<const float *>(stage);
+  PointGeom P;
+  P.g = e < A.e1 ? reinterpret_cast<const int *>(stage)[t] : 0;
+  P.xix = sg[1 * TW + t]; P.xiz = sg[2 * TW + t]; P.gax = sg[3 * TW + t]; P.gaz = sg[4 * TW + t];
+  P.jac = sg[5 * TW + t]; P.c0 = sg[6 * TW + t]; P.c1 = sg[7 * TW + t];
+  tile_compute<E, KIND>(S, A, e, q, iz, ix, P, base, hx, hz, wx, wz, wix, wiz, u_in, refill);
+}
+
 // The field at this thread's point of a tile (read from the tile's staged
 // global indices): issued one tile ahead, so its latency hides behind the
 // arithmetic of the current tile.
@@ -249,7 +268,7 @@ __global__ void __launch_bounds__(NP * E) k_stiffness_tma(StiffArgs A, int nt_el
     wz[l] = shpw[l * NG + iz];
   }
   const float wiz = sw[iz], wix = sw[ix];
-  float *base = work + le * (2 * 4 * NG * 8);
+  float *base = work + le * ELEM_WORK;
   int j = 0;
   float2 u_cur = make_float2(0.f, 0.f);
   if (nmine > 0) {

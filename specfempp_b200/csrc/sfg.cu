@@ -10,6 +10,7 @@
 #include <mutex>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <unordered_map>
 #include <vector>
 
@@ -399,7 +400,7 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
       else sfg::dev::k_stiffness_batched<1, false><<<grid, threads, 0, s>>>(B);
     }
   };
-  if (variant == 3 || variant == 4) {
+  if (variant >= 3) {
     launch(0, el.nspec, true);
     return;
   }
@@ -443,7 +444,7 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   U.dt2 = dt / 2.0f;
   U.dtsq2 = dt * dt / 2.0f;
   U.predict = predict ? 1 : 0;
-  if (h->variant == 3 || h->variant == 4) {
+  if (h->variant >= 3) {
     U.inv_start = D.inv_start;
     U.r = D.r;
   }
@@ -492,7 +493,7 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
   const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   const DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
   sfg::dev::UpdateArgs U = update_args(h, D, O, medium, predict, advance);
-  if (h->variant == 3 || h->variant == 4) {
+  if (h->variant >= 3) {
     if (D.S > 1 && D.S % 4 == 0)
       sfg::dev::k_update_batched4_gather<<<grid_for(U.n / 4), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
