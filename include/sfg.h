@@ -99,7 +99,11 @@ typedef struct sfg_source2d {
   int shot;                      /* shot this source belongs to (0..nshots-1) */
   int stf;                       /* SFG_STF_* */
   double f0, factor, tshift, angle;
+  int kind;                      /* SFG_SOURCE_FORCE or SFG_SOURCE_MOMENT_TENSOR */
+  double mxx, mzz, mxz;          /* moment tensor (kind SFG_SOURCE_MOMENT_TENSOR) */
 } sfg_source2d;
+
+enum { SFG_SOURCE_FORCE = 0, SFG_SOURCE_MOMENT_TENSOR = 1 };
 
 typedef struct sfg_info {
   int nspec, nspec_elastic, nspec_acoustic;

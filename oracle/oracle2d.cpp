@@ -577,6 +577,37 @@ struct Sim {
     }
   }
 
+  // Moment-tensor source array (P-SV): M . grad(l_x(xi) l_z(gamma)) with the
+  // stored Jacobian interpolated at the source
+  // (core/specfem/assembly/compute_source_array/dim2/impl/compute_source_array_from_tensor.cpp:17-86;
+  //  tensor [[Mxx, Mxz], [Mxz, Mzz]], core/specfem/source/dim2/tensor_source/moment_tensor_source.cpp:22-35).
+  // Interpolants and products in the setup precision.
+  void moment_tensor_array(Src &S, int e, double xi, double ga, double mxx, double mzz, double mxz) {
+    if (S.medium != MED_ELASTIC || ncomp_el != 2)
+      throw std::runtime_error("moment-tensor sources need an elastic P-SV element");
+    S.ncomp = 2;
+    double zd[NG], wd[NG], hx[NG], hpx[NG], hg[NG], hpg[NG];
+    gll_nodes(zd, wd);
+    lagrange_interp<double>(xi, zd, hx, hpx);
+    lagrange_interp<double>(ga, zd, hg, hpg);
+    double jx[4] = {0, 0, 0, 0};
+    for (int iz = 0; iz < NG; ++iz)
+      for (int ix = 0; ix < NG; ++ix) {
+        const size_t p = size_t(e) * NP + iz * NG + ix;
+        const double h = hx[ix] * hg[iz];
+        jx[0] += h * double(xix[p]); jx[1] += h * double(xiz[p]);
+        jx[2] += h * double(gax[p]); jx[3] += h * double(gaz[p]);
+      }
+    for (int iz = 0; iz < NG; ++iz)
+      for (int ix = 0; ix < NG; ++ix) {
+        const int q = iz * NG + ix;
+        const double dsx = (hpx[ix] * jx[0]) * hg[iz] + hx[ix] * (hpg[iz] * jx[2]);
+        const double dsz = (hpx[ix] * jx[1]) * hg[iz] + hx[ix] * (hpg[iz] * jx[3]);
+        S.arr[0][q] = T(mxx * dsx + mxz * dsz);
+        S.arr[1][q] = T(mxz * dsx + mzz * dsz);
+      }
+  }
+
   void sources() {
     const int nstep = in.nstep;
     for (int s = 0; s < in.nsrc; ++s) {
@@ -586,15 +617,19 @@ struct Sim {
       S.medium = medium[e];
       T h[NP];
       interpolants(xi, ga, h);
-      T fv[2];
-      if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
-      else {
-        S.ncomp = 2;
-        T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
-        fv[0] = std::sin(ang); fv[1] = std::cos(ang);
+      if (in.src_kind && in.src_kind[s] == 1) {
+        moment_tensor_array(S, e, xi, ga, in.src_mxx[s], in.src_mzz[s], in.src_mxz[s]);
+      } else {
+        T fv[2];
+        if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
+        else {
+          S.ncomp = 2;
+          T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
+          fv[0] = std::sin(ang); fv[1] = std::cos(ang);
+        }
+        for (int q = 0; q < NP; ++q)
+          for (int c = 0; c < S.ncomp; ++c) S.arr[c][q] = h[q] * fv[c];
       }
-      for (int q = 0; q < NP; ++q)
-        for (int c = 0; c < S.ncomp; ++c) S.arr[c][q] = h[q] * fv[c];
       S.stf.resize(size_t(nstep));
       if (in.stf_table) {
         for (int i = 0; i < nstep; ++i) S.stf[i] = T(in.stf_table[size_t(i) * in.nsrc + s]);

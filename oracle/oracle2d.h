@@ -30,6 +30,10 @@ typedef struct OracleInput2D {
    * rounded to the run precision; 1: setup in the run precision, as the
    * reference does with type_real. */
   int setup_in_run_precision;
+  /* optional per-source kind (NULL: all force sources): 0 force, 1 moment
+   * tensor with components src_mxx, src_mzz, src_mxz */
+  const int *src_kind;
+  const double *src_mxx, *src_mzz, *src_mxz;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

@@ -46,6 +46,7 @@ class OracleInput2D(C.Structure):
         ("ntypes", C.c_int), ("seis_types", _ip),
         ("dt", C.c_double), ("nstep", C.c_int), ("nstep_between_samples", C.c_int),
         ("setup_in_run_precision", C.c_int),
+        ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
     ]
 
 
@@ -94,6 +95,10 @@ class Source:
     tshift: float = 0.0
     angle: float = 0.0
     stf: str = "ricker"          # "ricker" or "dirac"
+    kind: str = "force"          # "force" or "moment_tensor"
+    mxx: float = 0.0
+    mzz: float = 0.0
+    mxz: float = 0.0
 
 
 @dataclass
@@ -190,6 +195,11 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     nsb = max(1, case.nstep_between_samples)
     inp.nstep_between_samples = nsb
     inp.setup_in_run_precision = int(case.setup_in_run_precision)
+    inp.src_kind = _ptr(arr([1 if getattr(s, "kind", "force") == "moment_tensor" else 0 for s in srcs],
+                            np.int32), _ip)
+    inp.src_mxx = _ptr(arr([getattr(s, "mxx", 0.0) for s in srcs], np.float64), _dp)
+    inp.src_mzz = _ptr(arr([getattr(s, "mzz", 0.0) for s in srcs], np.float64), _dp)
+    inp.src_mxz = _ptr(arr([getattr(s, "mxz", 0.0) for s in srcs], np.float64), _dp)
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()
@@ -233,9 +243,12 @@ def read_sources_yaml(path):
         d = yaml.safe_load(f)
     out = []
     for s in d["sources"]:
-        if "force" not in s:
-            raise ValueError("only force sources are on this path")
-        fs = s["force"]
+        if "force" in s:
+            fs, kind_src = s["force"], "force"
+        elif "moment-tensor" in s:
+            fs, kind_src = s["moment-tensor"], "moment_tensor"
+        else:
+            raise ValueError("only force and moment-tensor sources are on this path")
         if "Ricker" in fs:
             rk, kind = fs["Ricker"], "ricker"
         elif "Dirac" in fs:
@@ -244,7 +257,9 @@ def read_sources_yaml(path):
             raise ValueError("only Ricker and Dirac time functions are on this path")
         out.append(Source(x=float(fs["x"]), z=float(fs["z"]), f0=float(rk.get("f0", 0.0)),
                           factor=float(rk["factor"]), tshift=float(rk.get("tshift", 0.0)),
-                          angle=float(fs.get("angle", 0.0)), stf=kind))
+                          angle=float(fs.get("angle", 0.0)), stf=kind, kind=kind_src,
+                          mxx=float(fs.get("Mxx", 0.0)), mzz=float(fs.get("Mzz", 0.0)),
+                          mxz=float(fs.get("Mxz", 0.0))))
     return out
 
 
@@ -273,8 +288,8 @@ def stf_tables(sources, dt, nstep):
 def effective_f0(s, dt):
     """Dirac sources use f0 = 1/(10 dt) (dirac.cpp:25)."""
     if s.stf == "dirac":
-        return Source(x=s.x, z=s.z, f0=float(np.float32(1.0) / (np.float32(10.0) * np.float32(dt))),
-                      factor=s.factor, tshift=s.tshift, angle=s.angle, stf="dirac")
+        from dataclasses import replace
+        return replace(s, f0=float(np.float32(1.0) / (np.float32(10.0) * np.float32(dt))))
     return s
 
 
@@ -288,10 +303,11 @@ def load_fixture(fixture_dir, types=("displacement",)):
     mesh = read_database(os.path.join(fixture_dir, "database.bin"))
     names, rx, rz = read_stations(os.path.join(fixture_dir, "STATIONS"))
     src = read_sources_yaml(os.path.join(fixture_dir, "sources.yaml"))
+    sh = str(cfg["simulation-setup"].get("elastic-wave", "P_SV")).upper() == "SH"
     return Case2D(mesh=mesh, sources=src, rec_x=rx, rec_z=rz, dt=float(ts["dt"]),
                   nstep=int(ts["nstep"]), seis_types=list(types),
                   nstep_between_samples=int(rc.get("nstep_between_samples", 1)),
-                  rec_angle=float(rc.get("angle", 0.0)), stations=names)
+                  rec_angle=float(rc.get("angle", 0.0)), stations=names, elastic_sh=sh)
 
 
 def read_trace(path):

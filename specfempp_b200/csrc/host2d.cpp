@@ -96,6 +96,24 @@ void lagrange(double xi, const double z[NGLL], double h[NGLL]) {
   }
 }
 
+// Lagrange interpolants and their derivatives at xi
+// (src/quadrature/gll/lagrange_poly.cpp:12-44).
+void lagrange_d(double xi, const double z[NGLL], double h[NGLL], double hp[NGLL]) {
+  lagrange(xi, z, h);
+  for (int d = 0; d < NGLL; ++d) {
+    double den = 1, sum = 0;
+    for (int i = 0; i < NGLL; ++i) {
+      if (i == d) continue;
+      den *= z[d] - z[i];
+      double p = 1;
+      for (int j = 0; j < NGLL; ++j)
+        if (j != d && j != i) p *= xi - z[j];
+      sum += p;
+    }
+    hp[d] = sum / den;
+  }
+}
+
 // ----------------------------------------------------- shape functions ---
 void shape(int ngnod, double xi, double ga, double *s, double *dx, double *dg) {
   if (ngnod == 4) {
@@ -847,12 +865,34 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
     std::vector<int> &head = med == 1 ? a.el_src_head : a.ac_src_head;
     a.src_next[s] = head[ce];
     head[ce] = s;
-    double hx[NGLL], hg[NGLL];
-    lagrange(xi, a.zgll, hx);
-    lagrange(ga, a.zgll, hg);
+    double hx[NGLL], hg[NGLL], hpx[NGLL], hpg[NGLL];
+    lagrange_d(xi, a.zgll, hx, hpx);
+    lagrange_d(ga, a.zgll, hg, hpg);
     const MediumData &D = med == 1 ? a.el : a.ac;
     const double ang = S.angle * M_PI / 180.0;
-    for (int iz = 0; iz < NGLL; ++iz)
+    if (S.kind == 1) {
+      // moment tensor: source array M . grad(l_x l_z) with the Jacobian
+      // interpolated at the source (compute_source_array_from_tensor.cpp:17-86,
+      // moment_tensor_source.cpp:22-35); elastic P-SV only
+      if (med != 1 || D.ncomp != 2)
+        throw std::runtime_error("moment-tensor sources need an elastic P-SV element");
+      double jx[4] = {0, 0, 0, 0};  // xi_x, xi_z, gamma_x, gamma_z at the source
+      for (int iz = 0; iz < NGLL; ++iz)
+        for (int ix = 0; ix < NGLL; ++ix) {
+          const size_t p = size_t(ce) * NPTS + iz * NGLL + ix;
+          const double h = hx[ix] * hg[iz];
+          jx[0] += h * D.xix[p]; jx[1] += h * D.xiz[p]; jx[2] += h * D.gax[p]; jx[3] += h * D.gaz[p];
+        }
+      for (int iz = 0; iz < NGLL; ++iz)
+        for (int ix = 0; ix < NGLL; ++ix) {
+          const int q = iz * NGLL + ix;
+          const double dsx = (hpx[ix] * jx[0]) * hg[iz] + hx[ix] * (hpg[iz] * jx[2]);
+          const double dsz = (hpx[ix] * jx[1]) * hg[iz] + hx[ix] * (hpg[iz] * jx[3]);
+          a.src_arr[(size_t(s) * 2) * NPTS + q] = float(S.mxx * dsx + S.mxz * dsz);
+          a.src_arr[(size_t(s) * 2 + 1) * NPTS + q] = float(S.mxz * dsx + S.mzz * dsz);
+        }
+    }
+    for (int iz = 0; iz < NGLL && S.kind == 0; ++iz)
       for (int ix = 0; ix < NGLL; ++ix) {
         const int q = iz * NGLL + ix;
         const double h = hx[ix] * hg[iz];

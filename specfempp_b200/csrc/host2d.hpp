@@ -37,6 +37,8 @@ struct Source2D {
   double x, z;
   int shot, stf;
   double f0, factor, tshift, angle;
+  int kind = 0;                   // 0 force, 1 moment tensor
+  double mxx = 0, mzz = 0, mxz = 0;
 };
 
 // Per-medium device-ready arrays (element order = compute order of that medium).

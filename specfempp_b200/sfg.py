@@ -51,7 +51,8 @@ class Options(C.Structure):
 class Source2D(C.Structure):
     _fields_ = [("x", C.c_double), ("z", C.c_double), ("shot", C.c_int), ("stf", C.c_int),
                 ("f0", C.c_double), ("factor", C.c_double), ("tshift", C.c_double),
-                ("angle", C.c_double)]
+                ("angle", C.c_double), ("kind", C.c_int), ("mxx", C.c_double), ("mzz", C.c_double),
+                ("mxz", C.c_double)]
 
 
 class Info(C.Structure):
@@ -127,6 +128,13 @@ class Source:
     angle: float = 0.0
     stf: str = "ricker"
     shot: int = 0
+    kind: str = "force"            # "force" or "moment_tensor"
+    mxx: float = 0.0
+    mzz: float = 0.0
+    mxz: float = 0.0
+
+
+SOURCE_KIND = {"force": 0, "moment_tensor": 1}
 
 
 def _arr(x, dtype):
@@ -201,7 +209,10 @@ class Simulation2D:
         for i, s in enumerate(sources):
             arr[i] = Source2D(x=s.x, z=s.z, shot=getattr(s, "shot", 0), stf=STF[getattr(s, "stf", "ricker")],
                               f0=s.f0, factor=s.factor, tshift=getattr(s, "tshift", 0.0),
-                              angle=getattr(s, "angle", 0.0))
+                              angle=getattr(s, "angle", 0.0),
+                              kind=SOURCE_KIND[getattr(s, "kind", "force")],
+                              mxx=getattr(s, "mxx", 0.0), mzz=getattr(s, "mzz", 0.0),
+                              mxz=getattr(s, "mxz", 0.0))
         self._check(self.lib.sfg_set_sources(self.h, len(sources), arr))
 
     def set_stf_table(self, table):

@@ -33,11 +33,17 @@ def golden_case(name, nstep=None):
                   mat_vs=z["mat_vs"], abs_ispec=z["abs_ispec"], abs_type=z["abs_type"],
                   free_ispec=z["free_ispec"], free_type=z["free_type"],
                   coupled_pairs=np.zeros((0, 2), np.int32))
-    srcs = [runner.Source(x=s[0], z=s[1], f0=s[2], factor=s[3], tshift=s[4], angle=s[5],
-                          stf="dirac" if s[6] else "ricker") for s in z["src"]]
+    srcs = []
+    for s in z["src"]:
+        mt = len(s) > 7 and bool(s[7])
+        srcs.append(runner.Source(x=s[0], z=s[1], f0=s[2], factor=s[3], tshift=s[4], angle=s[5],
+                                  stf="dirac" if s[6] else "ricker",
+                                  kind="moment_tensor" if mt else "force",
+                                  mxx=s[8] if mt else 0.0, mzz=s[9] if mt else 0.0, mxz=s[10] if mt else 0.0))
     case = runner.Case2D(mesh=mesh, sources=srcs, rec_x=z["rec_x"], rec_z=z["rec_z"],
                          dt=float(z["dt"]), nstep=int(nstep or z["nstep"]),
-                         rec_angle=float(z["rec_angle"]))
+                         rec_angle=float(z["rec_angle"]),
+                         elastic_sh=bool(int(z["elastic_sh"])) if "elastic_sh" in z else False)
     return case, z["traces"], float(z["trace_t0"])
 
 
@@ -46,7 +52,7 @@ def reference_metric(computed, traces):
 
     computed: [nsig, nrec, ncomp]; traces: [nrec, ncomp, nsig]."""
     n = min(computed.shape[0], traces.shape[2])
-    c = np.transpose(computed[:n], (1, 2, 0))
+    c = np.transpose(computed[:n, :, :traces.shape[1]], (1, 2, 0))
     t = traces[:, :, :n]
     return np.abs(c - t).sum(axis=(1, 2)) / np.abs(t).sum(axis=(1, 2))
 
@@ -84,6 +90,7 @@ def product_run(case, types=("displacement",), nsteps=None, epb=0, spg=0, varian
     from specfempp_b200 import sfg
     sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=case.nstep,
                            nstep_between_samples=case.nstep_between_samples,
+                           elastic_wave="sh" if case.elastic_sh else "psv",
                            point_rho=case.point_rho, point_vp=case.point_vp, point_vs=case.point_vs,
                            elements_per_block=epb, steps_per_graph=spg, kernel_variant=variant)
     sim.set_sources(case.sources)

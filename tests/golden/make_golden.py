@@ -28,6 +28,8 @@ FIXTURES = {
     "HomogeneousElasticDomainStaceyBC": ("BXX", "BXZ"),
     "HomogeneousAcousticDomainDirichletBC": ("BXX", "BXZ"),
     "AcousticElasticCoupledDomainVariant2": ("BXX", "BXZ"),
+    "HomogeneousElasticDomainMomentTensor": ("BXX", "BXZ"),
+    "HomogeneousElasticIsotropicDomainSH": ("BXY",),
 }
 
 
@@ -35,24 +37,31 @@ def make(ref_root: str, name: str, comps) -> str:
     d = os.path.join(ref_root, "tests/unit-tests/displacement_tests/Newmark/serial/dim2", name)
     case = runner.load_fixture(d)
     m = case.mesh
-    traces = np.zeros((len(case.stations), len(comps), case.nstep), np.float32)
+    traces = {}
     t0 = None
-    for r, (net, sta) in enumerate(case.stations):
-        for c, comp in enumerate(comps):
-            t, v = runner.read_trace(os.path.join(d, "traces", f"{net}.{sta}.S2.{comp}.semd"))
-            traces[r, c, : len(v)] = v[: case.nstep]
-            t0 = t[0]
+    for ext in ("semd", "semv", "sema"):
+        if not os.path.exists(os.path.join(d, "traces", f"{case.stations[0][0]}.{case.stations[0][1]}.S2.{comps[0]}.{ext}")):
+            continue
+        tr = np.zeros((len(case.stations), len(comps), case.nstep), np.float32)
+        for r, (net, sta) in enumerate(case.stations):
+            for c, comp in enumerate(comps):
+                t, v = runner.read_trace(os.path.join(d, "traces", f"{net}.{sta}.S2.{comp}.{ext}"))
+                tr[r, c, : len(v)] = v[: case.nstep]
+                t0 = t[0]
+        traces[ext] = tr
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(
         out, nspec=m.nspec, npgeo=m.npgeo, ngnod=m.ngnod, coorg=m.coorg, knods=m.knods,
         kmato=m.kmato, mat_medium=m.mat_medium, mat_rho=m.mat_rho, mat_vp=m.mat_vp,
         mat_vs=m.mat_vs, abs_ispec=m.abs_ispec, abs_type=m.abs_type, free_ispec=m.free_ispec,
         free_type=m.free_type,
-        src=np.asarray([[s.x, s.z, s.f0, s.factor, s.tshift, s.angle, 1.0 if s.stf == "dirac" else 0.0]
+        src=np.asarray([[s.x, s.z, s.f0, s.factor, s.tshift, s.angle, 1.0 if s.stf == "dirac" else 0.0,
+                         1.0 if s.kind == "moment_tensor" else 0.0, s.mxx, s.mzz, s.mxz]
                         for s in case.sources]),
         rec_x=case.rec_x, rec_z=case.rec_z, dt=case.dt, nstep=case.nstep, rec_angle=case.rec_angle,
-        stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces,
-        trace_t0=t0, components=np.asarray(comps))
+        stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces["semd"],
+        **{f"traces_{k}": v for k, v in traces.items() if k != "semd"},
+        trace_t0=t0, components=np.asarray(comps), elastic_sh=int(case.elastic_sh))
     return out
 
 

@@ -19,7 +19,8 @@ pytestmark = pytest.mark.gpu
 
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
-            "AcousticElasticCoupledDomainVariant2"]
+            "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
+            "HomogeneousElasticIsotropicDomainSH"]
 
 
 def tolerance(kind, f32, f64):
@@ -160,3 +161,24 @@ def test_owner_computes_variants_equal_colour_passes(sfg_lib, name, variant):
     _, a = product_run(case, epb=16, variant=1)
     _, b = product_run(case, epb=8, variant=variant)
     assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
+
+
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH"])
+def test_moment_tensor_and_sh_all_types(sfg_lib, oracle_lib, name):
+    """Moment-tensor source (P-SV) and SH: displacement, velocity and
+    acceleration against the oracle (tolerances above) and against the
+    reference's golden traces (sum|d|/sum|ref| < 1e-3)."""
+    import os
+    from conftest import GOLDEN
+    from oracle import runner
+    case, _, _ = golden_case(name)
+    z = np.load(os.path.join(GOLDEN, f"{name}.npz"))
+    types = ("displacement", "velocity", "acceleration")
+    case.seis_types = list(types)
+    ref = runner.run(case, "f32", nthreads=1)["seis"]
+    ref64 = runner.run(case, "f64", nthreads=8)["seis"]
+    _, seis = product_run(case, types=types)
+    for t, (kind, key) in enumerate(zip(types, ("traces", "traces_semv", "traces_sema"))):
+        tol = 1e-5 if kind == "displacement" else tolerance(kind, ref[:, t], ref64[:, t])
+        assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
+        assert reference_metric(seis[:, t], z[key]).max() < 1e-3, kind

@@ -16,7 +16,8 @@ from conftest import golden_case, reference_metric
 
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
-            "AcousticElasticCoupledDomainVariant2"]
+            "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
+            "HomogeneousElasticIsotropicDomainSH"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -29,6 +30,23 @@ def test_oracle_matches_golden_traces(oracle_lib, name):
     assert np.all(np.isfinite(err))
     assert err.max() < 1e-3, err                          # the reference's tolerance
     assert err.max() < 5e-4                               # observed margin: <= 2e-4
+
+
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH"])
+@pytest.mark.parametrize("kind,key", [("velocity", "traces_semv"), ("acceleration", "traces_sema")])
+def test_oracle_matches_golden_velocity_acceleration(oracle_lib, name, kind, key):
+    """Velocity and acceleration traces of the moment-tensor (P-SV) and SH
+    fixtures, same metric and tolerance as the displacement traces."""
+    import os
+    from conftest import GOLDEN
+    from oracle import runner
+    case, _, _ = golden_case(name)
+    traces = np.load(os.path.join(GOLDEN, f"{name}.npz"))[key]
+    case.seis_types = [kind]
+    r = runner.run(case, "f32", nthreads=8)
+    err = reference_metric(r["seis"][:, 0], traces)
+    assert np.all(np.isfinite(err))
+    assert err.max() < 1e-3, err
 
 
 def test_oracle_fp32_vs_fp64_small(oracle_lib):
