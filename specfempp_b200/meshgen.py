@@ -342,3 +342,118 @@ def smooth_perturbations(mesh: Mesh, xmax: float, zmax: float, n: int, margin: f
             r = rng.uniform(300.0, 800.0)
             out[i] += rng.choice([-1.0, 1.0]) * np.exp(-((gx - x0) ** 2 + (gz - z0) ** 2) / r ** 2)
     return out
+
+
+# ------------------------------------------------------------------- 3D ---
+
+@dataclass
+class Mesh3D:
+    """Structured lattice of 8-node hexahedra: element e = (ez*ney + ey)*nex + ex,
+    control node (i, j, k) at nodes[(k*(ney+1) + j)*(nex+1) + i] = (x, y, z);
+    per-GLL-point model [nspec, 125] (point q = (iz*5 + iy)*5 + ix);
+    absorbing: Stacey on faces (xmin, xmax, ymin, ymax, zmin, zmax)."""
+    nex: int
+    ney: int
+    nez: int
+    nodes: np.ndarray
+    rho: np.ndarray
+    vp: np.ndarray
+    vs: np.ndarray
+    absorbing: tuple = (0, 0, 0, 0, 0, 0)
+
+    @property
+    def nspec(self):
+        return self.nex * self.ney * self.nez
+
+    @property
+    def nglob(self):
+        return (4 * self.nex + 1) * (4 * self.ney + 1) * (4 * self.nez + 1)
+
+
+def hex_lattice(nex, ney, nez, x0, x1, y0, y1, z0, z1) -> np.ndarray:
+    xs = np.linspace(x0, x1, nex + 1)
+    ys = np.linspace(y0, y1, ney + 1)
+    zs = np.linspace(z0, z1, nez + 1)
+    Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+    return np.stack([X, Y, Z], -1).reshape(-1, 3)
+
+
+def gll_coordinates3d(mesh: Mesh3D):
+    """(x, y, z) of every element GLL point, each [nspec, 125], for the trilinear map."""
+    r = np.sqrt(3.0 / 7.0)
+    z1 = np.array([-1.0, -r, 0.0, r, 1.0])
+    G, E, X = np.meshgrid(z1, z1, z1, indexing="ij")     # [iz, iy, ix]
+    cs = np.array([[-1, -1, -1], [1, -1, -1], [1, 1, -1], [-1, 1, -1],
+                   [-1, -1, 1], [1, -1, 1], [1, 1, 1], [-1, 1, 1]], float)
+    N = np.stack([0.125 * (1 + c[0] * X) * (1 + c[1] * E) * (1 + c[2] * G) for c in cs], -1).reshape(125, 8)
+    e = np.arange(mesh.nspec)
+    ex, ey, ez = e % mesh.nex, (e // mesh.nex) % mesh.ney, e // (mesh.nex * mesh.ney)
+    idx = np.stack([((ez + (c[2] > 0)) * (mesh.ney + 1) + ey + (c[1] > 0)) * (mesh.nex + 1) + ex + (c[0] > 0)
+                    for c in cs], -1)                    # [nspec, 8]
+    P = mesh.nodes[idx]                                  # [nspec, 8, 3]
+    return tuple(P[:, :, k] @ N.T for k in range(3))
+
+
+def homogeneous_hex_mesh(nex, ney, nez, extent, rho, vp, vs, absorbing=(0, 0, 0, 0, 0, 0)) -> Mesh3D:
+    x0, x1, y0, y1, z0, z1 = extent
+    nodes = hex_lattice(nex, ney, nez, x0, x1, y0, y1, z0, z1)
+    n = nex * ney * nez
+    one = np.ones((n, 125))
+    return Mesh3D(nex, ney, nez, nodes, rho * one, vp * one, vs * one, tuple(absorbing))
+
+
+@dataclass
+class Workload3D:
+    name: str
+    mesh: Mesh3D
+    sources: list       # oracle.runner3d.Source3D-like objects (x, y, z, f0, factor, kind, comp, tshift)
+    rec_xyz: np.ndarray
+    dt: float
+    nstep: int
+    description: str = ""
+
+
+@dataclass
+class Source3D:
+    x: float
+    y: float
+    z: float
+    f0: float
+    factor: float
+    kind: str = "force"
+    comp: tuple = (0.0, 0.0, 0.0, 0.0, 0.0, 0.0)
+    tshift: float = 0.0
+
+
+def elastic3d_layered_grf(nex=128, ney=128, nez=64, nstep=5000, nrec=1000, seed=0, grf=True) -> Workload3D:
+    """Hexahedral mesh over 64 x 64 x 32 km (h = 500 m at 128 x 128 x 64): a 1D
+    layered background (vp 4.0 to 6.5 km/s with depth, vs = vp/1.73,
+    rho = 1700 + 0.2 vp) times (1 + 0.05 GRF(corr. 4 km)); free surface on top
+    (z = 0), Stacey on the other five faces; a seeded moment tensor with a
+    Ricker of 1 Hz at 10 km depth; nrec receivers on the surface; dt = 2 ms."""
+    rng = np.random.default_rng(seed)
+    X, Y, Z = 64000.0 * nex / 128, 64000.0 * ney / 128, 32000.0 * nez / 64
+    nodes = hex_lattice(nex, ney, nez, 0.0, X, 0.0, Y, -Z, 0.0)
+    m = Mesh3D(nex, ney, nez, nodes, None, None, None, (1, 1, 1, 1, 1, 0))
+    gx, gy, gz = gll_coordinates3d(m)
+    depth = -gz
+    vp = np.interp(depth, [0.0, 3000.0, 12000.0, 20000.0, 32000.0], [4000.0, 4800.0, 5800.0, 6300.0, 6500.0])
+    if grf:
+        ng = (max(16, nez), max(16, ney), max(16, nex))
+        f = gaussian_random_field(ng, max(X, Y, Z) / max(ng), 4000.0, rng)
+        iz = np.clip((depth / Z * (ng[0] - 1)).round().astype(int), 0, ng[0] - 1)
+        iy = np.clip((gy / Y * (ng[1] - 1)).round().astype(int), 0, ng[1] - 1)
+        ix = np.clip((gx / X * (ng[2] - 1)).round().astype(int), 0, ng[2] - 1)
+        vp = vp * (1.0 + 0.05 * f[iz, iy, ix])
+    m.vp = vp
+    m.vs = vp / 1.73
+    m.rho = 1700.0 + 0.2 * vp
+    M = rng.standard_normal(6)
+    src = [Source3D(0.5 * X + rng.uniform(-0.1, 0.1) * X, 0.5 * Y + rng.uniform(-0.1, 0.1) * Y, -10000.0 * nez / 64,
+                    1.0, 1e15, "moment_tensor", tuple(float(c) for c in M))]
+    rx = rng.uniform(0.05 * X, 0.95 * X, nrec)
+    ry = rng.uniform(0.05 * Y, 0.95 * Y, nrec)
+    rec = np.stack([rx, ry, np.zeros(nrec)], -1)
+    return Workload3D(f"elastic3d_{nex}x{ney}x{nez}", m, src, rec, 2e-3, nstep,
+                      description=f"3D elastic {nex}x{ney}x{nez} hexes, layered + 5% GRF, moment tensor 1 Hz, "
+                                  f"{nrec} surface receivers, free top + Stacey")

@@ -65,7 +65,61 @@ def make(ref_root: str, name: str, comps) -> str:
     return out
 
 
+FIXTURE_3D = "HomogeneousHalfspaceSmallNoABCForceSource"
+
+
+def make3d(ref_root: str) -> str:
+    """The 3D fixture: a regular 8 x 6 x 6 hexahedral mesh over 8 x 7 x 7.5 km
+    (NEX_XI, NEX_ETA, depth and the single region of its Mesh_Par_file), one
+    homogeneous material, no absorbing boundary; stations in the 3D format
+    (station, network, y, x, elevation, z)."""
+    import yaml
+    d = os.path.join(ref_root, "tests/unit-tests/displacement_tests/Newmark/serial/dim3", FIXTURE_3D)
+    with open(os.path.join(d, "specfem_config.yaml")) as f:
+        cfg = yaml.safe_load(f)["parameters"]
+    ts = cfg["simulation-setup"]["solver"]["time-marching"]["time-scheme"]
+    with open(os.path.join(d, "force.yaml")) as f:
+        src = yaml.safe_load(f)["sources"][0]["force"]
+    mat = None
+    with open(os.path.join(d, "provenance", "specfempp", "Mesh_Par_file")) as f:
+        lines = [ln.split("#")[0].strip() for ln in f]
+    for i, ln in enumerate(lines):
+        if ln.startswith("NMATERIALS"):
+            nxt = next(x for x in lines[i + 1:] if x)             # first line after the comments
+            mat = [float(v) for v in nxt.split()[1:4]]            # rho vp vs
+    names, xyz = [], []
+    with open(os.path.join(d, "STATIONS")) as f:
+        for ln in f:
+            p = ln.split()
+            if len(p) >= 6:
+                names.append(f"{p[1]}.{p[0]}")
+                xyz.append([float(p[3]), float(p[2]), float(p[5])])
+    nstep = int(ts["nstep"])
+    traces = {}
+    t0 = None
+    for ext in ("semd", "semv", "sema"):
+        tr = np.zeros((len(names), 3, nstep), np.float32)
+        for r, nm in enumerate(names):
+            for c, comp in enumerate(("BXX", "BXY", "BXZ")):
+                t, v = runner.read_trace(os.path.join(d, "traces", f"{nm}.S3.{comp}.{ext}"))
+                tr[r, c, : len(v)] = v[:nstep]
+                t0 = t[0]
+        traces[ext] = tr
+    rk = src["Ricker"]
+    out = os.path.join(HERE, f"{FIXTURE_3D}.npz")
+    np.savez_compressed(out, nex=8, ney=6, nez=6, extent=np.array([0.0, 8000.0, 0.0, 7000.0, -7500.0, 0.0]),
+                        material=np.array(mat), src_xyz=np.array([src["x"], src["y"], src["z"]], float),
+                        src_force=np.array([src["fx"], src["fy"], src["fz"]], float),
+                        src_f0=float(rk["f0"]), src_factor=float(rk["factor"]), src_tshift=float(rk["tshift"]),
+                        dt=float(ts["dt"]), nstep=nstep, rec_xyz=np.array(xyz), stations=np.array(names),
+                        traces_semd=traces["semd"], traces_semv=traces["semv"], traces_sema=traces["sema"],
+                        trace_t0=t0)
+    return out
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     for name, comps in FIXTURES.items():
         print(make(root, name, comps), os.path.getsize(os.path.join(HERE, f"{name}.npz")))
+    out = make3d(root)
+    print(out, os.path.getsize(out))

@@ -85,3 +85,43 @@ def test_stress_known_answer(oracle_lib):
     oracle_lib.oracle_stress_psv(kappa, mu, du.ctypes.data_as(dp), out.ctypes.data_as(dp))
     lam = kappa + 4.0 / 3.0 * mu - 2 * mu
     assert np.allclose(out, [(lam + 2 * mu) * 1 + lam * 2, mu * 7, mu * 7, (lam + 2 * mu) * 2 + lam * 1])
+
+
+def golden3d_case(kind="displacement", nstep=None):
+    """The 3D fixture (regular 8 x 6 x 6 hexahedra, force source) as an oracle Case3D."""
+    import os
+    from conftest import GOLDEN
+    from oracle import runner3d
+    from specfempp_b200 import meshgen
+    z = np.load(os.path.join(GOLDEN, "HomogeneousHalfspaceSmallNoABCForceSource.npz"))
+    rho, vp, vs = z["material"]
+    m = meshgen.homogeneous_hex_mesh(int(z["nex"]), int(z["ney"]), int(z["nez"]), z["extent"], rho, vp, vs)
+    fx, fy, fz = z["src_force"]
+    src = [runner3d.Source3D(*z["src_xyz"], f0=float(z["src_f0"]), factor=float(z["src_factor"]),
+                             comp=(fx, fy, fz, 0.0, 0.0, 0.0), tshift=float(z["src_tshift"]))]
+    case = runner3d.Case3D(m, src, z["rec_xyz"], float(z["dt"]), int(nstep or z["nstep"]), [kind])
+    return case, z
+
+
+@pytest.mark.parametrize("kind,key", [("displacement", "traces_semd"), ("velocity", "traces_semv"),
+                                      ("acceleration", "traces_sema")])
+def test_oracle3d_matches_golden_traces(oracle_lib, kind, key):
+    """3D elastic (SPECFEM3D Fortran traces of the reference's dim3 Newmark
+    fixture): sum|d|/sum|ref| per station < 1e-3 (observed <= 7e-5)."""
+    from oracle import runner3d
+    case, z = golden3d_case(kind)
+    r = runner3d.run(case, "f32", nthreads=8)
+    assert abs(r["t0"] - float(z["trace_t0"])) < 1e-6
+    seis = np.transpose(r["seis"][:, 0], (1, 2, 0))     # [nrec, 3, nstep]
+    tr = z[key]
+    err = np.abs(seis - tr).sum(axis=(1, 2)) / np.abs(tr).sum(axis=(1, 2))
+    assert err.max() < 1e-3, err
+    assert err.max() < 2e-4
+
+
+def test_oracle3d_fp32_vs_fp64(oracle_lib):
+    from oracle import runner3d
+    case, _ = golden3d_case()
+    a = runner3d.run(case, "f32", nthreads=4)["seis"]
+    b = runner3d.run(case, "f64", nthreads=4)["seis"]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
