@@ -7,13 +7,13 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
-SOURCES = ["csrc/sfg.cu", "csrc/host2d.cpp"]
-HEADERS = ["csrc/kernels2d.cuh", "csrc/kernels2d_batched.cuh", "csrc/kernels2d_adjoint.cuh", "csrc/kernels2d_tma.cuh", "csrc/host2d.hpp", "../include/sfg.h"]
+SOURCES = ["csrc/sfg.cu", "csrc/sfg3d.cu", "csrc/host2d.cpp"]
+HEADERS = ["csrc/kernels2d.cuh", "csrc/kernels2d_batched.cuh", "csrc/kernels2d_adjoint.cuh", "csrc/kernels2d_tma.cuh", "csrc/kernels3d.cuh", "csrc/host2d.hpp", "../include/sfg.h", "../include/sfg3d.h"]
 # -fmad=false: products and sums are rounded separately unless a kernel asks
 # for an FMA explicitly, so every launch shape of a kernel (and the CPU oracle,
 # built with contraction off) performs the same rounding steps.
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
-              "-fmad=false", "-Xcompiler", "-fPIC,-O3", "-shared"]
+              "-fmad=false", "-Xcompiler", "-fPIC,-O3,-fopenmp", "-shared", "-lgomp"]
 
 
 def nvcc() -> str:

@@ -1,0 +1,254 @@
+// sm_100a kernels of the 3D elastic spectral-element time step (FP32).
+//
+// One step: [element kernel] -> [receivers] -> [point update].
+// * Element kernel: one thread per element GLL point (125 per element), E
+//   elements per block.  The displacement gathered at the 125 points goes to
+//   shared memory; the three 5-term Lagrange-derivative contractions per
+//   component (include/algorithms/gradient.hpp:103-156), the map to physical
+//   derivatives, the isotropic stress (include/medium/dim3/elastic/isotropic/
+//   stress.hpp:46-99) and F = |J| sigma . grad(xi_k) (core/specfem/point/
+//   stress.hpp:217-240) run in registers; F goes through shared memory for the
+//   divergence with its pairwise weight products (include/algorithms/
+//   divergence.hpp:90-137).  The epilogue applies the absorbing-face traction
+//   -C v (C: per element point, the symmetric 3x3 sum over the element's
+//   absorbing faces at that point, precomputed) and point sources, and stores
+//   the element point's contribution at its point-major slot (owner-computes
+//   assembly: the update sums each point's contributions in element order).
+// * Point update: a = (sum of contributions) M^-1, Newmark corrector, and the
+//   next step's predictor fused in (newmark.tpp:10-128); the last step of a
+//   run stops after the corrector.
+// * Receivers: one block per receiver, Lagrange interpolation of the chosen
+//   field with a fixed-order tree sum.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sfg3 {
+namespace dev {
+
+constexpr int NG = 5;
+constexpr int NQ = 125;
+
+__constant__ float c3_hp[NG * NG];    // hp[i*5+j] = l'_j(xi_i)
+__constant__ float c3_hpw[NG * NG];   // hp[l*5+i] * w[l]
+__constant__ float c3_w[NG];
+
+struct Elem3Args {
+  const int *__restrict__ ibool;      // [nspec][125] lattice point
+  const float *__restrict__ g9;       // [9][nspec*125] d xi_k / d x_j, k-major
+  const float *__restrict__ jac;      // [nspec*125]
+  const float *__restrict__ c0, *__restrict__ mu;   // lambda + 2 mu, mu
+  const int *__restrict__ slot;       // point-major position of each element point
+  const int *__restrict__ bc_slot;    // [nspec]: absorbing data slot or -1
+  const float *__restrict__ bc_c;     // [slot][6][125]: C xx yy zz xy xz yz
+  const int *__restrict__ src_head, *__restrict__ src_next;
+  const float *__restrict__ src_arr;  // [nsrc][3][125]
+  const float *__restrict__ stf;      // [nstep][nsrc]
+  int nsrc, nstep;
+  const int *__restrict__ step;
+  const float *__restrict__ u, *__restrict__ v;   // [nglob][3]
+  float *__restrict__ r;              // [slot][3]
+  int nspec;
+  size_t nloc;
+};
+
+template <int E>
+__global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
+  __shared__ float su[E][3][NQ];
+  __shared__ float sF[E][3][3][NQ];
+  const int tid = threadIdx.x;
+  const int le = tid / NQ, q = tid - le * NQ;
+  const int e = blockIdx.x * E + le;
+  const bool act = e < A.nspec;
+  const size_t p = size_t(act ? e : 0) * NQ + q;
+  const int ix = q % NG, iy = (q / NG) % NG, iz = q / (NG * NG);
+  const int g = act ? __ldg(A.ibool + p) : 0;
+  float gi[9];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) gi[k] = __ldg(A.g9 + size_t(k) * A.nloc + p);
+  const float jac = __ldg(A.jac + p), c0 = __ldg(A.c0 + p), mu = __ldg(A.mu + p);
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  const int src = act ? __ldg(A.src_head + e) : -1;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) su[le][c][q] = act ? A.u[size_t(g) * 3 + c] : 0.f;
+  __syncthreads();
+  float du[3][3];  // du[c][j] = d u_c / d x_j
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      d0 = fmaf(c3_hp[ix * NG + l], su[le][c][(iz * NG + iy) * NG + l], d0);
+      d1 = fmaf(c3_hp[iy * NG + l], su[le][c][(iz * NG + l) * NG + ix], d1);
+      d2 = fmaf(c3_hp[iz * NG + l], su[le][c][(l * NG + iy) * NG + ix], d2);
+    }
+#pragma unroll
+    for (int j = 0; j < 3; ++j) du[c][j] = d0 * gi[0 * 3 + j] + d1 * gi[1 * 3 + j] + d2 * gi[2 * 3 + j];
+  }
+  const float lam = c0 - 2.f * mu;
+  float sig[3][3];
+  sig[0][0] = c0 * du[0][0] + lam * (du[1][1] + du[2][2]);
+  sig[1][1] = c0 * du[1][1] + lam * (du[0][0] + du[2][2]);
+  sig[2][2] = c0 * du[2][2] + lam * (du[0][0] + du[1][1]);
+  sig[0][1] = sig[1][0] = mu * (du[0][1] + du[1][0]);
+  sig[0][2] = sig[2][0] = mu * (du[0][2] + du[2][0]);
+  sig[1][2] = sig[2][1] = mu * (du[1][2] + du[2][1]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+      sF[le][c][k][q] = jac * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
+  __syncthreads();
+  if (!act) return;
+  float a[3];
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float t1 = 0.f, t2 = 0.f, t3 = 0.f;
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      t1 = fmaf(sF[le][c][0][(iz * NG + iy) * NG + l], c3_hpw[l * NG + ix], t1);
+      t2 = fmaf(sF[le][c][1][(iz * NG + l) * NG + ix], c3_hpw[l * NG + iy], t2);
+      t3 = fmaf(sF[le][c][2][(l * NG + iy) * NG + ix], c3_hpw[l * NG + iz], t3);
+    }
+    a[c] = -(c3_w[iz] * c3_w[iy] * t1 + c3_w[iz] * c3_w[ix] * t2 + c3_w[iy] * c3_w[ix] * t3);
+  }
+  if (bs >= 0) {
+    const float *C = A.bc_c + size_t(bs) * 6 * NQ + q;
+    const float cxx = C[0], cyy = C[NQ], czz = C[2 * NQ], cxy = C[3 * NQ], cxz = C[4 * NQ], cyz = C[5 * NQ];
+    if (cxx != 0.f || cyy != 0.f || czz != 0.f) {
+      const float vx = A.v[size_t(g) * 3], vy = A.v[size_t(g) * 3 + 1], vz = A.v[size_t(g) * 3 + 2];
+      a[0] -= cxx * vx + cxy * vy + cxz * vz;
+      a[1] -= cxy * vx + cyy * vy + cyz * vz;
+      a[2] -= cxz * vx + cyz * vy + czz * vz;
+    }
+  }
+  if (src >= 0) {
+    const int step = *A.step;
+    for (int s = src; s >= 0; s = A.src_next[s]) {
+      const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) a[c] += f * A.src_arr[(size_t(s) * 3 + c) * NQ + q];
+    }
+  }
+  const size_t sl = size_t(__ldg(A.slot + p)) * 3;
+  A.r[sl] = a[0];
+  A.r[sl + 1] = a[1];
+  A.r[sl + 2] = a[2];
+}
+
+struct Update3Args {
+  float *__restrict__ u, *__restrict__ v, *__restrict__ a_store;
+  const float *__restrict__ minv;
+  const int *__restrict__ inv_start;
+  const float *__restrict__ r;
+  int npts;
+  float dt, dt2, dtsq2;
+  int predict;
+  int *flag;
+  int *step;
+  int advance;
+};
+
+__device__ __forceinline__ void nm_predict(float &u, float &v, float a, float dt, float dt2, float dtsq2) {
+  u = __fadd_rn(u, __fadd_rn(__fmul_rn(dt, v), __fmul_rn(dtsq2, a)));
+  v = __fadd_rn(v, __fmul_rn(dt2, a));
+}
+
+__global__ void __launch_bounds__(256) k_update3d(Update3Args A) {
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < A.npts; g += stride) {
+    float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+    const int k1 = A.inv_start[g + 1];
+    for (int k = A.inv_start[g]; k < k1; ++k) {
+      s0 = s0 + A.r[size_t(k) * 3];
+      s1 = s1 + A.r[size_t(k) * 3 + 1];
+      s2 = s2 + A.r[size_t(k) * 3 + 2];
+    }
+    const float acc[3] = {s0, s1, s2};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const size_t i = size_t(g) * 3 + c;
+      const float a = __fmul_rn(acc[c], A.minv[i]);
+      float vv = __fadd_rn(A.v[i], __fmul_rn(A.dt2, a));
+      float uu = A.u[i];
+      if (A.predict) nm_predict(uu, vv, a, A.dt, A.dt2, A.dtsq2);
+      if (A.predict) A.u[i] = uu;
+      A.v[i] = vv;
+      if (A.a_store) A.a_store[i] = a;
+      bad |= !isfinite(uu);
+    }
+  }
+  if (bad) *A.flag = 1;
+  if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
+__global__ void __launch_bounds__(256) k_predict3d(float *__restrict__ u, float *__restrict__ v,
+                                                   const float *__restrict__ a, size_t n, float dt, float dt2,
+                                                   float dtsq2) {
+  for (size_t i = blockIdx.x * size_t(blockDim.x) + threadIdx.x; i < n; i += size_t(gridDim.x) * blockDim.x) {
+    float uu = u[i], vv = v[i];
+    nm_predict(uu, vv, a[i], dt, dt2, dtsq2);
+    u[i] = uu;
+    v[i] = vv;
+  }
+}
+
+struct Rec3Args {
+  const int *__restrict__ ibool;
+  const int *__restrict__ rec_elem;
+  const float *__restrict__ rec_h;    // [nrec][125]
+  const int *__restrict__ types;      // per type: 0 displacement, 1 velocity, 2 acceleration
+  int ntypes, nrec, nsig;
+  const float *__restrict__ u, *__restrict__ v;
+  // acceleration of the step: the update's input (sum of contributions x M^-1)
+  const float *__restrict__ minv, *__restrict__ r;
+  const int *__restrict__ inv_start;
+  float dt2;
+  const int *__restrict__ step;
+  float *__restrict__ seis;           // [nsig][ntypes][nrec][3]
+};
+
+// One block of 128 threads per receiver; run before the update of the step
+// (velocity and acceleration are formed from the step's contributions the
+// same way the update forms them).
+__global__ void __launch_bounds__(128) k_receivers3d(Rec3Args A) {
+  __shared__ float red[3][128];
+  const int rr = blockIdx.x, q = threadIdx.x;
+  const int step = *A.step;
+  if (step >= A.nsig) return;
+  const int e = A.rec_elem[rr];
+  for (int t = 0; t < A.ntypes; ++t) {
+    float val[3] = {0.f, 0.f, 0.f};
+    if (q < NQ) {
+      const int g = A.ibool[size_t(e) * NQ + q];
+      const float h = A.rec_h[size_t(rr) * NQ + q];
+      float f[3];
+      if (A.types[t] == 0) {
+        for (int c = 0; c < 3; ++c) f[c] = A.u[size_t(g) * 3 + c];
+      } else {
+        float s[3] = {0.f, 0.f, 0.f};
+        for (int k = A.inv_start[g]; k < A.inv_start[g + 1]; ++k)
+          for (int c = 0; c < 3; ++c) s[c] = s[c] + A.r[size_t(k) * 3 + c];
+        for (int c = 0; c < 3; ++c) {
+          const float acc = __fmul_rn(s[c], A.minv[size_t(g) * 3 + c]);
+          f[c] = A.types[t] == 2 ? acc : __fadd_rn(A.v[size_t(g) * 3 + c], __fmul_rn(A.dt2, acc));
+        }
+      }
+      for (int c = 0; c < 3; ++c) val[c] = h * f[c];
+    }
+    for (int c = 0; c < 3; ++c) red[c][q] = val[c];
+    __syncthreads();
+    for (int o = 64; o > 0; o >>= 1) {
+      if (q < o)
+        for (int c = 0; c < 3; ++c) red[c][q] = red[c][q] + red[c][q + o];
+      __syncthreads();
+    }
+    if (q < 3) A.seis[((size_t(step) * A.ntypes + t) * A.nrec + rr) * 3 + q] = red[q][0];
+    __syncthreads();
+  }
+}
+
+}  // namespace dev
+}  // namespace sfg3

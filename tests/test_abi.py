@@ -96,3 +96,25 @@ def test_error_paths(tmp_path, sfg_lib):
     assert e.value.code == -5
     with pytest.raises(sfg.SfgError):
         sfg.Simulation2D(w.mesh, dt=-1.0, nstep=10)
+
+
+def test_library_exports_every_declared_3d_symbol(sfg_lib):
+    text = open(os.path.join(ROOT, "include", "sfg3d.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    syms = sorted(set(re.findall(r"\b(sfg3d_[a-z0-9_]+)\s*\(", text)))
+    assert len(syms) >= 14
+    for s in syms:
+        assert hasattr(sfg_lib, s), s
+    from specfempp_b200 import sfg3d
+    assert set(syms) == set(sfg3d.EXPORTS3D)
+
+
+def test_3d_create_errors(sfg_lib):
+    """Argument checks of the 3D interface that need no GPU."""
+    from specfempp_b200 import meshgen, sfg, sfg3d
+    m = meshgen.homogeneous_hex_mesh(2, 2, 2, (0, 1000, 0, 1000, -1000, 0), 2700.0, 3000.0, 1732.0)
+    with pytest.raises(sfg.SfgError):
+        sfg3d.Simulation3D(m, dt=-1.0, nstep=10)
+    bad = meshgen.homogeneous_hex_mesh(2, 2, 2, (0, 1000, 0, 1000, -1000, 0), 2700.0, 1000.0, 1732.0)
+    with pytest.raises(sfg.SfgError):
+        sfg3d.Simulation3D(bad, dt=1e-3, nstep=10)

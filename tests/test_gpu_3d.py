@@ -1,0 +1,105 @@
+"""3D elastic CUDA path against the 3D oracle and the reference's dim3 golden
+traces.
+
+Tolerances: displacement relative L2 <= 1e-5 against the oracle FP32;
+velocity and acceleration max(1e-5, 2 x the oracle's FP32-vs-FP64 gap);
+golden traces sum|d|/sum|ref| < 1e-3 per station.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+from test_oracle import golden3d_case
+
+pytestmark = pytest.mark.gpu
+
+TYPES = ("displacement", "velocity", "acceleration")
+
+
+def product3d(case, epb=0, types=TYPES):
+    from specfempp_b200 import sfg3d
+    sim = sfg3d.Simulation3D(case.mesh, dt=case.dt, nstep=case.nstep, elements_per_block=epb)
+    sim.set_sources(case.sources)
+    sim.set_receivers(case.rec_xyz, types=types)
+    sim.initialize()
+    sim.run(case.nstep)
+    return sim, sim.seismograms()
+
+
+def tol(kind, f32, f64):
+    return 1e-5 if kind == "displacement" else max(1e-5, 2.0 * rel_l2(f32, f64))
+
+
+def test_3d_golden_fixture(sfg_lib, oracle_lib):
+    from oracle import runner3d
+    case, z = golden3d_case()
+    case.seis_types = list(TYPES)
+    ref = runner3d.run(case, "f32", nthreads=8)["seis"]
+    ref64 = runner3d.run(case, "f64", nthreads=8)["seis"]
+    sim, seis = product3d(case)
+    assert sim.check_finite()
+    for t, (kind, key) in enumerate(zip(TYPES, ("traces_semd", "traces_semv", "traces_sema"))):
+        assert rel_l2(seis[:, t], ref[:, t]) <= tol(kind, ref[:, t], ref64[:, t]), (kind, rel_l2(seis[:, t], ref[:, t]))
+        c = np.transpose(seis[:, t], (1, 2, 0))
+        tr = z[key]
+        err = np.abs(c - tr).sum(axis=(1, 2)) / np.abs(tr).sum(axis=(1, 2))
+        assert err.max() < 1e-3, (kind, err.max())
+
+
+def small_absorbing_case(nstep=300):
+    from oracle import runner3d
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic3d_layered_grf(nex=10, ney=8, nez=6, nstep=nstep, nrec=12, seed=3)
+    s = w.sources[0]
+    src = [runner3d.Source3D(s.x, s.y, s.z, f0=4.0, factor=1e13, kind=s.kind, comp=s.comp),
+           runner3d.Source3D(0.3 * 5000, 0.6 * 4000, -1500.0, f0=3.0, factor=1e12, kind="force",
+                             comp=(0.3, -0.5, 1.0, 0, 0, 0), tshift=0.05)]
+    return runner3d.Case3D(w.mesh, src, w.rec_xyz, 2e-3, nstep, list(TYPES))
+
+
+def test_3d_absorbing_moment_tensor_vs_oracle(sfg_lib, oracle_lib):
+    """Layered GRF model, Stacey on five faces, free top, a moment tensor and
+    a force source with a time shift: all three seismogram types and the final
+    displacement field against the oracle."""
+    from oracle import runner3d
+    case = small_absorbing_case()
+    r = runner3d.run(case, "f32", nthreads=8, want_final=True)
+    r64 = runner3d.run(case, "f64", nthreads=8)
+    sim, seis = product3d(case, epb=2)
+    assert np.abs(r["seis"]).max() > 0
+    for t, kind in enumerate(TYPES):
+        assert rel_l2(seis[:, t], r["seis"][:, t]) <= tol(kind, r["seis"][:, t], r64["seis"][:, t]), kind
+    assert rel_l2(sim.field("displacement"), r["final"]) <= 1e-5
+
+
+def test_3d_launch_shapes_agree_and_deterministic(sfg_lib):
+    case = small_absorbing_case(nstep=120)
+    _, a = product3d(case, epb=1)
+    _, b = product3d(case, epb=4)
+    sim, c = product3d(case, epb=2)
+    assert np.array_equal(a, b) and np.array_equal(a, c)
+    sim.reset()
+    sim.run(case.nstep)
+    assert np.array_equal(sim.seismograms(), c)
+
+
+def test_3d_absorbing_energy_decays(sfg_lib):
+    """Absorbing faces take the (resolved, 1 Hz) wavefield out of the model:
+    late-time receiver energy falls below 1e-3 of its peak and far below the
+    same run with free faces everywhere."""
+    from specfempp_b200 import meshgen, sfg3d
+    from oracle import runner3d
+    late = {}
+    for absorb in (0, 1):
+        m = meshgen.homogeneous_hex_mesh(8, 8, 8, (0, 4000, 0, 4000, -4000, 0), 2500.0, 3000.0, 1732.0,
+                                         absorbing=(absorb,) * 6)
+        src = [runner3d.Source3D(2000.0, 2000.0, -2000.0, f0=1.0, factor=1e12, comp=(0, 0, 1.0, 0, 0, 0))]
+        sim = sfg3d.Simulation3D(m, dt=4e-3, nstep=1500)
+        sim.set_sources(src)
+        sim.set_receivers(np.array([[2000.0, 2000.0, -1000.0], [500.0, 500.0, -500.0]]), types=("velocity",))
+        sim.initialize()
+        sim.run(1500)
+        e = (sim.seismograms()[:, 0].astype(np.float64) ** 2).sum(axis=(1, 2))
+        late[absorb] = (e[1200:].max(), e.max())
+    assert late[1][0] < 1e-3 * late[1][1]
+    assert late[1][0] < 1e-2 * late[0][0]
