@@ -253,6 +253,48 @@ def bench_adjoint(args, world, barrier, max_over_ranks):
     return out
 
 
+def bench_3d(args, world, barrier, max_over_ranks):
+    """Config 5: 3D elastic hexahedral mesh (128x128x64 elements over 64x64x32 km,
+    67,634,433 global GLL points), layered background + 5% GRF, free top and
+    Stacey on the other faces, moment tensor (1 Hz), 1000 surface receivers,
+    dt = 2 ms.  A bounded run of the 5000-step configuration: 10 warm-up steps,
+    then K steps back to back (CUDA events, graph replay) and K steps each after
+    a 256 MiB L2 flush; model state (about 12.6 GB) far larger than L2."""
+    from specfempp_b200 import meshgen, sfg3d
+    nx, ny, nz = (int(v) for v in args.mesh3d.split("x"))
+    steps = args.steps3d
+    t0 = time.perf_counter()
+    w = meshgen.elastic3d_layered_grf(nx, ny, nz, nstep=2 * steps + 20, nrec=1000)
+    sim = sfg3d.Simulation3D(w.mesh, dt=w.dt, nstep=w.nstep)
+    sim.set_sources(w.sources)
+    sim.set_receivers(w.rec_xyz, types=("displacement",))
+    sim.initialize()
+    setup_s = time.perf_counter() - t0
+    inf = sim.info()
+    sim.run(10)
+    barrier()
+    ms_b2b = max_over_ranks(sim.run_timed(steps))
+    ms_fl = max_over_ranks(sim.run_timed_flushed(steps))
+    stiff = sim.time_kernel(0, 10)
+    upd = sim.time_kernel(1, 10)
+    finite = sim.check_finite()
+    r = 125.0 * inf.nspec / inf.nglob
+    alg = 84.0 + 52.0 * r                       # algorithmic bytes per point-step
+    peak, _ = peaks()
+    out = {"workload": f"elastic3d_{nx}x{ny}x{nz}", "nglob": inf.nglob, "nspec": inf.nspec,
+           "elements_per_block": inf.elements_per_block, "steps": steps, "setup_s": setup_s,
+           "device_gb": inf.device_bytes / 1e9,
+           "ms_per_step_flushed": ms_fl / steps, "ms_per_step_back_to_back": ms_b2b / steps,
+           "gll_pt_updates_per_s": world * inf.nglob * steps / (ms_fl / 1e3),
+           "gll_pt_updates_per_s_back_to_back": world * inf.nglob * steps / (ms_b2b / 1e3),
+           "element_kernel_ms": stiff, "update_kernel_ms": upd,
+           "algorithmic_bytes_per_point": alg,
+           "step_frac_of_hbm": alg * inf.nglob / (ms_fl / steps / 1e3) / 1e9 / peak,
+           "finite": bool(finite)}
+    sim.close()
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -289,6 +331,9 @@ def main():
                     help="elements of the batched-shot model, NXxNZ (config 3: 1000x500)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-steps", type=int, default=30)
+    ap.add_argument("--no-3d", action="store_true")
+    ap.add_argument("--mesh3d", default="128x128x64")
+    ap.add_argument("--steps3d", type=int, default=50)
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--adjoint-mesh", default="500x250")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
@@ -408,6 +453,10 @@ def main():
     if not args.no_adjoint:
         adj = bench_adjoint(args, world, barrier, max_over_ranks)
 
+    b3d = None
+    if not args.no_3d:
+        b3d = bench_3d(args, world, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -438,6 +487,7 @@ def main():
         "gpu_launches": inf.kernels_per_step * args.steps,
         "batched": batched,
         "adjoint": adj,
+        "elastic3d": b3d,
     }
     print(json.dumps(line), flush=True)
 

@@ -664,6 +664,32 @@ int sfg3d_initialize(sfg_handle3d *h) {
     std::vector<float>().swap(h->mu);
     std::vector<int>().swap(h->slot);
     SFG3_CUDA(cudaDeviceSynchronize());
+    if (!(h->opt.elements_per_block == 1 || h->opt.elements_per_block == 2 || h->opt.elements_per_block == 4)) {
+      // launch-shape autotuner: elements per block of the element kernel,
+      // whole steps timed on this mesh (all shapes give the same bits)
+      float best = 1e30f;
+      int pick = 2;
+      for (int e : {1, 2, 4}) {
+        h->epb = e;
+        for (int i = 0; i < 2; ++i) launch_step(h, h->stream, true);
+        SFG3_CUDA(cudaEventRecord(h->ev0, h->stream));
+        for (int i = 0; i < 3; ++i) launch_step(h, h->stream, true);
+        SFG3_CUDA(cudaEventRecord(h->ev1, h->stream));
+        SFG3_CUDA(cudaEventSynchronize(h->ev1));
+        float t = 0;
+        SFG3_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+        if (t < best) { best = t; pick = e; }
+      }
+      h->epb = pick;
+      const size_t nb = n * sizeof(float);
+      SFG3_CUDA(cudaMemset(h->d_u, 0, nb));
+      SFG3_CUDA(cudaMemset(h->d_v, 0, nb));
+      SFG3_CUDA(cudaMemset(h->d_a, 0, nb));
+      SFG3_CUDA(cudaMemset(h->d_step, 0, sizeof(int)));
+      SFG3_CUDA(cudaMemset(h->d_flag, 0, sizeof(int)));
+      SFG3_CUDA(cudaMemset(h->d_seis, 0, size_t(h->opt.nstep) * h->ntypes * std::max(h->nrec, 1) * 3 * sizeof(float)));
+      SFG3_CUDA(cudaDeviceSynchronize());
+    }
     h->graph_k = capture(h, h->graph_steps, true);
     h->graph_1 = capture(h, 1, true);
     h->graph_e = capture(h, 1, false);
