@@ -331,6 +331,10 @@ def main():
                     help="elements of the batched-shot model, NXxNZ (config 3: 1000x500)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-steps", type=int, default=30)
+    ap.add_argument("--kernel-variant", type=int, default=0,
+                    help="fix the element-kernel variant of the headline run (0 = autotuned)")
+    ap.add_argument("--elements-per-block", type=int, default=0,
+                    help="fix the elements per block of the headline run (0 = autotuned)")
     ap.add_argument("--no-3d", action="store_true")
     ap.add_argument("--mesh3d", default="128x128x64")
     ap.add_argument("--steps3d", type=int, default=50)
@@ -361,7 +365,8 @@ def main():
     from specfempp_b200 import sfg
     total_steps = args.warmup + args.steps
     w = make_workload(args.workload, total_steps)
-    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=total_steps)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=total_steps, kernel_variant=args.kernel_variant,
+                           elements_per_block=args.elements_per_block)
     sim.set_sources(w.sources)
     sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
     sim.initialize()

@@ -155,7 +155,10 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
  * step, and copies the seismogram sample of the step (when the step is a
  * sampling step) into seis_row[nshots][ntypes][nrec][2] (host, may be NULL);
  * returns after the copy has landed.  This is the per-step path a host driver
- * that streams sources in and traces out would call. */
+ * that streams sources in and traces out would call.  The step is the fused
+ * one of a run: afterwards the fields hold the next step's predictor, and
+ * sfg_get_field refuses them until sfg_step or sfg_run ends on the exact
+ * end-of-step state. */
 int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
 /* Average device time of one launch of a named kernel family, timed alone with
  * CUDA events: which = 0 element (stiffness) launches of one step, all colours

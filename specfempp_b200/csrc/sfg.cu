@@ -1053,9 +1053,11 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
       SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, row.data(), a.nsrc * sizeof(float),
                                cudaMemcpyHostToDevice, h->stream));
     }
+    // one fused step (the next step's predictor applied in the update); the
+    // step's seismograms are complete before its update runs
     resume(h);
-    SFG_CUDA(cudaGraphLaunch(h->graph_e, h->stream));
-    h->state_final = true;
+    SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+    h->state_final = false;
     ++h->host_step;
     if (seis_row && a.nrec > 0 && step % a.nsb == 0 && step / a.nsb < a.nsig) {
       const size_t row = size_t(a.ntypes) * a.nrec * 2;

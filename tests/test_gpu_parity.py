@@ -182,3 +182,31 @@ def test_moment_tensor_and_sh_all_types(sfg_lib, oracle_lib, name):
         tol = 1e-5 if kind == "displacement" else tolerance(kind, ref[:, t], ref64[:, t])
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
         assert reference_metric(seis[:, t], z[key]).max() < 1e-3, kind
+
+
+def test_step_io_matches_run(sfg_lib):
+    """The per-step host-buffer path gives the run's seismograms bit for bit
+    (with the library's own source table and with the same table streamed in
+    from the host); its fields are mid-step until a plain step ends the run."""
+    from specfempp_b200 import meshgen, sfg, stf
+    w = meshgen.elastic_psv_80x60(nstep=60)
+    case = workload_case(w)
+    sim, a = product_run(case)
+    inf = sim.info()
+    table = stf.table(w.sources, w.dt, case.nstep).astype(np.float32)
+    for streamed in (False, True):
+        sim.reset()
+        row = np.zeros((inf.nshots, inf.ntypes, inf.nrec, 2), np.float32)
+        rows = []
+        for k in range(case.nstep - 1):
+            sim.step_io(np.ascontiguousarray(table[k]) if streamed else None, row)
+            rows.append(row[0].copy())
+        with pytest.raises(sfg.SfgError):
+            sim.field("elastic")
+        sim.step()
+        got = np.concatenate([np.stack(rows), sim.seismograms()[0][-1:]])
+        if streamed:
+            assert np.allclose(got, a, rtol=0, atol=1e-6 * np.abs(a).max())
+        else:
+            assert np.array_equal(got, a)
+        assert np.all(np.isfinite(sim.field("elastic")))
