@@ -282,7 +282,8 @@ def bench_3d(args, world, barrier, max_over_ranks):
     alg = 84.0 + 52.0 * r                       # algorithmic bytes per point-step
     peak, _ = peaks()
     out = {"workload": f"elastic3d_{nx}x{ny}x{nz}", "nglob": inf.nglob, "nspec": inf.nspec,
-           "elements_per_block": inf.elements_per_block, "steps": steps, "setup_s": setup_s,
+           "elements_per_block": inf.elements_per_block, "kernel_variant": inf.kernel_variant,
+           "steps": steps, "setup_s": setup_s,
            "device_gb": inf.device_bytes / 1e9,
            "ms_per_step_flushed": ms_fl / steps, "ms_per_step_back_to_back": ms_b2b / steps,
            "gll_pt_updates_per_s": world * inf.nglob * steps / (ms_fl / 1e3),

@@ -432,9 +432,7 @@ void setup_sources(sfg_handle3d *h) {
   }
 }
 
-void launch_step(sfg_handle3d *h, cudaStream_t s, bool predict) {
-  sfg3::dev::Elem3Args A = h->EA;
-  A.step = h->d_step;
+void launch_elem(sfg_handle3d *h, const sfg3::dev::Elem3Args &A, cudaStream_t s) {
   const int E = h->epb;
   const int grid = (h->nspec + E - 1) / E;
   switch (E) {
@@ -442,6 +440,12 @@ void launch_step(sfg_handle3d *h, cudaStream_t s, bool predict) {
     case 2: sfg3::dev::k_stiffness3d<2><<<grid, NQ * 2, 0, s>>>(A); break;
     default: sfg3::dev::k_stiffness3d<4><<<grid, NQ * 4, 0, s>>>(A); break;
   }
+}
+
+void launch_step(sfg_handle3d *h, cudaStream_t s, bool predict) {
+  sfg3::dev::Elem3Args A = h->EA;
+  A.step = h->d_step;
+  launch_elem(h, A, s);
   if (h->nrec) {
     sfg3::dev::Rec3Args R{};
     R.ibool = h->d_ibool; R.rec_elem = h->d_rec_elem; R.rec_h = h->d_rec_h; R.types = h->d_types;
@@ -668,7 +672,7 @@ int sfg3d_initialize(sfg_handle3d *h) {
       // launch-shape autotuner: elements per block of the element kernel,
       // whole steps timed on this mesh (all shapes give the same bits)
       float best = 1e30f;
-      int pick = 2;
+      int pick = h->epb;
       for (int e : {1, 2, 4}) {
         h->epb = e;
         for (int i = 0; i < 2; ++i) launch_step(h, h->stream, true);
@@ -807,10 +811,7 @@ int sfg3d_time_kernel(sfg_handle3d *h, int which, int reps, float *ms) {
       if (which == 0) {
         sfg3::dev::Elem3Args A = h->EA;
         A.step = h->d_step;
-        const int E = h->epb, grid = (h->nspec + E - 1) / E;
-        if (E == 1) sfg3::dev::k_stiffness3d<1><<<grid, NQ, 0, h->stream>>>(A);
-        else if (E == 2) sfg3::dev::k_stiffness3d<2><<<grid, NQ * 2, 0, h->stream>>>(A);
-        else sfg3::dev::k_stiffness3d<4><<<grid, NQ * 4, 0, h->stream>>>(A);
+        launch_elem(h, A, h->stream);
       } else {
         sfg3::dev::Update3Args U{};
         U.u = h->d_u; U.v = h->d_v; U.minv = h->d_minv; U.inv_start = h->d_inv_start; U.r = h->d_r;
@@ -843,6 +844,7 @@ int sfg3d_get_info(sfg_handle3d *h, sfg_info3d *info) {
     info->device_bytes = h->mem ? h->mem->bytes : 0;
     info->elements_per_block = h->epb;
     info->kernels_per_step = 2 + (h->nrec > 0 ? 1 : 0);
+    info->kernel_variant = 1;
     return int(SFG_OK);
   });
 }

@@ -31,7 +31,7 @@ class Info3D(C.Structure):
     _fields_ = [("nspec", C.c_int), ("nglob", C.c_int), ("nstep", C.c_int), ("istep", C.c_int),
                 ("nrec", C.c_int), ("ntypes", C.c_int), ("nsig", C.c_int), ("nsrc", C.c_int),
                 ("t0", C.c_double), ("device_bytes", C.c_size_t), ("elements_per_block", C.c_int),
-                ("kernels_per_step", C.c_int)]
+                ("kernels_per_step", C.c_int), ("kernel_variant", C.c_int)]
 
 
 _vp = C.c_void_p
@@ -73,7 +73,8 @@ def _arr(x, dtype):
 class Simulation3D:
     """One 3D elastic forward simulation on the GPU (a libsfg 3D handle)."""
 
-    def __init__(self, mesh, *, dt: float, nstep: int, elements_per_block: int = 0, steps_per_graph: int = 0):
+    def __init__(self, mesh, *, dt: float, nstep: int, elements_per_block: int = 0, steps_per_graph: int = 0,
+                 kernel_variant: int = 0):
         self.lib = load_library3d()
         self._keep = []
         d = MeshDesc3D()
@@ -86,7 +87,7 @@ class Simulation3D:
         for i in range(6):
             d.absorbing[i] = int(mesh.absorbing[i])
         o = Options(dt=dt, nstep=nstep, nshots=1, nstep_between_samples=1, steps_per_graph=steps_per_graph,
-                    elements_per_block=elements_per_block, kernel_variant=0, store_acceleration=0)
+                    elements_per_block=elements_per_block, kernel_variant=kernel_variant, store_acceleration=0)
         h = _vp()
         rc = self.lib.sfg3d_create(C.byref(d), C.byref(o), C.byref(h))
         if rc != 0:

@@ -16,9 +16,10 @@ pytestmark = pytest.mark.gpu
 TYPES = ("displacement", "velocity", "acceleration")
 
 
-def product3d(case, epb=0, types=TYPES):
+def product3d(case, epb=0, types=TYPES, variant=0):
     from specfempp_b200 import sfg3d
-    sim = sfg3d.Simulation3D(case.mesh, dt=case.dt, nstep=case.nstep, elements_per_block=epb)
+    sim = sfg3d.Simulation3D(case.mesh, dt=case.dt, nstep=case.nstep, elements_per_block=epb,
+                             kernel_variant=variant)
     sim.set_sources(case.sources)
     sim.set_receivers(case.rec_xyz, types=types)
     sim.initialize()

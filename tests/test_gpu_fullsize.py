@@ -1,0 +1,69 @@
+"""Full-size configurations through size-independent properties (the oracle
+is too slow at these sizes):
+
+* linearity: doubling every source factor doubles every seismogram sample
+  exactly (a power-of-two scale commutes with every FP32 operation of the
+  step), at the full sizes of the coupled 400x200 model (4000 steps), the
+  batched 1000x500 GRF model (32 shots) and the 3D 128x128x64 model;
+* superposition: two sources in one run equal the sum of two one-source runs
+  to FP32 rounding (coupled 400x200, 4000 steps);
+* finiteness and non-trivial signal everywhere.
+"""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def run2d(w, srcs, nstep, nshots=1, **kw):
+    from specfempp_b200 import sfg
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=nstep, nshots=nshots, **kw)
+    sim.set_sources(srcs)
+    sim.set_receivers(w.rec_x, w.rec_z)
+    sim.initialize()
+    sim.run(nstep)
+    assert sim.check_finite()
+    return sim.seismograms()
+
+
+def test_coupled_400x200_linearity_and_superposition(sfg_lib):
+    from specfempp_b200 import meshgen
+    w = meshgen.coupled_400x200()
+    s0 = w.sources[0]
+    a = run2d(w, [s0], w.nstep)
+    b = run2d(w, [replace(s0, factor=2 * s0.factor)], w.nstep)
+    assert np.abs(a).max() > 0
+    assert np.array_equal(b, 2 * a)
+    s1 = replace(s0, x=s0.x + 3100.0, z=s0.z - 700.0, f0=4.0, factor=0.5 * s0.factor)
+    c = run2d(w, [s1], w.nstep)
+    both = run2d(w, [s0, s1], w.nstep)
+    assert np.linalg.norm(both - (a + c)) <= 1e-5 * np.linalg.norm(both)
+
+
+def test_batched_1000x500_linearity(sfg_lib):
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_grf_1000x500(nstep=600, nshots=32)
+    kw = dict(point_rho=w.point_rho, point_vp=w.point_vp, point_vs=w.point_vs)
+    a = run2d(w, w.sources, 600, nshots=32, **kw)
+    b = run2d(w, [replace(s, factor=2 * s.factor) for s in w.sources], 600, nshots=32, **kw)
+    assert np.all(np.abs(a).reshape(32, -1).max(axis=1) > 0)
+    assert np.array_equal(b, 2 * a)
+
+
+def test_elastic3d_128x128x64_linearity(sfg_lib):
+    from specfempp_b200 import meshgen, sfg3d
+    w = meshgen.elastic3d_layered_grf(nstep=300)
+    out = []
+    for scale in (1.0, 2.0):
+        sim = sfg3d.Simulation3D(w.mesh, dt=w.dt, nstep=300)
+        sim.set_sources([replace(s, factor=scale * s.factor) for s in w.sources])
+        sim.set_receivers(w.rec_xyz)
+        sim.initialize()
+        sim.run(300)
+        assert sim.check_finite()
+        out.append(sim.seismograms())
+        sim.close()
+    assert np.abs(out[0]).max() > 0
+    assert np.array_equal(out[1], 2 * out[0])
