@@ -247,8 +247,12 @@ def bench_adjoint(args, world, barrier, max_over_ranks):
             ad = float((grads[which] * d).sum())
             rows.append({"parameter": ["rho", "kappa", "mu"][which], "adjoint": ad, "fd4": fd,
                          "rel_err": abs(ad - fd) / abs(fd)})
+        scale = max(abs(r["fd4"]) for r in rows)
+        for r in rows:
+            r["err_vs_largest"] = abs(r["adjoint"] - r["fd4"]) / scale
         out["fd"] = {"misfit": L, "sources": len(w.sources), "step": h, "stencil": "4th-order central",
-                     "perturbations": rows, "max_rel_err": max(r["rel_err"] for r in rows)}
+                     "perturbations": rows, "max_rel_err": max(r["rel_err"] for r in rows),
+                     "max_err_vs_largest_derivative": max(r["err_vs_largest"] for r in rows)}
     del sim
     return out
 
