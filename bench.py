@@ -312,10 +312,12 @@ def run_reference(args, rank):
     cpu_oracle_throughput(w, warm, threads)
     v, secs = cpu_oracle_throughput(w, steps, threads)
     ms = secs * 1000.0 / steps
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": 0,
+    nglob = int(round(v * secs / steps))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "nglob": None, "steps_requested": args.steps},
+            "config": {"workload": args.workload, "nglob": nglob, "steps_requested": args.steps,
+                       "device": "host CPU only (rank 0)"},
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{steps} time steps of {args.workload} (full mesh), "
                                        f"FP32 C++ restatement of the reference, OpenMP atomics"},
