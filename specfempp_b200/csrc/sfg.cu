@@ -160,6 +160,8 @@ struct sfg_handle {
   int resident[2][3] = {{0}};  // persistent: resident blocks per SM [EK][E index]
   int resident_tma[2][3] = {{0}};  // bulk-copy element kernel: resident blocks per SM
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;  // receivers that overlap the element kernel
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaGraphExec_t graph_k = nullptr, graph_1 = nullptr, graph_e = nullptr;
   int graph_steps = 0;
   // true when u, v hold the end-of-step state of the reference (after the
@@ -194,6 +196,9 @@ struct sfg_handle {
     if (graph_e) cudaGraphExecDestroy(graph_e);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (side) cudaStreamDestroy(side);
     if (stream) cudaStreamDestroy(stream);
     if (flush_buf) cudaFree(flush_buf);
     mem.free_all();
@@ -523,23 +528,49 @@ void launch_predict(sfg_handle *h, cudaStream_t s) {
 // reads the predicted elastic displacement), then the elastic update (its
 // coupling reads the new acoustic chi_dd).  predict = fuse the next step's
 // predictor into the updates.
+// Seismograms of a medium that read only the step's displacement (elastic
+// displacement and pressure, acoustic displacement) can be taken while the
+// element kernel runs.
+bool receivers_early(const sfg_handle *h, int medium) {
+  for (int t = 0; t < h->asmb.ntypes; ++t) {
+    const int k = h->asmb.types[t];
+    if (!(k == SFG_SEIS_DISPLACEMENT || (k == SFG_SEIS_PRESSURE && medium == SFG_MEDIUM_ELASTIC))) return false;
+  }
+  return true;
+}
+
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
   if (h->recording) sfg::dev::k_record_begin<<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+  // a recorded (recomputed) step's seismograms are those of the forward run
+  const bool rec_ac = has_ac && h->ac.nrec > 0 && h->recording != 2;
+  const bool rec_el = has_el && h->el.nrec > 0 && h->recording != 2;
+  const bool early_ac = rec_ac && receivers_early(h, SFG_MEDIUM_ACOUSTIC);
+  const bool early_el = rec_el && receivers_early(h, SFG_MEDIUM_ELASTIC);
+  const bool fork = (early_ac || early_el) && h->side;
+  if (fork) {
+    // receivers on the side stream, concurrent with the element kernel; they
+    // join before the first update changes the displacement
+    SFG_CUDA(cudaEventRecord(h->ev_fork, s));
+    SFG_CUDA(cudaStreamWaitEvent(h->side, h->ev_fork, 0));
+    if (early_ac) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, h->side);
+    if (early_el) launch_receivers(h, SFG_MEDIUM_ELASTIC, h->side);
+    SFG_CUDA(cudaEventRecord(h->ev_join, h->side));
+  }
   launch_stiffness(h, s);
+  if (fork) SFG_CUDA(cudaStreamWaitEvent(s, h->ev_join, 0));
   if (has_ac) {
-    if (h->recording != 2) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
+    if (rec_ac && !(fork && early_ac)) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
     launch_update(h, SFG_MEDIUM_ACOUSTIC, predict, !has_el, s);
   }
   if (has_el) {
-    // a recorded (recomputed) step's seismograms are those of the forward run
-    if (h->recording != 2) launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
+    if (rec_el && !(fork && early_el)) launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
     launch_update(h, SFG_MEDIUM_ELASTIC, predict, true, s);
   }
 }
 
 int kernels_per_step(const sfg_handle *h) {
-  int n = std::max(ncolors(h->el), ncolors(h->ac));
+  int n = h->variant >= 3 ? 1 : std::max(ncolors(h->el), ncolors(h->ac));
   for (const DevMedium *D : {&h->ac, &h->el}) {
     if (D->nspec == 0) continue;
     n += (D->nrec > 0 ? 1 : 0) + 1;
@@ -884,6 +915,9 @@ int sfg_initialize(sfg_handle *h) {
     if (!h->have_receivers) { a.nrec = 0; a.ntypes = 1; a.types = {0}; }
     a.nsig = (a.nstep + a.nsb - 1) / a.nsb;
     SFG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    SFG_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
+    SFG_CUDA(cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming));
+    SFG_CUDA(cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming));
     SFG_CUDA(cudaEventCreate(&h->ev0));
     SFG_CUDA(cudaEventCreate(&h->ev1));
     for (int i = 0; i < sfg::NPTS; ++i) { h->quad.hp[i] = a.hprime[i]; h->quad.hpw[i] = a.hpw[i]; }
