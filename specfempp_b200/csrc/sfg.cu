@@ -117,7 +117,10 @@ struct AdjointState {
   float *lb_geo = nullptr;                      // [nlb][nx, nz, j1, wq]
   std::vector<size_t> lb_k;                     // index into the boundary arrays
   std::vector<size_t> lb_pm;                    // mesh-order element point
-  float *gtab = nullptr;                        // [nstep][nrec][2]
+  float *gtab = nullptr;                        // [nstep][nrec][2] (the reverse graphs hold this pointer)
+  size_t gtab_cap = 0;
+  float *h_stage = nullptr;                     // pinned host staging: gtab rows, then the sums
+  size_t h_stage_cap = 0;
   int *ad_head = nullptr, *ad_next = nullptr;
   int *st_pt = nullptr;
   float *st_c = nullptr;
@@ -128,6 +131,7 @@ struct AdjointState {
   cudaGraphExec_t graph_rev[2] = {nullptr, nullptr};  // reverse sweep of a full segment, per buffer
   int *d_k0 = nullptr;                          // first step of the segment in reverse
   bool forward_done = false;
+  int epb = 0;                                  // elements per block of k_adj_elem (timed once)
   size_t nsum() const { return off_lb + 4 * size_t(nlb); }
 };
 
@@ -180,6 +184,7 @@ struct sfg_handle {
                     (void *)adj.st_c, (void *)adj.d_rec, (void *)adj.seg_v, (void *)adj.lb_g,
                     (void *)adj.lb_j, (void *)adj.lb_geo})
       if (p) cudaFree(p);
+    if (adj.h_stage) cudaFreeHost(adj.h_stage);
     if (adj.graph_r1) cudaGraphExecDestroy(adj.graph_r1);
     if (adj.graph_rseg) cudaGraphExecDestroy(adj.graph_rseg);
     for (auto &g : adj.graph_rev)
@@ -1495,8 +1500,34 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
 }
 
+void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs);
+
+// Elements per block of the reverse element kernel: each shape timed over a
+// few launches on the live buffers (before the sums are cleared), the fastest
+// kept.  All shapes give the same bits.
+void tune_reverse(sfg_handle *h, cudaStream_t rs) {
+  AdjointState &A = h->adj;
+  if (A.epb) return;
+  float best = 1e30f;
+  A.epb = 8;
+  for (int e : {8, 16, 32}) {
+    const int save = A.epb;
+    A.epb = e;
+    for (int rep = 0; rep < 2; ++rep) {
+      if (rep == 1) SFG_CUDA(cudaEventRecord(h->ev0, rs));
+      for (int i = 0; i < 3; ++i) reverse_segment(h, 0, 1, true, rs);
+    }
+    SFG_CUDA(cudaEventRecord(h->ev1, rs));
+    SFG_CUDA(cudaEventSynchronize(h->ev1));
+    float t = 0;
+    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    if (t < best) best = t;
+    else A.epb = save;
+  }
+}
+
 void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
-  switch (h->epb) {
+  switch (h->adj.epb) {
     case 16: reverse_segment_E<16>(h, b, n, last, rs); break;
     case 32: reverse_segment_E<32>(h, b, n, last, rs); break;
     default: reverse_segment_E<8>(h, b, n, last, rs); break;
@@ -1554,21 +1585,37 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     const int nrec = as.nrec;
     cudaStream_t s = h->stream;
     // dL/d(seismogram) of every step on the device: [nstep][nrec][2]
-    if (A.gtab) cudaFree(A.gtab);
-    A.gtab = dalloc<float>(size_t(A.nstep) * nrec * 2);
+    const size_t ng = std::max<size_t>(size_t(A.nstep) * nrec * 2, 1);
+    if (ng > A.gtab_cap) {
+      // the reverse-sweep graphs hold the table's address: drop them with it
+      SFG_CUDA(cudaStreamSynchronize(s));
+      if (A.rstream) SFG_CUDA(cudaStreamSynchronize(A.rstream));
+      if (A.gtab) cudaFree(A.gtab);
+      A.gtab = dalloc<float>(ng);
+      A.gtab_cap = ng;
+      for (cudaGraphExec_t *g : {&A.graph_rev[0], &A.graph_rev[1]})
+        if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+    }
+    const size_t nstage = std::max(ng, A.nsum());
+    if (nstage > A.h_stage_cap) {
+      if (A.h_stage) cudaFreeHost(A.h_stage);
+      SFG_CUDA(cudaMallocHost(&A.h_stage, nstage * sizeof(float)));
+      A.h_stage_cap = nstage;
+    }
     if (nrec) {
       // the seismograms leave the library rotated by the receiver angle
       // (sfg_get_seismograms); the adjoint sources are rotated back
-      std::vector<float> g(size_t(A.nstep) * nrec * 2);
+      float *g = A.h_stage;
       const float ca = std::cos(float(M_PI) / 180.f * float(as.rec_angle));
       const float sa = std::sin(float(M_PI) / 180.f * float(as.rec_angle));
-      for (size_t i = 0; i < g.size(); i += 2) {
+      for (size_t i = 0; i + 1 < size_t(A.nstep) * nrec * 2; i += 2) {
         g[i] = ca * seis_grad[i] + sa * seis_grad[i + 1];
         g[i + 1] = -sa * seis_grad[i] + ca * seis_grad[i + 1];
       }
-      SFG_CUDA(cudaMemcpy(A.gtab, g.data(), g.size() * sizeof(float), cudaMemcpyHostToDevice));
+      SFG_CUDA(cudaMemcpyAsync(A.gtab, g, size_t(A.nstep) * nrec * 2 * sizeof(float), cudaMemcpyHostToDevice, s));
     }
     const size_t nv = A.nvals;
+    tune_reverse(h, s);
     for (float *p : {A.lu, A.lv, A.mu})
       SFG_CUDA(cudaMemsetAsync(p, 0, (nv + 4) * sizeof(float), s));
     for (float *p : {A.sum, A.comp, A.seg})
@@ -1613,9 +1660,9 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     const DevMedium &D = h->el;
     const float dt2 = float(as.dt) / 2.0f;
     // compute order -> mesh order; rho: -W_p G(g_p)
-    std::vector<float> tot(A.nsum());
-    SFG_CUDA(cudaMemcpy(tot.data(), A.sum, tot.size() * sizeof(float), cudaMemcpyDeviceToHost));
-    const float *grho = tot.data() + 2 * A.nloc;
+    const float *tot = A.h_stage;
+    SFG_CUDA(cudaMemcpy(A.h_stage, A.sum, A.nsum() * sizeof(float), cudaMemcpyDeviceToHost));
+    const float *grho = tot + 2 * A.nloc;
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = as.el.elem_mesh[ce];
       for (int q = 0; q < sfg::NPTS; ++q) {
@@ -1629,7 +1676,7 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       }
     }
     // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu)
-    const float *lbs = tot.data() + A.off_lb;
+    const float *lbs = tot + A.off_lb;
     for (int i = 0; i < A.nlb; ++i) {
       const size_t k = A.lb_k[i];
       const sfg::MediumData &M = as.el;
