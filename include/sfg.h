@@ -75,6 +75,9 @@ typedef struct sfg_mesh2d_desc {
   int nfree;
   const int *free_ispec, *free_type; /* acoustic free-surface edges */
   int elastic_wave;              /* SFG_WAVE_PSV or SFG_WAVE_SH */
+  const double *mat_aniso;       /* optional [numat][6] anisotropic elastic constants
+                                    (c11, c13, c15, c33, c35, c55; NaN rows: isotropic);
+                                    mat_vp = sqrt(c33/rho), mat_vs = sqrt(c55/rho) there */
 } sfg_mesh2d_desc;
 
 typedef struct sfg_options {

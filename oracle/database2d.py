@@ -54,6 +54,9 @@ class Mesh2D:
     coupled_pairs: np.ndarray    # [ncoupled, 2] (element a, element b)
     title: str = ""
     extra: dict = field(default_factory=dict)
+    # anisotropic elastic materials: (c11, c13, c15, c33, c35, c55) per
+    # material, NaN rows for isotropic ones; None when every material is isotropic
+    mat_aniso: np.ndarray | None = None
 
 
 def _records(buf: bytes):
@@ -122,14 +125,24 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
     mat_rho = np.zeros(numat)
     mat_vp = np.zeros(numat)
     mat_vs = np.zeros(numat)
+    mat_aniso = np.full((numat, 6), np.nan)
     for m in range(numat):
         vals = struct.unpack("<ii13d", take())
         n, indic = vals[0], vals[1]
         v = vals[2:]
         if n != m + 1:
             raise ValueError("Wrong material set number")
+        if indic == 2:
+            # anisotropic elastic: rho, c11, c13, c15, c33, c35, c55, c12, c23, c25
+            # (src/io/mesh/impl/fortran/dim2/read_material_properties.cpp:252-291)
+            mat_rho[m] = v[0]
+            mat_aniso[m] = v[1:7]
+            mat_vp[m] = np.sqrt(v[4] / v[0])          # sqrt(c33 / rho)
+            mat_vs[m] = np.sqrt(v[6] / v[0])          # sqrt(c55 / rho)
+            mat_medium[m] = ELASTIC
+            continue
         if indic != 1:
-            raise ValueError(f"material type {indic} (non-isotropic) is outside this path")
+            raise ValueError(f"material type {indic} is outside this path")
         mat_rho[m], mat_vp[m], mat_vs[m] = v[0], v[1], v[2]
         mat_medium[m] = ACOUSTIC if v[2] == 0 else ELASTIC
 
@@ -188,4 +201,5 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
                   free_ispec=np.asarray(free_ispec, np.int32),
                   free_type=np.asarray(free_type, np.int32),
                   coupled_pairs=np.asarray(pairs, np.int32).reshape(-1, 2),
-                  title=title, extra=extra)
+                  title=title, extra=extra,
+                  mat_aniso=mat_aniso if np.isfinite(mat_aniso).any() else None)

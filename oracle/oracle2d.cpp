@@ -208,6 +208,8 @@ struct Sim {
   std::vector<int> medium;          // [nspec]
   // elastic: kappa, mu, rho; acoustic: rho_inverse, kappa
   std::vector<T> p_kappa, p_mu, p_rho, p_rhoinv;
+  // anisotropic elastic (when in.aniso): c11, c13, c15, c33, c35, c55 per point
+  std::vector<T> p_c[6];
   // Stacey point data per element (dense, tag 0/1)
   std::vector<uint8_t> st_tag, fs_tag;   // [nspec][25]
   std::vector<T> st_nx, st_nz, st_w;     // [nspec][25]
@@ -360,11 +362,22 @@ struct Sim {
         p_rho[p] = rho;
       }
     }
+    if (in.aniso) {
+      if (in.elastic_sh) throw std::runtime_error("anisotropic SH is outside this path");
+      for (int k = 0; k < 6; ++k) {
+        p_c[k].resize(n);
+        for (size_t p = 0; p < n; ++p) p_c[k][p] = T(in.aniso[p * 6 + k]);
+      }
+    }
   }
 
   T lp2m(size_t p) const { return p_kappa[p] + T(4.0 / 3.0) * p_mu[p]; }
-  T rho_vp(size_t p) const { return std::sqrt(lp2m(p) / p_rho[p]) * p_rho[p]; }
-  T rho_vs(size_t p) const { return std::sqrt(p_rho[p] * p_mu[p]); }
+  // anisotropic: rho vp = sqrt(rho c33), rho vs = sqrt(rho c55)
+  // (include/medium/dim2/elastic/anisotropic/properties.hpp:88-94)
+  T rho_vp(size_t p) const {
+    return in.aniso ? std::sqrt(p_rho[p] * p_c[3][p]) : std::sqrt(lp2m(p) / p_rho[p]) * p_rho[p];
+  }
+  T rho_vs(size_t p) const { return in.aniso ? std::sqrt(p_rho[p] * p_c[5][p]) : std::sqrt(p_rho[p] * p_mu[p]); }
   T rho_vpinv(size_t p) const { return std::sqrt(p_rhoinv[p] * (T(1) / p_kappa[p])); }
 
   void normal(size_t p, int type, T &nx, T &nz) const {
@@ -688,6 +701,13 @@ struct Sim {
         } else if (ncomp == 1) {
           S[0][0] = p_mu[p] * du[0][0];
           S[0][1] = p_mu[p] * du[0][1];
+        } else if (in.aniso) {
+          // include/medium/dim2/elastic/anisotropic/stress.hpp
+          const T sh = du[1][0] + du[0][1];
+          const T sxx = p_c[0][p] * du[0][0] + p_c[1][p] * du[1][1] + p_c[2][p] * sh;
+          const T szz = p_c[1][p] * du[0][0] + p_c[3][p] * du[1][1] + p_c[4][p] * sh;
+          const T sxz = p_c[2][p] * du[0][0] + p_c[4][p] * du[1][1] + p_c[5][p] * sh;
+          S[0][0] = sxx; S[0][1] = sxz; S[1][0] = sxz; S[1][1] = szz;
         } else {
           const T l2m = lp2m(p), lam = l2m - T(2) * p_mu[p];
           const T sxx = l2m * du[0][0] + lam * du[1][1];

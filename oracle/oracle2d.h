@@ -34,6 +34,9 @@ typedef struct OracleInput2D {
    * tensor with components src_mxx, src_mzz, src_mxz */
   const int *src_kind;
   const double *src_mxx, *src_mzz, *src_mxz;
+  /* optional anisotropic elastic constants per GLL point [nspec][25][6]
+   * (c11, c13, c15, c33, c35, c55); NULL: isotropic from rho, vp, vs */
+  const double *aniso;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

@@ -47,6 +47,7 @@ class OracleInput2D(C.Structure):
         ("dt", C.c_double), ("nstep", C.c_int), ("nstep_between_samples", C.c_int),
         ("setup_in_run_precision", C.c_int),
         ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
+        ("aniso", _dp),
     ]
 
 
@@ -145,6 +146,23 @@ def _ptr(a, t):
     return a.ctypes.data_as(t) if a is not None else None
 
 
+def aniso_points(case):
+    """[nspec, 25, 6] anisotropic constants when the mesh has an anisotropic
+    material (isotropic elements as c11 = c33 = lambda + 2 mu, c13 = lambda,
+    c55 = mu, c15 = c35 = 0), else None."""
+    m = case.mesh
+    ma = getattr(m, "mat_aniso", None)
+    if ma is None or not np.isfinite(ma).any():
+        return None
+    rho, vp, vs = point_models(case)
+    mu = rho * vs * vs
+    l2m = rho * vp * vp
+    iso = np.stack([l2m, l2m - 2 * mu, 0 * mu, l2m, 0 * mu, mu], -1)      # [nspec, 25, 6]
+    per = ma[m.kmato]                                                    # [nspec, 6]
+    out = np.where(np.isfinite(per)[:, None, :], per[:, None, :], iso)
+    return np.ascontiguousarray(out)
+
+
 def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: bool = False):
     """Run the oracle; returns dict with 'seis' [nsig, ntypes, nrec, 2], 't0', 'times'."""
     m = case.mesh
@@ -200,6 +218,8 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     inp.src_mxx = _ptr(arr([getattr(s, "mxx", 0.0) for s in srcs], np.float64), _dp)
     inp.src_mzz = _ptr(arr([getattr(s, "mzz", 0.0) for s in srcs], np.float64), _dp)
     inp.src_mxz = _ptr(arr([getattr(s, "mxz", 0.0) for s in srcs], np.float64), _dp)
+    aniso = aniso_points(case)
+    inp.aniso = _ptr(arr(aniso, np.float64), _dp) if aniso is not None else None
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()

@@ -216,7 +216,18 @@ bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
       double v[13];
       for (double &x : v) x = rd<double>(p);
       if (n != i + 1) throw std::runtime_error("Wrong material set number");
-      if (indic != 1) throw std::runtime_error("only isotropic elastic/acoustic materials are supported");
+      if (indic == 2) {
+        // anisotropic elastic: rho, c11, c13, c15, c33, c35, c55, c12, c23, c25
+        // (src/io/mesh/impl/fortran/dim2/read_material_properties.cpp:252-291)
+        if (m.mat_aniso.empty()) m.mat_aniso.assign(size_t(m.numat) * 6, std::nan(""));
+        for (int k = 0; k < 6; ++k) m.mat_aniso[size_t(i) * 6 + k] = v[1 + k];
+        m.mat_rho[i] = v[0];
+        m.mat_vp[i] = std::sqrt(v[4] / v[0]);
+        m.mat_vs[i] = std::sqrt(v[6] / v[0]);
+        m.mat_medium[i] = 1;
+        continue;
+      }
+      if (indic != 1) throw std::runtime_error("only isotropic and anisotropic elastic / acoustic materials are supported");
       m.mat_rho[i] = v[0]; m.mat_vp[i] = v[1]; m.mat_vs[i] = v[2];
       m.mat_medium[i] = (v[2] == 0.0) ? 0 : 1;
     }
@@ -288,18 +299,37 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
     vp = m.pvp.empty() ? m.mat_vp[mat] : m.pvp[pm];
     vs = m.pvs.empty() ? m.mat_vs[mat] : m.pvs[pm];
   };
+  auto aniso_of = [&](int e) -> const double * {
+    if (m.mat_aniso.empty()) return nullptr;
+    const double *c = &m.mat_aniso[size_t(m.kmato[e]) * 6];
+    return std::isfinite(c[0]) ? c : nullptr;
+  };
+  a.el.aniso = false;
+  for (int ce = 0; ce < a.el.nspec; ++ce) a.el.aniso |= aniso_of(a.el.elem_mesh[ce]) != nullptr;
+  if (a.el.aniso && (a.el.ncomp != 2 || !m.prho.empty()))
+    throw std::runtime_error("anisotropic media: P-SV with material constants only (no SH, no point models)");
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
     const size_t n = size_t(D.nspec) * NPTS;
     D.prop0.resize(n);
     D.prop1.resize(n);
+    for (auto *v : {&D.prop2, &D.prop3, &D.prop4, &D.prop5}) v->assign(med == 1 && D.aniso ? n : 0, 0.0f);
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
       for (int q = 0; q < NPTS; ++q) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
-        if (med == 1) {
+        if (med == 1 && D.aniso) {
+          // c11, c13, c15, c33, c35, c55 (include/medium/dim2/elastic/anisotropic/
+          // properties.hpp); isotropic elements of the medium in the same form
+          const double *c = aniso_of(e);
+          const double mu = rho * vs * vs, l2m = rho * vp * vp;
+          const double iso[6] = {l2m, l2m - 2.0 * mu, 0.0, l2m, 0.0, mu};
+          const double *cc = c ? c : iso;
+          D.prop0[pc] = float(cc[0]); D.prop1[pc] = float(cc[1]); D.prop2[pc] = float(cc[2]);
+          D.prop3[pc] = float(cc[3]); D.prop4[pc] = float(cc[4]); D.prop5[pc] = float(cc[5]);
+        } else if (med == 1) {
           // kappa = rho (vp^2 - 4/3 vs^2), mu = rho vs^2; lambda+2mu = kappa + 4/3 mu
           // (include/medium/dim2/elastic/isotropic/material.hpp:66-69, properties.hpp:71-91)
           const double mu = rho * vs * vs;
@@ -322,7 +352,12 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
-        if (med == 1) {
+        if (med == 1 && D.aniso) {
+          // rho vp = sqrt(rho c33), rho vs = sqrt(rho c55)
+          // (include/medium/dim2/elastic/anisotropic/properties.hpp:88-94)
+          D.bc_imp0[k] = float(std::sqrt(rho * double(D.prop3[pc])));
+          D.bc_imp1[k] = float(std::sqrt(rho * double(D.prop5[pc])));
+        } else if (med == 1) {
           // rho*vp = sqrt((lambda+2mu)/rho)*rho, rho*vs = sqrt(rho*mu) (properties.hpp:77-87)
           const double l2m = D.prop0[pc], mu = D.prop1[pc];
           D.bc_imp0[k] = float(std::sqrt(l2m / rho) * rho);

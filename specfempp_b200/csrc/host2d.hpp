@@ -25,6 +25,9 @@ struct Mesh2D {
   int numat = 0;
   std::vector<int> mat_medium;        // [numat]
   std::vector<double> mat_rho, mat_vp, mat_vs;
+  // optional anisotropic elastic constants [numat][6] (c11, c13, c15, c33,
+  // c35, c55); rows of NaN for isotropic materials
+  std::vector<double> mat_aniso;
   std::vector<float> prho, pvp, pvs;  // optional [nspec][25]
   std::vector<int> abs_ispec, abs_type, free_ispec, free_type;
   int elastic_wave = 0;               // 0 P-SV, 1 SH
@@ -49,6 +52,9 @@ struct MediumData {
   std::vector<int> ibool;             // [nspec][25] -> medium point id
   std::vector<float> xix, xiz, gax, gaz, jac;  // [nspec][25]
   std::vector<float> prop0, prop1;    // elastic: lambda+2mu, mu; acoustic: 1/rho, kappa
+  // anisotropic elastic medium: prop0..prop5 = c11, c13, c15, c33, c35, c55
+  bool aniso = false;
+  std::vector<float> prop2, prop3, prop4, prop5;
   std::vector<float> minv;            // [nglob][ncomp]
   // Stacey / free-surface: slot per element (-1 none), compact [nslot][25]
   std::vector<int> bc_slot;

@@ -55,6 +55,7 @@ struct MedArgs {
   const int *__restrict__ ibool;
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
+  const float *__restrict__ prop2, *__restrict__ prop3, *__restrict__ prop4, *__restrict__ prop5;  // anisotropic
   const int *__restrict__ bc_slot;
   const float *__restrict__ bc_w, *__restrict__ bc_nx, *__restrict__ bc_nz, *__restrict__ bc_j1,
       *__restrict__ bc_imp0, *__restrict__ bc_imp1, *__restrict__ bc_keep;
@@ -86,14 +87,16 @@ __device__ __forceinline__ void load_quad(const Quad &Q, float *shp, float *shpw
   if (tid < NG) sw[tid] = Q.w[tid];
 }
 
-// Elastic element block; EK 0 = P-SV (two components), 1 = SH (one component).
+// Elastic element block; EK 0 = P-SV (two components), 1 = SH (one component),
+// 2 = anisotropic P-SV (prop0..prop5 = c11, c13, c15, c33, c35, c55;
+// include/medium/dim2/elastic/anisotropic/stress.hpp).
 // LOCAL: write the element's contribution to its own slot of A.r (summed per
 // point later by the update) instead of adding it into the accumulator.
 template <int E, int EK, bool LOCAL>
 __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs &A, int ebase,
                                               unsigned char *smem, float *shp, float *shpw,
                                               float *sw) {
-  constexpr int NC = EK == 0 ? 2 : 1;
+  constexpr int NC = EK == 1 ? 1 : 2;
   float *su = reinterpret_cast<float *>(smem);                               // [E][NC][25]
   float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * 2);  // [E][NC][2][25]
   const int tid = threadIdx.x;
@@ -138,7 +141,18 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   }
   // stress (P-SV: isotropic Hooke with lambda+2mu = c0; SH: sigma = mu grad u_y)
   float Sx[NC], Sz[NC];
-  if (EK == 0) {
+  if (EK == 2) {
+    const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+    const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
+    const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+    const float c15 = __ldg(A.prop2 + p), c33 = __ldg(A.prop3 + p), c35 = __ldg(A.prop4 + p),
+                c55 = __ldg(A.prop5 + p);
+    const float sh = du10 + du01;
+    const float sxx = c0 * du00 + mu * du11 + c15 * sh;     // c0 = c11, mu = c13 here
+    const float szz = mu * du00 + c33 * du11 + c35 * sh;
+    const float sxz = c15 * du00 + c35 * du11 + c55 * sh;
+    Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
+  } else if (EK == 0) {
     const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
     const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
     const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
@@ -176,7 +190,7 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     const float wq = A.bc_w[k];
     if (wq != 0.f) {
       const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
-      if (EK == 0) {
+      if (EK != 1) {
         const float2 vv = reinterpret_cast<const float2 *>(A.v)[g];
         const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
         const float vn = vv.x * nx + vv.y * nz;

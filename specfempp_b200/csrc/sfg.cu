@@ -75,6 +75,8 @@ struct DevMedium {
   int *ibool = nullptr;
   float *xix = nullptr, *xiz = nullptr, *gax = nullptr, *gaz = nullptr, *jac = nullptr,
         *prop0 = nullptr, *prop1 = nullptr;
+  float *prop2 = nullptr, *prop3 = nullptr, *prop4 = nullptr, *prop5 = nullptr;  // anisotropic
+  bool aniso = false;
   int *bc_slot = nullptr;
   float *bc_w = nullptr, *bc_nx = nullptr, *bc_nz = nullptr, *bc_j1 = nullptr,
         *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr;
@@ -245,6 +247,11 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.xix = padded(M.xix); D.xiz = padded(M.xiz); D.gax = padded(M.gax);
   D.gaz = padded(M.gaz); D.jac = padded(M.jac);
   D.prop0 = padded(M.prop0); D.prop1 = padded(M.prop1);
+  D.aniso = M.aniso;
+  if (M.aniso) {
+    D.prop2 = padded(M.prop2); D.prop3 = padded(M.prop3);
+    D.prop4 = padded(M.prop4); D.prop5 = padded(M.prop5);
+  }
   D.bc_slot = m.upload(M.bc_slot);
   D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
   D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
@@ -273,6 +280,7 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
   A.ibool = D.ibool;
   A.xix = D.xix; A.xiz = D.xiz; A.gax = D.gax; A.gaz = D.gaz; A.jac = D.jac;
   A.prop0 = D.prop0; A.prop1 = D.prop1;
+  A.prop2 = D.prop2; A.prop3 = D.prop3; A.prop4 = D.prop4; A.prop5 = D.prop5;
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
   A.src_head = D.src_head;
@@ -285,6 +293,8 @@ int ncolors(const DevMedium &D) { return D.nspec ? int(D.color_start.size()) - 1
 template <int E, int EK>
 void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
                         cudaStream_t s, int variant) {
+  // the anisotropic stress exists in the colour-pass and owner-computes kernels
+  if (EK == 2 && (variant == 2 || variant == 4)) variant = variant == 2 ? 1 : 3;
   sfg::dev::StiffArgs S{};
   S.el = med_args(el);
   S.ac = med_args(ac);
@@ -369,6 +379,7 @@ template <int E>
 void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
                         cudaStream_t s, int variant) {
   if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s, variant);
+  else if (el.aniso) launch_stiffness_E<E, 2>(h, el, ac, step, s, variant);
   else launch_stiffness_E<E, 0>(h, el, ac, step, s, variant);
 }
 
@@ -634,14 +645,19 @@ void autotune(sfg_handle *h) {
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
+  if (h->el.aniso && h->variant == 2) h->variant = 1;
+  if (h->el.aniso && h->variant == 4) h->variant = 3;
   std::vector<std::pair<int, int>> cand;
   if (h->asmb.nshots > 1) {
     for (int v : {1, 3})
       if (!fix_v || v == h->variant) cand.push_back({v, 16});
   } else {
-    for (int v : {1, 2, 3, 4})
+    for (int v : {1, 2, 3, 4}) {
+      // an anisotropic medium has the colour-pass and owner-computes kernels only
+      if (h->el.aniso && (v == 2 || v == 4)) continue;
       for (int e : {8, 16, 32})
         if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
+    }
   }
   if (cand.empty()) cand.push_back({h->variant, h->epb});
   if (cand.size() > 1) {
@@ -703,8 +719,8 @@ void finish_create(sfg_handle *h) {
   h->asmb.nstep = h->opt.nstep;
   h->asmb.nsb = h->opt.nstep_between_samples;
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
-  if (h->asmb.nshots > 1 && (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0))
-    throw std::runtime_error("batched shots (nshots > 1) need a single elastic medium");
+  if (h->asmb.nshots > 1 && (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0 || h->asmb.el.aniso))
+    throw std::runtime_error("batched shots (nshots > 1) need a single isotropic elastic medium");
 }
 
 // ---------------------------------------------------------------------------
@@ -776,6 +792,7 @@ int sfg_create2d(const sfg_mesh2d_desc *d, const sfg_options *opt, sfg_handle **
     m.mat_rho.assign(d->mat_rho, d->mat_rho + d->numat);
     m.mat_vp.assign(d->mat_vp, d->mat_vp + d->numat);
     m.mat_vs.assign(d->mat_vs, d->mat_vs + d->numat);
+    if (d->mat_aniso) m.mat_aniso.assign(d->mat_aniso, d->mat_aniso + 6 * size_t(d->numat));
     const size_t np = size_t(d->nspec) * sfg::NPTS;
     if (d->point_rho) m.prho.assign(d->point_rho, d->point_rho + np);
     if (d->point_vp) m.pvp.assign(d->point_vp, d->point_vp + np);
@@ -918,6 +935,12 @@ int sfg_initialize(sfg_handle *h) {
     sfg::Assembly2D &a = h->asmb;
     if (!h->have_sources) sfg::set_sources2d(h->mesh, a, {});
     if (!h->have_receivers) { a.nrec = 0; a.ntypes = 1; a.types = {0}; }
+    if (a.el.aniso)
+      for (int t : a.types)
+        if (t == SFG_SEIS_PRESSURE) {
+          h->err = "pressure seismograms are defined for isotropic media only";
+          return int(SFG_ERR_UNSUPPORTED);
+        }
     a.nsig = (a.nstep + a.nsb - 1) / a.nsb;
     SFG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     SFG_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -1310,7 +1333,7 @@ namespace {
 int adjoint_checks(sfg_handle *h) {
   if (!h->initialized) { h->err = "sfg_initialize first"; return SFG_ERR_STATE; }
   const sfg::Assembly2D &a = h->asmb;
-  if (h->ac.nspec || !h->el.nspec || h->el.ncomp != 2 || h->el.S != 1 || a.nsb != 1 ||
+  if (h->ac.nspec || !h->el.nspec || h->el.ncomp != 2 || h->el.aniso || h->el.S != 1 || a.nsb != 1 ||
       a.ntypes != 1 || a.types[0] != SFG_SEIS_DISPLACEMENT) {
     h->err = "the adjoint needs one elastic P-SV medium, one shot, and displacement seismograms "
              "sampled every step";

@@ -50,6 +50,9 @@ class Mesh:
     coupled_pairs: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), np.int32))
     nx: int = 0
     nz: int = 0
+    # optional [numat][6] anisotropic constants (c11, c13, c15, c33, c35, c55);
+    # NaN rows are isotropic materials
+    mat_aniso: np.ndarray | None = None
 
 
 def structured_mesh(nx, nz, xmin, xmax, zmin, zmax, row_material, materials,

@@ -38,6 +38,7 @@ class MeshDesc(C.Structure):
         ("nabs", C.c_int), ("abs_ispec", _ip), ("abs_type", _ip),
         ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
         ("elastic_wave", C.c_int),
+        ("mat_aniso", _dp),
     ]
 
 
@@ -198,6 +199,10 @@ class Simulation2D:
         d.free_ispec = self._k(_arr(m.free_ispec, np.int32)).ctypes.data_as(_ip)
         d.free_type = self._k(_arr(m.free_type, np.int32)).ctypes.data_as(_ip)
         d.elastic_wave = wave
+        aniso = getattr(m, "mat_aniso", None)
+        if aniso is not None:
+            aniso = _arr(aniso, np.float64).reshape(len(m.mat_rho), 6)
+            d.mat_aniso = self._k(np.ascontiguousarray(aniso)).ctypes.data_as(_dp)
         return d
 
     def _check(self, rc):

@@ -30,6 +30,7 @@ FIXTURES = {
     "AcousticElasticCoupledDomainVariant2": ("BXX", "BXZ"),
     "HomogeneousElasticDomainMomentTensor": ("BXX", "BXZ"),
     "HomogeneousElasticIsotropicDomainSH": ("BXY",),
+    "HomogeneousElasticAnisotropicDomain": ("BXX", "BXZ"),
 }
 
 
@@ -61,7 +62,8 @@ def make(ref_root: str, name: str, comps) -> str:
         rec_x=case.rec_x, rec_z=case.rec_z, dt=case.dt, nstep=case.nstep, rec_angle=case.rec_angle,
         stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces["semd"],
         **{f"traces_{k}": v for k, v in traces.items() if k != "semd"},
-        trace_t0=t0, components=np.asarray(comps), elastic_sh=int(case.elastic_sh))
+        trace_t0=t0, components=np.asarray(comps), elastic_sh=int(case.elastic_sh),
+        **({"mat_aniso": m.mat_aniso} if getattr(m, "mat_aniso", None) is not None else {}))
     return out
 
 

@@ -1,0 +1,88 @@
+"""Edge cases of the 2D path against the oracle: no sources, no receivers,
+sampling every n steps, rotated receivers, a source on a mesh node shared by
+four elements and receivers on element edges, several sources in one
+element; tolerances as in test_gpu_parity (1e-5 relative L2 for elastic
+displacement and velocity)."""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from conftest import product_run, rel_l2, workload_case
+
+pytestmark = pytest.mark.gpu
+
+
+def elastic(nstep=500):
+    from specfempp_b200 import meshgen
+    return meshgen.elastic_psv_80x60(nstep=nstep)
+
+
+def test_no_sources_stays_at_rest(sfg_lib):
+    from specfempp_b200 import sfg
+    w = elastic(100)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=100)
+    sim.set_sources([])
+    sim.set_receivers(w.rec_x, w.rec_z, types=("displacement", "velocity", "acceleration"))
+    sim.initialize()
+    sim.run(100)
+    assert not np.any(sim.seismograms())
+    assert not np.any(sim.field("elastic"))
+
+
+def test_no_receivers(sfg_lib):
+    from specfempp_b200 import sfg
+    w = elastic(100)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=100)
+    sim.set_sources(w.sources)
+    sim.initialize()
+    sim.run(100)
+    assert sim.seismograms().size == 0
+    assert np.abs(sim.field("elastic")).max() > 0
+
+
+@pytest.mark.parametrize("nsb", [2, 7])
+def test_sampling_every_n_steps(sfg_lib, oracle_lib, nsb):
+    from oracle import runner
+    w = elastic()
+    case = workload_case(w, types=("displacement", "velocity"))
+    case.nstep_between_samples = nsb
+    ref = runner.run(case, "f32", nthreads=1)["seis"]
+    _, seis = product_run(case, types=case.seis_types)
+    assert seis.shape[0] == (case.nstep + nsb - 1) // nsb
+    for t in range(2):
+        assert rel_l2(seis[:, t], ref[:, t]) <= 1e-5
+
+
+def test_rotated_receivers(sfg_lib, oracle_lib):
+    from oracle import runner
+    w = elastic()
+    case = workload_case(w, types=("displacement",))
+    case.rec_angle = 30.0
+    ref = runner.run(case, "f32", nthreads=1)["seis"]
+    _, seis = product_run(case, types=case.seis_types)
+    assert rel_l2(seis, ref) <= 1e-5
+    case.rec_angle = 0.0
+    _, plain = product_run(case, types=case.seis_types)
+    c, s = np.cos(np.pi / 6), np.sin(np.pi / 6)
+    rot = np.stack([c * plain[..., 0] - s * plain[..., 1], s * plain[..., 0] + c * plain[..., 1]], -1)
+    assert rel_l2(seis, rot) <= 1e-6
+
+
+def test_source_on_node_receivers_on_edges_several_sources_per_element(sfg_lib, oracle_lib):
+    from oracle import runner
+    w = elastic()
+    h = 4000.0 / 80
+    s0 = w.sources[0]
+    srcs = [replace(s0, x=40 * h, z=50 * h),                       # node shared by four elements
+            replace(s0, x=30.2 * h, z=20.5 * h, factor=0.7 * s0.factor, angle=25.0),
+            replace(s0, x=30.7 * h, z=20.3 * h, factor=-0.4 * s0.factor, f0=12.0)]   # same element
+    case = workload_case(w, types=("displacement", "velocity"))
+    case.sources = srcs
+    case.rec_x = np.array([10 * h, 25.5 * h, 61 * h, 70 * h])
+    case.rec_z = np.array([55.25 * h, 57 * h, 40 * h, 12 * h])               # on edges and a node
+    ref = runner.run(case, "f32", nthreads=1)["seis"]
+    _, seis = product_run(case, types=case.seis_types)
+    assert np.abs(ref).max() > 0
+    for t in range(2):
+        assert rel_l2(seis[:, t], ref[:, t]) <= 1e-5, (t, rel_l2(seis[:, t], ref[:, t]))

@@ -20,7 +20,7 @@ pytestmark = pytest.mark.gpu
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
-            "HomogeneousElasticIsotropicDomainSH"]
+            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain"]
 
 
 def tolerance(kind, f32, f64):
@@ -163,7 +163,8 @@ def test_owner_computes_variants_equal_colour_passes(sfg_lib, name, variant):
     assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
 
 
-@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH"])
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH",
+                                  "HomogeneousElasticAnisotropicDomain"])
 def test_moment_tensor_and_sh_all_types(sfg_lib, oracle_lib, name):
     """Moment-tensor source (P-SV) and SH: displacement, velocity and
     acceleration against the oracle (tolerances above) and against the
@@ -210,3 +211,42 @@ def test_step_io_matches_run(sfg_lib):
         else:
             assert np.array_equal(got, a)
         assert np.all(np.isfinite(sim.field("elastic")))
+
+
+def test_anisotropic_layered_parity(sfg_lib, oracle_lib):
+    """Tilted anisotropic half (c15, c35 != 0) under an isotropic half, Stacey
+    on three sides: displacement and velocity against the oracle at 1e-5,
+    acceleration at the FP32 noise tolerance; the owner-computes kernel gives
+    the colour passes' bits."""
+    from oracle import runner
+    from test_oracle import layered_aniso_case
+    case = layered_aniso_case(1200)
+    types = ("displacement", "velocity", "acceleration")
+    case.seis_types = list(types)
+    ref = runner.run(case, "f32", nthreads=1)["seis"]
+    ref64 = runner.run(case, "f64", nthreads=8)["seis"]
+    sim, seis = product_run(case, types=types, variant=1)
+    assert sim.info().kernel_variant == 1
+    for t, kind in enumerate(types):
+        tol = 1e-5 if kind != "acceleration" else tolerance(kind, ref[:, t], ref64[:, t])
+        assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
+    for v in (0, 2, 3, 4):
+        _, s2 = product_run(case, types=types, variant=v)
+        assert np.array_equal(s2, seis), v
+
+
+def test_anisotropic_unsupported_forms(sfg_lib):
+    """The anisotropic medium is P-SV only: elastic pressure seismograms, SH,
+    batched shots and the adjoint are refused with SFG_ERR_UNSUPPORTED."""
+    from specfempp_b200 import sfg
+    from test_oracle import layered_aniso_case
+    case = layered_aniso_case(10)
+    sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10)
+    sim.set_sources(case.sources)
+    sim.set_receivers(case.rec_x, case.rec_z, 0.0, ("pressure",))
+    with pytest.raises(sfg.SfgError, match="isotropic"):
+        sim.initialize()
+    with pytest.raises(sfg.SfgError):
+        sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10, elastic_wave="sh")
+    with pytest.raises(sfg.SfgError):
+        sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10, nshots=4)

@@ -17,7 +17,7 @@ from conftest import golden_case, reference_metric
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
-            "HomogeneousElasticIsotropicDomainSH"]
+            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -32,7 +32,8 @@ def test_oracle_matches_golden_traces(oracle_lib, name):
     assert err.max() < 5e-4                               # observed margin: <= 2e-4
 
 
-@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH"])
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainMomentTensor", "HomogeneousElasticIsotropicDomainSH",
+                                  "HomogeneousElasticAnisotropicDomain"])
 @pytest.mark.parametrize("kind,key", [("velocity", "traces_semv"), ("acceleration", "traces_sema")])
 def test_oracle_matches_golden_velocity_acceleration(oracle_lib, name, kind, key):
     """Velocity and acceleration traces of the moment-tensor (P-SV) and SH
@@ -47,6 +48,46 @@ def test_oracle_matches_golden_velocity_acceleration(oracle_lib, name, kind, key
     err = reference_metric(r["seis"][:, 0], traces)
     assert np.all(np.isfinite(err))
     assert err.max() < 1e-3, err
+
+
+def layered_aniso_case(nstep, tilt=True):
+    """80 x 60 elastic P-SV mesh (Stacey left/right/bottom): an anisotropic
+    lower half (c15, c35 != 0 when ``tilt``) under the isotropic upper half."""
+    from oracle import runner
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_psv_80x60(nstep=nstep)
+    rho, vp, vs = 2200.0, 2500.0, 1445.0
+    l2m, mu = rho * vp * vp, rho * vs * vs
+    mesh = meshgen.structured_mesh(80, 60, 0.0, 4000.0, 0.0, 3000.0,
+                                   np.r_[np.zeros(30, np.int32), np.ones(30, np.int32)],
+                                   [(1, rho, vp, vs), (1, rho, vp, vs)],
+                                   absorbing=("bottom", "right", "left"), free_surface=())
+    c = [1.15 * l2m, l2m - 2 * mu, 0.12 * mu, l2m, -0.09 * mu, mu] if tilt else [l2m, l2m - 2 * mu, 0.0, l2m, 0.0, mu]
+    mesh.mat_aniso = np.array([c, [np.nan] * 6])
+    src = [runner.Source(x=2000.0, z=1300.0, f0=10.0, factor=1e10),
+           runner.Source(x=1200.0, z=2500.0, f0=10.0, factor=1e10, angle=30.0)]
+    return runner.Case2D(mesh=mesh, sources=src, rec_x=w.rec_x, rec_z=np.r_[np.full(3, 2800.0), np.full(2, 1000.0)],
+                         dt=w.dt, nstep=nstep)
+
+
+def test_oracle_aniso_isotropic_constants_equal_isotropic(oracle_lib):
+    """Isotropic constants written as an anisotropic material reproduce the
+    isotropic medium (same stress up to FP32 rounding of lambda + 2 mu)."""
+    from oracle import runner
+    case = layered_aniso_case(500, tilt=False)
+    a = runner.run(case, "f32", nthreads=4)["seis"]
+    case.mesh.mat_aniso = None
+    b = runner.run(case, "f32", nthreads=4)["seis"]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-5
+
+
+def test_oracle_aniso_tilt_changes_wavefield(oracle_lib):
+    """c15 / c35 enter the stress: the tilted medium differs from the
+    untilted one by far more than rounding."""
+    from oracle import runner
+    a = runner.run(layered_aniso_case(700, tilt=True), "f32", nthreads=4)["seis"]
+    b = runner.run(layered_aniso_case(700, tilt=False), "f32", nthreads=4)["seis"]
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) > 1e-2
 
 
 def test_oracle_fp32_vs_fp64_small(oracle_lib):
