@@ -152,7 +152,8 @@ def test_step_and_run_agree(sfg_lib):
     assert np.array_equal(a, sim.seismograms()[0])
 
 
-@pytest.mark.parametrize("name", ["HomogeneousAcousticDomainDirichletBC", "HomogeneousElasticDomainStaceyBC"])
+@pytest.mark.parametrize("name", ["HomogeneousAcousticDomainDirichletBC", "HomogeneousElasticDomainStaceyBC",
+                                  "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticDomainMomentTensor"])
 @pytest.mark.parametrize("variant", [3, 4])
 def test_owner_computes_variants_equal_colour_passes(sfg_lib, name, variant):
     """Single-medium fixtures: the owner-computes kernels (plain and with
