@@ -11,8 +11,9 @@ One bench step = one time step of the whole model.  Reported keys:
           on the handle's stream, summed over the K steps, max over ranks;
 * e2e:    the same metric through the per-step C-ABI call with host buffers
           (STF row host->device, seismogram row device->host, a sync per step);
-* roofline: the dominant kernel (elastic stiffness, all colour passes of one
-          step) against the measured HBM bandwidth;
+* roofline: the dominant kernel (the element kernel of one step: one
+          owner-computes launch, or the colour passes, whichever the autotuner
+          chose) against the measured HBM bandwidth;
 * cpu_baseline: the CPU oracle (a C++ restatement of the reference) on all
           host cores, bounded sample of the same workload.
 ``--impl reference`` times that CPU implementation alone on the same
@@ -446,7 +447,7 @@ def main():
     if tr and tr.get("workload") == args.workload:
         traffic = tr.get("stiffness_bytes_per_launch")
     step_bytes = STEP_B_GLOB * nglob + STEP_B_LOCAL * inf.nspec * 25
-    kname = ("element kernel, one owner-computes launch of one step" if inf.kernel_variant == 3 else
+    kname = ("element kernel, one owner-computes launch of one step" if inf.kernel_variant >= 3 else
              f"element kernel, all {inf.ncolors_elastic} colour launches of one step")
     roofline = {"bound": "hbm", "kernel": f"{kname} (variant {inf.kernel_variant}, "
                                           f"{inf.elements_per_block} elements/block, both media)",

@@ -180,6 +180,12 @@ int sfg_get_field(sfg_handle *h, int medium, int which, float *out, size_t count
  * and the per-medium index of each global point (-1 if absent). */
 int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *glob_to_elastic,
                       int *glob_to_acoustic);
+/* Coordinates x, z and |J| of every element GLL point [nspec][25] (database
+ * element order, point q = iz*5 + ix; FP64) and the medium of every element
+ * (SFG_MEDIUM_*); any pointer may be NULL.  What the reference's kernel and
+ * wavefield writers take from its mesh (include/io/impl/medium_writer.tpp,
+ * include/io/wavefield/writer.tpp). */
+int sfg_get_geometry(sfg_handle *h, double *x, double *z, double *jac, int *medium);
 /* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
 int sfg_check_finite(sfg_handle *h);
 

@@ -1243,6 +1243,16 @@ int sfg_get_numbering(sfg_handle *h, int *ibool_global, int *g2e, int *g2a) {
   return SFG_OK;
 }
 
+int sfg_get_geometry(sfg_handle *h, double *x, double *z, double *jac, int *medium) {
+  if (!h) return SFG_ERR_ARG;
+  const sfg::Assembly2D &a = h->asmb;
+  if (x) std::copy(a.gx.begin(), a.gx.end(), x);
+  if (z) std::copy(a.gz.begin(), a.gz.end(), z);
+  if (jac) std::copy(a.jac_d.begin(), a.jac_d.end(), jac);
+  if (medium) std::copy(a.mesh_medium.begin(), a.mesh_medium.end(), medium);
+  return SFG_OK;
+}
+
 int sfg_check_finite(sfg_handle *h) {
   if (!h || !h->initialized) return 0;
   int f = 0;

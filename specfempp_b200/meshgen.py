@@ -270,6 +270,45 @@ def gll_coordinates(mesh: Mesh):
     return cz @ s.T, cx @ s.T
 
 
+GLL_NODES = np.array([-1.0, -np.sqrt(3.0 / 7.0), 0.0, np.sqrt(3.0 / 7.0), 1.0])
+GLL_WEIGHTS = np.array([0.1, 49.0 / 90.0, 32.0 / 45.0, 49.0 / 90.0, 0.1])
+
+
+def _shape2d(ngnod: int, xi, ga):
+    """Shape functions and their xi / gamma derivatives [..., ngnod] of the
+    4-node bilinear and 9-node biquadratic quadrilaterals (node order: corners
+    counter-clockwise from (-1, -1), then the edge mid-points, then the centre)."""
+    if ngnod == 4:
+        s = np.stack([0.25 * (xi - 1) * (ga - 1), -0.25 * (xi + 1) * (ga - 1),
+                      0.25 * (xi + 1) * (ga + 1), -0.25 * (xi - 1) * (ga + 1)], -1)
+        dx = np.stack([0.25 * (ga - 1), -0.25 * (ga - 1), 0.25 * (ga + 1), -0.25 * (ga + 1)], -1)
+        dg = np.stack([0.25 * (xi - 1), -0.25 * (xi + 1), 0.25 * (xi + 1), -0.25 * (xi - 1)], -1)
+        return s, dx, dg
+    lx = [0.5 * xi * (xi - 1), 1 - xi * xi, 0.5 * xi * (xi + 1)]
+    lg = [0.5 * ga * (ga - 1), 1 - ga * ga, 0.5 * ga * (ga + 1)]
+    dlx = [xi - 0.5, -2 * xi, xi + 0.5]
+    dlg = [ga - 0.5, -2 * ga, ga + 0.5]
+    ix = [0, 2, 2, 0, 1, 2, 1, 0, 1]
+    ig = [0, 0, 2, 2, 0, 1, 2, 1, 1]
+    s = np.stack([lx[a] * lg[b] for a, b in zip(ix, ig)], -1)
+    dx = np.stack([dlx[a] * lg[b] for a, b in zip(ix, ig)], -1)
+    dg = np.stack([lx[a] * dlg[b] for a, b in zip(ix, ig)], -1)
+    return s, dx, dg
+
+
+def gll_geometry(mesh):
+    """(x, z, |J|) of every element GLL point [nspec, 25] (point q = iz*5 + ix)
+    for 4- and 9-node meshes (FP64)."""
+    GA, XI = np.meshgrid(GLL_NODES, GLL_NODES, indexing="ij")      # [iz, ix]
+    s, dx, dg = (a.reshape(25, -1) for a in _shape2d(int(mesh.ngnod), XI, GA))
+    kn = np.asarray(mesh.knods).reshape(int(mesh.nspec), int(mesh.ngnod))
+    cx = np.asarray(mesh.coorg)[kn, 0]
+    cz = np.asarray(mesh.coorg)[kn, 1]
+    x, z = cx @ s.T, cz @ s.T
+    jac = (cx @ dx.T) * (cz @ dg.T) - (cx @ dg.T) * (cz @ dx.T)
+    return x, z, jac
+
+
 def elastic_grf_1000x500(nstep: int = 3000, nshots: int = 32, nrec: int = 400,
                          nx: int = 1000, nz: int = 500, seed: int = 0) -> Workload:
     xmax, zmax = 25.0 * nx, 25.0 * nz

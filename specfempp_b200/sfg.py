@@ -87,6 +87,7 @@ EXPORTS = {
     "sfg_get_seismograms": ([C.c_void_p, _fp, C.c_size_t], C.c_int),
     "sfg_get_field": ([C.c_void_p, C.c_int, C.c_int, _fp, C.c_size_t], C.c_int),
     "sfg_get_numbering": ([C.c_void_p, _ip, _ip, _ip], C.c_int),
+    "sfg_get_geometry": ([C.c_void_p, _dp, _dp, _dp, _ip], C.c_int),
     "sfg_check_finite": ([C.c_void_p], C.c_int),
     "sfg_set_model2d": ([C.c_void_p, _fp, _fp, _fp], C.c_int),
     "sfg_forward_checkpointed": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
@@ -300,6 +301,16 @@ class Simulation2D:
         self._check(self.lib.sfg_get_numbering(self.h, ib.ctypes.data_as(_ip), g2e.ctypes.data_as(_ip),
                                                g2a.ctypes.data_as(_ip)))
         return ib.reshape(i.nspec, 25), g2e, g2a
+
+    def geometry(self):
+        """(x, z, |J|) of every element GLL point [nspec, 25] (database element
+        order, FP64) and the medium of every element (0 acoustic, 1 elastic)."""
+        n = self.info().nspec
+        x, z, jac = (np.zeros((n, 25)) for _ in range(3))
+        med = np.zeros(n, np.int32)
+        self._check(self.lib.sfg_get_geometry(self.h, x.ctypes.data_as(_dp), z.ctypes.data_as(_dp),
+                                              jac.ctypes.data_as(_dp), med.ctypes.data_as(_ip)))
+        return x, z, jac, med
 
     def check_finite(self) -> bool:
         rc = self.lib.sfg_check_finite(self.h)

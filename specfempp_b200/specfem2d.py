@@ -5,7 +5,10 @@
 Reads the reference's ``specfem_config.yaml`` (forward, Newmark), its
 ``database.bin`` (xmeshfem2D output), ``sources.yaml`` and ``STATIONS``, runs
 the time loop on the GPU through libsfg, and writes the seismograms as the
-reference's ASCII traces (``NET.STA.S2.BXX.semd`` ...).  This mirrors the
+reference's ASCII traces (``NET.STA.S2.BXX.semd`` ...), and, when the
+configuration has a wavefield writer, the forward wavefield every
+``time-interval`` steps and at the last step in the reference's
+``ForwardWavefield`` layout (ASCII or NPY).  This mirrors the
 reference's ``specfem2d -p <config>`` program (src/specfem2d.cpp,
 core/specfem/program) for the forward 2D path.
 """
@@ -31,8 +34,34 @@ def run_config(config: str, root: str | None = None, output_directory: str | Non
     sim.set_receivers(rx, rz, angle=cfg.angle, types=tuple(cfg.seismogram_types))
     sim.initialize()
     setup_s = time.perf_counter() - t
+    writer = None
+    if cfg.wavefield_directory is not None:
+        wdir = cfg.wavefield_directory
+        if not os.path.isabs(wdir):
+            wdir = os.path.join(root or os.getcwd(), wdir)
+        if not os.path.isdir(wdir):
+            raise FileNotFoundError(f"Output folder : {wdir} does not exist.")
+        writer = io.WavefieldWriter(wdir, sim, library=cfg.wavefield_format)
+        writer.initialize()
     t = time.perf_counter()
-    sim.run(cfg.nstep)
+    written = []
+    if writer is not None and cfg.wavefield_interval > 0:
+        # snapshots after every time_interval steps (periodic_task.hpp:59-69)
+        done = 0
+        while done < cfg.nstep:
+            n = min(cfg.wavefield_interval - done % cfg.wavefield_interval, cfg.nstep - done)
+            sim.run(n)
+            done += n
+            if done % cfg.wavefield_interval == 0:
+                writer.write(done)
+                written.append(done)
+    else:
+        sim.run(cfg.nstep)
+    if writer is not None:
+        if cfg.wavefield_last_step and cfg.nstep not in written:
+            writer.write(cfg.nstep)
+            written.append(cfg.nstep)
+        writer.finalize()
     seis = sim.seismograms()[0]
     run_s = time.perf_counter() - t
     inf = sim.info()
@@ -43,7 +72,7 @@ def run_config(config: str, root: str | None = None, output_directory: str | Non
                                        cfg.nstep_between_samples, cfg.elastic_wave)
     sim.close()
     return {"nspec": inf.nspec, "nglob": inf.nglob, "nstep": cfg.nstep, "setup_s": setup_s, "run_s": run_s,
-            "files": len(paths), "output_directory": out_dir}
+            "files": len(paths), "output_directory": out_dir, "wavefield_steps": written}
 
 
 def main(argv=None):

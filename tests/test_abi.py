@@ -118,3 +118,16 @@ def test_3d_create_errors(sfg_lib):
     bad = meshgen.homogeneous_hex_mesh(2, 2, 2, (0, 1000, 0, 1000, -1000, 0), 2700.0, 1000.0, 1732.0)
     with pytest.raises(sfg.SfgError):
         sfg3d.Simulation3D(bad, dt=1e-3, nstep=10)
+
+
+def test_geometry_export(sfg_lib):
+    """sfg_get_geometry: GLL point coordinates and |J| of the library's set-up
+    equal the 4-node shape-function geometry; media per element."""
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.coupled_400x200(nstep=10, nx=40, nz=20)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=10)
+    x, z, jac, med = sim.geometry()
+    gx, gz, gj = meshgen.gll_geometry(w.mesh)
+    assert np.allclose(x, gx, rtol=0, atol=1e-6) and np.allclose(z, gz, rtol=0, atol=1e-6)
+    assert np.allclose(jac, gj, rtol=1e-12)
+    assert np.array_equal(med, np.asarray(w.mesh.mat_medium)[w.mesh.kmato])

@@ -200,3 +200,25 @@ def test_checkpointed_forward_equals_plain_run(problem, interval):
     plain = sim.seismograms()[0, :, 0].copy()
     ck = sim.forward_checkpointed(NSTEP, interval)
     assert np.array_equal(plain, ck)
+
+
+def test_kernel_files_from_the_gradient(problem, tmp_path):
+    """Relative kernels from the gradient, written in the reference's Kernels
+    layout: sum of W K_m dln(m) equals the gradient's directional derivative
+    along m dln(m); the NPY files read back to the kernels."""
+    from specfempp_b200 import io, meshgen
+    w, sim, model, weights = problem
+    g = [a.astype(np.float64) for a in gradient(sim, model, weights, 50)]
+    x, z, jac, med = sim.geometry()
+    k = io.isotropic_kernels(*model, *g, jac)
+    W = np.outer(meshgen.GLL_WEIGHTS, meshgen.GLL_WEIGHTS).ravel() * jac
+    d = bump(w.mesh, 2000.0, 2650.0, 250.0)
+    for name, which in (("rho", 0), ("kappa", 1), ("mu", 2)):
+        lhs = float((W * k[name] * d).sum())
+        rhs = float((g[which] * model[which] * d).sum())
+        assert abs(lhs - rhs) <= 1e-9 * abs(rhs), name
+    root = io.write_kernels(str(tmp_path), sim, k, library="npy")
+    for name in ("rho", "kappa", "mu", "rhop", "alpha", "beta"):
+        flat, dims = io.read_dataset(f"{root}/elastic_psv_isotropic", name)
+        assert dims == [w.mesh.nspec, 5, 5]
+        assert np.array_equal(io.from_element_order(flat), k[name].astype(np.float32)), name

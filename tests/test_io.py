@@ -42,3 +42,129 @@ def test_ascii_writer_format(tmp_path):
     assert np.allclose(a[:, 1], seis[:, 1, 1, 1], rtol=1e-6)
     line = open(os.path.join(tmp_path, "AA.S0001.S2.BXX.semd")).readline()
     assert line == f"{-0.12:e} {0.0:e}\n"
+
+
+def test_dataset_ascii_and_npy_layouts(tmp_path):
+    """ASCII: <name>.meta ("rank R", "dims d0 d1 ") and one %.10e value per
+    line with sub-normal magnitudes written as 0; NPY: Fortran-order header
+    with the dataset's dims.  Both read back."""
+    from specfempp_b200 import io
+    vals = np.array([1.5, -2.25e-3, 1e-42, 3.0e7, 0.0, 7.0], np.float32)
+    p = io.write_dataset(str(tmp_path), "A", vals, (3, 2), "ascii")
+    assert open(tmp_path / "A.meta").read() == "rank 2\ndims 3 2 \n"
+    lines = open(p).read().splitlines()
+    assert lines[0] == "1.5000000000e+00" and lines[1] == "-2.2499999031e-03"
+    assert lines[2] == "0.0000000000e+00"
+    back, dims = io.read_dataset(str(tmp_path), "A")
+    assert dims == [3, 2] and np.array_equal(back, np.where(np.abs(vals) < 1.2e-38, 0, vals))
+    io.write_dataset(str(tmp_path), "B", vals, (3, 2), "npy")
+    arr = np.load(tmp_path / "B.npy")
+    assert arr.shape == (3, 2) and np.array_equal(arr, vals.reshape(2, 3).T)   # Fortran order
+    back, dims = io.read_dataset(str(tmp_path), "B")
+    assert dims == [3, 2] and np.array_equal(back, vals)
+    io.write_dataset(str(tmp_path), "C", np.array([True]), (1,), "ascii")
+    assert open(tmp_path / "C.txt").read() == "1\n"
+
+
+def test_kernel_writer_layout_and_formulas(tmp_path):
+    """Kernels/<group>/{X, Z, rho, mu, kappa, rhop, alpha, beta}, dims [n][5][5],
+    element-tiled order; the derived kernels follow Tromp et al. 2005 Eq. 20."""
+    from specfempp_b200 import io, meshgen
+    w = meshgen.elastic_psv_80x60(nstep=10)
+    m = w.mesh
+    x, z, jac = meshgen.gll_geometry(m)
+    rng = np.random.default_rng(3)
+    shape = (m.nspec, 25)
+    rho = np.full(shape, 2200.0)
+    kappa, mu = rho * (2500.0 ** 2 - 4 / 3 * 1445.0 ** 2), rho * 1445.0 ** 2
+    g = [rng.standard_normal(shape) for _ in range(3)]
+    k = io.isotropic_kernels(rho, kappa, mu, *g, jac)
+    W = np.outer(meshgen.GLL_WEIGHTS, meshgen.GLL_WEIGHTS).ravel() * jac
+    assert np.allclose(k["mu"] * W, mu * g[2])
+    assert np.allclose(k["rhop"], k["rho"] + k["kappa"] + k["mu"])
+    assert np.allclose(k["alpha"], 2 * (1 + 4 / 3 * mu / kappa) * k["kappa"])
+    assert np.allclose(k["beta"], 2 * (k["mu"] - 4 / 3 * mu / kappa * k["kappa"]))
+    for lib in ("ascii", "npy"):
+        root = io.write_kernels(str(tmp_path / lib), m, k, library=lib)
+        grp = os.path.join(root, "elastic_psv_isotropic")
+        names = sorted(f.split(".")[0] for f in os.listdir(grp) if not f.endswith(".meta"))
+        assert names == sorted(["X", "Z", "rho", "mu", "kappa", "rhop", "alpha", "beta"])
+        flat, dims = io.read_dataset(grp, "X")
+        assert dims == [m.nspec, 5, 5]
+        assert np.allclose(io.from_element_order(flat), x, rtol=1e-6)
+        flat, _ = io.read_dataset(grp, "beta")
+        assert np.allclose(io.from_element_order(flat), k["beta"].astype(np.float32), rtol=1e-6, atol=0)
+
+
+class _FakeSim:
+    """numbering() and field() of a handle over a mesh, without a GPU."""
+
+    def __init__(self, mesh):
+        from specfempp_b200 import meshgen
+        x, z, _ = meshgen.gll_geometry(mesh)
+        key = np.round(np.stack([x.ravel(), z.ravel()], -1), 6)
+        _, ib = np.unique(key, axis=0, return_inverse=True)
+        self.ib = ib.reshape(mesh.nspec, 25).astype(np.int32)
+        self.n = int(self.ib.max()) + 1
+        self.ncomp = 2
+
+    def numbering(self):
+        g = np.arange(self.n, dtype=np.int32)
+        return self.ib, g, np.full(self.n, -1, np.int32)
+
+    def field(self, medium, which):
+        k = {"displacement": 1.0, "velocity": 2.0, "acceleration": 3.0}[which]
+        return (k * np.arange(self.n * 2, dtype=np.float32)).reshape(self.n, 2)
+
+
+def test_wavefield_writer_layout(tmp_path):
+    """ForwardWavefield/Coordinates/<medium>/{X, Z, mapping},
+    Step<6 digits>/<medium>/{Displacement, Velocity, Acceleration} in
+    LayoutLeft order, BoundaryValues/save_boundary_values."""
+    from specfempp_b200 import io, meshgen
+    m = meshgen.elastic_psv_80x60(nstep=10).mesh
+    sim = _FakeSim(m)
+    x, _, _ = meshgen.gll_geometry(m)
+    for lib in ("ascii", "npy"):
+        wr = io.WavefieldWriter(str(tmp_path / lib), sim, m, library=lib)
+        wr.initialize()
+        wr.write(100)
+        wr.finalize()
+        coords = os.path.join(wr.root, "Coordinates", "elastic_psv")
+        mp, dims = io.read_dataset(coords, "mapping")
+        assert dims == [m.nspec, 5, 5]
+        mp = mp.reshape(5, 5, m.nspec).transpose(2, 1, 0).reshape(m.nspec, 25).astype(int)   # LayoutLeft
+        px, _ = io.read_dataset(coords, "X")
+        assert np.allclose(px[mp], x, rtol=1e-6)
+        d, dims = io.read_dataset(os.path.join(wr.root, "Step000100", "elastic_psv"), "Velocity")
+        assert dims == [sim.n, 2]
+        assert np.array_equal(d.reshape(2, sim.n).T, sim.field("elastic", "velocity"))
+        b, _ = io.read_dataset(os.path.join(wr.root, "BoundaryValues"), "save_boundary_values")
+        assert b.tolist() == [0]
+
+
+def _with_wavefield_writer(cfg_path, **kw):
+    import yaml
+    with open(cfg_path) as f:
+        cfg = yaml.safe_load(f)
+    cfg["parameters"]["simulation-setup"]["simulation-mode"]["forward"]["writer"]["wavefield"] = kw
+    with open(cfg_path, "w") as f:
+        yaml.safe_dump(cfg, f)
+
+
+def test_config_wavefield_writer_keys(tmp_path):
+    import pytest
+    from specfempp_b200 import io
+    cfg, _ = write_fixture_dir(os.path.join(GOLDEN, "HomogeneousElasticDomain.npz"), str(tmp_path))
+    c = io.read_config(cfg, root=str(tmp_path))
+    assert c.wavefield_directory is None
+    _with_wavefield_writer(cfg, format="NPY", directory="OUT", **{"time-interval": 50})
+    c = io.read_config(cfg, root=str(tmp_path))
+    assert (c.wavefield_directory, c.wavefield_format, c.wavefield_interval, c.wavefield_last_step) == \
+        ("OUT", "npy", 50, True)
+    _with_wavefield_writer(cfg, format="HDF5", directory="OUT")
+    with pytest.raises(ValueError, match="HDF5|hdf5"):
+        io.read_config(cfg, root=str(tmp_path))
+    _with_wavefield_writer(cfg, format="ASCII", directory="OUT", **{"for-adjoint-simulations": True})
+    with pytest.raises(ValueError, match="boundary values"):
+        io.read_config(cfg, root=str(tmp_path))
