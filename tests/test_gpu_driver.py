@@ -37,7 +37,8 @@ def test_driver_wavefield_snapshots(sfg_lib, tmp_path, library):
     """A configuration with a wavefield writer: snapshots after every
     time-interval steps and at the last step, in the ForwardWavefield layout;
     the last snapshot is the field of a plain run of the same model, bit for
-    bit, at every element point."""
+    bit, at every element point (ASCII, like the reference's writer, writes
+    magnitudes below the smallest normal float as 0)."""
     import yaml
     from specfempp_b200 import io, specfem2d, sfg
     from test_io import _with_wavefield_writer
@@ -71,7 +72,10 @@ def test_driver_wavefield_snapshots(sfg_lib, tmp_path, library):
     ib, g2e, _ = sim.numbering()
     u = sim.field("elastic")
     assert np.abs(u).max() > 0
-    assert np.array_equal(d[mp], u[g2e[ib]])
+    want = u[g2e[ib]]
+    if library == "ascii":
+        want = np.where(np.abs(want) < np.finfo(np.float32).tiny, 0.0, want).astype(np.float32)
+    assert np.array_equal(d[mp], want)
     x, _, _, _ = sim.geometry()
     px, _ = io.read_dataset(coords, "X")
     assert np.allclose(px[mp], x, rtol=1e-6)
