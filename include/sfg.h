@@ -189,7 +189,8 @@ int sfg_get_geometry(sfg_handle *h, double *x, double *z, double *jac, int *medi
 /* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
 int sfg_check_finite(sfg_handle *h);
 
-/* ---- adjoint (2D elastic P-SV, one shot, displacement seismograms every step) ----
+/* ---- adjoint (2D isotropic elastic P-SV or SH, one shot, displacement
+ * seismograms every step; in SH the gradient with respect to kappa is zero) ----
  * Replace the model by per-GLL-point rho, kappa, mu ([nspec][25], database
  * element order; kappa = lambda + 2/3 mu as the reference stores it).
  * Reference: the property container, core/specfem/assembly/properties. */

@@ -1,4 +1,5 @@
-"""Model gradients of seismograms through the discrete adjoint (2D elastic P-SV).
+"""Model gradients of seismograms through the discrete adjoint (2D isotropic
+elastic P-SV and SH).
 
 ``SeismogramFunction`` is a ``torch.autograd.Function`` whose forward runs the
 library's checkpointed forward simulation for a per-GLL-point model
@@ -11,9 +12,10 @@ stores the wavefield (include/io/wavefield/writer.tpp), a combined
 adjoint/backward run (core/specfem/solver/time_marching.tpp:133-264) and the
 Frechet kernels (include/medium/dim2/elastic/isotropic/frechet_derivative.hpp)
 — with checkpoints kept in HBM instead of a wavefield file.  The Stacey
-impedances are held at the model they were built from (their dependence on
-the model is not differentiated), as in the reference, whose kernels carry
-no boundary term.
+impedances (rho vp, rho vs) are differentiated with the rest of the model,
+so the gradient is exact on the absorbing edges too (the reference's
+kernels carry no boundary term).  In SH the gradient with respect to kappa
+is zero.
 """
 from __future__ import annotations
 

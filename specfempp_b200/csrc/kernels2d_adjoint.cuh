@@ -29,6 +29,12 @@
 // kernels (include/medium/dim2/elastic/isotropic/frechet_derivative.hpp:55-181)
 // carry the same strain products (its mu bracket is half of the one above and
 // its kappa prefactor is lambda + mu), integrated in time with -dt.
+//
+// SH (one component u_y, sigma = mu grad u_y, Stacey traction -rho vs v):
+// the same sweep with scalar fields; dL/dmu_p += -W_p grad(mu) . grad(u~),
+// kappa does not enter, and of the Stacey sums only A2 and A4 exist (the SH
+// reference kernels: frechet_derivative.hpp:219-278).  Kernels that differ
+// per wave type take NC, the number of components.
 #pragma once
 
 #include "kernels2d.cuh"
@@ -138,9 +144,63 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
   reinterpret_cast<float2 *>(A.seg)[p] = sg;
 }
 
+// SH reverse element step (one component): -K mu with sigma = mu grad,
+// adjoint sources R^T g (first seismogram component, BXY), and the mu term.
+template <int E>
+__global__ void __launch_bounds__(NP * E) k_adj_elem_sh(AdjArgs A) {
+  __shared__ float sm_[E][NP], su_[E][NP];
+  __shared__ float sF[2][E][NP];
+  __shared__ float shp[NP], shpw[NP], sw[NG];
+  const int tid = threadIdx.x;
+  load_quad(A.quad, shp, shpw, sw, tid);
+  const int le = tid / NP, q = tid - le * NP;
+  const int e = blockIdx.x * E + le;
+  const bool act = e < A.nspec;
+  const size_t p = size_t(act ? e : 0) * NP + q;
+  const int g = act ? __ldg(A.ibool + p) : 0;
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float mu = __ldg(A.prop1 + p);
+  sm_[le][q] = act ? A.mu[g] : 0.f;
+  su_[le][q] = act ? A.uf[g] : 0.f;
+  const int rh = act ? __ldg(A.ad_head + e) : -1;
+  __syncthreads();
+  const int iz = q / NG, ix = q - iz * NG;
+  float dm0 = 0.f, dm1 = 0.f, du0 = 0.f, du1 = 0.f;
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    dm0 = fmaf(shp[ix * NG + l], sm_[le][iz * NG + l], dm0);
+    dm1 = fmaf(shp[iz * NG + l], sm_[le][l * NG + ix], dm1);
+    du0 = fmaf(shp[ix * NG + l], su_[le][iz * NG + l], du0);
+    du1 = fmaf(shp[iz * NG + l], su_[le][l * NG + ix], du1);
+  }
+  const float mx = xix * dm0 + gax * dm1, mz = xiz * dm0 + gaz * dm1;
+  const float ux = xix * du0 + gax * du1, uz = xiz * du0 + gaz * du1;
+  const float sx = mu * mx, sz = mu * mz;
+  sF[0][le][q] = jac * (sx * xix + sz * xiz);
+  sF[1][le][q] = jac * (sx * gax + sz * gaz);
+  __syncthreads();
+  if (!act) return;
+  float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    t1 = fmaf(sF[0][le][iz * NG + l], shpw[l * NG + ix], t1);
+    t2 = fmaf(sF[1][le][l * NG + ix], shpw[l * NG + iz], t2);
+  }
+  float r = -(sw[iz] * t1 + sw[ix] * t2);
+  if (rh >= 0) {
+    const float *g_k = A.gtab + size_t(*A.seg_k0 + A.slot) * A.nrec * 2;
+    for (int k = rh; k >= 0; k = A.ad_next[k]) r += g_k[2 * k] * A.ad_h[size_t(k) * NP + q];
+  }
+  A.r[__ldg(A.pslot + p)] = r;
+  const float W = sw[ix] * sw[iz] * jac;
+  A.seg[2 * p + 1] += -W * (mx * ux + mz * uz);
+}
+
 // Per point: lu~ = lu + sum of the element-point results (colour order);
 // G += mu_k . a'_k; then the transposed predictor and mu_(k-1).  lv holds
 // lv~ (Stacey already applied).  One thread per point.
+template <int NC>
 __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float *__restrict__ lv,
                                                   float *__restrict__ mu, float *__restrict__ grho,
                                                   const float *__restrict__ af,
@@ -149,38 +209,42 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
                                                   const int *__restrict__ inv_start, int npts, float dt,
                                                   float dt2, float dtsq2) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += gridDim.x * blockDim.x) {
-    float s0 = 0.f, s1 = 0.f;
+    float s[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) s[c] = 0.f;
     for (int k = inv_start[g]; k < inv_start[g + 1]; ++k) {
-      const float2 t = reinterpret_cast<const float2 *>(r)[k];
-      s0 = s0 + t.x;
-      s1 = s1 + t.y;
+#pragma unroll
+      for (int c = 0; c < NC; ++c) s[c] = s[c] + r[size_t(k) * NC + c];
     }
-    const float2 u = reinterpret_cast<const float2 *>(lu)[g];
-    const float2 v = reinterpret_cast<const float2 *>(lv)[g];
-    const float2 m = reinterpret_cast<const float2 *>(mu)[g];
-    const float2 a = reinterpret_cast<const float2 *>(af)[g];
-    const float2 mi = reinterpret_cast<const float2 *>(minv)[g];
-    grho[g] += m.x * a.x + m.y * a.y;
-    const float lux = u.x + s0, luz = u.y + s1;
-    const float lvx = dt * lux + v.x, lvz = dt * luz + v.y;
-    const float lax = dtsq2 * lux + dt2 * v.x, laz = dtsq2 * luz + dt2 * v.y;
-    reinterpret_cast<float2 *>(lu)[g] = make_float2(lux, luz);
-    reinterpret_cast<float2 *>(lv)[g] = make_float2(lvx, lvz);
-    reinterpret_cast<float2 *>(mu)[g] =
-        make_float2(__fmul_rn(mi.x, __fadd_rn(lax, __fmul_rn(dt2, lvx))),
-                    __fmul_rn(mi.y, __fadd_rn(laz, __fmul_rn(dt2, lvz))));
+    const size_t o = size_t(g) * NC;
+    float ma = mu[o] * af[o];
+    if (NC == 2) ma = ma + mu[o + NC - 1] * af[o + NC - 1];
+    grho[g] += ma;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const float l = lu[o + c] + s[c];
+      const float v = lv[o + c];
+      const float nv = dt * l + v;
+      const float la = dtsq2 * l + dt2 * v;
+      lu[o + c] = l;
+      lv[o + c] = nv;
+      mu[o + c] = __fmul_rn(minv[o + c], __fadd_rn(la, __fmul_rn(dt2, nv)));
+    }
   }
 }
 
 // Start of a recording step (one block): store the predicted velocity v~ of
 // the step at the Stacey points (the step's element kernels read v~ next),
 // then set the step counter to the segment's next step.
+template <int NC>
 __global__ void __launch_bounds__(512) k_record_begin(SegRecord *__restrict__ rec,
                                                       const float *__restrict__ v, int *step) {
   const int i = rec->i, n = rec->nst;
   float *dst = rec->vst + size_t(i) * rec->vstride;
-  for (int j = threadIdx.x; j < n; j += blockDim.x)
-    reinterpret_cast<float2 *>(dst)[j] = reinterpret_cast<const float2 *>(v)[rec->st_pt[j]];
+  for (int j = threadIdx.x; j < n; j += blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) dst[size_t(j) * NC + c] = v[size_t(rec->st_pt[j]) * NC + c];
+  }
   __syncthreads();
   if (threadIdx.x == 0) {
     *step = rec->k0 + i;
@@ -196,31 +260,44 @@ __global__ void __launch_bounds__(512) k_record_begin(SegRecord *__restrict__ re
 //   dL/drvp = -wq j1 (A1 + dt/2 A3),  dL/drvs = -wq j1 (A2 - A1 + dt/2 (A4 - A3))
 // with A1 = (mu.n)(n.v~)/j1^2, A2 = mu.v~, A3 = (nx + nz)/j1^2 sum_c mu_c n_c a'_c,
 // A4 = mu.a'.  The four sums are accumulated per point (acc[4 i + 0..3]).
+template <int NC>
 __device__ __forceinline__ void adj_stacey_grad(const int *__restrict__ lb_g, const int *__restrict__ lb_j,
                                                 const float4 *__restrict__ geo, const float *__restrict__ mu,
                                                 const float *__restrict__ vst, const float *__restrict__ af,
                                                 float *__restrict__ acc, int n, int first, int stride) {
-  for (int i = first; i < n; i += stride) {
-    const int g = lb_g[i];
-    const float4 q = geo[i];
-    const float2 m = reinterpret_cast<const float2 *>(mu)[g];
-    const float2 v = reinterpret_cast<const float2 *>(vst)[lb_j[i]];
-    const float2 a = reinterpret_cast<const float2 *>(af)[g];
-    const float inv = 1.0f / (q.z * q.z);
-    const float mn = m.x * q.x + m.y * q.y, vn = v.x * q.x + v.y * q.y;
-    float4 t = reinterpret_cast<float4 *>(acc)[i];
-    t.x += mn * vn * inv;
-    t.y += m.x * v.x + m.y * v.y;
-    t.z += (q.x + q.y) * inv * (m.x * q.x * a.x + m.y * q.y * a.y);
-    t.w += m.x * a.x + m.y * a.y;
-    reinterpret_cast<float4 *>(acc)[i] = t;
+  if constexpr (NC == 1) {
+    // SH: C = wq j1 rvs, only A2 = mu v~ and A4 = mu a'
+    for (int i = first; i < n; i += stride) {
+      const int g = lb_g[i];
+      const float m = mu[g];
+      float4 t = reinterpret_cast<float4 *>(acc)[i];
+      t.y += m * vst[lb_j[i]];
+      t.w += m * af[g];
+      reinterpret_cast<float4 *>(acc)[i] = t;
+    }
+  } else {
+    for (int i = first; i < n; i += stride) {
+      const int g = lb_g[i];
+      const float4 q = geo[i];
+      const float2 m = reinterpret_cast<const float2 *>(mu)[g];
+      const float2 v = reinterpret_cast<const float2 *>(vst)[lb_j[i]];
+      const float2 a = reinterpret_cast<const float2 *>(af)[g];
+      const float inv = 1.0f / (q.z * q.z);
+      const float mn = m.x * q.x + m.y * q.y, vn = v.x * q.x + v.y * q.y;
+      float4 t = reinterpret_cast<float4 *>(acc)[i];
+      t.x += mn * vn * inv;
+      t.y += m.x * v.x + m.y * v.y;
+      t.z += (q.x + q.y) * inv * (m.x * q.x * a.x + m.y * q.y * a.y);
+      t.w += m.x * a.x + m.y * a.y;
+      reinterpret_cast<float4 *>(acc)[i] = t;
+    }
   }
 }
 
 // Stacey part of the transposed step at the start of a reverse step, one
 // launch: blocks [0, nb_grad) accumulate the impedance terms per
 // element-local boundary point, the others apply lv -= C mu per Stacey point
-// (C symmetric 2x2 per point: xx, xz, zz).
+// (C symmetric 2x2 per point: xx, xz, zz; SH: the scalar in the xx slot).
 struct AdjStaceyArgs {
   const int *lb_g, *lb_j;
   const float4 *geo;
@@ -234,15 +311,20 @@ struct AdjStaceyArgs {
   int nb_grad;
 };
 
+template <int NC>
 __global__ void __launch_bounds__(256) k_adj_stacey(AdjStaceyArgs S) {
   if (int(blockIdx.x) < S.nb_grad) {
-    adj_stacey_grad(S.lb_g, S.lb_j, S.geo, S.mu, S.vst, S.af, S.acc, S.nlb,
+    adj_stacey_grad<NC>(S.lb_g, S.lb_j, S.geo, S.mu, S.vst, S.af, S.acc, S.nlb,
                     blockIdx.x * blockDim.x + threadIdx.x, S.nb_grad * blockDim.x);
     return;
   }
   const int stride = (gridDim.x - S.nb_grad) * blockDim.x;
   for (int j = (blockIdx.x - S.nb_grad) * blockDim.x + threadIdx.x; j < S.nst; j += stride) {
     const int g = S.pt[j];
+    if (NC == 1) {
+      S.lv[g] -= S.cm[3 * j] * S.mu[g];    // SH: C scalar in the xx slot
+      continue;
+    }
     const float mx = S.mu[2 * g], mz = S.mu[2 * g + 1];
     S.lv[2 * g] -= S.cm[3 * j] * mx + S.cm[3 * j + 1] * mz;
     S.lv[2 * g + 1] -= S.cm[3 * j + 1] * mx + S.cm[3 * j + 2] * mz;

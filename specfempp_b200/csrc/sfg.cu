@@ -557,7 +557,10 @@ bool receivers_early(const sfg_handle *h, int medium) {
 
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
-  if (h->recording) sfg::dev::k_record_begin<<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+  if (h->recording) {
+    if (h->el.ncomp == 1) sfg::dev::k_record_begin<1><<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+    else sfg::dev::k_record_begin<2><<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+  }
   // a recorded (recomputed) step's seismograms are those of the forward run
   const bool rec_ac = has_ac && h->ac.nrec > 0 && h->recording != 2;
   const bool rec_el = has_el && h->el.nrec > 0 && h->recording != 2;
@@ -1343,10 +1346,10 @@ namespace {
 int adjoint_checks(sfg_handle *h) {
   if (!h->initialized) { h->err = "sfg_initialize first"; return SFG_ERR_STATE; }
   const sfg::Assembly2D &a = h->asmb;
-  if (h->ac.nspec || !h->el.nspec || h->el.ncomp != 2 || h->el.aniso || h->el.S != 1 || a.nsb != 1 ||
+  if (h->ac.nspec || !h->el.nspec || h->el.aniso || h->el.S != 1 || a.nsb != 1 ||
       a.ntypes != 1 || a.types[0] != SFG_SEIS_DISPLACEMENT) {
-    h->err = "the adjoint needs one elastic P-SV medium, one shot, and displacement seismograms "
-             "sampled every step";
+    h->err = "the adjoint needs one isotropic elastic medium (P-SV or SH), one shot, and displacement "
+             "seismograms sampled every step";
     return SFG_ERR_UNSUPPORTED;
   }
   return SFG_OK;
@@ -1518,17 +1521,26 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   const size_t ob = size_t(b) * A.interval;
   for (int i = n - 1; i >= 0; --i) {
     const size_t sl = ob + size_t(i);
+    const bool sh = D.ncomp == 1;
     if (A.nst && !(last && i == n - 1)) {
       St.vst = A.seg_v + sl * A.vstride;
       St.af = A.seg_a + sl * A.stride;
-      sfg::dev::k_adj_stacey<<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
+      if (sh) sfg::dev::k_adj_stacey<1><<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
+      else sfg::dev::k_adj_stacey<2><<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
     }
     J.uf = A.seg_u + sl * A.stride;
     J.slot = i;
-    sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
-    sfg::dev::k_adj_post<<<grid_for(D.nglob), 256, 0, rs>>>(
-        A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
-        D.nglob, dt, dt2, dtsq2);
+    if (sh) {
+      sfg::dev::k_adj_elem_sh<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+      sfg::dev::k_adj_post<1><<<grid_for(D.nglob), 256, 0, rs>>>(
+          A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+          D.nglob, dt, dt2, dtsq2);
+    } else {
+      sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+      sfg::dev::k_adj_post<2><<<grid_for(D.nglob), 256, 0, rs>>>(
+          A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+          D.nglob, dt, dt2, dtsq2);
+    }
   }
   sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
 }
@@ -1720,7 +1732,12 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       const size_t pm = A.lb_pm[i];
       const double rho = h->mesh.prho.empty() ? h->mesh.mat_rho[h->mesh.kmato[pm / sfg::NPTS]] : h->mesh.prho[pm];
       const double rvp = M.bc_imp0[k], rvs = M.bc_imp1[k];
-      double dr = g_vp * rvp / (2 * rho), dk = g_vp * rho / (2 * rvp), dm = g_vp * (2.0 / 3.0) * rho / rvp;
+      double dr = 0, dk = 0, dm = 0;
+      if (rvp > 0) {      // P-SV only: SH has no P impedance (g_vp is 0 there)
+        dr = g_vp * rvp / (2 * rho);
+        dk = g_vp * rho / (2 * rvp);
+        dm = g_vp * (2.0 / 3.0) * rho / rvp;
+      }
       if (rvs > 0) {
         dr += g_vs * rvs / (2 * rho);
         dm += g_vs * rho / (2 * rvs);

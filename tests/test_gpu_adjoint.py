@@ -1,9 +1,10 @@
-"""Discrete-adjoint model gradients (2D elastic P-SV) against finite differences.
+"""Discrete-adjoint model gradients (2D elastic P-SV and SH) against finite
+differences.
 
 The gradient of L = sum(w * seis) for a seeded weight array w is checked,
 along smooth Gaussian perturbations of rho, kappa and mu placed between the
-source and the receivers (away from the absorbing edges, whose impedances
-the adjoint holds fixed), against central differences of two forward runs:
+source and the receivers, and on the absorbing edge (where the Stacey
+impedances depend on the model), against central differences of two forward runs:
 relative error <= 1e-2 (the FP32 forward limits the difference quotient to
 about 1e-3 at a 1% perturbation).  Gradients from different checkpoint
 intervals agree to 1e-5 (only the order of the FP32 time sum differs).
@@ -222,3 +223,92 @@ def test_kernel_files_from_the_gradient(problem, tmp_path):
         flat, dims = io.read_dataset(f"{root}/elastic_psv_isotropic", name)
         assert dims == [w.mesh.nspec, 5, 5]
         assert np.array_equal(io.from_element_order(flat), k[name].astype(np.float32)), name
+
+
+@pytest.fixture(scope="module")
+def problem_sh(sfg_lib):
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.elastic_psv_80x60(nstep=NSTEP)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=NSTEP, elastic_wave="sh")
+    sim.set_sources(w.sources)
+    sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
+    sim.initialize()
+    model = base_model(w.mesh)
+    weights = np.random.default_rng(12).standard_normal((NSTEP, len(w.rec_x), 2)).astype(np.float32)
+    return w, sim, model, weights
+
+
+EDGE_NSTEP = 1400
+
+
+def edge_problem(wave):
+    """80 x 60 elastic mesh, Stacey left/right/bottom: a source 700 m from the
+    absorbing left edge and receivers between the two, run long enough
+    (1400 steps, 0.7 s) for the waves to reach the edge and come back."""
+    from dataclasses import replace
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.elastic_psv_80x60(nstep=EDGE_NSTEP)
+    srcs = [replace(w.sources[0], x=700.0, z=1500.0)]
+    rx = np.array([300.0, 500.0, 900.0, 1300.0, 1700.0])
+    rz = np.array([2000.0, 1000.0, 2200.0, 800.0, 1500.0])
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=EDGE_NSTEP, elastic_wave=wave)
+    sim.set_sources(srcs)
+    sim.set_receivers(rx, rz, types=("displacement",))
+    sim.initialize()
+    weights = np.random.default_rng(13).standard_normal((EDGE_NSTEP, len(rx), 2)).astype(np.float32)
+    return w, sim, base_model(w.mesh), weights
+
+
+def _fd_check(w, sim, model, weights, which, x0, z0, sigma, nstep=NSTEP):
+    def mis(m):
+        sim.set_model(*[a.astype(np.float32) for a in m])
+        seis = sim.forward_checkpointed(nstep, 50).astype(np.float64)
+        return float((seis * weights).sum())
+    sim.set_model(*[m.astype(np.float32) for m in model])
+    sim.forward_checkpointed(nstep, 50)
+    g = sim.adjoint_gradient(weights)[which].astype(np.float64)
+    d = bump(w.mesh, x0, z0, sigma) * model[which]
+    eps = 1e-2
+    plus = [m.copy() for m in model]
+    minus = [m.copy() for m in model]
+    plus[which] += eps * d
+    minus[which] -= eps * d
+    fd = (mis(plus) - mis(minus)) / (2 * eps)
+    ad = float((g * d).sum())
+    return ad, fd
+
+
+@pytest.mark.parametrize("which", [0, 2], ids=["rho", "mu"])
+def test_sh_adjoint_matches_finite_differences(problem_sh, which):
+    """SH (u_y, sigma = mu grad u_y): the rho and mu gradients along a smooth
+    bump between source and receivers against central differences (relative
+    1e-2 as for P-SV); the kappa gradient is zero."""
+    w, sim, model, weights = problem_sh
+    ad, fd = _fd_check(w, sim, model, weights, which, 2000.0, 2650.0, 250.0)
+    assert abs(fd) > 0
+    assert abs(ad - fd) <= 1e-2 * abs(fd), (ad, fd, abs(ad - fd) / abs(fd))
+    gk = gradient(sim, model, weights, 50)[1]
+    assert not np.any(gk)
+
+
+@pytest.mark.parametrize("wave,which", [("psv", 0), ("psv", 1), ("psv", 2), ("sh", 0), ("sh", 2)],
+                         ids=["psv-rho", "psv-kappa", "psv-mu", "sh-rho", "sh-mu"])
+def test_adjoint_fd_on_absorbing_edge(sfg_lib, wave, which):
+    """A bump on the absorbing left edge, where the Stacey impedances (rho vp
+    and rho vs in P-SV, rho vs in SH) depend on the model, against central
+    differences (relative 1e-2)."""
+    w, sim, model, weights = edge_problem(wave)
+    ad, fd = _fd_check(w, sim, model, weights, which, 100.0, 1500.0, 250.0, nstep=EDGE_NSTEP)
+    big, _ = _fd_check(w, sim, model, weights, which, 1100.0, 1500.0, 250.0, nstep=EDGE_NSTEP)
+    assert abs(fd) > 1e-3 * abs(big), (fd, big)          # the edge matters to the misfit
+    assert abs(ad - fd) <= 1e-2 * abs(fd), (ad, fd, abs(ad - fd) / abs(fd))
+
+
+def test_sh_checkpoint_interval_invariance(problem_sh):
+    w, sim, model, weights = problem_sh
+    a = gradient(sim, model, weights, 1)
+    b = gradient(sim, model, weights, 37)
+    for x, y in ((a[0], b[0]), (a[2], b[2])):
+        n = np.linalg.norm(x)
+        assert n > 0
+        assert np.linalg.norm(x - y) <= 1e-5 * n
