@@ -372,12 +372,14 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
   // assembled per-point Stacey matrices of the elastic medium: the traction
   // of an element point is -C_e v with C_e = w |n| [(rho vp - rho vs) n n^T /
   // |n|^2 + rho vs I] in P-SV (stacey.tpp:50-80) and w |n| rho vs in SH
-  // (stacey.tpp:126-146, stored in the xx slot); the adjoint applies C^T = C
-  {
-    MediumData &D = a.el;
+  // (stacey.tpp:126-146, stored in the xx slot); acoustic: w |n| / (rho vp)
+  // times the free-surface mask of the element point (stacey.tpp:296-326,
+  // dirichlet.hpp:38-62), in the xx slot; the adjoint applies C^T = C
+  for (MediumData *Dp : {&a.el, &a.ac}) {
+    MediumData &D = *Dp;
     D.stacey_pt.clear();
     D.stacey_c.clear();
-    if (!D.aniso) {
+    if (D.nspec && !D.aniso) {
       std::unordered_map<int, size_t> slot;
       for (int ce = 0; ce < D.nspec; ++ce) {
         if (D.bc_slot[ce] < 0) continue;
@@ -398,6 +400,10 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
           const double nx = D.bc_nx[k], nz = D.bc_nz[k], j1 = D.bc_j1[k], wq = D.bc_w[k];
           const double rvp = D.bc_imp0[k], rvs = D.bc_imp1[k];
           const double f = wq * j1, d = (rvp - rvs) / (j1 * j1);
+          if (Dp == &a.ac) {
+            D.stacey_c[3 * j + 0] += float(f * rvp * double(D.bc_keep[k]));
+            continue;
+          }
           if (D.ncomp == 1) {
             D.stacey_c[3 * j + 0] += float(f * rvs);
             continue;

@@ -35,6 +35,14 @@
 // kappa does not enter, and of the Stacey sums only A2 and A4 exist (the SH
 // reference kernels: frechet_derivative.hpp:219-278).  Kernels that differ
 // per wave type take NC, the number of components.
+//
+// Acoustic (potential chi, sigma = rho^-1 grad chi, M = W / kappa, Stacey
+// traction -w |n| chi_dot / (rho vp), free-surface points masked by keep):
+// the scalar sweep with the mask applied to the gathered adjoint field;
+// dL/d(rho^-1)_p += -W_p grad(keep mu) . grad(chi~), the mass term gives
+// kappa, and pressure seismograms d_k = -R chi_dd'_k enter as -R^T g_k on
+// the adjoint acceleration (k_adj_psrc), not on lu (the reference's acoustic
+// kernels: include/medium/dim2/acoustic/isotropic/frechet_derivative.hpp:61-93).
 #pragma once
 
 #include "kernels2d.cuh"
@@ -55,6 +63,8 @@ struct AdjArgs {
   const float *__restrict__ ad_h;    // receiver Lagrange weights [nrec][25]
   const float *__restrict__ gtab;    // dL/d seismogram [nstep][nrec][2]
   const int *__restrict__ seg_k0;    // first step of the segment (device)
+  const int *__restrict__ bc_slot;   // acoustic: free-surface mask (bc_keep) per boundary element
+  const float *__restrict__ bc_keep;
   int slot;                          // step of the segment: k = *seg_k0 + slot
   int nrec;
   int nspec;
@@ -197,6 +207,94 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem_sh(AdjArgs A) {
   A.seg[2 * p + 1] += -W * (mx * ux + mz * uz);
 }
 
+// Acoustic reverse element step: -K (keep mu) with sigma = rho^-1 grad and
+// the rho^-1 term (no receiver term here: pressure seismograms act on the
+// adjoint acceleration, k_adj_psrc).
+template <int E>
+__global__ void __launch_bounds__(NP * E) k_adj_elem_ac(AdjArgs A) {
+  __shared__ float sm_[E][NP], su_[E][NP];
+  __shared__ float sF[2][E][NP];
+  __shared__ float shp[NP], shpw[NP], sw[NG];
+  const int tid = threadIdx.x;
+  load_quad(A.quad, shp, shpw, sw, tid);
+  const int le = tid / NP, q = tid - le * NP;
+  const int e = blockIdx.x * E + le;
+  const bool act = e < A.nspec;
+  const size_t p = size_t(act ? e : 0) * NP + q;
+  const int g = act ? __ldg(A.ibool + p) : 0;
+  const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+              gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+  const float rhoinv = __ldg(A.prop0 + p);
+  float m = act ? A.mu[g] : 0.f;
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  if (bs >= 0) m *= A.bc_keep[size_t(bs) * NP + q];
+  sm_[le][q] = m;
+  su_[le][q] = act ? A.uf[g] : 0.f;
+  __syncthreads();
+  const int iz = q / NG, ix = q - iz * NG;
+  float dm0 = 0.f, dm1 = 0.f, du0 = 0.f, du1 = 0.f;
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    dm0 = fmaf(shp[ix * NG + l], sm_[le][iz * NG + l], dm0);
+    dm1 = fmaf(shp[iz * NG + l], sm_[le][l * NG + ix], dm1);
+    du0 = fmaf(shp[ix * NG + l], su_[le][iz * NG + l], du0);
+    du1 = fmaf(shp[iz * NG + l], su_[le][l * NG + ix], du1);
+  }
+  const float mx = xix * dm0 + gax * dm1, mz = xiz * dm0 + gaz * dm1;
+  const float ux = xix * du0 + gax * du1, uz = xiz * du0 + gaz * du1;
+  const float sx = rhoinv * mx, sz = rhoinv * mz;
+  sF[0][le][q] = jac * (sx * xix + sz * xiz);
+  sF[1][le][q] = jac * (sx * gax + sz * gaz);
+  __syncthreads();
+  if (!act) return;
+  float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    t1 = fmaf(sF[0][le][iz * NG + l], shpw[l * NG + ix], t1);
+    t2 = fmaf(sF[1][le][l * NG + ix], shpw[l * NG + iz], t2);
+  }
+  A.r[__ldg(A.pslot + p)] = -(sw[iz] * t1 + sw[ix] * t2);
+  const float W = sw[ix] * sw[iz] * jac;
+  A.seg[2 * p + 1] += -W * (mx * ux + mz * uz);
+}
+
+// Pressure seismograms as adjoint sources: for step k = *seg_k0 + slot (if
+// k >= 0), mu(g) += M^-1(g) (-sum over the receivers around g of h g_k), over
+// the n points that receivers touch (CSR: start, receiver, weight; fixed
+// order).
+__global__ void __launch_bounds__(128) k_adj_psrc(float *__restrict__ mu, const float *__restrict__ minv,
+                                                  const int *__restrict__ pts, const int *__restrict__ start,
+                                                  const int *__restrict__ rec, const float *__restrict__ hw,
+                                                  const float *__restrict__ gtab, const int *__restrict__ seg_k0,
+                                                  int slot, int nrec, int n) {
+  const int k = *seg_k0 + slot;
+  if (k < 0) return;
+  const float *g_k = gtab + size_t(k) * nrec * 2;
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int i = start[j]; i < start[j + 1]; ++i) s = s + hw[i] * g_k[2 * rec[i]];
+    const int g = pts[j];
+    mu[g] += minv[g] * (-1.f * s);
+  }
+}
+
+// Acoustic pressure sources carry the source array l / kappa: per source
+// element point (t = s * 25 + q) sum mu_k(g) f_k over the steps (the kappa
+// derivative of the source term is -that * l / kappa^2), for step k =
+// *seg_k0 + slot.
+__global__ void __launch_bounds__(128) k_adj_srcterm(float *__restrict__ acc, const float *__restrict__ mu,
+                                                     const int *__restrict__ ibool, const int *__restrict__ src_ce,
+                                                     const float *__restrict__ stf, const int *__restrict__ seg_k0,
+                                                     int slot, int nsrc, int nstep) {
+  const int k = *seg_k0 + slot;
+  if (k >= nstep) return;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nsrc * NP; t += gridDim.x * blockDim.x) {
+    const int s = t / NP, q = t - s * NP;
+    const int g = ibool[size_t(src_ce[s]) * NP + q];
+    acc[t] += mu[g] * stf[size_t(k) * nsrc + s];
+  }
+}
+
 // Per point: lu~ = lu + sum of the element-point results (colour order);
 // G += mu_k . a'_k; then the transposed predictor and mu_(k-1).  lv holds
 // lv~ (Stacey already applied).  One thread per point.
@@ -271,7 +369,7 @@ __device__ __forceinline__ void adj_stacey_grad(const int *__restrict__ lb_g, co
       const int g = lb_g[i];
       const float m = mu[g];
       float4 t = reinterpret_cast<float4 *>(acc)[i];
-      t.y += m * vst[lb_j[i]];
+      t.y += geo[i].x * (m * vst[lb_j[i]]);     // x: 1, or the acoustic free-surface mask
       t.w += m * af[g];
       reinterpret_cast<float4 *>(acc)[i] = t;
     }

@@ -134,7 +134,17 @@ struct AdjointState {
   int *d_k0 = nullptr;                          // first step of the segment in reverse
   bool forward_done = false;
   int epb = 0;                                  // elements per block of k_adj_elem (timed once)
-  size_t nsum() const { return off_lb + 4 * size_t(nlb); }
+  // acoustic: per source element point, sum of mu f over the steps
+  int nsrc_t = 0;
+  int *src_ce = nullptr;
+  size_t off_src() const { return off_lb + 4 * size_t(nlb); }
+  size_t nsum() const { return off_src() + size_t(sfg::NPTS) * nsrc_t; }
+  // acoustic pressure seismograms as adjoint sources: CSR over the points the
+  // receivers touch (point, then receiver and Lagrange weight per entry)
+  bool pressure = false;
+  int nps = 0;
+  int *ps_pt = nullptr, *ps_start = nullptr, *ps_rec = nullptr;
+  float *ps_h = nullptr;
 };
 
 struct sfg_handle {
@@ -558,8 +568,9 @@ bool receivers_early(const sfg_handle *h, int medium) {
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
   if (h->recording) {
-    if (h->el.ncomp == 1) sfg::dev::k_record_begin<1><<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
-    else sfg::dev::k_record_begin<2><<<1, 512, 0, s>>>(h->adj.d_rec, h->el.v, h->d_step);
+    const DevMedium &R = h->el.nspec ? h->el : h->ac;
+    if (R.ncomp == 1) sfg::dev::k_record_begin<1><<<1, 512, 0, s>>>(h->adj.d_rec, R.v, h->d_step);
+    else sfg::dev::k_record_begin<2><<<1, 512, 0, s>>>(h->adj.d_rec, R.v, h->d_step);
   }
   // a recorded (recomputed) step's seismograms are those of the forward run
   const bool rec_ac = has_ac && h->ac.nrec > 0 && h->recording != 2;
@@ -1318,7 +1329,13 @@ int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const f
   return guarded(h, [&]() {
     if (!rho || !kappa || !mu) return int(SFG_ERR_ARG);
     sfg::set_model2d(h->mesh, h->asmb, rho, kappa, mu);
+    // pressure sources in acoustic elements carry l / kappa: rebuild them
+    const bool ac_src = h->have_sources && h->asmb.ac.nspec > 0 && h->asmb.nsrc > 0;
+    if (ac_src) sfg::set_sources2d(h->mesh, h->asmb, h->sources);
     if (h->initialized) {
+      if (ac_src)
+        SFG_CUDA(cudaMemcpy(h->d_src_arr, h->asmb.src_arr.data(), h->asmb.src_arr.size() * sizeof(float),
+                            cudaMemcpyHostToDevice));
       for (int med = 0; med < 2; ++med) {
         const sfg::MediumData &M = med == 1 ? h->asmb.el : h->asmb.ac;
         DevMedium &D = med == 1 ? h->el : h->ac;
@@ -1343,13 +1360,19 @@ int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const f
 
 namespace {
 
+// The medium of an adjoint run: the model has exactly one.
+DevMedium &adj_dev(sfg_handle *h) { return h->el.nspec ? h->el : h->ac; }
+const sfg::MediumData &adj_data(const sfg_handle *h) { return h->el.nspec ? h->asmb.el : h->asmb.ac; }
+bool adj_acoustic(const sfg_handle *h) { return h->el.nspec == 0; }
+
 int adjoint_checks(sfg_handle *h) {
   if (!h->initialized) { h->err = "sfg_initialize first"; return SFG_ERR_STATE; }
   const sfg::Assembly2D &a = h->asmb;
-  if (h->ac.nspec || !h->el.nspec || h->el.aniso || h->el.S != 1 || a.nsb != 1 ||
-      a.ntypes != 1 || a.types[0] != SFG_SEIS_DISPLACEMENT) {
-    h->err = "the adjoint needs one isotropic elastic medium (P-SV or SH), one shot, and displacement "
-             "seismograms sampled every step";
+  const bool one = (h->el.nspec > 0) != (h->ac.nspec > 0);
+  const int want = h->el.nspec ? SFG_SEIS_DISPLACEMENT : SFG_SEIS_PRESSURE;
+  if (!one || h->el.aniso || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
+    h->err = "the adjoint needs one medium (isotropic elastic P-SV or SH with displacement seismograms, "
+             "or acoustic with pressure seismograms), one shot, seismograms sampled every step";
     return SFG_ERR_UNSUPPORTED;
   }
   return SFG_OK;
@@ -1365,11 +1388,12 @@ T *dalloc(size_t n) {
 
 void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   AdjointState &A = h->adj;
-  const size_t nvals = h->el.values();
-  const size_t nloc = size_t(h->el.nspec) * sfg::NPTS;
+  const DevMedium &D = adj_dev(h);
+  const size_t nvals = D.values();
+  const size_t nloc = size_t(D.nspec) * sfg::NPTS;
   const size_t stride = ((nvals + 3) / 4) * 4 + 4;
   const int ncheck = (nstep + interval - 1) / interval;
-  const int nst = int(h->asmb.el.stacey_pt.size());
+  const int nst = int(adj_data(h).stacey_pt.size());
   const size_t vstride = ((2 * size_t(nst) + 3) / 4) * 4 + 4;
   if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck) {
     for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a, &A.seg_v})
@@ -1385,7 +1409,7 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   A.vstride = vstride;
   A.nvals = nvals;
   A.nloc = nloc;
-  A.nglob = size_t(h->el.nglob);
+  A.nglob = size_t(D.nglob);
   A.stride = stride;
   A.interval = interval;
   A.ncheck = ncheck;
@@ -1394,7 +1418,7 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
     A.r = dalloc<float>(2 * nloc);
     // element-local Stacey points: global point, Stacey slot, geometry
-    const sfg::MediumData &M = h->asmb.el;
+    const sfg::MediumData &M = adj_data(h);
     std::unordered_map<int, int> slot;
     for (size_t j = 0; j < M.stacey_pt.size(); ++j) slot[M.stacey_pt[j]] = int(j);
     std::vector<int> lg, lj;
@@ -1409,13 +1433,16 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
         const int g = M.ibool[size_t(ce) * sfg::NPTS + q];
         lg.push_back(g);
         lj.push_back(slot.at(g));
-        geo.insert(geo.end(), {M.bc_nx[k], M.bc_nz[k], M.bc_j1[k], M.bc_w[k]});
+        // P-SV: the normal; SH and acoustic: x is the free-surface mask (1 in SH)
+        geo.insert(geo.end(), {M.ncomp == 2 ? M.bc_nx[k] : M.bc_keep[k], M.bc_nz[k], M.bc_j1[k], M.bc_w[k]});
         A.lb_k.push_back(k);
         A.lb_pm.push_back(size_t(M.elem_mesh[ce]) * sfg::NPTS + q);
       }
     }
     A.nlb = int(lg.size());
     A.off_lb = ((2 * nloc + A.nglob + 3) / 4) * 4;
+    A.nsrc_t = adj_acoustic(h) ? h->asmb.nsrc : 0;
+    A.src_ce = dalloc<int>(std::max(A.nsrc_t, 1));
     A.lb_g = dalloc<int>(lg.size()); A.lb_j = dalloc<int>(lj.size()); A.lb_geo = dalloc<float>(geo.size());
     if (A.nlb) {
       SFG_CUDA(cudaMemcpy(A.lb_g, lg.data(), lg.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -1425,7 +1452,7 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     A.sum = dalloc<float>(A.nsum()); A.comp = dalloc<float>(A.nsum()); A.seg = dalloc<float>(A.nsum());
     // receivers as adjoint sources: chain per elastic compute element
     const sfg::Assembly2D &as = h->asmb;
-    std::vector<int> head(h->el.nspec, -1), next(std::max(as.nrec, 1), -1);
+    std::vector<int> head(D.nspec, -1), next(std::max(as.nrec, 1), -1);
     for (int r = 0; r < as.nrec; ++r) {
       next[r] = head[as.rec_elem[r]];
       head[as.rec_elem[r]] = r;
@@ -1434,8 +1461,35 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     SFG_CUDA(cudaMemcpy(A.ad_head, head.data(), head.size() * sizeof(int), cudaMemcpyHostToDevice));
     A.ad_next = dalloc<int>(next.size());
     SFG_CUDA(cudaMemcpy(A.ad_next, next.data(), next.size() * sizeof(int), cudaMemcpyHostToDevice));
-    const auto &sp = as.el.stacey_pt;
-    const auto &sc = as.el.stacey_c;
+    const auto &sp = M.stacey_pt;
+    const auto &sc = M.stacey_c;
+    // pressure receivers (acoustic): points they touch, with receiver and weight
+    A.pressure = adj_acoustic(h);
+    if (A.pressure) {
+      std::vector<std::vector<std::pair<int, float>>> by_pt(D.nglob);
+      for (int r = 0; r < as.nrec; ++r)
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const float hq = as.rec_h[size_t(r) * sfg::NPTS + q];
+          if (hq != 0.0f) by_pt[M.ibool[size_t(as.rec_elem[r]) * sfg::NPTS + q]].push_back({r, hq});
+        }
+      std::vector<int> pt, start{0}, rr;
+      std::vector<float> hw;
+      for (int g = 0; g < D.nglob; ++g) {
+        if (by_pt[g].empty()) continue;
+        pt.push_back(g);
+        for (auto &[r, hq] : by_pt[g]) { rr.push_back(r); hw.push_back(hq); }
+        start.push_back(int(rr.size()));
+      }
+      A.nps = int(pt.size());
+      A.ps_pt = dalloc<int>(pt.size()); A.ps_start = dalloc<int>(start.size());
+      A.ps_rec = dalloc<int>(rr.size()); A.ps_h = dalloc<float>(hw.size());
+      if (A.nps) {
+        SFG_CUDA(cudaMemcpy(A.ps_pt, pt.data(), pt.size() * sizeof(int), cudaMemcpyHostToDevice));
+        SFG_CUDA(cudaMemcpy(A.ps_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
+        SFG_CUDA(cudaMemcpy(A.ps_rec, rr.data(), rr.size() * sizeof(int), cudaMemcpyHostToDevice));
+        SFG_CUDA(cudaMemcpy(A.ps_h, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice));
+      }
+    }
     A.nst = int(sp.size());
     A.st_pt = dalloc<int>(sp.size());
     A.st_c = dalloc<float>(sc.size());
@@ -1469,10 +1523,11 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
 }
 
 void save_state(sfg_handle *h, float *dst) {
-  const size_t n = h->el.values() + 4;
-  SFG_CUDA(cudaMemcpyAsync(dst, h->el.u, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(dst + n, h->el.v, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, h->el.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  const DevMedium &D = adj_dev(h);
+  const size_t n = D.values() + 4;
+  SFG_CUDA(cudaMemcpyAsync(dst, D.u, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(dst + n, D.v, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, D.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
 }
 
 // Recompute (or, in the forward run, compute: `seismograms`) segment c from
@@ -1498,11 +1553,12 @@ void record_segment(sfg_handle *h, int c, bool seismograms) {
 
 // Reverse sweep over one segment of n steps held in buffer b (slots n-1 ..
 // 0), then the Kahan fold of its sums.  `last`: the run's final segment,
-// whose final step has no Stacey term (mu is zero there).
+// whose final step starts from mu = 0 (no Stacey term) unless pressure
+// seismograms set mu there.
 template <int E>
 void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
   AdjointState &A = h->adj;
-  const DevMedium &D = h->el;
+  const DevMedium &D = adj_dev(h);
   const float dt = float(h->asmb.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
   sfg::dev::AdjArgs J{};
   J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
@@ -1511,6 +1567,7 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
   J.gtab = A.gtab; J.seg_k0 = A.d_k0; J.nrec = h->asmb.nrec;
   J.nspec = D.nspec;
+  J.bc_slot = D.bc_slot; J.bc_keep = D.bc_keep;
   J.quad = h->quad;
   sfg::dev::AdjStaceyArgs St{};
   St.lb_g = A.lb_g; St.lb_j = A.lb_j; St.geo = reinterpret_cast<const float4 *>(A.lb_geo);
@@ -1519,10 +1576,16 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   St.nb_grad = grid_for(A.nlb);
   const int eblocks = (D.nspec + E - 1) / E;
   const size_t ob = size_t(b) * A.interval;
+  auto psrc = [&](int slot) {
+    if (A.nps)
+      sfg::dev::k_adj_psrc<<<std::min(grid_for(A.nps), 64), 128, 0, rs>>>(
+          A.mu, D.minv, A.ps_pt, A.ps_start, A.ps_rec, A.ps_h, A.gtab, A.d_k0, slot, h->asmb.nrec, A.nps);
+  };
+  if (last && A.pressure) psrc(n - 1);      // mu of the final step: B (-R^T g)
   for (int i = n - 1; i >= 0; --i) {
     const size_t sl = ob + size_t(i);
     const bool sh = D.ncomp == 1;
-    if (A.nst && !(last && i == n - 1)) {
+    if (A.nst && !(last && i == n - 1 && !A.pressure)) {
       St.vst = A.seg_v + sl * A.vstride;
       St.af = A.seg_a + sl * A.stride;
       if (sh) sfg::dev::k_adj_stacey<1><<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
@@ -1530,7 +1593,16 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
     }
     J.uf = A.seg_u + sl * A.stride;
     J.slot = i;
-    if (sh) {
+    if (A.pressure) {
+      sfg::dev::k_adj_elem_ac<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+      if (A.nsrc_t)
+        sfg::dev::k_adj_srcterm<<<(A.nsrc_t * sfg::NPTS + 127) / 128, 128, 0, rs>>>(
+            A.seg + A.off_src(), A.mu, D.ibool, A.src_ce, h->d_stf, A.d_k0, i, A.nsrc_t, h->asmb.nstep);
+      sfg::dev::k_adj_post<1><<<grid_for(D.nglob), 256, 0, rs>>>(
+          A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+          D.nglob, dt, dt2, dtsq2);
+      psrc(i - 1);                            // mu of the previous step gets its source
+    } else if (sh) {
       sfg::dev::k_adj_elem_sh<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
       sfg::dev::k_adj_post<1><<<grid_for(D.nglob), 256, 0, rs>>>(
           A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
@@ -1580,10 +1652,11 @@ void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
 }
 
 void restore_state(sfg_handle *h, const float *src) {
-  const size_t n = h->el.values() + 4;
-  SFG_CUDA(cudaMemcpyAsync(h->el.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(h->el.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(h->el.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  const DevMedium &D = adj_dev(h);
+  const size_t n = D.values() + 4;
+  SFG_CUDA(cudaMemcpyAsync(D.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(D.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  SFG_CUDA(cudaMemcpyAsync(D.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
   h->state_final = true;
 }
 
@@ -1659,6 +1732,10 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       }
       SFG_CUDA(cudaMemcpyAsync(A.gtab, g, size_t(A.nstep) * nrec * 2 * sizeof(float), cudaMemcpyHostToDevice, s));
     }
+    if (A.nsrc_t) {
+      // the sources' elements (they may have moved since the last call)
+      SFG_CUDA(cudaMemcpyAsync(A.src_ce, as.src_elem.data(), A.nsrc_t * sizeof(int), cudaMemcpyHostToDevice, s));
+    }
     const size_t nv = A.nvals;
     tune_reverse(h, s);
     for (float *p : {A.lu, A.lv, A.mu})
@@ -1702,34 +1779,50 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     SFG_CUDA(cudaStreamSynchronize(rs));
     SFG_CUDA(cudaStreamSynchronize(s));
     h->host_step = A.nstep;
-    const DevMedium &D = h->el;
+    const DevMedium &D = adj_dev(h);
+    const sfg::MediumData &M = adj_data(h);
+    const bool acoustic = adj_acoustic(h);
     const float dt2 = float(as.dt) / 2.0f;
-    // compute order -> mesh order; rho: -W_p G(g_p)
+    // compute order -> mesh order.  Elastic: kappa and mu terms, rho from the
+    // mass, -W_p G(g_p).  Acoustic: the stiffness term is d/d(rho^-1) (rho:
+    // times -rho^-2), the mass W / kappa gives kappa: +W_p G(g_p) / kappa^2.
     const float *tot = A.h_stage;
     SFG_CUDA(cudaMemcpy(A.h_stage, A.sum, A.nsum() * sizeof(float), cudaMemcpyDeviceToHost));
     const float *grho = tot + 2 * A.nloc;
     for (int ce = 0; ce < D.nspec; ++ce) {
-      const int e = as.el.elem_mesh[ce];
+      const int e = M.elem_mesh[ce];
       for (int q = 0; q < sfg::NPTS; ++q) {
         const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(e) * sfg::NPTS + q;
+        const double W = as.wgll_d[q % sfg::NGLL] * as.wgll_d[q / sfg::NGLL] * as.jac_d[pm];
+        const double G = double(grho[M.ibool[pc]]);
+        if (acoustic) {
+          const double ri = double(M.prop0[pc]), kap = double(M.prop1[pc]);
+          if (grad_rho) grad_rho[pm] = float(-ri * ri * double(tot[2 * pc + 1]));
+          if (grad_kappa) grad_kappa[pm] = float(W * G / (kap * kap));
+          continue;
+        }
         if (grad_kappa) grad_kappa[pm] = tot[2 * pc];
         if (grad_mu) grad_mu[pm] = tot[2 * pc + 1];
-        if (grad_rho) {
-          const double W = as.wgll_d[q % sfg::NGLL] * as.wgll_d[q / sfg::NGLL] * as.jac_d[pm];
-          grad_rho[pm] = float(-W * double(grho[as.el.ibool[pc]]));
-        }
+        if (grad_rho) grad_rho[pm] = float(-W * G);
       }
     }
-    // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu)
+    // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu);
+    // acoustic: 1 / (rho vp) = (rho kappa)^-1/2
     const float *lbs = tot + A.off_lb;
     for (int i = 0; i < A.nlb; ++i) {
       const size_t k = A.lb_k[i];
-      const sfg::MediumData &M = as.el;
       const double A1 = lbs[4 * i], A2 = lbs[4 * i + 1], A3 = lbs[4 * i + 2], A4 = lbs[4 * i + 3];
       const double wj = double(M.bc_w[k]) * double(M.bc_j1[k]);
       const double g_vp = -wj * (A1 + double(dt2) * A3);
       const double g_vs = -wj * (A2 - A1 + double(dt2) * (A4 - A3));
       const size_t pm = A.lb_pm[i];
+      if (acoustic) {
+        const size_t pc = size_t(as.mesh_to_compute[pm / sfg::NPTS]) * sfg::NPTS + pm % sfg::NPTS;
+        const double imp = M.bc_imp0[k], rho = 1.0 / double(M.prop0[pc]), kap = double(M.prop1[pc]);
+        if (grad_rho) grad_rho[pm] += float(g_vs * (-imp / (2 * rho)));
+        if (grad_kappa) grad_kappa[pm] += float(g_vs * (-imp / (2 * kap)));
+        continue;
+      }
       const double rho = h->mesh.prho.empty() ? h->mesh.mat_rho[h->mesh.kmato[pm / sfg::NPTS]] : h->mesh.prho[pm];
       const double rvp = M.bc_imp0[k], rvs = M.bc_imp1[k];
       double dr = 0, dk = 0, dm = 0;
@@ -1745,6 +1838,23 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       if (grad_rho) grad_rho[pm] += float(dr);
       if (grad_kappa) grad_kappa[pm] += float(dk);
       if (grad_mu) grad_mu[pm] += float(dm);
+    }
+    if (acoustic && grad_kappa) {
+      // kappa in the pressure sources' arrays l / kappa
+      const float *ss = tot + A.off_src();
+      for (int si = 0; si < A.nsrc_t; ++si) {
+        const int ce = as.src_elem[si];
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(M.elem_mesh[ce]) * sfg::NPTS + q;
+          const double sa = as.src_arr[(size_t(si) * 2) * sfg::NPTS + q];
+          grad_kappa[pm] += float(-double(ss[size_t(si) * sfg::NPTS + q]) * sa / double(M.prop1[pc]));
+        }
+      }
+    }
+    if (acoustic && grad_mu) {
+      // the acoustic medium uses kappa + 4/3 mu as its bulk modulus
+      const size_t n = size_t(as.nspec) * sfg::NPTS;
+      for (size_t pm = 0; pm < n; ++pm) grad_mu[pm] = grad_kappa ? float(4.0 / 3.0 * grad_kappa[pm]) : 0.0f;
     }
     return int(SFG_OK);
   });
