@@ -189,8 +189,10 @@ int sfg_get_geometry(sfg_handle *h, double *x, double *z, double *jac, int *medi
 /* Non-zero once a non-finite value was seen in the elastic/acoustic update. */
 int sfg_check_finite(sfg_handle *h);
 
-/* ---- adjoint (2D isotropic elastic P-SV or SH, one shot, displacement
- * seismograms every step; in SH the gradient with respect to kappa is zero) ----
+/* ---- adjoint (one 2D medium, one shot, seismograms every step: isotropic
+ * elastic P-SV or SH with displacement seismograms (in SH the gradient with
+ * respect to kappa is zero), or acoustic with pressure seismograms (there the
+ * bulk modulus is kappa + 4/3 mu, so dL/dmu = 4/3 dL/dkappa)) ----
  * Replace the model by per-GLL-point rho, kappa, mu ([nspec][25], database
  * element order; kappa = lambda + 2/3 mu as the reference stores it).
  * Reference: the property container, core/specfem/assembly/properties. */
