@@ -616,67 +616,98 @@ __global__ void __launch_bounds__(256) k_update(UpdateArgs A) {
 // the sum is the colour passes' sum bit for bit; then coupling, M^-1,
 // corrector and optional predictor as k_update.  No accumulator to clear.
 template <int NC>
+__device__ __forceinline__ bool update_gather_point(const UpdateArgs &A, int g) {
+  float acc[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+  const int k1 = A.inv_start[g + 1];
+  for (int k = A.inv_start[g]; k < k1; ++k) {
+    if (NC == 2) {
+      const float2 t = reinterpret_cast<const float2 *>(A.r)[k];
+      acc[0] = acc[0] + t.x;
+      acc[NC - 1] = acc[NC - 1] + t.y;
+    } else {
+      acc[0] = acc[0] + A.r[k];
+    }
+  }
+  if (g < A.niface) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] += coupling_term(A, g, c);
+  }
+  float uu[NC], vv[NC], mi[NC];
+  if (NC == 2) {
+    const float2 u2 = reinterpret_cast<const float2 *>(A.u)[g];
+    const float2 v2 = reinterpret_cast<const float2 *>(A.v)[g];
+    const float2 m2 = reinterpret_cast<const float2 *>(A.minv)[g];
+    uu[0] = u2.x; uu[NC - 1] = u2.y; vv[0] = v2.x; vv[NC - 1] = v2.y; mi[0] = m2.x; mi[NC - 1] = m2.y;
+  } else {
+    uu[0] = A.u[g]; vv[0] = A.v[g]; mi[0] = A.minv[g];
+  }
+  float a[NC];
+#pragma unroll
+  for (int c = 0; c < NC; ++c) a[c] = __fmul_rn(acc[c], mi[c]);
+  if (A.rec) {
+    const size_t off = size_t(*A.step - A.rec->k0) * A.rec->stride;
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      A.rec->u[off + size_t(g) * NC + c] = uu[c];
+      A.rec->a[off + size_t(g) * NC + c] = a[c];
+    }
+  }
+  bool bad = false;
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    vv[c] = newmark_correct(vv[c], a[c], A.dt2);
+    if (A.predict) newmark_predict(uu[c], vv[c], a[c], A.dt, A.dt2, A.dtsq2);
+    bad |= !isfinite(uu[c]);
+  }
+  if (NC == 2) {
+    if (A.predict) reinterpret_cast<float2 *>(A.u)[g] = make_float2(uu[0], uu[NC - 1]);
+    reinterpret_cast<float2 *>(A.v)[g] = make_float2(vv[0], vv[NC - 1]);
+    if (A.a_store) reinterpret_cast<float2 *>(A.a_store)[g] = make_float2(a[0], a[NC - 1]);
+  } else {
+    if (A.predict) A.u[g] = uu[0];
+    A.v[g] = vv[0];
+    if (A.a_store) A.a_store[g] = a[0];
+  }
+  return bad;
+}
+
+template <int NC>
 __global__ void __launch_bounds__(256) k_update_gather(UpdateArgs A) {
   const int npts = A.n / NC;
   const int stride = gridDim.x * blockDim.x;
   bool bad = false;
-  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride) {
-    float acc[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) acc[c] = 0.f;
-    const int k1 = A.inv_start[g + 1];
-    for (int k = A.inv_start[g]; k < k1; ++k) {
-      const int pl = k;
-      if (NC == 2) {
-        const float2 t = reinterpret_cast<const float2 *>(A.r)[pl];
-        acc[0] = acc[0] + t.x;
-        acc[NC - 1] = acc[NC - 1] + t.y;
-      } else {
-        acc[0] = acc[0] + A.r[pl];
-      }
-    }
-    if (g < A.niface) {
-#pragma unroll
-      for (int c = 0; c < NC; ++c) acc[c] += coupling_term(A, g, c);
-    }
-    float uu[NC], vv[NC], mi[NC];
-    if (NC == 2) {
-      const float2 u2 = reinterpret_cast<const float2 *>(A.u)[g];
-      const float2 v2 = reinterpret_cast<const float2 *>(A.v)[g];
-      const float2 m2 = reinterpret_cast<const float2 *>(A.minv)[g];
-      uu[0] = u2.x; uu[NC - 1] = u2.y; vv[0] = v2.x; vv[NC - 1] = v2.y; mi[0] = m2.x; mi[NC - 1] = m2.y;
-    } else {
-      uu[0] = A.u[g]; vv[0] = A.v[g]; mi[0] = A.minv[g];
-    }
-    float a[NC];
-#pragma unroll
-    for (int c = 0; c < NC; ++c) a[c] = __fmul_rn(acc[c], mi[c]);
-    if (A.rec) {
-      const size_t off = size_t(*A.step - A.rec->k0) * A.rec->stride;
-#pragma unroll
-      for (int c = 0; c < NC; ++c) {
-        A.rec->u[off + size_t(g) * NC + c] = uu[c];
-        A.rec->a[off + size_t(g) * NC + c] = a[c];
-      }
-    }
-#pragma unroll
-    for (int c = 0; c < NC; ++c) {
-      vv[c] = newmark_correct(vv[c], a[c], A.dt2);
-      if (A.predict) newmark_predict(uu[c], vv[c], a[c], A.dt, A.dt2, A.dtsq2);
-      bad |= !isfinite(uu[c]);
-    }
-    if (NC == 2) {
-      if (A.predict) reinterpret_cast<float2 *>(A.u)[g] = make_float2(uu[0], uu[NC - 1]);
-      reinterpret_cast<float2 *>(A.v)[g] = make_float2(vv[0], vv[NC - 1]);
-      if (A.a_store) reinterpret_cast<float2 *>(A.a_store)[g] = make_float2(a[0], a[NC - 1]);
-    } else {
-      if (A.predict) A.u[g] = uu[0];
-      A.v[g] = vv[0];
-      if (A.a_store) A.a_store[g] = a[0];
-    }
-  }
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += stride)
+    bad |= update_gather_point<NC>(A, g);
   if (bad) *A.flag = 1;
   if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) *A.step += 1;
+}
+
+// Both media's owner-computes point updates in one launch (coupled P-SV
+// model, one shot).  Threads [0, n_el) take the elastic points, the others
+// the acoustic points past the interface.  The acoustic update of an
+// interface point reads the elastic predicted displacement there, and the
+// elastic update reads the acoustic chi_dd: the interface points pair one to
+// one (elastic i <-> acoustic El.cp_other[i]), so the thread of elastic
+// interface point i first updates its acoustic partner (as the acoustic
+// launch would, before this thread overwrites the displacement) and then
+// itself (reading the chi_dd it has just stored).  Same arithmetic as the two
+// launches: equal bits.
+__global__ void __launch_bounds__(256) k_update_coupled(UpdateArgs El, UpdateArgs Ac) {
+  const int nel = El.n / 2, nac = Ac.n;
+  const int stride = gridDim.x * blockDim.x;
+  bool bad = false;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nel + nac - Ac.niface; t += stride) {
+    if (t < nel) {
+      if (t < El.niface) bad |= update_gather_point<1>(Ac, El.cp_other[t]);
+      bad |= update_gather_point<2>(El, t);
+    } else {
+      bad |= update_gather_point<1>(Ac, Ac.niface + (t - nel));
+    }
+  }
+  if (bad) *El.flag = 1;
+  if (El.advance && blockIdx.x == 0 && threadIdx.x == 0) *El.step += 1;
 }
 
 // Pending predictor of a run that ended on a corrector-only update.

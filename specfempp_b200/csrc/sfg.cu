@@ -152,6 +152,9 @@ struct sfg_handle {
   // update_args: record u~ and a' of each step (adjoint); 2 = recompute
   // (seismograms are those of the forward run and are not computed again)
   int recording = 0;
+  // coupled P-SV model whose interface points pair one to one: the two
+  // owner-computes point updates can run as one launch
+  bool fuse_ok = false;
   sfg::Mesh2D mesh;
   sfg::Assembly2D asmb;
   sfg_options opt{};
@@ -537,6 +540,20 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
   else sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
 }
 
+// Both media's point updates in one launch (owner-computes, interface points
+// paired one to one).
+void launch_update_coupled(sfg_handle *h, bool predict, cudaStream_t s) {
+  sfg::dev::UpdateArgs E = update_args(h, h->el, h->ac, SFG_MEDIUM_ELASTIC, predict, true);
+  sfg::dev::UpdateArgs A = update_args(h, h->ac, h->el, SFG_MEDIUM_ACOUSTIC, predict, false);
+  const int n = E.n / 2 + A.n - A.niface;
+  sfg::dev::k_update_coupled<<<grid_for(n), 256, 0, s>>>(E, A);
+}
+
+// Whether this step may use launch_update_coupled: owner-computes, one shot,
+// and no elastic receiver that reads this step's acoustic acceleration (the
+// elastic receivers then run before the update).
+bool fused_update(const sfg_handle *h);
+
 void launch_predict_medium(sfg_handle *h, const DevMedium &D, cudaStream_t s) {
   if (!D.nspec) return;
   const float dt = float(h->asmb.dt);
@@ -589,6 +606,12 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
   }
   launch_stiffness(h, s);
   if (fork) SFG_CUDA(cudaStreamWaitEvent(s, h->ev_join, 0));
+  if (fused_update(h)) {
+    if (rec_ac && !(fork && early_ac)) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
+    if (rec_el && !(fork && early_el)) launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
+    launch_update_coupled(h, predict, s);
+    return;
+  }
   if (has_ac) {
     if (rec_ac && !(fork && early_ac)) launch_receivers(h, SFG_MEDIUM_ACOUSTIC, s);
     launch_update(h, SFG_MEDIUM_ACOUSTIC, predict, !has_el, s);
@@ -605,7 +628,16 @@ int kernels_per_step(const sfg_handle *h) {
     if (D->nspec == 0) continue;
     n += (D->nrec > 0 ? 1 : 0) + 1;
   }
-  return n;
+  return fused_update(h) ? n - 1 : n;
+}
+
+bool fused_update(const sfg_handle *h) {
+  if (!h->fuse_ok || h->variant < 3 || h->recording) return false;
+  const sfg::Assembly2D &a = h->asmb;
+  if (h->el.nrec == 0) return true;
+  for (int t : a.types)
+    if (t != SFG_SEIS_DISPLACEMENT && t != SFG_SEIS_PRESSURE) return false;
+  return true;
 }
 
 cudaGraphExec_t capture(sfg_handle *h, int nsteps, bool last_predicts) {
@@ -991,6 +1023,16 @@ int sfg_initialize(sfg_handle *h) {
       int dev = 0;
       SFG_CUDA(cudaGetDevice(&dev));
       SFG_CUDA(cudaDeviceGetAttribute(&h->sm_count, cudaDevAttrMultiProcessorCount, dev));
+    }
+    {
+      // interface points paired one to one, one shot, P-SV: fused updates
+      const sfg::MediumData &E = a.el, &C = a.ac;
+      bool ok = E.nspec && C.nspec && a.nshots == 1 && E.ncomp == 2 && E.niface == C.niface;
+      for (int i = 0; ok && i < E.niface; ++i) {
+        const int j = E.cp_other[i];
+        ok = j >= 0 && j < C.niface && C.cp_other[j] == i;
+      }
+      h->fuse_ok = ok;
     }
     autotune(h);
     h->graph_steps = std::max(1, h->opt.steps_per_graph);
