@@ -54,7 +54,12 @@ enum { SFG_MEDIUM_ACOUSTIC = 0, SFG_MEDIUM_ELASTIC = 1 };
 enum { SFG_WAVE_PSV = 0, SFG_WAVE_SH = 1 };
 enum { SFG_SEIS_DISPLACEMENT = 0, SFG_SEIS_VELOCITY = 1, SFG_SEIS_ACCELERATION = 2,
        SFG_SEIS_PRESSURE = 3 };
-enum { SFG_STF_RICKER = 0, SFG_STF_DIRAC = 1 };
+/* Source-time functions (core/specfem/source_time_functions): Ricker, Dirac
+ * (f0 = 1/(10 dt)), Gaussian and its derivative by f0, Gaussian and Heaviside
+ * (error function) by half duration hdur (at least 5 dt; start time
+ * -2 hdur + tshift, evaluated with hdur / 1.628). */
+enum { SFG_STF_RICKER = 0, SFG_STF_DIRAC = 1, SFG_STF_GAUSSIAN = 2, SFG_STF_GAUSSIAN_HDUR = 3,
+       SFG_STF_DGAUSSIAN = 4, SFG_STF_HEAVISIDE = 5 };
 enum { SFG_FIELD_DISPLACEMENT = 0, SFG_FIELD_VELOCITY = 1, SFG_FIELD_ACCELERATION = 2 };
 
 typedef struct sfg_handle sfg_handle;
@@ -104,6 +109,7 @@ typedef struct sfg_source2d {
   double f0, factor, tshift, angle;
   int kind;                      /* SFG_SOURCE_FORCE or SFG_SOURCE_MOMENT_TENSOR */
   double mxx, mzz, mxz;          /* moment tensor (kind SFG_SOURCE_MOMENT_TENSOR) */
+  double hdur;                   /* half duration (SFG_STF_GAUSSIAN_HDUR, SFG_STF_HEAVISIDE) */
 } sfg_source2d;
 
 enum { SFG_SOURCE_FORCE = 0, SFG_SOURCE_MOMENT_TENSOR = 1 };

@@ -95,11 +95,12 @@ class Source:
     factor: float
     tshift: float = 0.0
     angle: float = 0.0
-    stf: str = "ricker"          # "ricker" or "dirac"
+    stf: str = "ricker"          # ricker, dirac, gaussian, dgaussian, gaussian_hdur, heaviside
     kind: str = "force"          # "force" or "moment_tensor"
     mxx: float = 0.0
     mzz: float = 0.0
     mxz: float = 0.0
+    hdur: float = 0.0            # half duration (gaussian_hdur, heaviside)
 
 
 @dataclass
@@ -122,10 +123,26 @@ class Case2D:
     setup_in_run_precision: bool = False   # True: reference-faithful FP32 setup geometry
 
 
-def start_time(sources) -> tuple[float, list]:
-    """t0 and effective tshifts (read_sources.cpp:142-172), in FP32 like the reference."""
+def _src_start(s, dt):
+    """Start time and evaluation parameter of one source, FP32: -1.2/f0 +
+    tshift for ricker / dirac / dgaussian (ricker.cpp:18-21, dgaussian.cpp:17-20),
+    -2/f0 + tshift for gaussian (gaussian.cpp:17-21, the 2D factor of
+    core/specfem/source/source.tpp:17-62), and for gaussian_hdur / heaviside
+    hdur raised to 5 dt, start -2 hdur + tshift, evaluated with hdur / 1.628
+    (gaussianhdur.cpp:17-37, heaviside.cpp:15-34)."""
     f32 = np.float32
-    t0s = [f32(-1.2) * (f32(1.0) / f32(s.f0)) + f32(s.tshift) for s in sources]
+    if s.stf in ("gaussian_hdur", "heaviside"):
+        h = f32(s.hdur)
+        if h < f32(5.0) * f32(dt if dt is not None else 0.0):
+            h = f32(5.0) * f32(dt)
+        return f32(-f32(2.0) * h + f32(s.tshift)), f32(h / f32(1.628))
+    k = f32(2.0) if s.stf == "gaussian" else f32(1.2)
+    return f32(-k * (f32(1.0) / f32(s.f0)) + f32(s.tshift)), f32(s.f0)
+
+
+def start_time(sources, dt=None) -> tuple[float, list]:
+    """t0 and effective tshifts (read_sources.cpp:142-172), in FP32 like the reference."""
+    t0s = [_src_start(s, dt)[0] for s in sources]
     t0 = min(t0s)
     return float(t0), [float(t - t0) for t in t0s]
 
@@ -176,7 +193,7 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
 
     rho, vp, vs = point_models(case)
     srcs = [effective_f0(s, case.dt) for s in case.sources]
-    t0, tsh = start_time(srcs)
+    t0, tsh = start_time(srcs, case.dt)
     stf_table = case.stf_table
     if stf_table is None and any(s.stf != "ricker" for s in srcs):
         stf_table = stf_tables(case.sources, case.dt, case.nstep)
@@ -269,39 +286,57 @@ def read_sources_yaml(path):
             fs, kind_src = s["moment-tensor"], "moment_tensor"
         else:
             raise ValueError("only force and moment-tensor sources are on this path")
-        if "Ricker" in fs:
-            rk, kind = fs["Ricker"], "ricker"
-        elif "Dirac" in fs:
-            rk, kind = fs["Dirac"], "dirac"
-        else:
-            raise ValueError("only Ricker and Dirac time functions are on this path")
+        rk = kind = None
+        for key, k in (("Ricker", "ricker"), ("Dirac", "dirac"), ("dGaussian", "dgaussian"),
+                       ("Heaviside", "heaviside")):
+            if key in fs:
+                rk, kind = fs[key], k
+        if "Gaussian" in fs:
+            rk = fs["Gaussian"]
+            kind = "gaussian_hdur" if "hdur" in rk else "gaussian"
+        if rk is None:
+            raise ValueError("time function not on this path")
         out.append(Source(x=float(fs["x"]), z=float(fs["z"]), f0=float(rk.get("f0", 0.0)),
                           factor=float(rk["factor"]), tshift=float(rk.get("tshift", 0.0)),
                           angle=float(fs.get("angle", 0.0)), stf=kind, kind=kind_src,
                           mxx=float(fs.get("Mxx", 0.0)), mzz=float(fs.get("Mzz", 0.0)),
-                          mxz=float(fs.get("Mxz", 0.0))))
+                          mxz=float(fs.get("Mxz", 0.0)), hdur=float(rk.get("hdur", 0.0))))
     return out
 
 
 def stf_tables(sources, dt, nstep):
-    """FP32 source-time-function table [nstep, nsrc] (ricker.cpp, dirac.cpp).
-
-    Ricker: factor * (1 - 2 a t^2) exp(-a t^2); Dirac: factor * (-exp(-a t^2) / (2a))
-    with f0 = 1 / (10 dt); a = pi^2 f0^2, t = t0 + i dt - tshift.
+    """FP32 source-time-function table [nstep, nsrc]
+    (core/specfem/source_time_functions/impl/time_functions.hpp), a = pi^2 f0^2:
+    ricker factor (1 - 2 a t^2) exp(-a t^2); dirac (f0 = 1/(10 dt)) and
+    gaussian factor (-exp(-a t^2) / (2a)); dgaussian factor t exp(-a t^2);
+    gaussian_hdur factor exp(-t^2/h^2) / (sqrt(pi) h); heaviside factor
+    (1 + erf(t/h)) / 2; t = t0 + i dt - tshift.
     """
+    import math
     f32 = np.float32
     srcs = [effective_f0(s, dt) for s in sources]
-    t0, tsh = start_time(srcs)
+    t0, tsh = start_time(srcs, dt)
     i = np.arange(nstep, dtype=f32)
     tab = np.zeros((nstep, len(srcs)), np.float32)
     pi = f32(np.pi)
     for k, s in enumerate(srcs):
         t = f32(t0) + i * f32(dt) - f32(tsh[k])
-        a = pi * pi * f32(s.f0) * f32(s.f0)
-        if s.stf == "dirac":
-            tab[:, k] = f32(s.factor) * (f32(-1.0) * np.exp(-a * t * t) / (f32(2.0) * a))
+        fac = f32(s.factor)
+        p = _src_start(s, dt)[1]
+        if s.stf == "heaviside":
+            e = np.array([math.erf(float(v)) for v in t / p], dtype=f32)
+            tab[:, k] = fac * (f32(0.5) * (f32(1.0) + e))
+            continue
+        if s.stf == "gaussian_hdur":
+            tab[:, k] = fac * (np.exp(-(f32(1.0) / (p * p)) * t * t) / (f32(math.sqrt(math.pi)) * p))
+            continue
+        a = pi * pi * p * p
+        if s.stf in ("dirac", "gaussian"):
+            tab[:, k] = fac * (f32(-1.0) * np.exp(-a * t * t) / (f32(2.0) * a))
+        elif s.stf == "dgaussian":
+            tab[:, k] = fac * (t * np.exp(-a * t * t))
         else:
-            tab[:, k] = f32(s.factor) * ((f32(1.0) - f32(2.0) * a * t * t) * np.exp(-a * t * t))
+            tab[:, k] = fac * ((f32(1.0) - f32(2.0) * a * t * t) * np.exp(-a * t * t))
     return tab
 
 
@@ -322,7 +357,8 @@ def load_fixture(fixture_dir, types=("displacement",)):
     rc = cfg["receivers"]
     mesh = read_database(os.path.join(fixture_dir, "database.bin"))
     names, rx, rz = read_stations(os.path.join(fixture_dir, "STATIONS"))
-    src = read_sources_yaml(os.path.join(fixture_dir, "sources.yaml"))
+    src_name = os.path.basename(str(cfg.get("sources", "sources.yaml")))   # sources.yaml or source.yaml
+    src = read_sources_yaml(os.path.join(fixture_dir, src_name))
     sh = str(cfg["simulation-setup"].get("elastic-wave", "P_SV")).upper() == "SH"
     return Case2D(mesh=mesh, sources=src, rec_x=rx, rec_z=rz, dt=float(ts["dt"]),
                   nstep=int(ts["nstep"]), seis_types=list(types),

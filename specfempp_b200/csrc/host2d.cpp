@@ -883,17 +883,31 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
   a.src_arr.assign(size_t(a.nsrc) * 2 * NPTS, 0.0f);
   a.el_src_head.assign(a.el.nspec, -1);
   a.ac_src_head.assign(a.ac.nspec, -1);
-  // start time per shot: t0 = min over the shot's sources of -1.2/f0 + tshift,
-  // and each source's shift becomes t0_source - t0 (read_sources.cpp:142-172);
-  // Dirac sources use f0 = 1/(10 dt) (dirac.cpp:25).
+  // start time per shot: t0 = min over the shot's sources of their start
+  // times, and each source's shift becomes t0_source - t0
+  // (read_sources.cpp:142-172).  Start times, FP32 like the reference:
+  // Ricker, Dirac (f0 = 1/(10 dt), dirac.cpp:25) and dGaussian -1.2/f0 +
+  // tshift; Gaussian -2/f0 + tshift; Gaussian by hdur and Heaviside, with hdur
+  // raised to 5 dt, -2 hdur + tshift, then evaluated with hdur / 1.628
+  // (ricker.cpp, gaussian.cpp, dgaussian.cpp, gaussianhdur.cpp, heaviside.cpp;
+  // the factor 2 is the 2D one of core/specfem/source/source.tpp:17-62).
   std::vector<double> f0(a.nsrc), t0s(a.nsrc);
   a.shot_t0.assign(a.nshots, 1e300);
   for (int s = 0; s < a.nsrc; ++s) {
     const Source2D &S = src[s];
     if (S.shot < 0 || S.shot >= a.nshots) throw std::runtime_error("source shot index out of range");
-    f0[s] = S.stf == 1 ? double(1.0f / (10.0f * float(a.dt))) : S.f0;
-    if (!(f0[s] > 0)) throw std::runtime_error("source f0 must be positive");
-    t0s[s] = double(-1.2f * (1.0f / float(f0[s])) + float(S.tshift));
+    if (S.stf < 0 || S.stf > 5) throw std::runtime_error("unknown source time function");
+    if (S.stf == 3 || S.stf == 5) {
+      if (!(S.hdur > 0)) throw std::runtime_error("source hdur must be positive");
+      const float hd = std::max(float(S.hdur), 5.0f * float(a.dt));
+      t0s[s] = double(-2.0f * hd + float(S.tshift));
+      f0[s] = double(hd / 1.628f);                // evaluation half duration
+    } else {
+      f0[s] = S.stf == 1 ? double(1.0f / (10.0f * float(a.dt))) : S.f0;
+      if (!(f0[s] > 0)) throw std::runtime_error("source f0 must be positive");
+      const float fac = S.stf == 2 ? 2.0f : 1.2f;
+      t0s[s] = double(-fac * (1.0f / float(f0[s])) + float(S.tshift));
+    }
     a.shot_t0[S.shot] = std::min(a.shot_t0[S.shot], t0s[s]);
   }
   for (double &t : a.shot_t0)
@@ -962,8 +976,18 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
     for (int i = 0; i < a.nstep; ++i) {
       const float t = t0 + float(i) * float(a.dt) - tsh;
       float v;
-      if (S.stf == 1) v = fac * (-1.0f * std::exp(-aa * t * t) / (2.0f * aa));
-      else v = fac * ((1.0f - 2.0f * aa * t * t) * std::exp(-aa * t * t));
+      switch (S.stf) {
+        case 1:                  // Dirac and Gaussian: -exp(-a t^2) / (2a)
+        case 2: v = fac * (-1.0f * std::exp(-aa * t * t) / (2.0f * aa)); break;
+        case 3: {                // Gaussian by hdur: exp(-t^2/h^2) / (sqrt(pi) h)
+          const float h = fz, ah = 1.0f / (h * h);
+          v = fac * (std::exp(-ah * t * t) / (std::sqrt(pi) * h));
+          break;
+        }
+        case 4: v = fac * (t * std::exp(-aa * t * t)); break;      // dGaussian
+        case 5: v = fac * (0.5f * (1.0f + std::erf(t / fz))); break;  // Heaviside
+        default: v = fac * ((1.0f - 2.0f * aa * t * t) * std::exp(-aa * t * t));  // Ricker
+      }
       a.stf[size_t(i) * a.nsrc + s] = med == 0 ? -v : v;
     }
   }

@@ -42,6 +42,7 @@ struct Source2D {
   double f0, factor, tshift, angle;
   int kind = 0;                   // 0 force, 1 moment tensor
   double mxx = 0, mzz = 0, mxz = 0;
+  double hdur = 0;                // half duration (Gaussian by hdur, Heaviside)
 };
 
 // Per-medium device-ready arrays (element order = compute order of that medium).

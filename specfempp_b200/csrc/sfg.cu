@@ -909,7 +909,7 @@ int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
     for (int i = 0; i < nsrc; ++i)
       h->sources.push_back({src[i].x, src[i].z, src[i].shot, src[i].stf, src[i].f0, src[i].factor,
                             src[i].tshift, src[i].angle, src[i].kind, src[i].mxx, src[i].mzz,
-                            src[i].mxz});
+                            src[i].mxz, src[i].hdur});
     try {
       sfg::set_sources2d(h->mesh, h->asmb, h->sources);
     } catch (const std::exception &ex) {

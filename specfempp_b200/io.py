@@ -137,18 +137,31 @@ def read_sources(path: str):
             fs, kind = s["moment-tensor"], "moment_tensor"
         else:
             raise ValueError(f"source type {list(s)} is not on this path")
-        if "Ricker" in fs:
-            tf, stf = fs["Ricker"], "ricker"
-        elif "Dirac" in fs:
-            tf, stf = fs["Dirac"], "dirac"
-        else:
-            raise ValueError("only Ricker and Dirac source time functions are on this path")
+        tf, stf = time_function(fs)
         out.append(Source(x=float(fs["x"]), z=float(fs["z"]), f0=float(tf.get("f0", 0.0)),
                           factor=float(tf["factor"]), tshift=float(tf.get("tshift", 0.0)),
                           angle=float(fs.get("angle", 0.0)), stf=stf, kind=kind,
                           mxx=float(fs.get("Mxx", 0.0)), mzz=float(fs.get("Mzz", 0.0)),
-                          mxz=float(fs.get("Mxz", 0.0))))
+                          mxz=float(fs.get("Mxz", 0.0)), hdur=float(tf.get("hdur", 0.0))))
     return out
+
+
+def time_function(fs):
+    """(parameters, kind) of a source's time function block
+    (core/specfem/source/source.tpp:10-70): Ricker, Dirac, Gaussian (by f0
+    or by hdur), dGaussian, Heaviside."""
+    for key, kind in (("Ricker", "ricker"), ("Dirac", "dirac"), ("dGaussian", "dgaussian"),
+                      ("Heaviside", "heaviside")):
+        if key in fs:
+            return fs[key], kind
+    if "Gaussian" in fs:
+        g = fs["Gaussian"]
+        if "hdur" in g:
+            return g, "gaussian_hdur"
+        if "f0" in g:
+            return g, "gaussian"
+        raise ValueError("a Gaussian time function needs hdur or f0")
+    raise ValueError("source time function not on this path (Ricker, Dirac, Gaussian, dGaussian, Heaviside)")
 
 
 def channels(kind: str, elastic_wave: str):

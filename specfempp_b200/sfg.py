@@ -19,7 +19,7 @@ LIB_PATH = os.path.join(HERE, "libsfg.so")
 
 SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC = 0, 1
 SEIS = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3}
-STF = {"ricker": 0, "dirac": 1}
+STF = {"ricker": 0, "dirac": 1, "gaussian": 2, "gaussian_hdur": 3, "dgaussian": 4, "heaviside": 5}
 FIELD = {"displacement": 0, "velocity": 1, "acceleration": 2}
 ERRORS = {0: "OK", -1: "SFG_ERR_ARG", -2: "SFG_ERR_IO", -3: "SFG_ERR_CUDA", -4: "SFG_ERR_LOCATE",
           -5: "SFG_ERR_STATE", -6: "SFG_ERR_NONFINITE", -7: "SFG_ERR_UNSUPPORTED"}
@@ -53,7 +53,7 @@ class Source2D(C.Structure):
     _fields_ = [("x", C.c_double), ("z", C.c_double), ("shot", C.c_int), ("stf", C.c_int),
                 ("f0", C.c_double), ("factor", C.c_double), ("tshift", C.c_double),
                 ("angle", C.c_double), ("kind", C.c_int), ("mxx", C.c_double), ("mzz", C.c_double),
-                ("mxz", C.c_double)]
+                ("mxz", C.c_double), ("hdur", C.c_double)]
 
 
 class Info(C.Structure):
@@ -134,6 +134,7 @@ class Source:
     mxx: float = 0.0
     mzz: float = 0.0
     mxz: float = 0.0
+    hdur: float = 0.0              # half duration of "gaussian_hdur" and "heaviside"
 
 
 SOURCE_KIND = {"force": 0, "moment_tensor": 1}
@@ -218,7 +219,7 @@ class Simulation2D:
                               angle=getattr(s, "angle", 0.0),
                               kind=SOURCE_KIND[getattr(s, "kind", "force")],
                               mxx=getattr(s, "mxx", 0.0), mzz=getattr(s, "mzz", 0.0),
-                              mxz=getattr(s, "mxz", 0.0))
+                              mxz=getattr(s, "mxz", 0.0), hdur=getattr(s, "hdur", 0.0))
         self._check(self.lib.sfg_set_sources(self.h, len(sources), arr))
 
     def set_stf_table(self, table):

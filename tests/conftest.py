@@ -37,8 +37,10 @@ def golden_case(name, nstep=None):
     srcs = []
     for s in z["src"]:
         mt = len(s) > 7 and bool(s[7])
+        codes = ["ricker", "dirac", "gaussian", "gaussian_hdur", "dgaussian", "heaviside"]
+        stf = codes[int(s[11])] if len(s) > 11 else ("dirac" if s[6] else "ricker")
         srcs.append(runner.Source(x=s[0], z=s[1], f0=s[2], factor=s[3], tshift=s[4], angle=s[5],
-                                  stf="dirac" if s[6] else "ricker",
+                                  stf=stf, hdur=float(s[12]) if len(s) > 12 else 0.0,
                                   kind="moment_tensor" if mt else "force",
                                   mxx=s[8] if mt else 0.0, mzz=s[9] if mt else 0.0, mxz=s[10] if mt else 0.0))
     case = runner.Case2D(mesh=mesh, sources=srcs, rec_x=z["rec_x"], rec_z=z["rec_z"],

@@ -20,8 +20,17 @@ def write_fixture_dir(npz_path, out_dir, types=("displacement",)):
             net, sta = str(name).split(".")
             f.write(f"{sta} {net} {x:.6f} {zz:.6f} 0.0 0.0\n")
     srcs = []
+    codes = ["ricker", "dirac", "gaussian", "gaussian_hdur", "dgaussian", "heaviside"]
+    keys = {"ricker": "Ricker", "dirac": "Dirac", "gaussian": "Gaussian", "gaussian_hdur": "Gaussian",
+            "dgaussian": "dGaussian", "heaviside": "Heaviside"}
     for s in z["src"]:
-        tf = {"Dirac" if s[6] else "Ricker": {"f0": float(s[2]), "factor": float(s[3]), "tshift": float(s[4])}}
+        stf = codes[int(s[11])] if len(s) > 11 else ("dirac" if s[6] else "ricker")
+        par = {"factor": float(s[3]), "tshift": float(s[4])}
+        if stf in ("gaussian_hdur", "heaviside"):
+            par["hdur"] = float(s[12])
+        else:
+            par["f0"] = float(s[2])
+        tf = {keys[stf]: par}
         if len(s) > 7 and s[7]:
             srcs.append({"moment-tensor": {"x": float(s[0]), "z": float(s[1]), "Mxx": float(s[8]),
                                            "Mzz": float(s[9]), "Mxz": float(s[10]), **tf}})

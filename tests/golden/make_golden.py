@@ -8,7 +8,7 @@ nstep and the golden displacement traces (``*.semd``, produced by Fortran
 SPECFEM2D), stored as float32.  The tests rebuild a Case2D from it, so they
 run without the reference tree.
 
-Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage:  python tests/golden/make_golden.py [REFERENCE_ROOT [FIXTURE ...]]
 """
 from __future__ import annotations
 
@@ -31,7 +31,14 @@ FIXTURES = {
     "HomogeneousElasticDomainMomentTensor": ("BXX", "BXZ"),
     "HomogeneousElasticIsotropicDomainSH": ("BXY",),
     "HomogeneousElasticAnisotropicDomain": ("BXX", "BXZ"),
+    "HomogeneousAcousticDomain": ("BXX", "BXZ"),
+    "HomogeneousAcousticDomainCompositeStaceyDirichletBC": ("BXX", "BXZ"),
+    "HomogeneousElasticDomainMomentTensorHeaviside": ("BXX", "BXZ"),
+    "HomogeneousElasticDomainWAdjacencyMap": ("BXX", "BXZ"),
 }
+
+# time-function codes stored in the fixtures' source rows
+STF_CODES = ["ricker", "dirac", "gaussian", "gaussian_hdur", "dgaussian", "heaviside"]
 
 
 def make(ref_root: str, name: str, comps) -> str:
@@ -57,7 +64,8 @@ def make(ref_root: str, name: str, comps) -> str:
         mat_vs=m.mat_vs, abs_ispec=m.abs_ispec, abs_type=m.abs_type, free_ispec=m.free_ispec,
         free_type=m.free_type,
         src=np.asarray([[s.x, s.z, s.f0, s.factor, s.tshift, s.angle, 1.0 if s.stf == "dirac" else 0.0,
-                         1.0 if s.kind == "moment_tensor" else 0.0, s.mxx, s.mzz, s.mxz]
+                         1.0 if s.kind == "moment_tensor" else 0.0, s.mxx, s.mzz, s.mxz,
+                         float(STF_CODES.index(s.stf)), s.hdur]
                         for s in case.sources]),
         rec_x=case.rec_x, rec_z=case.rec_z, dt=case.dt, nstep=case.nstep, rec_angle=case.rec_angle,
         stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces["semd"],
@@ -121,7 +129,9 @@ def make3d(ref_root: str) -> str:
 
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    for name, comps in FIXTURES.items():
-        print(make(root, name, comps), os.path.getsize(os.path.join(HERE, f"{name}.npz")))
-    out = make3d(root)
-    print(out, os.path.getsize(out))
+    names = sys.argv[2:] or list(FIXTURES)
+    for name in names:
+        print(make(root, name, FIXTURES[name]), os.path.getsize(os.path.join(HERE, f"{name}.npz")))
+    if not sys.argv[2:]:
+        out = make3d(root)
+        print(out, os.path.getsize(out))

@@ -14,6 +14,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.mark.parametrize("name,comps", [("HomogeneousElasticDomain", ("BXX", "BXZ")),
                                         ("HomogeneousElasticDomainMomentTensor", ("BXX", "BXZ")),
+                                        ("HomogeneousElasticDomainMomentTensorHeaviside", ("BXX", "BXZ")),
                                         ("HomogeneousElasticIsotropicDomainSH", ("BXY",))])
 def test_driver_writes_reference_traces(sfg_lib, tmp_path, name, comps):
     from specfempp_b200 import specfem2d

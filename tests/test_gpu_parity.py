@@ -20,7 +20,9 @@ pytestmark = pytest.mark.gpu
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
-            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain"]
+            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain",
+            "HomogeneousAcousticDomain", "HomogeneousAcousticDomainCompositeStaceyDirichletBC",
+            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap"]
 
 
 def tolerance(kind, f32, f64):

@@ -168,3 +168,39 @@ def test_config_wavefield_writer_keys(tmp_path):
     _with_wavefield_writer(cfg, format="ASCII", directory="OUT", **{"for-adjoint-simulations": True})
     with pytest.raises(ValueError, match="boundary values"):
         io.read_config(cfg, root=str(tmp_path))
+
+
+def test_time_function_tables_product_vs_oracle():
+    """Every time function kind: the library's Python table (the same
+    formulas as its C++ set-up) against the oracle's independent restatement,
+    both FP32; start times follow each kind's rule."""
+    from oracle import runner
+    from specfempp_b200 import sfg, stf
+    kinds = [("ricker", 10.0, 0.0), ("dirac", 0.0, 0.0), ("gaussian", 8.0, 0.0), ("dgaussian", 12.0, 0.0),
+             ("gaussian_hdur", 0.0, 0.02), ("heaviside", 0.0, 0.05), ("heaviside", 0.0, 1e-4)]
+    dt, nstep = 5e-4, 600
+    for kind, f0, hdur in kinds:
+        p = sfg.Source(x=0.0, z=0.0, f0=f0, factor=1e10, tshift=0.01, stf=kind, hdur=hdur)
+        o = runner.Source(x=0.0, z=0.0, f0=f0, factor=1e10, tshift=0.01, stf=kind, hdur=hdur)
+        a = stf.table([p], dt, nstep)[:, 0]
+        b = runner.stf_tables([o], dt, nstep)[:, 0]
+        assert np.all(np.isfinite(a)) and np.abs(a).max() > 0, kind
+        np.testing.assert_allclose(a, b, rtol=2e-6, atol=2e-6 * np.abs(b).max(), err_msg=kind)
+    # start rule of the half-duration kinds: hdur raised to 5 dt, start -2 hdur
+    t0, _ = stf.start(sfg.Source(x=0, z=0, f0=0, factor=1, stf="heaviside", hdur=1e-4), dt)
+    assert abs(t0 - (-2 * 5 * dt)) < 1e-7
+
+
+def test_sources_yaml_time_functions(tmp_path):
+    import yaml
+    from specfempp_b200 import io
+    srcs = [{"force": {"x": 1.0, "z": 2.0, "Heaviside": {"hdur": 0.1, "factor": 1e8}}},
+            {"force": {"x": 1.0, "z": 2.0, "Gaussian": {"hdur": 0.2, "factor": 1.0}}},
+            {"force": {"x": 1.0, "z": 2.0, "Gaussian": {"f0": 3.0, "factor": 1.0}}},
+            {"moment-tensor": {"x": 1.0, "z": 2.0, "Mxx": 1.0, "Mzz": 1.0, "Mxz": 0.0,
+                               "dGaussian": {"f0": 4.0, "factor": 2.0, "tshift": 0.5}}}]
+    p = tmp_path / "sources.yaml"
+    p.write_text(yaml.safe_dump({"number-of-sources": len(srcs), "sources": srcs}))
+    got = io.read_sources(str(p))
+    assert [s.stf for s in got] == ["heaviside", "gaussian_hdur", "gaussian", "dgaussian"]
+    assert got[0].hdur == 0.1 and got[2].f0 == 3.0 and got[3].tshift == 0.5 and got[3].kind == "moment_tensor"

@@ -17,7 +17,9 @@ from conftest import golden_case, reference_metric
 FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichletBC",
             "HomogeneousElasticDomainStaceyBC", "HomogeneousAcousticDomainDirichletBC",
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
-            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain"]
+            "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain",
+            "HomogeneousAcousticDomain", "HomogeneousAcousticDomainCompositeStaceyDirichletBC",
+            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
