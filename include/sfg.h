@@ -100,6 +100,11 @@ typedef struct sfg_options {
                                     with the element arrays staged by bulk copies; all give
                                     the same bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
+  int has_start_time;            /* 1: the run starts at start_time (the configuration's
+                                    time-scheme t0) and sources keep their own tshift;
+                                    0: start at the earliest source start, shifts relative
+                                    to it (src/io/sources/dim2/read_sources.cpp:142-172) */
+  double start_time;
 } sfg_options;
 
 typedef struct sfg_source2d {

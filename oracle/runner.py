@@ -121,6 +121,7 @@ class Case2D:
     stf_table: np.ndarray | None = None    # optional [nstep, nsrc]
     stations: list = field(default_factory=list)
     setup_in_run_precision: bool = False   # True: reference-faithful FP32 setup geometry
+    start_time: float | None = None        # the configuration's t0 (sources keep their tshift)
 
 
 def _src_start(s, dt):
@@ -195,6 +196,11 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     srcs = [effective_f0(s, case.dt) for s in case.sources]
     t0, tsh = start_time(srcs, case.dt)
     stf_table = case.stf_table
+    if case.start_time is not None:
+        # read_sources.cpp:155-161: the given start, each source's own tshift
+        t0, tsh = float(np.float32(case.start_time)), [float(np.float32(s.tshift)) for s in srcs]
+        if stf_table is None:
+            stf_table = stf_tables(case.sources, case.dt, case.nstep, start=case.start_time)
     if stf_table is None and any(s.stf != "ricker" for s in srcs):
         stf_table = stf_tables(case.sources, case.dt, case.nstep)
     inp = OracleInput2D()
@@ -304,7 +310,7 @@ def read_sources_yaml(path):
     return out
 
 
-def stf_tables(sources, dt, nstep):
+def stf_tables(sources, dt, nstep, start=None):
     """FP32 source-time-function table [nstep, nsrc]
     (core/specfem/source_time_functions/impl/time_functions.hpp), a = pi^2 f0^2:
     ricker factor (1 - 2 a t^2) exp(-a t^2); dirac (f0 = 1/(10 dt)) and
@@ -316,6 +322,8 @@ def stf_tables(sources, dt, nstep):
     f32 = np.float32
     srcs = [effective_f0(s, dt) for s in sources]
     t0, tsh = start_time(srcs, dt)
+    if start is not None:
+        t0, tsh = float(f32(start)), [float(f32(s.tshift)) for s in srcs]
     i = np.arange(nstep, dtype=f32)
     tab = np.zeros((nstep, len(srcs)), np.float32)
     pi = f32(np.pi)

@@ -912,6 +912,19 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
   }
   for (double &t : a.shot_t0)
     if (t > 1e299) t = 0.0;
+  if (a.user_t0) {
+    // a given start time: it must not come after the earliest start (less the
+    // smallest shift), and every source keeps its own tshift
+    // (read_sources.cpp:155-161)
+    float min_t0 = 3.4e38f, min_tshift = 3.4e38f;
+    for (int s = 0; s < a.nsrc; ++s) {
+      min_t0 = std::min(min_t0, float(t0s[s]));
+      min_tshift = std::min(min_tshift, float(src[s].tshift));
+    }
+    if (a.nsrc && float(a.user_t0_value) > min_t0 - min_tshift)
+      throw std::runtime_error("User defined start time is less than minimum required for stability");
+    a.shot_t0.assign(a.nshots, double(float(a.user_t0_value)));
+  }
   a.t0 = *std::min_element(a.shot_t0.begin(), a.shot_t0.end());
   a.stf.assign(size_t(a.nstep) * a.nsrc, 0.0f);
   for (int s = 0; s < a.nsrc; ++s) {
@@ -968,7 +981,7 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
         }
       }
     // STF on the shot's own time axis, FP32 like the reference tables
-    const float tsh = float(t0s[s] - a.shot_t0[S.shot]);
+    const float tsh = a.user_t0 ? float(S.tshift) : float(t0s[s] - a.shot_t0[S.shot]);
     const float t0 = float(a.shot_t0[S.shot]);
     const float fz = float(f0[s]), fac = float(S.factor);
     const float pi = float(M_PI);

@@ -80,6 +80,8 @@ struct Assembly2D {
   int nspec = 0, nglob = 0, nshots = 1, elastic_wave = 0;
   double dt = 0;
   int nstep = 0, nsb = 1;
+  bool user_t0 = false;               // start time given by the caller
+  double user_t0_value = 0;
   float hprime[NPTS];                 // hprime[i*5+j] = l'_j(xi_i)
   float hpw[NPTS];                    // hprime[l*5+i] * w[l]  (divergence form)
   float wgll[NGLL];

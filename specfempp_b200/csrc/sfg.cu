@@ -762,6 +762,8 @@ sfg_handle *make_handle(const sfg_options *opt) {
 void finish_create(sfg_handle *h) {
   h->mesh.elastic_wave = h->mesh.elastic_wave ? 1 : 0;
   h->asmb.nshots = h->opt.nshots;
+  h->asmb.user_t0 = h->opt.has_start_time != 0;
+  h->asmb.user_t0_value = h->opt.start_time;
   h->asmb.nstep = h->opt.nstep;
   h->asmb.nsb = h->opt.nstep_between_samples;
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);

@@ -48,6 +48,7 @@ class ForwardConfig:
     wavefield_format: str = "ascii"
     wavefield_interval: int = 0
     wavefield_last_step: bool = True
+    start_time: float | None = None   # time-scheme t0 (sources keep their tshift)
 
 
 def _resolve(path, roots):
@@ -106,7 +107,8 @@ def read_config(path: str, root: str | None = None) -> ForwardConfig:
                          sources=_resolve(cfg["sources"], roots), stations=_resolve(rc["stations"], roots),
                          angle=float(rc.get("angle", 0.0)), seismogram_types=types,
                          nstep_between_samples=int(rc.get("nstep_between_samples", 1)),
-                         output_directory=out_dir, output_format=out_fmt, **wf)
+                         output_directory=out_dir, output_format=out_fmt,
+                         start_time=float(ts["t0"]) if "t0" in ts else None, **wf)
 
 
 def read_stations(path: str):

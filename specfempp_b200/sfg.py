@@ -46,7 +46,7 @@ class Options(C.Structure):
     _fields_ = [("dt", C.c_double), ("nstep", C.c_int), ("nshots", C.c_int),
                 ("nstep_between_samples", C.c_int), ("steps_per_graph", C.c_int),
                 ("elements_per_block", C.c_int), ("kernel_variant", C.c_int),
-                ("store_acceleration", C.c_int)]
+                ("store_acceleration", C.c_int), ("has_start_time", C.c_int), ("start_time", C.c_double)]
 
 
 class Source2D(C.Structure):
@@ -157,12 +157,14 @@ class Simulation2D:
                  nshots: int = 1, nstep_between_samples: int = 1, elastic_wave: str = "psv",
                  point_rho=None, point_vp=None, point_vs=None, steps_per_graph: int = 0,
                  elements_per_block: int = 0, kernel_variant: int = 0,
-                 store_acceleration: bool = False):
+                 store_acceleration: bool = False, start_time: float | None = None):
         self.lib = load_library()
         self._keep = []
         opt = Options(dt=dt, nstep=nstep, nshots=nshots, nstep_between_samples=nstep_between_samples,
                       steps_per_graph=steps_per_graph, elements_per_block=elements_per_block,
-                      kernel_variant=kernel_variant, store_acceleration=int(store_acceleration))
+                      kernel_variant=kernel_variant, store_acceleration=int(store_acceleration),
+                      has_start_time=int(start_time is not None),
+                      start_time=float(start_time) if start_time is not None else 0.0)
         h = C.c_void_p()
         wave = 1 if elastic_wave.lower() == "sh" else 0
         if database is not None:

@@ -29,7 +29,8 @@ def run_config(config: str, root: str | None = None, output_directory: str | Non
     stations, rx, rz = io.read_stations(cfg.stations)
     t = time.perf_counter()
     sim = Simulation2D(database=cfg.database, dt=cfg.dt, nstep=cfg.nstep,
-                       nstep_between_samples=cfg.nstep_between_samples, elastic_wave=cfg.elastic_wave)
+                       nstep_between_samples=cfg.nstep_between_samples, elastic_wave=cfg.elastic_wave,
+                       start_time=cfg.start_time)
     sim.set_sources(sources)
     sim.set_receivers(rx, rz, angle=cfg.angle, types=tuple(cfg.seismogram_types))
     sim.initialize()

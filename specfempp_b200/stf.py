@@ -54,13 +54,19 @@ def values(kind: str, t: np.ndarray, p, factor) -> np.ndarray:
     return fac * ((_f32(1.0) - _f32(2.0) * a * t * t) * np.exp(-a * t * t))
 
 
-def table(sources, dt: float, nstep: int) -> np.ndarray:
-    """[nstep, nsrc] float32 table of the sources' time functions (one shot)."""
+def table(sources, dt: float, nstep: int, start_time: float | None = None) -> np.ndarray:
+    """[nstep, nsrc] float32 table of the sources' time functions (one shot);
+    with ``start_time`` the run starts there and each source keeps its own
+    tshift (read_sources.cpp:155-161)."""
     st = [start(s, dt) for s in sources]
     t0 = min(t for t, _ in st)
+    shifts = [_f32(a - t0) for a, _ in st]
+    if start_time is not None:
+        t0 = _f32(start_time)
+        shifts = [_f32(getattr(s, "tshift", 0.0)) for s in sources]
     i = np.arange(nstep, dtype=_f32)
     out = np.zeros((nstep, len(sources)), np.float32)
     for k, s in enumerate(sources):
-        t = _f32(t0) + i * _f32(dt) - _f32(st[k][0] - t0)
+        t = _f32(t0) + i * _f32(dt) - shifts[k]
         out[:, k] = values(getattr(s, "stf", "ricker"), t, st[k][1], s.factor)
     return out

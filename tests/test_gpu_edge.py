@@ -121,3 +121,31 @@ def test_every_time_function_kind(sfg_lib, oracle_lib, which):
     for t in range(2):
         tol = 1e-5 if t == 0 else max(1e-5, 2.0 * rel_l2(ref[:, t], ref64[:, t]))
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (t, rel_l2(seis[:, t], ref[:, t]), tol)
+
+
+def test_given_start_time(sfg_lib, oracle_lib):
+    """A start time given by the caller (the configuration's t0): every
+    source keeps its own tshift; seismograms against the oracle at 1e-5, the
+    handle's t0 is the given one, and a start after the earliest source start
+    is refused."""
+    from oracle import runner
+    from specfempp_b200 import sfg
+    w = elastic(900)
+    s0 = w.sources[0]
+    srcs = [replace(s0, tshift=0.05), replace(s0, x=1200.0, z=2200.0, f0=14.0)]
+    case = workload_case(w, types=("displacement", "velocity"))
+    case.sources = srcs
+    case.start_time = -0.2
+    ref = runner.run(case, "f32", nthreads=8)["seis"]
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=900, start_time=-0.2)
+    sim.set_sources(srcs)
+    sim.set_receivers(w.rec_x, w.rec_z, types=("displacement", "velocity"))
+    sim.initialize()
+    sim.run(900)
+    assert abs(sim.info().t0 - (-0.2)) < 1e-7
+    seis = sim.seismograms()[0]
+    for t in range(2):
+        assert rel_l2(seis[:, t], ref[:, t]) <= 1e-5, (t, rel_l2(seis[:, t], ref[:, t]))
+    late = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=900, start_time=-0.01)
+    with pytest.raises(sfg.SfgError, match="start time"):
+        late.set_sources(srcs)

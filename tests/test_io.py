@@ -204,3 +204,25 @@ def test_sources_yaml_time_functions(tmp_path):
     got = io.read_sources(str(p))
     assert [s.stf for s in got] == ["heaviside", "gaussian_hdur", "gaussian", "dgaussian"]
     assert got[0].hdur == 0.1 and got[2].f0 == 3.0 and got[3].tshift == 0.5 and got[3].kind == "moment_tensor"
+
+
+def test_given_start_time_table_and_config(tmp_path):
+    """A configuration t0 starts the run there with every source's own tshift
+    (library table and oracle table agree); config parsing carries it."""
+    import yaml
+    from oracle import runner
+    from specfempp_b200 import io, sfg, stf
+    srcs_p = [sfg.Source(x=0, z=0, f0=5.0, factor=1.0, tshift=0.3), sfg.Source(x=0, z=0, f0=8.0, factor=2.0)]
+    srcs_o = [runner.Source(x=0, z=0, f0=5.0, factor=1.0, tshift=0.3), runner.Source(x=0, z=0, f0=8.0, factor=2.0)]
+    a = stf.table(srcs_p, 1e-3, 800, start_time=-0.5)
+    b = runner.stf_tables(srcs_o, 1e-3, 800, start=-0.5)
+    np.testing.assert_allclose(a, b, rtol=1e-6, atol=1e-6)
+    # the Ricker of the second source peaks at t = 0, i.e. step 500
+    assert int(np.argmax(a[:, 1])) == 500
+    cfg, _ = write_fixture_dir(os.path.join(GOLDEN, "HomogeneousElasticDomain.npz"), str(tmp_path))
+    with open(cfg) as f:
+        c = yaml.safe_load(f)
+    c["parameters"]["simulation-setup"]["solver"]["time-marching"]["time-scheme"]["t0"] = -0.5
+    with open(cfg, "w") as f:
+        yaml.safe_dump(c, f)
+    assert io.read_config(cfg, root=str(tmp_path)).start_time == -0.5
