@@ -57,6 +57,9 @@ class Mesh2D:
     # anisotropic elastic materials: (c11, c13, c15, c33, c35, c55) per
     # material, NaN rows for isotropic ones; None when every material is isotropic
     mat_aniso: np.ndarray | None = None
+    # [numat][8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c, mu_c, nu_c);
+    # NaN rows for other materials
+    mat_cosserat: np.ndarray | None = None
 
 
 def _records(buf: bytes):
@@ -126,6 +129,7 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
     mat_vp = np.zeros(numat)
     mat_vs = np.zeros(numat)
     mat_aniso = np.full((numat, 6), np.nan)
+    mat_cos = np.full((numat, 8), np.nan)
     for m in range(numat):
         vals = struct.unpack("<ii13d", take())
         n, indic = vals[0], vals[1]
@@ -139,6 +143,15 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
             mat_aniso[m] = v[1:7]
             mat_vp[m] = np.sqrt(v[4] / v[0])          # sqrt(c33 / rho)
             mat_vs[m] = np.sqrt(v[6] / v[0])          # sqrt(c55 / rho)
+            mat_medium[m] = ELASTIC
+            continue
+        if indic == 5:
+            # isotropic Cosserat elastic (P-SV-T): rho, kappa, mu, nu, j,
+            # lambda_c, mu_c, nu_c (read_material_properties.cpp:366-395)
+            mat_cos[m] = v[0:8]
+            mat_rho[m] = v[0]
+            mat_vp[m] = np.sqrt((v[1] + 4.0 / 3.0 * v[2]) / v[0])
+            mat_vs[m] = np.sqrt(v[2] / v[0])
             mat_medium[m] = ELASTIC
             continue
         if indic != 1:
@@ -202,4 +215,5 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
                   free_type=np.asarray(free_type, np.int32),
                   coupled_pairs=np.asarray(pairs, np.int32).reshape(-1, 2),
                   title=title, extra=extra,
-                  mat_aniso=mat_aniso if np.isfinite(mat_aniso).any() else None)
+                  mat_aniso=mat_aniso if np.isfinite(mat_aniso).any() else None,
+                  mat_cosserat=mat_cos if np.isfinite(mat_cos).any() else None)

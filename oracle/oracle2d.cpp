@@ -210,6 +210,8 @@ struct Sim {
   std::vector<T> p_kappa, p_mu, p_rho, p_rhoinv;
   // anisotropic elastic (when in.aniso): c11, c13, c15, c33, c35, c55 per point
   std::vector<T> p_c[6];
+  // Cosserat (when in.cosserat): rho, kappa, mu, nu, j, lambda_c, mu_c, nu_c
+  std::vector<T> p_cs[8];
   // Stacey point data per element (dense, tag 0/1)
   std::vector<uint8_t> st_tag, fs_tag;   // [nspec][25]
   std::vector<T> st_nx, st_nz, st_w;     // [nspec][25]
@@ -222,7 +224,7 @@ struct Sim {
   struct CPoint { int ispec, iz, ix, iglob; T nx, nz, fac; };
   std::vector<CPoint> cpl_ac, cpl_el;   // self acoustic / self elastic
   // sources
-  struct Src { int ispec; int medium; T arr[2][NP]; int ncomp; std::vector<T> stf; };
+  struct Src { int ispec; int medium; T arr[3][NP]; int ncomp; std::vector<T> stf; };
   std::vector<Src> srcs;
   struct Rec { int ispec; T h[NP]; };
   std::vector<Rec> recs;
@@ -239,7 +241,7 @@ struct Sim {
       for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
     }
     dt = T(in.dt);
-    ncomp_el = in.elastic_sh ? 1 : 2;
+    ncomp_el = in.cosserat ? 3 : in.elastic_sh ? 1 : 2;
     number_points();
     geometry();
     properties();
@@ -362,6 +364,17 @@ struct Sim {
         p_rho[p] = rho;
       }
     }
+    if (in.cosserat) {
+      if (in.elastic_sh || in.aniso) throw std::runtime_error("Cosserat media are P-SV-T only");
+      for (int k = 0; k < 8; ++k) {
+        p_cs[k].resize(n);
+        for (size_t p = 0; p < n; ++p) p_cs[k][p] = T(in.cosserat[p * 8 + k]);
+      }
+      for (size_t p = 0; p < n; ++p)
+        if (medium[p / NP] == MED_ELASTIC) {
+          p_rho[p] = p_cs[0][p]; p_kappa[p] = p_cs[1][p]; p_mu[p] = p_cs[2][p];
+        }
+    }
     if (in.aniso) {
       if (in.elastic_sh) throw std::runtime_error("anisotropic SH is outside this path");
       for (int k = 0; k < 6; ++k) {
@@ -377,7 +390,13 @@ struct Sim {
   T rho_vp(size_t p) const {
     return in.aniso ? std::sqrt(p_rho[p] * p_c[3][p]) : std::sqrt(lp2m(p) / p_rho[p]) * p_rho[p];
   }
-  T rho_vs(size_t p) const { return in.aniso ? std::sqrt(p_rho[p] * p_c[5][p]) : std::sqrt(p_rho[p] * p_mu[p]); }
+  T rho_vs(size_t p) const {
+    if (in.cosserat)   // rho sqrt((mu + nu) / rho) (stacey.tpp:183-230)
+      return p_rho[p] * std::sqrt((p_mu[p] + p_cs[3][p]) / p_rho[p]);
+    return in.aniso ? std::sqrt(p_rho[p] * p_c[5][p]) : std::sqrt(p_rho[p] * p_mu[p]);
+  }
+  // Cosserat rotational impedance j sqrt((mu_c + nu_c) / j)
+  T j_vt(size_t p) const { return p_cs[4][p] * std::sqrt((p_cs[6][p] + p_cs[7][p]) / p_cs[4][p]); }
   T rho_vpinv(size_t p) const { return std::sqrt(p_rhoinv[p] * (T(1) / p_kappa[p])); }
 
   void normal(size_t p, int type, T &nx, T &nz) const {
@@ -429,6 +448,7 @@ struct Sim {
       auto [e1, t1] = kv.second[0];
       auto [e2, t2] = kv.second[1];
       if (medium[e1] == medium[e2]) continue;
+      if (ncomp_el == 3) throw std::runtime_error("Cosserat media are not coupled to acoustic ones here");
       for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
         for (int iz = 0; iz < NG; ++iz)
           for (int ix = 0; ix < NG; ++ix) {
@@ -462,6 +482,7 @@ struct Sim {
         fac[c] = ((vn * dn[c] / (j1 * j1)) * (rho_vp(p) - rho_vs(p))) + vel[c] * rho_vs(p);
       acc[0] += T(-1) * fac[0] * j1 * st_w[p];
       acc[1] += T(-1) * fac[1] * j1 * st_w[p];
+      if (ncomp_el == 3) acc[2] += T(-1) * j_vt(p) * vel[2] * j1 * st_w[p];
     }
   }
 
@@ -488,9 +509,10 @@ struct Sim {
             minv_a[g] += m;
           } else {
             is_el_glob[g] = 1;
-            T m[2] = {p_rho[p] * fac, p_rho[p] * fac};
+            // Cosserat: rho, rho, j (isotropic_cosserat/mass_matrix.tpp)
+            T m[3] = {p_rho[p] * fac, p_rho[p] * fac, ncomp_el == 3 ? p_cs[4][p] * fac : T(0)};
             if (st_tag[p]) {
-              T v[2] = {T(-1) * dt * T(0.5), T(-1) * dt * T(0.5)};
+              T v[3] = {T(-1) * dt * T(0.5), T(-1) * dt * T(0.5), T(-1) * dt * T(0.5)};
               stacey(p, v, m);
             }
             for (int c = 0; c < ncomp_el; ++c) minv_e[size_t(g) * ncomp_el + c] += m[c];
@@ -598,6 +620,7 @@ struct Sim {
   void moment_tensor_array(Src &S, int e, double xi, double ga, double mxx, double mzz, double mxz) {
     if (S.medium != MED_ELASTIC || ncomp_el != 2)
       throw std::runtime_error("moment-tensor sources need an elastic P-SV element");
+    for (int q = 0; q < NP; ++q) S.arr[2][q] = 0;
     S.ncomp = 2;
     double zd[NG], wd[NG], hx[NG], hpx[NG], hg[NG], hpg[NG];
     gll_nodes(zd, wd);
@@ -633,10 +656,11 @@ struct Sim {
       if (in.src_kind && in.src_kind[s] == 1) {
         moment_tensor_array(S, e, xi, ga, in.src_mxx[s], in.src_mzz[s], in.src_mxz[s]);
       } else {
-        T fv[2];
+        T fv[3] = {0, 0, 0};
         if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
         else {
-          S.ncomp = 2;
+          // Cosserat: (sin, cos, 0) (vector_source/force_source.cpp:62-67)
+          S.ncomp = ncomp_el;
           T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
           fv[0] = std::sin(ang); fv[1] = std::cos(ang);
         }
@@ -674,7 +698,7 @@ struct Sim {
   template <typename AddFn>
   void stiffness_element(int e, int ncomp, const std::vector<T> &u, const std::vector<T> &v,
                          AddFn add) const {
-    T fu[NP][2], F[NP][2][2];
+    T fu[NP][3], F[NP][3][2], Sa[NP][2];   // Sa: Cosserat sigma_xz, sigma_zx
     const int *ib = &ibool[size_t(e) * NP];
     for (int q = 0; q < NP; ++q)
       for (int c = 0; c < ncomp; ++c) fu[q][c] = u[size_t(ib[q]) * ncomp + c];
@@ -683,19 +707,36 @@ struct Sim {
       for (int ix = 0; ix < NG; ++ix) {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
-        T dxi[2] = {0, 0}, dga[2] = {0, 0};
+        T dxi[3] = {0, 0, 0}, dga[3] = {0, 0, 0};
         for (int l = 0; l < NG; ++l)
           for (int c = 0; c < ncomp; ++c) {
             dxi[c] += hp[ix][l] * fu[iz * NG + l][c];
             dga[c] += hp[iz][l] * fu[l * NG + ix][c];
           }
-        T du[2][2];
+        T du[3][2];
         for (int c = 0; c < ncomp; ++c) {
           du[c][0] = xix[p] * dxi[c] + gax[p] * dga[c];
           du[c][1] = xiz[p] * dxi[c] + gaz[p] * dga[c];
         }
-        T S[2][2];
-        if (acoustic) {
+        T S[3][2];
+        if (!acoustic && ncomp == 3) {
+          // Cosserat P-SV-T stress (isotropic_cosserat/stress.hpp, cosserat_stress.hpp):
+          // lambda = kappa - 2/3 mu; rows u_x: (sxx, szx), u_z: (sxz, szz),
+          // rotation: (mu_c + nu_c) grad(phi); sxz += 2 nu phi, szx -= 2 nu phi
+          const T mu = p_mu[p], nu = p_cs[3][p], lam = p_kappa[p] - T(2.0 / 3.0) * mu;
+          const T phi = fu[q][2];
+          const T dv = du[0][0] + du[1][1];
+          const T sxx = lam * dv + T(2) * mu * du[0][0];
+          const T szz = lam * dv + T(2) * mu * du[1][1];
+          T sxz = mu * (du[1][0] + du[0][1]) + nu * (du[1][0] - du[0][1]);
+          T szx = mu * (du[0][1] + du[1][0]) + nu * (du[0][1] - du[1][0]);
+          szx -= T(2) * nu * phi;
+          sxz += T(2) * nu * phi;
+          const T mc = p_cs[6][p] + p_cs[7][p];
+          S[0][0] = sxx; S[0][1] = szx; S[1][0] = sxz; S[1][1] = szz;
+          S[2][0] = mc * du[2][0]; S[2][1] = mc * du[2][1];
+          Sa[q][0] = sxz; Sa[q][1] = szx;
+        } else if (acoustic) {
           S[0][0] = p_rhoinv[p] * du[0][0];
           S[0][1] = p_rhoinv[p] * du[0][1];
         } else if (ncomp == 1) {
@@ -724,15 +765,18 @@ struct Sim {
       for (int ix = 0; ix < NG; ++ix) {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
-        T t1[2] = {0, 0}, t2[2] = {0, 0};
+        T t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
         for (int l = 0; l < NG; ++l) {
           for (int c = 0; c < ncomp; ++c) t1[c] += F[iz * NG + l][c][0] * hp[l][ix] * w[l];
           for (int c = 0; c < ncomp; ++c) t2[c] += F[l * NG + ix][c][1] * hp[l][iz] * w[l];
         }
-        T acc[2];
+        T acc[3];
         for (int c = 0; c < ncomp; ++c) acc[c] = T(-1) * (w[iz] * t1[c] + w[ix] * t2[c]);
+        // Cosserat couple stress: -W (sigma_xz - sigma_zx) on the rotation
+        // (compute_stiffness_interaction.tpp:216-229, cosserat_couple_stress.hpp)
+        if (!acoustic && ncomp == 3) acc[2] -= (Sa[q][0] - Sa[q][1]) * (w[ix] * w[iz] * jac[p]);
         if (st_tag[p]) {
-          T vel[2];
+          T vel[3];
           for (int c = 0; c < ncomp; ++c) vel[c] = v[size_t(ib[q]) * ncomp + c];
           stacey(p, vel, acc);
         }
@@ -841,9 +885,13 @@ struct Sim {
         }
       return;
     }
-    if (type == 3) {
-      // elastic pressure: -(lambda + 2/3 mu) div u (elastic/isotropic/wavefield.hpp:57-89)
-      if (ncomp_el != 2) return;
+    const int nc = ncomp_el;
+    if (type == 3 || type == 5 || type == 6) {
+      // elastic pressure -(lambda + 2/3 mu) div u (elastic/isotropic/wavefield.hpp:57-89;
+      // Cosserat: -kappa div u); Cosserat curl du_x/dz - du_z/dx and intrinsic
+      // rotation phi - curl / 2 (isotropic_cosserat/wavefield.hpp)
+      if (nc == 1) return;
+      if ((type == 5 || type == 6) && nc != 3) return;
       for (int iz = 0; iz < NG; ++iz)
         for (int ix = 0; ix < NG; ++ix) {
           const int q = iz * NG + ix;
@@ -851,19 +899,31 @@ struct Sim {
           T dxi[2] = {0, 0}, dga[2] = {0, 0};
           for (int l = 0; l < NG; ++l)
             for (int c = 0; c < 2; ++c) {
-              dxi[c] += hp[ix][l] * ue[size_t(ib[iz * NG + l]) * 2 + c];
-              dga[c] += hp[iz][l] * ue[size_t(ib[l * NG + ix]) * 2 + c];
+              dxi[c] += hp[ix][l] * ue[size_t(ib[iz * NG + l]) * nc + c];
+              dga[c] += hp[iz][l] * ue[size_t(ib[l * NG + ix]) * nc + c];
             }
-          const T dux = xix[p] * dxi[0] + gax[p] * dga[0];
-          const T duz = xiz[p] * dxi[1] + gaz[p] * dga[1];
-          const T lam = lp2m(p) - T(2) * p_mu[p];
-          out[0] += R.h[q] * (T(-1.0) * ((lam + T(2.0 / 3.0) * p_mu[p]) * (dux + duz)));
+          if (type == 3) {
+            const T dux = xix[p] * dxi[0] + gax[p] * dga[0];
+            const T duz = xiz[p] * dxi[1] + gaz[p] * dga[1];
+            const T k = nc == 3 ? p_kappa[p] : (lp2m(p) - T(2) * p_mu[p]) + T(2.0 / 3.0) * p_mu[p];
+            out[0] += R.h[q] * (T(-1.0) * (k * (dux + duz)));
+          } else {
+            const T duxz = xiz[p] * dxi[0] + gaz[p] * dga[0];   // d u_x / dz
+            const T duzx = xix[p] * dxi[1] + gax[p] * dga[1];   // d u_z / dx
+            const T curl = duxz - duzx;
+            out[0] += R.h[q] * (type == 6 ? curl : ue[size_t(ib[q]) * nc + 2] - T(0.5) * curl);
+          }
         }
+      return;
+    }
+    if (type == 4) {                       // Cosserat rotation
+      if (nc != 3) return;
+      for (int q = 0; q < NP; ++q) out[0] += R.h[q] * ue[size_t(ib[q]) * nc + 2];
       return;
     }
     const std::vector<T> &f = type == 0 ? ue : type == 1 ? ve : ae;
     for (int q = 0; q < NP; ++q)
-      for (int c = 0; c < ncomp_el; ++c) out[c] += R.h[q] * f[size_t(ib[q]) * ncomp_el + c];
+      for (int c = 0; c < std::min(nc, 2); ++c) out[c] += R.h[q] * f[size_t(ib[q]) * nc + c];
   }
 
   void run(double *seis, int nthreads) {

@@ -23,7 +23,8 @@ typedef struct OracleInput2D {
   const double *rec_x, *rec_z;
   double rec_angle;
   int ntypes;
-  const int *seis_types;   /* 0 displacement 1 velocity 2 acceleration 3 pressure */
+  const int *seis_types;   /* 0 displacement 1 velocity 2 acceleration 3 pressure
+                              4 rotation 5 intrinsic rotation 6 curl (Cosserat) */
   double dt;
   int nstep, nstep_between_samples;
   /* 0: setup geometry (Jacobians, point location, interpolants) in FP64 and
@@ -37,6 +38,10 @@ typedef struct OracleInput2D {
   /* optional anisotropic elastic constants per GLL point [nspec][25][6]
    * (c11, c13, c15, c33, c35, c55); NULL: isotropic from rho, vp, vs */
   const double *aniso;
+  /* optional Cosserat elastic constants per GLL point [nspec][25][8] (rho,
+   * kappa, mu, nu, j, lambda_c, mu_c, nu_c): three components (u_x, u_z,
+   * rotation); NULL: none */
+  const double *cosserat;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

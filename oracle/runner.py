@@ -25,7 +25,8 @@ from .database2d import Mesh2D, read_database
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
 
-SEIS_TYPES = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3}
+SEIS_TYPES = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3,
+              "rotation": 4, "intrinsic_rotation": 5, "curl": 6}
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -47,7 +48,7 @@ class OracleInput2D(C.Structure):
         ("dt", C.c_double), ("nstep", C.c_int), ("nstep_between_samples", C.c_int),
         ("setup_in_run_precision", C.c_int),
         ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
-        ("aniso", _dp),
+        ("aniso", _dp), ("cosserat", _dp),
     ]
 
 
@@ -181,6 +182,22 @@ def aniso_points(case):
     return np.ascontiguousarray(out)
 
 
+def cosserat_points(case):
+    """[nspec, 25, 8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
+    mu_c, nu_c) when the mesh has Cosserat materials, else None; every elastic
+    element must then be Cosserat."""
+    m = case.mesh
+    mc = getattr(m, "mat_cosserat", None)
+    if mc is None or not np.isfinite(mc).any():
+        return None
+    per = np.asarray(mc)[m.kmato]                                     # [nspec, 8]
+    elastic = np.asarray(m.mat_medium)[m.kmato] == 1
+    if not np.all(np.isfinite(per[elastic])):
+        raise ValueError("a mesh with Cosserat materials must be Cosserat in every elastic element")
+    per = np.where(np.isfinite(per), per, 0.0)
+    return np.ascontiguousarray(np.repeat(per[:, None, :], 25, axis=1))
+
+
 def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: bool = False):
     """Run the oracle; returns dict with 'seis' [nsig, ntypes, nrec, 2], 't0', 'times'."""
     m = case.mesh
@@ -243,6 +260,8 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     inp.src_mxz = _ptr(arr([getattr(s, "mxz", 0.0) for s in srcs], np.float64), _dp)
     aniso = aniso_points(case)
     inp.aniso = _ptr(arr(aniso, np.float64), _dp) if aniso is not None else None
+    cos = cosserat_points(case)
+    inp.cosserat = _ptr(arr(cos, np.float64), _dp) if cos is not None else None
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()
@@ -250,7 +269,7 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     final = None
     if want_final:
         nglob = L.oracle2d_count_nglob(C.byref(inp))
-        final = {"elastic": np.zeros((nglob, 1 if case.elastic_sh else 2)),
+        final = {"elastic": np.zeros((nglob, 3 if cos is not None else 1 if case.elastic_sh else 2)),
                  "acoustic": np.zeros(nglob),
                  "ibool": np.zeros((m.nspec, 25), np.int32)}
         out.final_u_elastic = _ptr(final["elastic"], _dp)

@@ -33,7 +33,8 @@ def golden_case(name, nstep=None):
                   mat_vs=z["mat_vs"], abs_ispec=z["abs_ispec"], abs_type=z["abs_type"],
                   free_ispec=z["free_ispec"], free_type=z["free_type"],
                   coupled_pairs=np.zeros((0, 2), np.int32),
-                  mat_aniso=z["mat_aniso"] if "mat_aniso" in z else None)
+                  mat_aniso=z["mat_aniso"] if "mat_aniso" in z else None,
+                  mat_cosserat=z["mat_cosserat"] if "mat_cosserat" in z else None)
     srcs = []
     for s in z["src"]:
         mt = len(s) > 7 and bool(s[7])

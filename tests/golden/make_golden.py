@@ -35,6 +35,9 @@ FIXTURES = {
     "HomogeneousAcousticDomainCompositeStaceyDirichletBC": ("BXX", "BXZ"),
     "HomogeneousElasticDomainMomentTensorHeaviside": ("BXX", "BXZ"),
     "HomogeneousElasticDomainWAdjacencyMap": ("BXX", "BXZ"),
+    "HomogeneousIsotropicCosseratDomainNu0": ("BXX", "BXZ"),
+    "HomogeneousIsotropicCosseratDomain": ("BXX", "BXZ"),
+    "HomogeneousIsotropicCosseratDomainHighFrequency": ("BXX", "BXZ"),
 }
 
 # time-function codes stored in the fixtures' source rows
@@ -57,6 +60,21 @@ def make(ref_root: str, name: str, comps) -> str:
                 tr[r, c, : len(v)] = v[: case.nstep]
                 t0 = t[0]
         traces[ext] = tr
+    # scalar traces: pressure (PRE) and, for Cosserat media, rotation,
+    # intrinsic rotation and curl (BXY)
+    for ext, ch in (("semp", "PRE"), ("semr", "BXY"), ("semir", "BXY"), ("semc", "BXY")):
+        if not os.path.exists(os.path.join(d, "traces", f"{case.stations[0][0]}.{case.stations[0][1]}.S2.{ch}.{ext}")):
+            continue
+        tr = np.zeros((len(case.stations), 1, case.nstep), np.float32)
+        for r, (net, sta) in enumerate(case.stations):
+            t, v = runner.read_trace(os.path.join(d, "traces", f"{net}.{sta}.S2.{ch}.{ext}"))
+            tr[r, 0, : len(v)] = v[: case.nstep]
+        traces[ext] = tr
+    extra = {}
+    if getattr(m, "mat_aniso", None) is not None:
+        extra["mat_aniso"] = m.mat_aniso
+    if getattr(m, "mat_cosserat", None) is not None:
+        extra["mat_cosserat"] = m.mat_cosserat
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(
         out, nspec=m.nspec, npgeo=m.npgeo, ngnod=m.ngnod, coorg=m.coorg, knods=m.knods,
@@ -70,8 +88,7 @@ def make(ref_root: str, name: str, comps) -> str:
         rec_x=case.rec_x, rec_z=case.rec_z, dt=case.dt, nstep=case.nstep, rec_angle=case.rec_angle,
         stations=np.asarray([f"{n}.{s}" for n, s in case.stations]), traces=traces["semd"],
         **{f"traces_{k}": v for k, v in traces.items() if k != "semd"},
-        trace_t0=t0, components=np.asarray(comps), elastic_sh=int(case.elastic_sh),
-        **({"mat_aniso": m.mat_aniso} if getattr(m, "mat_aniso", None) is not None else {}))
+        trace_t0=t0, components=np.asarray(comps), elastic_sh=int(case.elastic_sh), **extra)
     return out
 
 
