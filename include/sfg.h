@@ -52,8 +52,13 @@ enum {
 enum { SFG_EDGE_BOTTOM = 0, SFG_EDGE_RIGHT = 1, SFG_EDGE_TOP = 2, SFG_EDGE_LEFT = 3 };
 enum { SFG_MEDIUM_ACOUSTIC = 0, SFG_MEDIUM_ELASTIC = 1 };
 enum { SFG_WAVE_PSV = 0, SFG_WAVE_SH = 1 };
+/* Seismogram types; rotation, intrinsic rotation (rotation minus half the
+ * curl) and curl (du_x/dz - du_z/dx) exist in Cosserat media
+ * (include/medium/dim2/elastic/isotropic_cosserat/wavefield.hpp); scalar
+ * types fill the first component. */
 enum { SFG_SEIS_DISPLACEMENT = 0, SFG_SEIS_VELOCITY = 1, SFG_SEIS_ACCELERATION = 2,
-       SFG_SEIS_PRESSURE = 3 };
+       SFG_SEIS_PRESSURE = 3, SFG_SEIS_ROTATION = 4, SFG_SEIS_INTRINSIC_ROTATION = 5,
+       SFG_SEIS_CURL = 6 };
 /* Source-time functions (core/specfem/source_time_functions): Ricker, Dirac
  * (f0 = 1/(10 dt)), Gaussian and its derivative by f0, Gaussian and Heaviside
  * (error function) by half duration hdur (at least 5 dt; start time
@@ -83,6 +88,10 @@ typedef struct sfg_mesh2d_desc {
   const double *mat_aniso;       /* optional [numat][6] anisotropic elastic constants
                                     (c11, c13, c15, c33, c35, c55; NaN rows: isotropic);
                                     mat_vp = sqrt(c33/rho), mat_vs = sqrt(c55/rho) there */
+  const double *mat_cosserat;    /* optional [numat][8] isotropic Cosserat constants (rho,
+                                    kappa, mu, nu, j, lambda_c, mu_c, nu_c; NaN rows: other
+                                    materials); the elastic medium then has three
+                                    components (u_x, u_z, rotation), P-SV only */
 } sfg_mesh2d_desc;
 
 typedef struct sfg_options {
@@ -129,6 +138,8 @@ typedef struct sfg_info {
   size_t device_bytes;
   int kernels_per_step;
   int elements_per_block, kernel_variant; /* launch shape in use */
+  int ncomp_elastic;             /* components of the elastic fields: 2 P-SV, 1 SH,
+                                    3 Cosserat (u_x, u_z, rotation) */
 } sfg_info;
 
 /* ---- life cycle ---- */

@@ -227,7 +227,19 @@ bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
         m.mat_medium[i] = 1;
         continue;
       }
-      if (indic != 1) throw std::runtime_error("only isotropic and anisotropic elastic / acoustic materials are supported");
+      if (indic == 5) {
+        // isotropic Cosserat elastic (P-SV-T): rho, kappa, mu, nu, j, lambda_c,
+        // mu_c, nu_c (read_material_properties.cpp:366-395)
+        if (m.mat_cosserat.empty()) m.mat_cosserat.assign(size_t(m.numat) * 8, std::nan(""));
+        for (int k = 0; k < 8; ++k) m.mat_cosserat[size_t(i) * 8 + k] = v[k];
+        m.mat_rho[i] = v[0];
+        m.mat_vp[i] = std::sqrt((v[1] + 4.0 / 3.0 * v[2]) / v[0]);
+        m.mat_vs[i] = std::sqrt(v[2] / v[0]);
+        m.mat_medium[i] = 1;
+        continue;
+      }
+      if (indic != 1)
+        throw std::runtime_error("only isotropic, anisotropic and Cosserat elastic and acoustic materials are supported");
       m.mat_rho[i] = v[0]; m.mat_vp[i] = v[1]; m.mat_vs[i] = v[2];
       m.mat_medium[i] = (v[2] == 0.0) ? 0 : 1;
     }
@@ -306,6 +318,12 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
   };
   a.el.aniso = false;
   for (int ce = 0; ce < a.el.nspec; ++ce) a.el.aniso |= aniso_of(a.el.elem_mesh[ce]) != nullptr;
+  a.el.cosserat = a.el.ncomp == 3;
+  if (a.el.cosserat && a.el.niface > 0)
+    throw std::runtime_error("Cosserat media are not coupled to acoustic ones here");
+  if (a.el.cosserat && (a.el.aniso || !m.prho.empty()))
+    throw std::runtime_error("Cosserat media: material constants only (no anisotropy, no point models)");
+  auto cos_of = [&](int e) { return &m.mat_cosserat[size_t(m.kmato[e]) * 8]; };
   if (a.el.aniso && (a.el.ncomp != 2 || !m.prho.empty()))
     throw std::runtime_error("anisotropic media: P-SV with material constants only (no SH, no point models)");
   for (int med = 0; med < 2; ++med) {
@@ -314,13 +332,22 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
     D.prop0.resize(n);
     D.prop1.resize(n);
     for (auto *v : {&D.prop2, &D.prop3, &D.prop4, &D.prop5}) v->assign(med == 1 && D.aniso ? n : 0, 0.0f);
+    if (med == 1 && D.cosserat) for (auto *v : {&D.prop2, &D.prop3}) v->assign(n, 0.0f);
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
       for (int q = 0; q < NPTS; ++q) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
-        if (med == 1 && D.aniso) {
+        if (med == 1 && D.cosserat) {
+          // lambda = kappa - 2/3 mu, mu, nu, mu_c + nu_c
+          // (include/medium/dim2/elastic/isotropic_cosserat/properties.hpp, stress.hpp)
+          const double *c = cos_of(e);
+          D.prop0[pc] = float(c[1] - 2.0 / 3.0 * c[2]);
+          D.prop1[pc] = float(c[2]);
+          D.prop2[pc] = float(c[3]);
+          D.prop3[pc] = float(c[6] + c[7]);
+        } else if (med == 1 && D.aniso) {
           // c11, c13, c15, c33, c35, c55 (include/medium/dim2/elastic/anisotropic/
           // properties.hpp); isotropic elements of the medium in the same form
           const double *c = aniso_of(e);
@@ -352,7 +379,14 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
-        if (med == 1 && D.aniso) {
+        if (med == 1 && D.cosserat) {
+          // rho vp = sqrt((kappa + 4/3 mu) rho), rho vs = rho sqrt((mu + nu) / rho),
+          // j sqrt((mu_c + nu_c) / j) (stacey.tpp:183-230)
+          const double *c = cos_of(e);
+          D.bc_imp0[k] = float(std::sqrt((c[1] + 4.0 / 3.0 * c[2]) * c[0]));
+          D.bc_imp1[k] = float(c[0] * std::sqrt((c[2] + c[3]) / c[0]));
+          D.bc_imp2[k] = float(c[4] * std::sqrt((c[6] + c[7]) / c[4]));
+        } else if (med == 1 && D.aniso) {
           // rho vp = sqrt(rho c33), rho vs = sqrt(rho c55)
           // (include/medium/dim2/elastic/anisotropic/properties.hpp:88-94)
           D.bc_imp0[k] = float(std::sqrt(rho * double(D.prop3[pc])));
@@ -379,7 +413,7 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
     MediumData &D = *Dp;
     D.stacey_pt.clear();
     D.stacey_c.clear();
-    if (D.nspec && !D.aniso) {
+    if (D.nspec && !D.aniso && !D.cosserat) {
       std::unordered_map<int, size_t> slot;
       for (int ce = 0; ce < D.nspec; ++ce) {
         if (D.bc_slot[ce] < 0) continue;
@@ -430,9 +464,11 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
           const double fac = w[ix] * w[iz] * a.jac_d[pm];
           double rho, vp, vs;
           model(e, pm, rho, vp, vs);
-          double mc[2];
+          double mc[3] = {0, 0, 0};
           if (med == 1) mc[0] = mc[1] = rho * fac;
           else mc[0] = (1.0 / double(D.prop1[pc])) * fac;
+          // Cosserat: rho, rho, j (isotropic_cosserat/mass_matrix.tpp)
+          if (med == 1 && D.cosserat) mc[2] = m.mat_cosserat[size_t(m.kmato[e]) * 8 + 4] * fac;
           if (D.bc_slot[ce] >= 0) {
             const size_t k = size_t(D.bc_slot[ce]) * NPTS + q;
             if (D.bc_w[k] != 0.0f) {
@@ -450,6 +486,7 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
                                    vv * double(D.bc_imp1[k]);
                   mc[c] += -1.0 * f * j1 * wq;
                 }
+                if (D.cosserat) mc[2] += -1.0 * double(D.bc_imp2[k]) * vv * j1 * wq;
               }
             }
           }
@@ -659,6 +696,18 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
     D.ncomp = med == 1 ? (m.elastic_wave == 1 ? 1 : 2) : 1;
+    if (med == 1 && !m.mat_cosserat.empty()) {
+      // a Cosserat elastic medium: every elastic element Cosserat, P-SV-T
+      bool any = false, all = true;
+      for (int e = 0; e < nspec; ++e)
+        if (a.mesh_medium[e] == 1) {
+          const bool c = std::isfinite(m.mat_cosserat[size_t(m.kmato[e]) * 8]);
+          any |= c; all &= c;
+        }
+      if (any && (!all || m.elastic_wave == 1))
+        throw std::runtime_error("Cosserat media: every elastic element Cosserat, P-SV only");
+      if (any) D.ncomp = 3;
+    }
     int ncol = 0;
     for (int e = 0; e < nspec; ++e)
       if (a.mesh_medium[e] == med) ncol = std::max(ncol, color[e] + 1);
@@ -736,7 +785,7 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       if (bc.count(D.elem_mesh[ce])) D.bc_slot[ce] = ns++;
     const size_t n = size_t(ns) * NPTS;
     D.bc_w.assign(n, 0); D.bc_nx.assign(n, 0); D.bc_nz.assign(n, 0); D.bc_j1.assign(n, 0);
-    D.bc_imp0.assign(n, 0); D.bc_imp1.assign(n, 0); D.bc_keep.assign(n, 1.0f);
+    D.bc_imp0.assign(n, 0); D.bc_imp1.assign(n, 0); D.bc_keep.assign(n, 1.0f); D.bc_imp2.assign(n, 0);
     for (int ce = 0; ce < D.nspec; ++ce) {
       if (D.bc_slot[ce] < 0) continue;
       const auto &v = bc[D.elem_mesh[ce]];

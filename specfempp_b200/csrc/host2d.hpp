@@ -28,6 +28,9 @@ struct Mesh2D {
   // optional anisotropic elastic constants [numat][6] (c11, c13, c15, c33,
   // c35, c55); rows of NaN for isotropic materials
   std::vector<double> mat_aniso;
+  // optional isotropic Cosserat constants [numat][8] (rho, kappa, mu, nu, j,
+  // lambda_c, mu_c, nu_c); rows of NaN for other materials
+  std::vector<double> mat_cosserat;
   std::vector<float> prho, pvp, pvs;  // optional [nspec][25]
   std::vector<int> abs_ispec, abs_type, free_ispec, free_type;
   int elastic_wave = 0;               // 0 P-SV, 1 SH
@@ -56,10 +59,14 @@ struct MediumData {
   // anisotropic elastic medium: prop0..prop5 = c11, c13, c15, c33, c35, c55
   bool aniso = false;
   std::vector<float> prop2, prop3, prop4, prop5;
+  // isotropic Cosserat medium (ncomp 3: u_x, u_z, rotation): prop0 = lambda =
+  // kappa - 2/3 mu, prop1 = mu, prop2 = nu, prop3 = mu_c + nu_c; bc_imp2 the
+  // rotational Stacey impedance j sqrt((mu_c + nu_c) / j)
+  bool cosserat = false;
   std::vector<float> minv;            // [nglob][ncomp]
   // Stacey / free-surface: slot per element (-1 none), compact [nslot][25]
   std::vector<int> bc_slot;
-  std::vector<float> bc_w, bc_nx, bc_nz, bc_j1, bc_imp0, bc_imp1, bc_keep;
+  std::vector<float> bc_w, bc_nx, bc_nz, bc_j1, bc_imp0, bc_imp1, bc_keep, bc_imp2;
   // coupling with the other medium: the first niface points of the medium's
   // numbering lie on coupled edges; per point the sum over the coupled edges
   // of GLL weight * outward normal, and the other medium's id of the point

@@ -59,6 +59,7 @@ struct MedArgs {
   const int *__restrict__ bc_slot;
   const float *__restrict__ bc_w, *__restrict__ bc_nx, *__restrict__ bc_nz, *__restrict__ bc_j1,
       *__restrict__ bc_imp0, *__restrict__ bc_imp1, *__restrict__ bc_keep;
+  const float *__restrict__ bc_imp2;   // Cosserat rotational impedance
   const int *__restrict__ src_head;
   const float *__restrict__ u, *__restrict__ v;
   float *__restrict__ accum;
@@ -89,16 +90,23 @@ __device__ __forceinline__ void load_quad(const Quad &Q, float *shp, float *shpw
 
 // Elastic element block; EK 0 = P-SV (two components), 1 = SH (one component),
 // 2 = anisotropic P-SV (prop0..prop5 = c11, c13, c15, c33, c35, c55;
-// include/medium/dim2/elastic/anisotropic/stress.hpp).
+// include/medium/dim2/elastic/anisotropic/stress.hpp), 3 = isotropic Cosserat
+// P-SV-T (u_x, u_z, rotation phi; prop0..prop3 = lambda, mu, nu, mu_c + nu_c;
+// isotropic_cosserat/stress.hpp, cosserat_stress.hpp: the rows of u_x and u_z
+// carry (sxx, szx) and (sxz, szz) with sxz += 2 nu phi, szx -= 2 nu phi, the
+// rotation row (mu_c + nu_c) grad(phi); after the divergence the rotation
+// gets -W (sxz - szx), W = w_x w_z |J| (compute_stiffness_interaction.tpp:
+// 216-229, cosserat_couple_stress.hpp), then Stacey with the rotational
+// impedance on phi (stacey.tpp:183-230)).
 // LOCAL: write the element's contribution to its own slot of A.r (summed per
 // point later by the update) instead of adding it into the accumulator.
 template <int E, int EK, bool LOCAL>
 __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs &A, int ebase,
                                               unsigned char *smem, float *shp, float *shpw,
                                               float *sw) {
-  constexpr int NC = EK == 1 ? 1 : 2;
-  float *su = reinterpret_cast<float *>(smem);                               // [E][NC][25]
-  float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * 2);  // [E][NC][2][25]
+  constexpr int NC = EK == 1 ? 1 : (EK == 3 ? 3 : 2);
+  float *su = reinterpret_cast<float *>(smem);                                // [E][NC][25]
+  float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * NC);  // [E][NC][2][25]
   const int tid = threadIdx.x;
   const int le = tid / NP, q = tid - le * NP;
   const int e = ebase + le;
@@ -110,7 +118,13 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
               gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
   const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
   float uu[NC], acc[NC];
-  if (NC == 2) {
+  if (NC == 3) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      uu[c] = act ? A.u[size_t(g) * 3 + c] : 0.f;
+      if (!LOCAL) acc[c] = act ? A.accum[size_t(g) * 3 + c] : 0.f;
+    }
+  } else if (NC == 2) {
     const float2 t = act ? reinterpret_cast<const float2 *>(A.u)[g] : make_float2(0.f, 0.f);
     uu[0] = t.x; uu[NC - 1] = t.y;
     if (!LOCAL) {
@@ -141,7 +155,23 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   }
   // stress (P-SV: isotropic Hooke with lambda+2mu = c0; SH: sigma = mu grad u_y)
   float Sx[NC], Sz[NC];
-  if (EK == 2) {
+  float csxz = 0.f, cszx = 0.f;   // Cosserat sigma_xz, sigma_zx
+  if (EK == 3) {
+    const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+    const float du10 = xix * dxi[1] + gax * dga[1], du11 = xiz * dxi[1] + gaz * dga[1];
+    const float du20 = xix * dxi[NC - 1] + gax * dga[NC - 1], du21 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+    const float nu = __ldg(A.prop2 + p), mcn = __ldg(A.prop3 + p);
+    const float lam = c0, dv = du00 + du11;        // c0 = lambda here
+    const float sxx = lam * dv + 2.f * mu * du00;
+    const float szz = lam * dv + 2.f * mu * du11;
+    float sxz = mu * (du10 + du01) + nu * (du10 - du01);
+    float szx = mu * (du01 + du10) + nu * (du01 - du10);
+    szx -= 2.f * nu * uu[NC - 1];
+    sxz += 2.f * nu * uu[NC - 1];
+    csxz = sxz; cszx = szx;
+    Sx[0] = sxx; Sz[0] = szx; Sx[1] = sxz; Sz[1] = szz;
+    Sx[NC - 1] = mcn * du20; Sz[NC - 1] = mcn * du21;
+  } else if (EK == 2) {
     const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
     const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
     const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
@@ -185,12 +215,22 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     }
     a[c] = -(sw[iz] * t1 + sw[ix] * t2);
   }
+  if (EK == 3) a[NC - 1] -= (csxz - cszx) * (sw[ix] * sw[iz] * jac);   // couple stress
   if (bs >= 0) {
     const size_t k = size_t(bs) * NP + q;
     const float wq = A.bc_w[k];
     if (wq != 0.f) {
       const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
-      if (EK != 1) {
+      if (EK == 3) {
+        const float vx = A.v[size_t(g) * 3], vz = A.v[size_t(g) * 3 + 1], vr = A.v[size_t(g) * 3 + 2];
+        const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+        const float vn = vx * nx + vz * nz;
+        const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vx * rvs;
+        const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vz * rvs;
+        a[0] += -1.f * fx * j1 * wq;
+        a[1] += -1.f * fz * j1 * wq;
+        a[NC - 1] += -1.f * A.bc_imp2[k] * vr * j1 * wq;
+      } else if (EK != 1) {
         const float2 vv = reinterpret_cast<const float2 *>(A.v)[g];
         const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
         const float vn = vv.x * nx + vv.y * nz;
@@ -208,13 +248,19 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     for (int s = src; s >= 0; s = S.src_next[s]) {
       const float f = step < S.nstep ? S.stf[size_t(step) * S.nsrc + s] : 0.f;
 #pragma unroll
-      for (int c = 0; c < NC; ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
+      for (int c = 0; c < (NC < 2 ? NC : 2); ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
     }
   }
   if (LOCAL) {
     const int sl = __ldg(A.slot + p);
-    if (NC == 2) reinterpret_cast<float2 *>(A.r)[sl] = make_float2(a[0], a[NC - 1]);
+    if (NC == 3) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) A.r[size_t(sl) * 3 + c] = a[c];
+    } else if (NC == 2) reinterpret_cast<float2 *>(A.r)[sl] = make_float2(a[0], a[NC - 1]);
     else A.r[sl] = a[0];
+  } else if (NC == 3) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) A.accum[size_t(g) * 3 + c] = acc[c] + a[c];
   } else if (NC == 2) {
     reinterpret_cast<float2 *>(A.accum)[g] = make_float2(acc[0] + a[0], acc[NC - 1] + a[NC - 1]);
   } else {
@@ -285,7 +331,7 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
 // colour, the following ac.nblocks blocks acoustic ones.
 template <int E, int EK, bool LOCAL>
 __global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
-  __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * 6];
+  __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * (EK == 3 ? 9 : 6)];
   __shared__ float shp[NP], shpw[NP], sw[NG];
   load_quad(S.quad, shp, shpw, sw, threadIdx.x);
   if (int(blockIdx.x) < S.el.nblocks)
@@ -627,7 +673,8 @@ __device__ __forceinline__ bool update_gather_point(const UpdateArgs &A, int g) 
       acc[0] = acc[0] + t.x;
       acc[NC - 1] = acc[NC - 1] + t.y;
     } else {
-      acc[0] = acc[0] + A.r[k];
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] = acc[c] + A.r[size_t(k) * NC + c];
     }
   }
   if (g < A.niface) {
@@ -641,7 +688,11 @@ __device__ __forceinline__ bool update_gather_point(const UpdateArgs &A, int g) 
     const float2 m2 = reinterpret_cast<const float2 *>(A.minv)[g];
     uu[0] = u2.x; uu[NC - 1] = u2.y; vv[0] = v2.x; vv[NC - 1] = v2.y; mi[0] = m2.x; mi[NC - 1] = m2.y;
   } else {
-    uu[0] = A.u[g]; vv[0] = A.v[g]; mi[0] = A.minv[g];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const size_t i = size_t(g) * NC + c;
+      uu[c] = A.u[i]; vv[c] = A.v[i]; mi[c] = A.minv[i];
+    }
   }
   float a[NC];
 #pragma unroll
@@ -666,9 +717,13 @@ __device__ __forceinline__ bool update_gather_point(const UpdateArgs &A, int g) 
     reinterpret_cast<float2 *>(A.v)[g] = make_float2(vv[0], vv[NC - 1]);
     if (A.a_store) reinterpret_cast<float2 *>(A.a_store)[g] = make_float2(a[0], a[NC - 1]);
   } else {
-    if (A.predict) A.u[g] = uu[0];
-    A.v[g] = vv[0];
-    if (A.a_store) A.a_store[g] = a[0];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const size_t i = size_t(g) * NC + c;
+      if (A.predict) A.u[i] = uu[c];
+      A.v[i] = vv[c];
+      if (A.a_store) A.a_store[i] = a[c];
+    }
   }
   return bad;
 }
@@ -734,7 +789,7 @@ struct RecArgs {
   UpdateArgs cpl;                      // coupling data of the medium (niface, cp_*, other)
   int ncomp, acoustic;
   int ntypes;
-  int types[4];
+  int types[8];
   int nsb, nsig, nrec_total;
   float dt2;
   const int *__restrict__ step;
@@ -780,34 +835,47 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
   const int g = A.ibool[p];
   const float h = on ? A.rec_h[size_t(r) * NP + q] : 0.f;
   if (!A.acoustic) {
+    const int nc = A.ncomp;
     for (int t = 0; t < A.ntypes; ++t) {
       float o[2] = {0.f, 0.f};
-      if (A.types[t] == 3) {
-        // pressure -(lambda + 2/3 mu) div u from the displacement gradient
-        // (include/medium/dim2/elastic/isotropic/wavefield.hpp:57-89)
+      const int ty = A.types[t];
+      if (ty == 3 || ty == 5 || ty == 6) {
+        // from the displacement gradient at the element point: pressure
+        // -(lambda + 2/3 mu) div u (include/medium/dim2/elastic/isotropic/
+        // wavefield.hpp:57-89; Cosserat: prop0 = lambda); Cosserat curl
+        // du_x/dz - du_z/dx and intrinsic rotation phi - curl / 2
+        // (isotropic_cosserat/wavefield.hpp)
         float pr = 0.f;
-        if (A.ncomp == 2) {
+        if (nc >= 2) {
           const int iz = q / NG, ix = q - iz * NG;
           float dxi0 = 0.f, dxi1 = 0.f, dga0 = 0.f, dga1 = 0.f;
           for (int l = 0; l < NG; ++l) {
             const int gr = A.ibool[size_t(ce) * NP + iz * NG + l];
             const int gc = A.ibool[size_t(ce) * NP + l * NG + ix];
             const float hx = A.quad.hp[ix * NG + l], hz = A.quad.hp[iz * NG + l];
-            dxi0 += hx * A.u[size_t(gr) * 2];
-            dxi1 += hx * A.u[size_t(gr) * 2 + 1];
-            dga0 += hz * A.u[size_t(gc) * 2];
-            dga1 += hz * A.u[size_t(gc) * 2 + 1];
+            dxi0 += hx * A.u[size_t(gr) * nc];
+            dxi1 += hx * A.u[size_t(gr) * nc + 1];
+            dga0 += hz * A.u[size_t(gc) * nc];
+            dga1 += hz * A.u[size_t(gc) * nc + 1];
           }
-          if (on) {
+          if (on && ty == 3) {
             const float dux = A.xix[p] * dxi0 + A.gax[p] * dga0;
             const float duz = A.xiz[p] * dxi1 + A.gaz[p] * dga1;
             const float l2m = A.prop0[p], mu = A.prop1[p];
-            pr = -1.f * ((l2m - 2.f * mu + (2.f / 3.f) * mu) * (dux + duz));
+            pr = nc == 3 ? -1.f * ((l2m + (2.f / 3.f) * mu) * (dux + duz))
+                         : -1.f * ((l2m - 2.f * mu + (2.f / 3.f) * mu) * (dux + duz));
+          } else if (on && nc == 3) {
+            const float duxz = A.xiz[p] * dxi0 + A.gaz[p] * dga0;
+            const float duzx = A.xix[p] * dxi1 + A.gax[p] * dga1;
+            const float curl = duxz - duzx;
+            pr = ty == 6 ? curl : A.u[size_t(g) * 3 + 2] - 0.5f * curl;
           }
         }
         o[0] = warp_sum(h * pr);
+      } else if (ty == 4) {                    // Cosserat rotation
+        o[0] = warp_sum(nc == 3 ? h * A.u[size_t(g) * 3 + 2] : 0.f);
       } else {
-        for (int c = 0; c < A.ncomp; ++c) {
+        for (int c = 0; c < (nc < 2 ? nc : 2); ++c) {
           const size_t k = size_t(g) * A.ncomp + c;
           float val = 0.f;
           switch (A.types[t]) {

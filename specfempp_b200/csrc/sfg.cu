@@ -75,11 +75,11 @@ struct DevMedium {
   int *ibool = nullptr;
   float *xix = nullptr, *xiz = nullptr, *gax = nullptr, *gaz = nullptr, *jac = nullptr,
         *prop0 = nullptr, *prop1 = nullptr;
-  float *prop2 = nullptr, *prop3 = nullptr, *prop4 = nullptr, *prop5 = nullptr;  // anisotropic
+  float *prop2 = nullptr, *prop3 = nullptr, *prop4 = nullptr, *prop5 = nullptr;  // anisotropic / Cosserat
   bool aniso = false;
   int *bc_slot = nullptr;
   float *bc_w = nullptr, *bc_nx = nullptr, *bc_nz = nullptr, *bc_j1 = nullptr,
-        *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr;
+        *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr, *bc_imp2 = nullptr;
   int niface = 0;
   float *cp_nx = nullptr, *cp_nz = nullptr;
   int *cp_other = nullptr;
@@ -265,10 +265,16 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
     D.prop2 = padded(M.prop2); D.prop3 = padded(M.prop3);
     D.prop4 = padded(M.prop4); D.prop5 = padded(M.prop5);
   }
+  if (M.cosserat) {            // nu and mu_c + nu_c
+    if (M.prop2.size() != M.prop0.size() || M.prop3.size() != M.prop0.size())
+      throw std::runtime_error("Cosserat medium without its nu / mu_c + nu_c words");
+    D.prop2 = padded(M.prop2); D.prop3 = padded(M.prop3);
+  }
   D.bc_slot = m.upload(M.bc_slot);
   D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
   D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
   D.bc_keep = m.upload(M.bc_keep);
+  D.bc_imp2 = m.upload(M.bc_imp2);
   D.niface = M.niface;
   D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
   D.minv = m.upload(M.minv);
@@ -296,6 +302,7 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
   A.prop2 = D.prop2; A.prop3 = D.prop3; A.prop4 = D.prop4; A.prop5 = D.prop5;
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
+  A.bc_imp2 = D.bc_imp2;
   A.src_head = D.src_head;
   A.u = D.u; A.v = D.v; A.accum = D.accum; A.r = D.r; A.slot = D.slot;
   return A;
@@ -306,8 +313,11 @@ int ncolors(const DevMedium &D) { return D.nspec ? int(D.color_start.size()) - 1
 template <int E, int EK>
 void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
                         cudaStream_t s, int variant) {
-  // the anisotropic stress exists in the colour-pass and owner-computes kernels
-  if (EK == 2 && (variant == 2 || variant == 4)) variant = variant == 2 ? 1 : 3;
+  // the anisotropic and Cosserat stresses exist in the colour-pass and
+  // owner-computes kernels
+  if (EK >= 2 && (variant == 2 || variant == 4)) variant = variant == 2 ? 1 : 3;
+  if ((EK == 2 || EK == 3) && (!el.prop2 || !el.prop3))
+    throw std::runtime_error("element kernel: material words of the medium missing on the device");
   sfg::dev::StiffArgs S{};
   S.el = med_args(el);
   S.ac = med_args(ac);
@@ -393,6 +403,7 @@ void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
                         cudaStream_t s, int variant) {
   if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s, variant);
   else if (el.aniso) launch_stiffness_E<E, 2>(h, el, ac, step, s, variant);
+  else if (el.ncomp == 3) launch_stiffness_E<E, 3>(h, el, ac, step, s, variant);
   else launch_stiffness_E<E, 0>(h, el, ac, step, s, variant);
 }
 
@@ -511,7 +522,7 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.ncomp = D.ncomp;
   R.acoustic = medium == SFG_MEDIUM_ACOUSTIC;
   R.ntypes = h->asmb.ntypes;
-  for (int t = 0; t < R.ntypes && t < 4; ++t) R.types[t] = h->asmb.types[t];
+  for (int t = 0; t < R.ntypes && t < 8; ++t) R.types[t] = h->asmb.types[t];
   R.nsb = h->asmb.nsb;
   R.nsig = h->asmb.nsig;
   R.nrec_total = h->asmb.nrec;
@@ -532,6 +543,7 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
       sfg::dev::k_update_batched4_gather<<<grid_for(U.n / 4), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.ncomp == 2) sfg::dev::k_update_gather<2><<<grid_for(U.n / 2), 256, 0, s>>>(U);
+    else if (D.ncomp == 3) sfg::dev::k_update_gather<3><<<grid_for(U.n / 3), 256, 0, s>>>(U);
     else sfg::dev::k_update_gather<1><<<grid_for(U.n), 256, 0, s>>>(U);
     return;
   }
@@ -577,7 +589,11 @@ void launch_predict(sfg_handle *h, cudaStream_t s) {
 bool receivers_early(const sfg_handle *h, int medium) {
   for (int t = 0; t < h->asmb.ntypes; ++t) {
     const int k = h->asmb.types[t];
-    if (!(k == SFG_SEIS_DISPLACEMENT || (k == SFG_SEIS_PRESSURE && medium == SFG_MEDIUM_ELASTIC))) return false;
+    // types that read the displacement only (Cosserat rotation, intrinsic
+    // rotation and curl too) may run before the update
+    const bool disp = k == SFG_SEIS_DISPLACEMENT || k == SFG_SEIS_ROTATION ||
+                      k == SFG_SEIS_INTRINSIC_ROTATION || k == SFG_SEIS_CURL;
+    if (!(disp || (k == SFG_SEIS_PRESSURE && medium == SFG_MEDIUM_ELASTIC))) return false;
   }
   return true;
 }
@@ -691,8 +707,9 @@ void autotune(sfg_handle *h) {
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
-  if (h->el.aniso && h->variant == 2) h->variant = 1;
-  if (h->el.aniso && h->variant == 4) h->variant = 3;
+  const bool special = h->el.aniso || h->el.ncomp == 3;   // anisotropic or Cosserat
+  if (special && h->variant == 2) h->variant = 1;
+  if (special && h->variant == 4) h->variant = 3;
   std::vector<std::pair<int, int>> cand;
   if (h->asmb.nshots > 1) {
     for (int v : {1, 3})
@@ -700,7 +717,7 @@ void autotune(sfg_handle *h) {
   } else {
     for (int v : {1, 2, 3, 4}) {
       // an anisotropic medium has the colour-pass and owner-computes kernels only
-      if (h->el.aniso && (v == 2 || v == 4)) continue;
+      if (special && (v == 2 || v == 4)) continue;
       for (int e : {8, 16, 32})
         if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
     }
@@ -767,7 +784,8 @@ void finish_create(sfg_handle *h) {
   h->asmb.nstep = h->opt.nstep;
   h->asmb.nsb = h->opt.nstep_between_samples;
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
-  if (h->asmb.nshots > 1 && (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0 || h->asmb.el.aniso))
+  if (h->asmb.nshots > 1 &&
+      (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0 || h->asmb.el.aniso || h->asmb.el.ncomp == 3))
     throw std::runtime_error("batched shots (nshots > 1) need a single isotropic elastic medium");
 }
 
@@ -841,6 +859,7 @@ int sfg_create2d(const sfg_mesh2d_desc *d, const sfg_options *opt, sfg_handle **
     m.mat_vp.assign(d->mat_vp, d->mat_vp + d->numat);
     m.mat_vs.assign(d->mat_vs, d->mat_vs + d->numat);
     if (d->mat_aniso) m.mat_aniso.assign(d->mat_aniso, d->mat_aniso + 6 * size_t(d->numat));
+    if (d->mat_cosserat) m.mat_cosserat.assign(d->mat_cosserat, d->mat_cosserat + 8 * size_t(d->numat));
     const size_t np = size_t(d->nspec) * sfg::NPTS;
     if (d->point_rho) m.prho.assign(d->point_rho, d->point_rho + np);
     if (d->point_vp) m.pvp.assign(d->point_vp, d->point_vp + np);
@@ -958,12 +977,12 @@ int sfg_set_receivers(sfg_handle *h, int nrec, const double *x, const double *z,
                       int ntypes, const int *types) {
   return guarded(h, [&]() {
     if (h->initialized) { h->err = "receivers must be set before sfg_initialize"; return int(SFG_ERR_STATE); }
-    if (nrec < 0 || (nrec > 0 && (!x || !z)) || ntypes < 1 || ntypes > 4 || !types) {
+    if (nrec < 0 || (nrec > 0 && (!x || !z)) || ntypes < 1 || ntypes > 7 || !types) {
       h->err = "bad receiver arguments";
       return int(SFG_ERR_ARG);
     }
     for (int t = 0; t < ntypes; ++t)
-      if (types[t] < 0 || types[t] > 3) { h->err = "unknown seismogram type"; return int(SFG_ERR_ARG); }
+      if (types[t] < 0 || types[t] > 6) { h->err = "unknown seismogram type"; return int(SFG_ERR_ARG); }
     h->rec_x.assign(x, x + nrec);
     h->rec_z.assign(z, z + nrec);
     try {
@@ -989,6 +1008,11 @@ int sfg_initialize(sfg_handle *h) {
           h->err = "pressure seismograms are defined for isotropic media only";
           return int(SFG_ERR_UNSUPPORTED);
         }
+    for (int t : a.types)
+      if (t >= SFG_SEIS_ROTATION && !a.el.cosserat) {
+        h->err = "rotation, intrinsic rotation and curl seismograms need a Cosserat medium";
+        return int(SFG_ERR_UNSUPPORTED);
+      }
     a.nsig = (a.nstep + a.nsb - 1) / a.nsb;
     SFG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     SFG_CUDA(cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking));
@@ -1241,6 +1265,7 @@ int sfg_get_info(const sfg_handle *h, sfg_info *info) {
   info->kernels_per_step = h->initialized ? kernels_per_step(h) : 0;
   info->elements_per_block = h->epb;
   info->kernel_variant = h->variant;
+  info->ncomp_elastic = a.el.ncomp;
   return SFG_OK;
 }
 
@@ -1414,7 +1439,7 @@ int adjoint_checks(sfg_handle *h) {
   const sfg::Assembly2D &a = h->asmb;
   const bool one = (h->el.nspec > 0) != (h->ac.nspec > 0);
   const int want = h->el.nspec ? SFG_SEIS_DISPLACEMENT : SFG_SEIS_PRESSURE;
-  if (!one || h->el.aniso || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
+  if (!one || h->el.aniso || h->el.ncomp == 3 || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
     h->err = "the adjoint needs one medium (isotropic elastic P-SV or SH with displacement seismograms, "
              "or acoustic with pressure seismograms), one shot, seismograms sampled every step";
     return SFG_ERR_UNSUPPORTED;

@@ -25,7 +25,8 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-EXT = {"displacement": "semd", "velocity": "semv", "acceleration": "sema", "pressure": "semp"}
+EXT = {"displacement": "semd", "velocity": "semv", "acceleration": "sema", "pressure": "semp",
+       "rotation": "semr", "intrinsic_rotation": "semir", "curl": "semc"}
 
 
 @dataclass
@@ -167,6 +168,8 @@ def time_function(fs):
 
 
 def channels(kind: str, elastic_wave: str):
+    if kind in ("rotation", "intrinsic_rotation", "curl"):
+        return ["BXY"]                       # Cosserat scalar traces
     if kind == "pressure":
         if elastic_wave == "sh":
             raise ValueError("pressure seismograms are not defined for SH waves")

@@ -53,6 +53,9 @@ class Mesh:
     # optional [numat][6] anisotropic constants (c11, c13, c15, c33, c35, c55);
     # NaN rows are isotropic materials
     mat_aniso: np.ndarray | None = None
+    # optional [numat][8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
+    # mu_c, nu_c); NaN rows are other materials
+    mat_cosserat: np.ndarray | None = None
 
 
 def structured_mesh(nx, nz, xmin, xmax, zmin, zmax, row_material, materials,

@@ -18,7 +18,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsfg.so")
 
 SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC = 0, 1
-SEIS = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3}
+SEIS = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3, "rotation": 4,
+        "intrinsic_rotation": 5, "curl": 6}
 STF = {"ricker": 0, "dirac": 1, "gaussian": 2, "gaussian_hdur": 3, "dgaussian": 4, "heaviside": 5}
 FIELD = {"displacement": 0, "velocity": 1, "acceleration": 2}
 ERRORS = {0: "OK", -1: "SFG_ERR_ARG", -2: "SFG_ERR_IO", -3: "SFG_ERR_CUDA", -4: "SFG_ERR_LOCATE",
@@ -38,7 +39,7 @@ class MeshDesc(C.Structure):
         ("nabs", C.c_int), ("abs_ispec", _ip), ("abs_type", _ip),
         ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
         ("elastic_wave", C.c_int),
-        ("mat_aniso", _dp),
+        ("mat_aniso", _dp), ("mat_cosserat", _dp),
     ]
 
 
@@ -63,7 +64,7 @@ class Info(C.Structure):
                 ("nshots", C.c_int), ("nsig", C.c_int), ("nrec", C.c_int), ("ntypes", C.c_int),
                 ("nstep", C.c_int), ("istep", C.c_int), ("t0", C.c_double),
                 ("device_bytes", C.c_size_t), ("kernels_per_step", C.c_int),
-                ("elements_per_block", C.c_int), ("kernel_variant", C.c_int)]
+                ("elements_per_block", C.c_int), ("kernel_variant", C.c_int), ("ncomp_elastic", C.c_int)]
 
 
 EXPORTS = {
@@ -176,7 +177,7 @@ class Simulation2D:
             raise SfgError(rc, self.lib.sfg_last_error(None).decode())
         self.h = h
         self.dt, self.nstep = dt, nstep
-        self.ncomp = 1 if wave == 1 else 2
+        self.ncomp = int(self.info().ncomp_elastic) or (1 if wave == 1 else 2)
 
     def _k(self, a):
         self._keep.append(a)
@@ -203,6 +204,10 @@ class Simulation2D:
         d.free_ispec = self._k(_arr(m.free_ispec, np.int32)).ctypes.data_as(_ip)
         d.free_type = self._k(_arr(m.free_type, np.int32)).ctypes.data_as(_ip)
         d.elastic_wave = wave
+        cos = getattr(m, "mat_cosserat", None)
+        if cos is not None:
+            cos = _arr(cos, np.float64).reshape(len(m.mat_rho), 8)
+            d.mat_cosserat = self._k(np.ascontiguousarray(cos)).ctypes.data_as(_dp)
         aniso = getattr(m, "mat_aniso", None)
         if aniso is not None:
             aniso = _arr(aniso, np.float64).reshape(len(m.mat_rho), 6)

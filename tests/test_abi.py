@@ -131,3 +131,13 @@ def test_geometry_export(sfg_lib):
     assert np.allclose(x, gx, rtol=0, atol=1e-6) and np.allclose(z, gz, rtol=0, atol=1e-6)
     assert np.allclose(jac, gj, rtol=1e-12)
     assert np.array_equal(med, np.asarray(w.mesh.mat_medium)[w.mesh.kmato])
+
+
+def test_cosserat_mesh_has_three_components(sfg_lib):
+    """A mesh with Cosserat materials: the elastic medium carries u_x, u_z and
+    the rotation (sfg_info.ncomp_elastic 3)."""
+    from conftest import golden_case
+    from specfempp_b200 import sfg
+    case, _, _ = golden_case("HomogeneousIsotropicCosseratDomain", nstep=10)
+    sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10)
+    assert sim.info().ncomp_elastic == 3 and sim.ncomp == 3

@@ -22,7 +22,8 @@ FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichlet
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
             "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain",
             "HomogeneousAcousticDomain", "HomogeneousAcousticDomainCompositeStaceyDirichletBC",
-            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap"]
+            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap",
+            "HomogeneousIsotropicCosseratDomainNu0"]
 
 
 def tolerance(kind, f32, f64):
@@ -253,3 +254,37 @@ def test_anisotropic_unsupported_forms(sfg_lib):
         sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10, elastic_wave="sh")
     with pytest.raises(sfg.SfgError):
         sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10, nshots=4)
+
+
+COSSERAT = {
+    "HomogeneousIsotropicCosseratDomain": ["displacement", "rotation", "intrinsic_rotation", "curl", "pressure"],
+    "HomogeneousIsotropicCosseratDomainHighFrequency": ["displacement", "velocity", "rotation", "curl"],
+    "cosserat_80x60_stacey": ["displacement", "velocity", "acceleration", "rotation", "intrinsic_rotation",
+                              "curl", "pressure"],
+}
+
+
+@pytest.mark.parametrize("name", list(COSSERAT))
+def test_cosserat_parity(sfg_lib, oracle_lib, name):
+    """Isotropic Cosserat P-SV-T fixtures (displacement + rotation, couple
+    stress): every seismogram type against the oracle, displacement at 1e-5,
+    the others (time derivatives and displacement gradients) at max(1e-5,
+    twice the oracle's own FP32-vs-FP64 difference); colour passes and
+    owner-computes give the same bits."""
+    from oracle import runner
+    if name == "cosserat_80x60_stacey":
+        from test_oracle import cosserat_80x60
+        case = cosserat_80x60(1200)
+    else:
+        case, _, _ = golden_case(name)
+    types = COSSERAT[name]
+    case.seis_types = list(types)
+    ref = runner.run(case, "f32", nthreads=8)["seis"]
+    ref64 = runner.run(case, "f64", nthreads=8)["seis"]
+    sim, seis = product_run(case, types=types, variant=1)
+    assert sim.info().ncomp_elastic == 3
+    for t, kind in enumerate(types):
+        tol = 1e-5 if kind == "displacement" else tolerance(kind, ref[:, t], ref64[:, t])
+        assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
+    _, s3 = product_run(case, types=types, variant=3)
+    assert np.array_equal(s3, seis)

@@ -186,7 +186,8 @@ def cosserat_metric(seis, traces, per_station):
 
 
 @pytest.mark.parametrize("name,checks", [
-    # nu = 0 (traces from SPECFEM): every type at the reference's 1e-3
+    # the "nu = 0" fixture's database holds an isotropic elastic material:
+    # every type of the elastic path at the reference's 1e-3
     ("HomogeneousIsotropicCosseratDomainNu0",
      [("displacement", 1e-3, True), ("velocity", 1e-3, True), ("acceleration", 1e-3, True),
       ("pressure", 1e-3, True)]),
@@ -203,8 +204,8 @@ def cosserat_metric(seis, traces, per_station):
      [("displacement", 1e-1, True), ("intrinsic_rotation", 1e-1, False), ("curl", 1e-1, False)]),
 ])
 def test_oracle_cosserat_golden(oracle_lib, name, checks):
-    """Isotropic Cosserat P-SV-T medium (displacement + rotation, couple
-    stress) against the reference's fixtures."""
+    """The reference's Cosserat fixtures: the isotropic Cosserat P-SV-T medium
+    (displacement + rotation, couple stress) where the database holds one."""
     import os
     from conftest import GOLDEN
     from oracle import runner
@@ -216,3 +217,51 @@ def test_oracle_cosserat_golden(oracle_lib, name, checks):
         key, nc = COSSERAT_TYPES[kind]
         err = cosserat_metric(r["seis"][:, k, :, :nc], z[key], per_station)
         assert err < tol, (kind, err)
+
+
+def cosserat_80x60(nstep, nu_frac=0.1, absorbing=("bottom", "right", "left")):
+    """80 x 60 mesh of one isotropic Cosserat material (rho 2200, vp 2500,
+    vs 1445 for the displacement part; nu = nu_frac mu; j = rho; lambda_c,
+    mu_c, nu_c as fractions of mu like the reference's fixture), Stacey on
+    ``absorbing``; a force source, receivers on a line."""
+    from oracle import runner
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_psv_80x60(nstep=nstep)
+    rho, vp, vs = 2200.0, 2500.0, 1445.0
+    mu = rho * vs * vs
+    kappa = rho * vp * vp - 4.0 / 3.0 * mu
+    mesh = meshgen.structured_mesh(80, 60, 0.0, 4000.0, 0.0, 3000.0, np.zeros(60, np.int32),
+                                   [(1, rho, vp, vs)], absorbing=absorbing, free_surface=())
+    mesh.mat_cosserat = np.array([[rho, kappa, mu, nu_frac * mu, rho, 0.0957 * mu, 0.0185 * mu, 0.037 * mu]])
+    src = [runner.Source(x=2000.0, z=2000.0, f0=10.0, factor=1e10, angle=20.0)]
+    return runner.Case2D(mesh=mesh, sources=src, rec_x=w.rec_x, rec_z=np.full(5, 2600.0), dt=w.dt, nstep=nstep)
+
+
+def test_oracle_cosserat_nu0_is_elastic(oracle_lib):
+    """With nu = 0 the displacement decouples from the rotation: the Cosserat
+    medium's displacement equals the isotropic elastic one (FP32 rounding of
+    lambda aside), and the rotation stays at rest."""
+    from oracle import runner
+    case = cosserat_80x60(1200, nu_frac=0.0)      # long enough for the waves to arrive
+    case.seis_types = ["displacement", "rotation"]
+    a = runner.run(case, "f32", nthreads=8)["seis"]
+    case.mesh.mat_cosserat = None
+    case.seis_types = ["displacement"]
+    b = runner.run(case, "f32", nthreads=8)["seis"]
+    assert np.abs(b).max() > 0
+    assert np.linalg.norm(a[:, 0] - b[:, 0]) / np.linalg.norm(b[:, 0]) < 1e-5
+    assert not np.any(a[:, 1])
+
+
+def test_oracle_cosserat_nu_couples_rotation(oracle_lib):
+    """With nu > 0 the force source excites the rotation, which is bounded
+    (the explicit step is stable) and changes the displacement."""
+    from oracle import runner
+    case = cosserat_80x60(500)
+    case.seis_types = ["displacement", "rotation", "curl"]
+    a = runner.run(case, "f32", nthreads=8)["seis"]
+    assert np.all(np.isfinite(a)) and np.abs(a[:, 1]).max() > 0
+    b_case = cosserat_80x60(500, nu_frac=0.0)
+    b_case.seis_types = ["displacement"]
+    b = runner.run(b_case, "f32", nthreads=8)["seis"]
+    assert np.linalg.norm(a[:, 0] - b[:, 0]) / np.linalg.norm(b[:, 0]) > 1e-3
