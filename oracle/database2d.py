@@ -203,7 +203,13 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
     if i < len(recs):
         (nadj,) = struct.unpack("<i", take())
         extra["n_adjacency"] = nadj
-        i += nadj
+        adj = np.zeros((nadj, 4), np.int32)
+        for k in range(nadj):
+            e, nb, conn, orient = struct.unpack("<4i", take())
+            if conn not in (1, 3):
+                raise ValueError("Unknown connection type in adjacency graph.")
+            adj[k] = (e - 1, nb - 1, conn, orient - 1)
+        extra["adjacency"] = adj
     if i != len(recs):
         raise ValueError("The Database file wasn't fully read")
 

@@ -39,6 +39,11 @@
 //   coupling                    include/kokkos_kernels/impl/compute_coupling.tpp:21-115,
 //                               include/medium/dim2/coupling_terms/{acoustic_elastic,elastic_acoustic}.hpp,
 //                               core/specfem/assembly/conforming_interfaces/dim2/impl/interface_container.tpp
+//   nonconforming coupling      include/kokkos_kernels/impl/compute_coupling.tpp:117-249,
+//                               include/algorithms/{transfer.hpp,integrate/coupling_integral1d.hpp},
+//                               core/specfem/assembly/nonconforming_interfaces/dim2/impl/*,
+//                               core/specfem/assembly/edge_types/dim2/edge_types.cpp,
+//                               src/algorithms/dim2/locate_point_impl.cpp:126-198
 //   Newmark                     core/specfem/timescheme/newmark.tpp:10-128
 //   step order                  core/specfem/solver/time_marching.tpp:33-83
 //   seismograms                 include/kokkos_kernels/impl/compute_seismogram.tpp,
@@ -197,6 +202,43 @@ bool on_edge(int type, int iz, int ix) {
          (type == LEFT && ix == 0) || (type == RIGHT && ix == NG - 1);
 }
 
+// (xi, gamma) of the point at local coordinate c along an edge: xi runs along
+// bottom and top, gamma along left and right.
+template <typename S>
+void edge_local(int type, S c, S &xi, S &ga) {
+  if (type == BOTTOM) { xi = c; ga = S(-1); }
+  else if (type == RIGHT) { xi = S(1); ga = c; }
+  else if (type == TOP) { xi = c; ga = S(1); }
+  else { xi = S(-1); ga = c; }
+}
+
+// Local coordinate along one edge of an element of the point closest to
+// (X, Z): Newton steps on the edge coordinate from 0 with the inverse
+// Jacobian row of that coordinate, clamped to [-1, 1], stopping at an end
+// whose step points outside (src/algorithms/dim2/locate_point_impl.cpp:126-198).
+template <typename S>
+S edge_coordinate(S X, S Z, const S *cx, const S *cz, int ngnod, int type) {
+  const S deriv_eps = S(1e-12);
+  S xi, ga;
+  edge_local<S>(type, S(0), xi, ga);
+  S &c = (type == BOTTOM || type == TOP) ? xi : ga;
+  for (int it = 0; it < 100; ++it) {
+    S x, z;
+    location_at<S>(cx, cz, ngnod, xi, ga, x, z);
+    const Jac<S> J = jacobian_at<S>(cx, cz, ngnod, xi, ga);
+    const S dx = -(x - X), dz = -(z - Z);
+    const S d = (type == BOTTOM || type == TOP) ? J.xix * dx + J.xiz * dz
+                                                : J.gammax * dx + J.gammaz * dz;
+    if (c == S(-1) && d < -deriv_eps) return S(-1);
+    if (c == S(1) && d > deriv_eps) return S(1);
+    c += d;
+    if (c > S(1)) c = S(1);
+    else if (c < S(-1)) c = S(-1);
+    if (std::abs(d) < deriv_eps) break;
+  }
+  return c;
+}
+
 template <typename T>
 struct Sim {
   const OracleInput2D &in;
@@ -223,6 +265,18 @@ struct Sim {
   // coupling point lists
   struct CPoint { int ispec, iz, ix, iglob; T nx, nz, fac; };
   std::vector<CPoint> cpl_ac, cpl_el;   // self acoustic / self elastic
+  // nonconforming acoustic-elastic edge pairs: the self edge's points, the
+  // coupled edge's points, and on the NG-point intersection quadrature the
+  // self / coupled transfer functions, weight * |dx/dxi| and the self
+  // element's outward unit normal
+  struct NCEdge {
+    int self_e, self_t, cpl_e, cpl_t;
+    int gs[NG], gc[NG];
+    uint8_t fs[NG];
+    T ts[NG][NG], tc[NG][NG];   // [quadrature point][edge point]
+    T fac[NG], nx[NG], nz[NG];
+  };
+  std::vector<NCEdge> nc_ac, nc_el;     // self acoustic / self elastic
   // sources
   struct Src { int ispec; int medium; T arr[3][NP]; int ncomp; std::vector<T> stf; };
   std::vector<Src> srcs;
@@ -247,6 +301,7 @@ struct Sim {
     properties();
     boundaries();
     coupling();
+    nonconforming();
     mass();
     sources();
     receivers();
@@ -462,6 +517,112 @@ struct Sim {
           }
       }
     }
+  }
+
+  // Nonconforming acoustic-elastic edges from the mesh adjacency records
+  // (core/specfem/assembly/edge_types/dim2/edge_types.cpp: a nonconforming
+  // record between different media and its reverse record give the self and
+  // coupled edges).  Per pair, the intersection of the two edges in the self
+  // edge's local coordinate carries an NG-point GLL quadrature mapped
+  // linearly onto it; its points are located on the coupled edge, and the
+  // Lagrange interpolants there are the transfer functions
+  // (nonconforming_interfaces/dim2/impl/compute_intersection.cpp:49-167,
+  // compute_intersection.tpp:13-122).  The quadrature factor w_q |dx/dxi|
+  // and the self element's outward normal come from the derivative of the
+  // mapped quadrature points (impl/interface_container.tpp:20-180).
+  template <typename S>
+  void nonconforming_in() {
+    if (!in.adjacency || in.nadj <= 0) return;
+    std::map<std::pair<int, int>, int> orient;
+    for (int r = 0; r < in.nadj; ++r) {
+      const int *a = in.adjacency + 4 * size_t(r);
+      if (a[2] == 3) orient[{a[0], a[1]}] = a[3];
+      else if (a[2] != 1) throw std::runtime_error("Unknown connection type in adjacency graph.");
+    }
+    S zs[NG], ws[NG], hps[NG][NG];
+    {
+      double zd[NG], wd[NG], hpd[NG][NG];
+      gll_nodes(zd, wd);
+      gll_hprime(zd, hpd);
+      for (int i = 0; i < NG; ++i) {
+        zs[i] = S(zd[i]); ws[i] = S(wd[i]);
+        for (int j = 0; j < NG; ++j) hps[i][j] = S(hpd[i][j]);
+      }
+    }
+    auto ends = [](int t, int &a, int &b) {
+      if (t == BOTTOM) { a = 0; b = 1; } else if (t == RIGHT) { a = 1; b = 2; }
+      else if (t == TOP) { a = 3; b = 2; } else { a = 0; b = 3; }
+    };
+    auto edge_point = [](int t, int k) {
+      return t == BOTTOM ? k : t == RIGHT ? k * NG + NG - 1 : t == TOP ? (NG - 1) * NG + k : k * NG;
+    };
+    for (const auto &kv : orient) {
+      const int e1 = kv.first.first, e2 = kv.first.second, t1 = kv.second;
+      if (medium[e1] == medium[e2]) continue;
+      const auto back = orient.find({e2, e1});
+      if (back == orient.end())
+        throw std::runtime_error("Non-symmetric adjacency graph detected in `compute_intersection`.");
+      const int t2 = back->second;
+      if (t1 > LEFT || t2 > LEFT) throw std::runtime_error("compute_intersection must be given edges");
+      if (ncomp_el != 2)
+        throw std::runtime_error("nonconforming coupling: P-SV elastic media only");
+      NCEdge E;
+      E.self_e = e1; E.self_t = t1; E.cpl_e = e2; E.cpl_t = t2;
+      S c1x[9], c1z[9], c2x[9], c2z[9];
+      ctrl<S>(e1, c1x, c1z);
+      ctrl<S>(e2, c2x, c2z);
+      int a1, b1, a2, b2;
+      ends(t1, a1, b1);
+      ends(t2, a2, b2);
+      const S p2lo = edge_coordinate<S>(c2x[a2], c2z[a2], c1x, c1z, ngnod, t1);
+      const S p2hi = edge_coordinate<S>(c2x[b2], c2z[b2], c1x, c1z, ngnod, t1);
+      const S p1lo = edge_coordinate<S>(c1x[a1], c1z[a1], c2x, c2z, ngnod, t2);
+      const S p1hi = edge_coordinate<S>(c1x[b1], c1z[b1], c2x, c2z, ngnod, t2);
+      const S min1 = std::min(p2lo, p2hi), max1 = std::max(p2lo, p2hi);
+      const S min2 = std::min(p1lo, p1hi), max2 = std::max(p1lo, p1hi);
+      if (min1 > max1 - S(1e-5) || min2 > max2 - S(1e-5))
+        throw std::runtime_error("nonconforming edges without an intersection");
+      S ts[NG][NG], tc[NG][NG], hdum[NG];
+      for (int q = 0; q < NG; ++q) {
+        const S c1 = S(0.5) * ((max1 - min1) * zs[q] + (max1 + min1));
+        S xi, ga, X, Z;
+        edge_local<S>(t1, c1, xi, ga);
+        location_at<S>(c1x, c1z, ngnod, xi, ga, X, Z);
+        const S c2 = edge_coordinate<S>(X, Z, c2x, c2z, ngnod, t2);
+        lagrange_interp<S>(c1, zs, ts[q], hdum);
+        lagrange_interp<S>(c2, zs, tc[q], hdum);
+      }
+      S lx[NG], lz[NG];
+      for (int k = 0; k < NG; ++k) {
+        S lc = 0;
+        for (int i = 0; i < NG; ++i) lc += ts[k][i] * zs[i];
+        S xi, ga;
+        edge_local<S>(t1, lc, xi, ga);
+        location_at<S>(c1x, c1z, ngnod, xi, ga, lx[k], lz[k]);
+      }
+      for (int q = 0; q < NG; ++q) {
+        S drx = 0, drz = 0;
+        for (int k = 0; k < NG; ++k) { drx += hps[q][k] * lx[k]; drz += hps[q][k] * lz[k]; }
+        const S fac = ws[q] * std::sqrt(drx * drx + drz * drz);
+        S nx = drz, nz = -drx;
+        S mag = std::sqrt(nx * nx + nz * nz);
+        if (t1 == TOP || t1 == LEFT) mag *= S(-1);
+        E.fac[q] = T(fac); E.nx[q] = T(nx / mag); E.nz[q] = T(nz / mag);
+        for (int i = 0; i < NG; ++i) { E.ts[q][i] = T(ts[q][i]); E.tc[q][i] = T(tc[q][i]); }
+      }
+      for (int k = 0; k < NG; ++k) {
+        const size_t ps = size_t(e1) * NP + edge_point(t1, k);
+        E.gs[k] = ibool[ps];
+        E.fs[k] = fs_tag[ps];
+        E.gc[k] = ibool[size_t(e2) * NP + edge_point(t2, k)];
+      }
+      (medium[e1] == MED_ACOUSTIC ? nc_ac : nc_el).push_back(E);
+    }
+  }
+
+  void nonconforming() {
+    if (in.setup_in_run_precision) nonconforming_in<T>();
+    else nonconforming_in<double>();
   }
 
   // Stacey traction (stacey.tpp:50-80 P-SV, :130-146 SH, :296-326 acoustic)
@@ -815,6 +976,48 @@ struct Sim {
       for (const auto &c : cpl_el) {
         a[size_t(c.iglob) * 2 + 0] += c.fac * c.nx * aa[c.iglob];
         a[size_t(c.iglob) * 2 + 1] += c.fac * c.nz * aa[c.iglob];
+      }
+    }
+    // nonconforming coupling (compute_coupling.tpp:117-249): the coupled
+    // field interpolated to the intersection quadrature (algorithms/transfer.hpp),
+    // times the self normal (coupling_terms/*.hpp), integrated against the
+    // self edge's transfer functions (integrate/coupling_integral1d.hpp)
+    if (med == MED_ACOUSTIC) {
+      for (const auto &E : nc_ac) {
+        T f[NG];
+        for (int q = 0; q < NG; ++q) {
+          T u0 = 0, u1 = 0;
+          for (int j = 0; j < NG; ++j) {
+            u0 += ue[size_t(E.gc[j]) * 2 + 0] * E.tc[q][j];
+            u1 += ue[size_t(E.gc[j]) * 2 + 1] * E.tc[q][j];
+          }
+          f[q] = E.nx[q] * u0 + E.nz[q] * u1;
+        }
+        for (int i = 0; i < NG; ++i) {
+          T r = 0;
+          for (int q = 0; q < NG; ++q) r += f[q] * E.fac[q] * E.ts[q][i];
+          if (E.fs[i]) r = 0;
+          a[E.gs[i]] += r;
+        }
+      }
+    } else if (ncomp_el == 2) {
+      for (const auto &E : nc_el) {
+        T f0[NG], f1[NG];
+        for (int q = 0; q < NG; ++q) {
+          T p = 0;
+          for (int j = 0; j < NG; ++j) p += aa[E.gc[j]] * E.tc[q][j];
+          f0[q] = E.nx[q] * p;
+          f1[q] = E.nz[q] * p;
+        }
+        for (int i = 0; i < NG; ++i) {
+          T r0 = 0, r1 = 0;
+          for (int q = 0; q < NG; ++q) {
+            r0 += f0[q] * E.fac[q] * E.ts[q][i];
+            r1 += f1[q] * E.fac[q] * E.ts[q][i];
+          }
+          a[size_t(E.gs[i]) * 2 + 0] += r0;
+          a[size_t(E.gs[i]) * 2 + 1] += r1;
+        }
       }
     }
     // sources (:96-110)

@@ -42,6 +42,13 @@ typedef struct OracleInput2D {
    * kappa, mu, nu, j, lambda_c, mu_c, nu_c): three components (u_x, u_z,
    * rotation); NULL: none */
   const double *cosserat;
+  /* optional mesh adjacency records [nadj][4]: (element, neighbour,
+   * connection 1 strongly conforming / 3 nonconforming, orientation of the
+   * shared entity on the element 0 bottom 1 right 2 top 3 left, 4..7
+   * corners), 0-based.  Nonconforming acoustic-elastic records couple the
+   * two media through an intersection quadrature; NULL or nadj 0: none */
+  int nadj;
+  const int *adjacency;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

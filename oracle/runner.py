@@ -49,6 +49,7 @@ class OracleInput2D(C.Structure):
         ("setup_in_run_precision", C.c_int),
         ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
         ("aniso", _dp), ("cosserat", _dp),
+        ("nadj", C.c_int), ("adjacency", _ip),
     ]
 
 
@@ -182,6 +183,19 @@ def aniso_points(case):
     return np.ascontiguousarray(out)
 
 
+def nonconforming_records(m):
+    """The mesh's nonconforming adjacency records [n][4] (element, neighbour,
+    3, edge type), 0-based; the strongly conforming ones are implied by the
+    shared control nodes."""
+    adj = getattr(m, "adjacency", None)
+    if adj is None:
+        adj = getattr(m, "extra", {}).get("adjacency")
+    if adj is None or len(adj) == 0:
+        return np.zeros((0, 4), np.int32)
+    adj = np.asarray(adj, np.int32).reshape(-1, 4)
+    return np.ascontiguousarray(adj[adj[:, 2] == 3])
+
+
 def cosserat_points(case):
     """[nspec, 25, 8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
     mu_c, nu_c) when the mesh has Cosserat materials, else None; every elastic
@@ -262,6 +276,9 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     inp.aniso = _ptr(arr(aniso, np.float64), _dp) if aniso is not None else None
     cos = cosserat_points(case)
     inp.cosserat = _ptr(arr(cos, np.float64), _dp) if cos is not None else None
+    adj = nonconforming_records(m)
+    inp.nadj = len(adj)
+    inp.adjacency = _ptr(arr(adj, np.int32), _ip) if len(adj) else None
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()
@@ -383,9 +400,19 @@ def load_fixture(fixture_dir, types=("displacement",)):
     ts = cfg["simulation-setup"]["solver"]["time-marching"]["time-scheme"]
     rc = cfg["receivers"]
     mesh = read_database(os.path.join(fixture_dir, "database.bin"))
-    names, rx, rz = read_stations(os.path.join(fixture_dir, "STATIONS"))
-    src_name = os.path.basename(str(cfg.get("sources", "sources.yaml")))   # sources.yaml or source.yaml
-    src = read_sources_yaml(os.path.join(fixture_dir, src_name))
+
+    def local(path, default):
+        # the configuration's paths are relative to the test tree: a file of
+        # this fixture, else of the sibling fixture it names
+        path = str(path or default)
+        own = os.path.join(fixture_dir, os.path.basename(path))
+        if os.path.exists(own):
+            return own
+        return os.path.join(os.path.dirname(os.path.abspath(fixture_dir)),
+                            os.path.basename(os.path.dirname(path)), os.path.basename(path))
+
+    names, rx, rz = read_stations(local(rc.get("stations"), "STATIONS"))
+    src = read_sources_yaml(local(cfg.get("sources"), "sources.yaml"))   # sources.yaml or source.yaml
     sh = str(cfg["simulation-setup"].get("elastic-wave", "P_SV")).upper() == "SH"
     return Case2D(mesh=mesh, sources=src, rec_x=rx, rec_z=rz, dt=float(ts["dt"]),
                   nstep=int(ts["nstep"]), seis_types=list(types),

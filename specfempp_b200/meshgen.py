@@ -56,6 +56,11 @@ class Mesh:
     # optional [numat][8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
     # mu_c, nu_c); NaN rows are other materials
     mat_cosserat: np.ndarray | None = None
+    # optional adjacency records [n][4]: (element, neighbour, connection 1
+    # strongly conforming / 3 nonconforming, orientation of the shared entity
+    # on the element: 0 bottom 1 right 2 top 3 left, 4..7 corners
+    # bottom-left, bottom-right, top-right, top-left), 0-based
+    adjacency: np.ndarray | None = None
 
 
 def structured_mesh(nx, nz, xmin, xmax, zmin, zmax, row_material, materials,
@@ -160,7 +165,10 @@ def write_database(mesh: Mesh, path: str, title: str = "structured mesh") -> Non
     for ac, el in mesh.coupled_pairs:
         rec(struct.pack("<ii", int(ac) + 1, int(el) + 1))
     rec(struct.pack("<ii", 0, 0))
-    rec(struct.pack("<i", 0))
+    adj = np.zeros((0, 4), np.int32) if mesh.adjacency is None else np.asarray(mesh.adjacency)
+    rec(struct.pack("<i", len(adj)))
+    for e, nb, conn, orient in adj:
+        rec(struct.pack("<4i", int(e) + 1, int(nb) + 1, int(conn), int(orient) + 1))
     with open(path, "wb") as f:
         f.write(bytes(out))
 
@@ -233,6 +241,107 @@ def coupled_400x200(nstep: int = 4000, nx: int = 400, nz: int = 200, seed: int =
     return Workload("coupled_400x200", mesh, src, rx, rz, 1e-3, nstep,
                     description=f"2D coupled acoustic-elastic {nx}x{nz}, water 1.5 km, "
                                 f"elastic vp={np.round(vps, 1).tolist()}")
+
+
+def _grid_adjacency(nx, nz, first):
+    """Strongly conforming adjacency records of an nx*nz grid of elements
+    numbered first + iz*nx + ix: edge neighbours and diagonal corner neighbours."""
+    recs = []
+    steps = [(0, -1, BOTTOM), (1, 0, RIGHT), (0, 1, TOP), (-1, 0, LEFT),
+             (-1, -1, 4), (1, -1, 5), (1, 1, 6), (-1, 1, 7)]
+    for iz in range(nz):
+        for ix in range(nx):
+            for dx, dz, o in steps:
+                jx, jz = ix + dx, iz + dz
+                if 0 <= jx < nx and 0 <= jz < nz:
+                    recs.append((first + iz * nx + ix, first + jz * nx + jx, 1, o))
+    return recs
+
+
+def nonconforming_coupled(nx_el: int = 30, nx_ac: int = 45, nz_el: int = 16, nz_ac: int = 12,
+                          width: float = 3000.0, h_el: float = 1600.0, h_ac: float = 1200.0,
+                          nstep: int = 1200, absorbing=("bottom", "right", "left"),
+                          free_surface=("top",)) -> Workload:
+    """An elastic block (nx_el x nz_el quads) under a water block (nx_ac x
+    nz_ac quads) of the same width, with no shared control nodes: the
+    horizontal fluid-solid interface at z = h_el is nonconforming whenever
+    nx_el != nx_ac, and every overlapping pair of interface edges is listed
+    as a nonconforming adjacency record (both directions), the grid
+    neighbours as strongly conforming ones.  Elastic elements come first.
+    Stacey on the sides named in ``absorbing`` (both blocks), an acoustic free
+    surface on the top; Ricker 8 Hz pressure source in the water, 8
+    receivers on both sides of the interface, dt 5e-4."""
+    xs_e, zs_e = np.linspace(0.0, width, nx_el + 1), np.linspace(0.0, h_el, nz_el + 1)
+    xs_a, zs_a = np.linspace(0.0, width, nx_ac + 1), np.linspace(h_el, h_el + h_ac, nz_ac + 1)
+    Xe, Ze = np.meshgrid(xs_e, zs_e)
+    Xa, Za = np.meshgrid(xs_a, zs_a)
+    coorg = np.concatenate([np.stack([Xe.ravel(), Ze.ravel()], 1), np.stack([Xa.ravel(), Za.ravel()], 1)])
+    off = (nx_el + 1) * (nz_el + 1)
+
+    def quads(nx, nz, base):
+        iz, ix = np.divmod(np.arange(nx * nz), nx)
+        n0 = base + iz * (nx + 1) + ix
+        return np.stack([n0, n0 + 1, n0 + nx + 2, n0 + nx + 1], axis=1)
+
+    knods = np.concatenate([quads(nx_el, nz_el, 0), quads(nx_ac, nz_ac, off)]).astype(np.int32)
+    ne = nx_el * nz_el
+    nspec = ne + nx_ac * nz_ac
+    kmato = np.concatenate([np.zeros(ne, np.int32), np.ones(nx_ac * nz_ac, np.int32)])
+    abs_i, abs_t = [], []
+    for nx, nz, base in ((nx_el, nz_el, 0), (nx_ac, nz_ac, ne)):
+        iz, ix = np.divmod(np.arange(nx * nz), nx)
+        top_block = base == ne
+        sides = {"bottom": (iz == 0) & (not top_block), "right": ix == nx - 1,
+                 "top": (iz == nz - 1) & top_block, "left": ix == 0}
+        for name, t in (("bottom", BOTTOM), ("right", RIGHT), ("top", TOP), ("left", LEFT)):
+            if name in absorbing:
+                e = base + np.nonzero(sides[name])[0]
+                abs_i.append(e)
+                abs_t.append(np.full(len(e), t))
+    fr = np.arange(ne + (nz_ac - 1) * nx_ac, nspec) if "top" in free_surface else np.zeros(0, int)
+    adj = _grid_adjacency(nx_el, nz_el, 0) + _grid_adjacency(nx_ac, nz_ac, ne)
+    tol = 1e-9 * width
+    for i in range(nx_el):
+        e = (nz_el - 1) * nx_el + i
+        for j in range(nx_ac):
+            a = ne + j
+            lo, hi = max(xs_e[i], xs_a[j]), min(xs_e[i + 1], xs_a[j + 1])
+            if hi - lo > tol:
+                adj.append((e, a, 3, TOP))
+                adj.append((a, e, 3, BOTTOM))
+    mesh = Mesh(nspec=nspec, npgeo=len(coorg), ngnod=4, coorg=coorg, knods=knods, kmato=kmato,
+                mat_medium=np.array([ELASTIC, ACOUSTIC], np.int32),
+                mat_rho=np.array([2400.0, 1020.0]), mat_vp=np.array([3000.0, 1500.0]),
+                mat_vs=np.array([1700.0, 0.0]),
+                abs_ispec=np.concatenate(abs_i).astype(np.int32) if abs_i else np.zeros(0, np.int32),
+                abs_type=np.concatenate(abs_t).astype(np.int32) if abs_t else np.zeros(0, np.int32),
+                free_ispec=fr.astype(np.int32), free_type=np.full(len(fr), TOP, np.int32),
+                adjacency=np.asarray(adj, np.int32))
+    rx = np.linspace(0.3 * width, 0.6 * width, 8)
+    rz = np.array([h_el - 230.0, h_el - 130.0, h_el - 70.0, h_el - 20.0,
+                   h_el + 20.0, h_el + 70.0, h_el + 130.0, h_el + 230.0])
+    src = [RickerSource(0.43 * width, h_el + 0.45 * h_ac, 8.0, 1e9)]
+    return Workload(f"nonconforming_coupled_{nx_el}_{nx_ac}", mesh, src, rx, rz, 5e-4, nstep,
+                    description=f"2D acoustic-elastic, nonconforming interface {nx_el}:{nx_ac}")
+
+
+def merge_interface_nodes(mesh: Mesh) -> Mesh:
+    """The conforming twin of a nonconforming_coupled mesh whose interface
+    edges coincide (nx_el == nx_ac): the water block's interface nodes are
+    replaced by the elastic block's nodes at the same place, and the
+    adjacency records are dropped, so the interface couples through shared
+    edges."""
+    import copy
+    m = copy.deepcopy(mesh)
+    key = {}
+    for i, (x, z) in enumerate(m.coorg):
+        key.setdefault((round(x, 6), round(z, 6)), i)
+    remap = np.arange(m.npgeo)
+    for i, (x, z) in enumerate(m.coorg):
+        remap[i] = key[(round(x, 6), round(z, 6))]
+    m.knods = remap[m.knods].astype(np.int32)
+    m.adjacency = None
+    return m
 
 
 def gaussian_random_field(shape, spacing, corr_len, rng) -> np.ndarray:

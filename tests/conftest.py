@@ -35,6 +35,8 @@ def golden_case(name, nstep=None):
                   coupled_pairs=np.zeros((0, 2), np.int32),
                   mat_aniso=z["mat_aniso"] if "mat_aniso" in z else None,
                   mat_cosserat=z["mat_cosserat"] if "mat_cosserat" in z else None)
+    if "adjacency" in z:
+        mesh.extra["adjacency"] = z["adjacency"]
     srcs = []
     for s in z["src"]:
         mt = len(s) > 7 and bool(s[7])

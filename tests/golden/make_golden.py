@@ -38,6 +38,7 @@ FIXTURES = {
     "HomogeneousIsotropicCosseratDomainNu0": ("BXX", "BXZ"),
     "HomogeneousIsotropicCosseratDomain": ("BXX", "BXZ"),
     "HomogeneousIsotropicCosseratDomainHighFrequency": ("BXX", "BXZ"),
+    "AcousticElasticNonconformingCoupledDomain": ("BXX", "BXZ"),
 }
 
 # time-function codes stored in the fixtures' source rows
@@ -75,6 +76,9 @@ def make(ref_root: str, name: str, comps) -> str:
         extra["mat_aniso"] = m.mat_aniso
     if getattr(m, "mat_cosserat", None) is not None:
         extra["mat_cosserat"] = m.mat_cosserat
+    nc = runner.nonconforming_records(m)
+    if len(nc):
+        extra["adjacency"] = nc        # nonconforming records only
     out = os.path.join(HERE, f"{name}.npz")
     np.savez_compressed(
         out, nspec=m.nspec, npgeo=m.npgeo, ngnod=m.ngnod, coorg=m.coorg, knods=m.knods,

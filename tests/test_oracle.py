@@ -265,3 +265,62 @@ def test_oracle_cosserat_nu_couples_rotation(oracle_lib):
     b_case.seis_types = ["displacement"]
     b = runner.run(b_case, "f32", nthreads=8)["seis"]
     assert np.linalg.norm(a[:, 0] - b[:, 0]) / np.linalg.norm(b[:, 0]) > 1e-3
+
+
+def test_oracle_nonconforming_golden(oracle_lib):
+    """The reference's nonconforming fluid-solid fixture (a fine water mesh
+    over a coarser elastic one, coupled through 206 nonconforming edge pairs
+    each way) against the traces of the conforming run it shares its
+    stations and source with, the reference's metric and tolerance 1e-2
+    (its config.yaml)."""
+    from oracle import runner
+    case, traces, t0 = golden_case("AcousticElasticNonconformingCoupledDomain")
+    r = runner.run(case, "f32", nthreads=8)
+    assert abs(r["t0"] - t0) < 1e-3
+    err = reference_metric(r["seis"][:, 0], traces)
+    assert np.all(np.isfinite(err))
+    assert err.max() < 1e-2, err                          # the reference's tolerance
+    assert err.max() < 9e-3                               # observed: 7.8e-3 (elastic side)
+    assert np.abs(r["seis"][:, 0, :2]).max() > 0          # elastic receivers reached only by coupling
+
+
+def test_oracle_nonconforming_coincident_edges_equal_conforming(oracle_lib):
+    """Nonconforming records over edges that coincide (equal columns on both
+    sides, separate control nodes): the intersection quadrature reduces to
+    the GLL points, the transfer functions to the identity, so the run equals
+    the conforming twin that shares the interface nodes, to FP64 rounding."""
+    from specfempp_b200 import meshgen
+    from oracle import runner
+    from conftest import workload_case
+    w = meshgen.nonconforming_coupled(nx_el=16, nx_ac=16, nz_el=8, nz_ac=6, nstep=700)
+    a = runner.run(workload_case(w), "f64", nthreads=8)["seis"][:, 0]
+    twin = meshgen.merge_interface_nodes(w.mesh)
+    assert len(np.unique(twin.knods)) < len(np.unique(w.mesh.knods))
+    w.mesh = twin
+    b = runner.run(workload_case(w), "f64", nthreads=8)["seis"][:, 0]
+    assert np.abs(b[:, :4]).max() > 0                     # elastic side excited through the interface
+    assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-10
+
+
+def test_oracle_nonconforming_records_checked(oracle_lib):
+    """A nonconforming record without its reverse is refused (the reference's
+    symmetry check), as is a record pair whose edges do not overlap."""
+    from specfempp_b200 import meshgen
+    from oracle import runner
+    from conftest import workload_case
+    w = meshgen.nonconforming_coupled(nx_el=6, nx_ac=9, nz_el=3, nz_ac=3, nstep=5)
+    adj = w.mesh.adjacency
+    nc = np.nonzero(adj[:, 2] == 3)[0]
+    w.mesh.adjacency = np.delete(adj, nc[0], axis=0)
+    with pytest.raises(RuntimeError, match="Non-symmetric"):
+        runner.run(workload_case(w), "f32")
+    w = meshgen.nonconforming_coupled(nx_el=6, nx_ac=9, nz_el=3, nz_ac=3, nstep=5)
+    adj = w.mesh.adjacency.copy()
+    e, a = adj[nc[0], 0], adj[nc[0], 1]
+    far = a + 8                                            # a water element far from e
+    adj[nc[0], 1] = far
+    back = np.nonzero((adj[:, 0] == a) & (adj[:, 1] == e))[0][0]
+    adj[back, 0] = far
+    w.mesh.adjacency = adj
+    with pytest.raises(RuntimeError, match="intersection"):
+        runner.run(workload_case(w), "f32")
