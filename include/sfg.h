@@ -92,6 +92,16 @@ typedef struct sfg_mesh2d_desc {
                                     kappa, mu, nu, j, lambda_c, mu_c, nu_c; NaN rows: other
                                     materials); the elastic medium then has three
                                     components (u_x, u_z, rotation), P-SV only */
+  int nadj;                      /* adjacency records (0: none) */
+  const int *adjacency;          /* optional [nadj][4] (element, neighbour, connection 1
+                                    strongly conforming / 3 nonconforming, orientation of
+                                    the shared entity on the element 0 bottom 1 right 2 top
+                                    3 left 4..7 corners), 0-based: the mesh's adjacency
+                                    graph (src/io/mesh/impl/fortran/dim2/read_adjacency_graph.cpp).
+                                    A nonconforming acoustic-elastic record and its
+                                    reverse couple the two media through the edges'
+                                    intersection (P-SV elastic media); strongly
+                                    conforming records are implied by shared control nodes */
 } sfg_mesh2d_desc;
 
 typedef struct sfg_options {

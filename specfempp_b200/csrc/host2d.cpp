@@ -2,6 +2,8 @@
 #include "host2d.hpp"
 
 #include <algorithm>
+#include <map>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -172,6 +174,108 @@ void edge_normal(const JacD &J, int type, double &nx, double &nz) {
   }
 }
 
+// (xi, gamma) of local coordinate c along an edge: xi runs along bottom and
+// top, gamma along left and right.
+void edge_local(int t, double c, double &xi, double &ga) {
+  if (t == BOTTOM) { xi = c; ga = -1; }
+  else if (t == RIGHT) { xi = 1; ga = c; }
+  else if (t == TOP) { xi = c; ga = 1; }
+  else { xi = -1; ga = c; }
+}
+
+// Local coordinate along edge t of element e of the point closest to
+// (X, Z): Newton steps from 0 on the edge coordinate, clamped to [-1, 1],
+// stopping at an end whose step points outside
+// (src/algorithms/dim2/locate_point_impl.cpp:126-198).
+double edge_coordinate(const Mesh2D &m, int e, int t, double X, double Z) {
+  double xi, ga;
+  edge_local(t, 0.0, xi, ga);
+  double &c = (t == BOTTOM || t == TOP) ? xi : ga;
+  for (int it = 0; it < 100; ++it) {
+    const JacD J = jacobian(m, e, xi, ga);
+    const double dx = -(J.x - X), dz = -(J.z - Z);
+    const double d = (t == BOTTOM || t == TOP) ? J.xix * dx + J.xiz * dz : J.gax * dx + J.gaz * dz;
+    if (c == -1.0 && d < -1e-12) return -1.0;
+    if (c == 1.0 && d > 1e-12) return 1.0;
+    c = std::min(1.0, std::max(-1.0, c + d));
+    if (std::abs(d) < 1e-12) break;
+  }
+  return c;
+}
+
+int edge_point(int t, int k) {
+  return t == BOTTOM ? k : t == RIGHT ? k * NGLL + NGLL - 1 : t == TOP ? (NGLL - 1) * NGLL + k : k * NGLL;
+}
+
+// Coupling weights of one nonconforming edge pair: the self edge (e1, t1)
+// receives at its point i sum_j W[i][j] * (field of the coupled edge (e2,
+// t2) at its point j), W[i][j] = sum_q T1[q][i] f[q] n[q] T2[q][j] over an
+// NGLL-point GLL quadrature mapped linearly onto the edges' intersection in
+// the self edge's local coordinate; T1, T2 are the Lagrange interpolants at
+// the quadrature points on each edge, f[q] = w_q |dx/dxi| and n[q] the self
+// element's outward unit normal from the derivative of the mapped points
+// (core/specfem/assembly/nonconforming_interfaces/dim2/impl/compute_intersection.cpp:49-167,
+// impl/interface_container.tpp:20-180; applied as in
+// include/kokkos_kernels/impl/compute_coupling.tpp:117-249).
+void nonconforming_weights(const Mesh2D &m, const double z[NGLL], const double w[NGLL],
+                           const double hp[NGLL][NGLL], int e1, int t1, int e2, int t2,
+                           double W[NGLL][NGLL][2]) {
+  auto corner = [&](int e, int k, double &x, double &zz) {
+    const int id = m.knods[size_t(e) * m.ngnod + k];
+    x = m.coorg[2 * size_t(id)];
+    zz = m.coorg[2 * size_t(id) + 1];
+  };
+  auto ends = [](int t, int &a, int &b) {
+    if (t == BOTTOM) { a = 0; b = 1; } else if (t == RIGHT) { a = 1; b = 2; }
+    else if (t == TOP) { a = 3; b = 2; } else { a = 0; b = 3; }
+  };
+  int a1, b1, a2, b2;
+  ends(t1, a1, b1);
+  ends(t2, a2, b2);
+  double x, zz;
+  corner(e2, a2, x, zz); const double p2lo = edge_coordinate(m, e1, t1, x, zz);
+  corner(e2, b2, x, zz); const double p2hi = edge_coordinate(m, e1, t1, x, zz);
+  corner(e1, a1, x, zz); const double p1lo = edge_coordinate(m, e2, t2, x, zz);
+  corner(e1, b1, x, zz); const double p1hi = edge_coordinate(m, e2, t2, x, zz);
+  const double min1 = std::min(p2lo, p2hi), max1 = std::max(p2lo, p2hi);
+  const double min2 = std::min(p1lo, p1hi), max2 = std::max(p1lo, p1hi);
+  if (min1 > max1 - 1e-5 || min2 > max2 - 1e-5)
+    throw std::runtime_error("nonconforming edges without an intersection");
+  double T1[NGLL][NGLL], T2[NGLL][NGLL], lx[NGLL], lz[NGLL];
+  for (int q = 0; q < NGLL; ++q) {
+    const double c1 = 0.5 * ((max1 - min1) * z[q] + (max1 + min1));
+    double xi, ga;
+    edge_local(t1, c1, xi, ga);
+    const JacD J = jacobian(m, e1, xi, ga);
+    lagrange(c1, z, T1[q]);
+    lagrange(edge_coordinate(m, e2, t2, J.x, J.z), z, T2[q]);
+  }
+  for (int k = 0; k < NGLL; ++k) {
+    double lc = 0, xi, ga;
+    for (int i = 0; i < NGLL; ++i) lc += T1[k][i] * z[i];
+    edge_local(t1, lc, xi, ga);
+    const JacD J = jacobian(m, e1, xi, ga);
+    lx[k] = J.x;
+    lz[k] = J.z;
+  }
+  for (int i = 0; i < NGLL; ++i)
+    for (int j = 0; j < NGLL; ++j) W[i][j][0] = W[i][j][1] = 0.0;
+  for (int q = 0; q < NGLL; ++q) {
+    double drx = 0, drz = 0;
+    for (int k = 0; k < NGLL; ++k) { drx += hp[q][k] * lx[k]; drz += hp[q][k] * lz[k]; }
+    const double f = w[q] * std::sqrt(drx * drx + drz * drz);
+    double mag = std::sqrt(drx * drx + drz * drz);
+    if (t1 == TOP || t1 == LEFT) mag = -mag;
+    const double nx = drz / mag, nz = -drx / mag;
+    for (int i = 0; i < NGLL; ++i)
+      for (int j = 0; j < NGLL; ++j) {
+        const double c = T1[q][i] * f * T2[q][j];
+        W[i][j][0] += c * nx;
+        W[i][j][1] += c * nz;
+      }
+  }
+}
+
 }  // namespace
 
 bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
@@ -286,9 +390,18 @@ bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
     for (int i = 0; i < ntang; ++i) r.next();
     for (int i = 0; i < naxis; ++i) r.next();
     if (r.more()) {
+      // adjacency graph (src/io/mesh/impl/fortran/dim2/read_adjacency_graph.cpp:11-40)
       const char *p = r.next(4);
       int nadj = rd<int>(p);
-      for (int i = 0; i < nadj; ++i) r.next();
+      m.adjacency.reserve(4 * size_t(std::max(nadj, 0)));
+      for (int i = 0; i < nadj; ++i) {
+        const char *q = r.next(16);
+        const int e = rd<int>(q), nb = rd<int>(q), conn = rd<int>(q), orient = rd<int>(q);
+        if (conn != 1 && conn != 3) throw std::runtime_error("Unknown connection type in adjacency graph.");
+        if (e < 1 || e > m.nspec || nb < 1 || nb > m.nspec || orient < 1 || orient > 8)
+          throw std::runtime_error("bad adjacency record");
+        m.adjacency.insert(m.adjacency.end(), {e - 1, nb - 1, conn, orient - 1});
+      }
     }
     if (r.more()) throw std::runtime_error("The Database file wasn't fully read");
   } catch (const std::exception &ex) {
@@ -692,6 +805,51 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
     }
   }
 
+  // --- nonconforming acoustic-elastic coupling ----------------------
+  // A nonconforming record between different media and its reverse record
+  // give a self and a coupled edge (core/specfem/assembly/edge_types/dim2/edge_types.cpp);
+  // the self points receive weighted sums of the coupled edge's points
+  // (nonconforming_weights).  Contributions of acoustic points on the free
+  // surface are dropped as for conforming edges.
+  std::vector<std::unordered_map<int, std::map<int, std::array<double, 2>>>> ncw(2);
+  if (!m.adjacency.empty()) {
+    std::map<std::pair<int, int>, int> orient;
+    const size_t nadj = m.adjacency.size() / 4;
+    for (size_t r = 0; r < nadj; ++r) {
+      const int *rec = &m.adjacency[4 * r];
+      if (rec[2] == 3) orient[{rec[0], rec[1]}] = rec[3];
+      else if (rec[2] != 1) throw std::runtime_error("Unknown connection type in adjacency graph.");
+    }
+    for (const auto &kv : orient) {
+      const int e1 = kv.first.first, e2 = kv.first.second, t1 = kv.second;
+      if (e1 < 0 || e1 >= nspec || e2 < 0 || e2 >= nspec) throw std::runtime_error("bad adjacency record");
+      if (a.mesh_medium[e1] == a.mesh_medium[e2]) continue;
+      const auto back = orient.find({e2, e1});
+      if (back == orient.end())
+        throw std::runtime_error("Non-symmetric adjacency graph detected in `compute_intersection`.");
+      const int t2 = back->second;
+      if (t1 > LEFT || t2 > LEFT) throw std::runtime_error("compute_intersection must be given edges");
+      if (m.elastic_wave == 1 || !m.mat_cosserat.empty())
+        throw std::runtime_error("nonconforming coupling: P-SV isotropic or anisotropic elastic media only");
+      double W[NGLL][NGLL][2];
+      nonconforming_weights(m, z, w, hp, e1, t1, e2, t2, W);
+      const int med = a.mesh_medium[e1];
+      const auto it = bc.find(e1);
+      for (int i = 0; i < NGLL; ++i) {
+        const int q1 = edge_point(t1, i);
+        const int g = gid[size_t(e1) * NPTS + q1];
+        auto &row = ncw[med][g];      // marks the point as coupled
+        if (it != bc.end() && it->second[q1].fs) continue;
+        for (int j = 0; j < NGLL; ++j) {
+          auto &acc = row[gid[size_t(e2) * NPTS + edge_point(t2, j)]];
+          acc[0] += W[i][j][0];
+          acc[1] += W[i][j][1];
+        }
+      }
+    }
+  }
+  const bool nonconforming = !ncw[0].empty() || !ncw[1].empty();
+
   // --- compute order, per-medium numbering, element arrays -----------
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
@@ -731,7 +889,8 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
         const int e = D.elem_mesh[ce];
         for (int q = 0; q < NPTS; ++q) {
           const int g = gid[size_t(e) * NPTS + q];
-          if (g2m[g] >= 0 || (pass == 0) != bool(is_iface[med][g])) continue;
+          const bool iface = is_iface[med][g] || (nonconforming && ncw[med].count(g));
+          if (g2m[g] >= 0 || (pass == 0) != iface) continue;
           g2m[g] = D.nglob++;
           D.glob_of_point.push_back(g);
         }
@@ -766,6 +925,38 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
   for (int med = 0; med < 2; ++med) {
     MediumData &D = med == 1 ? a.el : a.ac;
     const std::vector<int> &other = med == 1 ? a.glob_to_ac : a.glob_to_el;
+    if (nonconforming) {
+      // several entries per point: the conforming one (same global point)
+      // and the nonconforming ones, merged per point of the other medium
+      D.cp_start.assign(D.niface + 1, 0);
+      D.cp_nx.clear(); D.cp_nz.clear(); D.cp_other.clear();
+      for (int i = 0; i < D.niface; ++i) {
+        const int g = D.glob_of_point[i];
+        std::map<int, std::array<double, 2>> ent;
+        if (is_iface[med][g]) {
+          if (other[g] < 0) throw std::runtime_error("coupled point missing in the other medium");
+          auto &e = ent[other[g]];
+          e[0] += cpl[med][2 * size_t(g)];
+          e[1] += cpl[med][2 * size_t(g) + 1];
+        }
+        const auto it = ncw[med].find(g);
+        if (it != ncw[med].end())
+          for (const auto &kv : it->second) {
+            const int o = other[kv.first];
+            if (o < 0) throw std::runtime_error("coupled point missing in the other medium");
+            auto &e = ent[o];
+            e[0] += kv.second[0];
+            e[1] += kv.second[1];
+          }
+        for (const auto &kv : ent) {
+          D.cp_other.push_back(kv.first);
+          D.cp_nx.push_back(float(kv.second[0]));
+          D.cp_nz.push_back(float(kv.second[1]));
+        }
+        D.cp_start[i + 1] = int(D.cp_other.size());
+      }
+      continue;
+    }
     D.cp_nx.assign(D.niface, 0.f); D.cp_nz.assign(D.niface, 0.f); D.cp_other.assign(D.niface, -1);
     for (int i = 0; i < D.niface; ++i) {
       const int g = D.glob_of_point[i];

@@ -34,6 +34,9 @@ struct Mesh2D {
   std::vector<float> prho, pvp, pvs;  // optional [nspec][25]
   std::vector<int> abs_ispec, abs_type, free_ispec, free_type;
   int elastic_wave = 0;               // 0 P-SV, 1 SH
+  // adjacency records [n][4] (element, neighbour, connection 1 strongly
+  // conforming / 3 nonconforming, orientation 0..7), 0-based
+  std::vector<int> adjacency;
 };
 
 // Reads a SPECFEM2D database.bin (Fortran unformatted records).
@@ -69,10 +72,14 @@ struct MediumData {
   std::vector<float> bc_w, bc_nx, bc_nz, bc_j1, bc_imp0, bc_imp1, bc_keep, bc_imp2;
   // coupling with the other medium: the first niface points of the medium's
   // numbering lie on coupled edges; per point the sum over the coupled edges
-  // of GLL weight * outward normal, and the other medium's id of the point
+  // of GLL weight * outward normal, and the other medium's id of the point.
+  // With nonconforming interfaces a point couples to several points of the
+  // other medium: cp_start [niface + 1] then gives each point's range of
+  // (cp_nx, cp_nz, cp_other) entries; empty = one entry per point.
   int niface = 0;
-  std::vector<float> cp_nx, cp_nz;    // [niface]
-  std::vector<int> cp_other;          // [niface]
+  std::vector<float> cp_nx, cp_nz;    // [niface] or [cp_start[niface]]
+  std::vector<int> cp_other;          // [niface] or [cp_start[niface]]
+  std::vector<int> cp_start;          // empty or [niface + 1]
   std::vector<int> glob_of_point;     // medium point id -> mesh global id
   // owner-computes assembly: for every medium point, the element-local
   // indices (compute element * 25 + GLL point) that contribute to it, in

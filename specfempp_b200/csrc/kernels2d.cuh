@@ -554,10 +554,13 @@ struct UpdateArgs {
   int ncomp;
   // coupling: the first niface points take cp_n . other[cp_other] (acoustic
   // self: other = elastic displacement, float2) or cp_n * other (elastic self:
-  // other = acoustic chi_dd)
+  // other = acoustic chi_dd); with nonconforming interfaces a sum of such
+  // terms over the entries cp_start[pt] .. cp_start[pt + 1] (cp_start null:
+  // entry pt alone)
   int niface;
   const float *__restrict__ cp_nx, *__restrict__ cp_nz;
   const int *__restrict__ cp_other;
+  const int *__restrict__ cp_start;
   const float *__restrict__ other;
   // owner-computes assembly: accum of point g = sum of r[inv_start[g] .. inv_start[g+1])
   const int *__restrict__ inv_start;
@@ -570,14 +573,22 @@ struct UpdateArgs {
   const SegRecord *rec;          // optional segment recording (then advance = 0)
 };
 
-__device__ __forceinline__ float coupling_term(const UpdateArgs &A, int pt, int comp) {
-  const int o = A.cp_other[pt];
+__device__ __forceinline__ float coupling_entry(const UpdateArgs &A, int k, int comp) {
+  const int o = A.cp_other[k];
   if (A.ncomp == 1) {  // acoustic self: n . u_elastic
     const float2 ue = reinterpret_cast<const float2 *>(A.other)[o];
-    return A.cp_nx[pt] * ue.x + A.cp_nz[pt] * ue.y;
+    return A.cp_nx[k] * ue.x + A.cp_nz[k] * ue.y;
   }
   const float chi_dd = A.other[o];  // elastic self: n * chi_dd
-  return (comp == 0 ? A.cp_nx[pt] : A.cp_nz[pt]) * chi_dd;
+  return (comp == 0 ? A.cp_nx[k] : A.cp_nz[k]) * chi_dd;
+}
+
+__device__ __forceinline__ float coupling_term(const UpdateArgs &A, int pt, int comp) {
+  if (!A.cp_start) return coupling_entry(A, pt, comp);
+  const int k1 = A.cp_start[pt + 1];
+  float t = 0.f;
+  for (int k = A.cp_start[pt]; k < k1; ++k) t += coupling_entry(A, k, comp);
+  return t;
 }
 
 // Newmark predictor u += dt v + dt^2/2 a; v += dt/2 a (newmark.tpp:64-128),

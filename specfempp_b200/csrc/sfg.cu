@@ -83,6 +83,7 @@ struct DevMedium {
   int niface = 0;
   float *cp_nx = nullptr, *cp_nz = nullptr;
   int *cp_other = nullptr;
+  int *cp_start = nullptr;         // nonconforming interfaces: entry ranges per point
   int *src_head = nullptr;
   float *minv = nullptr;
   float *u = nullptr, *v = nullptr, *accum = nullptr, *a = nullptr;
@@ -277,6 +278,7 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.bc_imp2 = m.upload(M.bc_imp2);
   D.niface = M.niface;
   D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
+  D.cp_start = M.cp_start.empty() ? nullptr : m.upload(M.cp_start);
   D.minv = m.upload(M.minv);
   D.S = h->asmb.nshots;
   const size_t n = D.values();
@@ -482,7 +484,7 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   U.n = int(D.values());
   U.ncomp = D.ncomp;
   U.niface = D.niface;
-  U.cp_nx = D.cp_nx; U.cp_nz = D.cp_nz; U.cp_other = D.cp_other;
+  U.cp_nx = D.cp_nx; U.cp_nz = D.cp_nz; U.cp_other = D.cp_other; U.cp_start = D.cp_start;
   U.other = medium == SFG_MEDIUM_ELASTIC ? O.a : O.u;
   const float dt = float(h->asmb.dt);
   U.dt = dt;
@@ -860,6 +862,8 @@ int sfg_create2d(const sfg_mesh2d_desc *d, const sfg_options *opt, sfg_handle **
     m.mat_vs.assign(d->mat_vs, d->mat_vs + d->numat);
     if (d->mat_aniso) m.mat_aniso.assign(d->mat_aniso, d->mat_aniso + 6 * size_t(d->numat));
     if (d->mat_cosserat) m.mat_cosserat.assign(d->mat_cosserat, d->mat_cosserat + 8 * size_t(d->numat));
+    if (d->nadj < 0 || (d->nadj > 0 && !d->adjacency)) throw std::runtime_error("bad adjacency records");
+    if (d->nadj > 0) m.adjacency.assign(d->adjacency, d->adjacency + 4 * size_t(d->nadj));
     const size_t np = size_t(d->nspec) * sfg::NPTS;
     if (d->point_rho) m.prho.assign(d->point_rho, d->point_rho + np);
     if (d->point_vp) m.pvp.assign(d->point_vp, d->point_vp + np);
@@ -1053,7 +1057,8 @@ int sfg_initialize(sfg_handle *h) {
     {
       // interface points paired one to one, one shot, P-SV: fused updates
       const sfg::MediumData &E = a.el, &C = a.ac;
-      bool ok = E.nspec && C.nspec && a.nshots == 1 && E.ncomp == 2 && E.niface == C.niface;
+      bool ok = E.nspec && C.nspec && a.nshots == 1 && E.ncomp == 2 && E.niface == C.niface &&
+                E.cp_start.empty() && C.cp_start.empty();
       for (int i = 0; ok && i < E.niface; ++i) {
         const int j = E.cp_other[i];
         ok = j >= 0 && j < C.niface && C.cp_other[j] == i;

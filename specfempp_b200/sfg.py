@@ -40,6 +40,7 @@ class MeshDesc(C.Structure):
         ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
         ("elastic_wave", C.c_int),
         ("mat_aniso", _dp), ("mat_cosserat", _dp),
+        ("nadj", C.c_int), ("adjacency", _ip),
     ]
 
 
@@ -212,6 +213,13 @@ class Simulation2D:
         if aniso is not None:
             aniso = _arr(aniso, np.float64).reshape(len(m.mat_rho), 6)
             d.mat_aniso = self._k(np.ascontiguousarray(aniso)).ctypes.data_as(_dp)
+        adj = getattr(m, "adjacency", None)
+        if adj is None:
+            adj = getattr(m, "extra", {}).get("adjacency")
+        if adj is not None and len(adj):
+            adj = _arr(adj, np.int32).reshape(-1, 4)
+            d.nadj = len(adj)
+            d.adjacency = self._k(np.ascontiguousarray(adj)).ctypes.data_as(_ip)
         return d
 
     def _check(self, rc):

@@ -141,3 +141,41 @@ def test_cosserat_mesh_has_three_components(sfg_lib):
     case, _, _ = golden_case("HomogeneousIsotropicCosseratDomain", nstep=10)
     sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=10)
     assert sim.info().ncomp_elastic == 3 and sim.ncomp == 3
+
+
+def test_nonconforming_records_host_side(tmp_path, sfg_lib):
+    """Adjacency records survive the database round trip (oracle reader and
+    the product's reader agree on the numbering); a nonconforming record
+    without its reverse, an out-of-range record and non-overlapping edges
+    are refused at creation (host assembly, no GPU)."""
+    from oracle.database2d import read_database
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.nonconforming_coupled(nx_el=6, nx_ac=9, nz_el=3, nz_ac=3, nstep=5)
+    p = str(tmp_path / "database.bin")
+    meshgen.write_database(w.mesh, p)
+    m = read_database(p)
+    assert np.array_equal(m.extra["adjacency"], w.mesh.adjacency)
+    a = sfg.Simulation2D(database=p, dt=w.dt, nstep=5)
+    b = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
+    ia, ib = a.info(), b.info()
+    assert (ia.nglob_elastic, ia.nglob_acoustic) == (ib.nglob_elastic, ib.nglob_acoustic)
+    # no shared control nodes across the interface: no conforming coupling
+    assert ia.nglob_elastic == (6 * 4 + 1) * (3 * 4 + 1)
+    adj = w.mesh.adjacency
+    nc = np.nonzero(adj[:, 2] == 3)[0]
+    w.mesh.adjacency = np.delete(adj, nc[0], axis=0)
+    with pytest.raises(sfg.SfgError, match="Non-symmetric"):
+        sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
+    bad = adj.copy()
+    bad[nc[0], 1] = w.mesh.nspec
+    w.mesh.adjacency = bad
+    with pytest.raises(sfg.SfgError, match="adjacency"):
+        sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
+    far = adj.copy()
+    e, ac = far[nc[0], 0], far[nc[0], 1]
+    back = np.nonzero((far[:, 0] == ac) & (far[:, 1] == e))[0][0]
+    far[nc[0], 1] = ac + 8
+    far[back, 0] = ac + 8
+    w.mesh.adjacency = far
+    with pytest.raises(sfg.SfgError, match="intersection"):
+        sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
