@@ -60,6 +60,10 @@ class Mesh2D:
     # [numat][8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c, mu_c, nu_c);
     # NaN rows for other materials
     mat_cosserat: np.ndarray | None = None
+    # [numat][13] isotropic poroelastic constants (rho_s, rho_f, phi,
+    # tortuosity, kxx, kxz, kzz, kappa_s, kappa_f, kappa_fr, eta_f, mu_fr,
+    # Q_mu); NaN rows are other materials
+    mat_poro: np.ndarray | None = None
 
 
 def _records(buf: bytes):
@@ -130,6 +134,7 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
     mat_vs = np.zeros(numat)
     mat_aniso = np.full((numat, 6), np.nan)
     mat_cos = np.full((numat, 8), np.nan)
+    mat_poro = np.full((numat, 13), np.nan)
     for m in range(numat):
         vals = struct.unpack("<ii13d", take())
         n, indic = vals[0], vals[1]
@@ -152,6 +157,15 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
             mat_rho[m] = v[0]
             mat_vp[m] = np.sqrt((v[1] + 4.0 / 3.0 * v[2]) / v[0])
             mat_vs[m] = np.sqrt(v[2] / v[0])
+            mat_medium[m] = ELASTIC
+            continue
+        if indic == 3:
+            # isotropic poroelastic: rho_s, rho_f, phi, tortuosity, kxx, kxz,
+            # kzz, kappa_s, kappa_f, kappa_fr, eta_f, mu_fr, Q_mu
+            # (read_material_properties.cpp:303-332)
+            mat_poro[m] = v[0:13]
+            mat_rho[m] = (1.0 - v[2]) * v[0] + v[2] * v[1]      # rho_bar
+            mat_vp[m] = mat_vs[m] = 0.0                        # unused: Biot constants
             mat_medium[m] = ELASTIC
             continue
         if indic != 1:
@@ -222,4 +236,5 @@ def read_database(path: str, elastic_wave: str = "psv") -> Mesh2D:
                   coupled_pairs=np.asarray(pairs, np.int32).reshape(-1, 2),
                   title=title, extra=extra,
                   mat_aniso=mat_aniso if np.isfinite(mat_aniso).any() else None,
-                  mat_cosserat=mat_cos if np.isfinite(mat_cos).any() else None)
+                  mat_cosserat=mat_cos if np.isfinite(mat_cos).any() else None,
+                  mat_poro=mat_poro if np.isfinite(mat_poro).any() else None)

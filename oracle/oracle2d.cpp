@@ -254,6 +254,9 @@ struct Sim {
   std::vector<T> p_c[6];
   // Cosserat (when in.cosserat): rho, kappa, mu, nu, j, lambda_c, mu_c, nu_c
   std::vector<T> p_cs[8];
+  // poroelastic (when in.poro): phi, rho_s, rho_f, tortuosity, mu_G, H_Biot,
+  // C_Biot, M_Biot, permxx, permxz, permzz, eta_f
+  std::vector<T> p_po[12];
   // Stacey point data per element (dense, tag 0/1)
   std::vector<uint8_t> st_tag, fs_tag;   // [nspec][25]
   std::vector<T> st_nx, st_nz, st_w;     // [nspec][25]
@@ -278,7 +281,7 @@ struct Sim {
   };
   std::vector<NCEdge> nc_ac, nc_el;     // self acoustic / self elastic
   // sources
-  struct Src { int ispec; int medium; T arr[3][NP]; int ncomp; std::vector<T> stf; };
+  struct Src { int ispec; int medium; T arr[4][NP]; int ncomp; std::vector<T> stf; };
   std::vector<Src> srcs;
   struct Rec { int ispec; T h[NP]; };
   std::vector<Rec> recs;
@@ -295,7 +298,7 @@ struct Sim {
       for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
     }
     dt = T(in.dt);
-    ncomp_el = in.cosserat ? 3 : in.elastic_sh ? 1 : 2;
+    ncomp_el = in.poro ? 4 : in.cosserat ? 3 : in.elastic_sh ? 1 : 2;
     number_points();
     geometry();
     properties();
@@ -430,6 +433,28 @@ struct Sim {
           p_rho[p] = p_cs[0][p]; p_kappa[p] = p_cs[1][p]; p_mu[p] = p_cs[2][p];
         }
     }
+    if (in.poro) {
+      if (in.elastic_sh || in.aniso || in.cosserat)
+        throw std::runtime_error("poroelastic media are P-SV isotropic only");
+      for (int k = 0; k < 12; ++k) p_po[k].assign(n, T(0));
+      for (size_t p = 0; p < n; ++p) {
+        if (medium[p / NP] != MED_ELASTIC) continue;
+        const double *v = in.poro + p * 13;
+        // material.hpp: Q_mu must be 9999 (no attenuation); Biot coefficients
+        // with the reference's mixed float / double literal arithmetic
+        if (std::abs(T(v[12]) - 9999.0) > 1e-6)
+          throw std::runtime_error("poroelastic attenuation is not implemented");
+        const T rhos = T(v[0]), rhof = T(v[1]), phi = T(v[2]), tort = T(v[3]);
+        const T ks = T(v[7]), kf = T(v[8]), kfr = T(v[9]), etaf = T(v[10]), mufr = T(v[11]);
+        const T D = T(double(ks) * (1.0 + double(phi) * (double(ks / kf) - 1.0)));
+        const T fac = T(1.0 / double(D - kfr));
+        const T H = T(double((ks - kfr) * (ks - kfr) * fac + kfr) + 4.0 / 3.0 * double(mufr));
+        const T C = ks * (ks - kfr) * fac;
+        const T M = ks * ks * fac;
+        const T vals[12] = {phi, rhos, rhof, tort, mufr, H, C, M, T(v[4]), T(v[5]), T(v[6]), etaf};
+        for (int k = 0; k < 12; ++k) p_po[k][p] = vals[k];
+      }
+    }
     if (in.aniso) {
       if (in.elastic_sh) throw std::runtime_error("anisotropic SH is outside this path");
       for (int k = 0; k < 6; ++k) {
@@ -440,6 +465,8 @@ struct Sim {
   }
 
   T lp2m(size_t p) const { return p_kappa[p] + T(4.0 / 3.0) * p_mu[p]; }
+  // poroelastic rho_bar = (1 - phi) rho_s + phi rho_f (poroelastic/isotropic/properties.hpp)
+  T rho_bar(size_t p) const { return ((T(1) - p_po[0][p]) * p_po[1][p]) + (p_po[0][p] * p_po[2][p]); }
   // anisotropic: rho vp = sqrt(rho c33), rho vs = sqrt(rho c55)
   // (include/medium/dim2/elastic/anisotropic/properties.hpp:88-94)
   T rho_vp(size_t p) const {
@@ -503,7 +530,8 @@ struct Sim {
       auto [e1, t1] = kv.second[0];
       auto [e2, t2] = kv.second[1];
       if (medium[e1] == medium[e2]) continue;
-      if (ncomp_el == 3) throw std::runtime_error("Cosserat media are not coupled to acoustic ones here");
+      if (ncomp_el >= 3)
+        throw std::runtime_error("Cosserat and poroelastic media are not coupled to acoustic ones here");
       for (auto [e, t] : {std::make_pair(e1, t1), std::make_pair(e2, t2)}) {
         for (int iz = 0; iz < NG; ++iz)
           for (int ix = 0; ix < NG; ++ix) {
@@ -670,9 +698,19 @@ struct Sim {
             minv_a[g] += m;
           } else {
             is_el_glob[g] = 1;
-            // Cosserat: rho, rho, j (isotropic_cosserat/mass_matrix.tpp)
-            T m[3] = {p_rho[p] * fac, p_rho[p] * fac, ncomp_el == 3 ? p_cs[4][p] * fac : T(0)};
+            // Cosserat: rho, rho, j (isotropic_cosserat/mass_matrix.tpp);
+            // poroelastic: rho_bar - phi rho_f / tort twice, then
+            // (rho_f tort rho_bar - phi rho_f^2) / (phi rho_bar) twice
+            // (poroelastic/isotropic/mass_matrix.tpp)
+            T m[4] = {p_rho[p] * fac, p_rho[p] * fac, ncomp_el == 3 ? p_cs[4][p] * fac : T(0), T(0)};
+            if (ncomp_el == 4) {
+              const T phi = p_po[0][p], rhof = p_po[2][p], tort = p_po[3][p], rb = rho_bar(p);
+              const T solid = rb - phi * rhof / tort;
+              const T fluid = (rhof * tort * rb - phi * rhof * rhof) / (phi * rb);
+              m[0] = solid * fac; m[1] = solid * fac; m[2] = fluid * fac; m[3] = fluid * fac;
+            }
             if (st_tag[p]) {
+              if (ncomp_el == 4) throw std::runtime_error("Stacey edges on poroelastic media are outside this path");
               T v[3] = {T(-1) * dt * T(0.5), T(-1) * dt * T(0.5), T(-1) * dt * T(0.5)};
               stacey(p, v, m);
             }
@@ -815,15 +853,19 @@ struct Sim {
       T h[NP];
       interpolants(xi, ga, h);
       if (in.src_kind && in.src_kind[s] == 1) {
+        if (ncomp_el == 4 && S.medium == MED_ELASTIC)
+          throw std::runtime_error("moment-tensor sources in poroelastic media are outside this path");
         moment_tensor_array(S, e, xi, ga, in.src_mxx[s], in.src_mzz[s], in.src_mxz[s]);
       } else {
-        T fv[3] = {0, 0, 0};
+        T fv[4] = {0, 0, 0, 0};
         if (S.medium == MED_ACOUSTIC || ncomp_el == 1) { S.ncomp = 1; fv[0] = 1; }
         else {
-          // Cosserat: (sin, cos, 0) (vector_source/force_source.cpp:62-67)
+          // Cosserat: (sin, cos, 0); poroelastic: (sin, cos, sin, cos)
+          // (vector_source/force_source.cpp:53-67)
           S.ncomp = ncomp_el;
           T ang = T(in.src_angle[s]) * T(M_PI) / T(180.0);
           fv[0] = std::sin(ang); fv[1] = std::cos(ang);
+          if (ncomp_el == 4) { fv[2] = fv[0]; fv[3] = fv[1]; }
         }
         for (int q = 0; q < NP; ++q)
           for (int c = 0; c < S.ncomp; ++c) S.arr[c][q] = h[q] * fv[c];
@@ -859,7 +901,7 @@ struct Sim {
   template <typename AddFn>
   void stiffness_element(int e, int ncomp, const std::vector<T> &u, const std::vector<T> &v,
                          AddFn add) const {
-    T fu[NP][3], F[NP][3][2], Sa[NP][2];   // Sa: Cosserat sigma_xz, sigma_zx
+    T fu[NP][4], F[NP][4][2], Sa[NP][2];   // Sa: Cosserat sigma_xz, sigma_zx
     const int *ib = &ibool[size_t(e) * NP];
     for (int q = 0; q < NP; ++q)
       for (int c = 0; c < ncomp; ++c) fu[q][c] = u[size_t(ib[q]) * ncomp + c];
@@ -868,19 +910,35 @@ struct Sim {
       for (int ix = 0; ix < NG; ++ix) {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
-        T dxi[3] = {0, 0, 0}, dga[3] = {0, 0, 0};
+        T dxi[4] = {0, 0, 0, 0}, dga[4] = {0, 0, 0, 0};
         for (int l = 0; l < NG; ++l)
           for (int c = 0; c < ncomp; ++c) {
             dxi[c] += hp[ix][l] * fu[iz * NG + l][c];
             dga[c] += hp[iz][l] * fu[l * NG + ix][c];
           }
-        T du[3][2];
+        T du[4][2];
         for (int c = 0; c < ncomp; ++c) {
           du[c][0] = xix[p] * dxi[c] + gax[p] * dga[c];
           du[c][1] = xiz[p] * dxi[c] + gaz[p] * dga[c];
         }
-        T S[3][2];
-        if (!acoustic && ncomp == 3) {
+        T S[4][2];
+        if (!acoustic && ncomp == 4) {
+          // poroelastic/isotropic/stress.hpp: solid stresses with lambda_G =
+          // H - 2 mu_G, fluid pressure sigma_p; rows u_s: sigma - phi/tort
+          // sigma_p, rows w: sigma_p delta - rho_f/rho_bar sigma
+          const T mu = p_po[4][p], C = p_po[6][p], M = p_po[7][p];
+          const T lam = p_po[5][p] - T(2.0) * mu, l2m = lam + T(2.0) * mu;
+          const T dw = du[2][0] + du[3][1];
+          const T sxx = l2m * du[0][0] + lam * du[1][1] + C * dw;
+          const T szz = l2m * du[1][1] + lam * du[0][0] + C * dw;
+          const T sxz = mu * (du[0][1] + du[1][0]);
+          const T sp = C * (du[0][0] + du[1][1]) + M * dw;
+          const T pt = p_po[0][p] / p_po[3][p], rr = p_po[2][p] / rho_bar(p);
+          S[0][0] = sxx - pt * sp; S[0][1] = sxz;
+          S[1][0] = sxz; S[1][1] = szz - pt * sp;
+          S[2][0] = sp - rr * sxx; S[2][1] = T(-1.0) * rr * sxz;
+          S[3][0] = T(-1.0) * rr * sxz; S[3][1] = sp - rr * szz;
+        } else if (!acoustic && ncomp == 3) {
           // Cosserat P-SV-T stress (isotropic_cosserat/stress.hpp, cosserat_stress.hpp):
           // lambda = kappa - 2/3 mu; rows u_x: (sxx, szx), u_z: (sxz, szz),
           // rotation: (mu_c + nu_c) grad(phi); sxz += 2 nu phi, szx -= 2 nu phi
@@ -926,18 +984,34 @@ struct Sim {
       for (int ix = 0; ix < NG; ++ix) {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
-        T t1[3] = {0, 0, 0}, t2[3] = {0, 0, 0};
+        T t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0};
         for (int l = 0; l < NG; ++l) {
           for (int c = 0; c < ncomp; ++c) t1[c] += F[iz * NG + l][c][0] * hp[l][ix] * w[l];
           for (int c = 0; c < ncomp; ++c) t2[c] += F[l * NG + ix][c][1] * hp[l][iz] * w[l];
         }
-        T acc[3];
+        T acc[4];
         for (int c = 0; c < ncomp; ++c) acc[c] = T(-1) * (w[iz] * t1[c] + w[ix] * t2[c]);
+        if (!acoustic && ncomp == 4) {
+          // viscous damping of the relative fluid motion (poroelastic/isotropic/damping.hpp,
+          // compute_stiffness_interaction.tpp:216-223): factor = w_x w_z |J|
+          const T fac = w[ix] * w[iz] * jac[p];
+          const T kxx = p_po[8][p], kxz = p_po[9][p], kzz = p_po[10][p], eta = p_po[11][p];
+          const T det = kxx * kzz - kxz * kxz;
+          const T ixx = kzz / det, ixz = T(-1.0) * kxz / det, izz = kxx / det;
+          const T v2 = v[size_t(ib[q]) * 4 + 2], v3 = v[size_t(ib[q]) * 4 + 3];
+          const T viscx = fac * ((eta * ixx * v2) + (eta * ixz * v3));
+          const T viscz = fac * ((eta * ixz * v2) + (eta * izz * v3));
+          const T pt = p_po[0][p] / p_po[3][p];
+          acc[0] += pt * viscx;
+          acc[1] += pt * viscz;
+          acc[2] -= viscx;
+          acc[3] -= viscz;
+        }
         // Cosserat couple stress: -W (sigma_xz - sigma_zx) on the rotation
         // (compute_stiffness_interaction.tpp:216-229, cosserat_couple_stress.hpp)
         if (!acoustic && ncomp == 3) acc[2] -= (Sa[q][0] - Sa[q][1]) * (w[ix] * w[iz] * jac[p]);
         if (st_tag[p]) {
-          T vel[3];
+          T vel[4];
           for (int c = 0; c < ncomp; ++c) vel[c] = v[size_t(ib[q]) * ncomp + c];
           stacey(p, vel, acc);
         }
@@ -1028,7 +1102,14 @@ struct Sim {
         size_t p = size_t(S.ispec) * NP + q;
         if (med == MED_ACOUSTIC)
           a[ib[q]] += -S.stf[istep] * S.arr[0][q] / p_kappa[p];
-        else
+        else if (ncomp == 4) {
+          // poroelastic/isotropic/source.hpp: solid rows times (1 - phi / tort),
+          // fluid rows times (1 - rho_f / rho_bar), double literals
+          const double fs = 1.0 - double(p_po[0][p] / p_po[3][p]);
+          const double ff = 1.0 - double(p_po[2][p] / rho_bar(p));
+          for (int c = 0; c < 4; ++c)
+            a[size_t(ib[q]) * 4 + c] += T(double(S.stf[istep] * S.arr[c][q]) * (c < 2 ? fs : ff));
+        } else
           for (int c = 0; c < ncomp; ++c) a[size_t(ib[q]) * ncomp + c] += S.stf[istep] * S.arr[c][q];
       }
     }
@@ -1105,7 +1186,20 @@ struct Sim {
               dxi[c] += hp[ix][l] * ue[size_t(ib[iz * NG + l]) * nc + c];
               dga[c] += hp[iz][l] * ue[size_t(ib[l * NG + ix]) * nc + c];
             }
-          if (type == 3) {
+          if (type == 3 && nc == 4) {
+            // poroelastic/isotropic/wavefield.hpp: -(C div u_s + M div w)
+            T dxf[2] = {0, 0}, dgf[2] = {0, 0};
+            for (int l = 0; l < NG; ++l)
+              for (int c = 0; c < 2; ++c) {
+                dxf[c] += hp[ix][l] * ue[size_t(ib[iz * NG + l]) * nc + 2 + c];
+                dgf[c] += hp[iz][l] * ue[size_t(ib[l * NG + ix]) * nc + 2 + c];
+              }
+            const T dux = xix[p] * dxi[0] + gax[p] * dga[0];
+            const T duz = xiz[p] * dxi[1] + gaz[p] * dga[1];
+            const T dwx = xix[p] * dxf[0] + gax[p] * dgf[0];
+            const T dwz = xiz[p] * dxf[1] + gaz[p] * dgf[1];
+            out[0] += R.h[q] * (T(-1.0) * (p_po[6][p] * (dux + duz) + p_po[7][p] * (dwx + dwz)));
+          } else if (type == 3) {
             const T dux = xix[p] * dxi[0] + gax[p] * dga[0];
             const T duz = xiz[p] * dxi[1] + gaz[p] * dga[1];
             const T k = nc == 3 ? p_kappa[p] : (lp2m(p) - T(2) * p_mu[p]) + T(2.0 / 3.0) * p_mu[p];

@@ -49,6 +49,11 @@ typedef struct OracleInput2D {
    * two media through an intersection quadrature; NULL or nadj 0: none */
   int nadj;
   const int *adjacency;
+  /* optional isotropic poroelastic materials per GLL point [nspec][25][13]
+   * (rho_s, rho_f, phi, tortuosity, kxx, kxz, kzz, kappa_s, kappa_f,
+   * kappa_fr, eta_f, mu_fr, Q_mu): four components (solid u_x, u_z, fluid
+   * w_x, w_z); NULL: none */
+  const double *poro;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

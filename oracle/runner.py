@@ -49,7 +49,7 @@ class OracleInput2D(C.Structure):
         ("setup_in_run_precision", C.c_int),
         ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
         ("aniso", _dp), ("cosserat", _dp),
-        ("nadj", C.c_int), ("adjacency", _ip),
+        ("nadj", C.c_int), ("adjacency", _ip), ("poro", _dp),
     ]
 
 
@@ -196,6 +196,23 @@ def nonconforming_records(m):
     return np.ascontiguousarray(adj[adj[:, 2] == 3])
 
 
+def poro_points(case):
+    """[nspec, 25, 13] poroelastic constants (rho_s, rho_f, phi, tortuosity,
+    kxx, kxz, kzz, kappa_s, kappa_f, kappa_fr, eta_f, mu_fr, Q_mu) when the mesh
+    has poroelastic materials, else None; every elastic element must then be
+    poroelastic."""
+    m = case.mesh
+    mp = getattr(m, "mat_poro", None)
+    if mp is None or not np.isfinite(mp).any():
+        return None
+    per = np.asarray(mp)[m.kmato]
+    elastic = np.asarray(m.mat_medium)[m.kmato] == 1
+    if not np.all(np.isfinite(per[elastic])):
+        raise ValueError("a mesh with poroelastic materials must be poroelastic in every elastic element")
+    per = np.where(np.isfinite(per), per, 0.0)
+    return np.ascontiguousarray(np.repeat(per[:, None, :], 25, axis=1))
+
+
 def cosserat_points(case):
     """[nspec, 25, 8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
     mu_c, nu_c) when the mesh has Cosserat materials, else None; every elastic
@@ -276,6 +293,8 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     inp.aniso = _ptr(arr(aniso, np.float64), _dp) if aniso is not None else None
     cos = cosserat_points(case)
     inp.cosserat = _ptr(arr(cos, np.float64), _dp) if cos is not None else None
+    poro = poro_points(case)
+    inp.poro = _ptr(arr(poro, np.float64), _dp) if poro is not None else None
     adj = nonconforming_records(m)
     inp.nadj = len(adj)
     inp.adjacency = _ptr(arr(adj, np.int32), _ip) if len(adj) else None
@@ -286,7 +305,8 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     final = None
     if want_final:
         nglob = L.oracle2d_count_nglob(C.byref(inp))
-        final = {"elastic": np.zeros((nglob, 3 if cos is not None else 1 if case.elastic_sh else 2)),
+        nce = 4 if poro is not None else 3 if cos is not None else 1 if case.elastic_sh else 2
+        final = {"elastic": np.zeros((nglob, nce)),
                  "acoustic": np.zeros(nglob),
                  "ibool": np.zeros((m.nspec, 25), np.int32)}
         out.final_u_elastic = _ptr(final["elastic"], _dp)

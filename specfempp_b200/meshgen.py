@@ -56,6 +56,10 @@ class Mesh:
     # optional [numat][8] Cosserat constants (rho, kappa, mu, nu, j, lambda_c,
     # mu_c, nu_c); NaN rows are other materials
     mat_cosserat: np.ndarray | None = None
+    # optional [numat][13] isotropic poroelastic constants (rho_s, rho_f, phi,
+    # tortuosity, kxx, kxz, kzz, kappa_s, kappa_f, kappa_fr, eta_f, mu_fr,
+    # Q_mu); NaN rows are other materials
+    mat_poro: np.ndarray | None = None
     # optional adjacency records [n][4]: (element, neighbour, connection 1
     # strongly conforming / 3 nonconforming, orientation of the shared entity
     # on the element: 0 bottom 1 right 2 top 3 left, 4..7 corners
@@ -148,6 +152,9 @@ def write_database(mesh: Mesh, path: str, title: str = "structured mesh") -> Non
                     0, 0, 0, 0))
     rec(struct.pack("<idi", 1, 0.0, 0))
     for m in range(len(mesh.mat_rho)):
+        if mesh.mat_poro is not None and np.isfinite(mesh.mat_poro[m]).all():
+            rec(struct.pack("<ii13d", m + 1, 3, *[float(x) for x in mesh.mat_poro[m]]))
+            continue
         vs = 0.0 if mesh.mat_medium[m] == ACOUSTIC else float(mesh.mat_vs[m])
         rec(struct.pack("<ii13d", m + 1, 1, float(mesh.mat_rho[m]), float(mesh.mat_vp[m]), vs,
                         0.0, 0.0, 9999.0, 9999.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0))
@@ -323,6 +330,41 @@ def nonconforming_coupled(nx_el: int = 30, nx_ac: int = 45, nz_el: int = 16, nz_
     src = [RickerSource(0.43 * width, h_el + 0.45 * h_ac, 8.0, 1e9)]
     return Workload(f"nonconforming_coupled_{nx_el}_{nx_ac}", mesh, src, rx, rz, 5e-4, nstep,
                     description=f"2D acoustic-elastic, nonconforming interface {nx_el}:{nx_ac}")
+
+
+# the saturated sandstone of the reference's poroelastic fixture:
+# rho_s, rho_f, phi, tortuosity, kxx, kxz, kzz, kappa_s, kappa_f, kappa_fr,
+# eta_f, mu_fr, Q_mu
+POROUS_SANDSTONE = (2650.0, 880.0, 0.1, 2.0, 1e-9, 0.0, 1e-9, 12.2e9, 1.985e9, 9.6e9, 0.0, 5.1e9, 9999.0)
+
+
+def poroelastic_model(nx: int = 50, nz: int = 50, width: float = 1000.0, height: float = 1000.0,
+                      eta_f: float = 0.0, kxz: float = 0.0, nstep: int = 1000,
+                      layered: bool = False) -> Workload:
+    """A block of fluid-saturated porous rock (the sandstone above, viscosity
+    eta_f and off-diagonal permeability kxz as given), free edges; with
+    ``layered`` the upper half has 20% porosity and a softer frame.
+    Ricker 30 Hz force source (both phases) in the middle, 6 receivers,
+    dt 1e-4."""
+    row_mat = np.zeros(nz, np.int32)
+    mats = [(ELASTIC, 0.0, 0.0, 0.0)]
+    poro = [list(POROUS_SANDSTONE)]
+    poro[0][10] = eta_f
+    poro[0][5] = kxz
+    if layered:
+        row_mat[nz // 2:] = 1
+        mats.append((ELASTIC, 0.0, 0.0, 0.0))
+        soft = list(poro[0])
+        soft[2], soft[9], soft[11] = 0.2, 6.0e9, 3.2e9
+        poro.append(soft)
+    mesh = structured_mesh(nx, nz, 0.0, width, 0.0, height, row_mat, mats, absorbing=(), free_surface=())
+    mesh.mat_poro = np.asarray(poro, np.float64)
+    mesh.mat_rho = np.asarray([(1 - p[2]) * p[0] + p[2] * p[1] for p in poro])
+    rx = np.linspace(0.3 * width, 0.7 * width, 6)
+    rz = np.full(6, 0.62 * height)
+    src = [RickerSource(0.5 * width, 0.45 * height, 30.0, 1e10)]
+    return Workload(f"poroelastic_{nx}x{nz}", mesh, src, rx, rz, 1e-4, nstep,
+                    description=f"2D isotropic poroelastic {nx}x{nz}, eta_f {eta_f}")
 
 
 def merge_interface_nodes(mesh: Mesh) -> Mesh:

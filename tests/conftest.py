@@ -34,7 +34,8 @@ def golden_case(name, nstep=None):
                   free_ispec=z["free_ispec"], free_type=z["free_type"],
                   coupled_pairs=np.zeros((0, 2), np.int32),
                   mat_aniso=z["mat_aniso"] if "mat_aniso" in z else None,
-                  mat_cosserat=z["mat_cosserat"] if "mat_cosserat" in z else None)
+                  mat_cosserat=z["mat_cosserat"] if "mat_cosserat" in z else None,
+                  mat_poro=z["mat_poro"] if "mat_poro" in z else None)
     if "adjacency" in z:
         mesh.extra["adjacency"] = z["adjacency"]
     srcs = []

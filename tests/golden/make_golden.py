@@ -39,6 +39,7 @@ FIXTURES = {
     "HomogeneousIsotropicCosseratDomain": ("BXX", "BXZ"),
     "HomogeneousIsotropicCosseratDomainHighFrequency": ("BXX", "BXZ"),
     "AcousticElasticNonconformingCoupledDomain": ("BXX", "BXZ"),
+    "PoroelasticCoupledDomainPSV": ("BXX", "BXZ"),
 }
 
 # time-function codes stored in the fixtures' source rows
@@ -76,6 +77,8 @@ def make(ref_root: str, name: str, comps) -> str:
         extra["mat_aniso"] = m.mat_aniso
     if getattr(m, "mat_cosserat", None) is not None:
         extra["mat_cosserat"] = m.mat_cosserat
+    if getattr(m, "mat_poro", None) is not None:
+        extra["mat_poro"] = m.mat_poro
     nc = runner.nonconforming_records(m)
     if len(nc):
         extra["adjacency"] = nc        # nonconforming records only

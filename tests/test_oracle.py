@@ -324,3 +324,42 @@ def test_oracle_nonconforming_records_checked(oracle_lib):
     w.mesh.adjacency = adj
     with pytest.raises(RuntimeError, match="intersection"):
         runner.run(workload_case(w), "f32")
+
+
+@pytest.mark.parametrize("kind,key", [("displacement", "traces"), ("velocity", "traces_semv"),
+                                      ("acceleration", "traces_sema")])
+def test_oracle_poroelastic_golden(oracle_lib, kind, key):
+    """The reference's poroelastic fixture (fluid-saturated sandstone, four
+    components: solid and fluid displacement): solid traces, the reference's
+    metric and tolerance 1e-3."""
+    import os
+    from conftest import GOLDEN
+    from oracle import runner
+    case, _, t0 = golden_case("PoroelasticCoupledDomainPSV")
+    traces = np.load(os.path.join(GOLDEN, "PoroelasticCoupledDomainPSV.npz"))[key]
+    case.seis_types = [kind]
+    r = runner.run(case, "f32", nthreads=8)
+    assert abs(r["t0"] - t0) < 1e-3
+    err = reference_metric(r["seis"][:, 0], traces)
+    assert np.all(np.isfinite(err))
+    assert err.max() < 1e-3, err
+    assert err.max() < 1e-4                               # observed: 1.5e-6 / 7.6e-6 / 5.8e-5
+
+
+def test_oracle_poroelastic_viscous_damping(oracle_lib):
+    """A viscous pore fluid (eta_f > 0) damps the wavefield: the run stays
+    bounded, differs from the inviscid one, and FP32 tracks FP64."""
+    from specfempp_b200 import meshgen
+    from oracle import runner
+    from conftest import workload_case
+    runs = {}
+    for eta in (0.0, 1e-3):
+        w = meshgen.poroelastic_model(nx=24, nz=24, eta_f=eta, kxz=2e-10, nstep=500, layered=True)
+        case = workload_case(w, types=("displacement", "pressure"))
+        a = runner.run(case, "f32", nthreads=8)["seis"]
+        b = runner.run(case, "f64", nthreads=8)["seis"]
+        assert np.all(np.isfinite(a)) and np.abs(b[:, 0]).max() > 0
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < 1e-4
+        runs[eta] = b
+    d = np.linalg.norm(runs[1e-3][:, 0] - runs[0.0][:, 0]) / np.linalg.norm(runs[0.0][:, 0])
+    assert 1e-3 < d < 0.5, d
