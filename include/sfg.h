@@ -102,6 +102,13 @@ typedef struct sfg_mesh2d_desc {
                                     reverse couple the two media through the edges'
                                     intersection (P-SV elastic media); strongly
                                     conforming records are implied by shared control nodes */
+  const double *mat_poro;        /* optional [numat][13] isotropic poroelastic constants
+                                    (rho_s, rho_f, phi, tortuosity, kxx, kxz, kzz, kappa_s,
+                                    kappa_f, kappa_fr, eta_f, mu_fr, Q_mu = 9999; NaN rows:
+                                    other materials); the elastic medium then has four
+                                    components (solid u_x, u_z, fluid w_x, w_z), P-SV, no
+                                    Stacey edges, no acoustic coupling; seismograms give
+                                    the solid motion and the pore pressure */
 } sfg_mesh2d_desc;
 
 typedef struct sfg_options {
@@ -149,7 +156,8 @@ typedef struct sfg_info {
   int kernels_per_step;
   int elements_per_block, kernel_variant; /* launch shape in use */
   int ncomp_elastic;             /* components of the elastic fields: 2 P-SV, 1 SH,
-                                    3 Cosserat (u_x, u_z, rotation) */
+                                    3 Cosserat (u_x, u_z, rotation), 4 poroelastic
+                                    (solid u_x, u_z, fluid w_x, w_z) */
 } sfg_info;
 
 /* ---- life cycle ---- */

@@ -174,6 +174,37 @@ void edge_normal(const JacD &J, int type, double &nx, double &nz) {
   }
 }
 
+// Per-point words of an isotropic poroelastic material
+// (include/medium/dim2/poroelastic/isotropic/material.hpp: Biot coefficients
+// evaluated as the reference does, FP32 values with double literals;
+// properties.hpp: rho_bar, the inverse permeability).
+struct PoroWords {
+  float H, mu, C, M, phi_tort, rhof_rhobar, exx, exz, ezz;
+};
+
+PoroWords poro_words(const double *v) {
+  if (std::abs(float(v[12]) - 9999.0) > 1e-6)
+    throw std::runtime_error("poroelastic attenuation (Q_mu != 9999) is not implemented");
+  const float rhos = float(v[0]), rhof = float(v[1]), phi = float(v[2]), tort = float(v[3]);
+  const float kxx = float(v[4]), kxz = float(v[5]), kzz = float(v[6]);
+  const float ks = float(v[7]), kf = float(v[8]), kfr = float(v[9]), eta = float(v[10]), mufr = float(v[11]);
+  const float D = float(double(ks) * (1.0 + double(phi) * (double(ks / kf) - 1.0)));
+  const float fac = float(1.0 / double(D - kfr));
+  PoroWords P;
+  P.H = float(double((ks - kfr) * (ks - kfr) * fac + kfr) + 4.0 / 3.0 * double(mufr));
+  P.C = ks * (ks - kfr) * fac;
+  P.M = ks * ks * fac;
+  P.mu = mufr;
+  P.phi_tort = phi / tort;
+  const float rb = ((1.0f - phi) * rhos) + (phi * rhof);
+  P.rhof_rhobar = rhof / rb;
+  const float det = kxx * kzz - kxz * kxz;
+  P.exx = eta * (kzz / det);
+  P.exz = eta * (-1.0f * kxz / det);
+  P.ezz = eta * (kxx / det);
+  return P;
+}
+
 // (xi, gamma) of local coordinate c along an edge: xi runs along bottom and
 // top, gamma along left and right.
 void edge_local(int t, double c, double &xi, double &ga) {
@@ -342,8 +373,19 @@ bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
         m.mat_medium[i] = 1;
         continue;
       }
+      if (indic == 3) {
+        // isotropic poroelastic: rho_s, rho_f, phi, tortuosity, kxx, kxz, kzz,
+        // kappa_s, kappa_f, kappa_fr, eta_f, mu_fr, Q_mu
+        // (read_material_properties.cpp:303-332)
+        if (m.mat_poro.empty()) m.mat_poro.assign(size_t(m.numat) * 13, std::nan(""));
+        for (int k = 0; k < 13; ++k) m.mat_poro[size_t(i) * 13 + k] = v[k];
+        m.mat_rho[i] = (1.0 - v[2]) * v[0] + v[2] * v[1];
+        m.mat_vp[i] = m.mat_vs[i] = 0.0;
+        m.mat_medium[i] = 1;
+        continue;
+      }
       if (indic != 1)
-        throw std::runtime_error("only isotropic, anisotropic and Cosserat elastic and acoustic materials are supported");
+        throw std::runtime_error("only isotropic, anisotropic, Cosserat and poroelastic elastic and acoustic materials are supported");
       m.mat_rho[i] = v[0]; m.mat_vp[i] = v[1]; m.mat_vs[i] = v[2];
       m.mat_medium[i] = (v[2] == 0.0) ? 0 : 1;
     }
@@ -432,6 +474,10 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
   a.el.aniso = false;
   for (int ce = 0; ce < a.el.nspec; ++ce) a.el.aniso |= aniso_of(a.el.elem_mesh[ce]) != nullptr;
   a.el.cosserat = a.el.ncomp == 3;
+  a.el.poro = a.el.ncomp == 4;
+  if (a.el.poro && (a.el.niface > 0 || a.el.aniso || !m.prho.empty()))
+    throw std::runtime_error("poroelastic media: material constants only, not coupled to acoustic media");
+  auto poro_of = [&](int e) { return &m.mat_poro[size_t(m.kmato[e]) * 13]; };
   if (a.el.cosserat && a.el.niface > 0)
     throw std::runtime_error("Cosserat media are not coupled to acoustic ones here");
   if (a.el.cosserat && (a.el.aniso || !m.prho.empty()))
@@ -446,13 +492,21 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
     D.prop1.resize(n);
     for (auto *v : {&D.prop2, &D.prop3, &D.prop4, &D.prop5}) v->assign(med == 1 && D.aniso ? n : 0, 0.0f);
     if (med == 1 && D.cosserat) for (auto *v : {&D.prop2, &D.prop3}) v->assign(n, 0.0f);
+    for (auto *v : {&D.prop6, &D.prop7, &D.prop8}) v->assign(med == 1 && D.poro ? n : 0, 0.0f);
+    if (med == 1 && D.poro)
+      for (auto *v : {&D.prop2, &D.prop3, &D.prop4, &D.prop5}) v->assign(n, 0.0f);
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
       for (int q = 0; q < NPTS; ++q) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
-        if (med == 1 && D.cosserat) {
+        if (med == 1 && D.poro) {
+          const PoroWords P = poro_words(poro_of(e));
+          D.prop0[pc] = P.H; D.prop1[pc] = P.mu; D.prop2[pc] = P.C; D.prop3[pc] = P.M;
+          D.prop4[pc] = P.phi_tort; D.prop5[pc] = P.rhof_rhobar;
+          D.prop6[pc] = P.exx; D.prop7[pc] = P.exz; D.prop8[pc] = P.ezz;
+        } else if (med == 1 && D.cosserat) {
           // lambda = kappa - 2/3 mu, mu, nu, mu_c + nu_c
           // (include/medium/dim2/elastic/isotropic_cosserat/properties.hpp, stress.hpp)
           const double *c = cos_of(e);
@@ -492,6 +546,7 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
         const size_t pm = size_t(e) * NPTS + q, pc = size_t(ce) * NPTS + q;
         double rho, vp, vs;
         model(e, pm, rho, vp, vs);
+        if (med == 1 && D.poro) throw std::runtime_error("Stacey edges on poroelastic media are not supported");
         if (med == 1 && D.cosserat) {
           // rho vp = sqrt((kappa + 4/3 mu) rho), rho vs = rho sqrt((mu + nu) / rho),
           // j sqrt((mu_c + nu_c) / j) (stacey.tpp:183-230)
@@ -526,7 +581,7 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
     MediumData &D = *Dp;
     D.stacey_pt.clear();
     D.stacey_c.clear();
-    if (D.nspec && !D.aniso && !D.cosserat) {
+    if (D.nspec && !D.aniso && !D.cosserat && !D.poro) {
       std::unordered_map<int, size_t> slot;
       for (int ce = 0; ce < D.nspec; ++ce) {
         if (D.bc_slot[ce] < 0) continue;
@@ -577,9 +632,17 @@ void assemble_model2d(const Mesh2D &m, Assembly2D &a) {
           const double fac = w[ix] * w[iz] * a.jac_d[pm];
           double rho, vp, vs;
           model(e, pm, rho, vp, vs);
-          double mc[3] = {0, 0, 0};
+          double mc[4] = {0, 0, 0, 0};
           if (med == 1) mc[0] = mc[1] = rho * fac;
           else mc[0] = (1.0 / double(D.prop1[pc])) * fac;
+          if (med == 1 && D.poro) {
+            // solid rho_bar - phi rho_f / tort, fluid (rho_f tort rho_bar -
+            // phi rho_f^2) / (phi rho_bar) (poroelastic/isotropic/mass_matrix.tpp)
+            const double *v = poro_of(e);
+            const double phi = v[2], rhof = v[1], tort = v[3], rb = (1.0 - phi) * v[0] + phi * rhof;
+            mc[0] = mc[1] = (rb - phi * rhof / tort) * fac;
+            mc[2] = mc[3] = ((rhof * tort * rb - phi * rhof * rhof) / (phi * rb)) * fac;
+          }
           // Cosserat: rho, rho, j (isotropic_cosserat/mass_matrix.tpp)
           if (med == 1 && D.cosserat) mc[2] = m.mat_cosserat[size_t(m.kmato[e]) * 8 + 4] * fac;
           if (D.bc_slot[ce] >= 0) {
@@ -866,6 +929,18 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
         throw std::runtime_error("Cosserat media: every elastic element Cosserat, P-SV only");
       if (any) D.ncomp = 3;
     }
+    if (med == 1 && !m.mat_poro.empty()) {
+      // a poroelastic medium: every elastic element poroelastic, four components
+      bool any = false, all = true;
+      for (int e = 0; e < nspec; ++e)
+        if (a.mesh_medium[e] == 1) {
+          const bool c = std::isfinite(m.mat_poro[size_t(m.kmato[e]) * 13]);
+          any |= c; all &= c;
+        }
+      if (any && (!all || m.elastic_wave == 1 || D.ncomp == 3))
+        throw std::runtime_error("poroelastic media: every elastic element poroelastic, P-SV only");
+      if (any) D.ncomp = 4;
+    }
     int ncol = 0;
     for (int e = 0; e < nspec; ++e)
       if (a.mesh_medium[e] == med) ncol = std::max(ncol, color[e] + 1);
@@ -1121,6 +1196,7 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
   a.src_medium.resize(a.nsrc); a.src_elem.resize(a.nsrc); a.src_shot.resize(a.nsrc);
   a.src_next.assign(a.nsrc, -1);
   a.src_arr.assign(size_t(a.nsrc) * 2 * NPTS, 0.0f);
+  a.src_arr2.assign(a.el.poro ? size_t(a.nsrc) * 2 * NPTS : 0, 0.0f);
   a.el_src_head.assign(a.el.nspec, -1);
   a.ac_src_head.assign(a.ac.nspec, -1);
   // start time per shot: t0 = min over the shot's sources of their start
@@ -1215,6 +1291,16 @@ void set_sources2d(const Mesh2D &m, Assembly2D &a, const std::vector<Source2D> &
           a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h / double(D.prop1[size_t(ce) * NPTS + q]));
         } else if (D.ncomp == 1) {
           a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h);
+        } else if (D.poro) {
+          // force on both phases, (sin, cos) each, the solid rows times
+          // (1 - phi / tort), the fluid rows times (1 - rho_f / rho_bar)
+          // (vector_source/force_source.cpp:53-60, poroelastic/isotropic/source.hpp)
+          const size_t pc = size_t(ce) * NPTS + q;
+          const double fs = 1.0 - double(D.prop4[pc]), ff = 1.0 - double(D.prop5[pc]);
+          a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h * std::sin(ang) * fs);
+          a.src_arr[(size_t(s) * 2 + 1) * NPTS + q] = float(h * std::cos(ang) * fs);
+          a.src_arr2[(size_t(s) * 2) * NPTS + q] = float(h * std::sin(ang) * ff);
+          a.src_arr2[(size_t(s) * 2 + 1) * NPTS + q] = float(h * std::cos(ang) * ff);
         } else {
           a.src_arr[(size_t(s) * 2) * NPTS + q] = float(h * std::sin(ang));
           a.src_arr[(size_t(s) * 2 + 1) * NPTS + q] = float(h * std::cos(ang));

@@ -31,6 +31,10 @@ struct Mesh2D {
   // optional isotropic Cosserat constants [numat][8] (rho, kappa, mu, nu, j,
   // lambda_c, mu_c, nu_c); rows of NaN for other materials
   std::vector<double> mat_cosserat;
+  // optional isotropic poroelastic constants [numat][13] (rho_s, rho_f, phi,
+  // tortuosity, kxx, kxz, kzz, kappa_s, kappa_f, kappa_fr, eta_f, mu_fr,
+  // Q_mu); rows of NaN for other materials
+  std::vector<double> mat_poro;
   std::vector<float> prho, pvp, pvs;  // optional [nspec][25]
   std::vector<int> abs_ispec, abs_type, free_ispec, free_type;
   int elastic_wave = 0;               // 0 P-SV, 1 SH
@@ -66,6 +70,12 @@ struct MediumData {
   // kappa - 2/3 mu, prop1 = mu, prop2 = nu, prop3 = mu_c + nu_c; bc_imp2 the
   // rotational Stacey impedance j sqrt((mu_c + nu_c) / j)
   bool cosserat = false;
+  // isotropic poroelastic medium (ncomp 4: solid u_x, u_z, fluid w_x, w_z):
+  // prop0 = H_Biot, prop1 = mu_G, prop2 = C_Biot, prop3 = M_Biot, prop4 =
+  // phi / tortuosity, prop5 = rho_f / rho_bar, prop6..prop8 = eta_f times the
+  // inverse permeability (xx, xz, zz)
+  bool poro = false;
+  std::vector<float> prop6, prop7, prop8;
   std::vector<float> minv;            // [nglob][ncomp]
   // Stacey / free-surface: slot per element (-1 none), compact [nslot][25]
   std::vector<int> bc_slot;
@@ -112,6 +122,7 @@ struct Assembly2D {
   int nsrc = 0;
   std::vector<int> src_medium, src_elem, src_shot, src_next, el_src_head, ac_src_head;
   std::vector<float> src_arr;         // [nsrc][2][25]
+  std::vector<float> src_arr2;        // poroelastic fluid rows [nsrc][2][25] (else empty)
   std::vector<float> stf;             // [nstep][nsrc]
   std::vector<double> shot_t0;        // per shot
   double t0 = 0;

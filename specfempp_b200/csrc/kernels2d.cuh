@@ -56,6 +56,7 @@ struct MedArgs {
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ jac, *__restrict__ prop0, *__restrict__ prop1;
   const float *__restrict__ prop2, *__restrict__ prop3, *__restrict__ prop4, *__restrict__ prop5;  // anisotropic
+  const float *__restrict__ prop6, *__restrict__ prop7, *__restrict__ prop8;  // poroelastic damping
   const int *__restrict__ bc_slot;
   const float *__restrict__ bc_w, *__restrict__ bc_nx, *__restrict__ bc_nz, *__restrict__ bc_j1,
       *__restrict__ bc_imp0, *__restrict__ bc_imp1, *__restrict__ bc_keep;
@@ -76,6 +77,7 @@ struct StiffArgs {
   MedArgs el, ac;
   const int *__restrict__ src_next;
   const float *__restrict__ src_arr;   // [nsrc][2][25]
+  const float *__restrict__ src_arr2;  // poroelastic fluid rows [nsrc][2][25] (else null)
   const float *__restrict__ stf;       // [nstep][nsrc]
   int nsrc, nstep;
   const int *__restrict__ step;        // device step counter
@@ -97,14 +99,21 @@ __device__ __forceinline__ void load_quad(const Quad &Q, float *shp, float *shpw
 // rotation row (mu_c + nu_c) grad(phi); after the divergence the rotation
 // gets -W (sxz - szx), W = w_x w_z |J| (compute_stiffness_interaction.tpp:
 // 216-229, cosserat_couple_stress.hpp), then Stacey with the rotational
-// impedance on phi (stacey.tpp:183-230)).
+// impedance on phi (stacey.tpp:183-230)), 4 = isotropic poroelastic (solid
+// u_x, u_z, fluid w_x, w_z; prop0..prop8 = H_Biot, mu_G, C_Biot, M_Biot,
+// phi / tort, rho_f / rho_bar, eta_f k^-1 (xx, xz, zz);
+// poroelastic/isotropic/stress.hpp: lambda_G = H - 2 mu_G, solid rows sigma -
+// phi/tort sigma_p, fluid rows sigma_p - rho_f/rho_bar sigma; after the
+// divergence the viscous damping of the fluid velocity, w_x w_z |J| eta_f k^-1
+// v_f, added to the solid rows times phi/tort and taken from the fluid rows
+// (damping.hpp, compute_stiffness_interaction.tpp:216-223)).
 // LOCAL: write the element's contribution to its own slot of A.r (summed per
 // point later by the update) instead of adding it into the accumulator.
 template <int E, int EK, bool LOCAL>
 __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs &A, int ebase,
                                               unsigned char *smem, float *shp, float *shpw,
                                               float *sw) {
-  constexpr int NC = EK == 1 ? 1 : (EK == 3 ? 3 : 2);
+  constexpr int NC = EK == 1 ? 1 : (EK == 3 ? 3 : (EK == 4 ? 4 : 2));
   float *su = reinterpret_cast<float *>(smem);                                // [E][NC][25]
   float *sF = reinterpret_cast<float *>(smem + sizeof(float) * NP * E * NC);  // [E][NC][2][25]
   const int tid = threadIdx.x;
@@ -118,7 +127,14 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
               gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
   const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
   float uu[NC], acc[NC];
-  if (NC == 3) {
+  if (NC == 4) {
+    const float4 t = act ? reinterpret_cast<const float4 *>(A.u)[g] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uu[0] = t.x; uu[1 % NC] = t.y; uu[2 % NC] = t.z; uu[3 % NC] = t.w;
+    if (!LOCAL) {
+      const float4 r = act ? reinterpret_cast<const float4 *>(A.accum)[g] : make_float4(0.f, 0.f, 0.f, 0.f);
+      acc[0] = r.x; acc[1 % NC] = r.y; acc[2 % NC] = r.z; acc[3 % NC] = r.w;
+    }
+  } else if (NC == 3) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
       uu[c] = act ? A.u[size_t(g) * 3 + c] : 0.f;
@@ -156,7 +172,24 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   // stress (P-SV: isotropic Hooke with lambda+2mu = c0; SH: sigma = mu grad u_y)
   float Sx[NC], Sz[NC];
   float csxz = 0.f, cszx = 0.f;   // Cosserat sigma_xz, sigma_zx
-  if (EK == 3) {
+  if (EK == 4) {
+    const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+    const float du10 = xix * dxi[1 % NC] + gax * dga[1 % NC], du11 = xiz * dxi[1 % NC] + gaz * dga[1 % NC];
+    const float du20 = xix * dxi[2 % NC] + gax * dga[2 % NC];
+    const float du31 = xiz * dxi[3 % NC] + gaz * dga[3 % NC];
+    const float C = __ldg(A.prop2 + p), M = __ldg(A.prop3 + p);
+    const float pt = __ldg(A.prop4 + p), rr = __ldg(A.prop5 + p);
+    const float lam = c0 - 2.0f * mu, l2m = lam + 2.0f * mu;   // c0 = H_Biot, mu = mu_G
+    const float dw = du20 + du31;
+    const float sxx = l2m * du00 + lam * du11 + C * dw;
+    const float szz = l2m * du11 + lam * du00 + C * dw;
+    const float sxz = mu * (du01 + du10);
+    const float sp = C * (du00 + du11) + M * dw;
+    Sx[0] = sxx - pt * sp; Sz[0] = sxz;
+    Sx[1 % NC] = sxz; Sz[1 % NC] = szz - pt * sp;
+    Sx[2 % NC] = sp - rr * sxx; Sz[2 % NC] = -1.0f * rr * sxz;
+    Sx[3 % NC] = -1.0f * rr * sxz; Sz[3 % NC] = sp - rr * szz;
+  } else if (EK == 3) {
     const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
     const float du10 = xix * dxi[1] + gax * dga[1], du11 = xiz * dxi[1] + gaz * dga[1];
     const float du20 = xix * dxi[NC - 1] + gax * dga[NC - 1], du21 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
@@ -216,6 +249,19 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     a[c] = -(sw[iz] * t1 + sw[ix] * t2);
   }
   if (EK == 3) a[NC - 1] -= (csxz - cszx) * (sw[ix] * sw[iz] * jac);   // couple stress
+  if (EK == 4) {
+    // viscous damping of the fluid motion; factor w_x w_z |J|
+    const float4 vv = reinterpret_cast<const float4 *>(A.v)[g];
+    const float fac = sw[ix] * sw[iz] * jac;
+    const float exx = __ldg(A.prop6 + p), exz = __ldg(A.prop7 + p), ezz = __ldg(A.prop8 + p);
+    const float viscx = fac * ((exx * vv.z) + (exz * vv.w));
+    const float viscz = fac * ((exz * vv.z) + (ezz * vv.w));
+    const float pt = __ldg(A.prop4 + p);
+    a[0] += pt * viscx;
+    a[1 % NC] += pt * viscz;
+    a[2 % NC] -= viscx;
+    a[3 % NC] -= viscz;
+  }
   if (bs >= 0) {
     const size_t k = size_t(bs) * NP + q;
     const float wq = A.bc_w[k];
@@ -249,15 +295,24 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
       const float f = step < S.nstep ? S.stf[size_t(step) * S.nsrc + s] : 0.f;
 #pragma unroll
       for (int c = 0; c < (NC < 2 ? NC : 2); ++c) a[c] += f * S.src_arr[(size_t(s) * 2 + c) * NP + q];
+      if (EK == 4) {
+        a[2 % NC] += f * S.src_arr2[(size_t(s) * 2) * NP + q];
+        a[3 % NC] += f * S.src_arr2[(size_t(s) * 2 + 1) * NP + q];
+      }
     }
   }
   if (LOCAL) {
     const int sl = __ldg(A.slot + p);
-    if (NC == 3) {
+    if (NC == 4) {
+      reinterpret_cast<float4 *>(A.r)[sl] = make_float4(a[0], a[1 % NC], a[2 % NC], a[3 % NC]);
+    } else if (NC == 3) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) A.r[size_t(sl) * 3 + c] = a[c];
     } else if (NC == 2) reinterpret_cast<float2 *>(A.r)[sl] = make_float2(a[0], a[NC - 1]);
     else A.r[sl] = a[0];
+  } else if (NC == 4) {
+    reinterpret_cast<float4 *>(A.accum)[g] = make_float4(acc[0] + a[0], acc[1 % NC] + a[1 % NC],
+                                                         acc[2 % NC] + a[2 % NC], acc[3 % NC] + a[3 % NC]);
   } else if (NC == 3) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) A.accum[size_t(g) * 3 + c] = acc[c] + a[c];
@@ -331,7 +386,7 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
 // colour, the following ac.nblocks blocks acoustic ones.
 template <int E, int EK, bool LOCAL>
 __global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
-  __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * (EK == 3 ? 9 : 6)];
+  __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * (EK == 4 ? 12 : EK == 3 ? 9 : 6)];
   __shared__ float shp[NP], shpw[NP], sw[NG];
   load_quad(S.quad, shp, shpw, sw, threadIdx.x);
   if (int(blockIdx.x) < S.el.nblocks)
@@ -796,6 +851,7 @@ struct RecArgs {
   const int *__restrict__ ibool;
   const float *__restrict__ xix, *__restrict__ xiz, *__restrict__ gax, *__restrict__ gaz,
       *__restrict__ prop0, *__restrict__ prop1;
+  const float *__restrict__ prop2, *__restrict__ prop3;   // poroelastic C_Biot, M_Biot
   const float *__restrict__ u, *__restrict__ v, *__restrict__ accum, *__restrict__ minv;
   UpdateArgs cpl;                      // coupling data of the medium (niface, cp_*, other)
   int ncomp, acoustic;
@@ -869,7 +925,24 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
             dga0 += hz * A.u[size_t(gc) * nc];
             dga1 += hz * A.u[size_t(gc) * nc + 1];
           }
-          if (on && ty == 3) {
+          if (on && ty == 3 && nc == 4) {
+            // pore pressure -(C div u_s + M div w) (poroelastic/isotropic/wavefield.hpp)
+            float dxi2 = 0.f, dxi3 = 0.f, dga2 = 0.f, dga3 = 0.f;
+            for (int l = 0; l < NG; ++l) {
+              const int gr = A.ibool[size_t(ce) * NP + iz * NG + l];
+              const int gc = A.ibool[size_t(ce) * NP + l * NG + ix];
+              const float hx = A.quad.hp[ix * NG + l], hz = A.quad.hp[iz * NG + l];
+              dxi2 += hx * A.u[size_t(gr) * 4 + 2];
+              dxi3 += hx * A.u[size_t(gr) * 4 + 3];
+              dga2 += hz * A.u[size_t(gc) * 4 + 2];
+              dga3 += hz * A.u[size_t(gc) * 4 + 3];
+            }
+            const float dux = A.xix[p] * dxi0 + A.gax[p] * dga0;
+            const float duz = A.xiz[p] * dxi1 + A.gaz[p] * dga1;
+            const float dwx = A.xix[p] * dxi2 + A.gax[p] * dga2;
+            const float dwz = A.xiz[p] * dxi3 + A.gaz[p] * dga3;
+            pr = -1.f * (A.prop2[p] * (dux + duz) + A.prop3[p] * (dwx + dwz));
+          } else if (on && ty == 3) {
             const float dux = A.xix[p] * dxi0 + A.gax[p] * dga0;
             const float duz = A.xiz[p] * dxi1 + A.gaz[p] * dga1;
             const float l2m = A.prop0[p], mu = A.prop1[p];

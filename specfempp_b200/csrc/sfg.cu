@@ -76,7 +76,8 @@ struct DevMedium {
   float *xix = nullptr, *xiz = nullptr, *gax = nullptr, *gaz = nullptr, *jac = nullptr,
         *prop0 = nullptr, *prop1 = nullptr;
   float *prop2 = nullptr, *prop3 = nullptr, *prop4 = nullptr, *prop5 = nullptr;  // anisotropic / Cosserat
-  bool aniso = false;
+  float *prop6 = nullptr, *prop7 = nullptr, *prop8 = nullptr;                      // poroelastic damping
+  bool aniso = false, poro = false;
   int *bc_slot = nullptr;
   float *bc_w = nullptr, *bc_nx = nullptr, *bc_nz = nullptr, *bc_j1 = nullptr,
         *bc_imp0 = nullptr, *bc_imp1 = nullptr, *bc_keep = nullptr, *bc_imp2 = nullptr;
@@ -168,6 +169,7 @@ struct sfg_handle {
   DevMedium el, ac;
   int *d_src_next = nullptr, *d_src_shot = nullptr;
   float *d_src_arr = nullptr, *d_stf = nullptr;
+  float *d_src_arr2 = nullptr;     // poroelastic fluid rows of the source arrays
   int *d_rec_elem = nullptr;
   float *d_rec_h = nullptr, *d_seis = nullptr;
   int *d_step = nullptr, *d_flag = nullptr;
@@ -271,6 +273,14 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
       throw std::runtime_error("Cosserat medium without its nu / mu_c + nu_c words");
     D.prop2 = padded(M.prop2); D.prop3 = padded(M.prop3);
   }
+  D.poro = M.poro;
+  if (M.poro) {                // C, M, phi / tort, rho_f / rho_bar, damping words
+    for (const auto *v : {&M.prop2, &M.prop3, &M.prop4, &M.prop5, &M.prop6, &M.prop7, &M.prop8})
+      if (v->size() != M.prop0.size()) throw std::runtime_error("poroelastic medium without its material words");
+    D.prop2 = padded(M.prop2); D.prop3 = padded(M.prop3); D.prop4 = padded(M.prop4);
+    D.prop5 = padded(M.prop5); D.prop6 = padded(M.prop6); D.prop7 = padded(M.prop7);
+    D.prop8 = padded(M.prop8);
+  }
   D.bc_slot = m.upload(M.bc_slot);
   D.bc_w = m.upload(M.bc_w); D.bc_nx = m.upload(M.bc_nx); D.bc_nz = m.upload(M.bc_nz);
   D.bc_j1 = m.upload(M.bc_j1); D.bc_imp0 = m.upload(M.bc_imp0); D.bc_imp1 = m.upload(M.bc_imp1);
@@ -302,6 +312,7 @@ sfg::dev::MedArgs med_args(const DevMedium &D) {
   A.xix = D.xix; A.xiz = D.xiz; A.gax = D.gax; A.gaz = D.gaz; A.jac = D.jac;
   A.prop0 = D.prop0; A.prop1 = D.prop1;
   A.prop2 = D.prop2; A.prop3 = D.prop3; A.prop4 = D.prop4; A.prop5 = D.prop5;
+  A.prop6 = D.prop6; A.prop7 = D.prop7; A.prop8 = D.prop8;
   A.bc_slot = D.bc_slot; A.bc_w = D.bc_w; A.bc_nx = D.bc_nx; A.bc_nz = D.bc_nz;
   A.bc_j1 = D.bc_j1; A.bc_imp0 = D.bc_imp0; A.bc_imp1 = D.bc_imp1; A.bc_keep = D.bc_keep;
   A.bc_imp2 = D.bc_imp2;
@@ -318,13 +329,16 @@ void launch_stiffness_E(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
   // the anisotropic and Cosserat stresses exist in the colour-pass and
   // owner-computes kernels
   if (EK >= 2 && (variant == 2 || variant == 4)) variant = variant == 2 ? 1 : 3;
-  if ((EK == 2 || EK == 3) && (!el.prop2 || !el.prop3))
+  if ((EK == 2 || EK == 3 || EK == 4) && (!el.prop2 || !el.prop3))
     throw std::runtime_error("element kernel: material words of the medium missing on the device");
+  if (EK == 4 && (!el.prop4 || !el.prop5 || !el.prop6 || !el.prop7 || !el.prop8 || !h->d_src_arr2))
+    throw std::runtime_error("element kernel: poroelastic words or source rows missing on the device");
   sfg::dev::StiffArgs S{};
   S.el = med_args(el);
   S.ac = med_args(ac);
   S.src_next = h->d_src_next;
   S.src_arr = h->d_src_arr;
+  S.src_arr2 = h->d_src_arr2;
   S.stf = h->d_stf;
   S.nsrc = h->asmb.nsrc;
   S.nstep = h->asmb.nstep;
@@ -406,6 +420,7 @@ void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
   if (el.ncomp == 1) launch_stiffness_E<E, 1>(h, el, ac, step, s, variant);
   else if (el.aniso) launch_stiffness_E<E, 2>(h, el, ac, step, s, variant);
   else if (el.ncomp == 3) launch_stiffness_E<E, 3>(h, el, ac, step, s, variant);
+  else if (el.ncomp == 4) launch_stiffness_E<E, 4>(h, el, ac, step, s, variant);
   else launch_stiffness_E<E, 0>(h, el, ac, step, s, variant);
 }
 
@@ -519,6 +534,7 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.ibool = D.ibool;
   R.xix = D.xix; R.xiz = D.xiz; R.gax = D.gax; R.gaz = D.gaz; R.prop0 = D.prop0;
   R.prop1 = D.prop1;
+  R.prop2 = D.prop2; R.prop3 = D.prop3;
   R.u = D.u; R.v = D.v; R.accum = D.accum; R.minv = D.minv;
   R.cpl = update_args(h, D, medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el, medium, true, false);
   R.ncomp = D.ncomp;
@@ -546,6 +562,7 @@ void launch_update(sfg_handle *h, int medium, bool predict, bool advance, cudaSt
     else if (D.S > 1) sfg::dev::k_update_batched_gather<<<grid_for(U.n), 256, 0, s>>>(U, D.S, D.ncomp);
     else if (D.ncomp == 2) sfg::dev::k_update_gather<2><<<grid_for(U.n / 2), 256, 0, s>>>(U);
     else if (D.ncomp == 3) sfg::dev::k_update_gather<3><<<grid_for(U.n / 3), 256, 0, s>>>(U);
+    else if (D.ncomp == 4) sfg::dev::k_update_gather<4><<<grid_for(U.n / 4), 256, 0, s>>>(U);
     else sfg::dev::k_update_gather<1><<<grid_for(U.n), 256, 0, s>>>(U);
     return;
   }
@@ -709,7 +726,7 @@ void autotune(sfg_handle *h) {
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
-  const bool special = h->el.aniso || h->el.ncomp == 3;   // anisotropic or Cosserat
+  const bool special = h->el.aniso || h->el.ncomp >= 3;   // anisotropic, Cosserat or poroelastic
   if (special && h->variant == 2) h->variant = 1;
   if (special && h->variant == 4) h->variant = 3;
   std::vector<std::pair<int, int>> cand;
@@ -787,7 +804,7 @@ void finish_create(sfg_handle *h) {
   h->asmb.nsb = h->opt.nstep_between_samples;
   sfg::assemble2d(h->mesh, h->opt.dt, h->asmb);
   if (h->asmb.nshots > 1 &&
-      (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0 || h->asmb.el.aniso || h->asmb.el.ncomp == 3))
+      (h->asmb.ac.nspec > 0 || h->asmb.el.nspec == 0 || h->asmb.el.aniso || h->asmb.el.ncomp >= 3))
     throw std::runtime_error("batched shots (nshots > 1) need a single isotropic elastic medium");
 }
 
@@ -862,6 +879,7 @@ int sfg_create2d(const sfg_mesh2d_desc *d, const sfg_options *opt, sfg_handle **
     m.mat_vs.assign(d->mat_vs, d->mat_vs + d->numat);
     if (d->mat_aniso) m.mat_aniso.assign(d->mat_aniso, d->mat_aniso + 6 * size_t(d->numat));
     if (d->mat_cosserat) m.mat_cosserat.assign(d->mat_cosserat, d->mat_cosserat + 8 * size_t(d->numat));
+    if (d->mat_poro) m.mat_poro.assign(d->mat_poro, d->mat_poro + 13 * size_t(d->numat));
     if (d->nadj < 0 || (d->nadj > 0 && !d->adjacency)) throw std::runtime_error("bad adjacency records");
     if (d->nadj > 0) m.adjacency.assign(d->adjacency, d->adjacency + 4 * size_t(d->nadj));
     const size_t np = size_t(d->nspec) * sfg::NPTS;
@@ -955,6 +973,7 @@ int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
       put(h->d_src_next, a.src_next);
       put(h->d_src_shot, a.src_shot);
       put(h->d_src_arr, a.src_arr);
+      put(h->d_src_arr2, a.src_arr2);
       put(h->d_stf, a.stf);
       h->adj.forward_done = false;
     }
@@ -1036,6 +1055,7 @@ int sfg_initialize(sfg_handle *h) {
     SFG_CUDA(cudaMemcpyToSymbol(sfg::dev::c_hpw, a.hpw, sizeof(a.hpw)));
     SFG_CUDA(cudaMemcpyToSymbol(sfg::dev::c_w, a.wgll, sizeof(a.wgll)));
     h->d_src_arr = h->mem.upload(a.src_arr);
+    h->d_src_arr2 = a.src_arr2.empty() ? nullptr : h->mem.upload(a.src_arr2);
     h->d_stf = h->mem.upload(a.stf);
     h->d_rec_elem = h->mem.upload(a.rec_elem);
     h->d_rec_h = h->mem.upload(a.rec_h);
@@ -1444,7 +1464,7 @@ int adjoint_checks(sfg_handle *h) {
   const sfg::Assembly2D &a = h->asmb;
   const bool one = (h->el.nspec > 0) != (h->ac.nspec > 0);
   const int want = h->el.nspec ? SFG_SEIS_DISPLACEMENT : SFG_SEIS_PRESSURE;
-  if (!one || h->el.aniso || h->el.ncomp == 3 || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
+  if (!one || h->el.aniso || h->el.ncomp >= 3 || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
     h->err = "the adjoint needs one medium (isotropic elastic P-SV or SH with displacement seismograms, "
              "or acoustic with pressure seismograms), one shot, seismograms sampled every step";
     return SFG_ERR_UNSUPPORTED;

@@ -40,7 +40,7 @@ class MeshDesc(C.Structure):
         ("nfree", C.c_int), ("free_ispec", _ip), ("free_type", _ip),
         ("elastic_wave", C.c_int),
         ("mat_aniso", _dp), ("mat_cosserat", _dp),
-        ("nadj", C.c_int), ("adjacency", _ip),
+        ("nadj", C.c_int), ("adjacency", _ip), ("mat_poro", _dp),
     ]
 
 
@@ -213,6 +213,10 @@ class Simulation2D:
         if aniso is not None:
             aniso = _arr(aniso, np.float64).reshape(len(m.mat_rho), 6)
             d.mat_aniso = self._k(np.ascontiguousarray(aniso)).ctypes.data_as(_dp)
+        poro = getattr(m, "mat_poro", None)
+        if poro is not None:
+            poro = _arr(poro, np.float64).reshape(len(m.mat_rho), 13)
+            d.mat_poro = self._k(np.ascontiguousarray(poro)).ctypes.data_as(_dp)
         adj = getattr(m, "adjacency", None)
         if adj is None:
             adj = getattr(m, "extra", {}).get("adjacency")

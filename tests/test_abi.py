@@ -179,3 +179,35 @@ def test_nonconforming_records_host_side(tmp_path, sfg_lib):
     w.mesh.adjacency = far
     with pytest.raises(sfg.SfgError, match="intersection"):
         sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
+
+
+def test_poroelastic_host_side(tmp_path, sfg_lib):
+    """A poroelastic mesh assembles with four elastic components, also from
+    a database.bin with material type 3; Stacey edges, an attenuating Q_mu
+    and a mix with isotropic elastic elements are refused (host assembly,
+    no GPU)."""
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.poroelastic_model(nx=6, nz=6, nstep=5, layered=True)
+    sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=5)
+    inf = sim.info()
+    assert inf.ncomp_elastic == 4 and inf.nspec_elastic == 36 and inf.nspec_acoustic == 0
+    p = str(tmp_path / "database.bin")
+    meshgen.write_database(w.mesh, p)
+    from oracle.database2d import read_database
+    m = read_database(p)
+    assert np.allclose(m.mat_poro, w.mesh.mat_poro)
+    assert sfg.Simulation2D(database=p, dt=w.dt, nstep=5).info().ncomp_elastic == 4
+    st = meshgen.poroelastic_model(nx=6, nz=6, nstep=5)
+    st.mesh.abs_ispec = np.array([0], np.int32)
+    st.mesh.abs_type = np.array([0], np.int32)
+    with pytest.raises(sfg.SfgError, match="Stacey"):
+        sfg.Simulation2D(st.mesh, dt=w.dt, nstep=5)
+    q = meshgen.poroelastic_model(nx=6, nz=6, nstep=5)
+    q.mesh.mat_poro[0, 12] = 50.0
+    with pytest.raises(sfg.SfgError, match="attenuation"):
+        sfg.Simulation2D(q.mesh, dt=w.dt, nstep=5)
+    mix = meshgen.poroelastic_model(nx=6, nz=6, nstep=5, layered=True)
+    mix.mesh.mat_poro[1] = np.nan
+    mix.mesh.mat_vp[1], mix.mesh.mat_vs[1], mix.mesh.mat_rho[1] = 3000.0, 1700.0, 2400.0
+    with pytest.raises(sfg.SfgError, match="poroelastic"):
+        sfg.Simulation2D(mix.mesh, dt=w.dt, nstep=5)
