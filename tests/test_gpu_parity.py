@@ -23,7 +23,7 @@ FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichlet
             "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain",
             "HomogeneousAcousticDomain", "HomogeneousAcousticDomainCompositeStaceyDirichletBC",
             "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap",
-            "HomogeneousIsotropicCosseratDomainNu0"]
+            "HomogeneousIsotropicCosseratDomainNu0", "AcousticElasticCoupledDomain"]
 
 
 def tolerance(kind, f32, f64):

@@ -19,7 +19,8 @@ FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichlet
             "AcousticElasticCoupledDomainVariant2", "HomogeneousElasticDomainMomentTensor",
             "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticAnisotropicDomain",
             "HomogeneousAcousticDomain", "HomogeneousAcousticDomainCompositeStaceyDirichletBC",
-            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap"]
+            "HomogeneousElasticDomainMomentTensorHeaviside", "HomogeneousElasticDomainWAdjacencyMap",
+            "AcousticElasticCoupledDomain"]
 
 
 @pytest.mark.parametrize("name", FIXTURES)
