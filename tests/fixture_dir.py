@@ -12,7 +12,9 @@ def write_fixture_dir(npz_path, out_dir, types=("displacement",)):
     mesh = meshgen.Mesh(nspec=int(z["nspec"]), npgeo=int(z["npgeo"]), ngnod=int(z["ngnod"]), coorg=z["coorg"],
                         knods=z["knods"], kmato=z["kmato"], mat_medium=z["mat_medium"], mat_rho=z["mat_rho"],
                         mat_vp=z["mat_vp"], mat_vs=z["mat_vs"], abs_ispec=z["abs_ispec"], abs_type=z["abs_type"],
-                        free_ispec=z["free_ispec"], free_type=z["free_type"])
+                        free_ispec=z["free_ispec"], free_type=z["free_type"],
+                        mat_poro=z["mat_poro"] if "mat_poro" in z else None,
+                        adjacency=z["adjacency"] if "adjacency" in z else None)
     os.makedirs(out_dir, exist_ok=True)
     meshgen.write_database(mesh, os.path.join(out_dir, "database.bin"))
     with open(os.path.join(out_dir, "STATIONS"), "w") as f:

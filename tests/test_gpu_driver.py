@@ -12,11 +12,13 @@ from fixture_dir import write_fixture_dir
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("name,comps", [("HomogeneousElasticDomain", ("BXX", "BXZ")),
-                                        ("HomogeneousElasticDomainMomentTensor", ("BXX", "BXZ")),
-                                        ("HomogeneousElasticDomainMomentTensorHeaviside", ("BXX", "BXZ")),
-                                        ("HomogeneousElasticIsotropicDomainSH", ("BXY",))])
-def test_driver_writes_reference_traces(sfg_lib, tmp_path, name, comps):
+@pytest.mark.parametrize("name,comps,tol", [("HomogeneousElasticDomain", ("BXX", "BXZ"), 1e-3),
+                                            ("HomogeneousElasticDomainMomentTensor", ("BXX", "BXZ"), 1e-3),
+                                            ("HomogeneousElasticDomainMomentTensorHeaviside", ("BXX", "BXZ"), 1e-3),
+                                            ("HomogeneousElasticIsotropicDomainSH", ("BXY",), 1e-3),
+                                            ("PoroelasticCoupledDomainPSV", ("BXX", "BXZ"), 1e-3),
+                                            ("AcousticElasticNonconformingCoupledDomain", ("BXX", "BXZ"), 1e-2)])
+def test_driver_writes_reference_traces(sfg_lib, tmp_path, name, comps, tol):
     from specfempp_b200 import specfem2d
     cfg, z = write_fixture_dir(os.path.join(GOLDEN, f"{name}.npz"), str(tmp_path))
     out = specfem2d.run_config(cfg, root=str(tmp_path))
@@ -30,7 +32,7 @@ def test_driver_writes_reference_traces(sfg_lib, tmp_path, name, comps):
             err += np.abs(v[:n] - ref[:n]).sum()
             norm += np.abs(ref[:n]).sum()
             assert abs(t[0] - float(z["trace_t0"])) < 1e-6
-        assert err / norm < 1e-3, (st, err / norm)
+        assert err / norm < tol, (st, err / norm)
 
 
 @pytest.mark.parametrize("library", ["ascii", "npy"])
