@@ -301,6 +301,52 @@ def bench_3d(args, world, barrier, max_over_ranks):
     return out
 
 
+def bench_media(args, world, barrier, max_over_ranks):
+    """Throughput of the other media on fixed synthetic meshes (seeded, no
+    dataset): a 400 x 400 porous block over 10 x 10 km (four components,
+    viscous pore fluid, layered), and an acoustic-elastic model with a nonconforming interface
+    (400 elastic columns under 600 water columns, 200 + 150 rows).  10
+    warm-up steps, then K steps after a 256 MiB L2 flush each and K steps
+    back to back (CUDA events, graph replay).  Algorithmic bytes per
+    poroelastic point-step: read u, v, a and M^-1 (4 components) and write
+    u, v, a = 112 B per global point, plus 60 B per element-local point
+    (ibool, Jacobian, 9 material words) times 25 nspec / nglob."""
+    from specfempp_b200 import meshgen, sfg
+    steps = args.media_steps
+    peak, _ = peaks()
+    out = {}
+    cases = [("poroelastic_400x400", lambda: meshgen.poroelastic_model(
+                  nx=400, nz=400, width=10000.0, height=10000.0, eta_f=1e-3, kxz=2e-10,
+                  nstep=2 * steps + 20, layered=True), 112.0, 60.0),
+             ("nonconforming_coupled_400_600", lambda: meshgen.nonconforming_coupled(
+                  nx_el=400, nx_ac=600, nz_el=200, nz_ac=150, width=40000.0, h_el=20000.0, h_ac=15000.0,
+                  nstep=2 * steps + 20), None, None)]
+    for name, make, glob_b, loc_b in cases:
+        w = make()
+        sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep)
+        sim.set_sources(w.sources)
+        sim.set_receivers(w.rec_x, w.rec_z, 0.0, ("displacement",))
+        sim.initialize()
+        inf = sim.info()
+        sim.run(10)
+        barrier()
+        ms_fl = max_over_ranks(sim.run_timed_flushed(steps))
+        ms_b2b = max_over_ranks(sim.run_timed(steps))
+        nglob = inf.nglob_elastic + inf.nglob_acoustic
+        rec = {"nglob": nglob, "nspec": inf.nspec, "ncomp_elastic": inf.ncomp_elastic,
+               "kernel_variant": inf.kernel_variant, "elements_per_block": inf.elements_per_block,
+               "steps": steps, "ms_per_step_flushed": ms_fl / steps, "ms_per_step_back_to_back": ms_b2b / steps,
+               "gll_pt_updates_per_s": world * nglob * steps / (ms_fl / 1e3),
+               "finite": bool(sim.check_finite())}
+        if glob_b is not None:
+            alg = glob_b + loc_b * 25.0 * inf.nspec / nglob
+            rec["algorithmic_bytes_per_point"] = alg
+            rec["step_frac_of_hbm"] = alg * nglob / (ms_fl / steps / 1e3) / 1e9 / peak
+        out[name] = rec
+        sim.close()
+    return out
+
+
 def run_reference(args, rank):
     if rank != 0:
         return
@@ -347,6 +393,8 @@ def main():
     ap.add_argument("--mesh3d", default="128x128x64")
     ap.add_argument("--steps3d", type=int, default=50)
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-media", action="store_true")
+    ap.add_argument("--media-steps", type=int, default=200)
     ap.add_argument("--adjoint-mesh", default="500x250")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-fd", type=int, default=0,
@@ -470,6 +518,10 @@ def main():
     if not args.no_3d:
         b3d = bench_3d(args, world, barrier, max_over_ranks)
 
+    media = None
+    if not args.no_media:
+        media = bench_media(args, world, barrier, max_over_ranks)
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -501,6 +553,7 @@ def main():
         "batched": batched,
         "adjoint": adj,
         "elastic3d": b3d,
+        "media": media,
     }
     print(json.dumps(line), flush=True)
 
