@@ -122,6 +122,17 @@ def make_workload(name, nstep):
     raise SystemExit(f"unknown workload {name}")
 
 
+def workload_config(name, w, nglob):
+    """The config dict of both arms (GPU and --impl reference): the workload
+    only, so that the two lines describe the same run."""
+    mesh = w.mesh
+    med = np.asarray(mesh.mat_medium)[np.asarray(mesh.kmato)]
+    nel = int((med == 1).sum())
+    return {"workload": name, "nglob": int(nglob), "nspec": int(mesh.nspec), "nspec_elastic": nel,
+            "nspec_acoustic": int(mesh.nspec) - nel, "dt": w.dt, "ngll": 5, "shots": 1,
+            "l2": "flushed (256 MiB write) before every timed step"}
+
+
 def cpu_oracle_throughput(w, steps, threads):
     from oracle import runner
     case = runner.Case2D(mesh=w.mesh, sources=w.sources, rec_x=w.rec_x, rec_z=w.rec_z, dt=w.dt,
@@ -354,17 +365,18 @@ def run_reference(args, rank):
     w = make_workload(args.workload, max(args.steps, 1))
     # each bench step is one time step of the full model; the timed sample is
     # capped so that warm-up plus timed steps stay near a minute on the host
-    steps = max(3, min(args.steps, 400))
-    warm = max(1, min(args.warmup, 3))
+    steps = max(3, min(args.steps, 3000))
+    warm = args.warmup
     cpu_oracle_throughput(w, warm, threads)
     v, secs = cpu_oracle_throughput(w, steps, threads)
     ms = secs * 1000.0 / steps
     nglob = int(round(v * secs / steps))
+    cfg = workload_config(args.workload, w, nglob)
+    cfg["parallelism"] = "replicas" if args.gpus > 1 else "single GPU"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": steps, "warmup": warm, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": args.workload, "nglob": nglob, "steps_requested": args.steps,
-                       "device": "host CPU only (rank 0)"},
+            "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{steps} time steps of {args.workload} (full mesh), "
                                        f"FP32 C++ restatement of the reference, OpenMP atomics"},
@@ -502,7 +514,7 @@ def main():
                 "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": stiff_bytes, "launch_ms": stiff_ms,
-                "update_launch_ms": upd_ms, "acoustic_stiffness_ms": ac_ms,
+                "update_launch_ms": upd_ms, "acoustic_update_launch_ms": ac_ms,
                 "step_algorithmic_bytes": step_bytes,
                 "step_frac_of_peak": step_bytes / (ms / args.steps / 1e3) / 1e9 / peak}
 
@@ -534,16 +546,16 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    cfg = workload_config(args.workload, w, nglob)
+    cfg["parallelism"] = "replicas" if world > 1 else "single GPU"
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": args.workload, "nglob": nglob, "nspec": inf.nspec,
-                   "nspec_elastic": inf.nspec_elastic, "nspec_acoustic": inf.nspec_acoustic,
-                   "dt": w.dt, "ngll": 5, "shots": 1, "l2": "flushed (256 MiB write) before every timed step",
-                   "parallelism": "replicas" if world > 1 else "single GPU",
-                   "value_back_to_back": world * nglob * args.steps / (ms_b2b / 1000.0),
-                   "ms_per_step_back_to_back": ms_b2b / args.steps, "finite": bool(finite)},
+        "config": cfg,
+        "back_to_back": {"value": world * nglob * args.steps / (ms_b2b / 1000.0),
+                         "ms_per_step": ms_b2b / args.steps, "l2": "not flushed (graph replay)"},
+        "finite": bool(finite),
         "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": 4 * nsrc,
                 "d2h_bytes_per_step": 4 * inf.nshots * inf.ntypes * inf.nrec * 2},
         "roofline": roofline,

@@ -258,19 +258,25 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
  * device memory itself (as the reference's Kokkos runtime does), or a time
  * loop that runs after the device memory has been sized and frozen.  The
  * handle must be initialised (that is where its read-only mesh arrays were
- * uploaded) and hold a single elastic medium.  u, v, a are the displacement,
+ * uploaded) and hold a single isotropic elastic medium (P-SV or SH; other
+ * media are refused with SFG_ERR_UNSUPPORTED).  u, v, a are the displacement,
  * velocity and acceleration in the handle's elastic point numbering
- * ([nglob_elastic][ncomp] floats on the handle's device), in the end-of-step
+ * ([nglob_elastic][ncomp] floats on the handle's device, each starting on a
+ * 16-byte boundary, else SFG_ERR_ARG before any launch), in the end-of-step
  * state that sfg_step leaves; the call applies the predictor, the element
  * kernel and the corrector exactly as sfg_step does and writes the new state
- * back into u, v, a, using source-time values of step istep.  The element
+ * back into u, v, a, using source-time values of step istep.  It records no
+ * seismogram sample (sfg_step does).  The work runs on the handle's stream,
+ * which does not wait for other streams: finish every write to u, v, a (for
+ * example with a device or stream synchronize) before the call.  The element
  * kernel's accumulator lives in a fixed array inside the library, limited to
  * 4,194,304 point values (2,097,152 two-component points); larger models are
  * rejected with SFG_ERR_ARG.  All calls share that array (it is cleared at
  * the start of every call), so calls that overlap on the GPU race.  The first
  * call on a device looks up the array's device address; make that first call
  * before any stream capture.  The handle's own fields and step count are not
- * touched; the call returns after the step has finished on the GPU. */
+ * touched; the call returns after the step has finished on the GPU, with
+ * SFG_ERR_NONFINITE when the new displacement holds a NaN or Inf. */
 int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a);
 
 #ifdef __cplusplus

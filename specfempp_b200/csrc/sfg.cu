@@ -1376,11 +1376,17 @@ int sfg_check_finite(sfg_handle *h) {
 int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
-    if (h->ac.nspec != 0 || h->el.nspec == 0 || h->el.S != 1) {
-      h->err = "sfg_step_noalloc advances single-shot, single-medium elastic models only";
+    if (h->ac.nspec != 0 || h->el.nspec == 0 || h->el.S != 1 || h->el.ncomp > 2 || h->el.aniso) {
+      h->err = "sfg_step_noalloc advances single-shot, single-medium isotropic elastic (P-SV or SH) models only";
       return int(SFG_ERR_UNSUPPORTED);
     }
     if (!u || !v || !a || istep < 0) { h->err = "null field pointer or negative step"; return int(SFG_ERR_ARG); }
+    // the kernels read and write the fields as float2 / float4 vectors
+    for (const float *p : {u, v, a})
+      if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
+        h->err = "sfg_step_noalloc: u, v and a must start on a 16-byte boundary";
+        return int(SFG_ERR_ARG);
+      }
     const size_t n = size_t(h->el.nglob) * h->el.ncomp;
     if (n > NOALLOC_MAX_VALUES) {
       h->err = "sfg_step_noalloc: the model has " + std::to_string(n) +
@@ -1413,6 +1419,13 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
     sfg::dev::k_update<<<grid_for(U.n / 4), 256, 0, s>>>(U);
     SFG_CUDA(cudaGetLastError());
     SFG_CUDA(cudaStreamSynchronize(s));
+    // the update's non-finite flag lives in the fixed words: read it back
+    int flag = 0;
+    SFG_CUDA(cudaMemcpy(&flag, nd.words + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) {
+      h->err = "sfg_step_noalloc: the displacement became NaN or Inf";
+      return int(SFG_ERR_NONFINITE);
+    }
     return int(SFG_OK);
   });
 }

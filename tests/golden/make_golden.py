@@ -178,7 +178,9 @@ def make3d(ref_root: str) -> str:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    if len(sys.argv) < 2:
+        sys.exit("usage: make_golden.py REFERENCE_ROOT [FIXTURE ...]  (the SPECFEM++ checkout to read)")
+    root = sys.argv[1]
     names = sys.argv[2:] or list(FIXTURES)
     for name in names:
         print(make(root, name, FIXTURES[name]), os.path.getsize(os.path.join(HERE, f"{name}.npz")))

@@ -77,3 +77,44 @@ def test_noalloc_refuses_models_above_the_scratch(sfg_lib):
                                   C.c_void_p(buf[1].data_ptr()), C.c_void_p(buf[2].data_ptr()))
     assert rc == -1
     assert b"fixed scratch" in sfg_lib.sfg_last_error(sim.h)
+
+
+def test_noalloc_reports_a_nonfinite_step(sfg_lib):
+    import torch
+    from specfempp_b200 import meshgen
+
+    w = meshgen.elastic_psv_80x60(nstep=8)
+    sim = _handle(w)
+    n = sim.info().nglob_elastic * 2
+    buf = torch.zeros(3, n, device="cuda")
+    buf[0, 7] = float("nan")                  # a blown-up displacement
+    torch.cuda.synchronize()
+    rc = sfg_lib.sfg_step_noalloc(sim.h, 0, C.c_void_p(buf[0].data_ptr()),
+                                  C.c_void_p(buf[1].data_ptr()), C.c_void_p(buf[2].data_ptr()))
+    assert rc == -6, sfg_lib.sfg_last_error(sim.h)
+    assert b"NaN" in sfg_lib.sfg_last_error(sim.h)
+    # a clean state steps again with SFG_OK: the flag is cleared per call
+    buf.zero_()
+    torch.cuda.synchronize()
+    rc = sfg_lib.sfg_step_noalloc(sim.h, 1, C.c_void_p(buf[0].data_ptr()),
+                                  C.c_void_p(buf[1].data_ptr()), C.c_void_p(buf[2].data_ptr()))
+    assert rc == 0, sfg_lib.sfg_last_error(sim.h)
+
+
+def test_noalloc_refuses_misaligned_fields_before_any_launch(sfg_lib):
+    import torch
+    from specfempp_b200 import meshgen
+
+    w = meshgen.elastic_psv_80x60(nstep=8)
+    sim = _handle(w)
+    n = sim.info().nglob_elastic * 2
+    buf = torch.zeros(3 * n + 8, device="cuda")
+    u = buf[1:1 + n]                          # 4 bytes past a 16-byte boundary
+    v = buf[n + 4:2 * n + 4]
+    a = buf[2 * n + 4:3 * n + 4]
+    rc = sfg_lib.sfg_step_noalloc(sim.h, 0, C.c_void_p(u.data_ptr()), C.c_void_p(v.data_ptr()),
+                                  C.c_void_p(a.data_ptr()))
+    assert rc == -1
+    assert b"16-byte" in sfg_lib.sfg_last_error(sim.h)
+    torch.cuda.synchronize()
+    assert torch.count_nonzero(buf).item() == 0   # nothing ran
