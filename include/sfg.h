@@ -123,8 +123,12 @@ typedef struct sfg_options {
                                     per chunk), 2 colour passes with a persistent
                                     prefetching kernel, 3 owner-computes (one element
                                     launch, per-point sum in colour order), 4 owner-computes
-                                    with the element arrays staged by bulk copies; all give
-                                    the same bits (0 = chosen by the autotuner) */
+                                    with the element arrays staged by bulk copies, 5 fused
+                                    tile kernel (element forces, assembly in shared memory
+                                    and the point update of tile-interior points in one
+                                    launch; one shot, isotropic P-SV / SH / acoustic media,
+                                    others fall back to 3); all give the same bits
+                                    (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
   int has_start_time;            /* 1: the run starts at start_time (the configuration's
                                     time-scheme t0) and sources keep their own tshift;
@@ -206,7 +210,10 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
 /* Average device time of one launch of a named kernel family, timed alone with
  * CUDA events: which = 0 element (stiffness) launches of one step, all colours
  * and both media; 1 elastic point update; 2 acoustic point update;
- * 3 receiver kernels.  Leaves the fields mid-step (sfg_reset_fields after). */
+ * 3 receiver kernels.  With the fused tile kernel (variant 5): 0 the tile
+ * kernel (elements and tile-interior points of both media), 1 the boundary
+ * points of both media, 2 nothing (0 ms), 3 receivers.  Leaves the fields
+ * mid-step (sfg_reset_fields after). */
 int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms_per_launch);
 
 /* ---- results ---- */

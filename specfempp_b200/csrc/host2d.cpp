@@ -307,6 +307,57 @@ void nonconforming_weights(const Mesh2D &m, const double z[NGLL], const double w
   }
 }
 
+// Spread the low 32 bits of x to the even bits of a 64-bit word.
+uint64_t spread_bits(uint64_t x) {
+  x &= 0xffffffffull;
+  x = (x | (x << 16)) & 0x0000ffff0000ffffull;
+  x = (x | (x << 8)) & 0x00ff00ff00ff00ffull;
+  x = (x | (x << 4)) & 0x0f0f0f0f0f0f0f0full;
+  x = (x | (x << 2)) & 0x3333333333333333ull;
+  x = (x | (x << 1)) & 0x5555555555555555ull;
+  return x;
+}
+
+// Tiles of TILE_E compute elements of one medium: the elements sorted by the
+// Morton code of their centre on a grid whose cell is the median element
+// extent (on a structured mesh the cell indices are the element's column and
+// row, and every aligned run of 16 codes is a 4 x 4 block of elements), then
+// cut into consecutive runs.  Returns [ntiles][TILE_E] compute elements, -1
+// past the last element.
+std::vector<int> make_tiles(const Assembly2D &a, const std::vector<int> &elem_mesh) {
+  const int n = int(elem_mesh.size());
+  if (n == 0) return {};
+  std::vector<double> cx(n), cz(n), ext(n);
+  for (int ce = 0; ce < n; ++ce) {
+    const size_t p = size_t(elem_mesh[ce]) * NPTS;
+    double x0 = 1e300, x1 = -1e300, z0 = 1e300, z1 = -1e300;
+    for (int q = 0; q < NPTS; ++q) {
+      x0 = std::min(x0, a.gx[p + q]); x1 = std::max(x1, a.gx[p + q]);
+      z0 = std::min(z0, a.gz[p + q]); z1 = std::max(z1, a.gz[p + q]);
+    }
+    cx[ce] = 0.25 * (a.gx[p] + a.gx[p + 4] + a.gx[p + 20] + a.gx[p + 24]);
+    cz[ce] = 0.25 * (a.gz[p] + a.gz[p + 4] + a.gz[p + 20] + a.gz[p + 24]);
+    ext[ce] = std::max(x1 - x0, z1 - z0);
+  }
+  std::vector<double> e2 = ext;
+  std::nth_element(e2.begin(), e2.begin() + n / 2, e2.end());
+  const double cell = e2[n / 2] > 0 ? e2[n / 2] : 1.0;
+  const double xmin = *std::min_element(cx.begin(), cx.end());
+  const double zmin = *std::min_element(cz.begin(), cz.end());
+  std::vector<std::pair<uint64_t, int>> key(n);
+  for (int ce = 0; ce < n; ++ce) {
+    const double fx = std::floor((cx[ce] - xmin) / cell + 0.5), fz = std::floor((cz[ce] - zmin) / cell + 0.5);
+    const uint64_t ix = uint64_t(std::min(std::max(fx, 0.0), 4.0e9));
+    const uint64_t iz = uint64_t(std::min(std::max(fz, 0.0), 4.0e9));
+    key[ce] = {spread_bits(ix) | (spread_bits(iz) << 1), ce};
+  }
+  std::sort(key.begin(), key.end());
+  const int ntiles = (n + TILE_E - 1) / TILE_E;
+  std::vector<int> tiles(size_t(ntiles) * TILE_E, -1);
+  for (int i = 0; i < n; ++i) tiles[i] = key[i].second;
+  return tiles;
+}
+
 }  // namespace
 
 bool read_database2d(const std::string &path, Mesh2D &m, std::string &err) {
@@ -954,27 +1005,99 @@ void assemble2d(const Mesh2D &m, double dt, Assembly2D &a) {
       D.color_start.push_back(int(D.elem_mesh.size()));
     }
     D.nspec = int(D.elem_mesh.size());
-    // per-medium point numbering: coupled-interface points first, then the
-    // others, each by first touch in compute order (locality of the gathers)
+    D.elem_color.assign(D.nspec, 0);
+    for (int c = 0; c < ncol; ++c)
+      for (int ce = D.color_start[c]; ce < D.color_start[c + 1]; ++ce) D.elem_color[ce] = c;
+    // tiles of the fused tile kernel
+    D.tile_elem = make_tiles(a, D.elem_mesh);
+    D.ntiles = int(D.tile_elem.size()) / TILE_E;
+    // per-medium point numbering (every assembly variant sums a point's
+    // contributions in colour order, so the numbering changes no result; it
+    // sets the locality of the gathers and the tiles' contiguous ranges):
+    // coupled-interface points first (by first touch in compute order), then
+    // the interior points of each tile in tile order (first touch inside the
+    // tile), then the points several tiles share (first touch in tile order)
     std::vector<int> &g2m = med == 1 ? a.glob_to_el : a.glob_to_ac;
     g2m.assign(a.nglob, -1);
     D.ibool.resize(size_t(D.nspec) * NPTS);
-    for (int pass = 0; pass < 2; ++pass)
-      for (int ce = 0; ce < D.nspec; ++ce) {
-        const int e = D.elem_mesh[ce];
-        for (int q = 0; q < NPTS; ++q) {
-          const int g = gid[size_t(e) * NPTS + q];
-          const bool iface = is_iface[med][g] || (nonconforming && ncw[med].count(g));
-          if (g2m[g] >= 0 || (pass == 0) != iface) continue;
-          g2m[g] = D.nglob++;
-          D.glob_of_point.push_back(g);
-        }
-        if (pass == 0 && ce == D.nspec - 1) D.niface = D.nglob;
+    for (int ce = 0; ce < D.nspec; ++ce) {
+      const int e = D.elem_mesh[ce];
+      for (int q = 0; q < NPTS; ++q) {
+        const int g = gid[size_t(e) * NPTS + q];
+        const bool iface = is_iface[med][g] || (nonconforming && ncw[med].count(g));
+        if (g2m[g] >= 0 || !iface) continue;
+        g2m[g] = D.nglob++;
+        D.glob_of_point.push_back(g);
       }
-    if (D.nspec == 0) D.niface = 0;
+    }
+    D.niface = D.nglob;
+    {
+      std::vector<int> tcount(a.nglob, 0), tlast(a.nglob, -1);
+      for (int t = 0; t < D.ntiles; ++t)
+        for (int s = 0; s < TILE_E; ++s) {
+          const int ce = D.tile_elem[size_t(t) * TILE_E + s];
+          if (ce < 0) continue;
+          for (int q = 0; q < NPTS; ++q) {
+            const int g = gid[size_t(D.elem_mesh[ce]) * NPTS + q];
+            if (tlast[g] != t) { tlast[g] = t; ++tcount[g]; }
+          }
+        }
+      D.tile_ibeg.assign(D.ntiles, 0);
+      D.tile_nint.assign(D.ntiles, 0);
+      for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) D.sh0 = D.nglob;
+        for (int t = 0; t < D.ntiles; ++t) {
+          if (pass == 0) D.tile_ibeg[t] = D.nglob;
+          for (int s = 0; s < TILE_E; ++s) {
+            const int ce = D.tile_elem[size_t(t) * TILE_E + s];
+            if (ce < 0) continue;
+            for (int q = 0; q < NPTS; ++q) {
+              const int g = gid[size_t(D.elem_mesh[ce]) * NPTS + q];
+              if (g2m[g] >= 0 || (pass == 0 && tcount[g] != 1)) continue;
+              g2m[g] = D.nglob++;
+              D.glob_of_point.push_back(g);
+            }
+          }
+          if (pass == 0) D.tile_nint[t] = D.nglob - D.tile_ibeg[t];
+        }
+      }
+    }
+    if (D.nspec == 0) D.niface = D.sh0 = 0;
     for (int ce = 0; ce < D.nspec; ++ce) {
       const int e = D.elem_mesh[ce];
       for (int q = 0; q < NPTS; ++q) D.ibool[size_t(ce) * NPTS + q] = g2m[gid[size_t(e) * NPTS + q]];
+    }
+    // tile-local indices: interior point k = point - tile_ibeg; the tile's
+    // shared points follow, in first-touch order
+    D.tile_lidx.assign(size_t(D.ntiles) * TILE_E * NPTS, 0);
+    D.tile_nsh.assign(D.ntiles, 0);
+    D.tile_sh_off.assign(D.ntiles, 0);
+    D.tile_sh.clear();
+    for (int t = 0; t < D.ntiles; ++t) {
+      const int ib = D.tile_ibeg[t], ni = D.tile_nint[t];
+      std::vector<int> shl;
+      std::unordered_map<int, int> pos;
+      for (int s = 0; s < TILE_E; ++s) {
+        const int ce = D.tile_elem[size_t(t) * TILE_E + s];
+        if (ce < 0) continue;
+        for (int q = 0; q < NPTS; ++q) {
+          const int pt = D.ibool[size_t(ce) * NPTS + q];
+          int k;
+          if (pt >= ib && pt < ib + ni) {
+            k = pt - ib;
+          } else {
+            auto it = pos.find(pt);
+            if (it == pos.end()) { it = pos.emplace(pt, int(shl.size())).first; shl.push_back(pt); }
+            k = ni + it->second;
+          }
+          if (k > 65535) throw std::runtime_error("tile with more than 65536 local points");
+          D.tile_lidx[(size_t(t) * TILE_E + s) * NPTS + q] = uint16_t(k);
+        }
+      }
+      D.tile_sh_off[t] = int(D.tile_sh.size());
+      D.tile_nsh[t] = int(shl.size());
+      D.tile_sh.insert(D.tile_sh.end(), shl.begin(), shl.end());
+      while (D.tile_sh.size() % 4) D.tile_sh.push_back(0);
     }
     D.inv_start.assign(D.nglob + 1, 0);
     for (int v : D.ibool) ++D.inv_start[v + 1];

@@ -98,7 +98,23 @@ struct MediumData {
   // assembled Stacey matrices (elastic P-SV): point ids and (Cxx, Cxz, Czz)
   std::vector<int> stacey_pt;
   std::vector<float> stacey_c;
+  // Tiles of the fused tile kernel: the medium's compute elements in groups of
+  // TILE_E that lie close together (Morton order of the element centres).  A
+  // point that only one tile touches and that is on no coupled edge is
+  // interior to that tile; the point numbering gives every tile's interior
+  // points one contiguous range [tile_ibeg, tile_ibeg + tile_nint).  The
+  // points that several tiles touch are numbered after all interior ranges,
+  // from sh0 on; with the interface points [0, niface) they are the boundary
+  // points, finished outside the tiles.
+  int ntiles = 0, sh0 = 0;
+  std::vector<int> elem_color;        // [nspec] colour of each compute element
+  std::vector<int> tile_elem;         // [ntiles][TILE_E] compute element, -1 past the tile's end
+  std::vector<int> tile_ibeg, tile_nint, tile_nsh, tile_sh_off;
+  std::vector<int> tile_sh;           // each tile's shared points (lists padded to 4 entries)
+  std::vector<uint16_t> tile_lidx;    // [ntiles][TILE_E][25] tile-local point index
 };
+
+constexpr int TILE_E = 16;          // elements per tile of the fused tile kernel
 
 struct Assembly2D {
   int nspec = 0, nglob = 0, nshots = 1, elastic_wave = 0;

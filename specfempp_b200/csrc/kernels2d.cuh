@@ -44,6 +44,14 @@ namespace dev {
 constexpr int NG = 5;
 constexpr int NP = 25;
 
+// Paired FP32 fused multiply-add (sm_100 FFMA2): each lane rounds exactly as
+// the scalar fmaf, so 5-term contractions (explicit fmaf in every kernel)
+// can run two at a time with unchanged results.  Products and sums stay
+// scalar: paired multiplies feeding paired adds are fused into FFMA2 by the
+// code generator even with explicit rounding, which would change rounding.
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 struct Quad {
   float hp[NP];    // hp[i*5+j] = l'_j(xi_i)
   float hpw[NP];   // hp[l*5+i] * w[l]

@@ -20,6 +20,7 @@
 #include "kernels2d_batched.cuh"
 #include "kernels2d_adjoint.cuh"
 #include "kernels2d_tma.cuh"
+#include "kernels2d_tile.cuh"
 
 namespace {
 
@@ -93,6 +94,17 @@ struct DevMedium {
   int *slot = nullptr;  // CSR position of each element point's contribution
   int *rec_list = nullptr;
   int nrec = 0;
+  // fused tile kernel: tile headers and records, shared-point lists,
+  // receiver points of the tiles, per-colour contributions at boundary
+  // points and the boundary points' side slots
+  int ntiles = 0, sh0 = 0, nb = 0, rec_bytes = 0, max_nint = 0, max_nsh = 0;
+  int4 *t_hdr = nullptr;
+  unsigned char *t_rec = nullptr;
+  int *t_sh = nullptr;
+  int2 *t_rp = nullptr;
+  float *t_r = nullptr;
+  int *b_side = nullptr;
+  std::vector<int> rp_off, rp_cnt;  // per tile (host)
 };
 
 }  // namespace
@@ -190,6 +202,13 @@ struct sfg_handle {
   // corrector); false inside a run, where the next predictor is already applied
   bool state_final = true;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  // fused tile kernel (variant 5): eligible model, side buffer of the
+  // receiver points, receiver -> side slot [nrec][25], shared-memory layout
+  bool tile_ok = false;
+  float *d_side = nullptr;
+  int *d_rslot = nullptr;
+  sfg::dev::TileArgs tile_layout{};
+  int tile_smem = 0, tile_blocks_per_sm = 0;
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
   std::string err;
@@ -289,7 +308,12 @@ void upload_medium(sfg_handle *h, const sfg::MediumData &M, DevMedium &D) {
   D.niface = M.niface;
   D.cp_nx = m.upload(M.cp_nx); D.cp_nz = m.upload(M.cp_nz); D.cp_other = m.upload(M.cp_other);
   D.cp_start = M.cp_start.empty() ? nullptr : m.upload(M.cp_start);
-  D.minv = m.upload(M.minv);
+  {
+    // padded: the tile kernel's bulk copies round ranges up to 16 bytes
+    std::vector<float> mp(M.minv);
+    if (!mp.empty()) mp.resize(mp.size() + 4, 0.f);
+    D.minv = m.upload(mp);
+  }
   D.S = h->asmb.nshots;
   const size_t n = D.values();
   // pad by 4 floats so float4 streaming never runs past an allocation
@@ -486,7 +510,8 @@ void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, c
 }
 
 void launch_stiffness(sfg_handle *h, cudaStream_t s) {
-  launch_stiffness(h, h->el, h->ac, h->d_step, s, h->variant);
+  // the fused tile variant falls back to owner-computes for recorded steps
+  launch_stiffness(h, h->el, h->ac, h->d_step, s, h->variant == 5 ? 3 : h->variant);
 }
 
 sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMedium &O, int medium,
@@ -523,9 +548,8 @@ int grid_for(int n) {
   return std::max(1, std::min(blocks, 148 * 8));
 }
 
-void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
+sfg::dev::RecArgs rec_args(sfg_handle *h, int medium) {
   DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
-  if (D.nrec == 0) return;
   sfg::dev::RecArgs R{};
   R.nrec = D.nrec;
   R.rec_list = D.rec_list;
@@ -548,6 +572,13 @@ void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
   R.step = h->d_step;
   R.seis = h->d_seis;
   R.quad = h->quad;
+  return R;
+}
+
+void launch_receivers(sfg_handle *h, int medium, cudaStream_t s) {
+  DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+  if (D.nrec == 0) return;
+  const sfg::dev::RecArgs R = rec_args(h, medium);
   if (D.S > 1) sfg::dev::k_receivers_batched<<<D.nrec, 32, 0, s>>>(R, D.S);
   else sfg::dev::k_receivers<<<D.nrec, 32, 0, s>>>(R);
 }
@@ -617,7 +648,297 @@ bool receivers_early(const sfg_handle *h, int medium) {
   return true;
 }
 
+// ---------------------------------------------------------------------------
+// Fused tile kernel (variant 5).
+
+// Whether the model can run the fused tile kernel: one shot, isotropic P-SV,
+// SH or acoustic media, conforming coupling whose interface points pair one
+// to one (P-SV), seismograms of displacement, velocity, acceleration or
+// pressure.
+static_assert(sfg::TILE_E == sfg::dev::TILE_E, "host and device tile sizes differ");
+
+bool compute_tile_ok(const sfg_handle *h) {
+  const sfg::Assembly2D &a = h->asmb;
+  const sfg::MediumData &E = a.el, &C = a.ac;
+  if (a.nshots != 1) return false;
+  if (E.nspec && (E.aniso || E.cosserat || E.poro || E.ncomp > 2)) return false;
+  if (!E.cp_start.empty() || !C.cp_start.empty()) return false;
+  if (E.nspec && C.nspec && !(h->fuse_ok && E.ncomp == 2)) return false;
+  for (int t : a.types)
+    if (t > SFG_SEIS_PRESSURE) return false;
+  for (const sfg::MediumData *M : {&E, &C})
+    if (M->nspec && int(M->color_start.size()) - 1 > sfg::dev::TILE_MAX_COLORS) return false;
+  return E.ntiles + C.ntiles > 0;
+}
+
+int tile_nf(const sfg::MediumData &M, int medium) { return medium == SFG_MEDIUM_ACOUSTIC || M.ncomp == 0 ? 6 : 7; }
+
+// Records of the fused tile kernel: header {ibeg, nint, nsh, nel, rp_off,
+// rp_cnt}, tile-local point indices, per element point the colours of the
+// tile's elements that touch its point (tile-interior points) and whether it
+// is the contribution of the lowest of them (which sums the point), the
+// Stacey slot / source head / colour of every element, and the Jacobian and
+// material arrays of the element points.  Rebuilt when the sources or the
+// model change.
+std::vector<unsigned char> tile_records(const sfg::MediumData &M, const std::vector<int> &src_head,
+                                        const DevMedium &D, int nf) {
+  namespace dv = sfg::dev;
+  const int rb = dv::tile_rec_bytes(nf);
+  std::vector<unsigned char> out(size_t(M.ntiles) * rb, 0);
+  const std::vector<float> *arr[7] = {&M.xix, &M.xiz, &M.gax, &M.gaz, &M.jac, &M.prop0, &M.prop1};
+  for (int t = 0; t < M.ntiles; ++t) {
+    unsigned char *r = out.data() + size_t(t) * rb;
+    int *hd = reinterpret_cast<int *>(r);
+    int nel = 0;
+    for (int e = 0; e < dv::TILE_E; ++e) nel += M.tile_elem[size_t(t) * dv::TILE_E + e] >= 0;
+    hd[0] = M.tile_ibeg[t]; hd[1] = M.tile_nint[t]; hd[2] = M.tile_nsh[t]; hd[3] = nel;
+    hd[4] = D.rp_off.empty() ? 0 : D.rp_off[t];
+    hd[5] = D.rp_cnt.empty() ? 0 : D.rp_cnt[t];
+    std::memcpy(r + dv::TREC_LIDX, &M.tile_lidx[size_t(t) * dv::TILE_P], dv::TILE_P * sizeof(uint16_t));
+    {
+      // colour masks of the tile-interior points, then the meta byte
+      std::vector<int> mask(M.tile_nint[t], 0);
+      for (int e = 0; e < dv::TILE_E; ++e) {
+        const int ce = M.tile_elem[size_t(t) * dv::TILE_E + e];
+        if (ce < 0) continue;
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const int k = M.tile_lidx[size_t(t) * dv::TILE_P + e * sfg::NPTS + q];
+          if (k < M.tile_nint[t]) mask[k] |= 1 << M.elem_color[ce];
+        }
+      }
+      unsigned char *meta = r + dv::TREC_META;
+      for (int e = 0; e < dv::TILE_E; ++e) {
+        const int ce = M.tile_elem[size_t(t) * dv::TILE_E + e];
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const int k = M.tile_lidx[size_t(t) * dv::TILE_P + e * sfg::NPTS + q];
+          unsigned char m = 0;
+          if (ce >= 0 && k < M.tile_nint[t]) {
+            const int mk = mask[k];
+            const int low = __builtin_ctz(unsigned(mk));
+            m = static_cast<unsigned char>((mk & 0x7f) | (low == M.elem_color[ce] ? 0x80 : 0));
+          }
+          meta[e * sfg::NPTS + q] = m;
+        }
+      }
+    }
+    int *bc = reinterpret_cast<int *>(r + dv::TREC_BC);
+    int *sr = reinterpret_cast<int *>(r + dv::TREC_SRC);
+    int *co = reinterpret_cast<int *>(r + dv::TREC_COL);
+    float *f = reinterpret_cast<float *>(r + dv::TREC_F);
+    for (int e = 0; e < dv::TILE_E; ++e) {
+      const int ce = M.tile_elem[size_t(t) * dv::TILE_E + e];
+      bc[e] = ce >= 0 ? M.bc_slot[ce] : -1;
+      sr[e] = ce >= 0 && !src_head.empty() ? src_head[ce] : -1;
+      co[e] = ce >= 0 ? M.elem_color[ce] : -1;
+      for (int k = 0; k < nf; ++k)
+        for (int q = 0; q < sfg::NPTS; ++q)
+          f[size_t(k) * dv::TILE_P + e * sfg::NPTS + q] = ce >= 0 ? (*arr[k])[size_t(ce) * sfg::NPTS + q] : 0.f;
+    }
+  }
+  return out;
+}
+
+void refresh_tile_records(sfg_handle *h) {
+  if (!h->tile_ok) return;
+  for (int med = 0; med < 2; ++med) {
+    DevMedium &D = med == 1 ? h->el : h->ac;
+    const sfg::MediumData &M = med == 1 ? h->asmb.el : h->asmb.ac;
+    if (!D.t_rec) continue;
+    const auto rec = tile_records(M, med == 1 ? h->asmb.el_src_head : h->asmb.ac_src_head, D,
+                                  tile_nf(M, med == 1 ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC));
+    SFG_CUDA(cudaMemcpy(D.t_rec, rec.data(), rec.size(), cudaMemcpyHostToDevice));
+  }
+}
+
+// Device data of the fused tile kernel (after the receivers are known) and
+// its shared-memory layout.  Clears h->tile_ok when the layout does not fit.
+void upload_tiles(sfg_handle *h) {
+  namespace dv = sfg::dev;
+  const sfg::Assembly2D &a = h->asmb;
+  // side slots: every point a receiver's element touches, per medium
+  std::vector<std::unordered_map<int, int>> slot_of(2);
+  std::vector<std::vector<std::pair<int, int>>> pts(2);   // (point, slot) in first-use order
+  std::vector<int> rslot(size_t(std::max(a.nrec, 1)) * sfg::NPTS, 0);
+  int nslot = 0;
+  for (int r = 0; r < a.nrec; ++r) {
+    const int med = a.rec_medium[r] == 1 ? 1 : 0;
+    const sfg::MediumData &M = med == 1 ? a.el : a.ac;
+    for (int q = 0; q < sfg::NPTS; ++q) {
+      const int pt = M.ibool[size_t(a.rec_elem[r]) * sfg::NPTS + q];
+      auto it = slot_of[med].find(pt);
+      if (it == slot_of[med].end()) {
+        it = slot_of[med].emplace(pt, nslot++).first;
+        pts[med].push_back({pt, it->second});
+      }
+      rslot[size_t(r) * sfg::NPTS + q] = it->second;
+    }
+  }
+  DevMem &m = h->mem;
+  h->d_side = m.zeros<float>(size_t(std::max(nslot, 1)) * dv::SIDE_W);
+  h->d_rslot = m.upload(rslot);
+  for (int med = 0; med < 2; ++med) {
+    DevMedium &D = med == 1 ? h->el : h->ac;
+    const sfg::MediumData &M = med == 1 ? a.el : a.ac;
+    D.ntiles = M.ntiles;
+    if (M.nspec == 0 || M.ntiles == 0) continue;
+    D.sh0 = M.sh0;
+    D.nb = M.niface + (M.nglob - M.sh0);
+    std::vector<std::vector<int2>> lists(M.ntiles);
+    std::vector<int> bside(std::max(D.nb, 1), -1);
+    for (const auto &ps : pts[med]) {
+      const int pt = ps.first;
+      if (pt < M.niface) { bside[pt] = ps.second; continue; }
+      if (pt >= M.sh0) { bside[M.niface + pt - M.sh0] = ps.second; continue; }
+      const int t = int(std::upper_bound(M.tile_ibeg.begin(), M.tile_ibeg.end(), pt) - M.tile_ibeg.begin()) - 1;
+      if (t < 0 || pt >= M.tile_ibeg[t] + M.tile_nint[t]) throw std::runtime_error("tile of a receiver point not found");
+      lists[t].push_back(make_int2(pt - M.tile_ibeg[t], ps.second));
+    }
+    D.rp_off.assign(M.ntiles, 0);
+    D.rp_cnt.assign(M.ntiles, 0);
+    std::vector<int2> rp;
+    for (int t = 0; t < M.ntiles; ++t) {
+      std::sort(lists[t].begin(), lists[t].end(), [](const int2 &x, const int2 &y) { return x.x < y.x; });
+      D.rp_off[t] = int(rp.size());
+      D.rp_cnt[t] = int(lists[t].size());
+      rp.insert(rp.end(), lists[t].begin(), lists[t].end());
+    }
+    std::vector<int4> hdr(M.ntiles);
+    D.max_nint = D.max_nsh = 0;
+    for (int t = 0; t < M.ntiles; ++t) {
+      hdr[t] = make_int4(M.tile_ibeg[t], M.tile_nint[t], M.tile_nsh[t], M.tile_sh_off[t]);
+      D.max_nint = std::max(D.max_nint, M.tile_nint[t]);
+      D.max_nsh = std::max(D.max_nsh, M.tile_nsh[t]);
+    }
+    const int nf = tile_nf(M, med == 1 ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC);
+    D.rec_bytes = dv::tile_rec_bytes(nf);
+    D.t_hdr = m.upload(hdr);
+    D.t_rec = m.upload(tile_records(M, med == 1 ? a.el_src_head : a.ac_src_head, D, nf));
+    {
+      std::vector<int> sh(M.tile_sh);
+      sh.resize(sh.size() + 4, 0);
+      D.t_sh = m.upload(sh);
+    }
+    D.t_rp = m.upload(rp);
+    D.t_r = m.zeros<float>(size_t(std::max(D.nb, 1)) * ncolors(D) * M.ncomp + 4);
+    D.b_side = m.upload(bside);
+  }
+  // shared-memory layout (uniform over the blocks of both media)
+  auto al4 = [](int x) { return (x + 3) & ~3; };
+  int rec = 0, fcap = 4, shcap = 4, accw = 4;
+  for (const DevMedium *D : {&h->el, &h->ac}) {
+    if (!D->t_rec) continue;
+    rec = std::max(rec, D->rec_bytes);
+    fcap = std::max(fcap, al4(D->max_nint * D->ncomp + 6));
+    shcap = std::max(shcap, al4(D->max_nsh));
+    accw = std::max(accw, al4(D->max_nint) * ncolors(*D) * D->ncomp);
+  }
+  dv::TileArgs &L = h->tile_layout;
+  L.off_sh = rec;
+  L.off_u = L.off_sh + 4 * shcap;
+  L.off_v = L.off_u + 4 * fcap;
+  L.off_m = L.off_v + 4 * fcap;
+  L.stage_bytes = L.off_m + 4 * fcap;
+  L.work_off = 64 + dv::TILE_STAGES * L.stage_bytes;
+  L.acc_off = L.work_off + 4 * dv::TILE_E * dv::TILE_WORK;
+  L.acc_words = accw;
+  h->tile_smem = L.acc_off + 4 * accw;
+  if (h->tile_smem > 227 * 1024) { h->tile_ok = false; return; }
+  auto kern = h->el.ncomp == 1 ? dv::k_tile<1> : dv::k_tile<0>;
+  SFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->tile_smem));
+  int nb = 0;
+  SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, dv::TILE_P, h->tile_smem));
+  h->tile_blocks_per_sm = std::max(nb, 1);
+}
+
+sfg::dev::TileMed tile_med(const DevMedium &D, int ncol, bool store_a) {
+  sfg::dev::TileMed M{};
+  M.hdr = D.t_hdr; M.rec = D.t_rec; M.sh = D.t_sh; M.rp = D.t_rp;
+  M.u = D.u; M.v = D.v; M.a = D.a; M.minv = D.minv; M.r = D.t_r;
+  M.rec_bytes = D.rec_bytes; M.ntiles = D.t_rec ? D.ntiles : 0; M.ncol = ncol;
+  M.niface = D.niface; M.sh0 = D.sh0;
+  M.store_a = store_a ? 1 : 0;
+  return M;
+}
+
+sfg::dev::BndMed bnd_med(const DevMedium &D, const sfg::MediumData &M) {
+  sfg::dev::BndMed B{};
+  B.r = D.t_r; B.b_side = D.b_side;
+  B.nb = D.t_rec ? D.nb : 0; B.niface = M.niface; B.sh0 = M.sh0; B.ncol = ncolors(D);
+  return B;
+}
+
+// The fused tile kernel of both media.
+void launch_tile_kernel(sfg_handle *h, bool predict, cudaStream_t s) {
+  namespace dv = sfg::dev;
+  const sfg::Assembly2D &a = h->asmb;
+  dv::TileArgs A = h->tile_layout;
+  A.el = tile_med(h->el, ncolors(h->el), !predict || h->opt.store_acceleration);
+  A.ac = tile_med(h->ac, ncolors(h->ac), !predict);
+  A.bel = med_args(h->el);
+  A.bac = med_args(h->ac);
+  A.src_next = h->d_src_next; A.src_arr = h->d_src_arr; A.stf = h->d_stf;
+  A.nsrc = a.nsrc; A.nstep = a.nstep; A.step = h->d_step;
+  const float dt = float(a.dt);
+  A.dt = dt; A.dt2 = dt / 2.0f; A.dtsq2 = dt * dt / 2.0f;
+  A.predict = predict ? 1 : 0;
+  A.flag = h->d_flag;
+  A.side = h->d_side;
+  A.quad = h->quad;
+  const int cap = h->tile_blocks_per_sm * h->sm_count;
+  const int te = A.el.ntiles, ta = A.ac.ntiles;
+  int be = te == 0 ? 0 : std::max(1, int(double(cap) * te / (te + ta) + 0.5));
+  if (ta > 0) be = std::min(be, cap - 1);
+  be = std::min(be, te);
+  const int ba = std::min(std::max(cap - be, ta > 0 ? 1 : 0), ta);
+  A.el.nblocks = be;
+  A.ac.nblocks = ba;
+  if (be + ba == 0) return;
+  if (h->el.ncomp == 1) dv::k_tile<1><<<be + ba, dv::TILE_P, h->tile_smem, s>>>(A);
+  else dv::k_tile<0><<<be + ba, dv::TILE_P, h->tile_smem, s>>>(A);
+}
+
+// Boundary points of both media (advances the step counter).
+void launch_tile_boundary(sfg_handle *h, bool predict, cudaStream_t s) {
+  namespace dv = sfg::dev;
+  const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
+  if (has_el && has_ac) {
+    dv::UpdateArgs E = update_args(h, h->el, h->ac, SFG_MEDIUM_ELASTIC, predict, true);
+    dv::UpdateArgs C = update_args(h, h->ac, h->el, SFG_MEDIUM_ACOUSTIC, predict, false);
+    const dv::BndMed be = bnd_med(h->el, h->asmb.el), ba = bnd_med(h->ac, h->asmb.ac);
+    const int n = be.nb + ba.nb - ba.niface;
+    dv::k_tile_boundary<2, true><<<grid_for(n), 256, 0, s>>>(E, be, C, ba, h->d_side);
+    return;
+  }
+  const int med = has_el ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC;
+  const DevMedium &D = has_el ? h->el : h->ac;
+  const DevMedium &O = has_el ? h->ac : h->el;
+  dv::UpdateArgs U = update_args(h, D, O, med, predict, true);
+  const dv::BndMed b = bnd_med(D, has_el ? h->asmb.el : h->asmb.ac);
+  if (D.ncomp == 2)
+    dv::k_tile_boundary<2, false><<<grid_for(b.nb), 256, 0, s>>>(U, b, U, b, h->d_side);
+  else
+    dv::k_tile_boundary<1, false><<<grid_for(b.nb), 256, 0, s>>>(U, b, U, b, h->d_side);
+}
+
+void launch_tile_receivers(sfg_handle *h, cudaStream_t s) {
+  for (int med : {SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC}) {
+    const DevMedium &D = med == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    if (D.nspec == 0 || D.nrec == 0) continue;
+    sfg::dev::k_receivers_side<<<D.nrec, 32, 0, s>>>(rec_args(h, med), h->d_rslot, h->d_side);
+  }
+}
+
+void enqueue_tile_step(sfg_handle *h, cudaStream_t s, bool predict) {
+  launch_tile_kernel(h, predict, s);
+  launch_tile_boundary(h, predict, s);
+  launch_tile_receivers(h, s);
+}
+
 void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
+  if (h->variant == 5 && !h->recording) {
+    enqueue_tile_step(h, s, predict);
+    return;
+  }
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
   if (h->recording) {
     const DevMedium &R = h->el.nspec ? h->el : h->ac;
@@ -658,6 +979,7 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
 }
 
 int kernels_per_step(const sfg_handle *h) {
+  if (h->variant == 5) return 2 + (h->el.nspec && h->el.nrec > 0) + (h->ac.nspec && h->ac.nrec > 0);
   int n = h->variant >= 3 ? 1 : std::max(ncolors(h->el), ncolors(h->ac));
   for (const DevMedium *D : {&h->ac, &h->el}) {
     if (D->nspec == 0) continue;
@@ -721,9 +1043,11 @@ void run_steps(sfg_handle *h, int nsteps) {
 void autotune(sfg_handle *h) {
   const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
                      h->opt.elements_per_block == 32;
-  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 4;
+  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 5;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
+  if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
+  if (h->variant == 5) h->epb = 16;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
   const bool special = h->el.aniso || h->el.ncomp >= 3;   // anisotropic, Cosserat or poroelastic
@@ -740,6 +1064,8 @@ void autotune(sfg_handle *h) {
       for (int e : {8, 16, 32})
         if ((!fix_v || v == h->variant) && (!fix_e || e == h->epb)) cand.push_back({v, e});
     }
+    // fused tile kernel: tiles of 16 elements
+    if (h->tile_ok && (!fix_v || h->variant == 5) && (!fix_e || h->epb == 16)) cand.push_back({5, 16});
   }
   if (cand.empty()) cand.push_back({h->variant, h->epb});
   if (cand.size() > 1) {
@@ -975,6 +1301,7 @@ int sfg_set_sources(sfg_handle *h, int nsrc, const sfg_source2d *src) {
       put(h->d_src_arr, a.src_arr);
       put(h->d_src_arr2, a.src_arr2);
       put(h->d_stf, a.stf);
+      refresh_tile_records(h);
       h->adj.forward_done = false;
     }
     return int(SFG_OK);
@@ -1085,6 +1412,8 @@ int sfg_initialize(sfg_handle *h) {
       }
       h->fuse_ok = ok;
     }
+    h->tile_ok = compute_tile_ok(h);
+    if (h->tile_ok) upload_tiles(h);
     autotune(h);
     h->graph_steps = std::max(1, h->opt.steps_per_graph);
     h->graph_k = capture(h, h->graph_steps, true);
@@ -1248,6 +1577,13 @@ int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms) {
     DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
     if (which != 0 && D.nspec == 0) { if (ms) *ms = 0; return int(SFG_OK); }
     auto launch = [&]() {
+      if (h->variant == 5) {
+        // fused tile kernel: 0 the tile kernel, 1 the boundary points, 3 receivers
+        if (which == 0) launch_tile_kernel(h, true, h->stream);
+        else if (which == 1) launch_tile_boundary(h, true, h->stream);
+        else if (which == 3) launch_tile_receivers(h, h->stream);
+        return;
+      }
       if (which == 0) launch_stiffness(h, h->stream);
       else if (which == 3) { launch_receivers(h, SFG_MEDIUM_ACOUSTIC, h->stream);
                              launch_receivers(h, SFG_MEDIUM_ELASTIC, h->stream); }
@@ -1381,18 +1717,18 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
       return int(SFG_ERR_UNSUPPORTED);
     }
     if (!u || !v || !a || istep < 0) { h->err = "null field pointer or negative step"; return int(SFG_ERR_ARG); }
-    // the kernels read and write the fields as float2 / float4 vectors
-    for (const float *p : {u, v, a})
-      if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
-        h->err = "sfg_step_noalloc: u, v and a must start on a 16-byte boundary";
-        return int(SFG_ERR_ARG);
-      }
     const size_t n = size_t(h->el.nglob) * h->el.ncomp;
     if (n > NOALLOC_MAX_VALUES) {
       h->err = "sfg_step_noalloc: the model has " + std::to_string(n) +
                " point values, above the fixed scratch of " + std::to_string(NOALLOC_MAX_VALUES);
       return int(SFG_ERR_ARG);
     }
+    // the kernels read and write the fields as float2 / float4 vectors
+    for (const float *p : {u, v, a})
+      if (reinterpret_cast<uintptr_t>(p) % 16 != 0) {
+        h->err = "sfg_step_noalloc: u, v and a must start on a 16-byte boundary";
+        return int(SFG_ERR_ARG);
+      }
     NoallocDevice nd;
     const int rc = noalloc_device(nd, h->err);
     if (rc != SFG_OK) return rc;
@@ -1454,6 +1790,7 @@ int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const f
         put(D.bc_imp0, M.bc_imp0); put(D.bc_imp1, M.bc_imp1);
         put(D.minv, M.minv);
       }
+      refresh_tile_records(h);
       if (h->adj.st_c && !h->asmb.el.stacey_c.empty())
         SFG_CUDA(cudaMemcpy(h->adj.st_c, h->asmb.el.stacey_c.data(), h->asmb.el.stacey_c.size() * sizeof(float),
                             cudaMemcpyHostToDevice));

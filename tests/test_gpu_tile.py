@@ -1,0 +1,144 @@
+"""The fused tile kernel (kernel variant 5) against the other variants.
+
+Variant 5 computes element forces, assembles them in shared memory tile by
+tile and finishes the tile-interior points in one launch; a second launch
+finishes the points that tiles share (and the coupled interface), a third
+interpolates the receivers from the end-of-step values of their points.
+Every point's contributions are still summed in colour order, so its
+seismograms and fields must equal the colour-pass kernel's bit for bit, for
+every seismogram type, with sources, Stacey edges, free surfaces and the
+acoustic-elastic coupling, across runs cut into pieces, single steps and the
+per-step host-buffer call.
+"""
+import numpy as np
+import pytest
+
+from conftest import golden_case, product_run, workload_case
+
+pytestmark = pytest.mark.gpu
+
+ALL_TYPES = ("displacement", "velocity", "acceleration", "pressure")
+
+
+def _fields(sim):
+    out = {}
+    inf = sim.info()
+    for med, n in (("elastic", inf.nglob_elastic), ("acoustic", inf.nglob_acoustic)):
+        if n == 0:
+            continue
+        for f in ("displacement", "velocity", "acceleration"):
+            out[(med, f)] = sim.field(med, f)
+    return out
+
+
+def _equal_runs(case, types, nsteps=None):
+    s1, a = product_run(case, types=types, nsteps=nsteps, variant=1)
+    s5, b = product_run(case, types=types, nsteps=nsteps, variant=5)
+    assert s5.info().kernel_variant == 5
+    assert s5.info().kernels_per_step <= 4
+    assert np.abs(a).max() > 0
+    assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
+    fa, fb = _fields(s1), _fields(s5)
+    for k in fa:
+        assert np.array_equal(fa[k], fb[k]), k
+    assert s5.check_finite()
+    return s5
+
+
+@pytest.mark.parametrize("nx,nz", [(40, 20), (80, 40)])
+def test_tile_kernel_coupled_all_types(sfg_lib, nx, nz):
+    from specfempp_b200 import meshgen
+    w = meshgen.coupled_400x200(nstep=150, nx=nx, nz=nz)
+    case = workload_case(w, types=ALL_TYPES)
+    _equal_runs(case, ALL_TYPES)
+
+
+@pytest.mark.parametrize("name", ["HomogeneousAcousticDomainDirichletBC", "HomogeneousElasticDomainStaceyBC",
+                                  "HomogeneousElasticDomainStaceyDirichletBC",
+                                  "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticDomainMomentTensor",
+                                  "AcousticElasticCoupledDomainVariant2", "HomogeneousAcousticDomain",
+                                  "HomogeneousAcousticDomainCompositeStaceyDirichletBC"])
+def test_tile_kernel_fixtures(sfg_lib, name):
+    case, _, _ = golden_case(name)
+    types = ALL_TYPES if not case.elastic_sh else ("displacement", "velocity", "acceleration")
+    _equal_runs(case, types, nsteps=min(case.nstep, 800))
+
+
+def test_tile_kernel_elastic_80x60(sfg_lib):
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_psv_80x60(nstep=400)
+    _equal_runs(workload_case(w, types=ALL_TYPES), ALL_TYPES)
+
+
+def test_tile_kernel_pieces_steps_and_step_io(sfg_lib):
+    """Runs cut into pieces, single steps and the host-buffer step give the
+    one-run seismograms (the pending predictor is resumed between runs)."""
+    from specfempp_b200 import meshgen
+    w = meshgen.coupled_400x200(nstep=90, nx=40, nz=20)
+    case = workload_case(w, types=("displacement", "velocity"))
+    sim, whole = product_run(case, types=case.seis_types, variant=5)
+    sim.reset()
+    sim.run(37)
+    for _ in range(3):
+        sim.step()
+    sim.run(50)
+    assert np.array_equal(sim.seismograms()[0], whole)
+    sim.reset()
+    inf = sim.info()
+    got = np.zeros((case.nstep, inf.ntypes, inf.nrec, 2), np.float32)
+    row = np.zeros((inf.nshots, inf.ntypes, inf.nrec, 2), np.float32)
+    for i in range(case.nstep):
+        sim.step_io(None, row)
+        got[i] = row[0]
+    assert np.array_equal(got, whole)
+
+
+def test_tile_kernel_new_sources_and_model(sfg_lib):
+    """Replacing the sources and the model after initialisation refreshes the
+    tile records: the results equal a handle built with them."""
+    from dataclasses import replace
+
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.elastic_psv_80x60(nstep=200)
+    src2 = [replace(w.sources[0], x=w.sources[0].x + 700.0, z=w.sources[0].z - 400.0)]
+
+    def make(srcs):
+        sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, kernel_variant=5)
+        sim.set_sources(srcs)
+        sim.set_receivers(w.rec_x, w.rec_z, types=("displacement", "velocity"))
+        sim.initialize()
+        return sim
+
+    a = make(w.sources)
+    a.set_sources(src2)
+    a.run(w.nstep)
+    b = make(src2)
+    b.run(w.nstep)
+    assert a.info().kernel_variant == 5
+    assert np.array_equal(a.seismograms(), b.seismograms())
+    # model: 3% slower shear waves everywhere, against the colour passes
+    nspec = w.mesh.nspec
+    rho = np.full((nspec, 25), float(w.mesh.mat_rho[0]), np.float32)
+    vp = float(w.mesh.mat_vp[0])
+    vs = 0.97 * float(w.mesh.mat_vs[0])
+    mu = rho * vs * vs
+    kappa = rho * vp * vp - 4.0 / 3.0 * mu
+    out = []
+    for v in (1, 5):
+        sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, kernel_variant=v)
+        sim.set_sources(w.sources)
+        sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
+        sim.initialize()
+        sim.set_model(rho, kappa.astype(np.float32), mu.astype(np.float32))
+        sim.run(w.nstep)
+        out.append(sim.seismograms())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_tile_kernel_refused_forms_fall_back(sfg_lib):
+    """Models the tile kernel does not cover (anisotropic) run another
+    variant when variant 5 is asked for."""
+    from test_oracle import layered_aniso_case
+    case = layered_aniso_case(50)
+    sim, _ = product_run(case, variant=5)
+    assert sim.info().kernel_variant == 3

@@ -86,7 +86,7 @@ def test_noalloc_reports_a_nonfinite_step(sfg_lib):
     w = meshgen.elastic_psv_80x60(nstep=8)
     sim = _handle(w)
     n = sim.info().nglob_elastic * 2
-    buf = torch.zeros(3, n, device="cuda")
+    buf = torch.zeros(3, (n + 3) // 4 * 4, device="cuda")   # rows on 16-byte boundaries
     buf[0, 7] = float("nan")                  # a blown-up displacement
     torch.cuda.synchronize()
     rc = sfg_lib.sfg_step_noalloc(sim.h, 0, C.c_void_p(buf[0].data_ptr()),
