@@ -23,12 +23,13 @@
 // free-surface / source epilogue), operand for operand.  Assembly: within a
 // mesh colour no two elements share a point, so every interior point has one
 // shared-memory slot per colour; each element point writes its contribution
-// to its point's slot of its element's colour, and after one barrier the
-// point's thread sums the slots in increasing colour order, as the
+// to its point's slot of its element's colour, and after one barrier one
+// thread per tile-interior point sums the slots of the colours that touch it
+// (a mask per point in the tile record) in increasing colour order, as the
 // colour-pass and owner-computes kernels sum: the results are bit-identical
-// to theirs (a slot of a colour that does not touch the point holds zero,
-// and adding zero changes no value).  Contributions at boundary points go to
-// the same per-colour slots in HBM.  Finally the interior points get
+// to theirs.  Contributions at boundary points go to per-colour slots in HBM
+// (slots of colours that do not touch a point hold zero; adding zero
+// changes no value).  Finally the interior points get
 // a = sum * M^-1, the corrector and (inside a run) the next predictor, and
 // are written back.
 // Reference: include/kokkos_kernels/impl/compute_stiffness_interaction.tpp:140-247,
@@ -61,11 +62,11 @@ constexpr int TILE_E = 16;
 constexpr int TILE_P = TILE_E * NP;  // element points of a tile = threads of a block
 constexpr int TILE_STAGES = 4;
 // tile record (bytes): header {ibeg, nint, nsh, nel, rp_off, rp_cnt, 0, 0},
-// lidx u16[400], meta u8[400] (bit 7: this element point sums its point;
-// bits 0..6: the colours of the tile's elements that touch the point),
+// lidx u16[400], mask u8[400] (tile-interior point k: the colours of the
+// tile's elements that touch it),
 // bc_slot / src_head / colour int[16] each, then nf float arrays [400]:
 // xi_x, xi_z, gamma_x, gamma_z, |J|, material words
-constexpr int TREC_LIDX = 32, TREC_META = 832, TREC_BC = 1232, TREC_SRC = 1296, TREC_COL = 1360,
+constexpr int TREC_LIDX = 32, TREC_MASK = 832, TREC_BC = 1232, TREC_SRC = 1296, TREC_COL = 1360,
               TREC_F = 1424;
 constexpr int TILE_MAX_COLORS = 7;
 __host__ __device__ constexpr int tile_rec_bytes(int nf) { return TREC_F + nf * TILE_P * 4; }
@@ -147,14 +148,14 @@ __device__ __forceinline__ float2 tile_fetch_u(const TileArgs &A, const TileMed 
 // are kept in shared memory (staged v, colour-0 slot) for the side buffer.
 template <int NC>
 __device__ __forceinline__ bool tile_finish(const TileArgs &A, const TileMed &M, int ibeg, int v0, int k, int kcap,
-                                            const float (&u)[NC], const float (&sum)[NC], const float *uin, float *vin,
+                                            const float (&sum)[NC], const float *uin, float *vin,
                                             const float *min, float *acc, bool keep) {
   const int o = (ibeg + k) * NC - v0;
   float au[NC], vv[NC], ac[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     ac[c] = __fmul_rn(sum[c], min[o + c]);
-    au[c] = u[c];
+    au[c] = uin[o + c];
     vv[c] = newmark_correct(vin[o + c], ac[c], A.dt2);
   }
   if (keep) {
@@ -177,7 +178,6 @@ __device__ __forceinline__ bool tile_finish(const TileArgs &A, const TileMed &M,
     M.v[gi] = vv[0];
     if (M.store_a) M.a[gi] = ac[0];
   }
-  (void)uin;
   return bad;
 }
 
@@ -258,8 +258,6 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
     const int *hd = reinterpret_cast<const int *>(stage);
     const int ibeg = hd[0], nint = hd[1], nel = hd[3], rp_off = hd[4], rp_cnt = hd[5];
     const int k = reinterpret_cast<const uint16_t *>(stage + TREC_LIDX)[tid];
-    // owner flag (bit 7) and the colours that touch the point (bits 0..6)
-    const int meta = stage[TREC_META + tid];
     const bool act = le < nel;
     const float *F = reinterpret_cast<const float *>(stage + TREC_F);
     const float xix = F[tid], xiz = F[TILE_P + tid], gax = F[2 * TILE_P + tid], gaz = F[3 * TILE_P + tid],
@@ -321,7 +319,6 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
       a[c] = -(wiz * t1 + wix * t2);
     }
     const bool interior = k < nint;
-    const int single = 0x80 | (1 << (col < 0 ? 0 : col));
     const int v0 = (ibeg * NC) & ~3;
     float *uin = reinterpret_cast<float *>(stage + A.off_u);
     float *vin = reinterpret_cast<float *>(stage + A.off_v);
@@ -359,18 +356,9 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
         }
       }
       if (interior) {
-        if (meta == single) {
-          // the only contribution to its point (the point is inside the
-          // element, or on a tile-interior mesh edge): finish it now
-          float sum[NC];
+        // the point's slot of this element's colour (one element per colour)
 #pragma unroll
-          for (int c = 0; c < NC; ++c) sum[c] = 0.f + a[c];
-          bad |= tile_finish<NC>(A, M, ibeg, v0, k, kcap, uu, sum, uin, vin, min, acc, rp_cnt > 0);
-        } else {
-          // the point's slot of this element's colour (one element per colour)
-#pragma unroll
-          for (int c = 0; c < NC; ++c) acc[(col * NC + c) * kcap + k] = a[c];
-        }
+        for (int c = 0; c < NC; ++c) acc[(col * NC + c) * kcap + k] = a[c];
       } else {
         const int g = reinterpret_cast<const int *>(stage + A.off_sh)[k - nint];
         const size_t bi = g < M.niface ? size_t(g) : size_t(M.niface) + (g - M.sh0);
@@ -380,18 +368,20 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
       }
     }
     __syncthreads();
-    // points with several contributions: the contributor of the lowest colour
-    // sums the slots of the colours present, in increasing colour order
-    if (act && interior && meta != single && (meta & 0x80)) {
+    // the tile-interior points, one thread each: the slots of the colours
+    // present, in increasing colour order, then M^-1, corrector, predictor
+    for (int kk = tid; kk < nint; kk += blockDim.x) {
+      const int mk = stage[TREC_MASK + kk];
       float sum[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) sum[c] = 0.f;
-      for (int cl = 0; cl < ncol; ++cl)
-        if (meta >> cl & 1) {
 #pragma unroll
-          for (int c = 0; c < NC; ++c) sum[c] = sum[c] + acc[(cl * NC + c) * kcap + k];
+      for (int cl = 0; cl < TILE_MAX_COLORS; ++cl)
+        if (mk >> cl & 1) {
+#pragma unroll
+          for (int c = 0; c < NC; ++c) sum[c] = sum[c] + acc[(cl * NC + c) * kcap + kk];
         }
-      bad |= tile_finish<NC>(A, M, ibeg, v0, k, kcap, uu, sum, uin, vin, min, acc, rp_cnt > 0);
+      bad |= tile_finish<NC>(A, M, ibeg, v0, kk, kcap, sum, uin, vin, min, acc, rp_cnt > 0);
     }
     if (rp_cnt > 0) {
       // receiver points of the tile: u of the step, corrected v, new a
@@ -441,15 +431,25 @@ __device__ __forceinline__ bool bnd_point(const UpdateArgs &A, const BndMed &B, 
   for (int c = 0; c < NC; ++c) acc[c] = 0.f;
   // the contributions in colour order (absent colours hold zero)
   const float *sl = B.r + size_t(bi) * B.ncol * NC;
-  for (int cl = 0; cl < B.ncol; ++cl) {
-    if (NC == 2) {
-      const float2 t = reinterpret_cast<const float2 *>(sl)[cl];
-      acc[0] = acc[0] + t.x;
-      acc[NC - 1] = acc[NC - 1] + t.y;
-    } else {
-      acc[0] = acc[0] + sl[cl];
+  float cv[TILE_MAX_COLORS][NC];
+#pragma unroll
+  for (int cl = 0; cl < TILE_MAX_COLORS; ++cl) {   // all loads first, then the sum in order
+    if (cl < B.ncol) {
+      if (NC == 2) {
+        const float2 t = reinterpret_cast<const float2 *>(sl)[cl];
+        cv[cl][0] = t.x;
+        cv[cl][NC - 1] = t.y;
+      } else {
+        cv[cl][0] = sl[cl];
+      }
     }
   }
+#pragma unroll
+  for (int cl = 0; cl < TILE_MAX_COLORS; ++cl)
+    if (cl < B.ncol) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] = acc[c] + cv[cl][c];
+    }
   if (g < A.niface) {
 #pragma unroll
     for (int c = 0; c < NC; ++c) acc[c] += coupling_term(A, g, c);

@@ -674,11 +674,10 @@ bool compute_tile_ok(const sfg_handle *h) {
 int tile_nf(const sfg::MediumData &M, int medium) { return medium == SFG_MEDIUM_ACOUSTIC || M.ncomp == 0 ? 6 : 7; }
 
 // Records of the fused tile kernel: header {ibeg, nint, nsh, nel, rp_off,
-// rp_cnt}, tile-local point indices, per element point the colours of the
-// tile's elements that touch its point (tile-interior points) and whether it
-// is the contribution of the lowest of them (which sums the point), the
-// Stacey slot / source head / colour of every element, and the Jacobian and
-// material arrays of the element points.  Rebuilt when the sources or the
+// rp_cnt}, tile-local point indices, per tile-interior point the colours of
+// the tile's elements that touch it, the Stacey slot / source head / colour
+// of every element, and the Jacobian and material arrays of the element
+// points.  Rebuilt when the sources or the
 // model change.
 std::vector<unsigned char> tile_records(const sfg::MediumData &M, const std::vector<int> &src_head,
                                         const DevMedium &D, int nf) {
@@ -696,28 +695,14 @@ std::vector<unsigned char> tile_records(const sfg::MediumData &M, const std::vec
     hd[5] = D.rp_cnt.empty() ? 0 : D.rp_cnt[t];
     std::memcpy(r + dv::TREC_LIDX, &M.tile_lidx[size_t(t) * dv::TILE_P], dv::TILE_P * sizeof(uint16_t));
     {
-      // colour masks of the tile-interior points, then the meta byte
-      std::vector<int> mask(M.tile_nint[t], 0);
+      // colour masks of the tile-interior points
+      unsigned char *mask = r + dv::TREC_MASK;
       for (int e = 0; e < dv::TILE_E; ++e) {
         const int ce = M.tile_elem[size_t(t) * dv::TILE_E + e];
         if (ce < 0) continue;
         for (int q = 0; q < sfg::NPTS; ++q) {
           const int k = M.tile_lidx[size_t(t) * dv::TILE_P + e * sfg::NPTS + q];
-          if (k < M.tile_nint[t]) mask[k] |= 1 << M.elem_color[ce];
-        }
-      }
-      unsigned char *meta = r + dv::TREC_META;
-      for (int e = 0; e < dv::TILE_E; ++e) {
-        const int ce = M.tile_elem[size_t(t) * dv::TILE_E + e];
-        for (int q = 0; q < sfg::NPTS; ++q) {
-          const int k = M.tile_lidx[size_t(t) * dv::TILE_P + e * sfg::NPTS + q];
-          unsigned char m = 0;
-          if (ce >= 0 && k < M.tile_nint[t]) {
-            const int mk = mask[k];
-            const int low = __builtin_ctz(unsigned(mk));
-            m = static_cast<unsigned char>((mk & 0x7f) | (low == M.elem_color[ce] ? 0x80 : 0));
-          }
-          meta[e * sfg::NPTS + q] = m;
+          if (k < M.tile_nint[t]) mask[k] = static_cast<unsigned char>(mask[k] | (1 << M.elem_color[ce]));
         }
       }
     }
