@@ -5,10 +5,15 @@
 // as the CPU baseline of bench.py.  The product (libsfg) never links it.
 //
 // Everything is templated on the arithmetic type so that the same code runs
-// in FP32 (the reference's type_real = float) and FP64.  Assembly is serial in
-// element order, so an FP32 run is deterministic; with nthreads > 1 the
-// element loop runs under OpenMP with atomic adds, as the reference's
-// Kokkos OpenMP backend does (timing use only).
+// in FP32 (the reference's type_real = float) and FP64.  With one thread the
+// assembly is serial in element order.  With nthreads > 1 the elements of
+// each medium are split into colours (greedy, in element order: no two
+// elements of a colour share a global point) and each colour is one OpenMP
+// loop with plain adds, colour after colour: every point's contributions are
+// summed in colour order whatever the thread count, so a multithreaded FP32
+// run is deterministic too.  The reference sums with atomic adds in
+// whatever order its threads arrive (compute_stiffness_interaction.tpp:
+// 244-245), so no single order is the reference's.
 //
 // Reference files restated (paths inside the SPECFEM++ tree):
 //   GLL points / weights        src/quadrature/gll/gll_library.cpp:102-190
@@ -244,6 +249,7 @@ struct Sim {
   const OracleInput2D &in;
   int nspec, nglob = 0, ngnod;
   T z[NG], w[NG], hp[NG][NG];
+  T hpw[NG][NG];                    // hp[l][i] * w[l] rounded once (device evaluation order)
   std::vector<int> ibool;           // [nspec][25]
   std::vector<T> xix, xiz, gax, gaz, jac;  // [nspec][25]
   std::vector<T> gx, gz;            // coordinates of local points
@@ -295,7 +301,7 @@ struct Sim {
     gll_hprime(zd, hpd);
     for (int i = 0; i < NG; ++i) {
       z[i] = T(zd[i]); w[i] = T(wd[i]);
-      for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
+      for (int j = 0; j < NG; ++j) { hp[i][j] = T(hpd[i][j]); hpw[i][j] = T(hpd[i][j] * wd[i]); }
     }
     dt = T(in.dt);
     ncomp_el = in.poro ? 4 : in.cosserat ? 3 : in.elastic_sh ? 1 : 2;
@@ -911,11 +917,19 @@ struct Sim {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
         T dxi[4] = {0, 0, 0, 0}, dga[4] = {0, 0, 0, 0};
-        for (int l = 0; l < NG; ++l)
-          for (int c = 0; c < ncomp; ++c) {
-            dxi[c] += hp[ix][l] * fu[iz * NG + l][c];
-            dga[c] += hp[iz][l] * fu[l * NG + ix][c];
-          }
+        if (in.device_order) {
+          for (int l = 0; l < NG; ++l)
+            for (int c = 0; c < ncomp; ++c) {
+              dxi[c] = std::fma(hp[ix][l], fu[iz * NG + l][c], dxi[c]);
+              dga[c] = std::fma(hp[iz][l], fu[l * NG + ix][c], dga[c]);
+            }
+        } else {
+          for (int l = 0; l < NG; ++l)
+            for (int c = 0; c < ncomp; ++c) {
+              dxi[c] += hp[ix][l] * fu[iz * NG + l][c];
+              dga[c] += hp[iz][l] * fu[l * NG + ix][c];
+            }
+        }
         T du[4][2];
         for (int c = 0; c < ncomp; ++c) {
           du[c][0] = xix[p] * dxi[c] + gax[p] * dga[c];
@@ -985,9 +999,17 @@ struct Sim {
         const int q = iz * NG + ix;
         const size_t p = size_t(e) * NP + q;
         T t1[4] = {0, 0, 0, 0}, t2[4] = {0, 0, 0, 0};
-        for (int l = 0; l < NG; ++l) {
-          for (int c = 0; c < ncomp; ++c) t1[c] += F[iz * NG + l][c][0] * hp[l][ix] * w[l];
-          for (int c = 0; c < ncomp; ++c) t2[c] += F[l * NG + ix][c][1] * hp[l][iz] * w[l];
+        if (in.device_order) {
+          for (int l = 0; l < NG; ++l)
+            for (int c = 0; c < ncomp; ++c) {
+              t1[c] = std::fma(F[iz * NG + l][c][0], hpw[l][ix], t1[c]);
+              t2[c] = std::fma(F[l * NG + ix][c][1], hpw[l][iz], t2[c]);
+            }
+        } else {
+          for (int l = 0; l < NG; ++l) {
+            for (int c = 0; c < ncomp; ++c) t1[c] += F[iz * NG + l][c][0] * hp[l][ix] * w[l];
+            for (int c = 0; c < ncomp; ++c) t2[c] += F[l * NG + ix][c][1] * hp[l][iz] * w[l];
+          }
         }
         T acc[4];
         for (int c = 0; c < ncomp; ++c) acc[c] = T(-1) * (w[iz] * t1[c] + w[ix] * t2[c]);
@@ -1031,6 +1053,26 @@ struct Sim {
   void corrector(std::vector<T> &v, const std::vector<T> &a) {
     const T dt2 = dt / T(2.0);
     for (size_t i = 0; i < v.size(); ++i) v[i] += dt2 * a[i];
+  }
+
+  // Greedy colouring of one medium's elements, in element order (built once).
+  std::vector<std::vector<int>> colour_lists[2];
+  const std::vector<std::vector<int>> &colours(int med) {
+    std::vector<std::vector<int>> &out = colour_lists[med == MED_ACOUSTIC ? 0 : 1];
+    if (!out.empty() || nspec == 0) return out;
+    std::vector<uint32_t> used(nglob, 0u);
+    for (int e = 0; e < nspec; ++e) {
+      if (medium[e] != med) continue;
+      uint32_t mask = 0;
+      for (int q = 0; q < NP; ++q) mask |= used[ibool[size_t(e) * NP + q]];
+      int c = 0;
+      while (c < 32 && (mask >> c & 1u)) ++c;
+      if (c == 32) throw std::runtime_error("mesh needs more than 32 colours");
+      for (int q = 0; q < NP; ++q) used[ibool[size_t(e) * NP + q]] |= 1u << c;
+      if (int(out.size()) <= c) out.resize(c + 1);
+      out[size_t(c)].push_back(e);
+    }
+    return out;
   }
 
   void update_medium(int med, int istep, int nthreads) {
@@ -1116,15 +1158,13 @@ struct Sim {
     // stiffness (:112-126)
 #ifdef _OPENMP
     if (nthreads > 1) {
+      const std::vector<std::vector<int>> &col = colours(med);
+      for (const std::vector<int> &L : col) {
 #pragma omp parallel for num_threads(nthreads) schedule(static)
-      for (int e = 0; e < nspec; ++e) {
-        if (medium[e] != med) continue;
-        stiffness_element(e, ncomp, u, v, [&](int g, const T *acc) {
-          for (int c = 0; c < ncomp; ++c) {
-#pragma omp atomic
-            a[size_t(g) * ncomp + c] += acc[c];
-          }
-        });
+        for (long long k = 0; k < (long long)L.size(); ++k)
+          stiffness_element(L[size_t(k)], ncomp, u, v, [&](int g, const T *acc) {
+            for (int c = 0; c < ncomp; ++c) a[size_t(g) * ncomp + c] += acc[c];
+          });
       }
     } else
 #endif

@@ -54,6 +54,11 @@ typedef struct OracleInput2D {
    * kappa_fr, eta_f, mu_fr, Q_mu): four components (solid u_x, u_z, fluid
    * w_x, w_z); NULL: none */
   const double *poro;
+  /* 0: the reference's evaluation order (products and sums rounded
+   * separately); 1: the device kernels' order (the 5-term contractions as
+   * fused multiply-adds, the divergence weights hprime * w rounded once).
+   * Both restate the same algorithm; they differ only in FP32 rounding. */
+  int device_order;
 } OracleInput2D;
 
 typedef struct OracleOutput2D {

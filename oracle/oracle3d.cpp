@@ -122,6 +122,7 @@ struct Sim3D {
   int nex, ney, nez, nspec, NX, NY, NZ, nglob;
   double zd[NG], wd[NG], hpd[NG][NG];
   T w[NG], hp[NG][NG];
+  T hpw[NG][NG];   // hp[l][i] * w[l] rounded once (device evaluation order)
   std::vector<int> ibool;                           // [nspec][125]
   std::vector<T> g9, jac, c0, mu;                   // g9: [nspec][125][9]
   std::vector<T> u, v, a, minv;                     // [nglob][3]
@@ -142,7 +143,7 @@ struct Sim3D {
     gll5(zd, wd, hpd);
     for (int i = 0; i < NG; ++i) {
       w[i] = T(wd[i]);
-      for (int j = 0; j < NG; ++j) hp[i][j] = T(hpd[i][j]);
+      for (int j = 0; j < NG; ++j) { hp[i][j] = T(hpd[i][j]); hpw[i][j] = T(hpd[i][j] * wd[i]); }
     }
     dt = T(in.dt);
   }
@@ -348,10 +349,18 @@ struct Sim3D {
           T dxi[3][3];  // [comp][xi, eta, gamma]
           for (int c = 0; c < 3; ++c) {
             T s0 = 0, s1 = 0, s2 = 0;
-            for (int l = 0; l < NG; ++l) {
-              s0 += hp[ix][l] * fu[(iz * NG + iy) * NG + l][c];
-              s1 += hp[iy][l] * fu[(iz * NG + l) * NG + ix][c];
-              s2 += hp[iz][l] * fu[(l * NG + iy) * NG + ix][c];
+            if (in.device_order) {
+              for (int l = 0; l < NG; ++l) {
+                s0 = std::fma(hp[ix][l], fu[(iz * NG + iy) * NG + l][c], s0);
+                s1 = std::fma(hp[iy][l], fu[(iz * NG + l) * NG + ix][c], s1);
+                s2 = std::fma(hp[iz][l], fu[(l * NG + iy) * NG + ix][c], s2);
+              }
+            } else {
+              for (int l = 0; l < NG; ++l) {
+                s0 += hp[ix][l] * fu[(iz * NG + iy) * NG + l][c];
+                s1 += hp[iy][l] * fu[(iz * NG + l) * NG + ix][c];
+                s2 += hp[iz][l] * fu[(l * NG + iy) * NG + ix][c];
+              }
             }
             dxi[c][0] = s0; dxi[c][1] = s1; dxi[c][2] = s2;
           }
@@ -378,10 +387,18 @@ struct Sim3D {
           const int q = (iz * NG + iy) * NG + ix;
           for (int c = 0; c < 3; ++c) {
             T t1 = 0, t2 = 0, t3 = 0;
-            for (int l = 0; l < NG; ++l) {
-              t1 += F[(iz * NG + iy) * NG + l][c][0] * hp[l][ix] * w[l];
-              t2 += F[(iz * NG + l) * NG + ix][c][1] * hp[l][iy] * w[l];
-              t3 += F[(l * NG + iy) * NG + ix][c][2] * hp[l][iz] * w[l];
+            if (in.device_order) {
+              for (int l = 0; l < NG; ++l) {
+                t1 = std::fma(F[(iz * NG + iy) * NG + l][c][0], hpw[l][ix], t1);
+                t2 = std::fma(F[(iz * NG + l) * NG + ix][c][1], hpw[l][iy], t2);
+                t3 = std::fma(F[(l * NG + iy) * NG + ix][c][2], hpw[l][iz], t3);
+              }
+            } else {
+              for (int l = 0; l < NG; ++l) {
+                t1 += F[(iz * NG + iy) * NG + l][c][0] * hp[l][ix] * w[l];
+                t2 += F[(iz * NG + l) * NG + ix][c][1] * hp[l][iy] * w[l];
+                t3 += F[(l * NG + iy) * NG + ix][c][2] * hp[l][iz] * w[l];
+              }
             }
             r[q][c] = T(-1) * (w[iz] * w[iy] * t1 + w[iz] * w[ix] * t2 + w[iy] * w[ix] * t3);
           }

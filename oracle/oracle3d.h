@@ -21,6 +21,9 @@ typedef struct OracleInput3D {
   const int *seis_types;      /* 0 displacement 1 velocity 2 acceleration */
   double dt;
   int nstep;
+  /* 0: the reference's evaluation order; 1: the device kernels' order (the
+   * 5-term contractions as fused multiply-adds, hprime * w rounded once) */
+  int device_order;
 } OracleInput3D;
 
 typedef struct OracleOutput3D {

@@ -50,7 +50,7 @@ class OracleInput2D(C.Structure):
         ("src_kind", _ip), ("src_mxx", _dp), ("src_mzz", _dp), ("src_mxz", _dp),
         ("aniso", _dp), ("cosserat", _dp),
         ("nadj", C.c_int), ("adjacency", _ip), ("poro", _dp),
-    ]
+        ("device_order", C.c_int)]
 
 
 class OracleOutput2D(C.Structure):
@@ -123,6 +123,7 @@ class Case2D:
     stf_table: np.ndarray | None = None    # optional [nstep, nsrc]
     stations: list = field(default_factory=list)
     setup_in_run_precision: bool = False   # True: reference-faithful FP32 setup geometry
+    device_order: bool = False             # True: FMA contractions as the CUDA kernels evaluate them
     start_time: float | None = None        # the configuration's t0 (sources keep their tshift)
 
 
@@ -284,6 +285,7 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     nsb = max(1, case.nstep_between_samples)
     inp.nstep_between_samples = nsb
     inp.setup_in_run_precision = int(case.setup_in_run_precision)
+    inp.device_order = int(case.device_order)
     inp.src_kind = _ptr(arr([1 if getattr(s, "kind", "force") == "moment_tensor" else 0 for s in srcs],
                             np.int32), _ip)
     inp.src_mxx = _ptr(arr([getattr(s, "mxx", 0.0) for s in srcs], np.float64), _dp)

@@ -26,7 +26,7 @@ class OracleInput3D(C.Structure):
         ("src_f0", _dp), ("src_factor", _dp), ("src_tshift", _dp), ("t0", C.c_double),
         ("nrec", C.c_int), ("rec_xyz", _dp),
         ("ntypes", C.c_int), ("seis_types", _ip),
-        ("dt", C.c_double), ("nstep", C.c_int),
+        ("dt", C.c_double), ("nstep", C.c_int), ("device_order", C.c_int),
     ]
 
 
@@ -55,6 +55,7 @@ class Case3D:
     dt: float
     nstep: int
     seis_types: list = field(default_factory=lambda: ["displacement"])
+    device_order: bool = False          # True: FMA contractions as the CUDA kernels evaluate them
 
 
 def start_time(sources):
@@ -96,6 +97,7 @@ def run(case: Case3D, precision: str = "f32", nthreads: int = 8, want_final: boo
     inp.ntypes = len(types)
     inp.seis_types = arr(types, np.int32)
     inp.dt, inp.nstep = case.dt, case.nstep
+    inp.device_order = int(case.device_order)
     seis = np.zeros((case.nstep, len(types), len(case.rec_xyz), 3))
     out = OracleOutput3D()
     out.seismograms = seis.ctypes.data_as(_dp)

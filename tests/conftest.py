@@ -64,6 +64,22 @@ def reference_metric(computed, traces):
     return np.abs(c - t).sum(axis=(1, 2)) / np.abs(t).sum(axis=(1, 2))
 
 
+def oracle_f32(case, nthreads=8, want_final=False):
+    """FP32 oracle run in the device kernels' evaluation order: the same
+    algorithm as the reference-order oracle (which tests/test_oracle.py pins
+    to the reference's golden traces), with the 5-term contractions as fused
+    multiply-adds and the divergence weights hprime * w rounded once, as the
+    CUDA kernels compute them.  The checker of the CUDA path: with the
+    evaluation order shared, the two agree to FP32 round-off at any size,
+    where the reference-order FP32 run differs from both by its own rounding
+    (up to 5e-5 in long-run velocity and acceleration, as far from FP64 as
+    the device order is)."""
+    from dataclasses import replace
+
+    from oracle import runner
+    return runner.run(replace(case, device_order=True), "f32", nthreads=nthreads, want_final=want_final)
+
+
 def rel_l2(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)

@@ -1,9 +1,9 @@
 """3D elastic CUDA path against the 3D oracle and the reference's dim3 golden
 traces.
 
-Tolerances: displacement relative L2 <= 1e-5 against the oracle FP32;
-velocity and acceleration max(1e-5, 2 x the oracle's FP32-vs-FP64 gap);
-golden traces sum|d|/sum|ref| < 1e-3 per station.
+Tolerances (fixed): displacement and velocity relative L2 <= 1e-5 against
+the oracle FP32, acceleration <= 1e-4 (FP32 noise floor, as in
+test_gpu_parity); golden traces sum|d|/sum|ref| < 1e-3 per station.
 """
 import numpy as np
 import pytest
@@ -27,8 +27,8 @@ def product3d(case, epb=0, types=TYPES, variant=0):
     return sim, sim.seismograms()
 
 
-def tol(kind, f32, f64):
-    return 1e-5 if kind == "displacement" else max(1e-5, 2.0 * rel_l2(f32, f64))
+def tol(kind, f32=None, f64=None):
+    return 1e-5 if kind in ("displacement", "velocity") else 1e-4
 
 
 def test_3d_golden_fixture(sfg_lib, oracle_lib):
