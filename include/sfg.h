@@ -216,6 +216,37 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
  * mid-step (sfg_reset_fields after). */
 int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms_per_launch);
 
+/* ---- step-wise interface: the reference's kernel facade ----
+ * One phase per call, in the reference's granularity, on the handle's own
+ * fields; a host loop that calls them in time_marching<forward>::run's order
+ * (predictor of every medium, update_wavefields and corrector of the acoustic
+ * medium, then of the elastic medium, then compute_seismograms) gives
+ * sfg_run's seismograms and fields bit for bit.  Single-shot handles; the
+ * calls are asynchronous on the handle's stream (sfg_synchronize to wait);
+ * the handle's own step count is not advanced (the caller passes istep).
+ *   sfg_predictor        newmark_impl::predictor_phase_impl
+ *                        core/specfem/timescheme/newmark.tpp:64-128: u += dt v +
+ *                        dt^2/2 a, v += dt/2 a, a = 0; returns the degrees of
+ *                        freedom updated (nglob * ncomp of the medium, 0 when absent)
+ *   sfg_update_wavefields domain_kernels::update_wavefields<medium>(istep)
+ *                        include/kokkos_kernels/domain_kernels.hpp:72-141: coupling
+ *                        with the other medium, sources of step istep, stiffness
+ *                        with Stacey / free surface, division by the mass matrix;
+ *                        returns the elements updated (the medium's nspec)
+ *   sfg_corrector        newmark_impl::corrector_phase_impl newmark.tpp:10-62:
+ *                        v += dt/2 a; returns nglob * ncomp
+ *   sfg_compute_seismograms domain_kernels::compute_seismograms(isig_step)
+ *                        domain_kernels.hpp:189-203: sample isig of every receiver
+ * frechet_kernels::compute_derivatives (include/kokkos_kernels/frechet_kernels.hpp:
+ * 37-49) has no step-wise counterpart: it accumulates per step against a
+ * backward wavefield that the reference reconstructs by running Newmark
+ * backwards, which the discrete adjoint here replaces by checkpoints and
+ * recomputation; sfg_adjoint_gradient runs the whole combined simulation. */
+int sfg_predictor(sfg_handle *h, int medium);
+int sfg_update_wavefields(sfg_handle *h, int medium, int istep);
+int sfg_corrector(sfg_handle *h, int medium);
+int sfg_compute_seismograms(sfg_handle *h, int isig);
+
 /* ---- results ---- */
 int sfg_get_info(const sfg_handle *h, sfg_info *info);
 /* Seismograms [nshots][nsig][ntypes][nrec][2], receiver-angle rotation applied. */

@@ -839,6 +839,38 @@ __global__ void __launch_bounds__(256) k_update_coupled(UpdateArgs El, UpdateArg
   if (El.advance && blockIdx.x == 0 && threadIdx.x == 0) *El.step += 1;
 }
 
+// Step-wise interface (the reference's update_wavefields / corrector phases):
+// a = (sum of the element contributions in colour order + coupling) * M^-1,
+// stored; divide_mass_matrix.tpp:10-65 after compute_coupling.
+template <int NC>
+__global__ void __launch_bounds__(256) k_accel_gather(UpdateArgs A) {
+  const int npts = A.n / NC;
+  for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += gridDim.x * blockDim.x) {
+    float acc[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) acc[c] = 0.f;
+    const int k1 = A.inv_start[g + 1];
+    for (int k = A.inv_start[g]; k < k1; ++k)
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] = acc[c] + A.r[size_t(k) * NC + c];
+    if (g < A.niface) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) acc[c] += coupling_term(A, g, c);
+    }
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+      const size_t i = size_t(g) * NC + c;
+      A.a_store[i] = __fmul_rn(acc[c], A.minv[i]);
+    }
+  }
+}
+
+// Newmark corrector phase v += dt/2 a (newmark.tpp:10-62).
+__global__ void __launch_bounds__(256) k_correct(float *__restrict__ v, const float *__restrict__ a, int n, float dt2) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    v[i] = newmark_correct(v[i], a[i], dt2);
+}
+
 // Pending predictor of a run that ended on a corrector-only update.
 __global__ void __launch_bounds__(256) k_predict(float *__restrict__ u, float *__restrict__ v,
                                                  const float *__restrict__ a, int n, float dt,
@@ -870,6 +902,11 @@ struct RecArgs {
   const int *__restrict__ step;
   float *__restrict__ seis;            // [nsig][ntypes][nrec_total][2]
   Quad quad;
+  // the end-of-step fields are final (corrected v, stored a: the step-wise
+  // interface): read them instead of reconstructing from the accumulator
+  const float *__restrict__ a;
+  int final_fields;
+  int isig_fixed;                      // sample index given by the caller (-1: from the step counter)
 };
 
 __device__ __forceinline__ float warp_sum(float x) {
@@ -897,9 +934,12 @@ __device__ __forceinline__ float rec_accel(const RecArgs &A, int g, int c) {
 // accumulator (plus the coupling term on interface points).
 __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
   __shared__ float sf[3][NP];
-  const int step = *A.step;
-  if (step % A.nsb != 0) return;
-  const int isig = step / A.nsb;
+  int isig = A.isig_fixed;
+  if (isig < 0) {
+    const int step = *A.step;
+    if (step % A.nsb != 0) return;
+    isig = step / A.nsb;
+  }
   if (isig >= A.nsig) return;
   const int r = A.rec_list[blockIdx.x];
   const int ce = A.rec_elem[r];
@@ -972,8 +1012,8 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
           float val = 0.f;
           switch (A.types[t]) {
             case 0: val = A.u[k]; break;
-            case 1: val = newmark_correct(A.v[k], rec_accel(A, g, c), A.dt2); break;
-            default: val = rec_accel(A, g, c); break;
+            case 1: val = A.final_fields ? A.v[k] : newmark_correct(A.v[k], rec_accel(A, g, c), A.dt2); break;
+            default: val = A.final_fields ? A.a[k] : rec_accel(A, g, c); break;
           }
           o[c] = warp_sum(h * val);
         }
@@ -987,10 +1027,10 @@ __global__ void __launch_bounds__(32) k_receivers(RecArgs A) {
     return;
   }
   // acoustic: displacement-like outputs are rho^-1 grad(field); pressure = -chi_dd
-  const float a = rec_accel(A, g, 0);
+  const float a = A.final_fields ? A.a[g] : rec_accel(A, g, 0);
   if (on) {
     sf[0][q] = A.u[g];
-    sf[1][q] = newmark_correct(A.v[g], a, A.dt2);
+    sf[1][q] = A.final_fields ? A.v[g] : newmark_correct(A.v[g], a, A.dt2);
     sf[2][q] = a;
   }
   __syncwarp();

@@ -572,6 +572,9 @@ sfg::dev::RecArgs rec_args(sfg_handle *h, int medium) {
   R.step = h->d_step;
   R.seis = h->d_seis;
   R.quad = h->quad;
+  R.a = D.a;
+  R.final_fields = 0;
+  R.isig_fixed = -1;
   return R;
 }
 
@@ -1747,6 +1750,93 @@ int sfg_step_noalloc(sfg_handle *h, int istep, float *u, float *v, float *a) {
       h->err = "sfg_step_noalloc: the displacement became NaN or Inf";
       return int(SFG_ERR_NONFINITE);
     }
+    return int(SFG_OK);
+  });
+}
+
+// ------------------------------------------------- step-wise interface ---
+// The granularity of the reference's kernel facade: Newmark predictor and
+// corrector phases per medium (newmark.tpp:10-128), update_wavefields per
+// medium (domain_kernels.hpp:72-141: coupling, sources, stiffness, division
+// by the mass matrix) and compute_seismograms (:189-203).  They run the
+// owner-computes element kernel restricted to one medium and keep the fields
+// in the reference's phase states, so a host loop that calls them in the
+// reference's order reproduces sfg_run bit for bit.
+
+int sfg_predictor(sfg_handle *h, int medium) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (h->asmb.nshots != 1) { h->err = "the step-wise interface runs single-shot handles"; return int(SFG_ERR_UNSUPPORTED); }
+    if (medium != SFG_MEDIUM_ACOUSTIC && medium != SFG_MEDIUM_ELASTIC) return int(SFG_ERR_ARG);
+    if (!h->state_final) { h->err = "fields are mid-step; end the run with sfg_step first"; return int(SFG_ERR_STATE); }
+    DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    if (D.nspec == 0) return 0;
+    launch_predict_medium(h, D, h->stream);
+    SFG_CUDA(cudaMemsetAsync(D.a, 0, D.values() * sizeof(float), h->stream));
+    SFG_CUDA(cudaGetLastError());
+    return int(D.values());
+  });
+}
+
+int sfg_update_wavefields(sfg_handle *h, int medium, int istep) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (h->asmb.nshots != 1) { h->err = "the step-wise interface runs single-shot handles"; return int(SFG_ERR_UNSUPPORTED); }
+    if ((medium != SFG_MEDIUM_ACOUSTIC && medium != SFG_MEDIUM_ELASTIC) || istep < 0) return int(SFG_ERR_ARG);
+    DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    DevMedium &O = medium == SFG_MEDIUM_ELASTIC ? h->ac : h->el;
+    if (D.nspec == 0) return 0;
+    cudaStream_t s = h->stream;
+    sfg::dev::k_set_step<<<1, 1, 0, s>>>(h->d_step, istep);
+    // element contributions of this medium only (sources and Stacey in the epilogue)
+    const DevMedium none{};
+    if (medium == SFG_MEDIUM_ELASTIC) launch_stiffness(h, h->el, none, h->d_step, s, 3);
+    else launch_stiffness(h, none, h->ac, h->d_step, s, 3);
+    // coupling and division by the mass matrix: a stored for the corrector
+    sfg::dev::UpdateArgs U = update_args(h, D, O, medium, false, false);
+    U.inv_start = D.inv_start;
+    U.r = D.r;
+    U.a_store = D.a;
+    const int npts = int(D.values()) / D.ncomp;
+    switch (D.ncomp) {
+      case 1: sfg::dev::k_accel_gather<1><<<grid_for(npts), 256, 0, s>>>(U); break;
+      case 2: sfg::dev::k_accel_gather<2><<<grid_for(npts), 256, 0, s>>>(U); break;
+      case 3: sfg::dev::k_accel_gather<3><<<grid_for(npts), 256, 0, s>>>(U); break;
+      default: sfg::dev::k_accel_gather<4><<<grid_for(npts), 256, 0, s>>>(U); break;
+    }
+    SFG_CUDA(cudaGetLastError());
+    return D.nspec;
+  });
+}
+
+int sfg_corrector(sfg_handle *h, int medium) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (h->asmb.nshots != 1) { h->err = "the step-wise interface runs single-shot handles"; return int(SFG_ERR_UNSUPPORTED); }
+    if (medium != SFG_MEDIUM_ACOUSTIC && medium != SFG_MEDIUM_ELASTIC) return int(SFG_ERR_ARG);
+    DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+    if (D.nspec == 0) return 0;
+    const int n = int(D.values());
+    sfg::dev::k_correct<<<grid_for(n), 256, 0, h->stream>>>(D.v, D.a, n, float(h->asmb.dt) / 2.0f);
+    SFG_CUDA(cudaGetLastError());
+    return n;
+  });
+}
+
+int sfg_compute_seismograms(sfg_handle *h, int isig) {
+  return guarded(h, [&]() {
+    if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
+    if (h->asmb.nshots != 1) { h->err = "the step-wise interface runs single-shot handles"; return int(SFG_ERR_UNSUPPORTED); }
+    if (isig < 0 || isig >= h->asmb.nsig) { h->err = "seismogram sample index out of range"; return int(SFG_ERR_ARG); }
+    for (int medium : {SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC}) {
+      const DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
+      if (D.nspec == 0 || D.nrec == 0) continue;
+      sfg::dev::RecArgs R = rec_args(h, medium);
+      R.final_fields = 1;
+      R.isig_fixed = isig;
+      sfg::dev::k_receivers<<<D.nrec, 32, 0, h->stream>>>(R);
+    }
+    SFG_CUDA(cudaGetLastError());
     return int(SFG_OK);
   });
 }

@@ -95,6 +95,10 @@ EXPORTS = {
     "sfg_forward_checkpointed": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "sfg_adjoint_gradient": ([C.c_void_p, _fp, _fp, _fp, _fp], C.c_int),
     "sfg_step_noalloc": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "sfg_predictor": ([C.c_void_p, C.c_int], C.c_int),
+    "sfg_update_wavefields": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
+    "sfg_corrector": ([C.c_void_p, C.c_int], C.c_int),
+    "sfg_compute_seismograms": ([C.c_void_p, C.c_int], C.c_int),
 }
 
 _lib = None

@@ -30,7 +30,7 @@ def test_nonconforming_golden_parity(sfg_lib, oracle_lib):
     assert np.all(np.isfinite(seis))
     assert np.abs(seis[:, 0, :2]).max() > 0               # elastic receivers, reached through the interface
     for t, kind in enumerate(TYPES):
-        tol = tolerance(kind, acoustic=True)   # acoustic-elastic model
+        tol = tolerance(kind, medium="coupled")
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
     assert reference_metric(seis[:, 0], traces).max() < 1e-2
 
@@ -47,7 +47,7 @@ def test_nonconforming_synthetic_parity(sfg_lib, oracle_lib):
     _, seis = product_run(case, types=TYPES)
     assert np.abs(ref[:, 0, :4]).max() > 0
     for t, kind in enumerate(TYPES):
-        tol = tolerance(kind, acoustic=True)   # acoustic-elastic model
+        tol = tolerance(kind, medium="coupled")
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
 
 

@@ -1,13 +1,20 @@
 """Parity of the CUDA path (through the C ABI) with the CPU oracle.
 
-Tolerances (fixed, relative L2, CUDA FP32 against oracle FP32):
-* elastic displacement and velocity seismograms and final wavefields: 1e-5;
-* acceleration, pressure (elastic and acoustic), every output of an acoustic
-  medium (derived from the potential) and the Cosserat rotation types: 1e-4.
-  These sit on the FP32 noise floor: the oracle's own FP32 run is 2-5e-5 from
-  its FP64 run for them, a change of summation order alone moves acoustic
-  traces by 1.2-1.4e-5, and two FP32 evaluations of different operation
-  order differ by up to about 1.4 times their FP32 error;
+Tolerances (fixed, relative L2, CUDA FP32 against oracle FP32), by medium of
+the receivers and output; the bounds above 1e-5 sit on the FP32 noise floor
+that the oracle itself shows (its FP32 run against its FP64 run, and two
+FP32 runs that differ only in summation order):
+* elastic displacement and velocity, final wavefields: 1e-5;
+* elastic acceleration and pressure, Cosserat rotation and curl, and every
+  output of coupled models (receivers in both media): 1e-4 (FP32 vs FP64
+  2-5e-5);
+* acoustic displacement (rho^-1 grad of the potential): 1e-4 (two summation
+  orders differ by 1.3e-5);
+* acoustic velocity, acceleration and pressure: 5e-3 (on the free-surface
+  acoustic fixture FP32 vs FP64 is 9.5e-5, 1.4e-3 and 1.2e-4, two summation
+  orders differ by 1.3e-4, 2.0e-3 and 1.8e-4);
+* Cosserat intrinsic rotation (rotation minus half the curl, a
+  cancellation): 5e-3 (FP32 vs FP64 7.7e-4);
 * against the reference's golden traces: the reference's own metric
   sum|d|/sum|ref| per station < 1e-3 (newmark_tests.cpp:331-373).
 The run is deterministic (colour-ordered assembly): two runs agree bitwise.
@@ -28,17 +35,23 @@ FIXTURES = ["HomogeneousElasticDomain", "HomogeneousElasticDomainStaceyDirichlet
             "HomogeneousIsotropicCosseratDomainNu0", "AcousticElasticCoupledDomain"]
 
 
-TOL_DV = 1e-5   # elastic displacement and velocity, final fields
-TOL_AP = 1e-4   # acceleration, pressure, acoustic-medium outputs, rotation types
+TOL_DV = 1e-5      # elastic displacement and velocity, final fields
+TOL_AP = 1e-4      # elastic acceleration / pressure, rotation, curl, coupled models, acoustic displacement
+TOL_NOISY = 5e-3   # acoustic velocity / acceleration / pressure, Cosserat intrinsic rotation
 
 
-def tolerance(kind, f32=None, f64=None, acoustic=False):
-    """The fixed bound of an output (see the module docstring).  The FP32 and
-    FP64 oracle results are accepted for the callers' convenience; the bound
-    does not depend on them."""
-    if kind in ("displacement", "velocity") and not acoustic:
-        return TOL_DV
-    return TOL_AP
+def tolerance(kind, f32=None, f64=None, medium="elastic"):
+    """The fixed bound of an output (see the module docstring) for receivers
+    in an elastic, acoustic or coupled model.  The FP32 and FP64 oracle
+    results are accepted for the callers' convenience; the bound does not
+    depend on them."""
+    if kind == "intrinsic_rotation":
+        return TOL_NOISY
+    if medium == "acoustic":
+        return TOL_AP if kind == "displacement" else TOL_NOISY
+    if medium == "coupled":
+        return TOL_AP
+    return TOL_DV if kind in ("displacement", "velocity") else TOL_AP
 
 
 @pytest.mark.parametrize("name", FIXTURES)
@@ -51,7 +64,8 @@ def test_golden_fixture_parity(sfg_lib, oracle_lib, name):
     got = seis[:, 0]
     assert np.all(np.isfinite(got))
     elastic = bool(np.all(case.mesh.mat_medium == 1))
-    tol = TOL_DV if elastic else tolerance("displacement", acoustic=True)
+    acoustic = bool(np.all(case.mesh.mat_medium == 0))
+    tol = TOL_DV if elastic else tolerance("displacement", medium="acoustic" if acoustic else "coupled")
     assert rel_l2(got, ref) <= tol, (rel_l2(got, ref), tol)
     assert reference_metric(got, traces).max() < 1e-3
 
@@ -92,7 +106,7 @@ def test_coupled_small_parity(sfg_lib, oracle_lib):
     assert np.all(np.isfinite(seis))
     assert np.abs(ref[:, 0]).max() > 0
     for t, kind in enumerate(types):
-        tol = tolerance(kind, acoustic=True)   # receivers in both media
+        tol = tolerance(kind, medium="coupled")
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
 
 
@@ -105,7 +119,7 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
     ref64 = runner.run(case, "f64", nthreads=8)["seis"]
     _, seis = product_run(case, types=types)
     for t, kind in enumerate(types):
-        tol = tolerance(kind, acoustic=True)
+        tol = tolerance(kind, medium="acoustic")
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
 
 
@@ -272,10 +286,9 @@ COSSERAT = {
 @pytest.mark.parametrize("name", list(COSSERAT))
 def test_cosserat_parity(sfg_lib, oracle_lib, name):
     """Isotropic Cosserat P-SV-T fixtures (displacement + rotation, couple
-    stress): every seismogram type against the oracle, displacement at 1e-5,
-    the others (time derivatives and displacement gradients) at max(1e-5,
-    twice the oracle's own FP32-vs-FP64 difference); colour passes and
-    owner-computes give the same bits."""
+    stress): every seismogram type against the oracle at the fixed bounds of
+    its class (module docstring); colour passes and owner-computes give the
+    same bits."""
     from oracle import runner
     if name == "cosserat_80x60_stacey":
         from test_oracle import cosserat_80x60

@@ -10,11 +10,13 @@ Per configuration and output the test measures and records:
 
 * CUDA FP32 vs oracle FP32 (device order, and reference order for
   configurations 1 and 2): displacement seismograms and elastic final fields
-  <= 1e-5; velocity, acceleration, pressure and the
-  acoustic potential <= 1e-4.  The second bound is the measured FP32 noise
-  floor of long runs: over thousands of steps each FP32 evaluation is 4-5e-5
-  from FP64 in these outputs, and two FP32 runs of different rounding differ
-  by about 1.4 times that (up to 6e-5);
+  <= 1e-5; velocity, elastic acceleration and the
+  acoustic potential <= 1e-4; acceleration and pressure of the coupled model
+  (acoustic-medium time derivatives) <= 5e-3.  The looser bounds are the
+  measured FP32 noise floor: over thousands of steps each FP32 evaluation is
+  4-5e-5 from FP64 in velocity and acceleration, two FP32 runs of different
+  rounding differ by about 1.4 times that (up to 6e-5), and acoustic
+  accelerations carry FP32 errors up to 1.4e-3 (see test_gpu_parity);
 * CUDA FP32 vs FP64 <= 1.25 x (oracle FP32 vs FP64) + 1e-6: the CUDA build is
   as accurate as a CPU FP32 build of the reference.
 
@@ -44,14 +46,17 @@ from conftest import oracle_f32, rel_l2, workload_case
 pytestmark = pytest.mark.gpu
 
 NT = max(1, os.cpu_count() or 1)
-TOL_DV = 1e-5   # displacement seismograms, elastic final fields
-TOL_AP = 1e-4   # velocity, acceleration, pressure, acoustic potential (FP32 noise floor)
+TOL_DV = 1e-5      # displacement seismograms, elastic final fields
+TOL_AP = 1e-4      # velocity, elastic acceleration, acoustic potential (FP32 noise floor)
+TOL_NOISY = 5e-3   # acceleration and pressure with receivers in an acoustic medium
 
 
-def bound(quantity):
+def bound(quantity, coupled=False):
     base = quantity.split(":")[0]
     if base == "displacement" or (base == "field" and "acoustic" not in quantity):
         return TOL_DV
+    if coupled and base in ("acceleration", "pressure"):
+        return TOL_NOISY
     return TOL_AP
 
 
@@ -74,7 +79,7 @@ def check(config, quantity, got, dev32, f64, ref32=None):
     if ref32 is not None:
         row["cuda_vs_oracle_f32_reference_order"] = rel_l2(got, ref32)
         row["oracle_f32_reference_order_vs_f64"] = rel_l2(ref32, f64)
-    row["bound"] = bound(quantity)
+    row["bound"] = bound(quantity, coupled=config.startswith("2 "))
     record(row)
     assert row["cuda_vs_oracle_f32_device_order"] <= row["bound"], row
     if ref32 is not None:
