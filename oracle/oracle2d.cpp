@@ -1263,6 +1263,177 @@ struct Sim {
       for (int c = 0; c < std::min(nc, 2); ++c) out[c] += R.h[q] * f[size_t(ib[q]) * nc + c];
   }
 
+  // ---------------------------------------------------------------------
+  // The reference's combined (adjoint + backward) simulation of an isotropic
+  // elastic P-SV model and its Frechet kernels
+  // (core/specfem/solver/time_marching.tpp:133-264,
+  //  include/kokkos_kernels/impl/compute_material_derivatives.tpp:14-153,
+  //  include/medium/dim2/elastic/isotropic/frechet_derivative.hpp:55-181).
+  //
+  // One elastic update on fields (u, v, a): the given sources at istep, the
+  // element forces, M^-1.  mode 0: plain; 1: record the contributions of the
+  // elements that carry Stacey points (forward run); 2: replay them instead
+  // of computing those elements (backward run,
+  // compute_stiffness_interaction.tpp:123-137, stored at :238-242).
+  std::vector<uint8_t> st_elem;                 // element carries Stacey points
+  std::vector<int> st_slot;                     // its slot in the replay buffer
+  std::vector<T> replay;                        // [nstep][nst_elem][25][2]
+  int nst_elem = 0;
+
+  void update_elastic(std::vector<T> &u, std::vector<T> &v, std::vector<T> &a, int istep,
+                      const std::vector<Src> &sources, int mode) {
+    for (const auto &S : sources) {
+      const int *ib = &ibool[size_t(S.ispec) * NP];
+      for (int q = 0; q < NP; ++q)
+        for (int c = 0; c < 2; ++c) a[size_t(ib[q]) * 2 + c] += S.stf[istep] * S.arr[c][q];
+    }
+    for (int e = 0; e < nspec; ++e) {
+      if (medium[e] != MED_ELASTIC) continue;
+      T *rec = nullptr;
+      if (mode != 0 && st_elem[e]) rec = &replay[((size_t(istep) * nst_elem + st_slot[e]) * NP) * 2];
+      if (mode == 2 && rec) {
+        for (int q = 0; q < NP; ++q)
+          for (int c = 0; c < 2; ++c) a[size_t(ibool[size_t(e) * NP + q]) * 2 + c] += rec[q * 2 + c];
+        continue;
+      }
+      int q = 0;
+      stiffness_element(e, 2, u, v, [&](int g, const T *acc) {
+        for (int c = 0; c < 2; ++c) {
+          a[size_t(g) * 2 + c] += acc[c];
+          if (rec) rec[q * 2 + c] = acc[c];
+        }
+        ++q;
+      });
+    }
+    for (int g = 0; g < nglob; ++g)
+      if (is_el_glob[g])
+        for (int c = 0; c < 2; ++c) a[size_t(g) * 2 + c] *= minv_e[size_t(g) * 2 + c];
+  }
+
+  // Element gradient of a field at every point of element e: du[q][c][j] =
+  // d u_c / d x_j (include/algorithms/gradient.hpp:40-82).  With `add` the
+  // xi / gamma derivatives of `add` are summed in before the Jacobian map, as
+  // the reference's two-field gradient does with its shared accumulators
+  // (gradient.hpp:296-317).
+  void element_grad(int e, const std::vector<T> &f, const std::vector<T> *add, T du[NP][2][2]) const {
+    const int *ib = &ibool[size_t(e) * NP];
+    for (int iz = 0; iz < NG; ++iz)
+      for (int ix = 0; ix < NG; ++ix) {
+        const int q = iz * NG + ix;
+        const size_t p = size_t(e) * NP + q;
+        T dxi[2] = {0, 0}, dga[2] = {0, 0};
+        for (int l = 0; l < NG; ++l)
+          for (int c = 0; c < 2; ++c) {
+            dxi[c] += hp[ix][l] * f[size_t(ib[iz * NG + l]) * 2 + c];
+            dga[c] += hp[iz][l] * f[size_t(ib[l * NG + ix]) * 2 + c];
+            if (add) {
+              dxi[c] += hp[ix][l] * (*add)[size_t(ib[iz * NG + l]) * 2 + c];
+              dga[c] += hp[iz][l] * (*add)[size_t(ib[l * NG + ix]) * 2 + c];
+            }
+          }
+        for (int c = 0; c < 2; ++c) {
+          du[q][c][0] = xix[p] * dxi[c] + gax[p] * dga[c];
+          du[q][c][1] = xiz[p] * dxi[c] + gaz[p] * dga[c];
+        }
+      }
+  }
+
+  // adj [nstep][nrec][2]: adjoint source time functions of the receivers
+  // (point forces at the receiver locations, applied at step istep as the
+  // iteration runs istep = nstep-1 .. 0).  quirk: the backward derivatives
+  // include the adjoint field's (the reference's two-field gradient).
+  // reconstruct: the reference's reverse-time backward field; else the
+  // forward run's own snapshots (to separate reconstruction error).
+  // Out: kernels rho, mu, kappa [nspec][25] and the quadrature weight
+  // w_x w_z |J| of every element point.
+  void adjoint_compat(const double *adj, int quirk, int reconstruct, double *out_rho, double *out_mu,
+                      double *out_kappa, double *out_w) {
+    if (ncomp_el != 2 || in.aniso || in.cosserat || in.poro)
+      throw std::runtime_error("the reference-compatible adjoint covers isotropic elastic P-SV media");
+    for (int e = 0; e < nspec; ++e)
+      if (medium[e] != MED_ELASTIC) throw std::runtime_error("the reference-compatible adjoint covers one elastic medium");
+    const int nstep = in.nstep;
+    st_elem.assign(nspec, 0);
+    st_slot.assign(nspec, -1);
+    nst_elem = 0;
+    for (int e = 0; e < nspec; ++e) {
+      for (int q = 0; q < NP; ++q) st_elem[e] |= st_tag[size_t(e) * NP + q];
+      if (st_elem[e]) st_slot[e] = nst_elem++;
+    }
+    replay.assign(size_t(nstep) * nst_elem * NP * 2, T(0));
+    std::vector<std::vector<T>> snaps;
+    // forward run (sources of the configuration), recording the Stacey elements
+    for (int istep = 0; istep < nstep; ++istep) {
+      predictor(ue, ve, ae);
+      update_elastic(ue, ve, ae, istep, srcs, 1);
+      corrector(ve, ae);
+      if (!reconstruct) snaps.push_back(ue);
+    }
+    const std::vector<T> fu = ue, fv = ve, fa = ae;   // the forward wavefield buffer
+    // adjoint sources: one point force per receiver and component
+    std::vector<Src> asrc;
+    for (int r = 0; r < in.nrec; ++r)
+      for (int c = 0; c < 2; ++c) {
+        Src S{};
+        S.ispec = recs[r].ispec;
+        S.medium = MED_ELASTIC;
+        S.ncomp = 2;
+        for (int q = 0; q < NP; ++q) { S.arr[c][q] = recs[r].h[q]; S.arr[1 - c][q] = T(0); }
+        S.stf.resize(nstep);
+        for (int k = 0; k < nstep; ++k) S.stf[k] = T(adj[(size_t(k) * in.nrec + r) * 2 + c]);
+        asrc.push_back(S);
+      }
+    const size_t ne = size_t(nglob) * 2;
+    std::vector<T> uA(ne, T(0)), vA(ne, T(0)), aA(ne, T(0)), uB(ne, T(0)), vB(ne, T(0)), aB(ne, T(0));
+    const size_t nloc = size_t(nspec) * NP;
+    std::vector<double> krho(nloc, 0.0), kmu(nloc, 0.0), kkap(nloc, 0.0);
+    const T dt2 = dt / T(2.0), dtsq2 = dt * dt / T(2.0);
+    T dA[NP][2][2], dB[NP][2][2];
+    for (int istep = nstep - 1; istep >= 0; --istep) {
+      // adjoint time step (newmark.tpp apply_*_phase_forward on the adjoint field)
+      predictor(uA, vA, aA);
+      update_elastic(uA, vA, aA, istep, asrc, 0);
+      corrector(vA, aA);
+      // backward time step: -dt, -dt/2, +dt^2/2 (newmark.tpp:222-267)
+      if (reconstruct) {
+        for (size_t i = 0; i < ne; ++i) {
+          uB[i] += T(-1) * dt * vB[i] + dtsq2 * aB[i];
+          vB[i] += T(-1) * dt2 * aB[i];
+          aB[i] = 0;
+        }
+        update_elastic(uB, vB, aB, istep, srcs, 2);
+        for (size_t i = 0; i < ne; ++i) vB[i] += T(-1) * dt2 * aB[i];
+        if (istep == nstep - 1) { uB = fu; vB = fv; aB = fa; }   // the buffer copy (time_marching.tpp:214-216)
+      } else {
+        uB = snaps[size_t(istep)];
+      }
+      // Frechet kernels of this step
+      for (int e = 0; e < nspec; ++e) {
+        element_grad(e, uA, nullptr, dA);
+        element_grad(e, uB, quirk ? &uA : nullptr, dB);
+        const int *ib = &ibool[size_t(e) * NP];
+        for (int q = 0; q < NP; ++q) {
+          const size_t p = size_t(e) * NP + q;
+          const T kap = lp2m(p) - p_mu[p];           // kappa2D = lambda + mu (frechet_derivative.hpp:77)
+          const T ad_xx = dA[q][0][0], ad_zz = dA[q][1][1], ad_xz = T(0.5) * (dA[q][1][0] + dA[q][0][1]);
+          const T b_xx = dB[q][0][0], b_zz = dB[q][1][1], b_xz = T(0.5) * (dB[q][1][0] + dB[q][0][1]);
+          const T kk = (ad_xx + ad_zz) * (b_xx + b_zz);
+          const T mm = ad_xx * b_xx + ad_zz * b_zz + T(2.0) * ad_xz * b_xz - T(1.0 / 3.0) * kk;
+          const size_t g = size_t(ib[q]) * 2;
+          const T rr = aA[g] * uB[g] + aA[g + 1] * uB[g + 1];
+          kkap[p] += double(T(-1.0) * kap * dt * kk);
+          kmu[p] += double(T(-2.0) * p_mu[p] * dt * mm);
+          krho[p] += double(T(-1.0) * p_rho[p] * dt * rr);
+        }
+      }
+    }
+    for (size_t p = 0; p < nloc; ++p) {
+      out_rho[p] = krho[p]; out_mu[p] = kmu[p]; out_kappa[p] = kkap[p];
+      const int q = int(p % NP), iz = q / NG, ix = q - iz * NG;
+      out_w[p] = double(w[ix]) * double(w[iz]) * double(jac[p]);
+    }
+  }
+
   void run(double *seis, int nthreads) {
     const int nsb = std::max(1, in.nstep_between_samples);
     int isig = 0;
@@ -1342,6 +1513,21 @@ int oracle2d_locate(const OracleInput2D *in, int precision64, double x, double z
     }
     return 0;
   } catch (const std::exception &) {
+    return -1;
+  }
+}
+
+// The reference's combined adjoint simulation and Frechet kernels (FP64).
+int oracle2d_adjoint_compat_f64(const OracleInput2D *in, const double *adj, int quirk, int reconstruct,
+                                double *rho_kl, double *mu_kl, double *kappa_kl, double *weight,
+                                char *error, int error_len) {
+  try {
+    Sim<double> s(*in);
+    s.setup();
+    s.adjoint_compat(adj, quirk, reconstruct, rho_kl, mu_kl, kappa_kl, weight);
+    return 0;
+  } catch (const std::exception &ex) {
+    if (error && error_len > 0) std::snprintf(error, size_t(error_len), "%s", ex.what());
     return -1;
   }
 }

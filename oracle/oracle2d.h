@@ -74,6 +74,16 @@ typedef struct OracleOutput2D {
 int oracle2d_run_f32(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
 int oracle2d_run_f64(const OracleInput2D *in, OracleOutput2D *out, int nthreads);
 int oracle2d_count_nglob(const OracleInput2D *in);
+/* The reference's combined simulation (adjoint field from the adjoint
+ * sources adj [nstep][nrec][2] at the receivers, backward field by reverse
+ * Newmark with Stacey replay, or the forward snapshots when reconstruct = 0)
+ * and its Frechet kernels rho, mu, kappa per element GLL point [nspec][25];
+ * quirk = 1 adds the adjoint derivatives into the backward ones as the
+ * reference's two-field gradient does.  weight: w_x w_z |J| per point.
+ * Isotropic elastic P-SV models; FP64. */
+int oracle2d_adjoint_compat_f64(const OracleInput2D *in, const double *adj, int quirk, int reconstruct,
+                                double *rho_kl, double *mu_kl, double *kappa_kl, double *weight,
+                                char *error, int error_len);
 int oracle2d_locate(const OracleInput2D *in, int precision64, double x, double z, int *ispec,
                     double *xi, double *gamma);
 void oracle_gll(double *z, double *w, double *hprime);

@@ -230,11 +230,10 @@ def cosserat_points(case):
     return np.ascontiguousarray(np.repeat(per[:, None, :], 25, axis=1))
 
 
-def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: bool = False):
-    """Run the oracle; returns dict with 'seis' [nsig, ntypes, nrec, 2], 't0', 'times'."""
+def _make_input(case: Case2D, keep: list):
+    """OracleInput2D of a case (arrays kept alive in `keep`); also returns the
+    seismogram type codes and the sampling interval."""
     m = case.mesh
-    L = lib()
-    keep = []
 
     def arr(x, dt):
         a = np.ascontiguousarray(x, dtype=dt)
@@ -300,6 +299,17 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     adj = nonconforming_records(m)
     inp.nadj = len(adj)
     inp.adjacency = _ptr(arr(adj, np.int32), _ip) if len(adj) else None
+    return inp, types, nsb
+
+
+def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: bool = False):
+    """Run the oracle; returns dict with 'seis' [nsig, ntypes, nrec, 2], 't0', 'times'."""
+    m = case.mesh
+    L = lib()
+    keep = []
+    inp, types, nsb = _make_input(case, keep)
+    t0 = inp.t0
+    poro, cos = poro_points(case), cosserat_points(case)
     nsig = (case.nstep + nsb - 1) // nsb
     seis = np.zeros((nsig, len(types), len(case.rec_x), 2))
     out = OracleOutput2D()
@@ -321,6 +331,35 @@ def run(case: Case2D, precision: str = "f32", nthreads: int = 1, want_final: boo
     times = np.arange(nsig) * (case.dt * nsb) + t0
     return {"seis": seis, "t0": t0, "times": times, "final": final, "nglob": out.nglob,
             "loop_seconds": out.loop_seconds}
+
+
+def adjoint_compat(case: Case2D, adj, quirk: bool = False, reconstruct: bool = True):
+    """The reference's combined adjoint simulation and Frechet kernels (FP64)
+    of an isotropic elastic P-SV case: adjoint sources adj [nstep][nrec][2]
+    at the receivers; kernels rho, mu, kappa [nspec, 25] (mesh element order)
+    as the reference accumulates them (kappa with respect to kappa2D =
+    lambda + mu), and the quadrature weight w_x w_z |J| of every point.
+    quirk: the backward field's derivatives include the adjoint field's, as
+    the reference's two-field gradient computes them; reconstruct: the
+    reference's reverse-time backward field (else the forward snapshots)."""
+    L = lib()
+    keep = []
+    inp, _, _ = _make_input(case, keep)
+    n = case.mesh.nspec * 25
+    out = {k: np.zeros((case.mesh.nspec, 25)) for k in ("rho", "mu", "kappa", "weight")}
+    a = np.ascontiguousarray(adj, np.float64)
+    if a.shape != (case.nstep, len(case.rec_x), 2):
+        raise ValueError("adjoint sources must be [nstep, nrec, 2]")
+    err = C.create_string_buffer(256)
+    fn = L.oracle2d_adjoint_compat_f64
+    fn.argtypes = [C.POINTER(OracleInput2D), _dp, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_char_p, C.c_int]
+    fn.restype = C.c_int
+    rc = fn(C.byref(inp), _ptr(a, _dp), int(quirk), int(reconstruct), _ptr(out["rho"], _dp), _ptr(out["mu"], _dp),
+            _ptr(out["kappa"], _dp), _ptr(out["weight"], _dp), err, 256)
+    if rc != 0:
+        raise RuntimeError(err.value.decode())
+    assert out["rho"].size == n
+    return out
 
 
 # ------------------------------------------------ reference fixtures ---
