@@ -161,11 +161,25 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   }
   const int bs = act ? __ldg(A.bc_slot + e) : -1;
   const int src = act ? __ldg(A.src_head + e) : -1;
+  const int iz = q / NG, ix = q - iz * NG;
+  float dxi[NC], dga[NC];
+  if (EK == 0) {
+    // P-SV: the two components' contractions paired (FFMA2, rounding as fmaf)
+    float2 *su2 = reinterpret_cast<float2 *>(smem);   // [E][25] (u_x, u_z)
+    su2[le * NP + q] = make_float2(uu[0], uu[NC - 1]);
+    __syncthreads();
+    const float2 *fu = su2 + le * NP;
+    float2 px = make_float2(0.f, 0.f), pg = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      px = fma2(f2(shp[ix * NG + l]), fu[iz * NG + l], px);
+      pg = fma2(f2(shp[iz * NG + l]), fu[l * NG + ix], pg);
+    }
+    dxi[0] = px.x; dxi[NC - 1] = px.y; dga[0] = pg.x; dga[NC - 1] = pg.y;
+  } else {
 #pragma unroll
   for (int c = 0; c < NC; ++c) su[(le * NC + c) * NP + q] = uu[c];
   __syncthreads();
-  const int iz = q / NG, ix = q - iz * NG;
-  float dxi[NC], dga[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     dxi[c] = 0.f;
@@ -176,6 +190,7 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
       dxi[c] = fmaf(shp[ix * NG + l], fu[iz * NG + l], dxi[c]);
       dga[c] = fmaf(shp[iz * NG + l], fu[l * NG + ix], dga[c]);
     }
+  }
   }
   // stress (P-SV: isotropic Hooke with lambda+2mu = c0; SH: sigma = mu grad u_y)
   float Sx[NC], Sz[NC];
@@ -236,6 +251,23 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
     Sx[0] = mu * (xix * dxi[0] + gax * dga[0]);
     Sz[0] = mu * (xiz * dxi[0] + gaz * dga[0]);
   }
+  float a[NC];
+  if (EK == 0) {
+    float2 *sF2 = reinterpret_cast<float2 *>(smem + sizeof(float) * NP * E * NC);   // [E][2][25]
+    sF2[(le * 2 + 0) * NP + q] = make_float2(jac * (Sx[0] * xix + Sz[0] * xiz), jac * (Sx[NC - 1] * xix + Sz[NC - 1] * xiz));
+    sF2[(le * 2 + 1) * NP + q] = make_float2(jac * (Sx[0] * gax + Sz[0] * gaz), jac * (Sx[NC - 1] * gax + Sz[NC - 1] * gaz));
+    __syncthreads();
+    if (!act) return;
+    const float2 *g0 = sF2 + (le * 2 + 0) * NP, *g1 = sF2 + (le * 2 + 1) * NP;
+    float2 t1 = make_float2(0.f, 0.f), t2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      t1 = fma2(g0[iz * NG + l], f2(shpw[l * NG + ix]), t1);
+      t2 = fma2(g1[l * NG + ix], f2(shpw[l * NG + iz]), t2);
+    }
+    a[0] = -(sw[iz] * t1.x + sw[ix] * t2.x);
+    a[NC - 1] = -(sw[iz] * t1.y + sw[ix] * t2.y);
+  } else {
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     sF[((le * NC + c) * 2 + 0) * NP + q] = jac * (Sx[c] * xix + Sz[c] * xiz);
@@ -243,7 +275,6 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
   }
   __syncthreads();
   if (!act) return;
-  float a[NC];
 #pragma unroll
   for (int c = 0; c < NC; ++c) {
     const float *f0 = sF + ((le * NC + c) * 2 + 0) * NP;
@@ -255,6 +286,7 @@ __device__ __forceinline__ void elastic_block(const StiffArgs &S, const MedArgs 
       t2 = fmaf(f1[l * NG + ix], shpw[l * NG + iz], t2);
     }
     a[c] = -(sw[iz] * t1 + sw[ix] * t2);
+  }
   }
   if (EK == 3) a[NC - 1] -= (csxz - cszx) * (sw[ix] * sw[iz] * jac);   // couple stress
   if (EK == 4) {
@@ -354,25 +386,25 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
   su[le * NP + q] = chi;
   __syncthreads();
   const int iz = q / NG, ix = q - iz * NG;
-  float dxi = 0.f, dga = 0.f;
+  // the two derivative directions paired (FFMA2, rounding as fmaf)
+  float2 d = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int l = 0; l < NG; ++l) {
-    dxi = fmaf(shp[ix * NG + l], su[le * NP + iz * NG + l], dxi);
-    dga = fmaf(shp[iz * NG + l], su[le * NP + l * NG + ix], dga);
-  }
+  for (int l = 0; l < NG; ++l)
+    d = fma2(make_float2(shp[ix * NG + l], shp[iz * NG + l]),
+             make_float2(su[le * NP + iz * NG + l], su[le * NP + l * NG + ix]), d);
+  const float dxi = d.x, dga = d.y;
   const float s0 = rhoinv * (xix * dxi + gax * dga);
   const float s1 = rhoinv * (xiz * dxi + gaz * dga);
   sF[(le * 2 + 0) * NP + q] = jac * (s0 * xix + s1 * xiz);
   sF[(le * 2 + 1) * NP + q] = jac * (s0 * gax + s1 * gaz);
   __syncthreads();
   if (!act) return;
-  float t1 = 0.f, t2 = 0.f;
+  float2 t = make_float2(0.f, 0.f);
 #pragma unroll
-  for (int l = 0; l < NG; ++l) {
-    t1 = fmaf(sF[(le * 2 + 0) * NP + iz * NG + l], shpw[l * NG + ix], t1);
-    t2 = fmaf(sF[(le * 2 + 1) * NP + l * NG + ix], shpw[l * NG + iz], t2);
-  }
-  float a = -(sw[iz] * t1 + sw[ix] * t2);
+  for (int l = 0; l < NG; ++l)
+    t = fma2(make_float2(sF[(le * 2 + 0) * NP + iz * NG + l], sF[(le * 2 + 1) * NP + l * NG + ix]),
+             make_float2(shpw[l * NG + ix], shpw[l * NG + iz]), t);
+  float a = -(sw[iz] * t.x + sw[ix] * t.y);
   if (bs >= 0) {
     const size_t k = size_t(bs) * NP + q;
     const float wq = A.bc_w[k];
@@ -392,8 +424,10 @@ __device__ __forceinline__ void acoustic_block(const StiffArgs &S, const MedArgs
 
 // One launch per colour: blocks [0, el.nblocks) run elastic elements of the
 // colour, the following ac.nblocks blocks acoustic ones.
+// occupancy held at the warp limit of an SM (64 warps): the kernel is bound
+// by memory latency, so registers may not grow past what that allows
 template <int E, int EK, bool LOCAL>
-__global__ void __launch_bounds__(NP * E) k_stiffness(StiffArgs S) {
+__global__ void __launch_bounds__(NP * E, 64 / ((NP * E + 31) / 32)) k_stiffness(StiffArgs S) {
   __shared__ __align__(16) unsigned char smem[sizeof(float) * NP * E * (EK == 4 ? 12 : EK == 3 ? 9 : 6)];
   __shared__ float shp[NP], shpw[NP], sw[NG];
   load_quad(S.quad, shp, shpw, sw, threadIdx.x);

@@ -1,11 +1,12 @@
 """Shot sharding with the real library: two processes, each with its own
 Simulation2D on the GPU, gloo collectives between them.
 
-The survey helpers (specfempp_b200.survey) must give exactly what one process
-gives for the whole survey: the gathered seismograms of every shot, and the
-summed L2 misfit and rho / kappa / mu gradient of every source.  The kernels
-are deterministic, so every source's traces and gradient are the same bits
-in either process; only the final float64 sum over sources differs in order.
+The survey helpers (specfempp_b200.survey) must give what one process gives
+for the whole survey: the gathered seismograms of every shot (the same bits:
+the forward kernels are deterministic), and the summed L2 misfit and rho /
+kappa / mu gradient of every source (to FP32 round-off: each process times
+the launch shape of its reverse kernels itself, and the float64 sum over
+sources runs in another order).
 """
 import os
 import socket
@@ -90,4 +91,4 @@ def test_two_processes_on_real_simulations_match_one_process(tmp_path, sfg_lib):
         assert np.array_equal(z["full"], obs.astype(np.float32))   # gathered in shot order
         assert np.isclose(float(z["L"]), L1, rtol=1e-12)
         for k in range(3):
-            assert np.allclose(z[f"g{k}"], g1[k], rtol=1e-10, atol=1e-12 * np.abs(g1[k]).max())
+            assert np.linalg.norm(z[f"g{k}"] - g1[k]) <= 1e-5 * np.linalg.norm(g1[k]), k
