@@ -162,7 +162,8 @@ def bench_batched(args, world, barrier, max_over_ranks):
 
     def make(nshots, srcs):
         sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=w.nstep, nshots=nshots, point_rho=w.point_rho,
-                               point_vp=w.point_vp, point_vs=w.point_vs)
+                               point_vp=w.point_vp, point_vs=w.point_vs,
+                               kernel_variant=args.batched_variant if nshots > 1 else 0)
         sim.set_sources(srcs)
         sim.set_receivers(w.rec_x, w.rec_z)
         sim.initialize()
@@ -186,6 +187,19 @@ def bench_batched(args, world, barrier, max_over_ranks):
     barrier()
     ms_1 = max_over_ranks(one.run_timed(steps))
     del one
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        # the reference runs one shot at a time: 50 steps of one shot on the
+        # host cores (oracle, FP32, full mesh and model)
+        from oracle import runner
+        threads = os.cpu_count() or 1
+        case = runner.Case2D(mesh=w.mesh, sources=[replace(w.sources[0], shot=0)], rec_x=w.rec_x, rec_z=w.rec_z,
+                             dt=w.dt, nstep=50, point_rho=w.point_rho, point_vp=w.point_vp,
+                             point_vs=w.point_vs)
+        r = runner.run(case, "f32", nthreads=threads)
+        cpu = {"value": 50 / r["loop_seconds"], "unit": "shot-steps/s", "cores": threads, "kind": "port",
+               "sample": f"50 time steps of one shot of elastic_grf_{nx}x{nz}, FP32 C++ restatement of the "
+                         f"reference on {threads} host threads ({r['loop_seconds']:.2f} s)"}
     rate_b = S_total * steps / (ms_b / 1e3)
     rate_1 = world * steps / (ms_1 / 1e3)
     per_shot_b = STEP_B_GLOB + STEP_B_LOCAL * inf.nspec * 25 / (inf.nglob * S)
@@ -197,7 +211,8 @@ def bench_batched(args, world, barrier, max_over_ranks):
             "gll_pt_updates_per_s_batched": rate_b * inf.nglob,
             "kernel_variant": variant, **kern,
             "batched_frac_of_hbm": per_shot_b * inf.nglob * S / (ms_b / steps / 1e3) / 1e9 / peaks()[0],
-            "timing": "CUDA events, graph-replayed steps, inputs larger than L2"}
+            "timing": "CUDA events, graph-replayed steps, inputs larger than L2",
+            "cpu_baseline": cpu}
 
 
 def bench_adjoint(args, world, barrier, max_over_ranks):
@@ -252,11 +267,14 @@ def bench_adjoint(args, world, barrier, max_over_ranks):
     t_fwd = max_over_ranks(min(forward_s() for _ in range(2)))
     t_grad = max_over_ranks(min(gradient_s()[0] for _ in range(2)))
     out = {"workload": f"elastic_adjoint_{nx}x{nz}", "nglob": inf.nglob, "steps": nstep,
-           "sources": len(srcs), "checkpoint_interval": aw.interval, "forward_s": t_fwd,
+           "sources": len(srcs), "checkpoint_interval": aw.interval,
+           "segments": -(-nstep // aw.interval), "segments_kept_from_forward": sim.adjoint_buffers(),
+           "segment_budget": "default: 60% of the free device memory", "forward_s": t_fwd,
            "gradient_s": t_grad, "cost_ratio": t_grad / t_fwd,
            "gradient_gll_pt_steps_per_s": inf.nglob * nstep * len(srcs) / t_grad,
            "timing": "wall clock around synchronous calls; forward = plain runs of every source; "
-                     "gradient = per source checkpointed forward + segment recompute + reverse sweep"}
+                     "gradient = per source checkpointed forward (recording the segments the buffers "
+                     "hold) + recompute of the other segments + reverse sweep"}
     if args.adjoint_fd > 0:
         xmax, zmax = 25.0 * nx, 25.0 * nz
         pert = meshgen.smooth_perturbations(w.mesh, xmax, zmax, args.adjoint_fd, 1000.0, seed=7)
@@ -328,6 +346,18 @@ def bench_3d(args, world, barrier, max_over_ranks):
            "step_frac_of_hbm": alg * inf.nglob / (ms_fl / steps / 1e3) / 1e9 / peak,
            "finite": bool(finite)}
     sim.close()
+    rank = int(os.environ.get("RANK", "0"))
+    if rank == 0 and not args.no_cpu_baseline:
+        # a bounded sample: 5 steps of the full 67.6 M-point model on the host
+        # cores (the oracle's 3D restatement, FP32)
+        from oracle import runner3d
+        threads = os.cpu_count() or 1
+        case = runner3d.Case3D(w.mesh, w.sources, w.rec_xyz, w.dt, 5)
+        r = runner3d.run(case, "f32", nthreads=threads)
+        out["cpu_baseline"] = {"value": inf.nglob * 5 / r["loop_seconds"], "unit": "GLL-pt/s", "cores": threads,
+                               "kind": "port",
+                               "sample": f"5 time steps of elastic3d_{nx}x{ny}x{nz}, FP32 C++ restatement of the "
+                                         f"reference on {threads} host threads ({r['loop_seconds']:.2f} s)"}
     return out
 
 
@@ -416,6 +446,8 @@ def main():
                     help="elements of the batched-shot model, NXxNZ (config 3: 1000x500)")
     ap.add_argument("--batched-shots", type=int, default=32)
     ap.add_argument("--batched-steps", type=int, default=30)
+    ap.add_argument("--batched-variant", type=int, default=0,
+                    help="assembly of the batched run (1 colour passes, 3 owner-computes, 5 fused tiles; 0 autotuned)")
     ap.add_argument("--kernel-variant", type=int, default=0,
                     help="fix the element-kernel variant of the headline run (0 = autotuned)")
     ap.add_argument("--elements-per-block", type=int, default=0,

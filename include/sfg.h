@@ -279,10 +279,23 @@ int sfg_set_model2d(sfg_handle *h, const float *rho, const float *kappa, const f
  * steps on the device (seismograms as sfg_run).  Replaces the reference's
  * forward-wavefield dump for adjoint runs (include/io/wavefield/writer.tpp). */
 int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval);
+/* Device memory for the adjoint's segment buffers (each holds one checkpoint
+ * interval of recorded forward states).  The forward run records its last
+ * segments into them on the way, as many as the buffers hold, so that the
+ * reverse sweep recomputes only the earlier segments; bytes = 0 (the
+ * default) takes 60% of the device memory free when the buffers are
+ * allocated (at the next sfg_forward_checkpointed); at least two buffers are
+ * always kept.  Gradients do not depend on it (bit for bit).  No counterpart
+ * in the reference, whose combined run reads the whole forward wavefield
+ * back from storage. */
+int sfg_set_adjoint_budget(sfg_handle *h, size_t bytes);
+/* Segment buffers allocated by the last sfg_forward_checkpointed (0 before). */
+int sfg_adjoint_buffers(sfg_handle *h);
 /* Gradient of a misfit L with respect to rho, kappa, mu at every GLL point
  * ([nspec][25], database element order) given seis_grad = dL/d(seismogram)
- * [nsteps][nrec][2]: the reverse sweep recomputes each checkpoint segment and
- * runs the discrete adjoint of the time step.  Replaces the reference's
+ * [nsteps][nrec][2]: the reverse sweep recomputes each checkpoint segment
+ * that the forward run did not keep and runs the discrete adjoint of the
+ * time step.  Replaces the reference's
  * combined adjoint/backward run and compute_material_derivatives
  * (core/specfem/solver/time_marching.tpp:133-264,
  *  include/kokkos_kernels/impl/compute_material_derivatives.tpp:14-153). */

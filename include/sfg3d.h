@@ -4,9 +4,10 @@
  * 8-node hexahedra (arbitrary control-node coordinates), isotropic elastic
  * media given per GLL point, force and moment-tensor sources, receivers, the
  * Newmark time loop captured in CUDA graphs.  Status codes and sfg_options
- * are those of sfg.h (elements_per_block 1, 2 or 4 fixes the element
- * kernel's launch shape, 0 lets the autotuner choose; all give the same
- * bits; kernel_variant is ignored).
+ * are those of sfg.h (elements_per_block fixes the element kernel's launch
+ * shape: 1, 2 or 4 elements per block with one thread per element GLL point,
+ * 8 or 16 with one thread per column of five points; 0 lets the autotuner
+ * choose; all give the same bits; kernel_variant is ignored).
  *
  * It replaces, for this mesh class, the reference's dim3 forward path:
  * the assembly (core/specfem/assembly/ dim3 containers), the element kernel
@@ -52,7 +53,7 @@ typedef struct sfg_info3d {
   size_t device_bytes;
   int elements_per_block;
   int kernels_per_step;
-  int kernel_variant;           /* element-kernel form in use (1) */
+  int kernel_variant;           /* element-kernel form in use: 1 point form, 2 column form */
 } sfg_info3d;
 
 /* Reference: specfem::assembly::assembly<dim3> construction from the mesh. */

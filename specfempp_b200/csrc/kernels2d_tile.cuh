@@ -240,7 +240,6 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
   for (; j < nmine; ++j) {
     const int st = j % S;
     unsigned char *stage = stages + st * A.stage_bytes;
-    const int t = b + j * G;
     float2 u_next = make_float2(0.f, 0.f);
     if (j + 1 < nmine) {
       const int sn = (j + 1) % S;
@@ -248,8 +247,10 @@ __device__ __forceinline__ void tile_loop(const TileArgs &A, const TileMed &M, c
       if (__syncthreads_or(!ok)) {
         if (tid == 0) {
           atomicExch(A.flag, 2);
-          // copies issued and not yet waited for: tiles j + 2 .. j + S - 1
-          for (int k = j + 2; k < nmine && k < j + S; ++k) mbar_wait(bar + (k % S), uint32_t((k / S) & 1));
+          // copies issued and not yet waited for: tiles j + 2 up to the last
+          // issued, S - 1 before the first refill (iteration 1), j + S - 2 after
+          const int issued = j == 0 ? S : j + S - 1;
+          for (int k = j + 2; k < nmine && k < issued; ++k) mbar_wait(bar + (k % S), uint32_t((k / S) & 1));
         }
         return;
       }
@@ -421,6 +422,7 @@ __global__ void __launch_bounds__(TILE_P, 2) k_tile(TileArgs A) {
 struct BndMed {
   const float *r;              // TileMed::r: one slot per colour and boundary point
   const int *b_side;           // side slot of a boundary point (-1: none), or null
+  const unsigned char *b_mask; // colours of the elements touching a boundary point
   int nb, niface, sh0, ncol;
 };
 

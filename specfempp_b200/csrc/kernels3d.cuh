@@ -72,6 +72,15 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
   const int src = act ? __ldg(A.src_head + e) : -1;
 #pragma unroll
   for (int c = 0; c < 3; ++c) su[le][c][q] = act ? A.u[size_t(g) * 3 + c] : 0.f;
+  // this point's Lagrange coefficients in registers: the points of a warp
+  // differ, so indexed constant-bank loads would serialize
+  float hx[NG], hy[NG], hz[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    hx[l] = c3_hp[ix * NG + l];
+    hy[l] = c3_hp[iy * NG + l];
+    hz[l] = c3_hp[iz * NG + l];
+  }
   __syncthreads();
   float du[3][3];  // du[c][j] = d u_c / d x_j
 #pragma unroll
@@ -79,9 +88,9 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
     float d0 = 0.f, d1 = 0.f, d2 = 0.f;
 #pragma unroll
     for (int l = 0; l < NG; ++l) {
-      d0 = fmaf(c3_hp[ix * NG + l], su[le][c][(iz * NG + iy) * NG + l], d0);
-      d1 = fmaf(c3_hp[iy * NG + l], su[le][c][(iz * NG + l) * NG + ix], d1);
-      d2 = fmaf(c3_hp[iz * NG + l], su[le][c][(l * NG + iy) * NG + ix], d2);
+      d0 = fmaf(hx[l], su[le][c][(iz * NG + iy) * NG + l], d0);
+      d1 = fmaf(hy[l], su[le][c][(iz * NG + l) * NG + ix], d1);
+      d2 = fmaf(hz[l], su[le][c][(l * NG + iy) * NG + ix], d2);
     }
 #pragma unroll
     for (int j = 0; j < 3; ++j) du[c][j] = d0 * gi[0 * 3 + j] + d1 * gi[1 * 3 + j] + d2 * gi[2 * 3 + j];
@@ -99,6 +108,13 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
 #pragma unroll
     for (int k = 0; k < 3; ++k)
       sF[le][c][k][q] = jac * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    hx[l] = c3_hpw[l * NG + ix];
+    hy[l] = c3_hpw[l * NG + iy];
+    hz[l] = c3_hpw[l * NG + iz];
+  }
+  const float wx = c3_w[ix], wy = c3_w[iy], wz = c3_w[iz];
   __syncthreads();
   if (!act) return;
   float a[3];
@@ -107,11 +123,11 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
     float t1 = 0.f, t2 = 0.f, t3 = 0.f;
 #pragma unroll
     for (int l = 0; l < NG; ++l) {
-      t1 = fmaf(sF[le][c][0][(iz * NG + iy) * NG + l], c3_hpw[l * NG + ix], t1);
-      t2 = fmaf(sF[le][c][1][(iz * NG + l) * NG + ix], c3_hpw[l * NG + iy], t2);
-      t3 = fmaf(sF[le][c][2][(l * NG + iy) * NG + ix], c3_hpw[l * NG + iz], t3);
+      t1 = fmaf(sF[le][c][0][(iz * NG + iy) * NG + l], hx[l], t1);
+      t2 = fmaf(sF[le][c][1][(iz * NG + l) * NG + ix], hy[l], t2);
+      t3 = fmaf(sF[le][c][2][(l * NG + iy) * NG + ix], hz[l], t3);
     }
-    a[c] = -(c3_w[iz] * c3_w[iy] * t1 + c3_w[iz] * c3_w[ix] * t2 + c3_w[iy] * c3_w[ix] * t3);
+    a[c] = -(wz * wy * t1 + wz * wx * t2 + wy * wx * t3);
   }
   if (bs >= 0) {
     const float *C = A.bc_c + size_t(bs) * 6 * NQ + q;
@@ -135,6 +151,141 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
   A.r[sl] = a[0];
   A.r[sl + 1] = a[1];
   A.r[sl + 2] = a[2];
+}
+
+// Column form of the element kernel: one thread per (x, y) column of GLL
+// points of an element, the column's five points (z = 0..4) in registers, E
+// elements per block (25 E threads).  The z-direction contractions of the
+// gradient and of the divergence run on the column's registers with
+// warp-uniform coefficients; the x- and y-direction ones read the element's
+// displacement and F arrays in shared memory, whose x rows are padded to 8
+// floats so that a row is one float4 load plus one float load.  Per point the
+// operations and their order are those of k_stiffness3d, so both kernels give
+// the same bits.  Dynamic shared memory: E x (3 + 6) x 25 x 8 floats.
+constexpr int RP3 = 8;
+template <int E>
+__global__ void __launch_bounds__(NG * NG * E, E <= 8 ? 3 : 1) k_stiffness3d_col(Elem3Args A) {
+  extern __shared__ __align__(16) float dyn3[];
+  const int tid = threadIdx.x;
+  const int le = tid / (NG * NG), cq = tid - le * (NG * NG);
+  const int iy = cq / NG, ix = cq - iy * NG;
+  const int e = blockIdx.x * E + le;
+  const bool act = e < A.nspec;
+  const size_t pe = size_t(act ? e : 0) * NQ;
+  float *su = dyn3 + size_t(le) * 9 * NG * NG * RP3;   // [c][z*5 + y][x]
+  float *sF = su + 3 * NG * NG * RP3;                  // [c][k = 0, 1][z*5 + y][x]
+  float uz[3][NG];
+  int g[NG];
+#pragma unroll
+  for (int iz = 0; iz < NG; ++iz) g[iz] = act ? __ldg(A.ibool + pe + (iz * NG + iy) * NG + ix) : 0;
+#pragma unroll
+  for (int iz = 0; iz < NG; ++iz)
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      uz[c][iz] = act ? A.u[size_t(g[iz]) * 3 + c] : 0.f;
+      su[(c * NG * NG + iz * NG + iy) * RP3 + ix] = uz[c][iz];
+    }
+  float hx[NG], hy[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    hx[l] = c3_hp[ix * NG + l];
+    hy[l] = c3_hp[iy * NG + l];
+  }
+  __syncthreads();
+  float fz[3][NG];   // F[c][2] of the column's points
+#pragma unroll
+  for (int iz = 0; iz < NG; ++iz) {
+    const size_t p = pe + (iz * NG + iy) * NG + ix;
+    float gi[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) gi[k] = __ldg(A.g9 + size_t(k) * A.nloc + p);
+    const float jac = __ldg(A.jac + p), c0 = __ldg(A.c0 + p), mu = __ldg(A.mu + p);
+    float du[3][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float *row = su + (c * NG * NG + iz * NG + iy) * RP3;
+      const float4 r4 = *reinterpret_cast<const float4 *>(row);
+      const float rv[NG] = {r4.x, r4.y, r4.z, r4.w, row[4]};
+      float d0 = 0.f, d1 = 0.f, d2 = 0.f;
+#pragma unroll
+      for (int l = 0; l < NG; ++l) {
+        d0 = fmaf(hx[l], rv[l], d0);
+        d1 = fmaf(hy[l], su[(c * NG * NG + iz * NG + l) * RP3 + ix], d1);
+        d2 = fmaf(c3_hp[iz * NG + l], uz[c][l], d2);
+      }
+#pragma unroll
+      for (int j = 0; j < 3; ++j) du[c][j] = d0 * gi[0 * 3 + j] + d1 * gi[1 * 3 + j] + d2 * gi[2 * 3 + j];
+    }
+    const float lam = c0 - 2.f * mu;
+    float sig[3][3];
+    sig[0][0] = c0 * du[0][0] + lam * (du[1][1] + du[2][2]);
+    sig[1][1] = c0 * du[1][1] + lam * (du[0][0] + du[2][2]);
+    sig[2][2] = c0 * du[2][2] + lam * (du[0][0] + du[1][1]);
+    sig[0][1] = sig[1][0] = mu * (du[0][1] + du[1][0]);
+    sig[0][2] = sig[2][0] = mu * (du[0][2] + du[2][0]);
+    sig[1][2] = sig[2][1] = mu * (du[1][2] + du[2][1]);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+#pragma unroll
+      for (int k = 0; k < 2; ++k)
+        sF[((c * 2 + k) * NG * NG + iz * NG + iy) * RP3 + ix] =
+            jac * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
+      fz[c][iz] = jac * (sig[c][0] * gi[6] + sig[c][1] * gi[7] + sig[c][2] * gi[8]);
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < NG; ++l) {
+    hx[l] = c3_hpw[l * NG + ix];
+    hy[l] = c3_hpw[l * NG + iy];
+  }
+  const float wx = c3_w[ix], wy = c3_w[iy];
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  const int src = act ? __ldg(A.src_head + e) : -1;
+  __syncthreads();
+  if (!act) return;
+#pragma unroll
+  for (int iz = 0; iz < NG; ++iz) {
+    const int q = (iz * NG + iy) * NG + ix;
+    const float wz = c3_w[iz];
+    float a[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      const float *row = sF + ((c * 2 + 0) * NG * NG + iz * NG + iy) * RP3;
+      const float4 r4 = *reinterpret_cast<const float4 *>(row);
+      const float rv[NG] = {r4.x, r4.y, r4.z, r4.w, row[4]};
+      float t1 = 0.f, t2 = 0.f, t3 = 0.f;
+#pragma unroll
+      for (int l = 0; l < NG; ++l) {
+        t1 = fmaf(rv[l], hx[l], t1);
+        t2 = fmaf(sF[((c * 2 + 1) * NG * NG + iz * NG + l) * RP3 + ix], hy[l], t2);
+        t3 = fmaf(fz[c][l], c3_hpw[l * NG + iz], t3);
+      }
+      a[c] = -(wz * wy * t1 + wz * wx * t2 + wy * wx * t3);
+    }
+    if (bs >= 0) {
+      const float *C = A.bc_c + size_t(bs) * 6 * NQ + q;
+      const float cxx = C[0], cyy = C[NQ], czz = C[2 * NQ], cxy = C[3 * NQ], cxz = C[4 * NQ], cyz = C[5 * NQ];
+      if (cxx != 0.f || cyy != 0.f || czz != 0.f) {
+        const size_t gv = size_t(g[iz]) * 3;
+        const float vx = A.v[gv], vy = A.v[gv + 1], vz = A.v[gv + 2];
+        a[0] -= cxx * vx + cxy * vy + cxz * vz;
+        a[1] -= cxy * vx + cyy * vy + cyz * vz;
+        a[2] -= cxz * vx + cyz * vy + czz * vz;
+      }
+    }
+    if (src >= 0) {
+      const int step = *A.step;
+      for (int s = src; s >= 0; s = A.src_next[s]) {
+        const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[c] += f * A.src_arr[(size_t(s) * 3 + c) * NQ + q];
+      }
+    }
+    const size_t sl = size_t(__ldg(A.slot + pe + q)) * 3;
+    A.r[sl] = a[0];
+    A.r[sl + 1] = a[1];
+    A.r[sl + 2] = a[2];
+  }
 }
 
 struct Update3Args {

@@ -21,6 +21,7 @@
 #include "kernels2d_adjoint.cuh"
 #include "kernels2d_tma.cuh"
 #include "kernels2d_tile.cuh"
+#include "kernels2d_tile_batched.cuh"
 
 namespace {
 
@@ -104,6 +105,7 @@ struct DevMedium {
   int2 *t_rp = nullptr;
   float *t_r = nullptr;
   int *b_side = nullptr;
+  unsigned char *b_mask = nullptr;  // per boundary point: the colours of the elements touching it
   std::vector<int> rp_off, rp_cnt;  // per tile (host)
 };
 
@@ -114,13 +116,18 @@ struct AdjointState {
   int nstep = 0, interval = 0, ncheck = 0;
   size_t nvals = 0, nloc = 0, stride = 0, nglob = 0;
   float *ckpt = nullptr;                        // [ncheck][u, v, a][nvals + 4]
-  // two segment buffers, so that the recompute of one segment overlaps the
-  // reverse sweep of the next (streams: the handle's and rstream)
-  float *seg_u = nullptr, *seg_a = nullptr;     // [2][interval][stride]
-  float *seg_v = nullptr;                       // [2][interval][vstride]: v~ at the Stacey points
+  // nbuf >= 2 segment buffers (as many as the memory budget holds, at most
+  // one per segment): the checkpointed forward run records its last nbuf
+  // segments on the way, so that only the earlier ones are recomputed, each
+  // while the reverse sweep of a later one runs (streams: the handle's and
+  // rstream)
+  int nbuf = 0;
+  size_t budget = 0;                            // bytes for segment buffers; 0: the default
+  float *seg_u = nullptr, *seg_a = nullptr;     // [nbuf][interval][stride]
+  float *seg_v = nullptr;                       // [nbuf][interval][vstride]: v~ at the Stacey points
   cudaStream_t rstream = nullptr;
-  cudaEvent_t ev_rec[2] = {nullptr, nullptr}, ev_rev[2] = {nullptr, nullptr};
-  int recorded = -1;                            // segment recorded by the forward run
+  std::vector<cudaEvent_t> ev_rec, ev_rev;      // per buffer
+  int rec_from = -1;                            // segments rec_from.. are held from the forward run (-1: none)
   size_t vstride = 0;
   float *lu = nullptr, *lv = nullptr, *mu = nullptr;
   float *r = nullptr;                           // [nloc][2]
@@ -144,7 +151,7 @@ struct AdjointState {
   sfg::dev::SegRecord *d_rec = nullptr;
   cudaGraphExec_t graph_r1 = nullptr, graph_re = nullptr;  // recording steps
   cudaGraphExec_t graph_rseg = nullptr;         // interval - 1 recording steps
-  cudaGraphExec_t graph_rev[2] = {nullptr, nullptr};  // reverse sweep of a full segment, per buffer
+  std::vector<cudaGraphExec_t> graph_rev;       // reverse sweep of a full segment, per buffer
   int *d_k0 = nullptr;                          // first step of the segment in reverse
   bool forward_done = false;
   int epb = 0;                                  // elements per block of k_adj_elem (timed once)
@@ -208,6 +215,7 @@ struct sfg_handle {
   float *d_side = nullptr;
   int *d_rslot = nullptr;
   sfg::dev::TileArgs tile_layout{};
+  sfg::dev::TileBArgs tileb_layout{};   // batched shots
   int tile_smem = 0, tile_blocks_per_sm = 0;
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
@@ -227,10 +235,9 @@ struct sfg_handle {
     for (auto &g : adj.graph_rev)
       if (g) cudaGraphExecDestroy(g);
     if (adj.d_k0) cudaFree(adj.d_k0);
-    for (int b = 0; b < 2; ++b) {
-      if (adj.ev_rec[b]) cudaEventDestroy(adj.ev_rec[b]);
-      if (adj.ev_rev[b]) cudaEventDestroy(adj.ev_rev[b]);
-    }
+    for (auto *ev : {&adj.ev_rec, &adj.ev_rev})
+      for (cudaEvent_t e : *ev)
+        if (e) cudaEventDestroy(e);
     if (adj.rstream) cudaStreamDestroy(adj.rstream);
     if (adj.graph_re) cudaGraphExecDestroy(adj.graph_re);
     if (graph_k) cudaGraphExecDestroy(graph_k);
@@ -657,13 +664,18 @@ bool receivers_early(const sfg_handle *h, int medium) {
 // Whether the model can run the fused tile kernel: one shot, isotropic P-SV,
 // SH or acoustic media, conforming coupling whose interface points pair one
 // to one (P-SV), seismograms of displacement, velocity, acceleration or
-// pressure.
+// pressure; or S shots (S a multiple of 4) on one isotropic elastic medium
+// with displacement, velocity or acceleration seismograms.
 static_assert(sfg::TILE_E == sfg::dev::TILE_E, "host and device tile sizes differ");
 
 bool compute_tile_ok(const sfg_handle *h) {
   const sfg::Assembly2D &a = h->asmb;
   const sfg::MediumData &E = a.el, &C = a.ac;
-  if (a.nshots != 1) return false;
+  if (a.nshots != 1) {
+    if (a.nshots % 4 != 0 || C.nspec || !E.nspec) return false;
+    for (int t : a.types)
+      if (t > SFG_SEIS_ACCELERATION) return false;
+  }
   if (E.nspec && (E.aniso || E.cosserat || E.poro || E.ncomp > 2)) return false;
   if (!E.cp_start.empty() || !C.cp_start.empty()) return false;
   if (E.nspec && C.nspec && !(h->fuse_ok && E.ncomp == 2)) return false;
@@ -762,7 +774,8 @@ void upload_tiles(sfg_handle *h) {
     }
   }
   DevMem &m = h->mem;
-  h->d_side = m.zeros<float>(size_t(std::max(nslot, 1)) * dv::SIDE_W);
+  const int S = a.nshots;
+  h->d_side = m.zeros<float>(size_t(std::max(nslot, 1)) * dv::SIDE_W * S);
   h->d_rslot = m.upload(rslot);
   for (int med = 0; med < 2; ++med) {
     DevMedium &D = med == 1 ? h->el : h->ac;
@@ -807,11 +820,40 @@ void upload_tiles(sfg_handle *h) {
       D.t_sh = m.upload(sh);
     }
     D.t_rp = m.upload(rp);
-    D.t_r = m.zeros<float>(size_t(std::max(D.nb, 1)) * ncolors(D) * M.ncomp + 4);
+    D.t_r = m.zeros<float>(size_t(std::max(D.nb, 1)) * ncolors(D) * M.ncomp * S + 4);
     D.b_side = m.upload(bside);
+    {
+      std::vector<unsigned char> bm(std::max(D.nb, 1), 0);
+      for (int ce = 0; ce < M.nspec; ++ce)
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const int g = M.ibool[size_t(ce) * sfg::NPTS + q];
+          if (g < M.niface) bm[g] |= static_cast<unsigned char>(1 << M.elem_color[ce]);
+          else if (g >= M.sh0) bm[M.niface + g - M.sh0] |= static_cast<unsigned char>(1 << M.elem_color[ce]);
+        }
+      D.b_mask = m.upload(bm);
+    }
+  }
+  auto al4 = [](int x) { return (x + 3) & ~3; };
+  if (S > 1) {
+    // batched: stages of record + shared-point ids, float4 work arrays and
+    // per-colour float4 accumulators
+    const DevMedium &D = h->el;
+    dv::TileBArgs &L = h->tileb_layout;
+    L.off_sh = D.rec_bytes;
+    L.stage_bytes = (L.off_sh + 4 * al4(std::max(D.max_nsh, 4)) + 15) & ~15;
+    L.work_off = 64 + dv::TILEB_STAGES * L.stage_bytes;
+    L.acc_off = L.work_off + 16 * dv::TILE_E * 3 * D.ncomp * sfg::NPTS;
+    L.kcap = al4(std::max(D.max_nint, 4));
+    h->tile_smem = L.acc_off + 16 * ncolors(D) * D.ncomp * L.kcap;
+    if (h->tile_smem > 227 * 1024) { h->tile_ok = false; return; }
+    auto kern = D.ncomp == 1 ? dv::k_tile_b<1> : dv::k_tile_b<2>;
+    SFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, h->tile_smem));
+    int nb = 0;
+    SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, dv::TILE_P, h->tile_smem));
+    h->tile_blocks_per_sm = std::max(nb, 1);
+    return;
   }
   // shared-memory layout (uniform over the blocks of both media)
-  auto al4 = [](int x) { return (x + 3) & ~3; };
   int rec = 0, fcap = 4, shcap = 4, accw = 4;
   for (const DevMedium *D : {&h->el, &h->ac}) {
     if (!D->t_rec) continue;
@@ -850,14 +892,43 @@ sfg::dev::TileMed tile_med(const DevMedium &D, int ncol, bool store_a) {
 
 sfg::dev::BndMed bnd_med(const DevMedium &D, const sfg::MediumData &M) {
   sfg::dev::BndMed B{};
-  B.r = D.t_r; B.b_side = D.b_side;
+  B.r = D.t_r; B.b_side = D.b_side; B.b_mask = D.b_mask;
   B.nb = D.t_rec ? D.nb : 0; B.niface = M.niface; B.sh0 = M.sh0; B.ncol = ncolors(D);
   return B;
+}
+
+// The batched fused tile kernel (one elastic medium, S shots): work items
+// are (tile, quad of shots), the quads of a tile adjacent in item order so
+// that they run at about the same time and share the record through L2.
+void launch_tile_kernel_b(sfg_handle *h, bool predict, cudaStream_t s) {
+  namespace dv = sfg::dev;
+  const sfg::Assembly2D &a = h->asmb;
+  dv::TileBArgs A = h->tileb_layout;
+  A.el = tile_med(h->el, ncolors(h->el), !predict || h->opt.store_acceleration);
+  A.bel = med_args(h->el);
+  A.src_next = h->d_src_next; A.src_shot = h->d_src_shot; A.src_arr = h->d_src_arr; A.stf = h->d_stf;
+  A.nsrc = a.nsrc; A.nstep = a.nstep; A.step = h->d_step;
+  const float dt = float(a.dt);
+  A.dt = dt; A.dt2 = dt / 2.0f; A.dtsq2 = dt * dt / 2.0f;
+  A.predict = predict ? 1 : 0;
+  A.flag = h->d_flag;
+  A.side = h->d_side;
+  A.S = h->el.S;
+  A.quad = h->quad;
+  const int items = A.el.ntiles * (A.S / 4);
+  const int grid = std::min(h->tile_blocks_per_sm * h->sm_count, items);
+  if (grid <= 0) return;
+  if (h->el.ncomp == 1) dv::k_tile_b<1><<<grid, dv::TILE_P, h->tile_smem, s>>>(A);
+  else dv::k_tile_b<2><<<grid, dv::TILE_P, h->tile_smem, s>>>(A);
 }
 
 // The fused tile kernel of both media.
 void launch_tile_kernel(sfg_handle *h, bool predict, cudaStream_t s) {
   namespace dv = sfg::dev;
+  if (h->asmb.nshots > 1) {
+    launch_tile_kernel_b(h, predict, s);
+    return;
+  }
   const sfg::Assembly2D &a = h->asmb;
   dv::TileArgs A = h->tile_layout;
   A.el = tile_med(h->el, ncolors(h->el), !predict || h->opt.store_acceleration);
@@ -888,6 +959,14 @@ void launch_tile_kernel(sfg_handle *h, bool predict, cudaStream_t s) {
 // Boundary points of both media (advances the step counter).
 void launch_tile_boundary(sfg_handle *h, bool predict, cudaStream_t s) {
   namespace dv = sfg::dev;
+  if (h->asmb.nshots > 1) {
+    dv::UpdateArgs U = update_args(h, h->el, h->ac, SFG_MEDIUM_ELASTIC, predict, true);
+    const dv::BndMed b = bnd_med(h->el, h->asmb.el);
+    const int n = b.nb * (h->el.S / 4);
+    if (h->el.ncomp == 1) dv::k_tile_boundary_b<1><<<grid_for(n), 256, 0, s>>>(U, b, h->d_side, h->el.S);
+    else dv::k_tile_boundary_b<2><<<grid_for(n), 256, 0, s>>>(U, b, h->d_side, h->el.S);
+    return;
+  }
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
   if (has_el && has_ac) {
     dv::UpdateArgs E = update_args(h, h->el, h->ac, SFG_MEDIUM_ELASTIC, predict, true);
@@ -912,7 +991,10 @@ void launch_tile_receivers(sfg_handle *h, cudaStream_t s) {
   for (int med : {SFG_MEDIUM_ACOUSTIC, SFG_MEDIUM_ELASTIC}) {
     const DevMedium &D = med == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
     if (D.nspec == 0 || D.nrec == 0) continue;
-    sfg::dev::k_receivers_side<<<D.nrec, 32, 0, s>>>(rec_args(h, med), h->d_rslot, h->d_side);
+    if (D.S > 1)
+      sfg::dev::k_receivers_side_b<<<D.nrec, 32, 0, s>>>(rec_args(h, med), h->d_rslot, h->d_side, D.S);
+    else
+      sfg::dev::k_receivers_side<<<D.nrec, 32, 0, s>>>(rec_args(h, med), h->d_rslot, h->d_side);
   }
 }
 
@@ -1045,6 +1127,7 @@ void autotune(sfg_handle *h) {
   if (h->asmb.nshots > 1) {
     for (int v : {1, 3})
       if (!fix_v || v == h->variant) cand.push_back({v, 16});
+    if (h->tile_ok && (!fix_v || h->variant == 5)) cand.push_back({5, 16});
   } else {
     for (int v : {1, 2, 3, 4}) {
       // an anisotropic medium has the colour-pass and owner-computes kernels only
@@ -1914,16 +1997,36 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   const int ncheck = (nstep + interval - 1) / interval;
   const int nst = int(adj_data(h).stacey_pt.size());
   const size_t vstride = ((2 * size_t(nst) + 3) / 4) * 4 + 4;
-  if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck) {
+  // segment buffers: as many as the budget holds (default: 60% of the device
+  // memory free before they are allocated), at least 2, at most ncheck
+  const size_t seg_bytes = size_t(interval) * (2 * stride + vstride) * sizeof(float);
+  size_t budget = A.budget;
+  if (budget == 0) {
+    size_t fr = 0, tot = 0;
+    SFG_CUDA(cudaMemGetInfo(&fr, &tot));
+    const size_t held = A.seg_u ? size_t(A.nbuf) * size_t(A.interval) * (2 * A.stride + A.vstride) * sizeof(float) : 0;
+    budget = size_t(0.6 * double(fr + held));
+  }
+  const int nbuf = int(std::max<size_t>(2, std::min<size_t>(size_t(std::max(ncheck, 2)), budget / seg_bytes)));
+  if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck || A.nbuf != nbuf) {
     for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a, &A.seg_v})
       if (*p) { cudaFree(*p); *p = nullptr; }
     A.ckpt = dalloc<float>(size_t(ncheck) * 3 * (nvals + 4));
-    A.seg_u = dalloc<float>(2 * size_t(interval) * stride);
-    A.seg_a = dalloc<float>(2 * size_t(interval) * stride);
-    A.seg_v = dalloc<float>(2 * size_t(interval) * vstride);
-    A.recorded = -1;
-    for (cudaGraphExec_t *g : {&A.graph_rseg, &A.graph_rev[0], &A.graph_rev[1]})
-      if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+    A.seg_u = dalloc<float>(size_t(nbuf) * interval * stride);
+    A.seg_a = dalloc<float>(size_t(nbuf) * interval * stride);
+    A.seg_v = dalloc<float>(size_t(nbuf) * interval * vstride);
+    A.rec_from = -1;
+    if (A.graph_rseg) { cudaGraphExecDestroy(A.graph_rseg); A.graph_rseg = nullptr; }
+    for (cudaGraphExec_t &g : A.graph_rev)
+      if (g) cudaGraphExecDestroy(g);
+    A.graph_rev.assign(nbuf, nullptr);
+    for (auto *ev : {&A.ev_rec, &A.ev_rev}) {
+      for (cudaEvent_t e : *ev)
+        if (e) cudaEventDestroy(e);
+      ev->assign(nbuf, nullptr);
+      for (cudaEvent_t &e : *ev) SFG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    A.nbuf = nbuf;
   }
   A.vstride = vstride;
   A.nvals = nvals;
@@ -2019,10 +2122,6 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     A.d_rec = dalloc<sfg::dev::SegRecord>(1);
     A.d_k0 = dalloc<int>(1);
     SFG_CUDA(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
-    for (int b = 0; b < 2; ++b) {
-      SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rec[b], cudaEventDisableTiming));
-      SFG_CUDA(cudaEventCreateWithFlags(&A.ev_rev[b], cudaEventDisableTiming));
-    }
   }
   sfg::dev::SegRecord rec{A.seg_u, A.seg_a, stride, 0, A.seg_v, vstride, A.st_pt, A.nst, 0};
   SFG_CUDA(cudaMemcpy(A.d_rec, &rec, sizeof(rec), cudaMemcpyHostToDevice));
@@ -2049,12 +2148,23 @@ void save_state(sfg_handle *h, float *dst) {
   SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, D.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
 }
 
+// Segments held from the forward run (the last min(nbuf, ncheck)) and the
+// buffer of segment c: a held segment has its own buffer; a recomputed one
+// takes, alternately, the buffers of the last two held segments, which are
+// the first the reverse sweep frees.
+int held_from(const AdjointState &A) { return A.ncheck - std::min(A.nbuf, A.ncheck); }
+int seg_buffer(const AdjointState &A, int c) {
+  const int c_r = held_from(A), R = A.ncheck - c_r;
+  if (c >= c_r) return c - c_r;
+  return R - 1 - ((c_r - 1 - c) & 1);
+}
+
 // Recompute (or, in the forward run, compute: `seismograms`) segment c from
 // the state in the fields, recording u~, a' and the Stacey v~ of each step
-// into segment buffer c % 2.  Stream-ordered on the handle's stream.
-void record_segment(sfg_handle *h, int c, bool seismograms) {
+// into segment buffer b.  Stream-ordered on the handle's stream.
+void record_segment(sfg_handle *h, int c, bool seismograms, int b) {
   AdjointState &A = h->adj;
-  const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
+  const int k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
   const size_t ob = size_t(b) * A.interval;
   sfg::dev::k_set_segment<<<1, 1, 0, h->stream>>>(A.d_rec, h->d_step, A.seg_u + ob * A.stride,
                                                   A.seg_a + ob * A.stride, A.seg_v + ob * A.vstride, k0);
@@ -2196,18 +2306,30 @@ int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval) {
     const int ret = sfg_reset_fields(h);
     if (ret != SFG_OK) return ret;
     const size_t stride = 3 * (A.nvals + 4);
+    const int c_r = held_from(A);
     for (int c = 0; c < A.ncheck; ++c) {
       save_state(h, A.ckpt + size_t(c) * stride);
-      // the last segment is recorded on the way, so the reverse sweep starts
-      // without recomputing it
-      if (c + 1 == A.ncheck) record_segment(h, c, true);
+      // the last nbuf segments are recorded on the way: the reverse sweep
+      // recomputes only the earlier ones
+      if (c >= c_r) record_segment(h, c, true, seg_buffer(A, c));
       else run_steps(h, std::min(A.interval, nsteps - c * A.interval));
     }
     SFG_CUDA(cudaStreamSynchronize(h->stream));
-    A.recorded = A.ncheck - 1;
+    A.rec_from = c_r;
     A.forward_done = true;
     return int(SFG_OK);
   });
+}
+
+int sfg_set_adjoint_budget(sfg_handle *h, size_t bytes) {
+  return guarded(h, [&]() {
+    h->adj.budget = bytes;
+    return int(SFG_OK);
+  });
+}
+
+int sfg_adjoint_buffers(sfg_handle *h) {
+  return guarded(h, [&]() { return h->adj.seg_u ? h->adj.nbuf : 0; });
 }
 
 int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho, float *grad_kappa,
@@ -2230,8 +2352,8 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       if (A.gtab) cudaFree(A.gtab);
       A.gtab = dalloc<float>(ng);
       A.gtab_cap = ng;
-      for (cudaGraphExec_t *g : {&A.graph_rev[0], &A.graph_rev[1]})
-        if (*g) { cudaGraphExecDestroy(*g); *g = nullptr; }
+      for (cudaGraphExec_t &g : A.graph_rev)
+        if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     }
     const size_t nstage = std::max(ng, A.nsum());
     if (nstage > A.h_stage_cap) {
@@ -2267,12 +2389,12 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     SFG_CUDA(cudaEventRecord(A.ev_rec[0], s));
     SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[0], 0));
     for (int c = A.ncheck - 1; c >= 0; --c) {
-      const int b = c & 1, k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
-      if (!(c == A.ncheck - 1 && A.recorded == c)) {
-        // buffer b is free once the reverse sweep of segment c + 2 is done
+      const int b = seg_buffer(A, c), k0 = c * A.interval, k1 = std::min(k0 + A.interval, A.nstep);
+      if (A.rec_from < 0 || c < A.rec_from) {
+        // buffer b is free once the reverse sweep of its last segment is done
         SFG_CUDA(cudaStreamWaitEvent(s, A.ev_rev[b], 0));
         restore_state(h, A.ckpt + size_t(c) * cstride);
-        record_segment(h, c, false);
+        record_segment(h, c, false, b);
       }
       SFG_CUDA(cudaEventRecord(A.ev_rec[b], s));
       SFG_CUDA(cudaStreamWaitEvent(rs, A.ev_rec[b], 0));
@@ -2294,7 +2416,7 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       SFG_CUDA(cudaEventRecord(A.ev_rev[b], rs));
       SFG_CUDA(cudaGetLastError());
     }
-    A.recorded = -1;
+    A.rec_from = -1;
     SFG_CUDA(cudaStreamSynchronize(rs));
     SFG_CUDA(cudaStreamSynchronize(s));
     h->host_step = A.nstep;

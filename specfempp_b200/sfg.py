@@ -94,6 +94,8 @@ EXPORTS = {
     "sfg_set_model2d": ([C.c_void_p, _fp, _fp, _fp], C.c_int),
     "sfg_forward_checkpointed": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
     "sfg_adjoint_gradient": ([C.c_void_p, _fp, _fp, _fp, _fp], C.c_int),
+    "sfg_set_adjoint_budget": ([C.c_void_p, C.c_size_t], C.c_int),
+    "sfg_adjoint_buffers": ([C.c_void_p], C.c_int),
     "sfg_step_noalloc": ([C.c_void_p, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sfg_predictor": ([C.c_void_p, C.c_int], C.c_int),
     "sfg_update_wavefields": ([C.c_void_p, C.c_int, C.c_int], C.c_int),
@@ -352,6 +354,15 @@ class Simulation2D:
     def forward_checkpointed(self, nsteps, interval):
         self._check(self.lib.sfg_forward_checkpointed(self.h, int(nsteps), int(interval)))
         return self.seismograms()[0, :nsteps, 0]
+
+    def set_adjoint_budget(self, nbytes: int):
+        """Device bytes for the adjoint's segment buffers (0: 60% of the free
+        memory); the forward run keeps as many recorded segments as they hold."""
+        self._check(self.lib.sfg_set_adjoint_budget(self.h, int(nbytes)))
+
+    def adjoint_buffers(self) -> int:
+        """Segment buffers of the last checkpointed forward run (0 before)."""
+        return int(self.lib.sfg_adjoint_buffers(self.h))
 
     def adjoint_gradient(self, seis_grad):
         """dL/d(rho, kappa, mu) per GLL point [nspec, 25] given dL/dseis [nsteps, nrec, 2]."""

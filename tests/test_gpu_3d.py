@@ -74,9 +74,17 @@ def test_3d_absorbing_moment_tensor_vs_oracle(sfg_lib, oracle_lib):
 
 
 def test_3d_launch_shapes_agree_and_deterministic(sfg_lib):
+    """Point form (1, 2, 4 elements per block) and column form (8, 16): the
+    same bits, seismograms and final field, with sources and absorbing
+    faces."""
     case = small_absorbing_case(nstep=120)
-    _, a = product3d(case, epb=1)
+    s1, a = product3d(case, epb=1)
     _, b = product3d(case, epb=4)
+    for e in (8, 16):
+        sc, d = product3d(case, epb=e)
+        assert sc.info().kernel_variant == 2
+        assert np.array_equal(a, d), e
+        assert np.array_equal(s1.field("displacement"), sc.field("displacement")), e
     sim, c = product3d(case, epb=2)
     assert np.array_equal(a, b) and np.array_equal(a, c)
     sim.reset()

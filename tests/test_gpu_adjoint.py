@@ -7,7 +7,8 @@ source and the receivers, and on the absorbing edge (where the Stacey
 impedances depend on the model), against central differences of two forward runs:
 relative error <= 1e-2 (the FP32 forward limits the difference quotient to
 about 1e-3 at a 1% perturbation).  Gradients from different checkpoint
-intervals agree to 1e-5 (only the order of the FP32 time sum differs).
+intervals agree to 1e-5 (only the order of the FP32 time sum differs); the
+memory budget of the recorded segments changes no bit.
 """
 import numpy as np
 import pytest
@@ -92,6 +93,26 @@ def test_checkpoint_interval_invariance(problem):
         assert n > 0
         assert np.linalg.norm(x - y) <= 1e-5 * n
         assert np.linalg.norm(x - z) <= 1e-5 * n
+
+
+def test_segment_budget_gives_the_same_gradient(problem):
+    """Two segment buffers (the forward run keeps its last two segments, the
+    reverse sweep recomputes the others) and the default budget (every
+    segment kept from the forward run) give the same bits; so does a second
+    gradient without a new forward run (everything recomputed)."""
+    w, sim, model, weights = problem
+    nseg = -(-NSTEP // 37)
+    sim.set_adjoint_budget(1)
+    a = gradient(sim, model, weights, 37)
+    assert sim.adjoint_buffers() == 2
+    sim.set_adjoint_budget(0)
+    b = gradient(sim, model, weights, 37)
+    assert sim.adjoint_buffers() == nseg
+    c = sim.adjoint_gradient(weights)
+    for x, y, z in zip(a, b, c):
+        assert np.abs(x).max() > 0
+        assert np.array_equal(x, y)
+        assert np.array_equal(x, z)
 
 
 def test_autograd_function(problem):

@@ -2,7 +2,8 @@
 
 Each shot's arithmetic is the single-shot kernel's, so a batched run must give
 the same bits as running the shots one at a time (seismograms and fields),
-including a partial second tile of 32 shots; shot 0 is also checked against
+including a partial second tile of 32 shots, for the colour-pass,
+owner-computes and fused tile kernels; shot 0 is also checked against
 the CPU oracle (relative L2 <= 1e-5).
 """
 import numpy as np
@@ -30,13 +31,15 @@ def run(w, srcs, nshots, types=("displacement", "velocity"), variant=0):
     return sim
 
 
-@pytest.mark.parametrize("nshots,variant", [(5, 1), (8, 1), (8, 3), (36, 1), (36, 3), (37, 3)])
+@pytest.mark.parametrize("nshots,variant", [(5, 1), (8, 1), (8, 3), (8, 5), (36, 1), (36, 3), (36, 5), (37, 3)])
 def test_batched_equals_single_shots(sfg_lib, nshots, variant):
     from dataclasses import replace
     from specfempp_b200 import meshgen
     w = meshgen.elastic_psv_80x60(nstep=400)
     srcs = shots(nshots)
     batched = run(w, srcs, nshots, variant=variant)
+    if variant == 5:
+        assert batched.info().kernel_variant == 5
     seis_b = batched.seismograms()
     u_b = batched.field("elastic", "displacement")
     assert seis_b.shape[0] == nshots and u_b.shape[0] == nshots

@@ -142,3 +142,71 @@ def test_tile_kernel_refused_forms_fall_back(sfg_lib):
     case = layered_aniso_case(50)
     sim, _ = product_run(case, variant=5)
     assert sim.info().kernel_variant == 3
+
+
+# ---------------------------------------------------------------------------
+# Batched shots (S a multiple of 4): the same tiles, one work item per tile
+# and quad of shots; every shot's bits must equal the colour-pass run's.
+
+def _batched_shots(nshots, seed, xr, zr):
+    from specfempp_b200 import meshgen
+    rng = np.random.default_rng(seed)
+    return [meshgen.RickerSource(float(rng.uniform(*xr)), float(rng.uniform(*zr)), float(rng.uniform(6.0, 14.0)),
+                                 1e10, shot=s) for s in range(nshots)]
+
+
+def _batched_run(case, srcs, nshots, types, variant, pieces=(None,)):
+    from specfempp_b200 import sfg
+    sim = sfg.Simulation2D(case.mesh, dt=case.dt, nstep=case.nstep, nshots=nshots,
+                           elastic_wave="sh" if case.elastic_sh else "psv",
+                           point_rho=case.point_rho, point_vp=case.point_vp, point_vs=case.point_vs,
+                           kernel_variant=variant)
+    sim.set_sources(srcs)
+    sim.set_receivers(case.rec_x, case.rec_z, case.rec_angle, types)
+    sim.initialize()
+    for n in pieces:
+        sim.run(case.nstep if n is None else n)
+    return sim
+
+
+def _batched_equal(case, srcs, nshots, types, pieces=(None,)):
+    s1 = _batched_run(case, srcs, nshots, types, 1)
+    s5 = _batched_run(case, srcs, nshots, types, 5, pieces)
+    assert s5.info().kernel_variant == 5
+    a, b = s1.seismograms(), s5.seismograms()
+    assert a.shape[0] == nshots and np.abs(a).max() > 0
+    assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
+    for f in ("displacement", "velocity", "acceleration"):
+        fa, fb = s1.field("elastic", f), s5.field("elastic", f)
+        assert np.abs(fa).max() > 0
+        assert np.array_equal(fa, fb), f
+    assert s5.check_finite()
+
+
+@pytest.mark.parametrize("nshots", [4, 8, 12])
+def test_batched_tile_kernel_elastic_80x60(sfg_lib, nshots):
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_psv_80x60(nstep=300)
+    case = workload_case(w)
+    types = ("displacement", "velocity", "acceleration")
+    _batched_equal(case, _batched_shots(nshots, 5, (600, 3400), (600, 2600)), nshots, types)
+
+
+def test_batched_tile_kernel_grf_model_in_pieces(sfg_lib):
+    """Heterogeneous model, a run cut into pieces (the pending predictor is
+    resumed between runs)."""
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_grf_1000x500(nstep=120, nshots=8, nx=100, nz=50)
+    case = workload_case(w)
+    types = ("displacement", "velocity", "acceleration")
+    _batched_equal(case, w.sources, 8, types, pieces=(50, 1, 69))
+
+
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainStaceyDirichletBC", "HomogeneousElasticIsotropicDomainSH"])
+def test_batched_tile_kernel_fixtures(sfg_lib, name):
+    case, _, _ = golden_case(name)
+    case.nstep = min(case.nstep, 600)
+    xs = [float(x) for x in case.rec_x]
+    zs = [float(z) for z in case.rec_z]
+    srcs = _batched_shots(8, 11, (min(xs), max(xs)), (min(zs), max(zs)))
+    _batched_equal(case, srcs, 8, ("displacement", "velocity", "acceleration"))
