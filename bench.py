@@ -318,7 +318,7 @@ def bench_3d(args, world, barrier, max_over_ranks):
     steps = args.steps3d
     t0 = time.perf_counter()
     w = meshgen.elastic3d_layered_grf(nx, ny, nz, nstep=2 * steps + 20, nrec=1000)
-    sim = sfg3d.Simulation3D(w.mesh, dt=w.dt, nstep=w.nstep)
+    sim = sfg3d.Simulation3D(w.mesh, dt=w.dt, nstep=w.nstep, elements_per_block=args.epb3d)
     sim.set_sources(w.sources)
     sim.set_receivers(w.rec_xyz, types=("displacement",))
     sim.initialize()
@@ -455,6 +455,8 @@ def main():
     ap.add_argument("--no-3d", action="store_true")
     ap.add_argument("--mesh3d", default="128x128x64")
     ap.add_argument("--steps3d", type=int, default=50)
+    ap.add_argument("--epb3d", type=int, default=0,
+                    help="3D element kernel launch shape: 1, 2, 4 point form, 8, 16 column form (0 autotuned)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-media", action="store_true")
     ap.add_argument("--media-steps", type=int, default=200)

@@ -217,6 +217,7 @@ struct sfg_handle {
   sfg::dev::TileArgs tile_layout{};
   sfg::dev::TileBArgs tileb_layout{};   // batched shots
   int tile_smem = 0, tile_blocks_per_sm = 0;
+  int b4p_blocks = 0;                    // grid of the persistent batched element kernel
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
   std::string err;
@@ -493,6 +494,22 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
       else sfg::dev::k_stiffness_batched<1, false><<<grid, threads, 0, s>>>(B);
     }
   };
+  if (variant == 4 && quad) {
+    // persistent owner-computes with the next item prefetched
+    B.nspec_b = el.nspec;
+    if (h->b4p_blocks == 0) {
+      int nb = 0;
+      if (el.ncomp == 2)
+        SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sfg::dev::k_stiffness_batched4p<2>, threads, 0));
+      else
+        SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sfg::dev::k_stiffness_batched4p<1>, threads, 0));
+      h->b4p_blocks = std::max(nb, 1) * h->sm_count;
+    }
+    const int grid = std::min(h->b4p_blocks, el.nspec * tiles);
+    if (el.ncomp == 2) sfg::dev::k_stiffness_batched4p<2><<<grid, threads, 0, s>>>(B, T, tiles);
+    else sfg::dev::k_stiffness_batched4p<1><<<grid, threads, 0, s>>>(B, T, tiles);
+    return;
+  }
   if (variant >= 3) {
     launch(0, el.nspec, true);
     return;
@@ -1119,14 +1136,15 @@ void autotune(sfg_handle *h) {
   if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
   if (h->variant == 5) h->epb = 16;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
-  if (h->asmb.nshots > 1 && h->variant == 4) h->variant = 3;  // nor a bulk-copy one
+  // batched: variant 4 is the persistent owner-computes kernel (shots in fours)
+  if (h->asmb.nshots > 1 && h->variant == 4 && h->asmb.nshots % 4 != 0) h->variant = 3;
   const bool special = h->el.aniso || h->el.ncomp >= 3;   // anisotropic, Cosserat or poroelastic
   if (special && h->variant == 2) h->variant = 1;
   if (special && h->variant == 4) h->variant = 3;
   std::vector<std::pair<int, int>> cand;
   if (h->asmb.nshots > 1) {
-    for (int v : {1, 3})
-      if (!fix_v || v == h->variant) cand.push_back({v, 16});
+    for (int v : {1, 3, 4})
+      if ((!fix_v || v == h->variant) && (v != 4 || h->asmb.nshots % 4 == 0)) cand.push_back({v, 16});
     if (h->tile_ok && (!fix_v || h->variant == 5)) cand.push_back({5, 16});
   } else {
     for (int v : {1, 2, 3, 4}) {

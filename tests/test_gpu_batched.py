@@ -31,7 +31,7 @@ def run(w, srcs, nshots, types=("displacement", "velocity"), variant=0):
     return sim
 
 
-@pytest.mark.parametrize("nshots,variant", [(5, 1), (8, 1), (8, 3), (8, 5), (36, 1), (36, 3), (36, 5), (37, 3)])
+@pytest.mark.parametrize("nshots,variant", [(5, 1), (8, 1), (8, 3), (8, 4), (8, 5), (36, 1), (36, 3), (36, 4), (36, 5), (37, 3)])
 def test_batched_equals_single_shots(sfg_lib, nshots, variant):
     from dataclasses import replace
     from specfempp_b200 import meshgen
