@@ -456,7 +456,7 @@ def main():
     ap.add_argument("--mesh3d", default="128x128x64")
     ap.add_argument("--steps3d", type=int, default=50)
     ap.add_argument("--epb3d", type=int, default=0,
-                    help="3D element kernel launch shape: 1, 2, 4 point form, 8, 16 column form (0 autotuned)")
+                    help="3D element kernel launch shape: 1, 2, 4 point form, 6, 8 column form (0 autotuned)")
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-media", action="store_true")
     ap.add_argument("--media-steps", type=int, default=200)

@@ -6,7 +6,7 @@
  * Newmark time loop captured in CUDA graphs.  Status codes and sfg_options
  * are those of sfg.h (elements_per_block fixes the element kernel's launch
  * shape: 1, 2 or 4 elements per block with one thread per element GLL point,
- * 8 or 16 with one thread per column of five points; 0 lets the autotuner
+ * 6 or 8 with one thread per column of five points; 0 lets the autotuner
  * choose; all give the same bits; kernel_variant is ignored).
  *
  * It replaces, for this mesh class, the reference's dim3 forward path:

@@ -161,10 +161,13 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
 // displacement and F arrays in shared memory, whose x rows are padded to 8
 // floats so that a row is one float4 load plus one float load.  Per point the
 // operations and their order are those of k_stiffness3d, so both kernels give
-// the same bits.  Dynamic shared memory: E x (3 + 6) x 25 x 8 floats.
+// the same bits.  Dynamic shared memory: E x (3 + 6) x 25 x 8 floats.  With 8
+// elements per block the registers are capped for three blocks per SM; with
+// 6 the compiler may keep the five points' index, Jacobian and material
+// loads of a column in flight together.
 constexpr int RP3 = 8;
 template <int E>
-__global__ void __launch_bounds__(NG * NG * E, E <= 8 ? 3 : 1) k_stiffness3d_col(Elem3Args A) {
+__global__ void __launch_bounds__(NG * NG * E, E == 8 ? 3 : 1) k_stiffness3d_col(Elem3Args A) {
   extern __shared__ __align__(16) float dyn3[];
   const int tid = threadIdx.x;
   const int le = tid / (NG * NG), cq = tid - le * (NG * NG);

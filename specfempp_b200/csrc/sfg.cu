@@ -1160,7 +1160,7 @@ void autotune(sfg_handle *h) {
   if (cand.size() > 1) {
     float best = 1e30f;
     std::pair<int, int> pick = cand.front();
-    const int reps = h->asmb.nshots > 1 ? 2 : 5;
+    const int reps = 5;
     for (auto [v, e] : cand) {
       h->variant = v;
       h->epb = e;

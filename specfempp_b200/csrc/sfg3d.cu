@@ -433,7 +433,7 @@ void setup_sources(sfg_handle3d *h) {
 }
 
 // Element kernel launch: 1, 2 or 4 elements per block run the point form
-// (one thread per element point), 8 or 16 the column form (one thread per
+// (one thread per element point), 6 or 8 the column form (one thread per
 // column of five points).
 int col3_smem(int E) { return E * 9 * 25 * sfg3::dev::RP3 * int(sizeof(float)); }
 
@@ -443,13 +443,13 @@ void launch_elem(sfg_handle3d *h, const sfg3::dev::Elem3Args &A, cudaStream_t s)
   switch (E) {
     case 1: sfg3::dev::k_stiffness3d<1><<<grid, NQ * 1, 0, s>>>(A); break;
     case 2: sfg3::dev::k_stiffness3d<2><<<grid, NQ * 2, 0, s>>>(A); break;
+    case 6: sfg3::dev::k_stiffness3d_col<6><<<grid, 25 * 6, col3_smem(6), s>>>(A); break;
     case 8: sfg3::dev::k_stiffness3d_col<8><<<grid, 25 * 8, col3_smem(8), s>>>(A); break;
-    case 16: sfg3::dev::k_stiffness3d_col<16><<<grid, 25 * 16, col3_smem(16), s>>>(A); break;
     default: sfg3::dev::k_stiffness3d<4><<<grid, NQ * 4, 0, s>>>(A); break;
   }
 }
 
-bool valid_epb3(int e) { return e == 1 || e == 2 || e == 4 || e == 8 || e == 16; }
+bool valid_epb3(int e) { return e == 1 || e == 2 || e == 4 || e == 6 || e == 8; }
 
 void launch_step(sfg_handle3d *h, cudaStream_t s, bool predict) {
   sfg3::dev::Elem3Args A = h->EA;
@@ -678,14 +678,14 @@ int sfg3d_initialize(sfg_handle3d *h) {
     SFG3_CUDA(cudaDeviceSynchronize());
     SFG3_CUDA(cudaFuncSetAttribute(sfg3::dev::k_stiffness3d_col<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    col3_smem(8)));
-    SFG3_CUDA(cudaFuncSetAttribute(sfg3::dev::k_stiffness3d_col<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   col3_smem(16)));
+    SFG3_CUDA(cudaFuncSetAttribute(sfg3::dev::k_stiffness3d_col<6>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   col3_smem(6)));
     if (!valid_epb3(h->opt.elements_per_block)) {
       // launch-shape autotuner: elements per block and form of the element
       // kernel, whole steps timed on this mesh (all shapes give the same bits)
       float best = 1e30f;
       int pick = h->epb;
-      for (int e : {1, 2, 4, 8, 16}) {
+      for (int e : {1, 2, 4, 6, 8}) {
         h->epb = e;
         for (int i = 0; i < 2; ++i) launch_step(h, h->stream, true);
         SFG3_CUDA(cudaEventRecord(h->ev0, h->stream));
@@ -856,7 +856,7 @@ int sfg3d_get_info(sfg_handle3d *h, sfg_info3d *info) {
     info->device_bytes = h->mem ? h->mem->bytes : 0;
     info->elements_per_block = h->epb;
     info->kernels_per_step = 2 + (h->nrec > 0 ? 1 : 0);
-    info->kernel_variant = h->epb >= 8 ? 2 : 1;
+    info->kernel_variant = h->epb >= 6 ? 2 : 1;
     return int(SFG_OK);
   });
 }
