@@ -220,6 +220,8 @@ struct sfg_handle {
   int b4p_blocks = 0;                    // grid of the persistent batched element kernel
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
+  float *h_stfrow = nullptr;             // pinned staging of sfg_step_io's source row
+  int h_stfrow_cap = 0;
   std::string err;
   sfg::dev::Quad quad{};
 
@@ -231,6 +233,7 @@ struct sfg_handle {
                     (void *)adj.lb_j, (void *)adj.lb_geo})
       if (p) cudaFree(p);
     if (adj.h_stage) cudaFreeHost(adj.h_stage);
+    if (h_stfrow) cudaFreeHost(h_stfrow);
     if (adj.graph_r1) cudaGraphExecDestroy(adj.graph_r1);
     if (adj.graph_rseg) cudaGraphExecDestroy(adj.graph_rseg);
     for (auto &g : adj.graph_rev)
@@ -1632,12 +1635,17 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
     const sfg::Assembly2D &a = h->asmb;
     const int step = h->host_step;
     if (stf_row && a.nsrc > 0 && step < a.nstep) {
-      // the table stores the acoustic (pressure) sign convention already applied
-      thread_local std::vector<float> row;
-      row.assign(stf_row, stf_row + a.nsrc);
-      for (int s = 0; s < a.nsrc; ++s)
-        if (a.src_medium[s] == 0) row[s] = -row[s];
-      SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, row.data(), a.nsrc * sizeof(float),
+      // the table stores the acoustic (pressure) sign convention already
+      // applied; the row goes through pinned staging (the previous call's
+      // copy has completed: every call ends with a synchronize)
+      if (h->h_stfrow_cap < a.nsrc) {
+        if (h->h_stfrow) cudaFreeHost(h->h_stfrow);
+        h->h_stfrow = nullptr;
+        SFG_CUDA(cudaMallocHost(&h->h_stfrow, a.nsrc * sizeof(float)));
+        h->h_stfrow_cap = a.nsrc;
+      }
+      for (int s = 0; s < a.nsrc; ++s) h->h_stfrow[s] = a.src_medium[s] == 0 ? -stf_row[s] : stf_row[s];
+      SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, h->h_stfrow, a.nsrc * sizeof(float),
                                cudaMemcpyHostToDevice, h->stream));
     }
     // one fused step (the next step's predictor applied in the update); the

@@ -83,7 +83,7 @@ EXPORTS = {
     "sfg_reset_fields": ([C.c_void_p], C.c_int),
     "sfg_run_timed": ([C.c_void_p, C.c_int, _fp], C.c_int),
     "sfg_run_timed_flushed": ([C.c_void_p, C.c_int, C.c_size_t, _fp], C.c_int),
-    "sfg_step_io": ([C.c_void_p, _fp, _fp], C.c_int),
+    "sfg_step_io": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sfg_time_kernel": ([C.c_void_p, C.c_int, C.c_int, _fp], C.c_int),
     "sfg_get_info": ([C.c_void_p, C.POINTER(Info)], C.c_int),
     "sfg_get_seismograms": ([C.c_void_p, _fp, C.c_size_t], C.c_int),
@@ -278,10 +278,14 @@ class Simulation2D:
         return ms.value
 
     def step_io(self, stf_row=None, seis_row=None):
-        """One step with host buffers (float32 numpy arrays, ideally pinned)."""
-        sp = stf_row.ctypes.data_as(_fp) if stf_row is not None else None
-        op = seis_row.ctypes.data_as(_fp) if seis_row is not None else None
-        self._check(self.lib.sfg_step_io(self.h, sp, op))
+        """One step with host buffers (contiguous float32 numpy arrays, ideally
+        pinned): the sources' time-function values of the step in, the step's
+        seismogram row out."""
+        sp = stf_row.ctypes.data if stf_row is not None else None
+        op = seis_row.ctypes.data if seis_row is not None else None
+        rc = self.lib.sfg_step_io(self.h, sp, op)
+        if rc:
+            self._check(rc)
 
     def time_kernel(self, which: int, iters: int) -> float:
         ms = C.c_float()
