@@ -129,9 +129,10 @@ typedef struct sfg_options {
                                     launch; isotropic P-SV / SH / acoustic media, or
                                     batched shots in fours on one elastic medium, others
                                     fall back to 3); with batched shots 2 is 1 and 4 is
-                                    owner-computes with a persistent element kernel that
-                                    prefetches its next element (shots in fours); all
-                                    give the same bits (0 = chosen by the autotuner) */
+                                    owner-computes with the row-form element kernel (one
+                                    thread per element row and quad of shots; shots in
+                                    fours); all give the same bits (0 = chosen by the
+                                    autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
   int has_start_time;            /* 1: the run starts at start_time (the configuration's
                                     time-scheme t0) and sources keep their own tshift;

@@ -316,156 +316,184 @@ __global__ void __launch_bounds__(NP * 8) k_stiffness_batched4(BatchArgs A, int 
   }
 }
 
-// Persistent owner-computes form of k_stiffness_batched4: a block walks the
-// (element, shot tile) work items b, b + G, ...; the next item's index,
-// Jacobian, material and displacement quads are loaded into registers while
-// the current item computes, so their latency hides behind its arithmetic.
-// Per shot the operations are those of k_stiffness_batched4 (same bits).
-struct Batch4Item {
-  int g, bs, src, slot;
-  float xix, xiz, gax, gaz, jac, c0, mu;
-  float4 u[2];
-};
-
-template <int NC>
-__device__ __forceinline__ void batch4_load(const BatchArgs &A, int w, int T, int ntiles, int q, int j,
-                                            Batch4Item &it) {
-  const int e = w / ntiles, tile = w - e * ntiles;
-  const int shot0 = (tile * T + j) * 4;
-  const size_t p = size_t(e) * NP + q;
-  it.g = __ldg(A.ibool + p);
-  it.xix = __ldg(A.xix + p); it.xiz = __ldg(A.xiz + p); it.gax = __ldg(A.gax + p);
-  it.gaz = __ldg(A.gaz + p); it.jac = __ldg(A.jac + p);
-  it.c0 = __ldg(A.prop0 + p); it.mu = __ldg(A.prop1 + p);
-  it.slot = __ldg(A.slot + p);
-  it.bs = __ldg(A.bc_slot + e);
-  it.src = __ldg(A.src_head + e);
-  const bool act = shot0 < A.S;
+// Row form of k_stiffness_batched4 (owner-computes): one thread per element
+// row (five points, iz fixed) and quad of shots; EB elements x 5 rows x T
+// quads per block.  The xi-direction contractions of the gradient and of the
+// divergence run on the row held in registers (warp-uniform coefficients);
+// the gamma-direction ones read columns of the element's displacement and F1
+// in shared memory.  Per shot the operations and their order are those of
+// k_stiffness_batched4 (same bits).  Dynamic shared memory: EB x NC x 2 x 25
+// x T float4.
+template <int NC, int EB>
+__global__ void __launch_bounds__(EB * NG * 8, EB <= 4 ? 3 : 2) k_stiffness_batched4r(BatchArgs A, int T) {
+  extern __shared__ __align__(16) float4 dynb[];
+  const int rowq = threadIdx.x / T, j = threadIdx.x - rowq * T;
+  const int le = rowq / NG, iz = rowq - le * NG;
+  const int shot0 = (blockIdx.y * T + j) * 4;
+  const int e = blockIdx.x * EB + le;
+  const bool act = shot0 < A.S && e < A.nspec_b;
+  float4 *su = dynb + size_t(le) * NC * 2 * NP * T;   // [c][25][T]
+  float4 *sF1 = su + NC * NP * T;                     // [c][25][T]
+  const size_t pe = size_t(act ? e : 0) * NP + iz * NG;
+  int g[NG];
+  float4 ur[NC][NG];
 #pragma unroll
-  for (int c = 0; c < NC; ++c)
-    it.u[c] = act ? *reinterpret_cast<const float4 *>(A.u + (size_t(it.g) * NC + c) * A.S + shot0)
-                  : make_float4(0.f, 0.f, 0.f, 0.f);
-}
-
-template <int NC>
-__global__ void __launch_bounds__(NP * 8, 4) k_stiffness_batched4p(BatchArgs A, int T, int ntiles) {
-  __shared__ float4 su[NC][NP][8];
-  __shared__ float4 sF[NC][2][NP][8];
-  const int q = threadIdx.x / T, j = threadIdx.x - q * T;
-  const int iz = q / NG, ix = q - iz * NG;
-  const int nwork = A.nspec_b * ntiles;
-  int w = blockIdx.x;
-  if (w >= nwork) return;
-  Batch4Item cur, nxt;
-  batch4_load<NC>(A, w, T, ntiles, q, j, cur);
-  for (; w < nwork; w += gridDim.x) {
-    const int wn = w + gridDim.x;
-    if (wn < nwork) batch4_load<NC>(A, wn, T, ntiles, q, j, nxt);
-    const int tile = w - (w / ntiles) * ntiles;
-    const int shot0 = (tile * T + j) * 4;
-    const bool act = shot0 < A.S;
+  for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
 #pragma unroll
-    for (int c = 0; c < NC; ++c) su[c][q][j] = cur.u[c];
-    __syncthreads();
-    float a[NC][4];
+  for (int ix = 0; ix < NG; ++ix)
 #pragma unroll
-    for (int w4 = 0; w4 < 4; ++w4) {
+    for (int c = 0; c < NC; ++c) {
+      ur[c][ix] = act ? *reinterpret_cast<const float4 *>(A.u + (size_t(g[ix]) * NC + c) * A.S + shot0)
+                      : make_float4(0.f, 0.f, 0.f, 0.f);
+      su[(c * NP + iz * NG + ix) * T + j] = ur[c][ix];
+    }
+  float hz[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) hz[l] = c_hp[iz * NG + l];
+  __syncthreads();
+  // xi-direction derivatives of the row's five points, in place of the row
+#pragma unroll
+  for (int c = 0; c < NC; ++c) {
+    float4 dx[NG];
+#pragma unroll
+    for (int ix = 0; ix < NG; ++ix) {
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        float d = 0.f;
+#pragma unroll
+        for (int l = 0; l < NG; ++l) d = fmaf(c_hp[ix * NG + l], (&ur[c][l].x)[w], d);
+        (&dx[ix].x)[w] = d;
+      }
+    }
+#pragma unroll
+    for (int ix = 0; ix < NG; ++ix) ur[c][ix] = dx[ix];
+  }
+  // per point: gamma-direction derivatives from the columns, stress, F; F0
+  // replaces the xi derivatives in registers, F1 goes to shared memory
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    const size_t p = pe + ix;
+    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+    const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+    float4 dg[NC];
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+#pragma unroll
+      for (int w = 0; w < 4; ++w) {
+        float d = 0.f;
+#pragma unroll
+        for (int l = 0; l < NG; ++l) d = fmaf(hz[l], (&su[(c * NP + l * NG + ix) * T + j].x)[w], d);
+        (&dg[c].x)[w] = d;
+      }
+    }
+    float4 f0[NC], f1[NC];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
       float dxi[NC], dga[NC];
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        dxi[c] = 0.f;
-        dga[c] = 0.f;
-#pragma unroll
-        for (int l = 0; l < NG; ++l) {
-          dxi[c] = fmaf(c_hp[ix * NG + l], (&su[c][iz * NG + l][j].x)[w4], dxi[c]);
-          dga[c] = fmaf(c_hp[iz * NG + l], (&su[c][l * NG + ix][j].x)[w4], dga[c]);
-        }
+        dxi[c] = (&ur[c][ix].x)[w];
+        dga[c] = (&dg[c].x)[w];
       }
       float Sx[NC], Sz[NC];
       if (NC == 2) {
-        const float du00 = cur.xix * dxi[0] + cur.gax * dga[0], du01 = cur.xiz * dxi[0] + cur.gaz * dga[0];
-        const float du10 = cur.xix * dxi[NC - 1] + cur.gax * dga[NC - 1];
-        const float du11 = cur.xiz * dxi[NC - 1] + cur.gaz * dga[NC - 1];
-        const float lam = cur.c0 - 2.f * cur.mu;
-        const float sxx = cur.c0 * du00 + lam * du11;
-        const float szz = cur.c0 * du11 + lam * du00;
-        const float sxz = cur.mu * (du01 + du10);
+        const float du00 = xix * dxi[0] + gax * dga[0], du01 = xiz * dxi[0] + gaz * dga[0];
+        const float du10 = xix * dxi[NC - 1] + gax * dga[NC - 1];
+        const float du11 = xiz * dxi[NC - 1] + gaz * dga[NC - 1];
+        const float lam = c0 - 2.f * mu;
+        const float sxx = c0 * du00 + lam * du11;
+        const float szz = c0 * du11 + lam * du00;
+        const float sxz = mu * (du01 + du10);
         Sx[0] = sxx; Sz[0] = sxz; Sx[NC - 1] = sxz; Sz[NC - 1] = szz;
       } else {
-        Sx[0] = cur.mu * (cur.xix * dxi[0] + cur.gax * dga[0]);
-        Sz[0] = cur.mu * (cur.xiz * dxi[0] + cur.gaz * dga[0]);
+        Sx[0] = mu * (xix * dxi[0] + gax * dga[0]);
+        Sz[0] = mu * (xiz * dxi[0] + gaz * dga[0]);
       }
 #pragma unroll
       for (int c = 0; c < NC; ++c) {
-        a[c][w4] = cur.jac * (Sx[c] * cur.xix + Sz[c] * cur.xiz);       // F0 for now
-        (&sF[c][1][q][j].x)[w4] = cur.jac * (Sx[c] * cur.gax + Sz[c] * cur.gaz);
+        (&f0[c].x)[w] = jac * (Sx[c] * xix + Sz[c] * xiz);
+        (&f1[c].x)[w] = jac * (Sx[c] * gax + Sz[c] * gaz);
       }
     }
 #pragma unroll
-    for (int c = 0; c < NC; ++c) sF[c][0][q][j] = make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
-    __syncthreads();
-    if (act) {
+    for (int c = 0; c < NC; ++c) {
+      ur[c][ix] = f0[c];
+      sF1[(c * NP + iz * NG + ix) * T + j] = f1[c];
+    }
+  }
+  const int bs = act ? __ldg(A.bc_slot + e) : -1;
+  const int src = act ? __ldg(A.src_head + e) : -1;
+  float wz[NG];
 #pragma unroll
-      for (int w4 = 0; w4 < 4; ++w4) {
+  for (int l = 0; l < NG; ++l) wz[l] = c_hpw[l * NG + iz];
+  const float wiz = c_w[iz];
+  __syncthreads();
+  if (!act) return;
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    const int q = iz * NG + ix;
+    float a[NC][4];
+#pragma unroll
+    for (int w = 0; w < 4; ++w) {
+#pragma unroll
+      for (int c = 0; c < NC; ++c) {
+        float t1 = 0.f, t2 = 0.f;
+#pragma unroll
+        for (int l = 0; l < NG; ++l) {
+          t1 = fmaf((&ur[c][l].x)[w], c_hpw[l * NG + ix], t1);
+          t2 = fmaf((&sF1[(c * NP + l * NG + ix) * T + j].x)[w], wz[l], t2);
+        }
+        a[c][w] = -(wiz * t1 + c_w[ix] * t2);
+      }
+    }
+    if (bs >= 0) {
+      const size_t k = size_t(bs) * NP + q;
+      const float wq = A.bc_w[k];
+      if (wq != 0.f) {
+        const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
+        if (NC == 2) {
+          const float4 vx4 = *reinterpret_cast<const float4 *>(A.v + (size_t(g[ix]) * NC) * A.S + shot0);
+          const float4 vz4 = *reinterpret_cast<const float4 *>(A.v + (size_t(g[ix]) * NC + NC - 1) * A.S + shot0);
+          const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
+#pragma unroll
+          for (int w = 0; w < 4; ++w) {
+            const float vx = (&vx4.x)[w], vz = (&vz4.x)[w];
+            const float vn = vx * nx + vz * nz;
+            const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vx * rvs;
+            const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vz * rvs;
+            a[0][w] += -1.f * fx * j1 * wq;
+            a[NC - 1][w] += -1.f * fz * j1 * wq;
+          }
+        } else {
+          const float4 v4 = *reinterpret_cast<const float4 *>(A.v + size_t(g[ix]) * A.S + shot0);
+#pragma unroll
+          for (int w = 0; w < 4; ++w) a[0][w] += -1.f * (wq * j1) * A.bc_imp1[k] * (&v4.x)[w];
+        }
+      }
+    }
+    if (src >= 0) {
+      const int step = *A.step;
+      for (int s = src; s >= 0; s = A.src_next[s]) {
+        const int ws = A.src_shot[s] - shot0;
+        if (ws < 0 || ws > 3) continue;
+        const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
 #pragma unroll
         for (int c = 0; c < NC; ++c) {
-          float t1 = 0.f, t2 = 0.f;
-#pragma unroll
-          for (int l = 0; l < NG; ++l) {
-            t1 = fmaf((&sF[c][0][iz * NG + l][j].x)[w4], c_hpw[l * NG + ix], t1);
-            t2 = fmaf((&sF[c][1][l * NG + ix][j].x)[w4], c_hpw[l * NG + iz], t2);
-          }
-          a[c][w4] = -(c_w[iz] * t1 + c_w[ix] * t2);
+          const float add = f * A.src_arr[(size_t(s) * 2 + c) * NP + q];
+          // sources in chain order, as the one-shot kernel adds them
+          if (ws == 0) a[c][0] += add;
+          else if (ws == 1) a[c][1] += add;
+          else if (ws == 2) a[c][2] += add;
+          else a[c][3] += add;
         }
       }
-      if (cur.bs >= 0) {
-        const size_t k = size_t(cur.bs) * NP + q;
-        const float wq = A.bc_w[k];
-        if (wq != 0.f) {
-          const float nx = A.bc_nx[k], nz = A.bc_nz[k], j1 = A.bc_j1[k];
-          if (NC == 2) {
-            const float4 vx4 = *reinterpret_cast<const float4 *>(A.v + (size_t(cur.g) * NC) * A.S + shot0);
-            const float4 vz4 = *reinterpret_cast<const float4 *>(A.v + (size_t(cur.g) * NC + NC - 1) * A.S + shot0);
-            const float rvp = A.bc_imp0[k], rvs = A.bc_imp1[k];
-#pragma unroll
-            for (int w4 = 0; w4 < 4; ++w4) {
-              const float vx = (&vx4.x)[w4], vz = (&vz4.x)[w4];
-              const float vn = vx * nx + vz * nz;
-              const float fx = ((vn * nx / (j1 * j1)) * (rvp - rvs)) + vx * rvs;
-              const float fz = ((vn * nz / (j1 * j1)) * (rvp - rvs)) + vz * rvs;
-              a[0][w4] += -1.f * fx * j1 * wq;
-              a[NC - 1][w4] += -1.f * fz * j1 * wq;
-            }
-          } else {
-            const float4 v4 = *reinterpret_cast<const float4 *>(A.v + size_t(cur.g) * A.S + shot0);
-#pragma unroll
-            for (int w4 = 0; w4 < 4; ++w4) a[0][w4] += -1.f * (wq * j1) * A.bc_imp1[k] * (&v4.x)[w4];
-          }
-        }
-      }
-      if (cur.src >= 0) {
-        const int step = *A.step;
-        for (int s = cur.src; s >= 0; s = A.src_next[s]) {
-          const int ws = A.src_shot[s] - shot0;
-          if (ws < 0 || ws > 3) continue;
-          const float f = step < A.nstep ? A.stf[size_t(step) * A.nsrc + s] : 0.f;
-#pragma unroll
-          for (int c = 0; c < NC; ++c) {
-            const float add = f * A.src_arr[(size_t(s) * 2 + c) * NP + q];
-            // the one-shot kernel adds sources in chain order; so does this loop
-            if (ws == 0) a[c][0] += add;
-            else if (ws == 1) a[c][1] += add;
-            else if (ws == 2) a[c][2] += add;
-            else a[c][3] += add;
-          }
-        }
-      }
-#pragma unroll
-      for (int c = 0; c < NC; ++c)
-        *reinterpret_cast<float4 *>(A.r + (size_t(cur.slot) * NC + c) * A.S + shot0) =
-            make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
     }
-    cur = nxt;
+    const int sl = __ldg(A.slot + pe + ix);
+#pragma unroll
+    for (int c = 0; c < NC; ++c)
+      *reinterpret_cast<float4 *>(A.r + (size_t(sl) * NC + c) * A.S + shot0) =
+          make_float4(a[c][0], a[c][1], a[c][2], a[c][3]);
   }
 }
 

@@ -217,7 +217,7 @@ struct sfg_handle {
   sfg::dev::TileArgs tile_layout{};
   sfg::dev::TileBArgs tileb_layout{};   // batched shots
   int tile_smem = 0, tile_blocks_per_sm = 0;
-  int b4p_blocks = 0;                    // grid of the persistent batched element kernel
+  bool b4r_attr = false;                 // shared-memory attribute of the row-form batched kernel set
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
   float *h_stfrow = nullptr;             // pinned staging of sfg_step_io's source row
@@ -498,19 +498,20 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
     }
   };
   if (variant == 4 && quad) {
-    // persistent owner-computes with the next item prefetched
+    // owner-computes with the row-form element kernel (4 elements per block)
+    constexpr int EB = 4;
     B.nspec_b = el.nspec;
-    if (h->b4p_blocks == 0) {
-      int nb = 0;
-      if (el.ncomp == 2)
-        SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sfg::dev::k_stiffness_batched4p<2>, threads, 0));
-      else
-        SFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sfg::dev::k_stiffness_batched4p<1>, threads, 0));
-      h->b4p_blocks = std::max(nb, 1) * h->sm_count;
+    const int smem = EB * el.ncomp * 2 * sfg::dev::NP * T * int(sizeof(float4));
+    if (!h->b4r_attr) {
+      SFG_CUDA(cudaFuncSetAttribute(sfg::dev::k_stiffness_batched4r<2, EB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, EB * 2 * 2 * 25 * 8 * 16));
+      SFG_CUDA(cudaFuncSetAttribute(sfg::dev::k_stiffness_batched4r<1, EB>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, EB * 1 * 2 * 25 * 8 * 16));
+      h->b4r_attr = true;
     }
-    const int grid = std::min(h->b4p_blocks, el.nspec * tiles);
-    if (el.ncomp == 2) sfg::dev::k_stiffness_batched4p<2><<<grid, threads, 0, s>>>(B, T, tiles);
-    else sfg::dev::k_stiffness_batched4p<1><<<grid, threads, 0, s>>>(B, T, tiles);
+    const dim3 grid((el.nspec + EB - 1) / EB, tiles);
+    if (el.ncomp == 2) sfg::dev::k_stiffness_batched4r<2, EB><<<grid, EB * sfg::dev::NG * T, smem, s>>>(B, T);
+    else sfg::dev::k_stiffness_batched4r<1, EB><<<grid, EB * sfg::dev::NG * T, smem, s>>>(B, T);
     return;
   }
   if (variant >= 3) {
@@ -1139,7 +1140,7 @@ void autotune(sfg_handle *h) {
   if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
   if (h->variant == 5) h->epb = 16;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
-  // batched: variant 4 is the persistent owner-computes kernel (shots in fours)
+  // batched: variant 4 is owner-computes with the row-form element kernel (shots in fours)
   if (h->asmb.nshots > 1 && h->variant == 4 && h->asmb.nshots % 4 != 0) h->variant = 3;
   const bool special = h->el.aniso || h->el.ncomp >= 3;   // anisotropic, Cosserat or poroelastic
   if (special && h->variant == 2) h->variant = 1;
