@@ -118,7 +118,8 @@ typedef struct sfg_options {
   int nstep_between_samples;     /* seismogram sampling (>= 1) */
   int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
   int elements_per_block;        /* elements per block of the element kernel: 8, 16, 32
-                                    (0 = chosen by the autotuner at sfg_initialize) */
+                                    (64 with the row form only; 0 = chosen by the
+                                    autotuner at sfg_initialize) */
   int kernel_variant;            /* assembly / element kernel: 1 colour passes (one block
                                     per chunk), 2 colour passes with a persistent
                                     prefetching kernel, 3 owner-computes (one element
@@ -131,8 +132,11 @@ typedef struct sfg_options {
                                     fall back to 3); with batched shots 2 is 1 and 4 is
                                     owner-computes with the row-form element kernel (one
                                     thread per element row and quad of shots; shots in
-                                    fours); all give the same bits (0 = chosen by the
-                                    autotuner) */
+                                    fours); 6 owner-computes with the row-form element
+                                    kernel of one shot (one thread per element row;
+                                    isotropic P-SV and acoustic media, 32 or 64 elements
+                                    per block, others fall back to 3); all give the same
+                                    bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
   int has_start_time;            /* 1: the run starts at start_time (the configuration's
                                     time-scheme t0) and sources keep their own tshift;

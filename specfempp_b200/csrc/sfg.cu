@@ -22,6 +22,7 @@
 #include "kernels2d_tma.cuh"
 #include "kernels2d_tile.cuh"
 #include "kernels2d_tile_batched.cuh"
+#include "kernels2d_row.cuh"
 
 namespace {
 
@@ -524,11 +525,43 @@ void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *ste
   }
 }
 
+// The row-form kernel covers isotropic P-SV and acoustic media.
+bool row_ok(const DevMedium &el) { return el.nspec == 0 || (el.ncomp == 2 && !el.aniso); }
+
+template <int E>
+void launch_stiffness_row(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
+                          cudaStream_t s) {
+  sfg::dev::StiffArgs S{};
+  S.el = med_args(el);
+  S.ac = med_args(ac);
+  S.src_next = h->d_src_next;
+  S.src_arr = h->d_src_arr;
+  S.src_arr2 = h->d_src_arr2;
+  S.stf = h->d_stf;
+  S.nsrc = h->asmb.nsrc;
+  S.nstep = h->asmb.nstep;
+  S.step = step;
+  S.quad = h->quad;
+  S.el.e0 = 0; S.el.e1 = el.nspec; S.el.nblocks = (el.nspec + E - 1) / E;
+  S.ac.e0 = 0; S.ac.e1 = ac.nspec; S.ac.nblocks = (ac.nspec + E - 1) / E;
+  const int grid = S.el.nblocks + S.ac.nblocks;
+  if (grid > 0) sfg::dev::k_stiffness_row<E><<<grid, sfg::dev::NG * E, 0, s>>>(S);
+}
+
 void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, const int *step,
                       cudaStream_t s, int variant) {
   if (el.S > 1) {
     launch_stiffness_batched(h, el, step, s, variant);
     return;
+  }
+  if (variant == 6) {
+    // owner-computes with the row-form element kernel (32 or 64 elements per block)
+    if (row_ok(el)) {
+      if (h->epb == 64) launch_stiffness_row<64>(h, el, ac, step, s);
+      else launch_stiffness_row<32>(h, el, ac, step, s);
+      return;
+    }
+    variant = 3;
   }
   switch (h->epb) {
     case 8: launch_stiffness_W<8>(h, el, ac, step, s, variant); break;
@@ -1133,12 +1166,16 @@ void run_steps(sfg_handle *h, int nsteps) {
 // captured; the fields and counters it touches are cleared afterwards.
 void autotune(sfg_handle *h) {
   const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
-                     h->opt.elements_per_block == 32;
-  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 5;
+                     h->opt.elements_per_block == 32 || h->opt.elements_per_block == 64;
+  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 6;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
   if (h->variant == 5) h->epb = 16;
+  // the row form: isotropic P-SV / acoustic, one shot, 32 or 64 elements per block
+  if (h->variant == 6 && (h->asmb.nshots > 1 || !row_ok(h->el))) h->variant = 3;
+  if (h->variant == 6 && h->epb != 64) h->epb = 32;
+  if (h->variant != 6 && h->epb == 64) h->epb = 16;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   // batched: variant 4 is owner-computes with the row-form element kernel (shots in fours)
   if (h->asmb.nshots > 1 && h->variant == 4 && h->asmb.nshots % 4 != 0) h->variant = 3;
@@ -1159,6 +1196,10 @@ void autotune(sfg_handle *h) {
     }
     // fused tile kernel: tiles of 16 elements
     if (h->tile_ok && (!fix_v || h->variant == 5) && (!fix_e || h->epb == 16)) cand.push_back({5, 16});
+    // row-form element kernel
+    if (row_ok(h->el) && (!fix_v || h->variant == 6))
+      for (int e : {32, 64})
+        if (!fix_e || e == h->epb) cand.push_back({6, e});
   }
   if (cand.empty()) cand.push_back({h->variant, h->epb});
   if (cand.size() > 1) {

@@ -126,7 +126,8 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
 @pytest.mark.parametrize("epb,spg,variant", [(8, 7, 1), (32, 1, 1), (8, 3, 2), (16, 20, 2), (32, 5, 2),
                                              (8, 4, 3), (16, 20, 3), (32, 1, 3),
                                              (8, 4, 4), (16, 20, 4), (32, 1, 4),
-                                             (16, 20, 5), (16, 3, 5), (16, 1, 5)])
+                                             (16, 20, 5), (16, 3, 5), (16, 1, 5),
+                                             (32, 20, 6), (64, 3, 6), (32, 1, 6)])
 def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg, variant):
     from specfempp_b200 import meshgen
     w = meshgen.coupled_400x200(nstep=120, nx=40, nz=20)
@@ -176,10 +177,11 @@ def test_step_and_run_agree(sfg_lib):
 
 @pytest.mark.parametrize("name", ["HomogeneousAcousticDomainDirichletBC", "HomogeneousElasticDomainStaceyBC",
                                   "HomogeneousElasticIsotropicDomainSH", "HomogeneousElasticDomainMomentTensor"])
-@pytest.mark.parametrize("variant", [3, 4, 5])
+@pytest.mark.parametrize("variant", [3, 4, 5, 6])
 def test_owner_computes_variants_equal_colour_passes(sfg_lib, name, variant):
-    """Single-medium fixtures: the owner-computes kernels (plain and with
-    bulk-copy staging) give the colour passes' bits."""
+    """Single-medium fixtures: the owner-computes kernels (plain, with
+    bulk-copy staging, fused tiles and the row form; media a form does not
+    cover fall back to plain owner-computes) give the colour passes' bits."""
     case, _, _ = golden_case(name)
     _, a = product_run(case, epb=16, variant=1)
     _, b = product_run(case, epb=8, variant=variant)
@@ -253,7 +255,7 @@ def test_anisotropic_layered_parity(sfg_lib, oracle_lib):
     for t, kind in enumerate(types):
         tol = 1e-5 if kind != "acceleration" else tolerance(kind, ref[:, t], ref64[:, t])
         assert rel_l2(seis[:, t], ref[:, t]) <= tol, (kind, rel_l2(seis[:, t], ref[:, t]), tol)
-    for v in (0, 2, 3, 4, 5):
+    for v in (0, 2, 3, 4, 5, 6):
         _, s2 = product_run(case, types=types, variant=v)
         assert np.array_equal(s2, seis), v
 
