@@ -558,7 +558,8 @@ def main():
     tr = traffic_from_profile()
     traffic = None
     if tr and tr.get("workload") == args.workload:
-        traffic = tr.get("stiffness_bytes_per_launch")
+        # the DRAM traffic of the element kernel in use, from its ncu capture
+        traffic = tr.get("stiffness_bytes_per_launch_by_variant", {}).get(str(inf.kernel_variant))
     step_bytes = STEP_B_GLOB * nglob + STEP_B_LOCAL * inf.nspec * 25
     kname = ("element kernel, one owner-computes launch of one step" if inf.kernel_variant >= 3 else
              f"element kernel, all {inf.ncolors_elastic} colour launches of one step")
