@@ -118,8 +118,8 @@ typedef struct sfg_options {
   int nstep_between_samples;     /* seismogram sampling (>= 1) */
   int steps_per_graph;           /* time steps per captured CUDA graph (0 = default) */
   int elements_per_block;        /* elements per block of the element kernel: 8, 16, 32
-                                    (64 with the row form only; 0 = chosen by the
-                                    autotuner at sfg_initialize) */
+                                    (the row form: 16 or 32; 0 = chosen by the autotuner
+                                    at sfg_initialize) */
   int kernel_variant;            /* assembly / element kernel: 1 colour passes (one block
                                     per chunk), 2 colour passes with a persistent
                                     prefetching kernel, 3 owner-computes (one element
@@ -134,7 +134,7 @@ typedef struct sfg_options {
                                     thread per element row and quad of shots; shots in
                                     fours); 6 owner-computes with the row-form element
                                     kernel of one shot (one thread per element row;
-                                    isotropic P-SV and acoustic media, 32 or 64 elements
+                                    isotropic P-SV and acoustic media, 16 or 32 elements
                                     per block, others fall back to 3); all give the same
                                     bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */

@@ -32,10 +32,12 @@ __device__ __forceinline__ void elastic_rows(const StiffArgs &S, const MedArgs &
   float2 *su = smem + le * NP;              // [25] (u_x, u_z)
   float2 *sF1 = smem + (E + le) * NP;       // [25] F1 of both components
   const size_t pe = size_t(act ? e : A.e0) * NP + iz * NG;
-  int g[NG];
+  int g[NG], sl[NG];
   float2 ur[NG];
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) sl[ix] = __ldg(A.slot + pe + ix);
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
     ur[ix] = act ? reinterpret_cast<const float2 *>(A.u)[g[ix]] : make_float2(0.f, 0.f);
@@ -120,7 +122,7 @@ __device__ __forceinline__ void elastic_rows(const StiffArgs &S, const MedArgs &
         a1 += f * S.src_arr[(size_t(s) * 2 + 1) * NP + q];
       }
     }
-    reinterpret_cast<float2 *>(A.r)[__ldg(A.slot + pe + ix)] = make_float2(a0, a1);
+    reinterpret_cast<float2 *>(A.r)[sl[ix]] = make_float2(a0, a1);
   }
 }
 
@@ -133,10 +135,12 @@ __device__ __forceinline__ void acoustic_rows(const StiffArgs &S, const MedArgs 
   float *su = smem + le * NP;               // [25] chi
   float *sF1 = smem + (E + le) * NP;        // [25] F1
   const size_t pe = size_t(act ? e : A.e0) * NP + iz * NG;
-  int g[NG];
+  int g[NG], sl[NG];
   float ur[NG];
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) sl[ix] = __ldg(A.slot + pe + ix);
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
     ur[ix] = act ? A.u[g[ix]] : 0.f;
@@ -192,13 +196,13 @@ __device__ __forceinline__ void acoustic_rows(const StiffArgs &S, const MedArgs 
         a += f * S.src_arr[(size_t(s) * 2) * NP + q];
       }
     }
-    A.r[__ldg(A.slot + pe + ix)] = a;
+    A.r[sl[ix]] = a;
   }
 }
 
 // Blocks [0, el.nblocks) run elastic P-SV elements, the others acoustic ones.
 template <int E>
-__global__ void __launch_bounds__(NG * E, E == 32 ? 6 : 1) k_stiffness_row(StiffArgs S) {
+__global__ void __launch_bounds__(NG * E, E == 16 ? 12 : (E == 32 ? 6 : 1)) k_stiffness_row(StiffArgs S) {
   __shared__ __align__(16) float2 smem[2 * E * NP];
   if (int(blockIdx.x) < S.el.nblocks)
     elastic_rows<E>(S, S.el, S.el.e0 + blockIdx.x * E, smem);

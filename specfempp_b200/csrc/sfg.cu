@@ -555,9 +555,9 @@ void launch_stiffness(sfg_handle *h, const DevMedium &el, const DevMedium &ac, c
     return;
   }
   if (variant == 6) {
-    // owner-computes with the row-form element kernel (32 or 64 elements per block)
+    // owner-computes with the row-form element kernel (16 or 32 elements per block)
     if (row_ok(el)) {
-      if (h->epb == 64) launch_stiffness_row<64>(h, el, ac, step, s);
+      if (h->epb == 16) launch_stiffness_row<16>(h, el, ac, step, s);
       else launch_stiffness_row<32>(h, el, ac, step, s);
       return;
     }
@@ -1166,16 +1166,15 @@ void run_steps(sfg_handle *h, int nsteps) {
 // captured; the fields and counters it touches are cleared afterwards.
 void autotune(sfg_handle *h) {
   const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
-                     h->opt.elements_per_block == 32 || h->opt.elements_per_block == 64;
+                     h->opt.elements_per_block == 32;
   const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 6;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
   if (h->variant == 5) h->epb = 16;
-  // the row form: isotropic P-SV / acoustic, one shot, 32 or 64 elements per block
+  // the row form: isotropic P-SV / acoustic, one shot, 16 or 32 elements per block
   if (h->variant == 6 && (h->asmb.nshots > 1 || !row_ok(h->el))) h->variant = 3;
-  if (h->variant == 6 && h->epb != 64) h->epb = 32;
-  if (h->variant != 6 && h->epb == 64) h->epb = 16;
+  if (h->variant == 6 && h->epb != 16) h->epb = 32;
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   // batched: variant 4 is owner-computes with the row-form element kernel (shots in fours)
   if (h->asmb.nshots > 1 && h->variant == 4 && h->asmb.nshots % 4 != 0) h->variant = 3;
@@ -1198,7 +1197,7 @@ void autotune(sfg_handle *h) {
     if (h->tile_ok && (!fix_v || h->variant == 5) && (!fix_e || h->epb == 16)) cand.push_back({5, 16});
     // row-form element kernel
     if (row_ok(h->el) && (!fix_v || h->variant == 6))
-      for (int e : {32, 64})
+      for (int e : {16, 32})
         if (!fix_e || e == h->epb) cand.push_back({6, e});
   }
   if (cand.empty()) cand.push_back({h->variant, h->epb});

@@ -127,7 +127,7 @@ def test_acoustic_receivers_all_types(sfg_lib, oracle_lib):
                                              (8, 4, 3), (16, 20, 3), (32, 1, 3),
                                              (8, 4, 4), (16, 20, 4), (32, 1, 4),
                                              (16, 20, 5), (16, 3, 5), (16, 1, 5),
-                                             (32, 20, 6), (64, 3, 6), (32, 1, 6)])
+                                             (32, 20, 6), (16, 3, 6), (32, 1, 6)])
 def test_launch_shapes_and_graphs_agree(sfg_lib, epb, spg, variant):
     from specfempp_b200 import meshgen
     w = meshgen.coupled_400x200(nstep=120, nx=40, nz=20)
