@@ -45,7 +45,7 @@
 // kernels: include/medium/dim2/acoustic/isotropic/frechet_derivative.hpp:61-93).
 #pragma once
 
-#include "kernels2d.cuh"
+#include "kernels2d_batched.cuh"
 
 namespace sfg {
 namespace dev {
@@ -152,6 +152,121 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
   sg.x += tk;
   sg.y += tm;
   reinterpret_cast<float2 *>(A.seg)[p] = sg;
+}
+
+// Row form of k_adj_elem: one thread per element row (five points) of E
+// elements; the xi-direction contractions of both fields and of the
+// divergence on the row in registers (warp-uniform coefficients, the two
+// components paired in FFMA2, which rounds each lane as fmaf), the
+// gamma-direction ones from shared-memory columns.  Per point the
+// operations and their order are those of k_adj_elem (same bits).
+template <int E>
+__global__ void __launch_bounds__(NG * E, 5) k_adj_elem_row(AdjArgs A) {
+  __shared__ float2 sm2[E][NP], su2[E][NP], sF1[E][NP];
+  const int tid = threadIdx.x;
+  const int le = tid / NG, iz = tid - le * NG;
+  const int e = blockIdx.x * E + le;
+  const bool act = e < A.nspec;
+  const size_t pe = size_t(act ? e : 0) * NP + iz * NG;
+  int g[NG], sl[NG];
+  float2 mr[NG], ur[NG];
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) sl[ix] = __ldg(A.pslot + pe + ix);
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    mr[ix] = act ? reinterpret_cast<const float2 *>(A.mu)[g[ix]] : make_float2(0.f, 0.f);
+    ur[ix] = act ? reinterpret_cast<const float2 *>(A.uf)[g[ix]] : make_float2(0.f, 0.f);
+    sm2[le][iz * NG + ix] = mr[ix];
+    su2[le][iz * NG + ix] = ur[ix];
+  }
+  const int rh = act ? __ldg(A.ad_head + e) : -1;
+  float hz[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) hz[l] = c_hp[iz * NG + l];
+  __syncthreads();
+  // xi derivatives of both fields, both components paired, in place
+  {
+    float2 dm[NG], du[NG];
+#pragma unroll
+    for (int ix = 0; ix < NG; ++ix) {
+      float2 a = make_float2(0.f, 0.f), b = make_float2(0.f, 0.f);
+#pragma unroll
+      for (int l = 0; l < NG; ++l) {
+        a = fma2(f2(c_hp[ix * NG + l]), mr[l], a);
+        b = fma2(f2(c_hp[ix * NG + l]), ur[l], b);
+      }
+      dm[ix] = a;
+      du[ix] = b;
+    }
+#pragma unroll
+    for (int ix = 0; ix < NG; ++ix) { mr[ix] = dm[ix]; ur[ix] = du[ix]; }
+  }
+  const float wiz = c_w[iz];
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    const size_t p = pe + ix;
+    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
+                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
+    const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+    float2 gm = make_float2(0.f, 0.f), gu = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      gm = fma2(f2(hz[l]), sm2[le][l * NG + ix], gm);
+      gu = fma2(f2(hz[l]), su2[le][l * NG + ix], gu);
+    }
+    // dm[c][0] = mr[ix].c (xi), dm[c][1] = gm.c (gamma)
+    const float mxx = xix * mr[ix].x + gax * gm.x, mxz = xiz * mr[ix].x + gaz * gm.x;
+    const float mzx = xix * mr[ix].y + gax * gm.y, mzz = xiz * mr[ix].y + gaz * gm.y;
+    const float uxx = xix * ur[ix].x + gax * gu.x, uxz = xiz * ur[ix].x + gaz * gu.x;
+    const float uzx = xix * ur[ix].y + gax * gu.y, uzz = xiz * ur[ix].y + gaz * gu.y;
+    const float lam = c0 - 2.f * mu;
+    const float sxx = c0 * mxx + lam * mzz;
+    const float szz = c0 * mzz + lam * mxx;
+    const float sxz = mu * (mxz + mzx);
+    mr[ix] = make_float2(jac * (sxx * xix + sxz * xiz), jac * (sxz * xix + szz * xiz));   // F0
+    sF1[le][iz * NG + ix] = make_float2(jac * (sxx * gax + sxz * gaz), jac * (sxz * gax + szz * gaz));
+    if (act) {
+      // gradient terms of this step, summed over the segment
+      const float W = c_w[ix] * wiz * jac;
+      const float divm = mxx + mzz, divu = uxx + uzz;
+      const float tk = -W * (divm * divu);
+      const float tm = -W * ((4.f / 3.f) * (mxx * uxx + mzz * uzz) - (2.f / 3.f) * (mxx * uzz + mzz * uxx) +
+                             (mxz + mzx) * (uxz + uzx));
+      float2 sg = reinterpret_cast<float2 *>(A.seg)[p];
+      sg.x += tk;
+      sg.y += tm;
+      reinterpret_cast<float2 *>(A.seg)[p] = sg;
+    }
+  }
+  float wz[NG];
+#pragma unroll
+  for (int l = 0; l < NG; ++l) wz[l] = c_hpw[l * NG + iz];
+  __syncthreads();
+  if (!act) return;
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    const int q = iz * NG + ix;
+    float2 t1 = make_float2(0.f, 0.f), t2 = make_float2(0.f, 0.f);
+#pragma unroll
+    for (int l = 0; l < NG; ++l) {
+      t1 = fma2(mr[l], f2(c_hpw[l * NG + ix]), t1);
+      t2 = fma2(sF1[le][l * NG + ix], f2(wz[l]), t2);
+    }
+    float r0 = -(wiz * t1.x + c_w[ix] * t2.x);
+    float r1 = -(wiz * t1.y + c_w[ix] * t2.y);
+    // receivers of this element inject R^T g (the adjoint sources)
+    if (rh >= 0) {
+      const float *g_k = A.gtab + size_t(*A.seg_k0 + A.slot) * A.nrec * 2;
+      for (int k = rh; k >= 0; k = A.ad_next[k]) {
+        const float h = A.ad_h[size_t(k) * NP + q];
+        r0 += g_k[2 * k] * h;
+        r1 += g_k[2 * k + 1] * h;
+      }
+    }
+    reinterpret_cast<float2 *>(A.r)[sl[ix]] = make_float2(r0, r1);
+  }
 }
 
 // SH reverse element step (one component): -K mu with sigma = mu grad,

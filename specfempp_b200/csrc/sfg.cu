@@ -2251,7 +2251,7 @@ void record_segment(sfg_handle *h, int c, bool seismograms, int b) {
 // 0), then the Kahan fold of its sums.  `last`: the run's final segment,
 // whose final step starts from mu = 0 (no Stacey term) unless pressure
 // seismograms set mu there.
-template <int E>
+template <int E, bool ROW = false>
 void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
   AdjointState &A = h->adj;
   const DevMedium &D = adj_dev(h);
@@ -2304,7 +2304,8 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
           A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
           D.nglob, dt, dt2, dtsq2);
     } else {
-      sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+      if (ROW) sfg::dev::k_adj_elem_row<32><<<(D.nspec + 31) / 32, sfg::dev::NG * 32, 0, rs>>>(J);
+      else sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
       sfg::dev::k_adj_post<2><<<grid_for(D.nglob), 256, 0, rs>>>(
           A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
           D.nglob, dt, dt2, dtsq2);
@@ -2315,15 +2316,21 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
 
 void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs);
 
-// Elements per block of the reverse element kernel: each shape timed over a
-// few launches on the live buffers (before the sums are cleared), the fastest
-// kept.  All shapes give the same bits.
+// Launch shape of the reverse element kernel: 8, 16 or 32 elements per block
+// of the point form, or (code 1) the P-SV row form; each timed over a few
+// launches on the live buffers (before the sums are cleared), the fastest
+// kept.  All shapes give the same bits.  A forward kernel_variant fixed to 6
+// fixes the row form, 1 to 5 the point form.
 void tune_reverse(sfg_handle *h, cudaStream_t rs) {
   AdjointState &A = h->adj;
   if (A.epb) return;
+  const bool row = adj_dev(h).ncomp == 2 && !A.pressure;
+  if (row && h->opt.kernel_variant == 6) { A.epb = 1; return; }
+  std::vector<int> cand{8, 16, 32};
+  if (row && h->opt.kernel_variant == 0) cand.push_back(1);
   float best = 1e30f;
   A.epb = 8;
-  for (int e : {8, 16, 32}) {
+  for (int e : cand) {
     const int save = A.epb;
     A.epb = e;
     for (int rep = 0; rep < 2; ++rep) {
@@ -2341,6 +2348,7 @@ void tune_reverse(sfg_handle *h, cudaStream_t rs) {
 
 void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
   switch (h->adj.epb) {
+    case 1: reverse_segment_E<32, true>(h, b, n, last, rs); break;
     case 16: reverse_segment_E<16>(h, b, n, last, rs); break;
     case 32: reverse_segment_E<32>(h, b, n, last, rs); break;
     default: reverse_segment_E<8>(h, b, n, last, rs); break;

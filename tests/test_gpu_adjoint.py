@@ -115,6 +115,27 @@ def test_segment_budget_gives_the_same_gradient(problem):
         assert np.array_equal(x, z)
 
 
+def test_row_form_reverse_kernel_gives_the_same_gradient(sfg_lib):
+    """kernel_variant 6 (row-form element kernels, forward and reverse) and 3
+    (point form): the same gradient bits."""
+    from specfempp_b200 import meshgen, sfg
+    w = meshgen.elastic_psv_80x60(nstep=NSTEP)
+    model = base_model(w.mesh)
+    weights = np.random.default_rng(17).standard_normal((NSTEP, len(w.rec_x), 2)).astype(np.float32)
+    out = []
+    for v in (3, 6):
+        sim = sfg.Simulation2D(w.mesh, dt=w.dt, nstep=NSTEP, kernel_variant=v)
+        sim.set_sources(w.sources)
+        sim.set_receivers(w.rec_x, w.rec_z, types=("displacement",))
+        sim.initialize()
+        assert sim.info().kernel_variant == v
+        out.append(gradient(sim, model, weights, 50))
+        sim.close()
+    for x, y in zip(*out):
+        assert np.abs(x).max() > 0
+        assert np.array_equal(x, y)
+
+
 def test_autograd_function(problem):
     import torch
     from specfempp_b200 import adjoint
