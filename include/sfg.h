@@ -201,9 +201,11 @@ int sfg_reset_fields(sfg_handle *h);                /* zero wavefields, istep = 
 /* Device time of nsteps graph-replayed steps, measured with CUDA events on the
  * handle's stream (inputs resident); ms_total receives the elapsed time. */
 int sfg_run_timed(sfg_handle *h, int nsteps, float *ms_total);
-/* Device time of nsteps steps, each launched separately after a write of
- * flush_bytes to a scratch buffer (clears L2 between timed steps); returns the
- * sum of the per-step times measured with CUDA events on the handle's stream. */
+/* Device time of nsteps steps, each launched separately after an L2 flush
+ * outside the timed interval (a write of flush_bytes to a scratch buffer, then
+ * a read of a second scratch buffer of flush_bytes, so that the cache holds
+ * none of the model's data and no dirty lines); returns the sum of the
+ * per-step times measured with CUDA events on the handle's stream. */
 int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *ms_total);
 /* One step with host buffers: copies this step's source-time values
  * stf_row[nsrc] (host, may be NULL to keep the table) to the device, runs the
@@ -223,6 +225,10 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row);
  * points of both media, 2 nothing (0 ms), 3 receivers.  Leaves the fields
  * mid-step (sfg_reset_fields after). */
 int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms_per_launch);
+/* The same with the L2 cache flushed before every launch, outside the timed
+ * interval, as sfg_run_timed_flushed does before a step, so that the launch
+ * reads all its inputs from HBM; flush_bytes = 0 is sfg_time_kernel. */
+int sfg_time_kernel_flushed(sfg_handle *h, int which, int iters, size_t flush_bytes, float *ms_per_launch);
 
 /* ---- step-wise interface: the reference's kernel facade ----
  * One phase per call, in the reference's granularity, on the handle's own

@@ -609,6 +609,35 @@ int grid_for(int n) {
   return std::max(1, std::min(blocks, 148 * 8));
 }
 
+// Reads a buffer (float4 by float4) so that the L2 afterwards holds its clean
+// lines; the sink is written only on a value the zero-filled buffer never has.
+__global__ void __launch_bounds__(256) k_read_flush(const float4 *__restrict__ b, size_t n4, float *sink) {
+  float acc = 0.f;
+  for (size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n4; i += size_t(gridDim.x) * blockDim.x) {
+    const float4 v = b[i];
+    acc += v.x + v.y + v.z + v.w;
+  }
+  if (acc == 1234.5f) *sink = acc;
+}
+
+// L2 flush before a timed launch or step: a device write of `bytes`, then a
+// read of a second buffer of `bytes`, so the cache holds neither the model's
+// data nor dirty lines whose write-back the timed work would pay for.
+void flush_l2(sfg_handle *h, size_t bytes, int pattern) {
+  if (bytes > h->flush_bytes) {
+    if (h->flush_buf) cudaFree(h->flush_buf);
+    h->flush_buf = nullptr;
+    h->flush_bytes = 0;
+    SFG_CUDA(cudaMalloc(&h->flush_buf, 2 * bytes + 16));
+    SFG_CUDA(cudaMemset(h->flush_buf, 0, 2 * bytes + 16));
+    h->flush_bytes = bytes;
+  }
+  char *base = static_cast<char *>(h->flush_buf);
+  SFG_CUDA(cudaMemsetAsync(base, pattern & 0xff, bytes, h->stream));
+  k_read_flush<<<148 * 8, 256, 0, h->stream>>>(reinterpret_cast<const float4 *>(base + h->flush_bytes),
+                                                bytes / 16, reinterpret_cast<float *>(base + 2 * h->flush_bytes));
+}
+
 sfg::dev::RecArgs rec_args(sfg_handle *h, int medium) {
   DevMedium &D = medium == SFG_MEDIUM_ELASTIC ? h->el : h->ac;
   sfg::dev::RecArgs R{};
@@ -1627,13 +1656,6 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
     if (nsteps < 0) return int(SFG_ERR_ARG);
-    if (flush_bytes > h->flush_bytes) {
-      if (h->flush_buf) cudaFree(h->flush_buf);
-      h->flush_buf = nullptr;
-      h->flush_bytes = 0;
-      SFG_CUDA(cudaMalloc(&h->flush_buf, flush_bytes));
-      h->flush_bytes = flush_bytes;
-    }
     const int batch = 256;
     std::vector<cudaEvent_t> ev(2 * batch);
     for (auto &e : ev) SFG_CUDA(cudaEventCreate(&e));
@@ -1644,7 +1666,7 @@ int sfg_run_timed_flushed(sfg_handle *h, int nsteps, size_t flush_bytes, float *
       while (done < nsteps) {
         const int n = std::min(batch, nsteps - done);
         for (int i = 0; i < n; ++i) {
-          if (flush_bytes) SFG_CUDA(cudaMemsetAsync(h->flush_buf, i & 0xff, flush_bytes, h->stream));
+          if (flush_bytes) flush_l2(h, flush_bytes, i);
           SFG_CUDA(cudaEventRecord(ev[2 * i], h->stream));
           SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
           SFG_CUDA(cudaEventRecord(ev[2 * i + 1], h->stream));
@@ -1708,6 +1730,10 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
 }
 
 int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms) {
+  return sfg_time_kernel_flushed(h, which, iters, 0, ms);
+}
+
+int sfg_time_kernel_flushed(sfg_handle *h, int which, int iters, size_t flush_bytes, float *ms) {
   return guarded(h, [&]() {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
     if (iters <= 0 || which < 0 || which > 3) return int(SFG_ERR_ARG);
@@ -1729,13 +1755,29 @@ int sfg_time_kernel(sfg_handle *h, int which, int iters, float *ms) {
     };
     h->state_final = false;
     for (int i = 0; i < 3; ++i) launch();
-    SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
-    for (int i = 0; i < iters; ++i) launch();
-    SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
-    SFG_CUDA(cudaEventSynchronize(h->ev1));
-    SFG_CUDA(cudaGetLastError());
     float t = 0;
-    SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    if (flush_bytes == 0) {
+      // back to back
+      SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+      for (int i = 0; i < iters; ++i) launch();
+      SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+      SFG_CUDA(cudaEventSynchronize(h->ev1));
+      SFG_CUDA(cudaGetLastError());
+      SFG_CUDA(cudaEventElapsedTime(&t, h->ev0, h->ev1));
+    } else {
+      // each launch after an L2 flush (the cache holds none of its inputs)
+      for (int i = 0; i < iters; ++i) {
+        flush_l2(h, flush_bytes, i);
+        SFG_CUDA(cudaEventRecord(h->ev0, h->stream));
+        launch();
+        SFG_CUDA(cudaEventRecord(h->ev1, h->stream));
+        SFG_CUDA(cudaEventSynchronize(h->ev1));
+        float ti = 0;
+        SFG_CUDA(cudaEventElapsedTime(&ti, h->ev0, h->ev1));
+        t += ti;
+      }
+      SFG_CUDA(cudaGetLastError());
+    }
     if (ms) *ms = t / iters;
     return int(SFG_OK);
   });

@@ -85,6 +85,7 @@ EXPORTS = {
     "sfg_run_timed_flushed": ([C.c_void_p, C.c_int, C.c_size_t, _fp], C.c_int),
     "sfg_step_io": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "sfg_time_kernel": ([C.c_void_p, C.c_int, C.c_int, _fp], C.c_int),
+    "sfg_time_kernel_flushed": ([C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.POINTER(C.c_float)], C.c_int),
     "sfg_get_info": ([C.c_void_p, C.POINTER(Info)], C.c_int),
     "sfg_get_seismograms": ([C.c_void_p, _fp, C.c_size_t], C.c_int),
     "sfg_get_field": ([C.c_void_p, C.c_int, C.c_int, _fp, C.c_size_t], C.c_int),
@@ -287,9 +288,12 @@ class Simulation2D:
         if rc:
             self._check(rc)
 
-    def time_kernel(self, which: int, iters: int) -> float:
+    def time_kernel(self, which: int, iters: int, flush_bytes: int = 0) -> float:
+        """Average device ms of one launch of a kernel family (sfg_time_kernel);
+        with flush_bytes > 0 the L2 is flushed before every launch."""
         ms = C.c_float()
-        self._check(self.lib.sfg_time_kernel(self.h, int(which), int(iters), C.byref(ms)))
+        self._check(self.lib.sfg_time_kernel_flushed(self.h, int(which), int(iters), int(flush_bytes),
+                                                     C.byref(ms)))
         return ms.value
 
     def synchronize(self):
