@@ -2,7 +2,9 @@
 // and acoustic media, one launch for both).
 //
 // One thread per element row (the five points of a row iz), E elements per
-// block (5 E threads).  The row's displacement is gathered into registers;
+// block (5 E threads).  The row's displacement is gathered into registers,
+// and its Jacobian, material words and slot indices are requested at the
+// same time (their latency overlaps the gather's);
 // the xi-direction contractions of the gradient and of the divergence run
 // on the row in registers with warp-uniform coefficients (constant bank),
 // the gamma-direction ones read columns of the element's displacement and
@@ -38,6 +40,14 @@ __device__ __forceinline__ void elastic_rows(const StiffArgs &S, const MedArgs &
   for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) sl[ix] = __ldg(A.slot + pe + ix);
+  // the row's Jacobian and material words, requested with the gather
+  float gxix[NG], gxiz[NG], ggax[NG], ggaz[NG], gjac[NG], gc0[NG], gmu[NG];
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    gxix[ix] = __ldg(A.xix + pe + ix); gxiz[ix] = __ldg(A.xiz + pe + ix);
+    ggax[ix] = __ldg(A.gax + pe + ix); ggaz[ix] = __ldg(A.gaz + pe + ix);
+    gjac[ix] = __ldg(A.jac + pe + ix); gc0[ix] = __ldg(A.prop0 + pe + ix); gmu[ix] = __ldg(A.prop1 + pe + ix);
+  }
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
     ur[ix] = act ? reinterpret_cast<const float2 *>(A.u)[g[ix]] : make_float2(0.f, 0.f);
@@ -62,10 +72,8 @@ __device__ __forceinline__ void elastic_rows(const StiffArgs &S, const MedArgs &
   }
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
-    const size_t p = pe + ix;
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+    const float xix = gxix[ix], xiz = gxiz[ix], gax = ggax[ix], gaz = ggaz[ix], jac = gjac[ix];
+    const float c0 = gc0[ix], mu = gmu[ix];
     float2 pg = make_float2(0.f, 0.f);
 #pragma unroll
     for (int l = 0; l < NG; ++l) pg = fma2(f2(hz[l]), su[l * NG + ix], pg);
@@ -141,6 +149,14 @@ __device__ __forceinline__ void acoustic_rows(const StiffArgs &S, const MedArgs 
   for (int ix = 0; ix < NG; ++ix) g[ix] = act ? __ldg(A.ibool + pe + ix) : 0;
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) sl[ix] = __ldg(A.slot + pe + ix);
+  // the row's Jacobian and material words, requested with the gather
+  float gxix[NG], gxiz[NG], ggax[NG], ggaz[NG], gjac[NG], grho[NG];
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    gxix[ix] = __ldg(A.xix + pe + ix); gxiz[ix] = __ldg(A.xiz + pe + ix);
+    ggax[ix] = __ldg(A.gax + pe + ix); ggaz[ix] = __ldg(A.gaz + pe + ix);
+    gjac[ix] = __ldg(A.jac + pe + ix); grho[ix] = __ldg(A.prop0 + pe + ix);
+  }
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
     ur[ix] = act ? A.u[g[ix]] : 0.f;
@@ -153,10 +169,8 @@ __device__ __forceinline__ void acoustic_rows(const StiffArgs &S, const MedArgs 
   float f0[NG];
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
-    const size_t p = pe + ix;
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    const float rhoinv = __ldg(A.prop0 + p);
+    const float xix = gxix[ix], xiz = gxiz[ix], gax = ggax[ix], gaz = ggaz[ix], jac = gjac[ix];
+    const float rhoinv = grho[ix];
     // the two derivative directions paired (FFMA2, rounding as fmaf)
     float2 d = make_float2(0.f, 0.f);
 #pragma unroll
@@ -202,7 +216,7 @@ __device__ __forceinline__ void acoustic_rows(const StiffArgs &S, const MedArgs 
 
 // Blocks [0, el.nblocks) run elastic P-SV elements, the others acoustic ones.
 template <int E>
-__global__ void __launch_bounds__(NG * E, E == 16 ? 12 : (E == 32 ? 6 : 1)) k_stiffness_row(StiffArgs S) {
+__global__ void __launch_bounds__(NG * E, E == 16 ? 8 : (E == 32 ? 4 : 1)) k_stiffness_row(StiffArgs S) {
   __shared__ __align__(16) float2 smem[2 * E * NP];
   if (int(blockIdx.x) < S.el.nblocks)
     elastic_rows<E>(S, S.el, S.el.e0 + blockIdx.x * E, smem);
