@@ -7,13 +7,16 @@ pressure source, 200 seafloor receivers, dt = 1e-3 s).  Synthetic, seeded.
 
 One bench step = one time step of the whole model.  Reported keys:
 * value:  GLL-point updates/s with inputs resident in HBM, every timed step
-          launched after a 256 MiB write that flushes L2, timed with CUDA events
-          on the handle's stream, summed over the K steps, max over ranks;
+          launched after an L2 flush (a 256 MiB write, then a read of another
+          256 MiB buffer: no input and no dirty line left in the cache), timed
+          with CUDA events on the handle's stream, summed over the K steps,
+          max over ranks;
 * e2e:    the same metric through the per-step C-ABI call with host buffers
           (STF row host->device, seismogram row device->host, a sync per step);
 * roofline: the dominant kernel (the element kernel of one step: one
           owner-computes launch, or the colour passes, whichever the autotuner
-          chose) against the measured HBM bandwidth;
+          chose) against the measured HBM bandwidth, its launch timed after the
+          same L2 flush (frac) and back to back (frac_back_to_back);
 * cpu_baseline: the CPU oracle (a C++ restatement of the reference) on all
           host cores, bounded sample of the same workload.
 ``--impl reference`` times that CPU implementation alone on the same
