@@ -327,6 +327,8 @@ __global__ void __launch_bounds__(NP * 8) k_stiffness_batched4(BatchArgs A, int 
 template <int NC, int EB>
 __global__ void __launch_bounds__(EB * NG * 8, EB <= 4 ? 3 : 2) k_stiffness_batched4r(BatchArgs A, int T) {
   extern __shared__ __align__(16) float4 dynb[];
+  // the block's Jacobian and material words [EB][7][25], loaded once by all threads
+  __shared__ float sgeo[EB * 7 * NP];
   const int rowq = threadIdx.x / T, j = threadIdx.x - rowq * T;
   const int le = rowq / NG, iz = rowq - le * NG;
   const int shot0 = (blockIdx.y * T + j) * 4;
@@ -334,6 +336,15 @@ __global__ void __launch_bounds__(EB * NG * 8, EB <= 4 ? 3 : 2) k_stiffness_batc
   const bool act = shot0 < A.S && e < A.nspec_b;
   float4 *su = dynb + size_t(le) * NC * 2 * NP * T;   // [c][25][T]
   float4 *sF1 = su + NC * NP * T;                     // [c][25][T]
+  for (int i = threadIdx.x; i < EB * NP; i += blockDim.x) {
+    const int ee = i / NP, q = i - ee * NP;
+    const int eg = blockIdx.x * EB + ee;
+    const size_t pg = size_t(eg < A.nspec_b ? eg : 0) * NP + q;
+    float *d = sgeo + ee * 7 * NP + q;
+    d[0] = __ldg(A.xix + pg); d[NP] = __ldg(A.xiz + pg); d[2 * NP] = __ldg(A.gax + pg);
+    d[3 * NP] = __ldg(A.gaz + pg); d[4 * NP] = __ldg(A.jac + pg);
+    d[5 * NP] = __ldg(A.prop0 + pg); d[6 * NP] = __ldg(A.prop1 + pg);
+  }
   const size_t pe = size_t(act ? e : 0) * NP + iz * NG;
   int g[NG];
   float4 ur[NC][NG];
@@ -372,10 +383,9 @@ __global__ void __launch_bounds__(EB * NG * 8, EB <= 4 ? 3 : 2) k_stiffness_batc
   // replaces the xi derivatives in registers, F1 goes to shared memory
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
-    const size_t p = pe + ix;
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+    const float *gw = sgeo + le * 7 * NP + iz * NG + ix;
+    const float xix = gw[0], xiz = gw[NP], gax = gw[2 * NP], gaz = gw[3 * NP], jac = gw[4 * NP];
+    const float c0 = gw[5 * NP], mu = gw[6 * NP];
     float4 dg[NC];
 #pragma unroll
     for (int c = 0; c < NC; ++c) {
