@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -221,8 +222,12 @@ struct sfg_handle {
   bool b4r_attr = false;                 // shared-memory attribute of the row-form batched kernel set
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
-  float *h_stfrow = nullptr;             // pinned staging of sfg_step_io's source row
-  int h_stfrow_cap = 0;
+  // sfg_step_io: one graph per step that reads the source row from and
+  // writes the seismogram row to mapped pinned host memory
+  // ([flag, pad x3][source row][seismogram rows of the shots])
+  void *io_host = nullptr;
+  void *io_dev = nullptr;
+  cudaGraphExec_t graph_io = nullptr;
   std::string err;
   sfg::dev::Quad quad{};
 
@@ -234,7 +239,8 @@ struct sfg_handle {
                     (void *)adj.lb_j, (void *)adj.lb_geo})
       if (p) cudaFree(p);
     if (adj.h_stage) cudaFreeHost(adj.h_stage);
-    if (h_stfrow) cudaFreeHost(h_stfrow);
+    if (io_host) cudaFreeHost(io_host);
+    if (graph_io) cudaGraphExecDestroy(graph_io);
     if (adj.graph_r1) cudaGraphExecDestroy(adj.graph_r1);
     if (adj.graph_rseg) cudaGraphExecDestroy(adj.graph_rseg);
     for (auto &g : adj.graph_rev)
@@ -618,6 +624,26 @@ __global__ void __launch_bounds__(256) k_read_flush(const float4 *__restrict__ b
     acc += v.x + v.y + v.z + v.w;
   }
   if (acc == 1234.5f) *sink = acc;
+}
+
+// sfg_step_io: the step's source row from mapped host memory into the table
+// (when the host set the flag), and after the step its seismogram rows back.
+__global__ void k_io_in(const int *__restrict__ io, float *stf, const int *step, int nsrc, int nstep) {
+  const int st = *step;
+  if (io[0] == 0 || st >= nstep) return;
+  const float *row = reinterpret_cast<const float *>(io + 4);
+  for (int s = threadIdx.x; s < nsrc; s += blockDim.x) stf[size_t(st) * nsrc + s] = row[s];
+}
+__global__ void k_io_out(const float *__restrict__ seis, float *out, const int *step, int nsb, int nsig, int nshots,
+                         int rowlen) {
+  const int st = *step - 1;    // the step just taken
+  if (st < 0 || st % nsb != 0 || st / nsb >= nsig) return;
+  const int isig = st / nsb;
+  const int n = nshots * rowlen;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const int sh = i / rowlen, k = i - sh * rowlen;
+    out[i] = seis[(size_t(sh) * nsig + isig) * rowlen + k];
+  }
 }
 
 // L2 flush before a timed launch or step: a device write of `bytes`, then a
@@ -1697,34 +1723,45 @@ int sfg_step_io(sfg_handle *h, const float *stf_row, float *seis_row) {
     if (!h->initialized) { h->err = "sfg_initialize first"; return int(SFG_ERR_STATE); }
     const sfg::Assembly2D &a = h->asmb;
     const int step = h->host_step;
-    if (stf_row && a.nsrc > 0 && step < a.nstep) {
-      // the table stores the acoustic (pressure) sign convention already
-      // applied; the row goes through pinned staging (the previous call's
-      // copy has completed: every call ends with a synchronize)
-      if (h->h_stfrow_cap < a.nsrc) {
-        if (h->h_stfrow) cudaFreeHost(h->h_stfrow);
-        h->h_stfrow = nullptr;
-        SFG_CUDA(cudaMallocHost(&h->h_stfrow, a.nsrc * sizeof(float)));
-        h->h_stfrow_cap = a.nsrc;
-      }
-      for (int s = 0; s < a.nsrc; ++s) h->h_stfrow[s] = a.src_medium[s] == 0 ? -stf_row[s] : stf_row[s];
-      SFG_CUDA(cudaMemcpyAsync(h->d_stf + size_t(step) * a.nsrc, h->h_stfrow, a.nsrc * sizeof(float),
-                               cudaMemcpyHostToDevice, h->stream));
+    const int rowlen = a.ntypes * a.nrec * 2;
+    const size_t io_bytes = 16 + 4 * size_t(a.nsrc) + 4 * size_t(a.nshots) * rowlen;
+    if (!h->graph_io) {
+      SFG_CUDA(cudaHostAlloc(&h->io_host, io_bytes, cudaHostAllocMapped));
+      std::memset(h->io_host, 0, io_bytes);
+      SFG_CUDA(cudaHostGetDevicePointer(&h->io_dev, h->io_host, 0));
+      const int *io_d = static_cast<const int *>(h->io_dev);
+      float *seis_d = reinterpret_cast<float *>(static_cast<char *>(h->io_dev) + 16 + 4 * size_t(a.nsrc));
+      // one fused step (the next step's predictor applied in the update)
+      // between the row copies; the step's seismograms are complete before
+      // its update runs
+      cudaGraph_t g = nullptr;
+      SFG_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+      k_io_in<<<1, 128, 0, h->stream>>>(io_d, h->d_stf, h->d_step, a.nsrc, a.nstep);
+      enqueue_step(h, h->stream, true);
+      if (a.nrec > 0)
+        k_io_out<<<std::max(1, std::min(64, (a.nshots * rowlen + 255) / 256)), 256, 0, h->stream>>>(
+            h->d_seis, seis_d, h->d_step, a.nsb, a.nsig, a.nshots, rowlen);
+      SFG_CUDA(cudaStreamEndCapture(h->stream, &g));
+      SFG_CUDA(cudaGraphInstantiate(&h->graph_io, g, 0));
+      cudaGraphDestroy(g);
     }
-    // one fused step (the next step's predictor applied in the update); the
-    // step's seismograms are complete before its update runs
+    int *io = static_cast<int *>(h->io_host);
+    io[0] = 0;
+    if (stf_row && a.nsrc > 0 && step < a.nstep) {
+      // the table stores the acoustic (pressure) sign convention already applied
+      float *row = reinterpret_cast<float *>(io + 4);
+      for (int s = 0; s < a.nsrc; ++s) row[s] = a.src_medium[s] == 0 ? -stf_row[s] : stf_row[s];
+      io[0] = 1;
+    }
+    std::atomic_thread_fence(std::memory_order_seq_cst);
     resume(h);
-    SFG_CUDA(cudaGraphLaunch(h->graph_1, h->stream));
+    SFG_CUDA(cudaGraphLaunch(h->graph_io, h->stream));
     h->state_final = false;
     ++h->host_step;
-    if (seis_row && a.nrec > 0 && step % a.nsb == 0 && step / a.nsb < a.nsig) {
-      const size_t row = size_t(a.ntypes) * a.nrec * 2;
-      const int isig = step / a.nsb;
-      for (int s = 0; s < a.nshots; ++s)
-        SFG_CUDA(cudaMemcpyAsync(seis_row + s * row, h->d_seis + (size_t(s) * a.nsig + isig) * row,
-                                 row * sizeof(float), cudaMemcpyDeviceToHost, h->stream));
-    }
     SFG_CUDA(cudaStreamSynchronize(h->stream));
+    if (seis_row && a.nrec > 0 && step % a.nsb == 0 && step / a.nsb < a.nsig)
+      std::memcpy(seis_row, static_cast<char *>(h->io_host) + 16 + 4 * size_t(a.nsrc),
+                  sizeof(float) * size_t(a.nshots) * rowlen);
     return int(SFG_OK);
   });
 }
