@@ -419,7 +419,7 @@ def run_reference(args, rank):
     w = make_workload(args.workload, max(args.steps, 1))
     # each bench step is one time step of the full model; the timed sample is
     # capped so that warm-up plus timed steps stay near a minute on the host
-    steps = max(3, min(args.steps, 3000))
+    steps = max(1, min(args.steps, 3000))
     warm = args.warmup
     cpu_oracle_throughput(w, warm, threads)
     v, secs = cpu_oracle_throughput(w, steps, threads)
