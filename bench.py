@@ -193,7 +193,7 @@ def bench_batched(args, world, barrier, max_over_ranks):
     ms_1 = max_over_ranks(one.run_timed(steps))
     del one
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         # the reference runs one shot at a time: 50 steps of one shot on the
         # host cores (oracle, FP32, full mesh and model)
         from oracle import runner
@@ -352,7 +352,7 @@ def bench_3d(args, world, barrier, max_over_ranks):
            "finite": bool(finite)}
     sim.close()
     rank = int(os.environ.get("RANK", "0"))
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         # a bounded sample: 5 steps of the full 67.6 M-point model on the host
         # cores (the oracle's 3D restatement, FP32)
         from oracle import runner3d
@@ -602,7 +602,7 @@ def main():
         media = bench_media(args, world, barrier, max_over_ranks)
 
     cpu = None
-    if rank == 0 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         v, secs = cpu_oracle_throughput(w, 40, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
