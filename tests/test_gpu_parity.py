@@ -164,6 +164,21 @@ def test_fields_after_timing_call_are_refused(sfg_lib):
     assert np.all(np.isfinite(sim.field("elastic")))
 
 
+def test_kernel_timing_with_flushed_cache(sfg_lib):
+    """sfg_time_kernel_flushed: every launch after an L2 flush; its inputs come
+    from HBM, so it takes at least about as long as back to back."""
+    from specfempp_b200 import meshgen
+    w = meshgen.coupled_400x200(nstep=20, nx=200, nz=100)
+    sim, _ = product_run(workload_case(w), nsteps=5)
+    b2b = sim.time_kernel(0, 10)
+    cold = sim.time_kernel(0, 10, 256 << 20)
+    assert b2b > 0 and cold > 0
+    assert cold >= 0.8 * b2b, (cold, b2b)
+    sim.reset()
+    sim.run(3)
+    assert sim.check_finite()
+
+
 def test_step_and_run_agree(sfg_lib):
     from specfempp_b200 import meshgen
     w = meshgen.elastic_psv_80x60(nstep=50)
