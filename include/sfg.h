@@ -135,8 +135,11 @@ typedef struct sfg_options {
                                     fours); 6 owner-computes with the row-form element
                                     kernel of one shot (one thread per element row;
                                     isotropic P-SV and acoustic media, 16 or 32 elements
-                                    per block, others fall back to 3); all give the same
-                                    bits (0 = chosen by the autotuner) */
+                                    per block, others fall back to 3); with batched shots
+                                    in fours and displacement receivers, 7 assembles and
+                                    finishes each four-element tile's interior points in
+                                    the element kernel (others fall back to 3); all give
+                                    the same bits (0 = chosen by the autotuner) */
   int store_acceleration;        /* also keep the elastic acceleration inside runs */
   int has_start_time;            /* 1: the run starts at start_time (the configuration's
                                     time-scheme t0) and sources keep their own tshift;

@@ -8,7 +8,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SOURCES = ["csrc/sfg.cu", "csrc/sfg3d.cu", "csrc/host2d.cpp"]
-HEADERS = ["csrc/kernels2d.cuh", "csrc/kernels2d_batched.cuh", "csrc/kernels2d_adjoint.cuh", "csrc/kernels2d_tma.cuh", "csrc/kernels2d_tile.cuh", "csrc/kernels2d_tile_batched.cuh", "csrc/kernels2d_row.cuh", "csrc/kernels3d.cuh", "csrc/host2d.hpp", "../include/sfg.h", "../include/sfg3d.h"]
+HEADERS = ["csrc/kernels2d.cuh", "csrc/kernels2d_batched.cuh", "csrc/kernels2d_adjoint.cuh", "csrc/kernels2d_tma.cuh", "csrc/kernels2d_tile.cuh", "csrc/kernels2d_tile_batched.cuh", "csrc/kernels2d_row.cuh", "csrc/kernels2d_btile.cuh", "csrc/kernels3d.cuh", "csrc/host2d.hpp", "../include/sfg.h", "../include/sfg3d.h"]
 # -fmad=false: products and sums are rounded separately unless a kernel asks
 # for an FMA explicitly, so every launch shape of a kernel (and the CPU oracle,
 # built with contraction off) performs the same rounding steps.

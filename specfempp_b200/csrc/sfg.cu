@@ -24,6 +24,7 @@
 #include "kernels2d_tile.cuh"
 #include "kernels2d_tile_batched.cuh"
 #include "kernels2d_row.cuh"
+#include "kernels2d_btile.cuh"
 
 namespace {
 
@@ -109,6 +110,11 @@ struct DevMedium {
   int *b_side = nullptr;
   unsigned char *b_mask = nullptr;  // per boundary point: the colours of the elements touching it
   std::vector<int> rp_off, rp_cnt;  // per tile (host)
+  // batched tiles of four elements (variant 7): elements in colour order,
+  // tile-interior index of each element point, interior points and their
+  // contributions, the points tiles share
+  int nbt = 0, nbp = 0;
+  int *bt_tel = nullptr, *bt_loc = nullptr, *bt_pt = nullptr, *bt_ctr = nullptr, *bt_bpts = nullptr;
 };
 
 }  // namespace
@@ -220,6 +226,7 @@ struct sfg_handle {
   sfg::dev::TileBArgs tileb_layout{};   // batched shots
   int tile_smem = 0, tile_blocks_per_sm = 0;
   bool b4r_attr = false;                 // shared-memory attribute of the row-form batched kernel set
+  bool btile_ok = false;                 // batched tiles of four elements (variant 7) built
   void *flush_buf = nullptr;
   size_t flush_bytes = 0;
   // sfg_step_io: one graph per step that reads the source row from and
@@ -464,6 +471,23 @@ void launch_stiffness_W(sfg_handle *h, const DevMedium &el, const DevMedium &ac,
   else if (el.ncomp == 3) launch_stiffness_E<E, 3>(h, el, ac, step, s, variant);
   else if (el.ncomp == 4) launch_stiffness_E<E, 4>(h, el, ac, step, s, variant);
   else launch_stiffness_E<E, 0>(h, el, ac, step, s, variant);
+}
+
+sfg::dev::BatchArgs batch_args(sfg_handle *h, const DevMedium &el, const int *step) {
+  sfg::dev::BatchArgs B{};
+  B.ibool = el.ibool;
+  B.xix = el.xix; B.xiz = el.xiz; B.gax = el.gax; B.gaz = el.gaz; B.jac = el.jac;
+  B.prop0 = el.prop0; B.prop1 = el.prop1;
+  B.bc_slot = el.bc_slot; B.bc_w = el.bc_w; B.bc_nx = el.bc_nx; B.bc_nz = el.bc_nz;
+  B.bc_j1 = el.bc_j1; B.bc_imp0 = el.bc_imp0; B.bc_imp1 = el.bc_imp1;
+  B.src_head = el.src_head; B.src_next = h->d_src_next; B.src_shot = h->d_src_shot;
+  B.src_arr = h->d_src_arr; B.stf = h->d_stf;
+  B.nsrc = h->asmb.nsrc; B.nstep = h->asmb.nstep;
+  B.step = step;
+  B.u = el.u; B.v = el.v; B.accum = el.accum; B.r = el.r; B.slot = el.slot;
+  B.S = el.S;
+  B.nspec_b = el.nspec;
+  return B;
 }
 
 void launch_stiffness_batched(sfg_handle *h, const DevMedium &el, const int *step, cudaStream_t s,
@@ -989,6 +1013,86 @@ void upload_tiles(sfg_handle *h) {
   h->tile_blocks_per_sm = std::max(nb, 1);
 }
 
+// Batched tiles of four elements (variant 7): consecutive groups of four of
+// the Morton-ordered 16-element tiles (2 x 2 patches on structured meshes),
+// each sorted by colour; a point is interior to a tile when only that tile's
+// elements touch it.  Needs S shots in fours, one elastic medium, and
+// receivers that record displacement only (they run before the step's
+// kernels).
+bool compute_btile_ok(const sfg_handle *h) {
+  const sfg::Assembly2D &a = h->asmb;
+  if (a.nshots <= 1 || a.nshots % 4 != 0 || a.ac.nspec || !a.el.nspec || a.el.ntiles == 0) return false;
+  if (a.el.aniso || a.el.cosserat || a.el.poro || a.el.ncomp > 2) return false;
+  for (int t : a.types)
+    if (t != SFG_SEIS_DISPLACEMENT) return false;
+  return true;
+}
+
+void upload_btiles(sfg_handle *h) {
+  namespace dv = sfg::dev;
+  const sfg::MediumData &M = h->asmb.el;
+  DevMedium &D = h->el;
+  const int n = M.nspec;
+  std::vector<int> cnt(size_t(M.nglob), 0);
+  for (size_t i = 0; i < size_t(n) * sfg::NPTS; ++i) ++cnt[M.ibool[i]];
+  std::vector<int> tel, loc(size_t(n) * sfg::NPTS, -1), tpt, tctr;
+  std::vector<char> interior(size_t(M.nglob), 0);
+  std::unordered_map<int, int> lcnt, kidx;
+  const int ngroups = M.ntiles * (sfg::TILE_E / dv::BT_E);
+  for (int gi = 0; gi < ngroups; ++gi) {
+    std::vector<int> els;
+    for (int i = 0; i < dv::BT_E; ++i) {
+      const int ce = M.tile_elem[size_t(gi) * dv::BT_E + i];
+      if (ce >= 0) els.push_back(ce);
+    }
+    if (els.empty()) continue;
+    std::stable_sort(els.begin(), els.end(), [&](int x, int y) { return M.elem_color[x] < M.elem_color[y]; });
+    const int t = int(tel.size() / dv::BT_E);
+    for (int i = 0; i < dv::BT_E; ++i) tel.push_back(i < int(els.size()) ? els[i] : -1);
+    lcnt.clear();
+    kidx.clear();
+    for (int ce : els)
+      for (int q = 0; q < sfg::NPTS; ++q) ++lcnt[M.ibool[size_t(ce) * sfg::NPTS + q]];
+    tpt.resize(size_t(t + 1) * dv::BT_MAXP, -1);
+    tctr.resize(size_t(t + 1) * dv::BT_MAXP * 4, -1);
+    for (int le = 0; le < int(els.size()); ++le)
+      for (int q = 0; q < sfg::NPTS; ++q) {
+        const int g = M.ibool[size_t(els[le]) * sfg::NPTS + q];
+        if (lcnt[g] != cnt[g]) continue;        // another tile touches it
+        auto it = kidx.find(g);
+        if (it == kidx.end()) {
+          const int k = int(kidx.size());
+          if (k >= dv::BT_MAXP) throw std::runtime_error("batched tile with too many interior points");
+          it = kidx.emplace(g, k).first;
+          tpt[size_t(t) * dv::BT_MAXP + k] = g;
+          interior[g] = 1;
+        }
+        const int k = it->second;
+        int *c = &tctr[(size_t(t) * dv::BT_MAXP + k) * 4];
+        int m = 0;
+        while (m < 4 && c[m] >= 0) ++m;
+        if (m == 4) throw std::runtime_error("batched tile point with more than four contributions");
+        c[m] = le * sfg::NPTS + q;
+        loc[size_t(els[le]) * sfg::NPTS + q] = k;
+      }
+  }
+  std::vector<int> bpts;
+  for (int g = 0; g < M.nglob; ++g)
+    if (!interior[g]) bpts.push_back(g);
+  DevMem &m = h->mem;
+  D.nbt = int(tel.size() / dv::BT_E);
+  D.nbp = int(bpts.size());
+  D.bt_tel = m.upload(tel);
+  D.bt_loc = m.upload(loc);
+  D.bt_pt = m.upload(tpt);
+  D.bt_ctr = m.upload(tctr);
+  if (bpts.empty()) bpts.push_back(0);
+  D.bt_bpts = m.upload(bpts);
+  const int smem_max = dv::BT_E * 2 * 2 * sfg::NPTS * 8 * int(sizeof(float4));
+  SFG_CUDA(cudaFuncSetAttribute(dv::k_btile_row<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max));
+  SFG_CUDA(cudaFuncSetAttribute(dv::k_btile_row<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_max / 2));
+}
+
 sfg::dev::TileMed tile_med(const DevMedium &D, int ncol, bool store_a) {
   sfg::dev::TileMed M{};
   M.hdr = D.t_hdr; M.rec = D.t_rec; M.sh = D.t_sh; M.rp = D.t_rp;
@@ -1004,6 +1108,37 @@ sfg::dev::BndMed bnd_med(const DevMedium &D, const sfg::MediumData &M) {
   B.r = D.t_r; B.b_side = D.b_side; B.b_mask = D.b_mask;
   B.nb = D.t_rec ? D.nb : 0; B.niface = M.niface; B.sh0 = M.sh0; B.ncol = ncolors(D);
   return B;
+}
+
+// Batched tiles of four elements (variant 7): the tile kernel, then the
+// points tiles share.
+void launch_btile(sfg_handle *h, bool predict, cudaStream_t s) {
+  namespace dv = sfg::dev;
+  const DevMedium &el = h->el;
+  dv::BTileArgs P{};
+  P.B = batch_args(h, el, h->d_step);
+  P.tel = el.bt_tel; P.tloc = el.bt_loc; P.tpt = el.bt_pt; P.tctr = el.bt_ctr;
+  P.minv = el.minv; P.v_out = el.v; P.u_out = el.u;
+  P.a_store = (!predict || h->opt.store_acceleration) ? el.a : nullptr;
+  const float dt = float(h->asmb.dt);
+  P.dt = dt; P.dt2 = dt / 2.0f; P.dtsq2 = dt * dt / 2.0f;
+  P.predict = predict ? 1 : 0;
+  P.flag = h->d_flag;
+  P.ntiles = el.nbt;
+  const int T = std::min(8, el.S / 4);
+  const int tiles = (el.S + 4 * T - 1) / (4 * T);
+  const int smem = dv::BT_E * el.ncomp * 2 * sfg::NPTS * T * int(sizeof(float4));
+  const dim3 grid(el.nbt, tiles);
+  if (el.nbt == 0) return;
+  if (el.ncomp == 2) dv::k_btile_row<2><<<grid, dv::BT_E * dv::NG * T, smem, s>>>(P, T);
+  else dv::k_btile_row<1><<<grid, dv::BT_E * dv::NG * T, smem, s>>>(P, T);
+}
+
+void launch_btile_shared(sfg_handle *h, bool predict, cudaStream_t s) {
+  const DevMedium &el = h->el;
+  sfg::dev::UpdateArgs U = update_args(h, el, h->ac, SFG_MEDIUM_ELASTIC, predict, true);
+  const int n4 = el.nbp * el.ncomp * el.S / 4;
+  sfg::dev::k_update_batched4_list<<<grid_for(std::max(n4, 1)), 256, 0, s>>>(U, el.S, el.ncomp, el.bt_bpts, el.nbp);
 }
 
 // The batched fused tile kernel (one elastic medium, S shots): work items
@@ -1118,6 +1253,15 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
     enqueue_tile_step(h, s, predict);
     return;
   }
+  if (h->variant == 7) {
+    // batched tiles: the receivers (displacement only) read the step's
+    // displacement first; the tile kernel finishes the tile-interior points,
+    // the list update the shared ones (and advances the step counter)
+    if (h->el.nrec > 0) launch_receivers(h, SFG_MEDIUM_ELASTIC, s);
+    launch_btile(h, predict, s);
+    launch_btile_shared(h, predict, s);
+    return;
+  }
   const bool has_el = h->el.nspec > 0, has_ac = h->ac.nspec > 0;
   if (h->recording) {
     const DevMedium &R = h->el.nspec ? h->el : h->ac;
@@ -1159,6 +1303,7 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
 
 int kernels_per_step(const sfg_handle *h) {
   if (h->variant == 5) return 2 + (h->el.nspec && h->el.nrec > 0) + (h->ac.nspec && h->ac.nrec > 0);
+  if (h->variant == 7) return 2 + (h->el.nrec > 0);
   int n = h->variant >= 3 ? 1 : std::max(ncolors(h->el), ncolors(h->ac));
   for (const DevMedium *D : {&h->ac, &h->el}) {
     if (D->nspec == 0) continue;
@@ -1222,7 +1367,7 @@ void run_steps(sfg_handle *h, int nsteps) {
 void autotune(sfg_handle *h) {
   const bool fix_e = h->opt.elements_per_block == 8 || h->opt.elements_per_block == 16 ||
                      h->opt.elements_per_block == 32;
-  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 6;
+  const bool fix_v = h->opt.kernel_variant >= 1 && h->opt.kernel_variant <= 7;
   if (fix_e) h->epb = h->opt.elements_per_block;
   if (fix_v) h->variant = h->opt.kernel_variant;
   if (h->variant == 5 && !h->tile_ok) h->variant = 3;   // the model cannot use the tile kernel
@@ -1230,6 +1375,7 @@ void autotune(sfg_handle *h) {
   // the row form: isotropic P-SV / acoustic, one shot, 16 or 32 elements per block
   if (h->variant == 6 && (h->asmb.nshots > 1 || !row_ok(h->el))) h->variant = 3;
   if (h->variant == 6 && h->epb != 16) h->epb = 32;
+  if (h->variant == 7 && !h->btile_ok) h->variant = 3;   // batched tiles of four elements
   if (h->asmb.nshots > 1 && h->variant == 2) h->variant = 1;  // no persistent batched kernel
   // batched: variant 4 is owner-computes with the row-form element kernel (shots in fours)
   if (h->asmb.nshots > 1 && h->variant == 4 && h->asmb.nshots % 4 != 0) h->variant = 3;
@@ -1241,6 +1387,7 @@ void autotune(sfg_handle *h) {
     for (int v : {1, 3, 4})
       if ((!fix_v || v == h->variant) && (v != 4 || h->asmb.nshots % 4 == 0)) cand.push_back({v, 16});
     if (h->tile_ok && (!fix_v || h->variant == 5)) cand.push_back({5, 16});
+    if (h->btile_ok && (!fix_v || h->variant == 7)) cand.push_back({7, 16});
   } else {
     for (int v : {1, 2, 3, 4}) {
       // an anisotropic medium has the colour-pass and owner-computes kernels only
@@ -1602,6 +1749,8 @@ int sfg_initialize(sfg_handle *h) {
     }
     h->tile_ok = compute_tile_ok(h);
     if (h->tile_ok) upload_tiles(h);
+    h->btile_ok = compute_btile_ok(h);
+    if (h->btile_ok) upload_btiles(h);
     autotune(h);
     h->graph_steps = std::max(1, h->opt.steps_per_graph);
     h->graph_k = capture(h, h->graph_steps, true);
@@ -1783,6 +1932,13 @@ int sfg_time_kernel_flushed(sfg_handle *h, int which, int iters, size_t flush_by
         if (which == 0) launch_tile_kernel(h, true, h->stream);
         else if (which == 1) launch_tile_boundary(h, true, h->stream);
         else if (which == 3) launch_tile_receivers(h, h->stream);
+        return;
+      }
+      if (h->variant == 7) {
+        // batched tiles: 0 the tile kernel, 1 the shared points, 3 receivers
+        if (which == 0) launch_btile(h, true, h->stream);
+        else if (which == 1) launch_btile_shared(h, true, h->stream);
+        else if (which == 3) launch_receivers(h, SFG_MEDIUM_ELASTIC, h->stream);
         return;
       }
       if (which == 0) launch_stiffness(h, h->stream);

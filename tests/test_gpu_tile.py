@@ -210,3 +210,45 @@ def test_batched_tile_kernel_fixtures(sfg_lib, name):
     zs = [float(z) for z in case.rec_z]
     srcs = _batched_shots(8, 11, (min(xs), max(xs)), (min(zs), max(zs)))
     _batched_equal(case, srcs, 8, ("displacement", "velocity", "acceleration"))
+
+
+# ---------------------------------------------------------------------------
+# Batched tiles of four elements (variant 7): tile-interior points assembled
+# and finished in the tile kernel, shared points by the list update;
+# displacement receivers.
+
+def _btile_equal(case, srcs, nshots, pieces=(None,)):
+    types = ("displacement",)
+    s1 = _batched_run(case, srcs, nshots, types, 1)
+    s7 = _batched_run(case, srcs, nshots, types, 7, pieces)
+    assert s7.info().kernel_variant == 7
+    a, b = s1.seismograms(), s7.seismograms()
+    assert np.abs(a).max() > 0
+    assert np.array_equal(a, b), float(np.abs(a - b).max() / np.abs(a).max())
+    for f in ("displacement", "velocity", "acceleration"):
+        fa, fb = s1.field("elastic", f), s7.field("elastic", f)
+        assert np.abs(fa).max() > 0
+        assert np.array_equal(fa, fb), f
+    assert s7.check_finite()
+
+
+@pytest.mark.parametrize("nshots", [4, 8, 36])
+def test_batched_four_element_tiles_elastic_80x60(sfg_lib, nshots):
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_psv_80x60(nstep=300)
+    _btile_equal(workload_case(w), _batched_shots(nshots, 5, (600, 3400), (600, 2600)), nshots)
+
+
+def test_batched_four_element_tiles_grf_in_pieces(sfg_lib):
+    from specfempp_b200 import meshgen
+    w = meshgen.elastic_grf_1000x500(nstep=120, nshots=8, nx=100, nz=50)
+    _btile_equal(workload_case(w), w.sources, 8, pieces=(50, 1, 69))
+
+
+@pytest.mark.parametrize("name", ["HomogeneousElasticDomainStaceyDirichletBC", "HomogeneousElasticIsotropicDomainSH"])
+def test_batched_four_element_tiles_fixtures(sfg_lib, name):
+    case, _, _ = golden_case(name)
+    case.nstep = min(case.nstep, 600)
+    xs = [float(x) for x in case.rec_x]
+    zs = [float(z) for z in case.rec_z]
+    _btile_equal(case, _batched_shots(8, 11, (min(xs), max(xs)), (min(zs), max(zs))), 8)
