@@ -274,7 +274,7 @@ def bench_adjoint(args, world, barrier, max_over_ranks):
     out = {"workload": f"elastic_adjoint_{nx}x{nz}", "nglob": inf.nglob, "steps": nstep,
            "sources": len(srcs), "checkpoint_interval": aw.interval,
            "segments": -(-nstep // aw.interval), "segments_kept_from_forward": sim.adjoint_buffers(),
-           "segment_budget": "default: 60% of the free device memory", "forward_s": t_fwd,
+           "segment_budget": "default: 75% of the free device memory", "forward_s": t_fwd,
            "gradient_s": t_grad, "cost_ratio": t_grad / t_fwd,
            "gradient_gll_pt_steps_per_s": inf.nglob * nstep * len(srcs) / t_grad,
            "timing": "wall clock around synchronous calls; forward = plain runs of every source; "

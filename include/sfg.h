@@ -300,7 +300,7 @@ int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval);
  * interval of recorded forward states).  The forward run records its last
  * segments into them on the way, as many as the buffers hold, so that the
  * reverse sweep recomputes only the earlier segments; bytes = 0 (the
- * default) takes 60% of the device memory free when the buffers are
+ * default) takes 75% of the device memory free when the buffers are
  * allocated (at the next sfg_forward_checkpointed); at least two buffers are
  * always kept.  Gradients do not depend on it (bit for bit).  No counterpart
  * in the reference, whose combined run reads the whole forward wavefield

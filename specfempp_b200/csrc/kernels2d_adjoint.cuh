@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(NP * E) k_adj_elem(AdjArgs A) {
 // gamma-direction ones from shared-memory columns.  Per point the
 // operations and their order are those of k_adj_elem (same bits).
 template <int E>
-__global__ void __launch_bounds__(NG * E, 5) k_adj_elem_row(AdjArgs A) {
+__global__ void __launch_bounds__(NG * E, 4) k_adj_elem_row(AdjArgs A) {
   __shared__ float2 sm2[E][NP], su2[E][NP], sF1[E][NP];
   const int tid = threadIdx.x;
   const int le = tid / NG, iz = tid - le * NG;
@@ -182,6 +182,14 @@ __global__ void __launch_bounds__(NG * E, 5) k_adj_elem_row(AdjArgs A) {
     su2[le][iz * NG + ix] = ur[ix];
   }
   const int rh = act ? __ldg(A.ad_head + e) : -1;
+  // the row's Jacobian and material words, requested with the gathers
+  float gxix[NG], gxiz[NG], ggax[NG], ggaz[NG], gjac[NG], gc0[NG], gmu[NG];
+#pragma unroll
+  for (int ix = 0; ix < NG; ++ix) {
+    gxix[ix] = __ldg(A.xix + pe + ix); gxiz[ix] = __ldg(A.xiz + pe + ix);
+    ggax[ix] = __ldg(A.gax + pe + ix); ggaz[ix] = __ldg(A.gaz + pe + ix);
+    gjac[ix] = __ldg(A.jac + pe + ix); gc0[ix] = __ldg(A.prop0 + pe + ix); gmu[ix] = __ldg(A.prop1 + pe + ix);
+  }
   float hz[NG];
 #pragma unroll
   for (int l = 0; l < NG; ++l) hz[l] = c_hp[iz * NG + l];
@@ -207,9 +215,8 @@ __global__ void __launch_bounds__(NG * E, 5) k_adj_elem_row(AdjArgs A) {
 #pragma unroll
   for (int ix = 0; ix < NG; ++ix) {
     const size_t p = pe + ix;
-    const float xix = __ldg(A.xix + p), xiz = __ldg(A.xiz + p), gax = __ldg(A.gax + p),
-                gaz = __ldg(A.gaz + p), jac = __ldg(A.jac + p);
-    const float c0 = __ldg(A.prop0 + p), mu = __ldg(A.prop1 + p);
+    const float xix = gxix[ix], xiz = gxiz[ix], gax = ggax[ix], gaz = ggaz[ix], jac = gjac[ix];
+    const float c0 = gc0[ix], mu = gmu[ix];
     float2 gm = make_float2(0.f, 0.f), gu = make_float2(0.f, 0.f);
 #pragma unroll
     for (int l = 0; l < NG; ++l) {

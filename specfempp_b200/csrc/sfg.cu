@@ -2299,7 +2299,7 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   const int ncheck = (nstep + interval - 1) / interval;
   const int nst = int(adj_data(h).stacey_pt.size());
   const size_t vstride = ((2 * size_t(nst) + 3) / 4) * 4 + 4;
-  // segment buffers: as many as the budget holds (default: 60% of the device
+  // segment buffers: as many as the budget holds (default: 75% of the device
   // memory free before they are allocated), at least 2, at most ncheck
   const size_t seg_bytes = size_t(interval) * (2 * stride + vstride) * sizeof(float);
   size_t budget = A.budget;
@@ -2307,7 +2307,7 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     size_t fr = 0, tot = 0;
     SFG_CUDA(cudaMemGetInfo(&fr, &tot));
     const size_t held = A.seg_u ? size_t(A.nbuf) * size_t(A.interval) * (2 * A.stride + A.vstride) * sizeof(float) : 0;
-    budget = size_t(0.6 * double(fr + held));
+    budget = size_t(0.75 * double(fr + held));
   }
   const int nbuf = int(std::max<size_t>(2, std::min<size_t>(size_t(std::max(ncheck, 2)), budget / seg_bytes)));
   if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck || A.nbuf != nbuf) {

@@ -364,7 +364,7 @@ class Simulation2D:
         return self.seismograms()[0, :nsteps, 0]
 
     def set_adjoint_budget(self, nbytes: int):
-        """Device bytes for the adjoint's segment buffers (0: 60% of the free
+        """Device bytes for the adjoint's segment buffers (0: 75% of the free
         memory); the forward run keeps as many recorded segments as they hold."""
         self._check(self.lib.sfg_set_adjoint_budget(self.h, int(nbytes)))
 
