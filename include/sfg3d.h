@@ -71,8 +71,9 @@ int sfg3d_initialize(sfg_handle3d *h);
 int sfg3d_run(sfg_handle3d *h, int nsteps);
 /* nsteps steps timed with CUDA events on the handle's stream (ms). */
 int sfg3d_run_timed(sfg_handle3d *h, int nsteps, float *ms);
-/* The same with a write of flush_bytes (larger than L2) before every step,
- * timing the steps only. */
+/* The same with an L2 flush before every step (a write of flush_bytes,
+ * larger than L2, then a read of a second buffer of that size, so that the
+ * cache holds no dirty lines when the step starts), timing the steps only. */
 int sfg3d_run_timed_flushed(sfg_handle3d *h, int nsteps, size_t flush_bytes, float *ms);
 /* One step with host input/output: stf_row [nsrc] (pinned host memory, this
  * step's source-time values) copied in, the step's seismogram row
