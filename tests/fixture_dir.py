@@ -57,3 +57,33 @@ def write_fixture_dir(npz_path, out_dir, types=("displacement",)):
     with open(path, "w") as f:
         yaml.safe_dump(cfg, f)
     return path, z
+
+
+def write_fixture_dir3d(npz_path, out_dir, types=("displacement", "velocity", "acceleration")):
+    """The 3D fixture's run directory: its own database.bin, STATIONS and
+    force.yaml (stored verbatim in the npz) plus a specfem_config.yaml with
+    the fixture's dt and nstep."""
+    z = np.load(npz_path)
+    os.makedirs(out_dir, exist_ok=True)
+    with open(os.path.join(out_dir, "database.bin"), "wb") as f:
+        f.write(z["database"].tobytes())
+    with open(os.path.join(out_dir, "STATIONS"), "w") as f:
+        f.write(str(z["stations_text"][()]))
+    with open(os.path.join(out_dir, "force.yaml"), "w") as f:
+        f.write(str(z["sources_text"][()]))
+    cfg = {"parameters": {
+        "simulation-setup": {
+            "quadrature": {"quadrature-type": "GLL4"},
+            "solver": {"time-marching": {"type-of-simulation": "forward",
+                                         "time-scheme": {"type": "Newmark", "dt": float(z["dt"]),
+                                                         "nstep": int(z["nstep"])}}},
+            "simulation-mode": {"forward": {"writer": {"seismogram": {"format": "ascii", "directory": "traces"}}}}},
+        "receivers": {"stations": "STATIONS", "angle": 0.0, "seismogram-type": list(types),
+                      "nstep_between_samples": 1},
+        "run-setup": {"number-of-processors": 1, "number-of-runs": 1},
+        "databases": {"mesh-database": "database.bin"},
+        "sources": "force.yaml"}}
+    path = os.path.join(out_dir, "specfem_config.yaml")
+    with open(path, "w") as f:
+        yaml.safe_dump(cfg, f)
+    return path, z

@@ -132,7 +132,9 @@ def make3d(ref_root: str) -> str:
     """The 3D fixture: a regular 8 x 6 x 6 hexahedral mesh over 8 x 7 x 7.5 km
     (NEX_XI, NEX_ETA, depth and the single region of its Mesh_Par_file), one
     homogeneous material, no absorbing boundary; stations in the 3D format
-    (station, network, y, x, elevation, z)."""
+    (station, network, y, x, elevation, z); the bytes of its database.bin
+    (the 3D mesher's output) and its STATIONS and source files as text, so
+    that the 3D configuration driver can be run on the fixture itself."""
     import yaml
     d = os.path.join(ref_root, "tests/unit-tests/displacement_tests/Newmark/serial/dim3", FIXTURE_3D)
     with open(os.path.join(d, "specfem_config.yaml")) as f:
@@ -173,7 +175,10 @@ def make3d(ref_root: str) -> str:
                         src_f0=float(rk["f0"]), src_factor=float(rk["factor"]), src_tshift=float(rk["tshift"]),
                         dt=float(ts["dt"]), nstep=nstep, rec_xyz=np.array(xyz), stations=np.array(names),
                         traces_semd=traces["semd"], traces_semv=traces["semv"], traces_sema=traces["sema"],
-                        trace_t0=t0)
+                        trace_t0=t0, database=np.frombuffer(open(os.path.join(d, "database.bin"), "rb").read(),
+                                                            np.uint8),
+                        stations_text=open(os.path.join(d, "STATIONS")).read(),
+                        sources_text=open(os.path.join(d, "force.yaml")).read())
     return out
 
 
@@ -181,9 +186,10 @@ if __name__ == "__main__":
     if len(sys.argv) < 2:
         sys.exit("usage: make_golden.py REFERENCE_ROOT [FIXTURE ...]  (the SPECFEM++ checkout to read)")
     root = sys.argv[1]
-    names = sys.argv[2:] or list(FIXTURES)
+    names = sys.argv[2:] or list(FIXTURES) + [FIXTURE_3D]
     for name in names:
+        if name == FIXTURE_3D:
+            out = make3d(root)
+            print(out, os.path.getsize(out))
+            continue
         print(make(root, name, FIXTURES[name]), os.path.getsize(os.path.join(HERE, f"{name}.npz")))
-    if not sys.argv[2:]:
-        out = make3d(root)
-        print(out, os.path.getsize(out))

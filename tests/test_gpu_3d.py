@@ -112,3 +112,38 @@ def test_3d_absorbing_energy_decays(sfg_lib):
         late[absorb] = (e[1200:].max(), e.max())
     assert late[1][0] < 1e-3 * late[1][1]
     assert late[1][0] < 1e-2 * late[0][0]
+
+
+def test_specfem3d_config_driver(sfg_lib, oracle_lib, tmp_path):
+    """The 3D configuration driver on the dim3 fixture's own run directory
+    (its database.bin, STATIONS and force.yaml): the written
+    ``NET.STA.S3.BX?.sem?`` traces against the golden SPECFEM3D traces
+    (sum|d|/sum|ref| < 1e-3 per station) and against the oracle FP32 on the
+    mesh read from the database (relative L2 as above)."""
+    import os
+    from conftest import GOLDEN
+    from fixture_dir import write_fixture_dir3d
+    from oracle import runner3d
+    from specfempp_b200 import database3d, specfem3d
+    cfg, z = write_fixture_dir3d(os.path.join(GOLDEN, "HomogeneousHalfspaceSmallNoABCForceSource.npz"),
+                                 str(tmp_path))
+    out = specfem3d.run_config(cfg, root=str(tmp_path))
+    assert out["lattice"] == [8, 6, 6] and out["files"] == len(z["stations"]) * 3 * 3
+    mesh = database3d.lattice_mesh(database3d.read_database3d(str(tmp_path / "database.bin")))
+    (s,) = specfem3d.read_sources3d(str(tmp_path / "force.yaml"))
+    case = runner3d.Case3D(mesh, [runner3d.Source3D(s.x, s.y, s.z, f0=s.f0, factor=s.factor, kind=s.kind,
+                                                    comp=s.comp, tshift=s.tshift)],
+                           z["rec_xyz"], float(z["dt"]), int(z["nstep"]), list(TYPES))
+    ref = runner3d.run(case, "f32", nthreads=8)["seis"]           # [nstep, ntypes, nrec, 3]
+    for t, (kind, ext) in enumerate(zip(TYPES, ("semd", "semv", "sema"))):
+        got = np.zeros((len(z["stations"]), 3, int(z["nstep"])))
+        for r, st in enumerate(z["stations"]):
+            for c, ch in enumerate(("BXX", "BXY", "BXZ")):
+                tt, v = np.loadtxt(os.path.join(out["output_directory"], f"{st}.S3.{ch}.{ext}")).T
+                assert abs(tt[0] - float(z["trace_t0"])) < 1e-6
+                got[r, c] = v
+        tr = z[f"traces_{ext}"]
+        err = np.abs(got - tr).sum(axis=(1, 2)) / np.abs(tr).sum(axis=(1, 2))
+        assert err.max() < 1e-3, (kind, err.max())
+        # the files hold 7 significant digits (%e), well inside the bar
+        assert rel_l2(np.transpose(got, (2, 0, 1)), ref[:, t]) <= tol(kind), kind
