@@ -312,7 +312,11 @@ int sfg_adjoint_buffers(sfg_handle *h);
  * ([nspec][25], database element order) given seis_grad = dL/d(seismogram)
  * [nsteps][nrec][2]: the reverse sweep recomputes each checkpoint segment
  * that the forward run did not keep and runs the discrete adjoint of the
- * time step.  Replaces the reference's
+ * time step.  Models: one isotropic elastic (P-SV or SH, displacement
+ * seismograms) or acoustic (pressure seismograms) medium, or a coupled
+ * acoustic-elastic model with conforming interfaces and either displacement
+ * seismograms at receivers in the elastic medium or pressure seismograms at
+ * receivers in the acoustic medium; else SFG_ERR_UNSUPPORTED.  Replaces the reference's
  * combined adjoint/backward run and compute_material_derivatives
  * (core/specfem/solver/time_marching.tpp:133-264,
  *  include/kokkos_kernels/impl/compute_material_derivatives.tpp:14-153). */

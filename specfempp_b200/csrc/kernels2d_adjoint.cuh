@@ -43,6 +43,11 @@
 // kappa, and pressure seismograms d_k = -R chi_dd'_k enter as -R^T g_k on
 // the adjoint acceleration (k_adj_psrc), not on lu (the reference's acoustic
 // kernels: include/medium/dim2/acoustic/isotropic/frechet_derivative.hpp:61-93).
+//
+// Coupled acoustic-elastic step (conforming interface): both media's sweeps
+// in one reverse step, joined by the transposed coupling of AdjCoupling
+// (the reference's combined run over both media:
+// include/kokkos_kernels/frechet_kernels.hpp:37-49, compute_coupling.tpp:21-115).
 #pragma once
 
 #include "kernels2d_batched.cuh"
@@ -404,30 +409,51 @@ __global__ void __launch_bounds__(128) k_adj_psrc(float *__restrict__ mu, const 
 // element point (t = s * 25 + q) sum mu_k(g) f_k over the steps (the kappa
 // derivative of the source term is -that * l / kappa^2), for step k =
 // *seg_k0 + slot.
+// src_id (null: s itself) is the source's column in the STF table [nstep][stf_cols]
+// when only some of the model's sources lie in the acoustic medium.
 __global__ void __launch_bounds__(128) k_adj_srcterm(float *__restrict__ acc, const float *__restrict__ mu,
                                                      const int *__restrict__ ibool, const int *__restrict__ src_ce,
                                                      const float *__restrict__ stf, const int *__restrict__ seg_k0,
-                                                     int slot, int nsrc, int nstep) {
+                                                     int slot, int nsrc, int nstep, const int *__restrict__ src_id,
+                                                     int stf_cols) {
   const int k = *seg_k0 + slot;
   if (k >= nstep) return;
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nsrc * NP; t += gridDim.x * blockDim.x) {
     const int s = t / NP, q = t - s * NP;
     const int g = ibool[size_t(src_ce[s]) * NP + q];
-    acc[t] += mu[g] * stf[size_t(k) * nsrc + s];
+    acc[t] += mu[g] * stf[size_t(k) * stf_cols + (src_id ? src_id[s] : s)];
   }
 }
 
+// Transposed acoustic-elastic coupling of a conforming interface (one
+// partner per interface point), for the coupled sweep.  Forward, the
+// acoustic force at interface point p takes n_p . u~_el(q_p) and the elastic
+// force at q takes n'_q chi_dd'(p_q) (k_update / coupling_entry).  So
+//   elastic lu~(q) += n_p mu_ac(p)        (p = other[q], n = the acoustic normal at p)
+//   acoustic adjoint of chi_dd'(p) += n'_q . mu_el(q)   (q = other[p], n' = the elastic normal at q)
+// other, nx, nz are indexed by this medium's interface point (< niface);
+// omu is the other medium's mu.
+struct AdjCoupling {
+  const int *__restrict__ other;
+  const float *__restrict__ nx, *__restrict__ nz;
+  const float *__restrict__ omu;
+  int niface;
+};
+
 // Per point: lu~ = lu + sum of the element-point results (colour order);
 // G += mu_k . a'_k; then the transposed predictor and mu_(k-1).  lv holds
-// lv~ (Stacey already applied).  One thread per point.
-template <int NC>
+// lv~ (Stacey already applied).  One thread per point.  CPL (coupled sweep):
+// the elastic post (NC 2) adds the acoustic mu_k to lu~ at interface points,
+// the acoustic post (NC 1, after the elastic one) adds the elastic mu_(k-1)
+// to the adjoint acceleration before B.
+template <int NC, bool CPL = false>
 __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float *__restrict__ lv,
                                                   float *__restrict__ mu, float *__restrict__ grho,
                                                   const float *__restrict__ af,
                                                   const float *__restrict__ minv,
                                                   const float *__restrict__ r,
                                                   const int *__restrict__ inv_start, int npts, float dt,
-                                                  float dt2, float dtsq2) {
+                                                  float dt2, float dtsq2, AdjCoupling cp = AdjCoupling{}) {
   for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < npts; g += gridDim.x * blockDim.x) {
     float s[NC];
 #pragma unroll
@@ -435,6 +461,17 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
     for (int k = inv_start[g]; k < inv_start[g + 1]; ++k) {
 #pragma unroll
       for (int c = 0; c < NC; ++c) s[c] = s[c] + r[size_t(k) * NC + c];
+    }
+    float cpa = 0.f;
+    if (CPL && g < cp.niface) {
+      const int o2 = cp.other[g];
+      if (NC == 2) {
+        const float m = cp.omu[o2];
+        s[0] = s[0] + cp.nx[g] * m;
+        s[NC - 1] = s[NC - 1] + cp.nz[g] * m;
+      } else {
+        cpa = cp.nx[g] * cp.omu[2 * size_t(o2)] + cp.nz[g] * cp.omu[2 * size_t(o2) + 1];
+      }
     }
     const size_t o = size_t(g) * NC;
     float ma = mu[o] * af[o];
@@ -445,7 +482,8 @@ __global__ void __launch_bounds__(256) k_adj_post(float *__restrict__ lu, float 
       const float l = lu[o + c] + s[c];
       const float v = lv[o + c];
       const float nv = dt * l + v;
-      const float la = dtsq2 * l + dt2 * v;
+      float la = dtsq2 * l + dt2 * v;
+      if (CPL && NC == 1) la = la + cpa;
       lu[o + c] = l;
       lv[o + c] = nv;
       mu[o + c] = __fmul_rn(minv[o + c], __fadd_rn(la, __fmul_rn(dt2, nv)));

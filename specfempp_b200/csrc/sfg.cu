@@ -174,10 +174,19 @@ struct AdjointState {
   int nps = 0;
   int *ps_pt = nullptr, *ps_start = nullptr, *ps_rec = nullptr;
   float *ps_h = nullptr;
+  // coupled sweep: acoustic sources' STF columns; transposed coupling of this
+  // medium's interface points (partner, partner-side normal)
+  int *src_id = nullptr;
+  std::vector<int> src_list, src_ce_h;
+  int *cp_other = nullptr;
+  float *cp_nx = nullptr, *cp_nz = nullptr;
 };
 
 struct sfg_handle {
-  AdjointState adj;
+  // adjoint: adj holds the sweep's control and the (first) medium's state;
+  // adj2 the acoustic medium's state in a coupled model (adj_coupled)
+  AdjointState adj, adj2;
+  bool adj_coupled = false;
   // update_args: record u~ and a' of each step (adjoint); 2 = recompute
   // (seismograms are those of the forward run and are not computed again)
   int recording = 0;
@@ -239,12 +248,16 @@ struct sfg_handle {
   sfg::dev::Quad quad{};
 
   ~sfg_handle() {
-    for (void *p : {(void *)adj.ckpt, (void *)adj.seg_u, (void *)adj.seg_a, (void *)adj.lu, (void *)adj.lv,
-                    (void *)adj.mu, (void *)adj.r, (void *)adj.sum, (void *)adj.comp, (void *)adj.seg,
-                    (void *)adj.gtab, (void *)adj.ad_head, (void *)adj.ad_next, (void *)adj.st_pt,
-                    (void *)adj.st_c, (void *)adj.d_rec, (void *)adj.seg_v, (void *)adj.lb_g,
-                    (void *)adj.lb_j, (void *)adj.lb_geo})
-      if (p) cudaFree(p);
+    for (const AdjointState *A : {&adj, &adj2})
+      for (void *p : {(void *)A->ckpt, (void *)A->seg_u, (void *)A->seg_a, (void *)A->lu, (void *)A->lv,
+                      (void *)A->mu, (void *)A->r, (void *)A->sum, (void *)A->comp, (void *)A->seg,
+                      (void *)A->ad_head, (void *)A->ad_next, (void *)A->st_pt, (void *)A->st_c,
+                      (void *)A->d_rec, (void *)A->seg_v, (void *)A->lb_g, (void *)A->lb_j, (void *)A->lb_geo,
+                      (void *)A->src_ce, (void *)A->ps_pt, (void *)A->ps_start, (void *)A->ps_rec,
+                      (void *)A->ps_h, (void *)A->src_id, (void *)A->cp_other, (void *)A->cp_nx,
+                      (void *)A->cp_nz})
+        if (p) cudaFree(p);
+    if (adj.gtab) cudaFree(adj.gtab);
     if (adj.h_stage) cudaFreeHost(adj.h_stage);
     if (io_host) cudaFreeHost(io_host);
     if (graph_io) cudaGraphExecDestroy(graph_io);
@@ -629,7 +642,7 @@ sfg::dev::UpdateArgs update_args(sfg_handle *h, const DevMedium &D, const DevMed
   U.flag = h->d_flag;
   U.step = h->d_step;
   U.advance = advance && !h->recording ? 1 : 0;
-  if (h->recording) U.rec = h->adj.d_rec;
+  if (h->recording) U.rec = (h->adj_coupled && medium == SFG_MEDIUM_ACOUSTIC) ? h->adj2.d_rec : h->adj.d_rec;
   return U;
 }
 
@@ -1267,6 +1280,7 @@ void enqueue_step(sfg_handle *h, cudaStream_t s, bool predict) {
     const DevMedium &R = h->el.nspec ? h->el : h->ac;
     if (R.ncomp == 1) sfg::dev::k_record_begin<1><<<1, 512, 0, s>>>(h->adj.d_rec, R.v, h->d_step);
     else sfg::dev::k_record_begin<2><<<1, 512, 0, s>>>(h->adj.d_rec, R.v, h->d_step);
+    if (h->adj_coupled) sfg::dev::k_record_begin<1><<<1, 512, 0, s>>>(h->adj2.d_rec, h->ac.v, h->d_step);
   }
   // a recorded (recomputed) step's seismograms are those of the forward run
   const bool rec_ac = has_ac && h->ac.nrec > 0 && h->recording != 2;
@@ -2269,16 +2283,47 @@ DevMedium &adj_dev(sfg_handle *h) { return h->el.nspec ? h->el : h->ac; }
 const sfg::MediumData &adj_data(const sfg_handle *h) { return h->el.nspec ? h->asmb.el : h->asmb.ac; }
 bool adj_acoustic(const sfg_handle *h) { return h->el.nspec == 0; }
 
+// A coupled model's two interface point lists pair one to one (conforming
+// edges): every acoustic interface point p has the elastic partner q =
+// ac.cp_other[p] whose partner is p again.
+bool conforming_pairs(const sfg::Assembly2D &a) {
+  const sfg::MediumData &E = a.el, &A = a.ac;
+  if (!E.cp_start.empty() || !A.cp_start.empty() || E.niface != A.niface) return false;
+  for (int p = 0; p < A.niface; ++p) {
+    const int q = A.cp_other[p];
+    if (q < 0 || q >= E.niface || E.cp_other[q] != p) return false;
+  }
+  return true;
+}
+
 int adjoint_checks(sfg_handle *h) {
   if (!h->initialized) { h->err = "sfg_initialize first"; return SFG_ERR_STATE; }
   const sfg::Assembly2D &a = h->asmb;
-  const bool one = (h->el.nspec > 0) != (h->ac.nspec > 0);
+  if (h->el.nspec > 0 && h->ac.nspec > 0) {
+    // coupled acoustic-elastic model: isotropic P-SV, conforming interfaces,
+    // displacement seismograms at elastic receivers or pressure seismograms
+    // at acoustic receivers
+    bool ok = !h->el.aniso && h->el.ncomp == 2 && h->el.S == 1 && a.nsb == 1 && a.ntypes == 1 &&
+              conforming_pairs(a) &&
+              (a.types[0] == SFG_SEIS_DISPLACEMENT || a.types[0] == SFG_SEIS_PRESSURE);
+    const int rec_medium = ok && a.types[0] == SFG_SEIS_PRESSURE ? SFG_MEDIUM_ACOUSTIC : SFG_MEDIUM_ELASTIC;
+    for (int r = 0; ok && r < a.nrec; ++r) ok = a.rec_medium[r] == rec_medium;
+    if (!ok) {
+      h->err = "the coupled adjoint needs isotropic elastic P-SV and acoustic media with conforming interfaces, "
+               "one shot, seismograms sampled every step: displacement at receivers in the elastic medium or "
+               "pressure at receivers in the acoustic medium";
+      return SFG_ERR_UNSUPPORTED;
+    }
+    h->adj_coupled = true;
+    return SFG_OK;
+  }
   const int want = h->el.nspec ? SFG_SEIS_DISPLACEMENT : SFG_SEIS_PRESSURE;
-  if (!one || h->el.aniso || h->el.ncomp >= 3 || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
+  if (h->el.aniso || h->el.ncomp >= 3 || adj_dev(h).S != 1 || a.nsb != 1 || a.ntypes != 1 || a.types[0] != want) {
     h->err = "the adjoint needs one medium (isotropic elastic P-SV or SH with displacement seismograms, "
-             "or acoustic with pressure seismograms), one shot, seismograms sampled every step";
+             "or acoustic with pressure seismograms) or a coupled pair, one shot, seismograms sampled every step";
     return SFG_ERR_UNSUPPORTED;
   }
+  h->adj_coupled = false;
   return SFG_OK;
 }
 
@@ -2290,33 +2335,161 @@ T *dalloc(size_t n) {
   return p;
 }
 
+// Sizes of one medium's adjoint arrays.
+void adj_medium_sizes(AdjointState &A, const DevMedium &D, const sfg::MediumData &M) {
+  A.nvals = D.values();
+  A.nloc = size_t(D.nspec) * sfg::NPTS;
+  A.stride = ((A.nvals + 3) / 4) * 4 + 4;
+  A.nglob = size_t(D.nglob);
+  A.vstride = ((2 * M.stacey_pt.size() + 3) / 4) * 4 + 4;
+}
+
+size_t adj_segment_bytes(const AdjointState &A, int interval) {
+  return size_t(interval) * (2 * A.stride + A.vstride) * sizeof(float);
+}
+
+// Checkpoints and segment buffers of one medium.
+void adj_medium_segments(AdjointState &A, int ncheck, int nbuf, int interval) {
+  for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a, &A.seg_v})
+    if (*p) { cudaFree(*p); *p = nullptr; }
+  A.ckpt = dalloc<float>(size_t(ncheck) * 3 * (A.nvals + 4));
+  A.seg_u = dalloc<float>(size_t(nbuf) * interval * A.stride);
+  A.seg_a = dalloc<float>(size_t(nbuf) * interval * A.stride);
+  A.seg_v = dalloc<float>(size_t(nbuf) * interval * A.vstride);
+}
+
+template <typename T>
+T *dupload(const std::vector<T> &v) {
+  T *p = dalloc<T>(v.size());
+  if (!v.empty()) SFG_CUDA(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return p;
+}
+
+// One medium's sweep state (once per handle): adjoint fields, element-point
+// results, gradient sums, the element-local Stacey points, receivers as
+// adjoint sources (displacement: per element chain; pressure: per point
+// CSR), the acoustic sources' columns and, in a coupled model, the
+// transposed coupling of the interface points.
+void adj_medium_init(sfg_handle *h, AdjointState &A, const DevMedium &D, const sfg::MediumData &M, int medium) {
+  const sfg::Assembly2D &as = h->asmb;
+  const bool acoustic = medium == SFG_MEDIUM_ACOUSTIC;
+  const size_t nvals = A.nvals, nloc = A.nloc;
+  A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
+  A.r = dalloc<float>(2 * nloc);
+  // element-local Stacey points: global point, Stacey slot, geometry
+  std::unordered_map<int, int> slot;
+  for (size_t j = 0; j < M.stacey_pt.size(); ++j) slot[M.stacey_pt[j]] = int(j);
+  std::vector<int> lg, lj;
+  std::vector<float> geo;
+  A.lb_k.clear();
+  A.lb_pm.clear();
+  for (int ce = 0; ce < M.nspec; ++ce) {
+    if (M.bc_slot[ce] < 0) continue;
+    for (int q = 0; q < sfg::NPTS; ++q) {
+      const size_t k = size_t(M.bc_slot[ce]) * sfg::NPTS + q;
+      if (M.bc_w[k] == 0.0f) continue;
+      const int g = M.ibool[size_t(ce) * sfg::NPTS + q];
+      lg.push_back(g);
+      lj.push_back(slot.at(g));
+      // P-SV: the normal; SH and acoustic: x is the free-surface mask (1 in SH)
+      geo.insert(geo.end(), {M.ncomp == 2 ? M.bc_nx[k] : M.bc_keep[k], M.bc_nz[k], M.bc_j1[k], M.bc_w[k]});
+      A.lb_k.push_back(k);
+      A.lb_pm.push_back(size_t(M.elem_mesh[ce]) * sfg::NPTS + q);
+    }
+  }
+  A.nlb = int(lg.size());
+  A.off_lb = ((2 * nloc + A.nglob + 3) / 4) * 4;
+  // acoustic sources (their STF columns)
+  A.src_list.clear();
+  if (acoustic)
+    for (int si = 0; si < as.nsrc; ++si)
+      if (as.src_medium[si] == SFG_MEDIUM_ACOUSTIC) A.src_list.push_back(si);
+  A.nsrc_t = int(A.src_list.size());
+  A.src_ce = dalloc<int>(std::max(A.nsrc_t, 1));
+  A.src_id = dupload(A.src_list);
+  A.lb_g = dupload(lg); A.lb_j = dupload(lj); A.lb_geo = dupload(geo);
+  A.sum = dalloc<float>(A.nsum()); A.comp = dalloc<float>(A.nsum()); A.seg = dalloc<float>(A.nsum());
+  // displacement receivers of this medium as adjoint sources: chain per
+  // compute element
+  const bool disp = as.ntypes > 0 && as.types[0] == SFG_SEIS_DISPLACEMENT;
+  std::vector<int> head(D.nspec, -1), next(std::max(as.nrec, 1), -1);
+  for (int r = 0; r < as.nrec; ++r) {
+    if (!disp || as.rec_medium[r] != medium) continue;
+    next[r] = head[as.rec_elem[r]];
+    head[as.rec_elem[r]] = r;
+  }
+  A.ad_head = dupload(head);
+  A.ad_next = dupload(next);
+  // pressure receivers (acoustic): points they touch, with receiver and weight
+  A.pressure = acoustic && as.ntypes > 0 && as.types[0] == SFG_SEIS_PRESSURE;
+  if (A.pressure) {
+    std::vector<std::vector<std::pair<int, float>>> by_pt(D.nglob);
+    for (int r = 0; r < as.nrec; ++r) {
+      if (as.rec_medium[r] != SFG_MEDIUM_ACOUSTIC) continue;
+      for (int q = 0; q < sfg::NPTS; ++q) {
+        const float hq = as.rec_h[size_t(r) * sfg::NPTS + q];
+        if (hq != 0.0f) by_pt[M.ibool[size_t(as.rec_elem[r]) * sfg::NPTS + q]].push_back({r, hq});
+      }
+    }
+    std::vector<int> pt, start{0}, rr;
+    std::vector<float> hw;
+    for (int g = 0; g < D.nglob; ++g) {
+      if (by_pt[g].empty()) continue;
+      pt.push_back(g);
+      for (auto &[r, hq] : by_pt[g]) { rr.push_back(r); hw.push_back(hq); }
+      start.push_back(int(rr.size()));
+    }
+    A.nps = int(pt.size());
+    A.ps_pt = dupload(pt); A.ps_start = dupload(start); A.ps_rec = dupload(rr); A.ps_h = dupload(hw);
+  }
+  A.nst = int(M.stacey_pt.size());
+  A.st_pt = dupload(M.stacey_pt);
+  A.st_c = dupload(M.stacey_c);
+  if (h->adj_coupled) {
+    // partner of each interface point and the partner side's normal
+    const sfg::MediumData &O = acoustic ? as.el : as.ac;
+    std::vector<int> other(M.niface);
+    std::vector<float> nx(M.niface), nz(M.niface);
+    for (int i = 0; i < M.niface; ++i) {
+      other[i] = M.cp_other[i];
+      nx[i] = O.cp_nx[other[i]];
+      nz[i] = O.cp_nz[other[i]];
+    }
+    A.cp_other = dupload(other); A.cp_nx = dupload(nx); A.cp_nz = dupload(nz);
+  }
+  A.d_rec = dalloc<sfg::dev::SegRecord>(1);
+}
+
+void adj_write_record(AdjointState &A) {
+  sfg::dev::SegRecord rec{A.seg_u, A.seg_a, A.stride, 0, A.seg_v, A.vstride, A.st_pt, A.nst, 0};
+  SFG_CUDA(cudaMemcpy(A.d_rec, &rec, sizeof(rec), cudaMemcpyHostToDevice));
+}
+
 void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   AdjointState &A = h->adj;
+  AdjointState &A2 = h->adj2;
+  const bool cpl = h->adj_coupled;
   const DevMedium &D = adj_dev(h);
-  const size_t nvals = D.values();
-  const size_t nloc = size_t(D.nspec) * sfg::NPTS;
-  const size_t stride = ((nvals + 3) / 4) * 4 + 4;
   const int ncheck = (nstep + interval - 1) / interval;
-  const int nst = int(adj_data(h).stacey_pt.size());
-  const size_t vstride = ((2 * size_t(nst) + 3) / 4) * 4 + 4;
+  const size_t old_nvals = A.nvals;
+  const size_t old_bytes = A.seg_u ? size_t(A.nbuf) * (adj_segment_bytes(A, A.interval) +
+                                                       (A2.seg_u ? adj_segment_bytes(A2, A.interval) : 0)) : 0;
+  adj_medium_sizes(A, D, adj_data(h));
+  if (cpl) adj_medium_sizes(A2, h->ac, h->asmb.ac);
   // segment buffers: as many as the budget holds (default: 75% of the device
   // memory free before they are allocated), at least 2, at most ncheck
-  const size_t seg_bytes = size_t(interval) * (2 * stride + vstride) * sizeof(float);
+  const size_t seg_bytes = adj_segment_bytes(A, interval) + (cpl ? adj_segment_bytes(A2, interval) : 0);
   size_t budget = A.budget;
   if (budget == 0) {
     size_t fr = 0, tot = 0;
     SFG_CUDA(cudaMemGetInfo(&fr, &tot));
-    const size_t held = A.seg_u ? size_t(A.nbuf) * size_t(A.interval) * (2 * A.stride + A.vstride) * sizeof(float) : 0;
-    budget = size_t(0.75 * double(fr + held));
+    budget = size_t(0.75 * double(fr + old_bytes));
   }
   const int nbuf = int(std::max<size_t>(2, std::min<size_t>(size_t(std::max(ncheck, 2)), budget / seg_bytes)));
-  if (A.nvals != nvals || A.interval != interval || A.ncheck < ncheck || A.nbuf != nbuf) {
-    for (float **p : {&A.ckpt, &A.seg_u, &A.seg_a, &A.seg_v})
-      if (*p) { cudaFree(*p); *p = nullptr; }
-    A.ckpt = dalloc<float>(size_t(ncheck) * 3 * (nvals + 4));
-    A.seg_u = dalloc<float>(size_t(nbuf) * interval * stride);
-    A.seg_a = dalloc<float>(size_t(nbuf) * interval * stride);
-    A.seg_v = dalloc<float>(size_t(nbuf) * interval * vstride);
+  if (old_nvals != A.nvals || A.interval != interval || A.ncheck < ncheck || A.nbuf != nbuf ||
+      (cpl && !A2.seg_u)) {
+    adj_medium_segments(A, ncheck, nbuf, interval);
+    if (cpl) adj_medium_segments(A2, ncheck, nbuf, interval);
     A.rec_from = -1;
     if (A.graph_rseg) { cudaGraphExecDestroy(A.graph_rseg); A.graph_rseg = nullptr; }
     for (cudaGraphExec_t &g : A.graph_rev)
@@ -2330,103 +2503,20 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
     }
     A.nbuf = nbuf;
   }
-  A.vstride = vstride;
-  A.nvals = nvals;
-  A.nloc = nloc;
-  A.nglob = size_t(D.nglob);
-  A.stride = stride;
-  A.interval = interval;
-  A.ncheck = ncheck;
-  A.nstep = nstep;
+  for (AdjointState *X : {&A, &A2}) {
+    X->interval = interval;
+    X->ncheck = ncheck;
+    X->nstep = nstep;
+    X->nbuf = nbuf;
+  }
   if (!A.lu) {
-    A.lu = dalloc<float>(nvals + 4); A.lv = dalloc<float>(nvals + 4); A.mu = dalloc<float>(nvals + 4);
-    A.r = dalloc<float>(2 * nloc);
-    // element-local Stacey points: global point, Stacey slot, geometry
-    const sfg::MediumData &M = adj_data(h);
-    std::unordered_map<int, int> slot;
-    for (size_t j = 0; j < M.stacey_pt.size(); ++j) slot[M.stacey_pt[j]] = int(j);
-    std::vector<int> lg, lj;
-    std::vector<float> geo;
-    A.lb_k.clear();
-    A.lb_pm.clear();
-    for (int ce = 0; ce < M.nspec; ++ce) {
-      if (M.bc_slot[ce] < 0) continue;
-      for (int q = 0; q < sfg::NPTS; ++q) {
-        const size_t k = size_t(M.bc_slot[ce]) * sfg::NPTS + q;
-        if (M.bc_w[k] == 0.0f) continue;
-        const int g = M.ibool[size_t(ce) * sfg::NPTS + q];
-        lg.push_back(g);
-        lj.push_back(slot.at(g));
-        // P-SV: the normal; SH and acoustic: x is the free-surface mask (1 in SH)
-        geo.insert(geo.end(), {M.ncomp == 2 ? M.bc_nx[k] : M.bc_keep[k], M.bc_nz[k], M.bc_j1[k], M.bc_w[k]});
-        A.lb_k.push_back(k);
-        A.lb_pm.push_back(size_t(M.elem_mesh[ce]) * sfg::NPTS + q);
-      }
-    }
-    A.nlb = int(lg.size());
-    A.off_lb = ((2 * nloc + A.nglob + 3) / 4) * 4;
-    A.nsrc_t = adj_acoustic(h) ? h->asmb.nsrc : 0;
-    A.src_ce = dalloc<int>(std::max(A.nsrc_t, 1));
-    A.lb_g = dalloc<int>(lg.size()); A.lb_j = dalloc<int>(lj.size()); A.lb_geo = dalloc<float>(geo.size());
-    if (A.nlb) {
-      SFG_CUDA(cudaMemcpy(A.lb_g, lg.data(), lg.size() * sizeof(int), cudaMemcpyHostToDevice));
-      SFG_CUDA(cudaMemcpy(A.lb_j, lj.data(), lj.size() * sizeof(int), cudaMemcpyHostToDevice));
-      SFG_CUDA(cudaMemcpy(A.lb_geo, geo.data(), geo.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
-    A.sum = dalloc<float>(A.nsum()); A.comp = dalloc<float>(A.nsum()); A.seg = dalloc<float>(A.nsum());
-    // receivers as adjoint sources: chain per elastic compute element
-    const sfg::Assembly2D &as = h->asmb;
-    std::vector<int> head(D.nspec, -1), next(std::max(as.nrec, 1), -1);
-    for (int r = 0; r < as.nrec; ++r) {
-      next[r] = head[as.rec_elem[r]];
-      head[as.rec_elem[r]] = r;
-    }
-    A.ad_head = dalloc<int>(head.size());
-    SFG_CUDA(cudaMemcpy(A.ad_head, head.data(), head.size() * sizeof(int), cudaMemcpyHostToDevice));
-    A.ad_next = dalloc<int>(next.size());
-    SFG_CUDA(cudaMemcpy(A.ad_next, next.data(), next.size() * sizeof(int), cudaMemcpyHostToDevice));
-    const auto &sp = M.stacey_pt;
-    const auto &sc = M.stacey_c;
-    // pressure receivers (acoustic): points they touch, with receiver and weight
-    A.pressure = adj_acoustic(h);
-    if (A.pressure) {
-      std::vector<std::vector<std::pair<int, float>>> by_pt(D.nglob);
-      for (int r = 0; r < as.nrec; ++r)
-        for (int q = 0; q < sfg::NPTS; ++q) {
-          const float hq = as.rec_h[size_t(r) * sfg::NPTS + q];
-          if (hq != 0.0f) by_pt[M.ibool[size_t(as.rec_elem[r]) * sfg::NPTS + q]].push_back({r, hq});
-        }
-      std::vector<int> pt, start{0}, rr;
-      std::vector<float> hw;
-      for (int g = 0; g < D.nglob; ++g) {
-        if (by_pt[g].empty()) continue;
-        pt.push_back(g);
-        for (auto &[r, hq] : by_pt[g]) { rr.push_back(r); hw.push_back(hq); }
-        start.push_back(int(rr.size()));
-      }
-      A.nps = int(pt.size());
-      A.ps_pt = dalloc<int>(pt.size()); A.ps_start = dalloc<int>(start.size());
-      A.ps_rec = dalloc<int>(rr.size()); A.ps_h = dalloc<float>(hw.size());
-      if (A.nps) {
-        SFG_CUDA(cudaMemcpy(A.ps_pt, pt.data(), pt.size() * sizeof(int), cudaMemcpyHostToDevice));
-        SFG_CUDA(cudaMemcpy(A.ps_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice));
-        SFG_CUDA(cudaMemcpy(A.ps_rec, rr.data(), rr.size() * sizeof(int), cudaMemcpyHostToDevice));
-        SFG_CUDA(cudaMemcpy(A.ps_h, hw.data(), hw.size() * sizeof(float), cudaMemcpyHostToDevice));
-      }
-    }
-    A.nst = int(sp.size());
-    A.st_pt = dalloc<int>(sp.size());
-    A.st_c = dalloc<float>(sc.size());
-    if (!sp.empty()) {
-      SFG_CUDA(cudaMemcpy(A.st_pt, sp.data(), sp.size() * sizeof(int), cudaMemcpyHostToDevice));
-      SFG_CUDA(cudaMemcpy(A.st_c, sc.data(), sc.size() * sizeof(float), cudaMemcpyHostToDevice));
-    }
-    A.d_rec = dalloc<sfg::dev::SegRecord>(1);
+    adj_medium_init(h, A, D, adj_data(h), h->el.nspec ? SFG_MEDIUM_ELASTIC : SFG_MEDIUM_ACOUSTIC);
     A.d_k0 = dalloc<int>(1);
     SFG_CUDA(cudaStreamCreateWithFlags(&A.rstream, cudaStreamNonBlocking));
   }
-  sfg::dev::SegRecord rec{A.seg_u, A.seg_a, stride, 0, A.seg_v, vstride, A.st_pt, A.nst, 0};
-  SFG_CUDA(cudaMemcpy(A.d_rec, &rec, sizeof(rec), cudaMemcpyHostToDevice));
+  if (cpl && !A2.lu) adj_medium_init(h, A2, h->ac, h->asmb.ac, SFG_MEDIUM_ACOUSTIC);
+  adj_write_record(A);
+  if (cpl) adj_write_record(A2);
   if (!A.graph_r1) {
     // one recording step with the next predictor fused, and one ending on
     // the corrector (the segment's last step)
@@ -2442,12 +2532,17 @@ void adjoint_alloc(sfg_handle *h, int nstep, int interval) {
   }
 }
 
-void save_state(sfg_handle *h, float *dst) {
-  const DevMedium &D = adj_dev(h);
-  const size_t n = D.values() + 4;
-  SFG_CUDA(cudaMemcpyAsync(dst, D.u, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(dst + n, D.v, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, D.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+// Checkpoint c of every medium in the sweep: u, v, a at the segment's start.
+void save_state(sfg_handle *h, int c) {
+  for (int m = 0; m < (h->adj_coupled ? 2 : 1); ++m) {
+    const AdjointState &A = m ? h->adj2 : h->adj;
+    const DevMedium &D = m ? h->ac : adj_dev(h);
+    const size_t n = D.values() + 4;
+    float *dst = A.ckpt + size_t(c) * 3 * n;
+    SFG_CUDA(cudaMemcpyAsync(dst, D.u, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    SFG_CUDA(cudaMemcpyAsync(dst + n, D.v, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    SFG_CUDA(cudaMemcpyAsync(dst + 2 * n, D.a, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  }
 }
 
 // Segments held from the forward run (the last min(nbuf, ncheck)) and the
@@ -2470,6 +2565,11 @@ void record_segment(sfg_handle *h, int c, bool seismograms, int b) {
   const size_t ob = size_t(b) * A.interval;
   sfg::dev::k_set_segment<<<1, 1, 0, h->stream>>>(A.d_rec, h->d_step, A.seg_u + ob * A.stride,
                                                   A.seg_a + ob * A.stride, A.seg_v + ob * A.vstride, k0);
+  if (h->adj_coupled) {
+    const AdjointState &A2 = h->adj2;
+    sfg::dev::k_set_segment<<<1, 1, 0, h->stream>>>(A2.d_rec, h->d_step, A2.seg_u + ob * A2.stride,
+                                                    A2.seg_a + ob * A2.stride, A2.seg_v + ob * A2.vstride, k0);
+  }
   resume(h);
   if (!seismograms && k1 - k0 == A.interval && A.graph_rseg) {
     SFG_CUDA(cudaGraphLaunch(A.graph_rseg, h->stream));
@@ -2491,28 +2591,87 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
   AdjointState &A = h->adj;
   const DevMedium &D = adj_dev(h);
   const float dt = float(h->asmb.dt), dt2 = dt / 2.0f, dtsq2 = dt * dt / 2.0f;
-  sfg::dev::AdjArgs J{};
-  J.ibool = D.ibool; J.xix = D.xix; J.xiz = D.xiz; J.gax = D.gax; J.gaz = D.gaz; J.jac = D.jac;
-  J.prop0 = D.prop0; J.prop1 = D.prop1;
-  J.mu = A.mu; J.r = A.r; J.pslot = D.slot; J.seg = A.seg;
-  J.ad_head = A.ad_head; J.ad_next = A.ad_next; J.ad_h = h->d_rec_h;
-  J.gtab = A.gtab; J.seg_k0 = A.d_k0; J.nrec = h->asmb.nrec;
-  J.nspec = D.nspec;
-  J.bc_slot = D.bc_slot; J.bc_keep = D.bc_keep;
-  J.quad = h->quad;
-  sfg::dev::AdjStaceyArgs St{};
-  St.lb_g = A.lb_g; St.lb_j = A.lb_j; St.geo = reinterpret_cast<const float4 *>(A.lb_geo);
-  St.mu = A.mu; St.acc = A.seg + A.off_lb; St.nlb = A.nlb;
-  St.lv = A.lv; St.pt = A.st_pt; St.cm = A.st_c; St.nst = A.nst;
-  St.nb_grad = grid_for(A.nlb);
+  auto args = [&](AdjointState &X, const DevMedium &M) {
+    sfg::dev::AdjArgs J{};
+    J.ibool = M.ibool; J.xix = M.xix; J.xiz = M.xiz; J.gax = M.gax; J.gaz = M.gaz; J.jac = M.jac;
+    J.prop0 = M.prop0; J.prop1 = M.prop1;
+    J.mu = X.mu; J.r = X.r; J.pslot = M.slot; J.seg = X.seg;
+    J.ad_head = X.ad_head; J.ad_next = X.ad_next; J.ad_h = h->d_rec_h;
+    J.gtab = A.gtab; J.seg_k0 = A.d_k0; J.nrec = h->asmb.nrec;
+    J.nspec = M.nspec;
+    J.bc_slot = M.bc_slot; J.bc_keep = M.bc_keep;
+    J.quad = h->quad;
+    return J;
+  };
+  auto stacey_args = [&](AdjointState &X) {
+    sfg::dev::AdjStaceyArgs St{};
+    St.lb_g = X.lb_g; St.lb_j = X.lb_j; St.geo = reinterpret_cast<const float4 *>(X.lb_geo);
+    St.mu = X.mu; St.acc = X.seg + X.off_lb; St.nlb = X.nlb;
+    St.lv = X.lv; St.pt = X.st_pt; St.cm = X.st_c; St.nst = X.nst;
+    St.nb_grad = grid_for(X.nlb);
+    return St;
+  };
+  sfg::dev::AdjArgs J = args(A, D);
+  sfg::dev::AdjStaceyArgs St = stacey_args(A);
   const int eblocks = (D.nspec + E - 1) / E;
   const size_t ob = size_t(b) * A.interval;
-  auto psrc = [&](int slot) {
-    if (A.nps)
-      sfg::dev::k_adj_psrc<<<std::min(grid_for(A.nps), 64), 128, 0, rs>>>(
-          A.mu, D.minv, A.ps_pt, A.ps_start, A.ps_rec, A.ps_h, A.gtab, A.d_k0, slot, h->asmb.nrec, A.nps);
+  auto psrc = [&](AdjointState &X, const DevMedium &M, int slot) {
+    if (X.nps)
+      sfg::dev::k_adj_psrc<<<std::min(grid_for(X.nps), 64), 128, 0, rs>>>(
+          X.mu, M.minv, X.ps_pt, X.ps_start, X.ps_rec, X.ps_h, A.gtab, A.d_k0, slot, h->asmb.nrec, X.nps);
   };
-  if (last && A.pressure) psrc(n - 1);      // mu of the final step: B (-R^T g)
+  auto srcterm = [&](AdjointState &X, const DevMedium &M, int slot) {
+    if (X.nsrc_t)
+      sfg::dev::k_adj_srcterm<<<(X.nsrc_t * sfg::NPTS + 127) / 128, 128, 0, rs>>>(
+          X.seg + X.off_src(), X.mu, M.ibool, X.src_ce, h->d_stf, A.d_k0, slot, X.nsrc_t, h->asmb.nstep,
+          X.src_id, h->asmb.nsrc);
+  };
+  if (h->adj_coupled) {
+    // coupled P-SV + acoustic step in reverse: both media's Stacey and
+    // element terms with their own mu_k, then the elastic post (lu~ takes the
+    // acoustic mu_k through the interface) and the acoustic post (its
+    // adjoint acceleration takes the elastic mu_(k-1)), in that order
+    AdjointState &C = h->adj2;
+    const DevMedium &Ac = h->ac;
+    sfg::dev::AdjArgs Ja = args(C, Ac);
+    sfg::dev::AdjStaceyArgs Sa = stacey_args(C);
+    const int ablocks = (Ac.nspec + E - 1) / E;
+    const sfg::dev::AdjCoupling cp_el{A.cp_other, A.cp_nx, A.cp_nz, C.mu, D.niface};
+    const sfg::dev::AdjCoupling cp_ac{C.cp_other, C.cp_nx, C.cp_nz, A.mu, Ac.niface};
+    if (last && C.pressure) psrc(C, Ac, n - 1);
+    for (int i = n - 1; i >= 0; --i) {
+      const size_t sl = ob + size_t(i);
+      if (A.nst) {
+        St.vst = A.seg_v + sl * A.vstride;
+        St.af = A.seg_a + sl * A.stride;
+        sfg::dev::k_adj_stacey<2><<<St.nb_grad + grid_for(A.nst), 256, 0, rs>>>(St);
+      }
+      if (C.nst) {
+        Sa.vst = C.seg_v + sl * C.vstride;
+        Sa.af = C.seg_a + sl * C.stride;
+        sfg::dev::k_adj_stacey<1><<<Sa.nb_grad + grid_for(C.nst), 256, 0, rs>>>(Sa);
+      }
+      J.uf = A.seg_u + sl * A.stride;
+      J.slot = i;
+      if (ROW) sfg::dev::k_adj_elem_row<32><<<(D.nspec + 31) / 32, sfg::dev::NG * 32, 0, rs>>>(J);
+      else sfg::dev::k_adj_elem<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
+      Ja.uf = C.seg_u + sl * C.stride;
+      Ja.slot = i;
+      sfg::dev::k_adj_elem_ac<E><<<ablocks, sfg::dev::NP * E, 0, rs>>>(Ja);
+      srcterm(C, Ac, i);
+      sfg::dev::k_adj_post<2, true><<<grid_for(D.nglob), 256, 0, rs>>>(
+          A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
+          D.nglob, dt, dt2, dtsq2, cp_el);
+      sfg::dev::k_adj_post<1, true><<<grid_for(Ac.nglob), 256, 0, rs>>>(
+          C.lu, C.lv, C.mu, C.seg + 2 * C.nloc, C.seg_a + sl * C.stride, Ac.minv, C.r, Ac.inv_start,
+          Ac.nglob, dt, dt2, dtsq2, cp_ac);
+      psrc(C, Ac, i - 1);
+    }
+    sfg::dev::k_kahan_fold<<<grid_for(int(A.nsum())), 256, 0, rs>>>(A.sum, A.comp, A.seg, int(A.nsum()));
+    sfg::dev::k_kahan_fold<<<grid_for(int(C.nsum())), 256, 0, rs>>>(C.sum, C.comp, C.seg, int(C.nsum()));
+    return;
+  }
+  if (last && A.pressure) psrc(A, D, n - 1);      // mu of the final step: B (-R^T g)
   for (int i = n - 1; i >= 0; --i) {
     const size_t sl = ob + size_t(i);
     const bool sh = D.ncomp == 1;
@@ -2526,13 +2685,11 @@ void reverse_segment_E(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) 
     J.slot = i;
     if (A.pressure) {
       sfg::dev::k_adj_elem_ac<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
-      if (A.nsrc_t)
-        sfg::dev::k_adj_srcterm<<<(A.nsrc_t * sfg::NPTS + 127) / 128, 128, 0, rs>>>(
-            A.seg + A.off_src(), A.mu, D.ibool, A.src_ce, h->d_stf, A.d_k0, i, A.nsrc_t, h->asmb.nstep);
+      srcterm(A, D, i);
       sfg::dev::k_adj_post<1><<<grid_for(D.nglob), 256, 0, rs>>>(
           A.lu, A.lv, A.mu, A.seg + 2 * A.nloc, A.seg_a + sl * A.stride, D.minv, A.r, D.inv_start,
           D.nglob, dt, dt2, dtsq2);
-      psrc(i - 1);                            // mu of the previous step gets its source
+      psrc(A, D, i - 1);                      // mu of the previous step gets its source
     } else if (sh) {
       sfg::dev::k_adj_elem_sh<E><<<eblocks, sfg::dev::NP * E, 0, rs>>>(J);
       sfg::dev::k_adj_post<1><<<grid_for(D.nglob), 256, 0, rs>>>(
@@ -2590,12 +2747,16 @@ void reverse_segment(sfg_handle *h, int b, int n, bool last, cudaStream_t rs) {
   }
 }
 
-void restore_state(sfg_handle *h, const float *src) {
-  const DevMedium &D = adj_dev(h);
-  const size_t n = D.values() + 4;
-  SFG_CUDA(cudaMemcpyAsync(D.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(D.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
-  SFG_CUDA(cudaMemcpyAsync(D.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+void restore_state(sfg_handle *h, int c) {
+  for (int m = 0; m < (h->adj_coupled ? 2 : 1); ++m) {
+    const AdjointState &A = m ? h->adj2 : h->adj;
+    const DevMedium &D = m ? h->ac : adj_dev(h);
+    const size_t n = D.values() + 4;
+    const float *src = A.ckpt + size_t(c) * 3 * n;
+    SFG_CUDA(cudaMemcpyAsync(D.u, src, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    SFG_CUDA(cudaMemcpyAsync(D.v, src + n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+    SFG_CUDA(cudaMemcpyAsync(D.a, src + 2 * n, n * sizeof(float), cudaMemcpyDeviceToDevice, h->stream));
+  }
   h->state_final = true;
 }
 
@@ -2615,10 +2776,9 @@ int sfg_forward_checkpointed(sfg_handle *h, int nsteps, int interval) {
     AdjointState &A = h->adj;
     const int ret = sfg_reset_fields(h);
     if (ret != SFG_OK) return ret;
-    const size_t stride = 3 * (A.nvals + 4);
     const int c_r = held_from(A);
     for (int c = 0; c < A.ncheck; ++c) {
-      save_state(h, A.ckpt + size_t(c) * stride);
+      save_state(h, c);
       // the last nbuf segments are recorded on the way: the reverse sweep
       // recomputes only the earlier ones
       if (c >= c_r) record_segment(h, c, true, seg_buffer(A, c));
@@ -2665,7 +2825,9 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       for (cudaGraphExec_t &g : A.graph_rev)
         if (g) { cudaGraphExecDestroy(g); g = nullptr; }
     }
-    const size_t nstage = std::max(ng, A.nsum());
+    AdjointState &A2 = h->adj2;
+    const bool cpl = h->adj_coupled;
+    const size_t nstage = std::max({ng, A.nsum(), cpl ? A2.nsum() : size_t(0)});
     if (nstage > A.h_stage_cap) {
       if (A.h_stage) cudaFreeHost(A.h_stage);
       SFG_CUDA(cudaMallocHost(&A.h_stage, nstage * sizeof(float)));
@@ -2683,17 +2845,21 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       }
       SFG_CUDA(cudaMemcpyAsync(A.gtab, g, size_t(A.nstep) * nrec * 2 * sizeof(float), cudaMemcpyHostToDevice, s));
     }
-    if (A.nsrc_t) {
-      // the sources' elements (they may have moved since the last call)
-      SFG_CUDA(cudaMemcpyAsync(A.src_ce, as.src_elem.data(), A.nsrc_t * sizeof(int), cudaMemcpyHostToDevice, s));
+    for (AdjointState *X : {&A, &A2}) {
+      if (!X->nsrc_t || (X == &A2 && !cpl)) continue;
+      // the acoustic sources' elements (they may have moved since the last call)
+      X->src_ce_h.resize(X->nsrc_t);
+      for (int j = 0; j < X->nsrc_t; ++j) X->src_ce_h[j] = as.src_elem[X->src_list[j]];
+      SFG_CUDA(cudaMemcpyAsync(X->src_ce, X->src_ce_h.data(), X->nsrc_t * sizeof(int), cudaMemcpyHostToDevice, s));
     }
-    const size_t nv = A.nvals;
     tune_reverse(h, s);
-    for (float *p : {A.lu, A.lv, A.mu})
-      SFG_CUDA(cudaMemsetAsync(p, 0, (nv + 4) * sizeof(float), s));
-    for (float *p : {A.sum, A.comp, A.seg})
-      SFG_CUDA(cudaMemsetAsync(p, 0, A.nsum() * sizeof(float), s));
-    const size_t cstride = 3 * (nv + 4);
+    for (AdjointState *X : {&A, &A2}) {
+      if (X == &A2 && !cpl) continue;
+      for (float *p : {X->lu, X->lv, X->mu})
+        SFG_CUDA(cudaMemsetAsync(p, 0, (X->nvals + 4) * sizeof(float), s));
+      for (float *p : {X->sum, X->comp, X->seg})
+        SFG_CUDA(cudaMemsetAsync(p, 0, X->nsum() * sizeof(float), s));
+    }
     cudaStream_t rs = A.rstream;
     // the reverse stream starts after the set-up above
     SFG_CUDA(cudaEventRecord(A.ev_rec[0], s));
@@ -2703,7 +2869,7 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
       if (A.rec_from < 0 || c < A.rec_from) {
         // buffer b is free once the reverse sweep of its last segment is done
         SFG_CUDA(cudaStreamWaitEvent(s, A.ev_rev[b], 0));
-        restore_state(h, A.ckpt + size_t(c) * cstride);
+        restore_state(h, c);
         record_segment(h, c, false, b);
       }
       SFG_CUDA(cudaEventRecord(A.ev_rec[b], s));
@@ -2730,83 +2896,89 @@ int sfg_adjoint_gradient(sfg_handle *h, const float *seis_grad, float *grad_rho,
     SFG_CUDA(cudaStreamSynchronize(rs));
     SFG_CUDA(cudaStreamSynchronize(s));
     h->host_step = A.nstep;
-    const DevMedium &D = adj_dev(h);
-    const sfg::MediumData &M = adj_data(h);
-    const bool acoustic = adj_acoustic(h);
     const float dt2 = float(as.dt) / 2.0f;
-    // compute order -> mesh order.  Elastic: kappa and mu terms, rho from the
-    // mass, -W_p G(g_p).  Acoustic: the stiffness term is d/d(rho^-1) (rho:
-    // times -rho^-2), the mass W / kappa gives kappa: +W_p G(g_p) / kappa^2.
-    const float *tot = A.h_stage;
-    SFG_CUDA(cudaMemcpy(A.h_stage, A.sum, A.nsum() * sizeof(float), cudaMemcpyDeviceToHost));
-    const float *grho = tot + 2 * A.nloc;
-    for (int ce = 0; ce < D.nspec; ++ce) {
-      const int e = M.elem_mesh[ce];
-      for (int q = 0; q < sfg::NPTS; ++q) {
-        const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(e) * sfg::NPTS + q;
-        const double W = as.wgll_d[q % sfg::NGLL] * as.wgll_d[q / sfg::NGLL] * as.jac_d[pm];
-        const double G = double(grho[M.ibool[pc]]);
+    // per medium of the sweep (a coupled model: elastic, then acoustic)
+    auto extract = [&](AdjointState &A, const DevMedium &D, const sfg::MediumData &M, bool acoustic) {
+      // compute order -> mesh order.  Elastic: kappa and mu terms, rho from the
+      // mass, -W_p G(g_p).  Acoustic: the stiffness term is d/d(rho^-1) (rho:
+      // times -rho^-2), the mass W / kappa gives kappa: +W_p G(g_p) / kappa^2.
+      const float *tot = h->adj.h_stage;
+      SFG_CUDA(cudaMemcpy(h->adj.h_stage, A.sum, A.nsum() * sizeof(float), cudaMemcpyDeviceToHost));
+      const float *grho = tot + 2 * A.nloc;
+      for (int ce = 0; ce < D.nspec; ++ce) {
+        const int e = M.elem_mesh[ce];
+        for (int q = 0; q < sfg::NPTS; ++q) {
+          const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(e) * sfg::NPTS + q;
+          const double W = as.wgll_d[q % sfg::NGLL] * as.wgll_d[q / sfg::NGLL] * as.jac_d[pm];
+          const double G = double(grho[M.ibool[pc]]);
+          if (acoustic) {
+            const double ri = double(M.prop0[pc]), kap = double(M.prop1[pc]);
+            if (grad_rho) grad_rho[pm] = float(-ri * ri * double(tot[2 * pc + 1]));
+            if (grad_kappa) grad_kappa[pm] = float(W * G / (kap * kap));
+            continue;
+          }
+          if (grad_kappa) grad_kappa[pm] = tot[2 * pc];
+          if (grad_mu) grad_mu[pm] = tot[2 * pc + 1];
+          if (grad_rho) grad_rho[pm] = float(-W * G);
+        }
+      }
+      // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu);
+      // acoustic: 1 / (rho vp) = (rho kappa)^-1/2
+      const float *lbs = tot + A.off_lb;
+      for (int i = 0; i < A.nlb; ++i) {
+        const size_t k = A.lb_k[i];
+        const double A1 = lbs[4 * i], A2 = lbs[4 * i + 1], A3 = lbs[4 * i + 2], A4 = lbs[4 * i + 3];
+        const double wj = double(M.bc_w[k]) * double(M.bc_j1[k]);
+        const double g_vp = -wj * (A1 + double(dt2) * A3);
+        const double g_vs = -wj * (A2 - A1 + double(dt2) * (A4 - A3));
+        const size_t pm = A.lb_pm[i];
         if (acoustic) {
-          const double ri = double(M.prop0[pc]), kap = double(M.prop1[pc]);
-          if (grad_rho) grad_rho[pm] = float(-ri * ri * double(tot[2 * pc + 1]));
-          if (grad_kappa) grad_kappa[pm] = float(W * G / (kap * kap));
+          const size_t pc = size_t(as.mesh_to_compute[pm / sfg::NPTS]) * sfg::NPTS + pm % sfg::NPTS;
+          const double imp = M.bc_imp0[k], rho = 1.0 / double(M.prop0[pc]), kap = double(M.prop1[pc]);
+          if (grad_rho) grad_rho[pm] += float(g_vs * (-imp / (2 * rho)));
+          if (grad_kappa) grad_kappa[pm] += float(g_vs * (-imp / (2 * kap)));
           continue;
         }
-        if (grad_kappa) grad_kappa[pm] = tot[2 * pc];
-        if (grad_mu) grad_mu[pm] = tot[2 * pc + 1];
-        if (grad_rho) grad_rho[pm] = float(-W * G);
+        const double rho = h->mesh.prho.empty() ? h->mesh.mat_rho[h->mesh.kmato[pm / sfg::NPTS]] : h->mesh.prho[pm];
+        const double rvp = M.bc_imp0[k], rvs = M.bc_imp1[k];
+        double dr = 0, dk = 0, dm = 0;
+        if (rvp > 0) {      // P-SV only: SH has no P impedance (g_vp is 0 there)
+          dr = g_vp * rvp / (2 * rho);
+          dk = g_vp * rho / (2 * rvp);
+          dm = g_vp * (2.0 / 3.0) * rho / rvp;
+        }
+        if (rvs > 0) {
+          dr += g_vs * rvs / (2 * rho);
+          dm += g_vs * rho / (2 * rvs);
+        }
+        if (grad_rho) grad_rho[pm] += float(dr);
+        if (grad_kappa) grad_kappa[pm] += float(dk);
+        if (grad_mu) grad_mu[pm] += float(dm);
       }
-    }
-    // Stacey impedances rvp = sqrt(rho (kappa + 4/3 mu)), rvs = sqrt(rho mu);
-    // acoustic: 1 / (rho vp) = (rho kappa)^-1/2
-    const float *lbs = tot + A.off_lb;
-    for (int i = 0; i < A.nlb; ++i) {
-      const size_t k = A.lb_k[i];
-      const double A1 = lbs[4 * i], A2 = lbs[4 * i + 1], A3 = lbs[4 * i + 2], A4 = lbs[4 * i + 3];
-      const double wj = double(M.bc_w[k]) * double(M.bc_j1[k]);
-      const double g_vp = -wj * (A1 + double(dt2) * A3);
-      const double g_vs = -wj * (A2 - A1 + double(dt2) * (A4 - A3));
-      const size_t pm = A.lb_pm[i];
-      if (acoustic) {
-        const size_t pc = size_t(as.mesh_to_compute[pm / sfg::NPTS]) * sfg::NPTS + pm % sfg::NPTS;
-        const double imp = M.bc_imp0[k], rho = 1.0 / double(M.prop0[pc]), kap = double(M.prop1[pc]);
-        if (grad_rho) grad_rho[pm] += float(g_vs * (-imp / (2 * rho)));
-        if (grad_kappa) grad_kappa[pm] += float(g_vs * (-imp / (2 * kap)));
-        continue;
-      }
-      const double rho = h->mesh.prho.empty() ? h->mesh.mat_rho[h->mesh.kmato[pm / sfg::NPTS]] : h->mesh.prho[pm];
-      const double rvp = M.bc_imp0[k], rvs = M.bc_imp1[k];
-      double dr = 0, dk = 0, dm = 0;
-      if (rvp > 0) {      // P-SV only: SH has no P impedance (g_vp is 0 there)
-        dr = g_vp * rvp / (2 * rho);
-        dk = g_vp * rho / (2 * rvp);
-        dm = g_vp * (2.0 / 3.0) * rho / rvp;
-      }
-      if (rvs > 0) {
-        dr += g_vs * rvs / (2 * rho);
-        dm += g_vs * rho / (2 * rvs);
-      }
-      if (grad_rho) grad_rho[pm] += float(dr);
-      if (grad_kappa) grad_kappa[pm] += float(dk);
-      if (grad_mu) grad_mu[pm] += float(dm);
-    }
-    if (acoustic && grad_kappa) {
-      // kappa in the pressure sources' arrays l / kappa
-      const float *ss = tot + A.off_src();
-      for (int si = 0; si < A.nsrc_t; ++si) {
-        const int ce = as.src_elem[si];
-        for (int q = 0; q < sfg::NPTS; ++q) {
-          const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(M.elem_mesh[ce]) * sfg::NPTS + q;
-          const double sa = as.src_arr[(size_t(si) * 2) * sfg::NPTS + q];
-          grad_kappa[pm] += float(-double(ss[size_t(si) * sfg::NPTS + q]) * sa / double(M.prop1[pc]));
+      if (acoustic && grad_kappa) {
+        // kappa in the pressure sources' arrays l / kappa
+        const float *ss = tot + A.off_src();
+        for (int j = 0; j < A.nsrc_t; ++j) {
+          const int si = A.src_list[j];
+          const int ce = as.src_elem[si];
+          for (int q = 0; q < sfg::NPTS; ++q) {
+            const size_t pc = size_t(ce) * sfg::NPTS + q, pm = size_t(M.elem_mesh[ce]) * sfg::NPTS + q;
+            const double sa = as.src_arr[(size_t(si) * 2) * sfg::NPTS + q];
+            grad_kappa[pm] += float(-double(ss[size_t(j) * sfg::NPTS + q]) * sa / double(M.prop1[pc]));
+          }
         }
       }
-    }
-    if (acoustic && grad_mu) {
-      // the acoustic medium uses kappa + 4/3 mu as its bulk modulus
-      const size_t n = size_t(as.nspec) * sfg::NPTS;
-      for (size_t pm = 0; pm < n; ++pm) grad_mu[pm] = grad_kappa ? float(4.0 / 3.0 * grad_kappa[pm]) : 0.0f;
-    }
+      if (acoustic && grad_mu) {
+        // the acoustic medium uses kappa + 4/3 mu as its bulk modulus
+        for (int ce = 0; ce < D.nspec; ++ce)
+          for (int q = 0; q < sfg::NPTS; ++q) {
+            const size_t pm = size_t(M.elem_mesh[ce]) * sfg::NPTS + q;
+            grad_mu[pm] = grad_kappa ? float(4.0 / 3.0 * grad_kappa[pm]) : 0.0f;
+          }
+      }
+    };
+    extract(A, adj_dev(h), adj_data(h), adj_acoustic(h));
+    if (cpl) extract(A2, h->ac, as.ac, true);
     return int(SFG_OK);
   });
 }

@@ -1,5 +1,5 @@
-"""Discrete-adjoint model gradients (2D elastic P-SV and SH) against finite
-differences.
+"""Discrete-adjoint model gradients (2D elastic P-SV, SH, acoustic and coupled
+acoustic-elastic) against finite differences.
 
 The gradient of L = sum(w * seis) for a seeded weight array w is checked,
 along smooth Gaussian perturbations of rho, kappa and mu placed between the
@@ -8,7 +8,8 @@ impedances depend on the model), against central differences of two forward runs
 relative error <= 1e-2 (the FP32 forward limits the difference quotient to
 about 1e-3 at a 1% perturbation).  Gradients from different checkpoint
 intervals agree to 1e-5 (only the order of the FP32 time sum differs); the
-memory budget of the recorded segments changes no bit.
+memory budget of the recorded segments changes no bit.  Coupled
+acoustic-elastic models are checked against FP64-oracle differences.
 """
 import numpy as np
 import pytest
@@ -457,3 +458,120 @@ def test_acoustic_checkpoint_interval_invariance(sfg_lib):
         n = np.linalg.norm(x)
         assert n > 0
         assert np.linalg.norm(x - y) <= 1e-5 * n
+
+
+# --------------------------------------------------------------------------
+# Coupled acoustic-elastic models (conforming interface): the discrete
+# adjoint of the coupled step (transposed coupling terms in both directions).
+
+COUPLED_NSTEP = 700
+
+
+def coupled_problem(kind, nstep=COUPLED_NSTEP):
+    """60 x 50 model over 3000 x 2500 m: 30 elastic rows (rho 2300, vp 3000,
+    vs 1730) under 20 water rows (rho 1020, vp 1500), seafloor at z = 1500 m,
+    free surface on top, Stacey on the other sides; a pressure source in the
+    water 250 m above the seafloor and a force source in the solid; receivers
+    50 m under the seafloor (displacement) or 100 m above it (pressure)."""
+    from specfempp_b200 import meshgen, sfg
+    rows = np.zeros(50, np.int32)
+    rows[30:] = 1
+    mesh = meshgen.structured_mesh(60, 50, 0.0, 3000.0, 0.0, 2500.0, rows,
+                                   [(meshgen.ELASTIC, 2300.0, 3000.0, 1730.0), (meshgen.ACOUSTIC, 1020.0, 1500.0, 0.0)],
+                                   absorbing=("bottom", "right", "left"), free_surface=("top",))
+    srcs = [meshgen.RickerSource(1500.0, 1750.0, 12.0, 1e10), meshgen.RickerSource(900.0, 1100.0, 12.0, 1e9,
+                                                                                  angle=30.0)]
+    rx = np.array([600.0, 1100.0, 1900.0, 2400.0])
+    rz = np.full(4, 1450.0 if kind == "displacement" else 1600.0)
+    sim = sfg.Simulation2D(mesh, dt=4e-4, nstep=nstep)
+    sim.set_sources(srcs)
+    sim.set_receivers(rx, rz, types=(kind,))
+    sim.initialize()
+    weights = np.random.default_rng(17).standard_normal((nstep, len(rx), 2)).astype(np.float32)
+    return mesh, sim, base_model(mesh), weights
+
+
+# (parameter, bump centre, radius): in the water, in the solid, across the seafloor
+COUPLED_BUMPS = {"water_rho": (0, (1300.0, 1650.0), 120.0), "water_kappa": (1, (1300.0, 1650.0), 120.0),
+                 "solid_rho": (0, (1700.0, 1250.0), 150.0), "solid_kappa": (1, (1700.0, 1250.0), 150.0),
+                 "solid_mu": (2, (1700.0, 1250.0), 150.0), "seafloor_rho": (0, (1200.0, 1500.0), 150.0)}
+
+
+def coupled_oracle_misfit(mesh, kind, model, weights, which, d, h):
+    """The misfit of the FP64 CPU oracle for the model moved by h * d."""
+    from oracle import runner
+    m = [x.copy() for x in model]
+    m[which] = m[which] + h * d
+    rho, kap, mu = m
+    vp = np.sqrt((kap + 4.0 / 3.0 * mu) / rho)
+    vs = np.sqrt(mu / rho)
+    src = [runner.Source(x=1500.0, z=1750.0, f0=12.0, factor=1e10),
+           runner.Source(x=900.0, z=1100.0, f0=12.0, factor=1e9, angle=30.0)]
+    rx = np.array([600.0, 1100.0, 1900.0, 2400.0])
+    rz = np.full(4, 1450.0 if kind == "displacement" else 1600.0)
+    case = runner.Case2D(mesh=mesh, sources=src, rec_x=rx, rec_z=rz, dt=4e-4, nstep=COUPLED_NSTEP,
+                         seis_types=[kind], point_rho=rho, point_vp=vp, point_vs=vs)
+    s = runner.run(case, "f64", nthreads=8)["seis"][:, 0]
+    return float((s[:COUPLED_NSTEP] * weights).sum())
+
+
+@pytest.mark.parametrize("kind", ["displacement", "pressure"])
+@pytest.mark.parametrize("case", list(COUPLED_BUMPS))
+def test_coupled_adjoint_matches_finite_differences(sfg_lib, oracle_lib, kind, case):
+    """Coupled model, displacement seismograms at solid receivers or pressure
+    seismograms at water receivers: the gradient along smooth bumps in the
+    water, in the solid and across the seafloor against central differences
+    of the FP64 CPU oracle at a 0.1% step: relative 1e-3 (observed about
+    1e-6).  FP32 differences of the product's own forward runs are too noisy
+    here: the water receivers' misfit is about 1e4 times its sensitivity to
+    the solid bumps."""
+    mesh, sim, model, weights = coupled_problem(kind)
+    which, (x0, z0), r = COUPLED_BUMPS[case]
+    sim.set_model(*[m.astype(np.float32) for m in model])
+    sim.forward_checkpointed(COUPLED_NSTEP, 50)
+    g = sim.adjoint_gradient(weights)[which].astype(np.float64)
+    d = bump(mesh, x0, z0, r) * model[which]
+    fd = (coupled_oracle_misfit(mesh, kind, model, weights, which, d, 1e-3) -
+          coupled_oracle_misfit(mesh, kind, model, weights, which, d, -1e-3)) / 2e-3
+    ad = float((g * d).sum())
+    assert abs(fd) > 0
+    assert abs(ad - fd) <= 1e-3 * abs(fd), (ad, fd, abs(ad - fd) / abs(fd))
+
+
+@pytest.mark.parametrize("kind", ["displacement", "pressure"])
+def test_coupled_checkpoint_interval_and_budget(sfg_lib, kind):
+    """Coupled sweep: gradients from checkpoint intervals 1, 37 and the whole
+    run agree to 1e-5; two segment buffers and the default budget give the
+    same bits."""
+    mesh, sim, model, weights = coupled_problem(kind, nstep=300)
+    sim.set_model(*[m.astype(np.float32) for m in model])
+
+    def grad(interval):
+        sim.forward_checkpointed(300, interval)
+        return sim.adjoint_gradient(weights)
+    a, b, c = grad(1), grad(37), grad(300)
+    for x, y, z in zip(a, b, c):
+        n = np.linalg.norm(x)
+        assert n > 0
+        assert np.linalg.norm(x - y) <= 1e-5 * n
+        assert np.linalg.norm(x - z) <= 1e-5 * n
+    sim.set_adjoint_budget(1)
+    p = grad(37)
+    assert sim.adjoint_buffers() == 2
+    sim.set_adjoint_budget(0)
+    q = grad(37)
+    for x, y in zip(p, q):
+        assert np.array_equal(x, y)
+
+
+def test_coupled_adjoint_refusals(sfg_lib):
+    """Displacement seismograms at water receivers (or pressure at solid
+    ones) have no adjoint here: SFG_ERR_UNSUPPORTED, nothing run."""
+    from specfempp_b200 import sfg
+    mesh, sim, model, weights = coupled_problem("displacement", nstep=50)
+    sim2 = sfg.Simulation2D(mesh, dt=4e-4, nstep=50)
+    sim2.set_sources([sfg.Source(x=1500.0, z=1750.0, f0=12.0, factor=1e10)])
+    sim2.set_receivers(np.array([600.0]), np.array([1600.0]), types=("displacement",))
+    sim2.initialize()
+    with pytest.raises(sfg.SfgError, match="coupled adjoint"):
+        sim2.forward_checkpointed(50, 10)
