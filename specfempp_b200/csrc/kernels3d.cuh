@@ -53,6 +53,24 @@ struct Elem3Args {
   size_t nloc;
 };
 
+// Point algebra shared by both element-kernel forms, written as explicit FMA
+// chains (the build turns off contraction, so these are the only FMAs and
+// every form rounds alike): the map to physical derivatives, the isotropic
+// stress and F = |J| sigma . grad(xi_k).
+__device__ __forceinline__ float dot3(float a0, float b0, float a1, float b1, float a2, float b2) {
+  return fmaf(a2, b2, fmaf(a1, b1, a0 * b0));
+}
+
+__device__ __forceinline__ void stress3(const float du[3][3], float c0, float mu, float sig[3][3]) {
+  const float lam = c0 - 2.f * mu;
+  sig[0][0] = fmaf(c0, du[0][0], lam * (du[1][1] + du[2][2]));
+  sig[1][1] = fmaf(c0, du[1][1], lam * (du[0][0] + du[2][2]));
+  sig[2][2] = fmaf(c0, du[2][2], lam * (du[0][0] + du[1][1]));
+  sig[0][1] = sig[1][0] = mu * (du[0][1] + du[1][0]);
+  sig[0][2] = sig[2][0] = mu * (du[0][2] + du[2][0]);
+  sig[1][2] = sig[2][1] = mu * (du[1][2] + du[2][1]);
+}
+
 template <int E>
 __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
   __shared__ float su[E][3][NQ];
@@ -93,21 +111,15 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
       d2 = fmaf(hz[l], su[le][c][(l * NG + iy) * NG + ix], d2);
     }
 #pragma unroll
-    for (int j = 0; j < 3; ++j) du[c][j] = d0 * gi[0 * 3 + j] + d1 * gi[1 * 3 + j] + d2 * gi[2 * 3 + j];
+    for (int j = 0; j < 3; ++j) du[c][j] = dot3(d0, gi[0 * 3 + j], d1, gi[1 * 3 + j], d2, gi[2 * 3 + j]);
   }
-  const float lam = c0 - 2.f * mu;
   float sig[3][3];
-  sig[0][0] = c0 * du[0][0] + lam * (du[1][1] + du[2][2]);
-  sig[1][1] = c0 * du[1][1] + lam * (du[0][0] + du[2][2]);
-  sig[2][2] = c0 * du[2][2] + lam * (du[0][0] + du[1][1]);
-  sig[0][1] = sig[1][0] = mu * (du[0][1] + du[1][0]);
-  sig[0][2] = sig[2][0] = mu * (du[0][2] + du[2][0]);
-  sig[1][2] = sig[2][1] = mu * (du[1][2] + du[2][1]);
+  stress3(du, c0, mu, sig);
 #pragma unroll
   for (int c = 0; c < 3; ++c)
 #pragma unroll
     for (int k = 0; k < 3; ++k)
-      sF[le][c][k][q] = jac * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
+      sF[le][c][k][q] = jac * dot3(sig[c][0], gi[k * 3 + 0], sig[c][1], gi[k * 3 + 1], sig[c][2], gi[k * 3 + 2]);
 #pragma unroll
   for (int l = 0; l < NG; ++l) {
     hx[l] = c3_hpw[l * NG + ix];
@@ -115,6 +127,7 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
     hz[l] = c3_hpw[l * NG + iz];
   }
   const float wx = c3_w[ix], wy = c3_w[iy], wz = c3_w[iz];
+  const float wzy = wz * wy, wzx = wz * wx, wyx = wy * wx;
   __syncthreads();
   if (!act) return;
   float a[3];
@@ -127,7 +140,7 @@ __global__ void __launch_bounds__(NQ * E) k_stiffness3d(Elem3Args A) {
       t2 = fmaf(sF[le][c][1][(iz * NG + l) * NG + ix], hy[l], t2);
       t3 = fmaf(sF[le][c][2][(l * NG + iy) * NG + ix], hz[l], t3);
     }
-    a[c] = -(wz * wy * t1 + wz * wx * t2 + wy * wx * t3);
+    a[c] = -dot3(wzy, t1, wzx, t2, wyx, t3);
   }
   if (bs >= 0) {
     const float *C = A.bc_c + size_t(bs) * 6 * NQ + q;
@@ -217,23 +230,17 @@ __global__ void __launch_bounds__(NG * NG * E, E == 8 ? 3 : 1) k_stiffness3d_col
         d2 = fmaf(c3_hp[iz * NG + l], uz[c][l], d2);
       }
 #pragma unroll
-      for (int j = 0; j < 3; ++j) du[c][j] = d0 * gi[0 * 3 + j] + d1 * gi[1 * 3 + j] + d2 * gi[2 * 3 + j];
+      for (int j = 0; j < 3; ++j) du[c][j] = dot3(d0, gi[0 * 3 + j], d1, gi[1 * 3 + j], d2, gi[2 * 3 + j]);
     }
-    const float lam = c0 - 2.f * mu;
     float sig[3][3];
-    sig[0][0] = c0 * du[0][0] + lam * (du[1][1] + du[2][2]);
-    sig[1][1] = c0 * du[1][1] + lam * (du[0][0] + du[2][2]);
-    sig[2][2] = c0 * du[2][2] + lam * (du[0][0] + du[1][1]);
-    sig[0][1] = sig[1][0] = mu * (du[0][1] + du[1][0]);
-    sig[0][2] = sig[2][0] = mu * (du[0][2] + du[2][0]);
-    sig[1][2] = sig[2][1] = mu * (du[1][2] + du[2][1]);
+    stress3(du, c0, mu, sig);
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
 #pragma unroll
       for (int k = 0; k < 2; ++k)
         sF[((c * 2 + k) * NG * NG + iz * NG + iy) * RP3 + ix] =
-            jac * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
-      fz[c][iz] = jac * (sig[c][0] * gi[6] + sig[c][1] * gi[7] + sig[c][2] * gi[8]);
+            jac * dot3(sig[c][0], gi[k * 3 + 0], sig[c][1], gi[k * 3 + 1], sig[c][2], gi[k * 3 + 2]);
+      fz[c][iz] = jac * dot3(sig[c][0], gi[6], sig[c][1], gi[7], sig[c][2], gi[8]);
     }
   }
 #pragma unroll
@@ -250,6 +257,7 @@ __global__ void __launch_bounds__(NG * NG * E, E == 8 ? 3 : 1) k_stiffness3d_col
   for (int iz = 0; iz < NG; ++iz) {
     const int q = (iz * NG + iy) * NG + ix;
     const float wz = c3_w[iz];
+    const float wzy = wz * wy, wzx = wz * wx, wyx = wy * wx;
     float a[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -263,7 +271,7 @@ __global__ void __launch_bounds__(NG * NG * E, E == 8 ? 3 : 1) k_stiffness3d_col
         t2 = fmaf(sF[((c * 2 + 1) * NG * NG + iz * NG + l) * RP3 + ix], hy[l], t2);
         t3 = fmaf(fz[c][l], c3_hpw[l * NG + iz], t3);
       }
-      a[c] = -(wz * wy * t1 + wz * wx * t2 + wy * wx * t3);
+      a[c] = -dot3(wzy, t1, wzx, t2, wyx, t3);
     }
     if (bs >= 0) {
       const float *C = A.bc_c + size_t(bs) * 6 * NQ + q;
