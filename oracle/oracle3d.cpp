@@ -365,20 +365,33 @@ struct Sim3D {
             dxi[c][0] = s0; dxi[c][1] = s1; dxi[c][2] = s2;
           }
           const T *gi = &g9[p * 9];
+          // device order: the map, the normal stresses and F as FMA chains,
+          // as the CUDA element kernels compute them (dot3 / stress3)
+          const bool dv = in.device_order;
+          auto dot3 = [dv](T a0, T b0, T a1, T b1, T a2, T b2) {
+            return dv ? T(std::fma(a2, b2, std::fma(a1, b1, a0 * b0))) : a0 * b0 + a1 * b1 + a2 * b2;
+          };
           T du[3][3];  // du[c][j] = d u_c / d x_j
           for (int c = 0; c < 3; ++c)
-            for (int j = 0; j < 3; ++j) du[c][j] = dxi[c][0] * gi[0 * 3 + j] + dxi[c][1] * gi[1 * 3 + j] + dxi[c][2] * gi[2 * 3 + j];
+            for (int j = 0; j < 3; ++j)
+              du[c][j] = dot3(dxi[c][0], gi[0 * 3 + j], dxi[c][1], gi[1 * 3 + j], dxi[c][2], gi[2 * 3 + j]);
           const T l2m = c0[p], m = mu[p], lam = l2m - T(2) * m;
           T sig[3][3];
-          sig[0][0] = l2m * du[0][0] + lam * (du[1][1] + du[2][2]);
-          sig[1][1] = l2m * du[1][1] + lam * (du[0][0] + du[2][2]);
-          sig[2][2] = l2m * du[2][2] + lam * (du[0][0] + du[1][1]);
+          if (dv) {
+            sig[0][0] = std::fma(l2m, du[0][0], lam * (du[1][1] + du[2][2]));
+            sig[1][1] = std::fma(l2m, du[1][1], lam * (du[0][0] + du[2][2]));
+            sig[2][2] = std::fma(l2m, du[2][2], lam * (du[0][0] + du[1][1]));
+          } else {
+            sig[0][0] = l2m * du[0][0] + lam * (du[1][1] + du[2][2]);
+            sig[1][1] = l2m * du[1][1] + lam * (du[0][0] + du[2][2]);
+            sig[2][2] = l2m * du[2][2] + lam * (du[0][0] + du[1][1]);
+          }
           sig[0][1] = sig[1][0] = m * (du[0][1] + du[1][0]);
           sig[0][2] = sig[2][0] = m * (du[0][2] + du[2][0]);
           sig[1][2] = sig[2][1] = m * (du[1][2] + du[2][1]);
           for (int c = 0; c < 3; ++c)
             for (int k = 0; k < 3; ++k)
-              F[q][c][k] = jac[p] * (sig[c][0] * gi[k * 3 + 0] + sig[c][1] * gi[k * 3 + 1] + sig[c][2] * gi[k * 3 + 2]);
+              F[q][c][k] = jac[p] * dot3(sig[c][0], gi[k * 3 + 0], sig[c][1], gi[k * 3 + 1], sig[c][2], gi[k * 3 + 2]);
         }
     T r[NP3][3];
     for (int iz = 0; iz < NG; ++iz)
@@ -400,7 +413,12 @@ struct Sim3D {
                 t3 += F[(l * NG + iy) * NG + ix][c][2] * hp[l][iz] * w[l];
               }
             }
-            r[q][c] = T(-1) * (w[iz] * w[iy] * t1 + w[iz] * w[ix] * t2 + w[iy] * w[ix] * t3);
+            if (in.device_order) {
+              const T wzy = w[iz] * w[iy], wzx = w[iz] * w[ix], wyx = w[iy] * w[ix];
+              r[q][c] = -T(std::fma(wyx, t3, std::fma(wzx, t2, wzy * t1)));
+            } else {
+              r[q][c] = T(-1) * (w[iz] * w[iy] * t1 + w[iz] * w[ix] * t2 + w[iy] * w[ix] * t3);
+            }
           }
         }
     for (int fi : face_of_elem[size_t(e)]) {
