@@ -110,3 +110,67 @@ def test_config_inputs(tmp_path):
     assert [os.path.basename(q) for q in p[:3]] == ["XX.A1.S3.BXX.semv", "XX.A1.S3.BXY.semv", "XX.A1.S3.BXZ.semv"]
     t, v = np.loadtxt(p[4]).T
     assert np.allclose(t, [-1.0, -0.965]) and np.allclose(v, seis[:, 0, 1, 1])
+
+
+def _with_hex27(db, bend=0.0):
+    """The same mesh with 27-node elements: the 19 extra nodes of every
+    element at its edge midpoints, face centres and centre (new control
+    nodes, in a shuffled order per element); `bend` moves the centre node of
+    element 0 off the trilinear map."""
+    from specfempp_b200 import database3d
+    rng = np.random.default_rng(5)
+    P = db.coords[db.elements[:, :8]]
+    coords = [db.coords]
+    extra = np.zeros((db.nspec, 19), np.int64)
+    nxt = len(db.coords)
+    for e in range(db.nspec):
+        pts = []
+        for a, b, c in database3d._HEX27_REST:
+            w = np.array([(a if s[0] else 1 - a) * (b if s[1] else 1 - b) * (c if s[2] else 1 - c)
+                          for s in database3d.CORNER_SIGNS])
+            pts.append(w @ P[e])
+        pts = np.array(pts)
+        if e == 0 and bend:
+            pts[-1] += bend
+        perm = rng.permutation(19)
+        coords.append(pts[perm])
+        extra[e] = nxt + np.arange(19)
+        nxt += 19
+    return database3d.Database3D(27, np.concatenate(coords), np.concatenate([db.elements, extra], 1),
+                                 db.material_of, db.materials, db.ngll, db.faces)
+
+
+def test_hex27_straight_accepted_curved_refused():
+    """27-node elements whose extra nodes lie on the trilinear map of their
+    corners (in any order) give the 8-node lattice; a centre node moved off
+    it is refused (the library maps elements trilinearly)."""
+    from specfempp_b200 import database3d
+    m = _distorted(3, 2, 2, 4)
+    db = database3d.parse_database3d(database3d.database3d_bytes(m, [(2000.0, 2500.0, 1400.0)],
+                                                                 np.zeros(m.nspec, np.int64)))
+    got = database3d.lattice_mesh(_with_hex27(db))
+    assert np.array_equal(got.nodes, m.nodes)
+    with pytest.raises(ValueError, match="curved"):
+        database3d.lattice_mesh(_with_hex27(db, bend=25.0))
+
+
+def test_sources3d_moment_tensor_and_refusals(tmp_path):
+    """Moment-tensor sources keep (Mxx, Myy, Mzz, Mxy, Mxz, Myz); time
+    functions other than Ricker and a wrong source count are refused."""
+    import yaml
+    from specfempp_b200 import specfem3d
+    mt = {"x": 1.0, "y": 2.0, "z": -3.0, "Mxx": 1.0, "Myy": 2.0, "Mzz": 3.0, "Mxy": 4.0, "Mxz": 5.0, "Myz": 6.0,
+          "Ricker": {"factor": 1e15, "tshift": 0.1, "f0": 2.0}}
+    p = tmp_path / "s.yaml"
+    p.write_text(yaml.safe_dump({"number-of-sources": 1, "sources": [{"moment-tensor": mt}]}))
+    (s,) = specfem3d.read_sources3d(str(p))
+    assert s.kind == "moment_tensor" and s.comp == (1.0, 2.0, 3.0, 4.0, 5.0, 6.0) and s.tshift == 0.1
+    bad = dict(mt)
+    del bad["Ricker"]
+    bad["Dirac"] = {"factor": 1.0}
+    p.write_text(yaml.safe_dump({"number-of-sources": 1, "sources": [{"moment-tensor": bad}]}))
+    with pytest.raises(ValueError, match="Ricker"):
+        specfem3d.read_sources3d(str(p))
+    p.write_text(yaml.safe_dump({"number-of-sources": 2, "sources": [{"moment-tensor": mt}]}))
+    with pytest.raises(ValueError, match="number of sources"):
+        specfem3d.read_sources3d(str(p))
