@@ -29,7 +29,7 @@ Configurations (seeded synthetic inputs of the benchmark shapes):
    + final fields of both media;
 3. batched elastic 1000x500 GRF model, 32 shots in one run, 300 steps: the
    final fields of shots 0, 15 and 31 and the traces of shot 0 against
-   single-shot oracle runs;
+   single-shot oracle runs (FP64 for shot 0 only);
 5. 3D elastic 128x128x64 hexahedra (67.6 M points), layered + GRF model,
    moment tensor: the final displacement field after 60 steps (10 Hz wavelet,
    so that the source has peaked inside the window).
@@ -69,13 +69,16 @@ def record(row):
 
 
 def check(config, quantity, got, dev32, f64, ref32=None):
+    """Record and assert one row; f64 None: the FP32 comparison alone."""
     got = np.asarray(got, np.float64)
     assert np.all(np.isfinite(got))
-    assert np.linalg.norm(f64) > 0
+    assert np.linalg.norm(dev32) > 0
     row = {"config": config, "quantity": quantity,
-           "cuda_vs_oracle_f32_device_order": rel_l2(got, dev32),
-           "cuda_vs_oracle_f64": rel_l2(got, f64),
-           "oracle_f32_device_order_vs_f64": rel_l2(dev32, f64)}
+           "cuda_vs_oracle_f32_device_order": rel_l2(got, dev32)}
+    if f64 is not None:
+        assert np.linalg.norm(f64) > 0
+        row["cuda_vs_oracle_f64"] = rel_l2(got, f64)
+        row["oracle_f32_device_order_vs_f64"] = rel_l2(dev32, f64)
     if ref32 is not None:
         row["cuda_vs_oracle_f32_reference_order"] = rel_l2(got, ref32)
         row["oracle_f32_reference_order_vs_f64"] = rel_l2(ref32, f64)
@@ -84,8 +87,9 @@ def check(config, quantity, got, dev32, f64, ref32=None):
     assert row["cuda_vs_oracle_f32_device_order"] <= row["bound"], row
     if ref32 is not None:
         assert row["cuda_vs_oracle_f32_reference_order"] <= row["bound"], row
-    floor = max(row["oracle_f32_device_order_vs_f64"], row.get("oracle_f32_reference_order_vs_f64", 0.0))
-    assert row["cuda_vs_oracle_f64"] <= 1.25 * floor + 1e-6, row
+    if f64 is not None:
+        floor = max(row["oracle_f32_device_order_vs_f64"], row.get("oracle_f32_reference_order_vs_f64", 0.0))
+        assert row["cuda_vs_oracle_f64"] <= 1.25 * floor + 1e-6, row
 
 
 def run_cuda2d(w, srcs, nstep, types, nshots=1):
@@ -171,7 +175,9 @@ def test_config3_batched_1000x500_shots(sfg_lib, oracle_lib):
         case = workload_case(w, nstep=nstep, types=types)
         case.sources = [replace(s, shot=0) for s in w.sources if s.shot == shot]
         dev = oracle_f32(case, nthreads=NT, want_final=True)
-        r64 = runner.run(case, "f64", nthreads=NT, want_final=True)
+        # FP64 for shot 0 (the error statement); shots 15 and 31 against the
+        # FP32 oracle alone (every shot runs the same arithmetic)
+        r64 = runner.run(case, "f64", nthreads=NT, want_final=True) if shot == 0 else None
         u, o = elastic_points(sim, {"dev": dev, "f64": r64}, shot=shot)
         check(cfg, f"field:displacement, shot {shot}", u, o["dev"], o["f64"])
         if shot == 0:
