@@ -10,7 +10,7 @@ Per configuration and output the test measures and records:
 
 * CUDA FP32 vs oracle FP32 (device order, and reference order for
   configurations 1 and 2): displacement seismograms and elastic final fields
-  <= 1e-5; velocity, elastic acceleration and the
+  <= 1e-5 (the parity bar of this path); velocity, elastic acceleration and the
   acoustic potential <= 1e-4; acceleration and pressure of the coupled model
   (acoustic-medium time derivatives) <= 5e-3.  The looser bounds are the
   measured FP32 noise floor: over thousands of steps each FP32 evaluation is
