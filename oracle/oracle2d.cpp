@@ -1042,17 +1042,28 @@ struct Sim {
       }
   }
 
+  // Threads of the point-wise loops below (element-wise arithmetic: the
+  // thread count changes no bit); set by run().
+  int nthr = 1;
   void predictor(std::vector<T> &u, std::vector<T> &v, std::vector<T> &a) {
     const T dt2 = dt / T(2.0), dtsq2 = dt * dt / T(2.0);
-    for (size_t i = 0; i < u.size(); ++i) {
-      u[i] += dt * v[i] + dtsq2 * a[i];
-      v[i] += dt2 * a[i];
-      a[i] = 0;
+    const long long n = (long long)u.size();
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nthr) schedule(static) if (nthr > 1 && n > 65536)
+#endif
+    for (long long i = 0; i < n; ++i) {
+      u[size_t(i)] += dt * v[size_t(i)] + dtsq2 * a[size_t(i)];
+      v[size_t(i)] += dt2 * a[size_t(i)];
+      a[size_t(i)] = 0;
     }
   }
   void corrector(std::vector<T> &v, const std::vector<T> &a) {
     const T dt2 = dt / T(2.0);
-    for (size_t i = 0; i < v.size(); ++i) v[i] += dt2 * a[i];
+    const long long n = (long long)v.size();
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nthr) schedule(static) if (nthr > 1 && n > 65536)
+#endif
+    for (long long i = 0; i < n; ++i) v[size_t(i)] += dt2 * a[size_t(i)];
   }
 
   // Greedy colouring of one medium's elements, in element order (built once).
@@ -1178,6 +1189,9 @@ struct Sim {
     }
     // divide by mass (:128-138), only on this medium's points
     const std::vector<uint8_t> &own = med == MED_ACOUSTIC ? is_ac_glob : is_el_glob;
+#ifdef _OPENMP
+#pragma omp parallel for num_threads(nthr) schedule(static) if (nthr > 1 && nglob > 65536)
+#endif
     for (int g = 0; g < nglob; ++g)
       if (own[g])
         for (int c = 0; c < ncomp; ++c) a[size_t(g) * ncomp + c] *= minv[size_t(g) * ncomp + c];
@@ -1435,6 +1449,7 @@ struct Sim {
   }
 
   void run(double *seis, int nthreads) {
+    nthr = std::max(1, nthreads);
     const int nsb = std::max(1, in.nstep_between_samples);
     int isig = 0;
     const T ca = std::cos(T(M_PI) / T(180) * T(in.rec_angle));

@@ -24,6 +24,21 @@ from .database2d import Mesh2D, read_database
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+# the same sources built for x86-64-v3 (AVX2, hardware FMA): the same bits
+LIB_PATH_V3 = os.path.join(HERE, "_build", "liboracle_v3.so")
+_V3_FLAGS = {"avx", "avx2", "bmi1", "bmi2", "f16c", "fma", "abm", "movbe", "xsave"}
+
+
+def cpu_has_x86_64_v3() -> bool:
+    """Whether the host CPU lists the x86-64-v3 instruction sets (Linux)."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return _V3_FLAGS <= set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return False
 
 SEIS_TYPES = {"displacement": 0, "velocity": 1, "acceleration": 2, "pressure": 3,
               "rotation": 4, "intrinsic_rotation": 5, "curl": 6}
@@ -65,17 +80,24 @@ _lib = None
 
 
 def build() -> str:
-    """Compile the oracle shared library with its Makefile."""
+    """Compile the oracle shared libraries with their Makefile."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
     return LIB_PATH
+
+
+def lib_path() -> str:
+    """The library this host runs: the x86-64-v3 build where the CPU has its
+    instructions, else the baseline build."""
+    return LIB_PATH_V3 if cpu_has_x86_64_v3() else LIB_PATH
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
+        path = lib_path()
+        if not os.path.exists(path):
             build()
-        _lib = C.CDLL(LIB_PATH)
+        _lib = C.CDLL(path)
         for name in ("oracle2d_run_f32", "oracle2d_run_f64"):
             fn = getattr(_lib, name)
             fn.argtypes = [C.POINTER(OracleInput2D), C.POINTER(OracleOutput2D), C.c_int]
