@@ -174,3 +174,15 @@ def test_sources3d_moment_tensor_and_refusals(tmp_path):
     p.write_text(yaml.safe_dump({"number-of-sources": 2, "sources": [{"moment-tensor": mt}]}))
     with pytest.raises(ValueError, match="number of sources"):
         specfem3d.read_sources3d(str(p))
+
+
+def test_seismogram_subsampling(tmp_path):
+    """nstep_between_samples: samples of steps 0, nsb, 2 nsb, ... written at
+    t0 + k dt nsb."""
+    from specfempp_b200 import specfem3d
+    seis = np.arange(10 * 1 * 1 * 3, dtype=np.float32).reshape(10, 1, 1, 3)
+    sub = specfem3d.subsample(seis, 4)
+    assert np.array_equal(sub[:, 0, 0, 0], seis[[0, 4, 8], 0, 0, 0])
+    p = specfem3d.write_seismograms3d(str(tmp_path), [("XX", "A")], sub, ["displacement"], -0.5, 0.01, 4)
+    t, v = np.loadtxt(p[2]).T
+    assert np.allclose(t, [-0.5, -0.46, -0.42]) and np.allclose(v, seis[[0, 4, 8], 0, 0, 2])
