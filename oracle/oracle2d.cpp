@@ -904,9 +904,23 @@ struct Sim {
   }
 
   // --------------------------------------------------------- kernels ---
+  // One element's forces for a medium of ncomp components.  The body is
+  // instantiated per component count (the loops then have fixed trip counts);
+  // the arithmetic and its order are the same for every count.
   template <typename AddFn>
   void stiffness_element(int e, int ncomp, const std::vector<T> &u, const std::vector<T> &v,
                          AddFn add) const {
+    switch (ncomp) {
+      case 1: stiffness_element_nc<1>(e, u, v, add); return;
+      case 2: stiffness_element_nc<2>(e, u, v, add); return;
+      case 3: stiffness_element_nc<3>(e, u, v, add); return;
+      default: stiffness_element_nc<4>(e, u, v, add); return;
+    }
+  }
+
+  template <int NC, typename AddFn>
+  void stiffness_element_nc(int e, const std::vector<T> &u, const std::vector<T> &v, AddFn add) const {
+    constexpr int ncomp = NC;
     T fu[NP][4], F[NP][4][2], Sa[NP][2];   // Sa: Cosserat sigma_xz, sigma_zx
     const int *ib = &ibool[size_t(e) * NP];
     for (int q = 0; q < NP; ++q)
