@@ -433,7 +433,8 @@ def run_reference(args, rank):
             "config": cfg,
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{steps} time steps of {args.workload} (full mesh), "
-                                       f"FP32 C++ restatement of the reference, OpenMP atomics"},
+                                       f"FP32 C++ restatement of the reference (reference evaluation order), "
+                                       f"colour-ordered OpenMP assembly on {threads} threads"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
