@@ -18,7 +18,8 @@ One bench step = one time step of the whole model.  Reported keys:
           chose) against the measured HBM bandwidth, its launch timed after the
           same L2 flush (frac) and back to back (frac_back_to_back);
 * cpu_baseline: the CPU oracle (a C++ restatement of the reference) on all
-          host cores, bounded sample of the same workload.
+          host cores, a bounded sample of the same workload sized by a short
+          probe run to about CPU_SAMPLE_S (10 s) of CPU time.
 ``--impl reference`` times that CPU implementation alone on the same
 workload and metric.  With --gpus N > 1 every rank runs an independent
 replica (the single-shot path does not shard) and value sums the ranks.
@@ -27,6 +28,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -138,6 +140,15 @@ def workload_config(name, w, nglob):
                   "outside the timed interval: the cache holds no input and no dirty line)"}
 
 
+CPU_SAMPLE_S = 10.0   # seconds of CPU work per baseline sample (a short probe sizes it)
+
+
+def sample_steps(probe_steps, probe_seconds, cap):
+    """Steps for about CPU_SAMPLE_S seconds of oracle time, from a probe run."""
+    per = max(probe_seconds / max(probe_steps, 1), 1e-6)
+    return int(min(cap, max(probe_steps, math.ceil(CPU_SAMPLE_S / per))))
+
+
 def cpu_oracle_throughput(w, steps, threads):
     from oracle import runner
     case = runner.Case2D(mesh=w.mesh, sources=w.sources, rec_x=w.rec_x, rec_z=w.rec_z, dt=w.dt,
@@ -198,13 +209,17 @@ def bench_batched(args, world, barrier, max_over_ranks):
         # host cores (oracle, FP32, full mesh and model)
         from oracle import runner
         threads = os.cpu_count() or 1
-        case = runner.Case2D(mesh=w.mesh, sources=[replace(w.sources[0], shot=0)], rec_x=w.rec_x, rec_z=w.rec_z,
-                             dt=w.dt, nstep=50, point_rho=w.point_rho, point_vp=w.point_vp,
-                             point_vs=w.point_vs)
-        r = runner.run(case, "f32", nthreads=threads)
-        cpu = {"value": 50 / r["loop_seconds"], "unit": "shot-steps/s", "cores": threads, "kind": "port",
-               "sample": f"50 time steps of one shot of elastic_grf_{nx}x{nz}, FP32 C++ restatement of the "
-                         f"reference on {threads} host threads ({r['loop_seconds']:.2f} s)"}
+
+        def one_shot(n):
+            case = runner.Case2D(mesh=w.mesh, sources=[replace(w.sources[0], shot=0)], rec_x=w.rec_x,
+                                 rec_z=w.rec_z, dt=w.dt, nstep=n, point_rho=w.point_rho, point_vp=w.point_vp,
+                                 point_vs=w.point_vs)
+            return runner.run(case, "f32", nthreads=threads)["loop_seconds"]
+        n = sample_steps(10, one_shot(10), 3000)
+        secs = one_shot(n)
+        cpu = {"value": n / secs, "unit": "shot-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{n} time steps of one shot of elastic_grf_{nx}x{nz}, FP32 C++ restatement of the "
+                         f"reference on {threads} host threads ({secs:.2f} s)"}
     rate_b = S_total * steps / (ms_b / 1e3)
     rate_1 = world * steps / (ms_1 / 1e3)
     per_shot_b = STEP_B_GLOB + STEP_B_LOCAL * inf.nspec * 25 / (inf.nglob * S)
@@ -357,12 +372,16 @@ def bench_3d(args, world, barrier, max_over_ranks):
         # cores (the oracle's 3D restatement, FP32)
         from oracle import runner3d
         threads = os.cpu_count() or 1
-        case = runner3d.Case3D(w.mesh, w.sources, w.rec_xyz, w.dt, 5)
-        r = runner3d.run(case, "f32", nthreads=threads)
-        out["cpu_baseline"] = {"value": inf.nglob * 5 / r["loop_seconds"], "unit": "GLL-pt/s", "cores": threads,
+
+        def run3d(n):
+            return runner3d.run(runner3d.Case3D(w.mesh, w.sources, w.rec_xyz, w.dt, n), "f32",
+                                nthreads=threads)["loop_seconds"]
+        n = sample_steps(2, run3d(2), 200)
+        secs = run3d(n)
+        out["cpu_baseline"] = {"value": inf.nglob * n / secs, "unit": "GLL-pt/s", "cores": threads,
                                "kind": "port",
-                               "sample": f"5 time steps of elastic3d_{nx}x{ny}x{nz}, FP32 C++ restatement of the "
-                                         f"reference on {threads} host threads ({r['loop_seconds']:.2f} s)"}
+                               "sample": f"{n} time steps of elastic3d_{nx}x{ny}x{nz}, FP32 C++ restatement of the "
+                                         f"reference on {threads} host threads ({secs:.2f} s)"}
     return out
 
 
@@ -605,9 +624,10 @@ def main():
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, secs = cpu_oracle_throughput(w, 40, threads)
+        n = sample_steps(20, cpu_oracle_throughput(w, 20, threads)[1], 4000)
+        v, secs = cpu_oracle_throughput(w, n, threads)
         cpu = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-               "sample": f"40 time steps of {args.workload} (full mesh), FP32 C++ restatement of the "
+               "sample": f"{n} time steps of {args.workload} (full mesh), FP32 C++ restatement of the "
                          f"reference on {threads} host threads ({secs:.2f} s)"}
 
     if world > 1:
