@@ -36,7 +36,7 @@ class ForwardConfig:
     elastic_wave: str                 # "psv" or "sh"
     database: str                     # path of database.bin
     sources: str                      # path of sources.yaml
-    stations: str                     # path of STATIONS
+    stations: object                  # path of STATIONS, or the YAML list of stations
     angle: float = 0.0
     seismogram_types: list = field(default_factory=lambda: ["displacement"])
     nstep_between_samples: int = 1
@@ -105,15 +105,25 @@ def read_config(path: str, root: str | None = None) -> ForwardConfig:
             raise ValueError(f"seismogram type {t!r} is not on this path")
     return ForwardConfig(dt=float(ts["dt"]), nstep=int(ts["nstep"]), elastic_wave="sh" if wave == "SH" else "psv",
                          database=_resolve(cfg["databases"]["mesh-database"], roots),
-                         sources=_resolve(cfg["sources"], roots), stations=_resolve(rc["stations"], roots),
+                         sources=_resolve(cfg["sources"], roots),
+                         stations=(rc["stations"] if isinstance(rc["stations"], list)
+                                   else _resolve(rc["stations"], roots)),
                          angle=float(rc.get("angle", 0.0)), seismogram_types=types,
                          nstep_between_samples=int(rc.get("nstep_between_samples", 1)),
                          output_directory=out_dir, output_format=out_fmt,
                          start_time=float(ts["t0"]) if "t0" in ts else None, **wf)
 
 
-def read_stations(path: str):
-    """2D STATIONS: (network, station) names and x, z coordinates."""
+def read_stations(path):
+    """2D STATIONS: (network, station) names and x, z coordinates; ``path``
+    may also be the configuration's YAML list of stations (network, station,
+    x, z), the reference's second form (src/io/receivers/dim2/read_receivers.cpp)."""
+    if isinstance(path, list):
+        if not path:
+            raise ValueError("No receiver stations found in the YAML file")
+        names = [(str(st["network"]), str(st["station"])) for st in path]
+        return (names, np.asarray([float(st["x"]) for st in path], np.float64),
+                np.asarray([float(st["z"]) for st in path], np.float64))
     names, xs, zs = [], [], []
     with open(path) as f:
         for line in f:

@@ -45,10 +45,16 @@ class Source3DSpec:
     comp: tuple         # (fx, fy, fz, 0, 0, 0) or (Mxx, Myy, Mzz, Mxy, Mxz, Myz)
 
 
-def read_stations3d(path: str):
+def read_stations3d(path):
     """3D STATIONS lines ``station network y x elevation z`` (the y and x
     columns are latitude-like and longitude-like): (network, station) names
-    and [nrec, 3] (x, y, z)."""
+    and [nrec, 3] (x, y, z).  ``path`` may also be the configuration's YAML
+    list of stations (network, station, x, y, z)."""
+    if isinstance(path, list):
+        if not path:
+            raise ValueError("No receiver stations found in the YAML file")
+        return ([(str(st["network"]), str(st["station"])) for st in path],
+                np.asarray([[float(st["x"]), float(st["y"]), float(st["z"])] for st in path], np.float64))
     names, xyz = [], []
     with open(path) as f:
         for line in f:

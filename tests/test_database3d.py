@@ -186,3 +186,27 @@ def test_seismogram_subsampling(tmp_path):
     p = specfem3d.write_seismograms3d(str(tmp_path), [("XX", "A")], sub, ["displacement"], -0.5, 0.01, 4)
     t, v = np.loadtxt(p[2]).T
     assert np.allclose(t, [-0.5, -0.46, -0.42]) and np.allclose(v, seis[[0, 4, 8], 0, 0, 2])
+
+
+def test_stations_as_yaml_sequences(tmp_path):
+    """Stations given inline in the configuration (the readers' second form):
+    the 3D list gives the same receivers as the fixture's STATIONS file, and
+    the 2D reader takes (network, station, x, z) entries."""
+    import yaml
+    from specfempp_b200 import io, specfem3d
+    cfg_path, z = write_fixture_dir3d(FIX3D, str(tmp_path))
+    names, xyz = specfem3d.read_stations3d(str(tmp_path / "STATIONS"))
+    cfg = yaml.safe_load(open(cfg_path))
+    cfg["parameters"]["receivers"]["stations"] = [
+        {"network": n, "station": s, "x": float(p[0]), "y": float(p[1]), "z": float(p[2])}
+        for (n, s), p in zip(names, xyz)]
+    with open(cfg_path, "w") as f:
+        yaml.safe_dump(cfg, f)
+    c = io.read_config(cfg_path, str(tmp_path))
+    n2, xyz2 = specfem3d.read_stations3d(c.stations)
+    assert n2 == names and np.array_equal(xyz2, xyz)
+    n, x, zz = io.read_stations([{"network": "AA", "station": "S1", "x": 10.0, "z": 20.0},
+                                 {"network": "AA", "station": "S2", "x": 30.0, "z": 40.0}])
+    assert n == [("AA", "S1"), ("AA", "S2")] and np.array_equal(x, [10.0, 30.0]) and np.array_equal(zz, [20.0, 40.0])
+    with pytest.raises(ValueError):
+        specfem3d.read_stations3d([])
