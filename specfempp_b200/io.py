@@ -35,7 +35,7 @@ class ForwardConfig:
     nstep: int
     elastic_wave: str                 # "psv" or "sh"
     database: str                     # path of database.bin
-    sources: str                      # path of sources.yaml
+    sources: object                   # path of sources.yaml, or the sources node itself
     stations: object                  # path of STATIONS, or the YAML list of stations
     angle: float = 0.0
     seismogram_types: list = field(default_factory=lambda: ["displacement"])
@@ -105,7 +105,8 @@ def read_config(path: str, root: str | None = None) -> ForwardConfig:
             raise ValueError(f"seismogram type {t!r} is not on this path")
     return ForwardConfig(dt=float(ts["dt"]), nstep=int(ts["nstep"]), elastic_wave="sh" if wave == "SH" else "psv",
                          database=_resolve(cfg["databases"]["mesh-database"], roots),
-                         sources=_resolve(cfg["sources"], roots),
+                         sources=(cfg["sources"] if isinstance(cfg["sources"], dict)
+                                  else _resolve(cfg["sources"], roots)),
                          stations=(rc["stations"] if isinstance(rc["stations"], list)
                                    else _resolve(rc["stations"], roots)),
                          angle=float(rc.get("angle", 0.0)), seismogram_types=types,
@@ -136,12 +137,22 @@ def read_stations(path):
     return names, np.asarray(xs, np.float64), np.asarray(zs, np.float64)
 
 
-def read_sources(path: str):
-    """Sources of a ``sources.yaml`` as ``sfg.Source`` objects."""
+def load_sources_node(path):
+    """The sources node: a ``sources.yaml`` file, or the node given inline in
+    the configuration (the reference tries the file first, then the node:
+    src/io/sources/dim2/read_sources.cpp, dim3/read_sources.cpp)."""
+    if isinstance(path, dict):
+        return path
     import yaml
-    from .sfg import Source
     with open(path) as f:
-        d = yaml.safe_load(f)
+        return yaml.safe_load(f)
+
+
+def read_sources(path):
+    """Sources of a ``sources.yaml`` (or an inline sources node) as
+    ``sfg.Source`` objects."""
+    from .sfg import Source
+    d = load_sources_node(path)
     out = []
     for s in d["sources"]:
         if "force" in s:

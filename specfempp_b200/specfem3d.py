@@ -68,12 +68,11 @@ def read_stations3d(path):
     return names, np.asarray(xyz, np.float64).reshape(-1, 3)
 
 
-def read_sources3d(path: str):
+def read_sources3d(path):
     """Force (x, y, z, fx, fy, fz) and moment-tensor (x, y, z, Mxx, Myy, Mzz,
-    Mxy, Mxz, Myz) sources with a Ricker time function."""
-    import yaml
-    with open(path) as f:
-        d = yaml.safe_load(f)
+    Mxy, Mxz, Myz) sources with a Ricker time function, from a sources file
+    or the sources node given inline in the configuration."""
+    d = io.load_sources_node(path)
     out = []
     for s in d["sources"]:
         if "force" in s:

@@ -210,3 +210,22 @@ def test_stations_as_yaml_sequences(tmp_path):
     assert n == [("AA", "S1"), ("AA", "S2")] and np.array_equal(x, [10.0, 30.0]) and np.array_equal(zz, [20.0, 40.0])
     with pytest.raises(ValueError):
         specfem3d.read_stations3d([])
+
+
+def test_sources_inline_node(tmp_path):
+    """The sources node given inline in the configuration reads like the
+    fixture's force.yaml (3D) and like a sources.yaml (2D)."""
+    import yaml
+    from specfempp_b200 import io, specfem3d
+    cfg_path, z = write_fixture_dir3d(FIX3D, str(tmp_path))
+    node = yaml.safe_load(open(tmp_path / "force.yaml"))
+    cfg = yaml.safe_load(open(cfg_path))
+    cfg["parameters"]["sources"] = node
+    with open(cfg_path, "w") as f:
+        yaml.safe_dump(cfg, f)
+    c = io.read_config(cfg_path, str(tmp_path))
+    assert specfem3d.read_sources3d(c.sources) == specfem3d.read_sources3d(str(tmp_path / "force.yaml"))
+    two = {"number-of-sources": 1, "sources": [{"force": {"x": 1.0, "z": 2.0, "angle": 0.0,
+                                                          "Ricker": {"factor": 1e10, "tshift": 0.0, "f0": 5.0}}}]}
+    (s,) = io.read_sources(two)
+    assert (s.x, s.z, s.f0, s.factor, s.kind) == (1.0, 2.0, 5.0, 1e10, "force")
